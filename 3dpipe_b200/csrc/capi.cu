@@ -1,0 +1,193 @@
+// capi.cu -- context management and the refine seam of the C ABI (include/tdp.h).
+#include <float.h>
+#include <string.h>
+#include <vector>
+#include "ctx.cuh"
+#include "refine.cuh"
+
+namespace tdp {
+
+int fail(tdp_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    return code;
+}
+
+cudaError_t dmalloc(tdp_ctx* ctx, void** p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (ctx->budget && ctx->in_use + bytes > ctx->budget) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) { *p = nullptr; return e; }
+    ctx->allocs[*p] = bytes;
+    ctx->in_use += bytes;
+    if (ctx->in_use > ctx->peak) ctx->peak = ctx->in_use;
+    return cudaSuccess;
+}
+
+void dfree(tdp_ctx* ctx, void* p) {
+    if (!p) return;
+    auto it = ctx->allocs.find(p);
+    if (it != ctx->allocs.end()) {
+        ctx->in_use -= it->second;
+        ctx->allocs.erase(it);
+    }
+    cudaFree(p);
+}
+
+int ensure(tdp_ctx* ctx, Buf& b, size_t bytes) {
+    if (bytes <= b.cap && b.p) return TDP_OK;
+    if (b.p) { dfree(ctx, b.p); b.p = nullptr; b.cap = 0; }
+    size_t want = bytes + bytes / 4 + 256;
+    cudaError_t e = dmalloc(ctx, &b.p, want);
+    if (e != cudaSuccess) {
+        e = dmalloc(ctx, &b.p, bytes);
+        if (e != cudaSuccess)
+            return fail(ctx, TDP_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed: " +
+                                               (ctx->budget && ctx->in_use + bytes > ctx->budget
+                                                    ? std::string("context budget exceeded")
+                                                    : std::string(cudaGetErrorString(e))));
+        b.cap = bytes;
+        return TDP_OK;
+    }
+    b.cap = want;
+    return TDP_OK;
+}
+
+}  // namespace tdp
+
+using namespace tdp;
+
+extern "C" {
+
+int tdp_ctx_create(int device, size_t budget_bytes, unsigned flags, tdp_ctx** out) {
+    (void)flags;
+    if (!out) return TDP_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return TDP_ERR_NODEV;
+    if (device < 0 || device >= n) return TDP_ERR_ARG;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return TDP_ERR_NODEV;
+    if (prop.major != 10) return TDP_ERR_NODEV;  // kernels are built for sm_100a only
+    if (cudaSetDevice(device) != cudaSuccess) return TDP_ERR_NODEV;
+    tdp_ctx* ctx = new tdp_ctx();
+    ctx->device = device;
+    ctx->budget = budget_bytes;
+    ctx->num_sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return TDP_ERR_CUDA; }
+    for (auto& e : ctx->ev) cudaEventCreate(&e);
+    if (dmalloc(ctx, (void**)&ctx->d_counter, 64 * sizeof(unsigned)) != cudaSuccess ||
+        dmalloc(ctx, (void**)&ctx->d_stats, 64 * sizeof(unsigned long long)) != cudaSuccess) {
+        tdp_ctx_destroy(ctx);
+        return TDP_ERR_NOMEM;
+    }
+    *out = ctx;
+    return TDP_OK;
+}
+
+int tdp_ctx_destroy(tdp_ctx* ctx) {
+    if (!ctx) return TDP_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    std::vector<void*> ptrs;
+    for (auto& kv : ctx->allocs) ptrs.push_back(kv.first);
+    for (void* p : ptrs) dfree(ctx, p);
+    for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return TDP_OK;
+}
+
+const char* tdp_last_error(const tdp_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int tdp_last_stats(const tdp_ctx* ctx, tdp_stats* o) {
+    if (!ctx || !o) return TDP_ERR_ARG;
+    const LastStats& s = ctx->stats;
+    o->refine_ms = s.refine_ms;
+    o->filter_ms = s.filter_ms;
+    o->total_ms = s.total_ms;
+    o->full_evals = s.full_evals;
+    o->tri_pairs = s.tri_pairs;
+    o->refine_items = s.refine_items;
+    o->refine_launches = s.refine_launches;
+    o->recheck_pairs = s.recheck_pairs;
+    o->filter_pairs = s.filter_pairs;
+    o->filter_voxel_pairs = s.filter_voxel_pairs;
+    o->kernel_launches = s.kernel_launches;
+    return TDP_OK;
+}
+
+int tdp_ctx_memory(const tdp_ctx* ctx, size_t* in_use, size_t* peak) {
+    if (!ctx) return TDP_ERR_ARG;
+    if (in_use) *in_use = ctx->in_use;
+    if (peak) *peak = ctx->peak;
+    return TDP_OK;
+}
+
+int tdp_refine_batch(tdp_ctx* ctx, const float* data, const float* hausdorff, size_t element_num,
+                     const size_t* offset_size, uint32_t pair_num, int form, float* out) {
+    if (!ctx) return TDP_ERR_ARG;
+    if (pair_num == 0) return TDP_OK;
+    if (!data || !offset_size || !out) return fail(ctx, TDP_ERR_ARG, "null buffer");
+    if (form != TDP_FORM_PLAIN && form != TDP_FORM_TUNED) return fail(ctx, TDP_ERR_ARG, "unknown form");
+    if (element_num == 0 || element_num > 0xffffffffull) return fail(ctx, TDP_ERR_ARG, "element_num out of range");
+    cudaSetDevice(ctx->device);
+    std::vector<RefineItem> items(pair_num);
+    double tri_pairs = 0;
+    for (uint32_t i = 0; i < pair_num; ++i) {
+        size_t o1 = offset_size[4 * i], n1 = offset_size[4 * i + 1];
+        size_t o2 = offset_size[4 * i + 2], n2 = offset_size[4 * i + 3];
+        if (o1 + n1 > element_num || o2 + n2 > element_num || o1 + n1 < o1 || o2 + n2 < o2)
+            return fail(ctx, TDP_ERR_ARG, "offset_size entry " + std::to_string(i) + " out of range");
+        items[i] = RefineItem{(uint32_t)o1, (uint32_t)n1, (uint32_t)o2, (uint32_t)n2};
+        tri_pairs += (double)n1 * (double)n2;
+    }
+    int rc;
+    if ((rc = ensure(ctx, ctx->scratch[kSlotRawData], element_num * 9 * sizeof(float)))) return rc;
+    if (hausdorff && (rc = ensure(ctx, ctx->scratch[kSlotRawHd], element_num * 2 * sizeof(float)))) return rc;
+    if ((rc = ensure(ctx, ctx->scratch[kSlotTris], element_num * kTriF4 * sizeof(float4)))) return rc;
+    if ((rc = ensure(ctx, ctx->scratch[kSlotItems], pair_num * sizeof(RefineItem)))) return rc;
+    if ((rc = ensure(ctx, ctx->scratch[kSlotOut], pair_num * sizeof(float4)))) return rc;
+    float* d_data = (float*)ctx->scratch[kSlotRawData].p;
+    float* d_hd = hausdorff ? (float*)ctx->scratch[kSlotRawHd].p : nullptr;
+    float4* d_tri = (float4*)ctx->scratch[kSlotTris].p;
+    RefineItem* d_items = (RefineItem*)ctx->scratch[kSlotItems].p;
+    float4* d_out = (float4*)ctx->scratch[kSlotOut].p;
+    cudaStream_t s = ctx->stream;
+    TDP_CUDA_TRY(cudaMemcpyAsync(d_data, data, element_num * 9 * sizeof(float), cudaMemcpyHostToDevice, s));
+    if (d_hd) TDP_CUDA_TRY(cudaMemcpyAsync(d_hd, hausdorff, element_num * 2 * sizeof(float), cudaMemcpyHostToDevice, s));
+    TDP_CUDA_TRY(cudaMemcpyAsync(d_items, items.data(), pair_num * sizeof(RefineItem), cudaMemcpyHostToDevice, s));
+    TDP_CUDA_TRY(launch_pack_triangles(d_data, d_hd, element_num, d_tri, s));
+    TDP_CUDA_TRY(cudaMemsetAsync(ctx->d_stats, 0, sizeof(unsigned long long), s));
+    TDP_CUDA_TRY(cudaEventRecord(ctx->ev[0], s));
+    if (form == TDP_FORM_PLAIN) {
+        TDP_CUDA_TRY(launch_refine_plain(d_tri, d_tri, d_items, (int)pair_num, d_out, s));
+    } else {
+        TDP_CUDA_TRY(launch_refine_tuned(d_tri, d_tri, d_items, (int)pair_num, d_out, ctx->d_counter, ctx->d_stats,
+                                         ctx->num_sms, ctx->tuned_ctas_per_sm, s));
+    }
+    TDP_CUDA_TRY(cudaEventRecord(ctx->ev[1], s));
+    std::vector<float4> res(pair_num);
+    unsigned long long full = 0;
+    TDP_CUDA_TRY(cudaMemcpyAsync(res.data(), d_out, pair_num * sizeof(float4), cudaMemcpyDeviceToHost, s));
+    TDP_CUDA_TRY(cudaMemcpyAsync(&full, ctx->d_stats, sizeof(full), cudaMemcpyDeviceToHost, s));
+    TDP_CUDA_TRY(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    ctx->stats = LastStats();
+    ctx->stats.refine_ms = ms;
+    ctx->stats.total_ms = ms;
+    ctx->stats.tri_pairs = tri_pairs;
+    ctx->stats.full_evals = form == TDP_FORM_PLAIN ? (unsigned long long)tri_pairs : full;
+    ctx->stats.refine_items = pair_num;
+    ctx->stats.refine_launches = 1;
+    ctx->stats.kernel_launches = 2;
+    for (uint32_t i = 0; i < pair_num; ++i) {
+        out[3 * i] = res[i].x;
+        out[3 * i + 1] = hausdorff ? res[i].y : FLT_MAX;
+        out[3 * i + 2] = hausdorff ? res[i].z : FLT_MAX;
+    }
+    return TDP_OK;
+}
+
+}  // extern "C"

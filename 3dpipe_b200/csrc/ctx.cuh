@@ -1,0 +1,61 @@
+// ctx.cuh -- the context object behind the C ABI: device, stream, memory budget,
+// reusable scratch buffers and the statistics of the last call.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <unordered_map>
+#include "common.cuh"
+#include "../../include/tdp.h"
+
+namespace tdp {
+
+struct Buf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+// Statistics of the last refine launch / join, filled by the library.
+struct LastStats {
+    double refine_ms = 0;            // device time of refine kernels (CUDA events)
+    double filter_ms = 0;            // device time of filter kernels
+    double total_ms = 0;             // device time of the whole call
+    unsigned long long full_evals = 0;  // triangle pairs fully evaluated
+    double tri_pairs = 0;            // sum of n1*n2 over refined voxel pairs
+    long refine_items = 0;           // voxel pairs refined (all LODs)
+    long refine_launches = 0;
+    long recheck_pairs = 0;          // object pairs recomputed in FP64
+    long filter_pairs = 0;           // object pairs through the filter
+    double filter_voxel_pairs = 0;   // voxel pairs evaluated by the filter
+    long kernel_launches = 0;        // kernels launched by the call
+};
+
+}  // namespace tdp
+
+struct tdp_ctx {
+    int device = 0;
+    int num_sms = 148;
+    size_t budget = 0, in_use = 0, peak = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[8] = {};
+    std::string last_error;
+    std::unordered_map<void*, size_t> allocs;
+    tdp::Buf scratch[16];
+    unsigned* d_counter = nullptr;            // work counters (device)
+    unsigned long long* d_stats = nullptr;    // device-side statistics
+    tdp::LastStats stats;
+    int tuned_ctas_per_sm = 4;
+};
+
+namespace tdp {
+
+int fail(tdp_ctx* ctx, int code, const std::string& msg);
+cudaError_t dmalloc(tdp_ctx* ctx, void** p, size_t bytes);
+void dfree(tdp_ctx* ctx, void* p);
+// grow-only scratch buffer; returns TDP_OK or an error status (recorded in ctx)
+int ensure(tdp_ctx* ctx, Buf& b, size_t bytes);
+
+enum ScratchSlot {
+    kSlotRawData = 0, kSlotRawHd, kSlotTris, kSlotItems, kSlotOut,
+};
+
+}  // namespace tdp

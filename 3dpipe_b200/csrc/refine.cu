@@ -1,0 +1,305 @@
+// refine.cu -- the LOD refine: for every voxel pair, the minimum triangle
+// distance and the two Hausdorff-widened bounds over all triangle pairs.
+//
+// Reference: TriDist_cuda_op_shm_flat_fused (src/geometry/computing_gpu.cu:1069-1152),
+// launched one CTA of 512 threads per voxel pair by
+// MeshDist_batch_gpu_op_shm_flat_stream (computing_gpu.cu:6540-6658).
+// Outputs per voxel pair (float4):
+//   x = min d,  y = min max(d - ph1 - ph2, 0),  z = min d + h1 + h2,
+//   w = R, the largest |coordinate| after translation to the pair origin
+//       (the FP32 error bound of x is err_bound(R), see common.cuh).
+//
+// Two forms:
+//   refine_plain_kernel  one CTA per voxel pair, both voxels staged in shared
+//                        memory, every triangle pair fully evaluated.  This is the
+//                        "plain GPU form" the tuned form is measured against.
+//   refine_tuned_kernel  persistent, one warp per voxel pair pulled from an atomic
+//                        work counter; A-side triangles are pre-processed once
+//                        into shared memory, each lane owns one B-side triangle
+//                        in registers, and a bounding-sphere test against the
+//                        warp's running minima skips pairs that cannot lower any
+//                        of the three minima.
+#include <float.h>
+#include "common.cuh"
+#include "tridist.cuh"
+#include "refine.cuh"
+
+namespace tdp {
+
+__device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
+
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// ------------------------------------------------------------------ plain form
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) refine_plain_kernel(const float4* __restrict__ triA,
+                                                             const float4* __restrict__ triB,
+                                                             const RefineItem* __restrict__ items,
+                                                             int n_items, float4* __restrict__ out) {
+    constexpr int CH = 128;  // triangles staged per side per round
+    __shared__ float4 sa[CH * kTriF4];
+    __shared__ float4 sb[CH * kTriF4];
+    __shared__ float red[4][BLOCK / 32];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const RefineItem w = items[it];
+        if (w.a_cnt == 0 || w.b_cnt == 0) {
+            if (tid == 0) out[it] = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, 0.f);
+            continue;
+        }
+        const float4 o4 = triA[(size_t)w.a_off * kTriF4];
+        float dmin = FLT_MAX, lomin = FLT_MAX, himin = FLT_MAX, rmax = 0.f;
+        for (uint32_t a0 = 0; a0 < w.a_cnt; a0 += CH) {
+            const int ca = min((uint32_t)CH, w.a_cnt - a0);
+            for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += CH) {
+                const int cb = min((uint32_t)CH, w.b_cnt - b0);
+                __syncthreads();
+                for (int k = tid; k < ca * kTriF4; k += BLOCK) {
+                    float4 t = triA[((size_t)w.a_off + a0) * kTriF4 + k];
+                    t.x -= o4.x; t.y -= o4.y; t.z -= o4.z;
+                    rmax = fmaxf(rmax, fmaxf(fabsf(t.x), fmaxf(fabsf(t.y), fabsf(t.z))));
+                    sa[k] = t;
+                }
+                for (int k = tid; k < cb * kTriF4; k += BLOCK) {
+                    float4 t = triB[((size_t)w.b_off + b0) * kTriF4 + k];
+                    t.x -= o4.x; t.y -= o4.y; t.z -= o4.z;
+                    rmax = fmaxf(rmax, fmaxf(fabsf(t.x), fmaxf(fabsf(t.y), fabsf(t.z))));
+                    sb[k] = t;
+                }
+                __syncthreads();
+                for (int p = tid; p < ca * cb; p += BLOCK) {
+                    const int i = p / cb, j = p - i * cb;
+                    const float4 a0v = sa[3 * i], a1v = sa[3 * i + 1], a2v = sa[3 * i + 2];
+                    const float4 b0v = sb[3 * j], b1v = sb[3 * j + 1], b2v = sb[3 * j + 2];
+                    PreTri<float> A, B;
+                    pretri(A, v3(a0v.x, a0v.y, a0v.z), v3(a1v.x, a1v.y, a1v.z), v3(a2v.x, a2v.y, a2v.z));
+                    pretri(B, v3(b0v.x, b0v.y, b0v.z), v3(b1v.x, b1v.y, b1v.z), v3(b2v.x, b2v.y, b2v.z));
+                    const float d = sqrtf(tri_dist2(A, B));
+                    dmin = fminf(dmin, d);
+                    lomin = fminf(lomin, fmaxf(d - a0v.w - b0v.w, 0.f));
+                    himin = fminf(himin, d + a1v.w + b1v.w);
+                }
+            }
+        }
+        dmin = warp_min(dmin); lomin = warp_min(lomin); himin = warp_min(himin); rmax = warp_max(rmax);
+        __syncthreads();
+        if (lane == 0) { red[0][wid] = dmin; red[1][wid] = lomin; red[2][wid] = himin; red[3][wid] = rmax; }
+        __syncthreads();
+        if (tid == 0) {
+            for (int k = 1; k < BLOCK / 32; ++k) {
+                dmin = fminf(dmin, red[0][k]); lomin = fminf(lomin, red[1][k]);
+                himin = fminf(himin, red[2][k]); rmax = fmaxf(rmax, red[3][k]);
+            }
+            out[it] = make_float4(dmin, lomin, himin, rmax);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ tuned form
+// Shared-memory image of one pre-processed triangle, structure-of-arrays so a
+// broadcast read of triangle k by the whole warp is conflict-free.
+constexpr int kPreF = 43;  // 37 PreTri floats + centre(3) + radius + ph + h
+constexpr int kTunedCA = 64;  // A-side triangles per shared-memory chunk
+
+__device__ __forceinline__ void store_pre(float* s, int k, const PreTri<float>& t, float3 c, float r,
+                                          float ph, float h) {
+    float* p = s + k;
+#define PUT(i, v) p[(i) * kTunedCA] = (v)
+    PUT(0, t.v[0].x); PUT(1, t.v[0].y); PUT(2, t.v[0].z);
+    PUT(3, t.v[1].x); PUT(4, t.v[1].y); PUT(5, t.v[1].z);
+    PUT(6, t.v[2].x); PUT(7, t.v[2].y); PUT(8, t.v[2].z);
+    PUT(9, t.e[0].x); PUT(10, t.e[0].y); PUT(11, t.e[0].z);
+    PUT(12, t.e[1].x); PUT(13, t.e[1].y); PUT(14, t.e[1].z);
+    PUT(15, t.e[2].x); PUT(16, t.e[2].y); PUT(17, t.e[2].z);
+    PUT(18, t.n.x); PUT(19, t.n.y); PUT(20, t.n.z); PUT(21, t.inn);
+    PUT(22, t.ee[0]); PUT(23, t.ee[1]); PUT(24, t.ee[2]);
+    PUT(25, t.iee[0]); PUT(26, t.iee[1]); PUT(27, t.iee[2]);
+    PUT(28, t.m[0].x); PUT(29, t.m[0].y); PUT(30, t.m[0].z);
+    PUT(31, t.m[1].x); PUT(32, t.m[1].y); PUT(33, t.m[1].z);
+    PUT(34, t.m[2].x); PUT(35, t.m[2].y); PUT(36, t.m[2].z);
+    PUT(37, c.x); PUT(38, c.y); PUT(39, c.z); PUT(40, r); PUT(41, ph); PUT(42, h);
+#undef PUT
+}
+
+__device__ __forceinline__ void load_pre(const float* s, int k, PreTri<float>& t) {
+    const float* p = s + k;
+#define GET(i) p[(i) * kTunedCA]
+    t.v[0] = v3(GET(0), GET(1), GET(2)); t.v[1] = v3(GET(3), GET(4), GET(5)); t.v[2] = v3(GET(6), GET(7), GET(8));
+    t.e[0] = v3(GET(9), GET(10), GET(11)); t.e[1] = v3(GET(12), GET(13), GET(14)); t.e[2] = v3(GET(15), GET(16), GET(17));
+    t.n = v3(GET(18), GET(19), GET(20)); t.inn = GET(21);
+    t.ee[0] = GET(22); t.ee[1] = GET(23); t.ee[2] = GET(24);
+    t.iee[0] = GET(25); t.iee[1] = GET(26); t.iee[2] = GET(27);
+    t.m[0] = v3(GET(28), GET(29), GET(30)); t.m[1] = v3(GET(31), GET(32), GET(33)); t.m[2] = v3(GET(34), GET(35), GET(36));
+#undef GET
+}
+
+__device__ __forceinline__ void tri_sphere(const PreTri<float>& t, float3& c, float& r) {
+    c = make_float3((t.v[0].x + t.v[1].x + t.v[2].x) * (1.f / 3.f), (t.v[0].y + t.v[1].y + t.v[2].y) * (1.f / 3.f),
+                    (t.v[0].z + t.v[1].z + t.v[2].z) * (1.f / 3.f));
+    float r2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float dx = t.v[k].x - c.x, dy = t.v[k].y - c.y, dz = t.v[k].z - c.z;
+        r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
+    }
+    // inflate so FP32 rounding of the centre/radius can never cull a needed pair
+    r = sqrtf(r2) * 1.0001f + 1e-6f;
+}
+
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) refine_tuned_kernel(const float4* __restrict__ triA,
+                                                                  const float4* __restrict__ triB,
+                                                                  const RefineItem* __restrict__ items,
+                                                                  int n_items, float4* __restrict__ out,
+                                                                  unsigned* __restrict__ work_counter,
+                                                                  unsigned long long* __restrict__ n_full) {
+    extern __shared__ float smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float* sA = smem + (size_t)wid * kPreF * kTunedCA;
+    unsigned long long full_evals = 0;
+
+    while (true) {
+        unsigned it = 0;
+        if (lane == 0) it = atomicAdd(work_counter, 1u);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= (unsigned)n_items) break;
+        const RefineItem w = items[it];
+        if (w.a_cnt == 0 || w.b_cnt == 0) {
+            if (lane == 0) out[it] = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, 0.f);
+            continue;
+        }
+        const float4 o4 = triA[(size_t)w.a_off * kTriF4];
+        float bd = FLT_MAX, bl = FLT_MAX, bh = FLT_MAX, rmax = 0.f;
+
+        for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += 32) {
+            const bool bval = b0 + lane < w.b_cnt;
+            PreTri<float> B;
+            float3 cB = make_float3(0.f, 0.f, 0.f);
+            float rB = 0.f, phB = 0.f, hB = 0.f;
+            if (bval) {
+                const float4* tb = triB + ((size_t)w.b_off + b0 + lane) * kTriF4;
+                float4 t0 = tb[0], t1 = tb[1], t2 = tb[2];
+                pretri(B, v3(t0.x - o4.x, t0.y - o4.y, t0.z - o4.z), v3(t1.x - o4.x, t1.y - o4.y, t1.z - o4.z),
+                       v3(t2.x - o4.x, t2.y - o4.y, t2.z - o4.z));
+                phB = t0.w; hB = t1.w;
+                tri_sphere(B, cB, rB);
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    rmax = fmaxf(rmax, fmaxf(fabsf(B.v[k].x), fmaxf(fabsf(B.v[k].y), fabsf(B.v[k].z))));
+            }
+            for (uint32_t a0 = 0; a0 < w.a_cnt; a0 += kTunedCA) {
+                const int ca = min((uint32_t)kTunedCA, w.a_cnt - a0);
+                __syncwarp();
+                for (int k = lane; k < ca; k += 32) {
+                    const float4* ta = triA + ((size_t)w.a_off + a0 + k) * kTriF4;
+                    float4 t0 = ta[0], t1 = ta[1], t2 = ta[2];
+                    PreTri<float> A;
+                    pretri(A, v3(t0.x - o4.x, t0.y - o4.y, t0.z - o4.z), v3(t1.x - o4.x, t1.y - o4.y, t1.z - o4.z),
+                           v3(t2.x - o4.x, t2.y - o4.y, t2.z - o4.z));
+                    float3 c; float r;
+                    tri_sphere(A, c, r);
+#pragma unroll
+                    for (int q = 0; q < 3; ++q)
+                        rmax = fmaxf(rmax, fmaxf(fabsf(A.v[q].x), fmaxf(fabsf(A.v[q].y), fabsf(A.v[q].z))));
+                    store_pre(sA, k, A, c, r, t0.w, t1.w);
+                }
+                __syncwarp();
+                for (int k = 0; k < ca; ++k) {
+                    if ((k & 7) == 0) { bd = warp_min(bd); bl = warp_min(bl); bh = warp_min(bh); }
+                    if (!bval) continue;
+                    const float* p = sA + k;
+                    const float cx = p[37 * kTunedCA], cy = p[38 * kTunedCA], cz = p[39 * kTunedCA];
+                    const float rA = p[40 * kTunedCA], phA = p[41 * kTunedCA], hA = p[42 * kTunedCA];
+                    const float thr = fmaxf(bd, fmaxf(bl + phA + phB, bh - hA - hB));
+                    const float reach = rA + rB + thr;
+                    const float dx = cx - cB.x, dy = cy - cB.y, dz = cz - cB.z;
+                    const float cc = dx * dx + dy * dy + dz * dz;
+                    if (reach < 0.f || cc > reach * reach) continue;  // cannot lower any minimum
+                    PreTri<float> A;
+                    load_pre(sA, k, A);
+                    const float d = sqrtf(tri_dist2(A, B));
+                    ++full_evals;
+                    bd = fminf(bd, d);
+                    bl = fminf(bl, fmaxf(d - phA - phB, 0.f));
+                    bh = fminf(bh, d + hA + hB);
+                }
+            }
+        }
+        bd = warp_min(bd); bl = warp_min(bl); bh = warp_min(bh); rmax = warp_max(rmax);
+        if (lane == 0) out[it] = make_float4(bd, bl, bh, rmax);
+    }
+    // per-warp count of full evaluations (the rest were culled)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) full_evals += __shfl_xor_sync(0xffffffffu, full_evals, o);
+    if (lane == 0 && n_full) atomicAdd(n_full, full_evals);
+}
+
+// ------------------------------------------------------------------ launchers
+constexpr int kPlainBlock = 256;
+constexpr int kTunedWarps = 4;
+
+cudaError_t launch_refine_plain(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
+                                float4* out, cudaStream_t s) {
+    if (n_items <= 0) return cudaSuccess;
+    int grid = n_items < (1 << 30) ? n_items : (1 << 30);
+    refine_plain_kernel<kPlainBlock><<<grid, kPlainBlock, 0, s>>>(triA, triB, items, n_items, out);
+    return cudaGetLastError();
+}
+
+size_t tuned_smem_bytes(int warps) { return (size_t)warps * kPreF * kTunedCA * sizeof(float); }
+
+cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
+                                float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
+                                int ctas_per_sm, cudaStream_t s) {
+    if (n_items <= 0) return cudaSuccess;
+    static bool attr_set = false;
+    const size_t smem = tuned_smem_bytes(kTunedWarps);
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(refine_tuned_kernel<kTunedWarps>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    cudaError_t e = cudaMemsetAsync(work_counter, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    long want = (long)num_sms * ctas_per_sm;
+    long need = ((long)n_items + kTunedWarps - 1) / kTunedWarps;
+    int grid = (int)(want < need ? want : need);
+    if (grid < 1) grid = 1;
+    refine_tuned_kernel<kTunedWarps><<<grid, kTunedWarps * 32, smem, s>>>(triA, triB, items, n_items, out,
+                                                                          work_counter, n_full);
+    return cudaGetLastError();
+}
+
+// Pack the reference's flat layout (9 floats per triangle + 2 Hausdorff floats)
+// into 48-byte triangle records.
+__global__ void pack_triangles_kernel(const float* __restrict__ data, const float* __restrict__ hd, size_t n,
+                                      float4* __restrict__ tri) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float* d = data + 9 * i;
+        float ph = hd ? hd[2 * i] : 0.f, h = hd ? hd[2 * i + 1] : 0.f;
+        tri[3 * i + 0] = make_float4(d[0], d[1], d[2], ph);
+        tri[3 * i + 1] = make_float4(d[3], d[4], d[5], h);
+        tri[3 * i + 2] = make_float4(d[6], d[7], d[8], 0.f);
+    }
+}
+
+cudaError_t launch_pack_triangles(const float* data, const float* hd, size_t n, float4* tri, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    size_t blocks = (n + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    pack_triangles_kernel<<<(unsigned)blocks, 256, 0, s>>>(data, hd, n, tri);
+    return cudaGetLastError();
+}
+
+}  // namespace tdp

@@ -1,0 +1,16 @@
+// refine.cuh -- launchers for the refine kernels (see refine.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace tdp {
+
+cudaError_t launch_refine_plain(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
+                                float4* out, cudaStream_t s);
+cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
+                                float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
+                                int ctas_per_sm, cudaStream_t s);
+size_t tuned_smem_bytes(int warps);
+cudaError_t launch_pack_triangles(const float* data, const float* hd, size_t n, float4* tri, cudaStream_t s);
+
+}  // namespace tdp

@@ -1,0 +1,25 @@
+/*
+ * oracle/oracle.h -- TEST INFRASTRUCTURE ONLY (the FP64 checker for the CUDA path).
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load this.
+ */
+#ifndef TDP_ORACLE_H
+#define TDP_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* triangle-triangle distance, FP64, closest-feature method (see tridist.c) */
+double tdo_tri_dist(const double *S9, const double *T9);
+/* independent FP64 formulation used to cross-check tdo_tri_dist */
+double tdo_tri_dist_features(const double *S9, const double *T9);
+void tdo_tri_dist_batch(const double *S, const double *T, size_t n, double *out_pqp, double *out_feat);
+/* MeshDist restated in FP64: out = {distance, min low bound, min high bound} */
+void tdo_voxel_pair(const float *tri1, const float *hd1, size_t n1,
+                    const float *tri2, const float *hd2, size_t n2, double out[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
