@@ -27,7 +27,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = shutil.which("g++") or "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                     "--expt-relaxed-constexpr", "-I", str(ROOT / "include")]
+                     "--expt-relaxed-constexpr", "-I", str(ROOT / "include"), "-I", str(PKG / "src")]
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-Wall", "-Wno-unused-function",
              "-I", str(ROOT / "include"), "-I", str(PKG / "src"),
              "-I", "/usr/local/cuda/include"]

@@ -39,7 +39,7 @@ struct tdp_ctx {
     cudaEvent_t ev[8] = {};
     std::string last_error;
     std::unordered_map<void*, size_t> allocs;
-    tdp::Buf scratch[16];
+    tdp::Buf scratch[64];
     unsigned* d_counter = nullptr;            // work counters (device)
     unsigned long long* d_stats = nullptr;    // device-side statistics
     tdp::LastStats stats;

@@ -1,0 +1,356 @@
+// join_kernels.cu -- the filter and LOD-loop kernels of the spatial join.
+//
+// Reference correspondence (paths inside lyuheng/3dpipe):
+//   k_pair_bounds      voxel_pair_dist_kernel_for_all_aggregate_distance and the
+//                      min reduction of the streaming kernels
+//                      (src/geometry/computing_gpu.cu:1984-2043, :2155-2359),
+//                      voxel bounds voxel_dist_core (:1606-1631)
+//   k_within_decide    filter-time classification (src/join/WithinJoin.cpp:164-252)
+//                      and the per-LOD within decision (WithinJoin.cpp:769-792)
+//   k_knn_rank         evaluate_knn_kernel (computing_gpu.cu:105-151) + the confirm
+//                      cap in candidate order (src/join/KNNJoin.cpp:133-202)
+//   k_count/write_vps  record_valid_voxel_pairs_streaming_{knn,within}
+//                      (computing_gpu.cu:2604-2812): voxel pairs with
+//                      min <= object min-max (and <= tau for within), in (i,j) order
+//   k_build_items      packing_data_stream's voxel-pair list (src/join/SpatialJoin.cpp:169-248),
+//                      skipping voxels empty at this LOD (KNNJoin.cpp:1662)
+//   k_apply_results    the per-voxel-pair bound update (KNNJoin.cpp:1668-1705)
+//   k_pair_update      SpatialJoin::update_voxel_pair_list (SpatialJoin.cpp:48-69):
+//                      object min over all voxel pairs, max over the updated ones,
+//                      eviction of voxel pairs whose min exceeds that max
+// The reference's block reductions in the filter assume a power-of-two block
+// (computing_gpu.cu:2027-2033, blockDim = min(max_voxel_size, 1024)); the
+// reductions here are exact for any voxel count.
+#include <cub/device/device_scan.cuh>
+#include <float.h>
+
+#include "join_kernels.cuh"
+
+namespace tdp {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ float wmin(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// voxel_dist_core: box gap and core-core distance, a = tile-1 voxel, b = tile-2 voxel
+__device__ __forceinline__ void vox_dist(const float4* __restrict__ va, const float4* __restrict__ vb, float& mn,
+                                         float& mx) {
+    const float4 alo = va[0], ahi = va[1], ac = va[2];
+    const float4 blo = vb[0], bhi = vb[1], bc = vb[2];
+    float m = 0.f, M = 0.f, t1, t2, dc;
+    t1 = alo.x - bhi.x; t2 = ahi.x - blo.x;
+    if (t2 < 0.f) m += t2 * t2; else if (t1 > 0.f) m += t1 * t1;
+    dc = ac.x - bc.x; M += dc * dc;
+    t1 = alo.y - bhi.y; t2 = ahi.y - blo.y;
+    if (t2 < 0.f) m += t2 * t2; else if (t1 > 0.f) m += t1 * t1;
+    dc = ac.y - bc.y; M += dc * dc;
+    t1 = alo.z - bhi.z; t2 = ahi.z - blo.z;
+    if (t2 < 0.f) m += t2 * t2; else if (t1 > 0.f) m += t1 * t1;
+    dc = ac.z - bc.z; M += dc * dc;
+    mn = sqrtf(m);
+    mx = sqrtf(M);
+}
+
+// relative FP32 error of a box gap / core distance: a handful of roundings
+constexpr float kVoxRel = 8.0f * kUnitRoundoff;
+
+__global__ void __launch_bounds__(kBlock) k_pair_bounds(JoinDev d) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
+        const int q = d.pq[p], t = d.pt[p];
+        const uint32_t a0 = d.ovox1[q], a1 = d.ovox1[q + 1], b0 = d.ovox2[t], b1 = d.ovox2[t + 1];
+        float mn = FLT_MAX, mx = FLT_MAX;
+        for (uint32_t b = b0 + lane; b < b1; b += 32) {
+            const float4* vb = d.vox2 + 3 * (size_t)b;
+            for (uint32_t a = a0; a < a1; ++a) {
+                float m, M;
+                vox_dist(d.vox1 + 3 * (size_t)a, vb, m, M);
+                mn = fminf(mn, m);
+                mx = fminf(mx, M);
+            }
+        }
+        mn = wmin(mn);
+        mx = wmin(mx);
+        if (lane == 0) {
+            d.pmn[p] = mn;
+            d.pmx[p] = mx;
+            d.perr[p] = kVoxRel * fmaxf(mn, mx);
+            d.pstat[p] = kUndecided;
+        }
+    }
+}
+
+__global__ void k_within_decide(JoinDev d, float tau, int tuned) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.P; p += gridDim.x * blockDim.x) {
+        if (d.pstat[p] != kUndecided) continue;
+        const float e = tuned ? d.perr[p] : 0.f;
+        if (d.pmx[p] + e <= tau) d.pstat[p] = kReported;
+        else if (d.pmn[p] - e > tau) d.pstat[p] = kDropped;
+    }
+}
+
+__global__ void k_knn_rank(JoinDev d, int K, int tuned, int* __restrict__ st) {
+    for (int q = blockIdx.x; q < d.N1; q += gridDim.x) {
+        const int64_t b = d.qoff[q], e = d.qoff[q + 1];
+        int conf = d.qconf[q];
+        if (conf < K) {
+            const int cand_left = K - conf;
+            for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+                if (d.pstat[i] != kUndecided) continue;
+                const float ei = tuned ? d.perr[i] : 0.f;
+                const float lo = d.pmn[i] - ei, hi = d.pmx[i] + ei;
+                int sure = 0, maybe = 0;
+                for (int64_t j = b; j < e; ++j) {
+                    if (j == i || d.pstat[j] != kUndecided) continue;
+                    const float ej = tuned ? d.perr[j] : 0.f;
+                    if (lo >= d.pmx[j] + ej) ++sure;
+                    if (!(hi <= d.pmn[j] - ej)) ++maybe;
+                }
+                st[i] = maybe < cand_left ? 1 : (sure >= cand_left ? 2 : 0);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (int64_t i = b; i < e; ++i) {
+                    if (d.pstat[i] != kUndecided) continue;
+                    if (conf >= K) break;
+                    if (st[i] == 1) { d.pstat[i] = kReported; ++conf; }
+                    else if (st[i] == 2) d.pstat[i] = kDropped;
+                }
+                d.qconf[q] = conf;
+            }
+            __syncthreads();
+            conf = d.qconf[q];
+        }
+        if (conf >= K)  // query complete: nothing left to refine for it
+            for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x)
+                if (d.pstat[i] == kUndecided) d.pstat[i] = kDropped;
+        __syncthreads();
+    }
+}
+
+template <bool WRITE>
+__global__ void __launch_bounds__(kBlock) k_vps(JoinDev d, int within, float tau, int tuned, int64_t* __restrict__ cnt) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
+        if (d.pstat[p] != kUndecided) {
+            if (!WRITE && lane == 0) cnt[p] = 0;
+            continue;
+        }
+        const int q = d.pq[p], t = d.pt[p];
+        const uint32_t a0 = d.ovox1[q], b0 = d.ovox2[t];
+        const uint32_t n1 = d.ovox1[q + 1] - a0, n2 = d.ovox2[t + 1] - b0;
+        const float slack = tuned ? d.perr[p] : 0.f;
+        const float lim = d.pmx[p] + slack;
+        const uint64_t total = (uint64_t)n1 * n2;
+        int64_t pos = WRITE ? d.pvp[p] : 0;
+        int64_t count = 0;
+        for (uint64_t base = 0; base < total; base += 32) {
+            const uint64_t k = base + lane;
+            bool keep = false;
+            float m = 0.f, M = 0.f;
+            uint32_t a = 0, bb = 0;
+            if (k < total) {
+                a = (uint32_t)(k / n2);
+                bb = (uint32_t)(k - (uint64_t)a * n2);
+                vox_dist(d.vox1 + 3 * (size_t)(a0 + a), d.vox2 + 3 * (size_t)(b0 + bb), m, M);
+                keep = (m - slack <= lim) && (!within || m - slack <= tau);
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (WRITE && keep) {
+                const int64_t w = pos + __popc(bal & ((1u << lane) - 1u));
+                d.vpa[w] = (int)(a0 + a);
+                d.vpb[w] = (int)(b0 + bb);
+                d.vpair[w] = p;
+                d.vmn[w] = m;
+                d.vmx[w] = M;
+                d.verr[w] = kVoxRel * fmaxf(m, M);
+                d.valive[w] = 1;
+                d.vupd[w] = -1;
+            }
+            pos += __popc(bal);
+            count += __popc(bal);
+        }
+        if (!WRITE && lane == 0) cnt[p] = count;
+    }
+}
+
+__global__ void k_build_items(JoinDev d, const uint32_t* __restrict__ vt1, const uint32_t* __restrict__ vt2,
+                              RefineItem* __restrict__ items, int* __restrict__ item_vp, unsigned* __restrict__ counter) {
+    // counter[0] = items, counter[2..3] = sum n1*n2 (u64)
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < d.V; v += (int64_t)gridDim.x * blockDim.x) {
+        bool ok = d.valive[v] && d.pstat[d.vpair[v]] == kUndecided;
+        uint32_t o1 = 0, n1 = 0, o2 = 0, n2 = 0;
+        if (ok) {
+            const int a = d.vpa[v], b = d.vpb[v];
+            o1 = vt1[a]; n1 = vt1[a + 1] - o1;
+            o2 = vt2[b]; n2 = vt2[b + 1] - o2;
+            ok = n1 > 0 && n2 > 0;
+        }
+        if (ok) {
+            const unsigned w = atomicAdd(counter, 1u);
+            items[w] = RefineItem{o1, n1, o2, n2};
+            item_vp[w] = (int)v;
+            atomicAdd(reinterpret_cast<unsigned long long*>(counter + 2), (unsigned long long)n1 * n2);
+        }
+    }
+}
+
+__global__ void k_apply_results(JoinDev d, const float4* __restrict__ res, const int* __restrict__ item_vp, int W,
+                                int highest, int level, int li, int stamp) {
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) {
+        const int v = item_vp[w];
+        const float4 r = res[w];
+        float mn = d.vmn[v], mx = d.vmx[v];
+        const float e = err_bound(r.w);
+        if (highest) {
+            mn = r.x;
+            mx = r.x;
+        } else if (level == 2) {
+            mn = fminf(mn, r.y);
+            mx = fminf(mx, r.z);
+        } else if (level == 1) {
+            const int p = d.vpair[v];
+            const int q = d.pq[p], t = d.pt[p];
+            mn = fminf(mn, r.x - d.ohd1[q * 5 + li] - d.ohd2[t * 5 + li]);
+            mx = fminf(mx, r.x + d.ophd1[q * 5 + li] + d.ophd2[t * 5 + li]);
+        } else {
+            mx = fminf(mx, r.x);
+        }
+        d.vmn[v] = mn;
+        d.vmx[v] = mx;
+        d.verr[v] = fmaxf(d.verr[v], e + 4.f * kUnitRoundoff * fmaxf(fabsf(mn), fabsf(mx)));
+        d.vupd[v] = stamp;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_pair_update(JoinDev d, int stamp) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
+        if (d.pstat[p] != kUndecided) continue;
+        const int64_t b = d.pvp[p], e = d.pvp[p + 1];
+        float minmax = INFINITY, mindist = FLT_MAX, err = 0.f;
+        for (int64_t v = b + lane; v < e; v += 32) {
+            if (!d.valive[v]) continue;
+            mindist = fminf(mindist, d.vmn[v]);
+            err = fmaxf(err, d.verr[v]);
+            if (d.vupd[v] == stamp) minmax = fminf(minmax, d.vmx[v]);
+        }
+        minmax = wmin(minmax);
+        mindist = wmin(mindist);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) err = fmaxf(err, __shfl_xor_sync(0xffffffffu, err, o));
+        for (int64_t v = b + lane; v < e; v += 32)
+            if (d.valive[v] && d.vmn[v] > minmax) d.valive[v] = 0;
+        if (lane == 0) {
+            d.pmn[p] = mindist;
+            d.pmx[p] = minmax;
+            d.perr[p] = err;
+        }
+    }
+}
+
+__global__ void k_count_status(JoinDev d, unsigned* __restrict__ c) {
+    unsigned und = 0, rep = 0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.P; p += gridDim.x * blockDim.x) {
+        und += d.pstat[p] == kUndecided;
+        rep += d.pstat[p] == kReported;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        und += __shfl_xor_sync(0xffffffffu, und, o);
+        rep += __shfl_xor_sync(0xffffffffu, rep, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (und) atomicAdd(c + 0, und);
+        if (rep) atomicAdd(c + 1, rep);
+    }
+}
+
+__global__ void k_collect(JoinDev d, int* __restrict__ oq, int* __restrict__ ot, float* __restrict__ od,
+                          unsigned* __restrict__ counter) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.P; p += gridDim.x * blockDim.x) {
+        if (d.pstat[p] != kReported) continue;
+        const unsigned w = atomicAdd(counter, 1u);
+        oq[w] = d.pq[p];
+        ot[w] = d.pt[p];
+        if (od) od[w] = d.pmx[p];
+    }
+}
+
+int grid_for(int64_t n, int per_block, int cap = 148 * 32) {
+    int64_t g = (n + per_block - 1) / per_block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (int)g;
+}
+
+}  // namespace
+
+cudaError_t launch_pair_bounds(const JoinDev& d, cudaStream_t s) {
+    if (d.P <= 0) return cudaSuccess;
+    k_pair_bounds<<<grid_for(d.P, kBlock / 32), kBlock, 0, s>>>(d);
+    return cudaGetLastError();
+}
+cudaError_t launch_within_decide(const JoinDev& d, float tau, int tuned, cudaStream_t s) {
+    if (d.P <= 0) return cudaSuccess;
+    k_within_decide<<<grid_for(d.P, 256), 256, 0, s>>>(d, tau, tuned);
+    return cudaGetLastError();
+}
+cudaError_t launch_knn_rank(const JoinDev& d, int K, int tuned, int* st, cudaStream_t s) {
+    if (d.N1 <= 0) return cudaSuccess;
+    k_knn_rank<<<grid_for(d.N1, 1, 148 * 64), 128, 0, s>>>(d, K, tuned, st);
+    return cudaGetLastError();
+}
+cudaError_t launch_count_vps(const JoinDev& d, int within, float tau, int tuned, int64_t* cnt, cudaStream_t s) {
+    if (d.P <= 0) return cudaSuccess;
+    k_vps<false><<<grid_for(d.P, kBlock / 32), kBlock, 0, s>>>(d, within, tau, tuned, cnt);
+    return cudaGetLastError();
+}
+cudaError_t launch_write_vps(const JoinDev& d, int within, float tau, int tuned, cudaStream_t s) {
+    if (d.P <= 0) return cudaSuccess;
+    k_vps<true><<<grid_for(d.P, kBlock / 32), kBlock, 0, s>>>(d, within, tau, tuned, nullptr);
+    return cudaGetLastError();
+}
+cudaError_t launch_build_items(const JoinDev& d, const uint32_t* vt1, const uint32_t* vt2, RefineItem* items,
+                               int* item_vp, unsigned* counter, cudaStream_t s) {
+    if (d.V <= 0) return cudaSuccess;
+    k_build_items<<<grid_for(d.V, 256), 256, 0, s>>>(d, vt1, vt2, items, item_vp, counter);
+    return cudaGetLastError();
+}
+cudaError_t launch_apply_results(const JoinDev& d, const float4* res, const int* item_vp, int W, int highest,
+                                 int level, int li, int stamp, cudaStream_t s) {
+    if (W <= 0) return cudaSuccess;
+    k_apply_results<<<grid_for(W, 256), 256, 0, s>>>(d, res, item_vp, W, highest, level, li, stamp);
+    return cudaGetLastError();
+}
+cudaError_t launch_pair_update(const JoinDev& d, int stamp, cudaStream_t s) {
+    if (d.P <= 0) return cudaSuccess;
+    k_pair_update<<<grid_for(d.P, kBlock / 32), kBlock, 0, s>>>(d, stamp);
+    return cudaGetLastError();
+}
+cudaError_t launch_count_status(const JoinDev& d, unsigned* c, cudaStream_t s) {
+    if (d.P <= 0) return cudaSuccess;
+    k_count_status<<<grid_for(d.P, 256, 148 * 8), 256, 0, s>>>(d, c);
+    return cudaGetLastError();
+}
+cudaError_t launch_collect(const JoinDev& d, int* oq, int* ot, float* od, unsigned* counter, cudaStream_t s) {
+    if (d.P <= 0) return cudaSuccess;
+    k_collect<<<grid_for(d.P, 256), 256, 0, s>>>(d, oq, ot, od, counter);
+    return cudaGetLastError();
+}
+
+cudaError_t scan_counts(const int64_t* cnt, int64_t* out, int n, void* temp, size_t& temp_bytes, cudaStream_t s) {
+    // exclusive scan of n+1 values (cnt[n] must be 0) so out[n] is the total
+    return cub::DeviceScan::ExclusiveSum(temp, temp_bytes, cnt, out, n + 1, s);
+}
+
+}  // namespace tdp

@@ -1,0 +1,72 @@
+// join_kernels.cuh -- device state of one join and the launchers of its kernels.
+// The orchestration (LOD loop, decisions, result collection) lives in
+// src/join/join_driver.cpp; every kernel here is one step of the reference's
+// filter + LOD refine loop (reference src/join/KNNJoin.cpp, WithinJoin.cpp,
+// src/geometry/computing_gpu.cu), restated for device-resident state.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace tdp {
+
+enum PairStatus : uint8_t { kUndecided = 0, kReported = 1, kDropped = 2 };
+
+struct JoinDev {
+    // tiles
+    const float4* vox1;
+    const uint32_t* ovox1;
+    const float4* vox2;
+    const uint32_t* ovox2;
+    const float* ohd1;
+    const float* ophd1;
+    const float* ohd2;
+    const float* ophd2;
+    // object pairs (candidates), grouped by query object
+    int P;
+    const int* pq;
+    const int* pt;
+    float* pmn;
+    float* pmx;
+    float* perr;  // FP32 error bound of the pair range (tuned form)
+    uint8_t* pstat;
+    int64_t* pvp;  // [P+1] first voxel pair of each pair
+    // queries
+    int N1;
+    const int64_t* qoff;  // [N1+1]
+    int* qconf;
+    // voxel pairs kept after the filter
+    int64_t V;
+    int* vpa;
+    int* vpb;
+    int* vpair;
+    float* vmn;
+    float* vmx;
+    float* verr;
+    uint8_t* valive;
+    int* vupd;
+};
+
+// filter: per object pair, min box gap and min core distance over all voxel pairs
+cudaError_t launch_pair_bounds(const JoinDev& d, cudaStream_t s);
+// within: classify pairs at the filter (min > tau drop, max <= tau report)
+cudaError_t launch_within_decide(const JoinDev& d, float tau, int tuned, cudaStream_t s);
+// kNN: the bulk rank rule per query object, then the confirm cap at K
+cudaError_t launch_knn_rank(const JoinDev& d, int K, int tuned, int* scratch_status, cudaStream_t s);
+// voxel-pair compaction of undecided pairs: count, then write in order
+cudaError_t launch_count_vps(const JoinDev& d, int within, float tau, int tuned, int64_t* cnt, cudaStream_t s);
+cudaError_t launch_write_vps(const JoinDev& d, int within, float tau, int tuned, cudaStream_t s);
+// LOD step
+cudaError_t launch_build_items(const JoinDev& d, const uint32_t* vtri1, const uint32_t* vtri2, RefineItem* items,
+                               int* item_vp, unsigned* counter, cudaStream_t s);
+cudaError_t launch_apply_results(const JoinDev& d, const float4* res, const int* item_vp, int W, int highest,
+                                 int level, int lod_idx, int stamp, cudaStream_t s);
+cudaError_t launch_pair_update(const JoinDev& d, int stamp, cudaStream_t s);
+cudaError_t launch_count_status(const JoinDev& d, unsigned* counters, cudaStream_t s);
+cudaError_t launch_collect(const JoinDev& d, int* out_q, int* out_t, float* out_d, unsigned* counter,
+                           cudaStream_t s);
+// exclusive scan of n int64 counts into out[0..n] (out[n] = total)
+cudaError_t scan_counts(const int64_t* cnt, int64_t* out, int n, void* temp, size_t& temp_bytes, cudaStream_t s);
+
+}  // namespace tdp

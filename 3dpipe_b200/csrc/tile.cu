@@ -1,0 +1,196 @@
+// tile.cu -- upload of a RAW .dt tile into HBM (tdp_tile_upload / tdp_tile_free).
+//
+// Replaces Tile::load + HiMesh_Wrapper(RAW) + HiMesh_Wrapper::decode_to and the
+// per-chunk packing of triangles into pinned buffers (reference
+// src/storage/tile_IO.cpp:13-49, src/spatial/himesh_wrapper.cpp:17-83 and
+// :137-169, src/join/SpatialJoin.cpp:169-248): the whole tile, every LOD, is
+// made resident once, so no LOD step ever re-packs or re-copies triangles.
+//
+// The raw bytes are copied to the device in chunks of whole objects and
+// unpacked by a kernel (one warp per voxel/LOD segment) into 48-byte triangle
+// records.  Every field of a RAW object is 4 or 8 bytes, so every float sits a
+// multiple of 4 bytes after its object's first byte; a chunk is copied starting
+// at an object's first byte into a 256-byte aligned staging buffer, which makes
+// every float 4-byte aligned on the device (checked on the host per segment).
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ctx.cuh"
+#include "storage/dev_tile.h"
+
+namespace tdp {
+
+struct UnpackSeg {
+    uint64_t src;      // byte offset of the segment's triangles in the staging buffer
+    uint32_t dst;      // first destination triangle in tri[lod]
+    uint32_t cnt_lod;  // count (low 24 bits) | lod << 24
+};
+
+struct TriPtrs {
+    float4* p[kNumLods];
+};
+
+__global__ void unpack_kernel(const uint8_t* __restrict__ raw, const UnpackSeg* __restrict__ segs, int nseg,
+                              TriPtrs tri) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nseg; s += warps) {
+        const UnpackSeg g = segs[s];
+        const uint32_t n = g.cnt_lod & 0xffffffu;
+        float4* dst = tri.p[g.cnt_lod >> 24] + (size_t)g.dst * 3;
+        const float* t = reinterpret_cast<const float*>(raw + g.src);
+        const float* h = t + 9 * (size_t)n;
+        for (uint32_t i = lane; i < n; i += 32) {
+            const float* q = t + 9 * (size_t)i;
+            dst[3 * (size_t)i + 0] = make_float4(q[0], q[1], q[2], h[2 * i]);
+            dst[3 * (size_t)i + 1] = make_float4(q[3], q[4], q[5], h[2 * i + 1]);
+            dst[3 * (size_t)i + 2] = make_float4(q[6], q[7], q[8], 0.f);
+        }
+    }
+}
+
+void tile_release(tdp_ctx* ctx, tdp_tile* t) {
+    if (!t) return;
+    dfree(ctx, t->vox);
+    dfree(ctx, t->obj_vox);
+    dfree(ctx, t->obj_hd);
+    dfree(ctx, t->obj_phd);
+    for (int l = 0; l < kNumLods; ++l) {
+        dfree(ctx, t->tri[l]);
+        dfree(ctx, t->vtri[l]);
+    }
+    delete t;
+}
+
+}  // namespace tdp
+
+using namespace tdp;
+
+extern "C" {
+
+int tdp_tile_upload(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, tdp_tile** out) {
+    if (!ctx || !out) return TDP_ERR_ARG;
+    *out = nullptr;
+    if (!raw_dt) return fail(ctx, TDP_ERR_ARG, "null tile buffer");
+    cudaSetDevice(ctx->device);
+    const uint8_t* buf = (const uint8_t*)raw_dt;
+    tdp_tile* T = new tdp_tile();
+    T->device = ctx->device;
+    std::string err;
+    int rc = parse_raw_dt(buf, len, max_objects, T->host, err);
+    if (rc != TDP_OK) {
+        delete T;
+        return fail(ctx, rc, err);
+    }
+    TileHost& H = T->host;
+    T->n_obj = H.n_obj;
+    T->n_vox = H.n_vox;
+    for (int l = 0; l < kNumLods; ++l) {
+        if (H.n_tris[l] >= 0xffffffffull) { delete T; return fail(ctx, TDP_ERR_FORMAT, "more than 2^32 triangles in one LOD"); }
+        for (long v = 0; v < H.n_vox; ++v)
+            if ((H.vox_byte_off[l][v] & 3u) != 1u) { delete T; return fail(ctx, TDP_ERR_FORMAT, "misaligned triangle data"); }
+        T->h_vtri[l].resize(H.n_vox + 1);
+        T->h_vtri[l][0] = 0;
+        for (long v = 0; v < H.n_vox; ++v) T->h_vtri[l][v + 1] = T->h_vtri[l][v] + H.vox_cnt[l][v];
+    }
+    auto alloc = [&](void** p, size_t bytes) -> int {
+        if (dmalloc(ctx, p, bytes) != cudaSuccess)
+            return fail(ctx, TDP_ERR_NOMEM, "tile upload: cannot allocate " + std::to_string(bytes) + " bytes" +
+                                                (ctx->budget ? " within the context budget" : ""));
+        T->device_bytes += bytes;
+        return TDP_OK;
+    };
+    cudaStream_t s = ctx->stream;
+#define TRY(x) do { int _r = (x); if (_r) { tile_release(ctx, T); return _r; } } while (0)
+#define CTRY(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { tile_release(ctx, T); return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } } while (0)
+    TRY(alloc((void**)&T->vox, (size_t)H.n_vox * 3 * sizeof(float4)));
+    TRY(alloc((void**)&T->obj_vox, (size_t)(H.n_obj + 1) * sizeof(uint32_t)));
+    TRY(alloc((void**)&T->obj_hd, (size_t)H.n_obj * kNumLods * sizeof(float)));
+    TRY(alloc((void**)&T->obj_phd, (size_t)H.n_obj * kNumLods * sizeof(float)));
+    for (int l = 0; l < kNumLods; ++l) {
+        TRY(alloc((void**)&T->tri[l], (size_t)H.n_tris[l] * 3 * sizeof(float4)));
+        TRY(alloc((void**)&T->vtri[l], (size_t)(H.n_vox + 1) * sizeof(uint32_t)));
+    }
+    {
+        std::vector<float4> v4((size_t)H.n_vox * 3);
+        for (long v = 0; v < H.n_vox; ++v) {
+            const float* b = &H.vox_box[9 * v];
+            v4[3 * v + 0] = make_float4(b[0], b[1], b[2], 0.f);
+            v4[3 * v + 1] = make_float4(b[3], b[4], b[5], 0.f);
+            v4[3 * v + 2] = make_float4(b[6], b[7], b[8], 0.f);
+        }
+        CTRY(cudaMemcpyAsync(T->vox, v4.data(), v4.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
+        CTRY(cudaMemcpyAsync(T->obj_vox, H.obj_vox_off.data(), H.obj_vox_off.size() * 4, cudaMemcpyHostToDevice, s));
+        CTRY(cudaMemcpyAsync(T->obj_hd, H.obj_hd.data(), H.obj_hd.size() * 4, cudaMemcpyHostToDevice, s));
+        CTRY(cudaMemcpyAsync(T->obj_phd, H.obj_phd.data(), H.obj_phd.size() * 4, cudaMemcpyHostToDevice, s));
+        for (int l = 0; l < kNumLods; ++l)
+            CTRY(cudaMemcpyAsync(T->vtri[l], T->h_vtri[l].data(), T->h_vtri[l].size() * 4, cudaMemcpyHostToDevice, s));
+        CTRY(cudaStreamSynchronize(s));
+    }
+    // chunked copy + unpack of the triangle data, whole objects per chunk
+    const size_t kChunk = (size_t)1 << 30;
+    Buf& stage = ctx->scratch[12];
+    Buf& segbuf = ctx->scratch[13];
+    TriPtrs tp;
+    for (int l = 0; l < kNumLods; ++l) tp.p[l] = T->tri[l];
+    std::vector<UnpackSeg> segs;
+    long o0 = 0;
+    while (o0 < H.n_obj) {
+        // the object's first byte: its floats sit at a multiple of 4 bytes from it
+        const uint64_t base = H.obj_data_off[o0] - 8;
+        long o1 = o0 + 1;
+        while (o1 < H.n_obj && H.obj_data_off[o1] + H.obj_data_size[o1] - base <= kChunk) ++o1;
+        const uint64_t end = H.obj_data_off[o1 - 1] + H.obj_data_size[o1 - 1];
+        const size_t bytes = (size_t)(end - base);
+        TRY(ensure(ctx, stage, bytes + 16));
+        segs.clear();
+        for (long o = o0; o < o1; ++o)
+            for (uint32_t v = H.obj_vox_off[o]; v < H.obj_vox_off[o + 1]; ++v)
+                for (int l = 0; l < kNumLods; ++l) {
+                    uint32_t n = H.vox_cnt[l][v];
+                    if (!n) continue;
+                    const uint64_t src = H.vox_byte_off[l][v] - base;
+                    if ((src & 3u) || src + (uint64_t)n * 44 > bytes) {  // never launch a misaligned read
+                        tile_release(ctx, T);
+                        return fail(ctx, TDP_ERR_FORMAT, "triangle block of object " + std::to_string(o) +
+                                                             " is not 4-byte aligned within its object");
+                    }
+                    segs.push_back({src, T->h_vtri[l][v], n | ((uint32_t)l << 24)});
+                }
+        TRY(ensure(ctx, segbuf, std::max<size_t>(segs.size(), 1) * sizeof(UnpackSeg)));
+        CTRY(cudaMemcpyAsync(stage.p, buf + base, bytes, cudaMemcpyHostToDevice, s));
+        CTRY(cudaMemcpyAsync(segbuf.p, segs.data(), segs.size() * sizeof(UnpackSeg), cudaMemcpyHostToDevice, s));
+        if (!segs.empty()) {
+            int blocks = (int)std::min<size_t>((segs.size() + 7) / 8, (size_t)ctx->num_sms * 16);
+            unpack_kernel<<<blocks, 256, 0, s>>>((const uint8_t*)stage.p, (const UnpackSeg*)segbuf.p, (int)segs.size(), tp);
+            CTRY(cudaGetLastError());
+        }
+        CTRY(cudaStreamSynchronize(s));
+        o0 = o1;
+    }
+#undef TRY
+#undef CTRY
+    *out = T;
+    return TDP_OK;
+}
+
+int tdp_tile_free(tdp_ctx* ctx, tdp_tile* tile) {
+    if (!ctx || !tile) return TDP_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    tile_release(ctx, tile);
+    return TDP_OK;
+}
+
+int tdp_tile_get_info(const tdp_tile* t, tdp_tile_info* o) {
+    if (!t || !o) return TDP_ERR_ARG;
+    o->n_objects = t->n_obj;
+    o->n_voxels = t->n_vox;
+    for (int l = 0; l < kNumLods; ++l) o->n_tris[l] = (long)t->host.n_tris[l];
+    o->device_bytes = t->device_bytes;
+    return TDP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,216 @@
+// candidates.cpp -- grid-based object candidate generation (see candidates.h).
+#include "index/candidates.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <queue>
+#include <thread>
+
+namespace tdp {
+
+float box_gap(const float* a, const float* b) {
+    // aab::distance (reference src/spatial/himesh_box.cpp:149-168), mindist part,
+    // with a = the indexed object, b = the query box
+    float m = 0.f;
+    for (int i = 0; i < 3; ++i) {
+        float t1 = a[i] - b[3 + i];
+        float t2 = a[3 + i] - b[i];
+        if (t2 < 0.f)
+            m += t2 * t2;
+        else if (t1 > 0.f)
+            m += t1 * t1;
+    }
+    return std::sqrt(m);
+}
+
+float point_dist(const float* a, const float* b) {
+    // octree.cpp:268-272: distance between the two objects' transform points
+    float dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+    return std::sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+namespace {
+
+struct Grid {
+    float lo[3] = {0, 0, 0};
+    float cell = 1.f;
+    int n[3] = {1, 1, 1};
+    std::vector<int64_t> start;  // CSR over cells
+    std::vector<int32_t> items;
+
+    int ci(float v, int k) const {
+        long c = (long)std::floor((v - lo[k]) / cell);
+        return (int)std::min<long>(std::max<long>(c, 0), n[k] - 1);
+    }
+    size_t id(int x, int y, int z) const { return ((size_t)x * n[1] + y) * n[2] + z; }
+
+    // boxes: 6 floats per object (a point grid passes lo == hi)
+    void build(const float* boxes, long count, int stride_lo, int stride_hi, float cell_) {
+        cell = cell_;
+        float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        lo[0] = lo[1] = lo[2] = INFINITY;
+        for (long i = 0; i < count; ++i)
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = std::min(lo[k], boxes[i * stride_lo + k]);
+                hi[k] = std::max(hi[k], boxes[i * stride_lo + stride_hi + k]);
+            }
+        // keep the number of cells bounded (about 8 per object)
+        const double max_cells = std::max(4096.0, 8.0 * (double)count);
+        auto cells_for = [&](float c) {
+            double p = 1;
+            for (int k = 0; k < 3; ++k) p *= std::ceil((hi[k] - lo[k]) / c) + 1;
+            return p;
+        };
+        while (cells_for(cell) > max_cells) cell *= 1.25f;
+        for (int k = 0; k < 3; ++k) n[k] = std::max(1, (int)std::ceil((hi[k] - lo[k]) / cell) + 1);
+        std::vector<int64_t> cnt(id(n[0] - 1, n[1] - 1, n[2] - 1) + 2, 0);
+        auto each = [&](long i, auto fn) {
+            const float* b = boxes + i * stride_lo;
+            int x0 = ci(b[0], 0), x1 = ci(b[stride_hi + 0], 0), y0 = ci(b[1], 1), y1 = ci(b[stride_hi + 1], 1);
+            int z0 = ci(b[2], 2), z1 = ci(b[stride_hi + 2], 2);
+            for (int x = x0; x <= x1; ++x)
+                for (int y = y0; y <= y1; ++y)
+                    for (int z = z0; z <= z1; ++z) fn(id(x, y, z));
+        };
+        for (long i = 0; i < count; ++i) each(i, [&](size_t c) { cnt[c + 1]++; });
+        for (size_t c = 1; c < cnt.size(); ++c) cnt[c] += cnt[c - 1];
+        start = cnt;
+        items.resize(start.back());
+        std::vector<int64_t> fill(start.begin(), start.end() - 1);
+        for (long i = 0; i < count; ++i) each(i, [&](size_t c) { items[fill[c]++] = (int32_t)i; });
+    }
+};
+
+float pick_cell(const float* box, long n) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    std::vector<float> ext;
+    ext.reserve(n);
+    for (long i = 0; i < n; ++i) {
+        float e = 0;
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], box[6 * i + k]);
+            hi[k] = std::max(hi[k], box[6 * i + 3 + k]);
+            e = std::max(e, box[6 * i + 3 + k] - box[6 * i + k]);
+        }
+        ext.push_back(e);
+    }
+    std::nth_element(ext.begin(), ext.begin() + ext.size() / 2, ext.end());
+    double vol = 1;
+    for (int k = 0; k < 3; ++k) vol *= std::max(1e-3f, hi[k] - lo[k]);
+    float dens = (float)std::cbrt(vol / std::max<long>(n, 1));
+    return std::max({ext[ext.size() / 2], dens, 1e-3f});
+}
+
+}  // namespace
+
+void generate_candidates(const CandidateQuery& q, std::vector<int64_t>& off, std::vector<int32_t>& ids) {
+    off.assign(q.n1 + 1, 0);
+    ids.clear();
+    if (q.n1 <= 0) return;
+    const float cell = pick_cell(q.box2, q.n2);
+    Grid boxes, points;
+    boxes.build(q.box2, q.n2, 6, 3, cell);
+    if (q.is_knn) points.build(q.xf2, q.n2, 3, 0, cell);
+
+    const int threads = q.threads > 0 ? q.threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    const long chunk = 256;
+    const long nchunks = (q.n1 + chunk - 1) / chunk;
+    std::vector<std::vector<int32_t>> part_ids(nchunks);
+    std::vector<std::vector<int64_t>> part_cnt(nchunks);
+    std::atomic<long> next{0};
+
+    auto worker = [&]() {
+        std::vector<int> stamp(q.n2, -1);
+        std::vector<std::pair<float, int32_t>> found;
+        for (long c; (c = next.fetch_add(1)) < nchunks;) {
+            auto& out = part_ids[c];
+            auto& cnts = part_cnt[c];
+            for (long i = c * chunk; i < std::min(q.n1, (c + 1) * chunk); ++i) {
+                const float* qb = q.box1 + 6 * i;
+                const float* qx = q.xf1 + 3 * i;
+                found.clear();
+                if (!q.is_knn) {
+                    const float r = q.within;
+                    int x0 = boxes.ci(qb[0] - r, 0), x1 = boxes.ci(qb[3] + r, 0);
+                    int y0 = boxes.ci(qb[1] - r, 1), y1 = boxes.ci(qb[4] + r, 1);
+                    int z0 = boxes.ci(qb[2] - r, 2), z1 = boxes.ci(qb[5] + r, 2);
+                    for (int x = x0; x <= x1; ++x)
+                        for (int y = y0; y <= y1; ++y)
+                            for (int z = z0; z <= z1; ++z) {
+                                size_t cc = boxes.id(x, y, z);
+                                for (int64_t k = boxes.start[cc]; k < boxes.start[cc + 1]; ++k) {
+                                    int32_t o = boxes.items[k];
+                                    if (stamp[o] == (int)i) continue;
+                                    stamp[o] = (int)i;
+                                    if (q.self_join && o == i) continue;
+                                    if (box_gap(q.box2 + 6 * o, qb) <= q.within) found.push_back({0.f, o});
+                                }
+                            }
+                    std::sort(found.begin(), found.end(), [](auto& a, auto& b) { return a.second < b.second; });
+                } else {
+                    // 1) the K smallest transform distances (ring search on the point grid)
+                    const int K = q.knn;
+                    std::priority_queue<std::pair<float, int32_t>> heap;  // max-heap of (dist, id)
+                    int cx = points.ci(qx[0], 0), cy = points.ci(qx[1], 1), cz = points.ci(qx[2], 2);
+                    int maxr = std::max({points.n[0], points.n[1], points.n[2]});
+                    for (int r = 0; r <= maxr; ++r) {
+                        for (int x = cx - r; x <= cx + r; ++x)
+                            for (int y = cy - r; y <= cy + r; ++y)
+                                for (int z = cz - r; z <= cz + r; ++z) {
+                                    if (std::max({std::abs(x - cx), std::abs(y - cy), std::abs(z - cz)}) != r) continue;
+                                    if (x < 0 || y < 0 || z < 0 || x >= points.n[0] || y >= points.n[1] || z >= points.n[2]) continue;
+                                    size_t cc = points.id(x, y, z);
+                                    for (int64_t k = points.start[cc]; k < points.start[cc + 1]; ++k) {
+                                        int32_t o = points.items[k];
+                                        if (q.self_join && o == i) continue;
+                                        std::pair<float, int32_t> e = {point_dist(qx, q.xf2 + 3 * o), o};
+                                        if ((int)heap.size() < K) heap.push(e);
+                                        else if (e < heap.top()) { heap.pop(); heap.push(e); }
+                                    }
+                                }
+                        if ((int)heap.size() == K && heap.top().first <= (float)r * points.cell) break;
+                    }
+                    const float maxk = (int)heap.size() == K ? heap.top().first : INFINITY;
+                    std::vector<int32_t> topk;
+                    while (!heap.empty()) { topk.push_back(heap.top().second); heap.pop(); }
+                    for (int32_t o : topk) stamp[o] = (int)i;
+                    for (int32_t o : topk) found.push_back({point_dist(qx, q.xf2 + 3 * o), o});
+                    // 2) every object whose box gap is below the K-th distance
+                    const float r = std::isfinite(maxk) ? maxk : 3e38f;
+                    int x0 = boxes.ci(qb[0] - r, 0), x1 = boxes.ci(qb[3] + r, 0);
+                    int y0 = boxes.ci(qb[1] - r, 1), y1 = boxes.ci(qb[4] + r, 1);
+                    int z0 = boxes.ci(qb[2] - r, 2), z1 = boxes.ci(qb[5] + r, 2);
+                    for (int x = x0; x <= x1; ++x)
+                        for (int y = y0; y <= y1; ++y)
+                            for (int z = z0; z <= z1; ++z) {
+                                size_t cc = boxes.id(x, y, z);
+                                for (int64_t k = boxes.start[cc]; k < boxes.start[cc + 1]; ++k) {
+                                    int32_t o = boxes.items[k];
+                                    if (stamp[o] == (int)i) continue;
+                                    stamp[o] = (int)i;
+                                    if (q.self_join && o == i) continue;
+                                    if (box_gap(q.box2 + 6 * o, qb) < maxk) found.push_back({point_dist(qx, q.xf2 + 3 * o), o});
+                                }
+                            }
+                    std::sort(found.begin(), found.end());
+                }
+                for (auto& f : found) out.push_back(f.second);
+                cnts.push_back((int64_t)found.size());
+            }
+        }
+    };
+    std::vector<std::thread> ts;
+    for (int t = 0; t < threads; ++t) ts.emplace_back(worker);
+    for (auto& t : ts) t.join();
+    long i = 0;
+    for (long c = 0; c < nchunks; ++c) {
+        for (int64_t n : part_cnt[c]) {
+            off[i + 1] = off[i] + n;
+            ++i;
+        }
+        ids.insert(ids.end(), part_ids[c].begin(), part_ids[c].end());
+    }
+}
+
+}  // namespace tdp

@@ -1,0 +1,283 @@
+// join_driver.cpp -- host orchestration of the spatial join (tdp_join).
+//
+// Follows the reference's chunked joins step for step, with all state in HBM:
+//   SpatialJoin::nearest_neighbor_chunking   src/join/KNNJoin.cpp:1524-1811
+//   SpatialJoin::within_chunking             src/join/WithinJoin.cpp:644-813
+//   mbb_knn_op_gpu_one_kernel / mbb_within_op_gpu_one_kernel (the filter)
+//                                            KNNJoin.cpp:497-851, WithinJoin.cpp:26-258
+// 1. object candidates (src/index, host), uploaded as a CSR of object pairs;
+// 2. filter: object ranges from all voxel pairs, kNN rank rule or within
+//    classification, compaction of the voxel pairs that can still matter;
+// 3. per LOD: refine every live, non-empty voxel pair, update voxel and
+//    object ranges (with eviction), decide; stop when nothing is undecided.
+// The host only reads a few counters per LOD; no triangle ever crosses PCIe.
+//
+// Forms: TDP_FORM_PLAIN uses the reference's FP32 decision rules and the
+// one-CTA-per-voxel-pair refine; TDP_FORM_TUNED uses the persistent culled
+// refine and decides only outside each range's FP32 error band.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../csrc/ctx.cuh"
+#include "../../csrc/join_kernels.cuh"
+#include "../../csrc/refine.cuh"
+#include "index/candidates.h"
+#include "storage/dev_tile.h"
+#include "tdp.h"
+
+struct tdp_result {
+    std::vector<int> q, t;
+    std::vector<float> d;
+};
+
+namespace tdp {
+
+namespace {
+
+enum Slot {
+    kPq = 20, kPt, kQoff, kPmn, kPmx, kPerr, kPstat, kPvp, kQconf, kCnt, kScanTmp, kRankSt,
+    kVpa, kVpb, kVpair, kVmn, kVmx, kVerr, kValive, kVupd, kItems, kItemVp, kRes, kOutQ, kOutT, kOutD,
+    kRecheck,
+};
+
+template <typename T>
+T* buf(tdp_ctx* ctx, int slot) { return (T*)ctx->scratch[slot].p; }
+
+}  // namespace
+}  // namespace tdp
+
+using namespace tdp;
+
+extern "C" {
+
+void tdp_join_default_params(tdp_join_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->query = TDP_QUERY_NN;
+    p->knn = 1;
+    p->within_dist = 1000.f;
+    p->n_lods = 0;
+    p->hausdorff_level = 2;
+    p->form = TDP_FORM_TUNED;
+}
+
+int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_join_params* prm, tdp_result** out) {
+    if (!ctx || !t1 || !prm || !out) return TDP_ERR_ARG;
+    *out = nullptr;
+    const bool self = (t2 == nullptr || t2 == t1);
+    if (!t2) t2 = t1;
+    const bool knn = prm->query == TDP_QUERY_NN;
+    if (!knn && prm->query != TDP_QUERY_WITHIN) return fail(ctx, TDP_ERR_ARG, "query must be nn or within");
+    if (knn && prm->knn < 1) return fail(ctx, TDP_ERR_ARG, "knn must be >= 1");
+    if (prm->hausdorff_level < 0 || prm->hausdorff_level > 2) return fail(ctx, TDP_ERR_ARG, "hausdorff_level must be 0, 1 or 2");
+    if (prm->form != TDP_FORM_PLAIN && prm->form != TDP_FORM_TUNED) return fail(ctx, TDP_ERR_ARG, "unknown form");
+    if (t1->device != ctx->device || t2->device != ctx->device) return fail(ctx, TDP_ERR_ARG, "tile lives on another device");
+    const bool tuned = prm->form == TDP_FORM_TUNED;
+    std::vector<int> lods;
+    if (prm->n_lods <= 0) lods.assign(kLods, kLods + kNumLods);
+    else {
+        if (prm->n_lods > 8) return fail(ctx, TDP_ERR_ARG, "at most 8 LODs");
+        lods.assign(prm->lods, prm->lods + prm->n_lods);
+    }
+    std::sort(lods.begin(), lods.end());
+    lods.erase(std::unique(lods.begin(), lods.end()), lods.end());
+    for (int l : lods)
+        if (lod_index(l) < 0) return fail(ctx, TDP_ERR_ARG, "LOD " + std::to_string(l) + " not in the tile (20,40,60,80,100)");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    LastStats st;
+
+    // ---- 1. object candidates (host) ----
+    CandidateQuery cq{t1->host.obj_box.data(), t1->host.obj_xf.data(), t1->n_obj, t2->host.obj_box.data(),
+                      t2->host.obj_xf.data(), t2->n_obj, self, knn, knn ? prm->knn : 0, prm->within_dist, 0};
+    std::vector<int64_t> qoff;
+    std::vector<int32_t> ids;
+    generate_candidates(cq, qoff, ids);
+    const long P = (long)ids.size();
+    if (P >= (1L << 31) - 1) return fail(ctx, TDP_ERR_ARG, "too many candidate pairs");
+    std::vector<int32_t> pq(P);
+    for (long i = 0; i < t1->n_obj; ++i)
+        for (int64_t k = qoff[i]; k < qoff[i + 1]; ++k) pq[k] = (int32_t)i;
+
+    int rc;
+#define ENS(slot, bytes) do { if ((rc = ensure(ctx, ctx->scratch[slot], (bytes)))) return rc; } while (0)
+#define CU(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } while (0)
+    const size_t Pz = (size_t)std::max<long>(P, 1);
+    ENS(kPq, Pz * 4); ENS(kPt, Pz * 4); ENS(kQoff, (t1->n_obj + 1) * 8);
+    ENS(kPmn, Pz * 4); ENS(kPmx, Pz * 4); ENS(kPerr, Pz * 4); ENS(kPstat, Pz);
+    ENS(kPvp, (Pz + 1) * 8); ENS(kQconf, (t1->n_obj + 1) * 4); ENS(kCnt, (Pz + 1) * 8); ENS(kRankSt, Pz * 4);
+    ENS(kOutQ, Pz * 4); ENS(kOutT, Pz * 4); ENS(kOutD, Pz * 4);
+
+    JoinDev d{};
+    d.vox1 = t1->vox; d.ovox1 = t1->obj_vox; d.vox2 = t2->vox; d.ovox2 = t2->obj_vox;
+    d.ohd1 = t1->obj_hd; d.ophd1 = t1->obj_phd; d.ohd2 = t2->obj_hd; d.ophd2 = t2->obj_phd;
+    d.P = (int)P;
+    d.pq = buf<int>(ctx, kPq); d.pt = buf<int>(ctx, kPt);
+    d.pmn = buf<float>(ctx, kPmn); d.pmx = buf<float>(ctx, kPmx); d.perr = buf<float>(ctx, kPerr);
+    d.pstat = buf<uint8_t>(ctx, kPstat); d.pvp = buf<int64_t>(ctx, kPvp);
+    d.N1 = (int)t1->n_obj; d.qoff = buf<int64_t>(ctx, kQoff); d.qconf = buf<int>(ctx, kQconf);
+
+    unsigned* cnt_items = ctx->d_counter + 8;    // [0] items, [2..3] tri-pair sum (u64)
+    unsigned* cnt_status = ctx->d_counter + 16;  // undecided, reported
+    unsigned* cnt_collect = ctx->d_counter + 20;
+
+    CU(cudaEventRecord(ctx->ev[0], s));
+    if (P > 0) {
+        CU(cudaMemcpyAsync((void*)d.pq, pq.data(), P * 4, cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync((void*)d.pt, ids.data(), P * 4, cudaMemcpyHostToDevice, s));
+    }
+    CU(cudaMemcpyAsync((void*)d.qoff, qoff.data(), qoff.size() * 8, cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(d.qconf, 0, t1->n_obj * 4, s));
+    long launches = 0;
+
+    // ---- 2. filter ----
+    CU(launch_pair_bounds(d, s)); ++launches;
+    if (knn) { CU(launch_knn_rank(d, prm->knn, tuned, buf<int>(ctx, kRankSt), s)); }
+    else { CU(launch_within_decide(d, prm->within_dist, tuned, s)); }
+    ++launches;
+    int64_t* cnt = buf<int64_t>(ctx, kCnt);
+    CU(cudaMemsetAsync(cnt + P, 0, 8, s));
+    CU(launch_count_vps(d, !knn, prm->within_dist, tuned, cnt, s)); ++launches;
+    size_t tmp_bytes = 0;
+    CU(scan_counts(cnt, d.pvp, (int)P, nullptr, tmp_bytes, s));
+    ENS(kScanTmp, tmp_bytes + 16);
+    CU(scan_counts(cnt, d.pvp, (int)P, ctx->scratch[kScanTmp].p, tmp_bytes, s)); ++launches;
+    int64_t V = 0;
+    CU(cudaMemcpyAsync(&V, d.pvp + P, 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    const size_t Vz = (size_t)std::max<int64_t>(V, 1);
+    ENS(kVpa, Vz * 4); ENS(kVpb, Vz * 4); ENS(kVpair, Vz * 4); ENS(kVmn, Vz * 4); ENS(kVmx, Vz * 4);
+    ENS(kVerr, Vz * 4); ENS(kValive, Vz); ENS(kVupd, Vz * 4);
+    ENS(kItems, Vz * sizeof(RefineItem)); ENS(kItemVp, Vz * 4); ENS(kRes, Vz * sizeof(float4));
+    d.V = V;
+    d.vpa = buf<int>(ctx, kVpa); d.vpb = buf<int>(ctx, kVpb); d.vpair = buf<int>(ctx, kVpair);
+    d.vmn = buf<float>(ctx, kVmn); d.vmx = buf<float>(ctx, kVmx); d.verr = buf<float>(ctx, kVerr);
+    d.valive = buf<uint8_t>(ctx, kValive); d.vupd = buf<int>(ctx, kVupd);
+    CU(launch_write_vps(d, !knn, prm->within_dist, tuned, s)); ++launches;
+    CU(cudaEventRecord(ctx->ev[1], s));
+    st.filter_pairs = P;
+    for (long i = 0; i < t1->n_obj; ++i)
+        for (int64_t k = qoff[i]; k < qoff[i + 1]; ++k)
+            st.filter_voxel_pairs += (double)(t1->host.obj_vox_off[i + 1] - t1->host.obj_vox_off[i]) *
+                                     (double)(t2->host.obj_vox_off[ids[k] + 1] - t2->host.obj_vox_off[ids[k]]);
+
+    // ---- 3. LOD loop ----
+    RefineItem* items = buf<RefineItem>(ctx, kItems);
+    int* item_vp = buf<int>(ctx, kItemVp);
+    float4* res = buf<float4>(ctx, kRes);
+    double refine_ms = 0;
+    unsigned long long full_total = 0;
+    double tri_total = 0;
+    long refine_items = 0;
+    for (size_t k = 0; k < lods.size() && V > 0; ++k) {
+        const int li = lod_index(lods[k]);
+        const bool highest = (k + 1 == lods.size());
+        CU(cudaMemsetAsync(ctx->d_counter + 8, 0, 32, s));
+        CU(launch_build_items(d, t1->vtri[li], t2->vtri[li], items, item_vp, cnt_items, s)); ++launches;
+        unsigned hc[4];
+        CU(cudaMemcpyAsync(hc, cnt_items, 16, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        const int W = (int)hc[0];
+        unsigned long long trip;
+        std::memcpy(&trip, &hc[2], 8);
+        tri_total += (double)trip;
+        refine_items += W;
+        if (W > 0) {
+            CU(cudaMemsetAsync(ctx->d_stats, 0, 8, s));
+            CU(cudaEventRecord(ctx->ev[2], s));
+            if (tuned)
+                CU(launch_refine_tuned(t1->tri[li], t2->tri[li], items, W, res, ctx->d_counter, ctx->d_stats,
+                                       ctx->num_sms, ctx->tuned_ctas_per_sm, s));
+            else
+                CU(launch_refine_plain(t1->tri[li], t2->tri[li], items, W, res, s));
+            CU(cudaEventRecord(ctx->ev[3], s));
+            ++launches;
+            st.refine_launches++;
+            CU(launch_apply_results(d, res, item_vp, W, highest, prm->hausdorff_level, li, (int)k, s)); ++launches;
+        }
+        CU(launch_pair_update(d, (int)k, s)); ++launches;
+        if (knn) CU(launch_knn_rank(d, prm->knn, tuned, buf<int>(ctx, kRankSt), s));
+        else CU(launch_within_decide(d, prm->within_dist, tuned, s));
+        ++launches;
+        CU(cudaMemsetAsync(cnt_status, 0, 8, s));
+        CU(launch_count_status(d, cnt_status, s)); ++launches;
+        unsigned sc[2];
+        unsigned long long fe = 0;
+        CU(cudaMemcpyAsync(sc, cnt_status, 8, cudaMemcpyDeviceToHost, s));
+        if (W > 0 && tuned) CU(cudaMemcpyAsync(&fe, ctx->d_stats, 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (W > 0) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+            refine_ms += ms;
+            full_total += tuned ? fe : trip;
+        }
+        if (sc[0] == 0) break;
+    }
+
+    // ---- 4. results ----
+    CU(cudaMemsetAsync(cnt_collect, 0, 4, s));
+    CU(launch_collect(d, buf<int>(ctx, kOutQ), buf<int>(ctx, kOutT), buf<float>(ctx, kOutD), cnt_collect, s)); ++launches;
+    CU(cudaEventRecord(ctx->ev[4], s));
+    unsigned nres = 0;
+    CU(cudaMemcpyAsync(&nres, cnt_collect, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    tdp_result* R = new tdp_result();
+    std::vector<int> q(nres), t(nres);
+    std::vector<float> dd(nres);
+    if (nres) {
+        cudaMemcpyAsync(q.data(), buf<int>(ctx, kOutQ), nres * 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(t.data(), buf<int>(ctx, kOutT), nres * 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(dd.data(), buf<float>(ctx, kOutD), nres * 4, cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { delete R; return fail(ctx, TDP_ERR_CUDA, cudaGetErrorString(e)); }
+    }
+    std::vector<unsigned> order(nres);
+    std::iota(order.begin(), order.end(), 0u);
+    std::sort(order.begin(), order.end(), [&](unsigned a, unsigned b) { return q[a] != q[b] ? q[a] < q[b] : t[a] < t[b]; });
+    R->q.resize(nres); R->t.resize(nres); R->d.resize(nres);
+    for (unsigned i = 0; i < nres; ++i) { R->q[i] = q[order[i]]; R->t[i] = t[order[i]]; R->d[i] = dd[order[i]]; }
+    float f_ms = 0, tot_ms = 0;
+    cudaEventElapsedTime(&f_ms, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&tot_ms, ctx->ev[0], ctx->ev[4]);
+    st.filter_ms = f_ms;
+    st.total_ms = tot_ms;
+    st.refine_ms = refine_ms;
+    st.tri_pairs = tri_total;
+    st.full_evals = full_total;
+    st.refine_items = refine_items;
+    st.kernel_launches = launches;
+    ctx->stats = st;
+    *out = R;
+#undef ENS
+#undef CU
+    return TDP_OK;
+}
+
+int tdp_result_count(const tdp_result* r, long* n) {
+    if (!r || !n) return TDP_ERR_ARG;
+    *n = (long)r->q.size();
+    return TDP_OK;
+}
+
+int tdp_result_copy(const tdp_result* r, int* qid, int* rid, float* dist) {
+    if (!r) return TDP_ERR_ARG;
+    const size_t n = r->q.size();
+    if (qid) std::memcpy(qid, r->q.data(), n * 4);
+    if (rid) std::memcpy(rid, r->t.data(), n * 4);
+    if (dist) std::memcpy(dist, r->d.data(), n * 4);
+    return TDP_OK;
+}
+
+int tdp_result_free(tdp_result* r) {
+    if (!r) return TDP_ERR_ARG;
+    delete r;
+    return TDP_OK;
+}
+
+}  // extern "C"

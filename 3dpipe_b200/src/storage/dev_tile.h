@@ -1,0 +1,32 @@
+// dev_tile.h -- a tile resident in HBM (behind the opaque tdp_tile of the C ABI).
+//
+// Layout in device memory:
+//   vox       3 float4 per voxel: (low xyz, 0) (high xyz, 0) (core xyz, 0)
+//   obj_vox   [n_obj+1] first voxel of each object
+//   obj_hd    [n_obj*5] object-level hausdorff per LOD, obj_phd proxy
+//   tri[l]    3 float4 per triangle of LOD l (see csrc/common.cuh RefineItem),
+//             grouped by voxel in voxel order
+//   vtri[l]   [n_vox+1] first triangle of each voxel at LOD l
+// The host keeps the parsed metadata (boxes, transforms, counts) for candidate
+// generation and for the join driver.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "storage/dt_format.h"
+
+struct tdp_tile {
+    tdp::TileHost host;
+    long n_obj = 0, n_vox = 0;
+    float4* vox = nullptr;
+    uint32_t* obj_vox = nullptr;
+    float* obj_hd = nullptr;
+    float* obj_phd = nullptr;
+    float4* tri[tdp::kNumLods] = {};
+    uint32_t* vtri[tdp::kNumLods] = {};
+    std::vector<uint32_t> h_vtri[tdp::kNumLods];  // host copy of vtri
+    size_t device_bytes = 0;
+    int device = 0;
+};

@@ -1,0 +1,62 @@
+// dt_format.h -- the reference's RAW tile format (`.dt`, Decoding_Type RAW = 1).
+//
+// Layout (written by Tile::dump_raw_stream, reference src/storage/tile_IO.cpp:79-172;
+// read by HiMesh_Wrapper(char*, id, RAW), src/spatial/himesh_wrapper.cpp:17-83, and
+// Tile::load, src/storage/tile_IO.cpp:13-49):
+//
+//   uint8   type                                   (1 = RAW)
+//   per object, in file order (object id = position):
+//     size_t  data_size
+//     data block: for lod in 20,40,60,80,100: for each voxel:
+//                 float tri[9*n]  then  float hd[2*n]   (hd = proxy, hausdorff)
+//     size_t  vnum
+//     for lod in 20..100:  float hausdorff, float proxyhausdorff     (object level)
+//     for each voxel: float low[3], high[3], core[3];
+//                     for lod in 20..100: size_t offset (bytes, into the data block), size_t count
+//     float   transform[3]
+//
+// The object's box is the union of its voxel boxes (himesh_wrapper.cpp:40, :80).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace tdp {
+
+constexpr int kNumLods = 5;
+constexpr int kLods[kNumLods] = {20, 40, 60, 80, 100};
+constexpr uint8_t kRawType = 1;
+
+inline int lod_index(int lod) {
+    for (int i = 0; i < kNumLods; ++i)
+        if (kLods[i] == lod) return i;
+    return -1;
+}
+
+// Host-side view of a parsed RAW tile.  Offsets point into the caller's byte buffer.
+struct TileHost {
+    long n_obj = 0;
+    long n_vox = 0;
+    std::vector<uint64_t> obj_data_off;     // byte offset of each object's data block
+    std::vector<uint64_t> obj_data_size;
+    std::vector<uint32_t> obj_vox_off;      // [n_obj+1]
+    std::vector<float> obj_box;             // 6 per object: low xyz, high xyz
+    std::vector<float> obj_xf;              // 3 per object
+    std::vector<float> obj_hd;              // kNumLods per object (hausdorff)
+    std::vector<float> obj_phd;             // kNumLods per object (proxy hausdorff)
+    std::vector<float> vox_box;             // 9 per voxel: low xyz, high xyz, core xyz
+    std::vector<uint64_t> vox_byte_off[kNumLods];  // absolute byte offset of the voxel's triangles
+    std::vector<uint32_t> vox_cnt[kNumLods];
+    uint64_t n_tris[kNumLods] = {0, 0, 0, 0, 0};
+};
+
+// Parse `len` bytes; at most max_objects objects (<= 0: all).  Returns 0 or a
+// TDP_ERR_* code with a message in `err`.
+int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& out, std::string& err);
+
+// Size in bytes of one object's record given its voxel count and per-(lod,voxel)
+// triangle counts (counts[l * nvox + v]).
+size_t raw_object_bytes(uint32_t nvox, const uint32_t* counts);
+
+}  // namespace tdp

@@ -26,7 +26,7 @@ QUERY_NN, QUERY_WITHIN = 1, 2
 # Every symbol include/tdp.h declares; tests check the library exports them all.
 EXPORTED = [
     "tdp_ctx_create", "tdp_ctx_destroy", "tdp_last_error", "tdp_ctx_memory", "tdp_last_stats",
-    "tdp_refine_batch",
+    "tdp_refine_batch", "tdp_gen_default_params", "tdp_gen_tiles",
 ]
 
 
@@ -66,12 +66,47 @@ def lib() -> C.CDLL:
     L.tdp_ctx_memory.argtypes = [P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
     L.tdp_last_stats.argtypes = [P, C.POINTER(Stats)]
     L.tdp_refine_batch.argtypes = [P, P, P, C.c_size_t, P, C.c_uint32, C.c_int, P]
+    L.tdp_gen_default_params.argtypes = [P]
+    L.tdp_gen_default_params.restype = None
+    L.tdp_gen_tiles.argtypes = [P, P, C.c_size_t, P, P, C.c_size_t, P, C.c_char_p, C.c_size_t]
+    _bind_join(L)
     _lib = L
     return L
 
 
 def _ptr(a: np.ndarray | None):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class GenParams(C.Structure):
+    _fields_ = [("n_vessels", C.c_int), ("nuclei_per_vessel", C.c_int), ("seed", C.c_uint64),
+                ("voxel_size", C.c_int), ("nucleus_subdiv", C.c_int), ("tube_sides", C.c_int),
+                ("tube_rings", C.c_int), ("threads", C.c_int), ("grid", C.c_float),
+                ("shell_min", C.c_float), ("shell_max", C.c_float)]
+
+
+def gen_tiles(n_vessels: int = 10, nuclei_per_vessel: int = 20, seed: int = 20260001, out=None, **kw):
+    """Generate (nuclei_tile_bytes, vessel_tile_bytes) as uint8 arrays in RAW .dt format.
+
+    `out`, if given, is a callable (nbytes) -> writable uint8 array (for example a
+    pinned buffer); otherwise numpy arrays are allocated."""
+    L = lib()
+    p = GenParams()
+    L.tdp_gen_default_params(C.byref(p))
+    p.n_vessels, p.nuclei_per_vessel, p.seed = n_vessels, nuclei_per_vessel, seed
+    for k, v in kw.items():
+        setattr(p, k, v)
+    nl, vl = C.c_size_t(), C.c_size_t()
+    err = C.create_string_buffer(512)
+    rc = L.tdp_gen_tiles(C.byref(p), None, 0, C.byref(nl), None, 0, C.byref(vl), err, 512)
+    if rc != TDP_OK:
+        raise TdpError(rc, err.value.decode())
+    alloc = out or (lambda n: np.empty(n, np.uint8))
+    nb, vb = alloc(nl.value), alloc(vl.value)
+    rc = L.tdp_gen_tiles(C.byref(p), _ptr(nb), nb.size, C.byref(nl), _ptr(vb), vb.size, C.byref(vl), err, 512)
+    if rc != TDP_OK:
+        raise TdpError(rc, err.value.decode())
+    return nb[:nl.value], vb[:vl.value]
 
 
 class Context:
@@ -134,3 +169,112 @@ class Context:
         self.check(lib().tdp_refine_batch(self._h, _ptr(data), _ptr(hd), data.shape[0], _ptr(osz),
                                           osz.shape[0], form, _ptr(out)))
         return out
+
+
+class TileInfo(C.Structure):
+    _fields_ = [("n_objects", C.c_long), ("n_voxels", C.c_long), ("n_tris", C.c_long * 5),
+                ("device_bytes", C.c_size_t)]
+
+
+class JoinParams(C.Structure):
+    _fields_ = [("query", C.c_int), ("knn", C.c_int), ("within_dist", C.c_float), ("lods", C.c_int * 8),
+                ("n_lods", C.c_int), ("hausdorff_level", C.c_int), ("form", C.c_int)]
+
+
+def _bind_join(L):
+    P = C.c_void_p
+    L.tdp_tile_upload.argtypes = [P, P, C.c_size_t, C.c_long, C.POINTER(P)]
+    L.tdp_tile_free.argtypes = [P, P]
+    L.tdp_tile_get_info.argtypes = [P, C.POINTER(TileInfo)]
+    L.tdp_candidates.argtypes = [P, P, C.c_long, P, P, C.c_long, C.c_int, C.c_int, C.c_int, C.c_float, P, P, C.c_long]
+    L.tdp_candidates.restype = C.c_long
+    L.tdp_join_default_params.argtypes = [C.POINTER(JoinParams)]
+    L.tdp_join_default_params.restype = None
+    L.tdp_join.argtypes = [P, P, P, C.POINTER(JoinParams), C.POINTER(P)]
+    L.tdp_result_count.argtypes = [P, C.POINTER(C.c_long)]
+    L.tdp_result_copy.argtypes = [P, P, P, P]
+    L.tdp_result_free.argtypes = [P]
+
+
+EXPORTED += ["tdp_tile_upload", "tdp_tile_free", "tdp_tile_get_info", "tdp_candidates",
+             "tdp_join_default_params", "tdp_join", "tdp_result_count", "tdp_result_copy", "tdp_result_free"]
+
+
+class Tile:
+    """A RAW .dt tile resident in HBM (Tile::load + decode to every LOD)."""
+
+    def __init__(self, ctx: "Context", raw: np.ndarray, max_objects: int = 0):
+        raw = np.ascontiguousarray(raw, np.uint8)
+        h = C.c_void_p()
+        ctx.check(lib().tdp_tile_upload(ctx.handle, _ptr(raw), raw.size, max_objects, C.byref(h)))
+        self._ctx, self._h = ctx, h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> dict:
+        i = TileInfo()
+        lib().tdp_tile_get_info(self._h, C.byref(i))
+        return {"n_objects": i.n_objects, "n_voxels": i.n_voxels, "n_tris": list(i.n_tris),
+                "device_bytes": i.device_bytes}
+
+    def free(self):
+        if getattr(self, "_h", None):
+            lib().tdp_tile_free(self._ctx.handle, self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def candidates(box1, xf1, box2, xf2, self_join=False, knn=0, within=0.0):
+    """Object candidates (CSR offsets, ids); knn > 0 selects the kNN query."""
+    L = lib()
+    box1 = np.ascontiguousarray(box1, np.float32).reshape(-1, 6)
+    box2 = np.ascontiguousarray(box2, np.float32).reshape(-1, 6)
+    xf1 = np.ascontiguousarray(xf1, np.float32).reshape(-1, 3)
+    xf2 = np.ascontiguousarray(xf2, np.float32).reshape(-1, 3)
+    off = np.zeros(len(box1) + 1, np.int64)
+    n = L.tdp_candidates(_ptr(box1), _ptr(xf1), len(box1), _ptr(box2), _ptr(xf2), len(box2), int(self_join),
+                         int(knn > 0), max(knn, 1), float(within), _ptr(off), None, 0)
+    ids = np.zeros(max(-n, 1), np.int32)
+    n = L.tdp_candidates(_ptr(box1), _ptr(xf1), len(box1), _ptr(box2), _ptr(xf2), len(box2), int(self_join),
+                         int(knn > 0), max(knn, 1), float(within), _ptr(off), _ptr(ids), ids.size)
+    if n < 0:
+        raise TdpError(1, "tdp_candidates failed")
+    return off, ids[:n]
+
+
+def _join(self, tile1: Tile, tile2: Tile | None, query: str = "nn", knn: int = 1, within: float = 1000.0,
+          lods=None, hausdorff_level: int = 2, form: int = FORM_TUNED):
+    """tdbase join on resident tiles; returns (query_ids, result_ids, dist) sorted by (query, result)."""
+    L = lib()
+    p = JoinParams()
+    L.tdp_join_default_params(C.byref(p))
+    p.query = QUERY_NN if query == "nn" else QUERY_WITHIN
+    if query not in ("nn", "within"):
+        raise ValueError("query must be nn or within")
+    p.knn, p.within_dist, p.hausdorff_level, p.form = knn, within, hausdorff_level, form
+    if lods:
+        p.n_lods = len(lods)
+        for i, l in enumerate(lods):
+            p.lods[i] = l
+    r = C.c_void_p()
+    self.check(L.tdp_join(self._h, tile1.handle, None if tile2 is None else tile2.handle, C.byref(p), C.byref(r)))
+    try:
+        n = C.c_long()
+        L.tdp_result_count(r, C.byref(n))
+        q = np.empty(n.value, np.int32)
+        t = np.empty(n.value, np.int32)
+        d = np.empty(n.value, np.float32)
+        L.tdp_result_copy(r, _ptr(q), _ptr(t), _ptr(d))
+    finally:
+        L.tdp_result_free(r)
+    return q, t, d
+
+
+Context.join = _join

@@ -71,6 +71,62 @@ typedef struct {
 } tdp_stats;
 int tdp_last_stats(const tdp_ctx *ctx, tdp_stats *out);
 
+/* ---- tiles ------------------------------------------------------------------
+ * Upload a RAW .dt tile (the bytes of the file, host memory, pinned or not)
+ * into HBM: voxel records and every LOD's triangles become resident.
+ * max_objects <= 0 loads all objects (reference --max_objects1/2).
+ * Errors: TDP_ERR_FORMAT for malformed bytes, TDP_ERR_NOMEM over budget. */
+typedef struct {
+    long n_objects;
+    long n_voxels;
+    long n_tris[5];        /* per LOD 20,40,60,80,100 */
+    size_t device_bytes;
+} tdp_tile_info;
+int tdp_tile_upload(tdp_ctx *ctx, const void *raw_dt, size_t len, long max_objects, tdp_tile **out);
+int tdp_tile_free(tdp_ctx *ctx, tdp_tile *tile);
+int tdp_tile_get_info(const tdp_tile *tile, tdp_tile_info *out);
+
+/* ---- object candidates (host only) ------------------------------------------
+ * The object-level filter: replaces OctreeNode::query_knn_fast / query_within
+ * over Tile::build_octree (reference src/index/octree.cpp:215-330,
+ * src/storage/tile.cpp:76-85).  Boxes are 6 floats (low xyz, high xyz),
+ * transforms 3 floats.  kNN (is_knn != 0): the knn objects with the smallest
+ * transform distance plus every object whose box gap is below the knn-th of
+ * those distances, ordered by (transform distance, id).  within: every object
+ * with box gap <= within, ordered by id.  self_join excludes the query object.
+ * off: [n1+1] CSR offsets.  Returns the number of candidates, or -(needed) when
+ * cap is too small (off is then valid, ids is not), LONG_MIN on bad arguments. */
+long tdp_candidates(const float *box1, const float *xf1, long n1, const float *box2, const float *xf2, long n2,
+                    int self_join, int is_knn, int knn, float within, int64_t *off, int32_t *ids, long cap);
+
+/* ---- join ---------------------------------------------------------------------
+ * `tdbase join` (reference src/tools/tdbase.cpp:482-549) on device-resident tiles:
+ * object candidates (grid restatement of the octree queries), voxel-pair filter,
+ * then the LOD loop of refine + bound update + decision.  tile2 == NULL or
+ * tile2 == tile1 is a self-join (query object excluded from its own candidates;
+ * within results then hold both (a,b) and (b,a), as in the reference).
+ * Results are (query id, result id) pairs sorted by query then result id. */
+enum { TDP_QUERY_NN = 1, TDP_QUERY_WITHIN = 2 };
+typedef struct {
+    int query;             /* TDP_QUERY_NN (-q nn) or TDP_QUERY_WITHIN (-q within)   */
+    int knn;               /* --knn K                      (default 1)             */
+    float within_dist;     /* --within_dist tau            (default 1000)          */
+    int lods[8];           /* -l/--lods, ascending; n_lods = 0 -> 20,40,60,80,100  */
+    int n_lods;
+    int hausdorff_level;   /* --hausdorff_level 0|1|2      (default 2)             */
+    int form;              /* TDP_FORM_PLAIN (reference decision rules in FP32) or
+                              TDP_FORM_TUNED (persistent refine, FP32 with error
+                              bands and an FP64 recheck of undecided pairs)        */
+} tdp_join_params;
+void tdp_join_default_params(tdp_join_params *p);
+int tdp_join(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, const tdp_join_params *p,
+             tdp_result **out);
+int tdp_result_count(const tdp_result *r, long *n);
+/* any output pointer may be NULL; dist = the pair's upper distance bound when
+ * it was decided (the exact FP32 distance for pairs decided at the last LOD) */
+int tdp_result_copy(const tdp_result *r, int *query_ids, int *result_ids, float *dist);
+int tdp_result_free(tdp_result *r);
+
 /* ---- refine seam ------------------------------------------------------------
  * Drop-in for the reference's batched refine (MeshDist_batch_gpu_op_shm_flat_stream):
  *   data        9 floats per triangle (3 vertices), element_num triangles   (host)
@@ -85,6 +141,28 @@ int tdp_last_stats(const tdp_ctx *ctx, tdp_stats *out);
 enum { TDP_FORM_PLAIN = 0, TDP_FORM_TUNED = 1 };
 int tdp_refine_batch(tdp_ctx *ctx, const float *data, const float *hausdorff, size_t element_num,
                      const size_t *offset_size, uint32_t pair_num, int form, float *out);
+
+/* ---- synthetic tiles (host only, no context) --------------------------------
+ * Seeded generator of nuclei/vessel tiles in the reference's RAW .dt format.
+ * Replaces the CGAL simulator + `tdbase convert` (reference
+ * src/tools/simulator.cpp:332-458, src/storage/tile_IO.cpp:79-172), which cannot
+ * be built without CGAL.  Call once with null buffers to learn the sizes, then
+ * with buffers of at least those sizes.  err (optional) receives a message. */
+typedef struct {
+    int n_vessels;          /* vessels, one per cell of a `grid`-unit grid      */
+    int nuclei_per_vessel;  /* nuclei in a shell around each vessel             */
+    uint64_t seed;
+    int voxel_size;         /* target triangles per voxel (100)                 */
+    int nucleus_subdiv;     /* icosphere subdivision (3 -> 1280 triangles)      */
+    int tube_sides;         /* vessel tube resolution (20 x 72 -> ~20k tris)    */
+    int tube_rings;
+    int threads;            /* 0 = all hardware threads                         */
+    float grid;             /* 1000                                             */
+    float shell_min, shell_max; /* 30, 300                                      */
+} tdp_gen_params;
+void tdp_gen_default_params(tdp_gen_params *p);
+int tdp_gen_tiles(const tdp_gen_params *p, uint8_t *nuclei, size_t nuclei_cap, size_t *nuclei_len,
+                  uint8_t *vessels, size_t vessels_cap, size_t *vessels_len, char *err, size_t err_cap);
 
 #ifdef __cplusplus
 }

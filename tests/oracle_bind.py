@@ -99,3 +99,46 @@ def oracle():
 
 def reference():
     return Reference() if REF_SO.exists() else None
+
+
+def join_exact(tile1, tile2, self_join, is_knn, knn=1, tau=0.0, threads=0):
+    """FP64 exact join: every evaluated (q, t, D, in_result) as numpy arrays."""
+    O = oracle()
+    L = O.L
+    L.tdo_join_exact.argtypes = [P, C.c_size_t, P, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int,
+                                 P, P, P, P, C.c_long]
+    L.tdo_join_exact.restype = C.c_long
+    t1 = np.ascontiguousarray(tile1, np.uint8)
+    t2 = t1 if tile2 is None else np.ascontiguousarray(tile2, np.uint8)
+    cap = 1 << 16
+    while True:
+        q = np.empty(cap, np.int32); t = np.empty(cap, np.int32); d = np.empty(cap); i = np.empty(cap, np.int32)
+        n = L.tdo_join_exact(_p(t1), t1.size, _p(t2), t2.size, int(self_join), int(is_knn), int(knn), float(tau),
+                             int(threads), _p(q), _p(t), _p(d), _p(i), cap)
+        if n >= 0:
+            return q[:n], t[:n], d[:n], i[:n].astype(bool)
+        cap = -n
+
+
+def ref_join(tile1, tile2, self_join, is_knn, knn=1, tau=0.0, lods=None, level=2, threads=0, max_queries=0):
+    """The reference's join rules on the CPU with the reference's own MeshDist/octree.
+    Returns (q, t, stats) with stats = (seconds, tri_pairs, voxel_pairs_refined, candidates)."""
+    R = reference()
+    if R is None:
+        return None
+    L = R.L
+    L.tdr_join.argtypes = [P, C.c_size_t, P, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_float, P, C.c_int, C.c_int,
+                           C.c_int, C.c_long, P, P, C.c_long, P]
+    L.tdr_join.restype = C.c_long
+    t1 = np.ascontiguousarray(tile1, np.uint8)
+    t2 = t1 if tile2 is None else np.ascontiguousarray(tile2, np.uint8)
+    lods = np.array(lods or [20, 40, 60, 80, 100], np.int32)
+    cap = 1 << 16
+    while True:
+        q = np.empty(cap, np.int32); t = np.empty(cap, np.int32); st = np.zeros(4)
+        n = L.tdr_join(_p(t1), t1.size, _p(t2), t2.size, int(self_join), int(is_knn), int(knn), float(tau), _p(lods),
+                       len(lods), int(level), int(threads), int(max_queries), _p(q), _p(t), cap, _p(st))
+        if n >= 0:
+            o = np.lexsort((t[:n], q[:n]))
+            return q[:n][o], t[:n][o], st
+        cap = -n

@@ -1,0 +1,106 @@
+"""End-to-end join parity on the GPU, through the C ABI.
+
+For every seeded case, both forms (plain, tuned) must return exactly the result
+set of (a) the reference's own join rules run on the CPU with the reference's
+compiled FP32 MeshDist and octree (oracle/_ref) and (b) the FP64 exact oracle
+(asserted only when the exact distances keep every decision at least 1e-3
+away from a tie, which the generator's seeds guarantee for these cases).
+Result sets are compared as sorted (query id, result id) pairs, the way the
+reference's tools/evaluate.cpp compares result files.
+"""
+import numpy as np
+import pytest
+
+from join_cases import CASES, exact_truth, tiles
+from oracle_bind import ref_join
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu_tiles(pkg, ctx):
+    cache = {}
+
+    def get(nv, npv, seed):
+        key = (nv, npv, seed)
+        if key not in cache:
+            nb, vb = tiles(nv, npv, seed)
+            cache[key] = (pkg.tdp.Tile(ctx, nb), pkg.tdp.Tile(ctx, vb))
+        return cache[key]
+    return get
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_join_matches_reference_and_oracle(pkg, ctx, gpu_tiles, name):
+    nv, npv, seed, query, knn, tau, self_join, lods, level = CASES[name]
+    nb, vb = tiles(nv, npv, seed)
+    T1, T2 = gpu_tiles(nv, npv, seed)
+    ref = ref_join(nb, None if self_join else vb, self_join, query == "nn", knn=knn, tau=tau, lods=lods, level=level)
+    got = {}
+    for form in (pkg.FORM_PLAIN, pkg.FORM_TUNED):
+        q, t, d = ctx.join(T1, None if self_join else T2, query=query, knn=knn, within=tau, lods=lods,
+                           hausdorff_level=level, form=form)
+        assert np.all(np.diff(q) >= 0)
+        got[form] = set(zip(q.tolist(), t.tolist()))
+        st = ctx.stats()
+        assert st["total_ms"] > 0
+    assert got[pkg.FORM_PLAIN] == got[pkg.FORM_TUNED], name
+    if ref is not None:
+        rq, rt, _ = ref
+        assert got[pkg.FORM_PLAIN] == set(zip(rq.tolist(), rt.tolist())), name
+    if lods is None or lods[-1] == 100:
+        truth, margin = exact_truth(nb, vb, self_join, query, knn, tau)
+        if margin > 1e-3 and level != 1:
+            assert got[pkg.FORM_TUNED] == truth, name
+            if query == "nn":
+                n_q = len(set(q for q, _ in truth))
+                assert len(truth) == knn * n_q
+
+
+def test_knn_reports_exactly_k(pkg, ctx, gpu_tiles):
+    nv, npv, seed = 6, 12, 101
+    T1, T2 = gpu_tiles(nv, npv, seed)
+    for K in (1, 2, 4):
+        q, t, _ = ctx.join(T1, T2, query="nn", knn=K)
+        counts = np.bincount(q, minlength=nv * npv)
+        assert (counts == min(K, nv)).all()
+
+
+def test_within_self_join_is_symmetric(pkg, ctx, gpu_tiles):
+    T1, _ = gpu_tiles(4, 16, 106)
+    q, t, _ = ctx.join(T1, None, query="within", within=60.0)
+    pairs = set(zip(q.tolist(), t.tolist()))
+    assert pairs == {(b, a) for a, b in pairs}
+    assert all(a != b for a, b in pairs)
+
+
+def test_join_stats_and_repeatability(pkg, ctx, gpu_tiles):
+    T1, T2 = gpu_tiles(8, 10, 104)
+    a = ctx.join(T1, T2, query="within", within=400.0)
+    s1 = ctx.stats()
+    b = ctx.join(T1, T2, query="within", within=400.0)
+    s2 = ctx.stats()
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    assert s1["tri_pairs"] == s2["tri_pairs"]
+    assert s1["filter_pairs"] > 0
+
+
+def test_bad_arguments_are_errors(pkg, ctx, gpu_tiles):
+    T1, T2 = gpu_tiles(6, 12, 101)
+    with pytest.raises(pkg.TdpError):
+        ctx.join(T1, T2, query="nn", knn=0)
+    with pytest.raises(pkg.TdpError):
+        ctx.join(T1, T2, query="nn", knn=2, lods=[30])
+    with pytest.raises(pkg.TdpError):
+        pkg.tdp.Tile(ctx, np.zeros(10, np.uint8))
+    with pytest.raises(pkg.TdpError):
+        pkg.tdp.Tile(ctx, np.frombuffer(bytes([1]) + bytes(7), np.uint8))
+
+
+def test_tile_info(pkg, ctx, gpu_tiles):
+    T1, T2 = gpu_tiles(6, 12, 101)
+    i = T1.info()
+    assert i["n_objects"] == 72 and i["n_tris"][4] == 72 * 1280
+    assert i["n_tris"][0] == 72 * 256
+    assert T2.info()["n_objects"] == 6
