@@ -1,5 +1,6 @@
 // capi.cu -- context management and the refine seam of the C ABI (include/tdp.h).
 #include <float.h>
+#include <algorithm>
 #include <string.h>
 #include <vector>
 #include "ctx.cuh"
@@ -51,6 +52,21 @@ int ensure(tdp_ctx* ctx, Buf& b, size_t bytes) {
     }
     b.cap = want;
     return TDP_OK;
+}
+
+// FP32 FMA throughput probe: 8 independent FMA chains per thread.
+__global__ void fma_probe_kernel(float* out, int iters, float b, float c) {
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = threadIdx.x * 1e-3f + k;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fmaf(a[k], b, c);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k];
+    if (s == 1.2345f) out[blockIdx.x] = s;  // keeps the chains live
 }
 
 }  // namespace tdp
@@ -114,6 +130,27 @@ int tdp_last_stats(const tdp_ctx* ctx, tdp_stats* o) {
     o->filter_pairs = s.filter_pairs;
     o->filter_voxel_pairs = s.filter_voxel_pairs;
     o->kernel_launches = s.kernel_launches;
+    return TDP_OK;
+}
+
+int tdp_fp32_peak(tdp_ctx* ctx, double* tflops) {
+    if (!ctx || !tflops) return TDP_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    const int blocks = ctx->num_sms * 8, threads = 256, iters = 1 << 15;
+    float* out = (float*)ctx->d_stats;
+    double best = 0;
+    for (int rep = 0; rep < 6; ++rep) {
+        TDP_CUDA_TRY(cudaEventRecord(ctx->ev[6], ctx->stream));
+        fma_probe_kernel<<<blocks, threads, 0, ctx->stream>>>(out, iters, 0.999f, 1e-3f);
+        TDP_CUDA_TRY(cudaGetLastError());
+        TDP_CUDA_TRY(cudaEventRecord(ctx->ev[7], ctx->stream));
+        TDP_CUDA_TRY(cudaEventSynchronize(ctx->ev[7]));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[6], ctx->ev[7]);
+        const double fl = 2.0 * 8.0 * iters * (double)blocks * threads;
+        if (rep > 0 && ms > 0) best = std::max(best, fl / (ms * 1e-3) / 1e12);
+    }
+    *tflops = best;
     return TDP_OK;
 }
 

@@ -231,7 +231,69 @@ __global__ void k_apply_results(JoinDev d, const float4* __restrict__ res, const
     }
 }
 
-__global__ void __launch_bounds__(kBlock) k_pair_update(JoinDev d, int stamp) {
+// ---- FP64 recheck (tuned form) of pairs still undecided after the last LOD ----
+__global__ void k_recheck_items(JoinDev d, const uint32_t* __restrict__ vt1, const uint32_t* __restrict__ vt2,
+                                RefineItem* __restrict__ items, int* __restrict__ item_vp, double* __restrict__ vexact,
+                                unsigned* __restrict__ counter) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < d.V; v += (int64_t)gridDim.x * blockDim.x) {
+        if (!d.valive[v] || d.pstat[d.vpair[v]] != kUndecided) continue;
+        vexact[v] = 1e300;
+        const int a = d.vpa[v], b = d.vpb[v];
+        const uint32_t o1 = vt1[a], n1 = vt1[a + 1] - o1, o2 = vt2[b], n2 = vt2[b + 1] - o2;
+        if (!n1 || !n2) continue;
+        const unsigned w = atomicAdd(counter, 1u);
+        items[w] = RefineItem{o1, n1, o2, n2};
+        item_vp[w] = (int)v;
+    }
+}
+
+__global__ void k_recheck_apply(const double* __restrict__ res, const int* __restrict__ item_vp, int W,
+                                double* __restrict__ vexact) {
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) vexact[item_vp[w]] = res[w];
+}
+
+__global__ void __launch_bounds__(kBlock) k_recheck_pairs(JoinDev d, const double* __restrict__ vexact,
+                                                          double* __restrict__ pexact, int within, float tau) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
+        if (d.pstat[p] != kUndecided) continue;
+        double D = 1e300;
+        for (int64_t v = d.pvp[p] + lane; v < d.pvp[p + 1]; v += 32)
+            if (d.valive[v]) D = vexact[v] < D ? vexact[v] : D;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double x = __shfl_xor_sync(0xffffffffu, D, o);
+            D = x < D ? x : D;
+        }
+        if (lane == 0) {
+            pexact[p] = D;
+            d.pmn[p] = d.pmx[p] = (float)D;
+            if (within) d.pstat[p] = D <= (double)tau ? kReported : kDropped;
+        }
+    }
+}
+
+// kNN: the still-undecided candidates of a query compete for its open slots by exact distance
+__global__ void k_recheck_knn(JoinDev d, int K, const double* __restrict__ pexact) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < d.N1; q += gridDim.x * blockDim.x) {
+        const int64_t b = d.qoff[q], e = d.qoff[q + 1];
+        int conf = d.qconf[q];
+        while (conf < K) {
+            int64_t best = -1;
+            for (int64_t i = b; i < e; ++i)
+                if (d.pstat[i] == kUndecided && (best < 0 || pexact[i] < pexact[best])) best = i;
+            if (best < 0) break;
+            d.pstat[best] = kReported;
+            ++conf;
+        }
+        for (int64_t i = b; i < e; ++i)
+            if (d.pstat[i] == kUndecided) d.pstat[i] = kDropped;
+        d.qconf[q] = conf;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_pair_update(JoinDev d, int stamp, int tuned) {
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
@@ -248,8 +310,11 @@ __global__ void __launch_bounds__(kBlock) k_pair_update(JoinDev d, int stamp) {
         mindist = wmin(mindist);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) err = fmaxf(err, __shfl_xor_sync(0xffffffffu, err, o));
+        // evict voxel pairs that cannot hold the minimum; the tuned form keeps any
+        // whose FP32 bounds overlap within the error band
+        const float slack = tuned ? 2.f * err : 0.f;
         for (int64_t v = b + lane; v < e; v += 32)
-            if (d.valive[v] && d.vmn[v] > minmax) d.valive[v] = 0;
+            if (d.valive[v] && d.vmn[v] - slack > minmax) d.valive[v] = 0;
         if (lane == 0) {
             d.pmn[p] = mindist;
             d.pmx[p] = minmax;
@@ -332,9 +397,22 @@ cudaError_t launch_apply_results(const JoinDev& d, const float4* res, const int*
     k_apply_results<<<grid_for(W, 256), 256, 0, s>>>(d, res, item_vp, W, highest, level, li, stamp);
     return cudaGetLastError();
 }
-cudaError_t launch_pair_update(const JoinDev& d, int stamp, cudaStream_t s) {
+cudaError_t launch_pair_update(const JoinDev& d, int stamp, int tuned, cudaStream_t s) {
     if (d.P <= 0) return cudaSuccess;
-    k_pair_update<<<grid_for(d.P, kBlock / 32), kBlock, 0, s>>>(d, stamp);
+    k_pair_update<<<grid_for(d.P, kBlock / 32), kBlock, 0, s>>>(d, stamp, tuned);
+    return cudaGetLastError();
+}
+cudaError_t launch_recheck_items(const JoinDev& d, const uint32_t* vt1, const uint32_t* vt2, RefineItem* items,
+                                 int* item_vp, double* vexact, unsigned* counter, cudaStream_t s) {
+    if (d.V <= 0) return cudaSuccess;
+    k_recheck_items<<<grid_for(d.V, 256), 256, 0, s>>>(d, vt1, vt2, items, item_vp, vexact, counter);
+    return cudaGetLastError();
+}
+cudaError_t launch_recheck_finish(const JoinDev& d, const double* res, const int* item_vp, int W, double* vexact,
+                                  double* pexact, int knn, int K, float tau, cudaStream_t s) {
+    if (W > 0) k_recheck_apply<<<grid_for(W, 256), 256, 0, s>>>(res, item_vp, W, vexact);
+    if (d.P > 0) k_recheck_pairs<<<grid_for(d.P, kBlock / 32), kBlock, 0, s>>>(d, vexact, pexact, !knn, tau);
+    if (knn && d.N1 > 0) k_recheck_knn<<<grid_for(d.N1, 128), 128, 0, s>>>(d, K, pexact);
     return cudaGetLastError();
 }
 cudaError_t launch_count_status(const JoinDev& d, unsigned* c, cudaStream_t s) {

@@ -281,6 +281,60 @@ cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const Re
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ FP64 recheck
+// Exact (FP64) minimum triangle distance of a few voxel pairs: the tuned form's
+// recheck of object pairs whose FP32 decision fell inside the error band.
+constexpr int kF64Block = 128;
+
+__global__ void __launch_bounds__(kF64Block) refine_f64_kernel(const float4* __restrict__ triA,
+                                                               const float4* __restrict__ triB,
+                                                               const RefineItem* __restrict__ items, int n_items,
+                                                               double* __restrict__ out) {
+    __shared__ double red[kF64Block / 32];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const RefineItem w = items[it];
+        double best = 1e300;
+        if (w.a_cnt && w.b_cnt) {
+            const float4 o4 = triA[(size_t)w.a_off * kTriF4];
+            const double ox = o4.x, oy = o4.y, oz = o4.z;
+            const uint64_t total = (uint64_t)w.a_cnt * w.b_cnt;
+            for (uint64_t p = tid; p < total; p += kF64Block) {
+                const uint32_t i = (uint32_t)(p / w.b_cnt), j = (uint32_t)(p - (uint64_t)i * w.b_cnt);
+                const float4* a = triA + ((size_t)w.a_off + i) * kTriF4;
+                const float4* b = triB + ((size_t)w.b_off + j) * kTriF4;
+                PreTri<double> A, B;
+                pretri(A, v3<double>(a[0].x - ox, a[0].y - oy, a[0].z - oz), v3<double>(a[1].x - ox, a[1].y - oy, a[1].z - oz),
+                       v3<double>(a[2].x - ox, a[2].y - oy, a[2].z - oz));
+                pretri(B, v3<double>(b[0].x - ox, b[0].y - oy, b[0].z - oz), v3<double>(b[1].x - ox, b[1].y - oy, b[1].z - oz),
+                       v3<double>(b[2].x - ox, b[2].y - oy, b[2].z - oz));
+                const double d2 = tri_dist2(A, B);
+                best = d2 < best ? d2 : best;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double v = __shfl_xor_sync(0xffffffffu, best, o);
+            best = v < best ? v : best;
+        }
+        __syncthreads();
+        if (lane == 0) red[wid] = best;
+        __syncthreads();
+        if (tid == 0) {
+            for (int k = 1; k < kF64Block / 32; ++k) best = red[k] < best ? red[k] : best;
+            out[it] = (w.a_cnt && w.b_cnt) ? sqrt(best) : 1e300;
+        }
+    }
+}
+
+cudaError_t launch_refine_f64(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
+                              double* out, cudaStream_t s) {
+    if (n_items <= 0) return cudaSuccess;
+    int grid = n_items < 148 * 64 ? n_items : 148 * 64;
+    refine_f64_kernel<<<grid, kF64Block, 0, s>>>(triA, triB, items, n_items, out);
+    return cudaGetLastError();
+}
+
 // Pack the reference's flat layout (9 floats per triangle + 2 Hausdorff floats)
 // into 48-byte triangle records.
 __global__ void pack_triangles_kernel(const float* __restrict__ data, const float* __restrict__ hd, size_t n,

@@ -11,6 +11,9 @@ cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const Re
                                 float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
                                 int ctas_per_sm, cudaStream_t s);
 size_t tuned_smem_bytes(int warps);
+// exact FP64 minimum distance per item (recheck of undecided object pairs)
+cudaError_t launch_refine_f64(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
+                              double* out, cudaStream_t s);
 cudaError_t launch_pack_triangles(const float* data, const float* hd, size_t n, float4* tri, cudaStream_t s);
 
 }  // namespace tdp

@@ -42,7 +42,7 @@ namespace {
 enum Slot {
     kPq = 20, kPt, kQoff, kPmn, kPmx, kPerr, kPstat, kPvp, kQconf, kCnt, kScanTmp, kRankSt,
     kVpa, kVpb, kVpair, kVmn, kVmx, kVerr, kValive, kVupd, kItems, kItemVp, kRes, kOutQ, kOutT, kOutD,
-    kRecheck,
+    kVexact, kPexact, kRes64,
 };
 
 template <typename T>
@@ -91,6 +91,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     cudaSetDevice(ctx->device);
     cudaStream_t s = ctx->stream;
     LastStats st;
+    if (cudaEventRecord(ctx->ev[0], s) != cudaSuccess) return fail(ctx, TDP_ERR_CUDA, "event record failed");
 
     // ---- 1. object candidates (host) ----
     CandidateQuery cq{t1->host.obj_box.data(), t1->host.obj_xf.data(), t1->n_obj, t2->host.obj_box.data(),
@@ -126,7 +127,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     unsigned* cnt_status = ctx->d_counter + 16;  // undecided, reported
     unsigned* cnt_collect = ctx->d_counter + 20;
 
-    CU(cudaEventRecord(ctx->ev[0], s));
+    CU(cudaEventRecord(ctx->ev[5], s));
     if (P > 0) {
         CU(cudaMemcpyAsync((void*)d.pq, pq.data(), P * 4, cudaMemcpyHostToDevice, s));
         CU(cudaMemcpyAsync((void*)d.pt, ids.data(), P * 4, cudaMemcpyHostToDevice, s));
@@ -174,6 +175,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     unsigned long long full_total = 0;
     double tri_total = 0;
     long refine_items = 0;
+    unsigned undecided = 0;
     for (size_t k = 0; k < lods.size() && V > 0; ++k) {
         const int li = lod_index(lods[k]);
         const bool highest = (k + 1 == lods.size());
@@ -200,7 +202,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
             st.refine_launches++;
             CU(launch_apply_results(d, res, item_vp, W, highest, prm->hausdorff_level, li, (int)k, s)); ++launches;
         }
-        CU(launch_pair_update(d, (int)k, s)); ++launches;
+        CU(launch_pair_update(d, (int)k, tuned, s)); ++launches;
         if (knn) CU(launch_knn_rank(d, prm->knn, tuned, buf<int>(ctx, kRankSt), s));
         else CU(launch_within_decide(d, prm->within_dist, tuned, s));
         ++launches;
@@ -217,7 +219,25 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
             refine_ms += ms;
             full_total += tuned ? fe : trip;
         }
+        undecided = sc[0];
         if (sc[0] == 0) break;
+    }
+
+    // ---- 3b. tuned form: FP64 recheck of pairs whose FP32 ranges stayed inside
+    // their error band through LOD 100 ----
+    if (tuned && undecided > 0 && V > 0 && lods.back() == 100) {
+        ENS(kVexact, Vz * 8); ENS(kPexact, Pz * 8); ENS(kRes64, Vz * 8);
+        double* vexact = buf<double>(ctx, kVexact);
+        CU(cudaMemsetAsync(cnt_items, 0, 4, s));
+        CU(launch_recheck_items(d, t1->vtri[4], t2->vtri[4], items, item_vp, vexact, cnt_items, s)); ++launches;
+        unsigned W64 = 0;
+        CU(cudaMemcpyAsync(&W64, cnt_items, 4, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        CU(launch_refine_f64(t1->tri[4], t2->tri[4], items, (int)W64, buf<double>(ctx, kRes64), s)); ++launches;
+        CU(launch_recheck_finish(d, buf<double>(ctx, kRes64), item_vp, (int)W64, vexact, buf<double>(ctx, kPexact),
+                                 knn, prm->knn, prm->within_dist, s));
+        launches += knn ? 3 : 2;
+        st.recheck_pairs = undecided;
     }
 
     // ---- 4. results ----
@@ -243,7 +263,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     R->q.resize(nres); R->t.resize(nres); R->d.resize(nres);
     for (unsigned i = 0; i < nres; ++i) { R->q[i] = q[order[i]]; R->t[i] = t[order[i]]; R->d[i] = dd[order[i]]; }
     float f_ms = 0, tot_ms = 0;
-    cudaEventElapsedTime(&f_ms, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&f_ms, ctx->ev[5], ctx->ev[1]);
     cudaEventElapsedTime(&tot_ms, ctx->ev[0], ctx->ev[4]);
     st.filter_ms = f_ms;
     st.total_ms = tot_ms;

@@ -828,7 +828,9 @@ int gen_tiles(const GenParams& p, uint8_t* nuc_buf, size_t nuc_cap, size_t* nuc_
     const Proto& PV = PR->ves;
     const size_t nuc_obj = object_bytes(PN), ves_obj = object_bytes(PV);
     const long n_nuc = (long)p.n_vessels * p.nuclei_per_vessel;
-    const size_t need_n = 1 + nuc_obj * (size_t)n_nuc, need_v = 1 + ves_obj * (size_t)p.n_vessels;
+    const long nb0 = std::max(0L, std::min(p.nuclei_begin, n_nuc));
+    const long nb1 = p.nuclei_end <= 0 ? n_nuc : std::max(nb0, std::min(p.nuclei_end, n_nuc));
+    const size_t need_n = 1 + nuc_obj * (size_t)(nb1 - nb0), need_v = 1 + ves_obj * (size_t)p.n_vessels;
     if (nuc_len) *nuc_len = need_n;
     if (ves_len) *ves_len = need_v;
     if (!nuc_buf && !ves_buf) return TDP_OK;
@@ -910,13 +912,14 @@ int gen_tiles(const GenParams& p, uint8_t* nuc_buf, size_t nuc_cap, size_t* nuc_
     }
     if (nuc_buf) {
         nuc_buf[0] = kRawType;
-        parallel_for(n_nuc, threads, [&](long i) {
+        parallel_for(nb1 - nb0, threads, [&](long j) {
+            const long i = nb0 + j;
             std::vector<float> Vf(3 * PN.m.V.size());
             for (size_t k = 0; k < PN.m.V.size(); ++k) {
                 D3 q = nucleus_vertex(nuc[i], PN.m.V[k]);
                 Vf[3 * k] = (float)q.x; Vf[3 * k + 1] = (float)q.y; Vf[3 * k + 2] = (float)q.z;
             }
-            write_object(PN, Vf, nuc_buf + 1 + nuc_obj * (size_t)i);
+            write_object(PN, Vf, nuc_buf + 1 + nuc_obj * (size_t)j);
         });
     }
     if (ves_buf) {

@@ -38,6 +38,7 @@ struct GenParams {
     int threads = 0;           // 0 = hardware concurrency
     float grid = 1000.f;
     float shell_min = 30.f, shell_max = 300.f;
+    long nuclei_begin = 0, nuclei_end = 0;  // emit nuclei [begin, end) only (end <= 0: all)
 };
 
 // Two-phase: call with null buffers to get the byte sizes, then with buffers of

@@ -21,6 +21,8 @@ void tdp_gen_default_params(tdp_gen_params* p) {
     p->grid = d.grid;
     p->shell_min = d.shell_min;
     p->shell_max = d.shell_max;
+    p->nuclei_begin = 0;
+    p->nuclei_end = 0;
 }
 
 int tdp_gen_tiles(const tdp_gen_params* p, uint8_t* nuclei, size_t nuclei_cap, size_t* nuclei_len,
@@ -38,6 +40,8 @@ int tdp_gen_tiles(const tdp_gen_params* p, uint8_t* nuclei, size_t nuclei_cap, s
     g.grid = p->grid;
     g.shell_min = p->shell_min;
     g.shell_max = p->shell_max;
+    g.nuclei_begin = p->nuclei_begin;
+    g.nuclei_end = p->nuclei_end;
     std::string msg;
     int rc = tdp::gen_tiles(g, nuclei, nuclei_cap, nuclei_len, vessels, vessels_cap, vessels_len, msg);
     if (rc != TDP_OK && err && err_cap) {

@@ -82,7 +82,8 @@ class GenParams(C.Structure):
     _fields_ = [("n_vessels", C.c_int), ("nuclei_per_vessel", C.c_int), ("seed", C.c_uint64),
                 ("voxel_size", C.c_int), ("nucleus_subdiv", C.c_int), ("tube_sides", C.c_int),
                 ("tube_rings", C.c_int), ("threads", C.c_int), ("grid", C.c_float),
-                ("shell_min", C.c_float), ("shell_max", C.c_float)]
+                ("shell_min", C.c_float), ("shell_max", C.c_float), ("nuclei_begin", C.c_long),
+                ("nuclei_end", C.c_long)]
 
 
 def gen_tiles(n_vessels: int = 10, nuclei_per_vessel: int = 20, seed: int = 20260001, out=None, **kw):
@@ -278,3 +279,17 @@ def _join(self, tile1: Tile, tile2: Tile | None, query: str = "nn", knn: int = 1
 
 
 Context.join = _join
+
+
+EXPORTED += ["tdp_fp32_peak"]
+
+
+def _fp32_peak(self) -> float:
+    """Measured FP32 FMA throughput (TFLOP/s) of this context's GPU."""
+    v = C.c_double()
+    lib().tdp_fp32_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    self.check(lib().tdp_fp32_peak(self._h, C.byref(v)))
+    return v.value
+
+
+Context.fp32_peak = _fp32_peak

@@ -1,0 +1,342 @@
+"""Benchmark of the spatial-join hot path (filter + LOD refine) on B200.
+
+Workload (one step = one whole join on resident tiles): the within-distance
+join at tau = 400 of 200k nuclei (1000 vessels x 200 nuclei, icosphere
+nuclei of 1280 triangles, ~20k-triangle branching tube vessels, LODs
+20/40/60/80/100, Hausdorff level 2), seeded synthetic tiles in the reference's
+RAW .dt format.  The reference publishes no numbers, so vs_baseline is null.
+
+  value        triangle pairs refined per second by the tuned form, inputs
+               resident in HBM (tiles of ~37 GB: far larger than L2, so no
+               flush is needed between steps); device time of the whole join
+               call (CUDA events on the library's stream, host candidate
+               generation included), max over ranks
+  plain        the same join through the plain form (one CTA per voxel pair,
+               reference FP32 decision rules): the tuned/plain ratio
+  e2e          the same metric through the public C ABI from pinned host tile
+               bytes: tile upload (H2D + unpack) + join + result read-back
+  roofline     the dominant kernel (tuned refine), FP32 CUDA-core bound
+  cpu_baseline the reference's own CPU code (MeshDist, octree; compiled from
+               source into oracle/_ref) on a bounded sample of query nuclei,
+               all host cores
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "within-400 join, 1000 vessels x 200 nuclei (200k nuclei), LODs 20-100, hausdorff level 2"
+N_VESSELS, NUCLEI_PER_VESSEL, TAU, SEED = 1000, 200, 400.0, 20260002
+METRIC = "tri-pairs/s of the within-400 spatial join (filter + LOD refine), tuned form"
+F_TRI = 966.0      # FLOPs of one full triangle-pair evaluation (3dpipe_b200/csrc/tridist.cuh)
+F_CULL = 14.0      # FLOPs of one bounding-sphere cull test (refine_tuned_kernel)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.f:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.f.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Pinned:
+    """Page-locks numpy buffers in place (cudaHostRegister) so host->device
+    copies of the tiles run at full PCIe/C2C speed."""
+
+    def __init__(self, arrays):
+        import torch
+        self.rt = torch.cuda.cudart()
+        self.ptrs = []
+        for a in arrays:
+            ptr = a.ctypes.data
+            if int(self.rt.cudaHostRegister(ptr, a.nbytes, 0)) == 0:
+                self.ptrs.append(ptr)
+
+    def release(self):
+        for p in self.ptrs:
+            self.rt.cudaHostUnregister(p)
+        self.ptrs = []
+
+
+def make_tiles(rank, ws):
+    """Generate the tiles.  With N ranks each rank takes the nuclei of its own
+    contiguous block of vessels (all vessels are replicated): strong scaling."""
+    pkg = importlib.import_module("3dpipe_b200")
+    v0 = rank * N_VESSELS // ws
+    v1 = (rank + 1) * N_VESSELS // ws
+    t = time.time()
+    nb, vb = pkg.tdp.gen_tiles(N_VESSELS, NUCLEI_PER_VESSEL, seed=SEED,
+                               nuclei_begin=v0 * NUCLEI_PER_VESSEL, nuclei_end=v1 * NUCLEI_PER_VESSEL)
+    log(f"[rank {rank}] generated {nb.size / 1e9:.2f} + {vb.size / 1e9:.2f} GB in {time.time() - t:.1f}s")
+    return nb, vb
+
+
+def cpu_reference(nb, vb, steps, warmup, sample_queries, target_s=15.0):
+    """The reference's CPU implementation (oracle/_ref) on a bounded sample of
+    query nuclei, sized so one run takes about target_s seconds."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_bind import ref_join
+    threads = os.cpu_count() or 1
+    r = ref_join(nb, vb, False, False, tau=TAU, threads=threads, max_queries=sample_queries)
+    if r is None:
+        return None
+    n_total = N_VESSELS * NUCLEI_PER_VESSEL
+    sec = max(r[2][0], 1e-3)
+    sample = int(min(n_total, max(sample_queries, sample_queries * target_s / sec)))
+    vals, last = [], None
+    for i in range(warmup + steps):
+        _, _, st = ref_join(nb, vb, False, False, tau=TAU, threads=threads, max_queries=sample)
+        if i >= warmup:
+            vals.append(st[1] / st[0])
+        last = st
+    return {"value": statistics.median(vals), "unit": "tri-pairs/s", "cores": threads, "kind": "reference",
+            "sample": f"first {sample} of {n_total} query nuclei (all their candidate vessels, all LODs); "
+                      f"{last[0]:.1f} s per run, {last[1]:.3g} tri-pairs; join seconds for all nuclei "
+                      f"extrapolate linearly to {last[0] * n_total / sample:.0f} s",
+            "seconds_per_sample": last[0], "tri_pairs_per_sample": last[1]}
+
+
+def run_reference_arm(a):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    ref_so = ROOT / "oracle" / "_ref" / "libtdp_ref.so"
+    if not ref_so.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtdp_ref.so was not built "
+                                                               "(needs the reference sources at build time)"}))
+        return 0
+    nb, vb = make_tiles(0, 1)
+    cb = cpu_reference(nb, vb, a.steps, max(0, min(a.warmup, 1)), a.cpu_sample)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "tri-pairs/s", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": cb["seconds_per_sample"] * 1e3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "impl": "reference CPU (MeshDist + octree compiled from source)"},
+            "impl": "reference", "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "tri-pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=1500, help="query nuclei in the CPU-baseline sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    a = ap.parse_args()
+    if a.impl == "reference":
+        return run_reference_arm(a)
+
+    import torch
+    import torch.distributed as dist
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    pkg = importlib.import_module("3dpipe_b200")
+    nb, vb = make_tiles(rank, ws)
+    t = time.time()
+    pinned = Pinned([nb, vb])
+    log(f"[rank {rank}] page-locked {len(pinned.ptrs)} tile buffers in {time.time() - t:.1f}s")
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def allsum(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    out = {}
+    with pkg.Context(local) as ctx:
+        fp32_peak = ctx.fp32_peak()
+        t = time.time()
+        T1, T2 = pkg.tdp.Tile(ctx, nb), pkg.tdp.Tile(ctx, vb)
+        log(f"[rank {rank}] tiles resident in {time.time() - t:.1f}s, {ctx.memory()[0] / 1e9:.1f} GB on device")
+        # the two forms must agree before anything is timed
+        qa, ra, _ = ctx.join(T1, T2, query="within", within=TAU, form=pkg.FORM_PLAIN)
+        qb, rb, _ = ctx.join(T1, T2, query="within", within=TAU, form=pkg.FORM_TUNED)
+        if not (np.array_equal(qa, qb) and np.array_equal(ra, rb)):
+            raise SystemExit("plain and tuned forms returned different result sets")
+        n_results = len(qb)
+
+        def timed(form, steps, warmup):
+            for _ in range(warmup):
+                ctx.join(T1, T2, query="within", within=TAU, form=form)
+            barrier()
+            ms, st_last, launches = [], None, 0
+            for _ in range(steps):
+                ctx.join(T1, T2, query="within", within=TAU, form=form)
+                st = ctx.stats()
+                ms.append(st["total_ms"])
+                launches += st["kernel_launches"]
+                st_last = st
+            barrier()
+            return ms, st_last, launches
+
+        with ClockSampler(local) as clk:
+            ms_t, st_t, launches_t = timed(pkg.FORM_TUNED, a.steps, a.warmup)
+        clocks = clk.summary()
+        ms_p, st_p, _ = timed(pkg.FORM_PLAIN, max(2, a.steps // 2), 1)
+
+        step_ms = allmax(statistics.median(ms_t))
+        tri = allsum(st_t["tri_pairs"])
+        value = tri / (step_ms / 1e3)
+        plain_ms = allmax(statistics.median(ms_p))
+        plain_value = allsum(st_p["tri_pairs"]) / (plain_ms / 1e3)
+        refine_ms = st_t["refine_ms"]
+        launches_refine = max(1, st_t["refine_launches"])
+        flops = st_t["full_evals"] * F_TRI + st_t["tri_pairs"] * F_CULL
+        achieved = flops / (refine_ms / 1e3) / 1e12
+
+        # end to end through the C ABI from pinned host bytes
+        e2e_ms = []
+        d2h = 0
+        for i in range(a.e2e_steps + 1):
+            barrier()
+            t0 = time.perf_counter()
+            U1, U2 = pkg.tdp.Tile(ctx, nb), pkg.tdp.Tile(ctx, vb)
+            q, r, d = ctx.join(U1, U2, query="within", within=TAU, form=pkg.FORM_TUNED)
+            U1.free(); U2.free()
+            torch.cuda.synchronize()
+            dt = (time.perf_counter() - t0) * 1e3
+            d2h = q.nbytes + r.nbytes + d.nbytes
+            if i > 0:
+                e2e_ms.append(dt)
+        e2e_step = allmax(statistics.median(e2e_ms))
+        e2e_value = tri / (e2e_step / 1e3)
+
+    pinned.release()
+    cpu = None
+    if rank == 0 and not a.no_cpu:
+        cpu = cpu_reference(nb, vb, 1, 0, a.cpu_sample)
+    prof = ROOT / "profiles" / "traffic.json"
+    traffic = None
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get("refine_tuned_bytes_per_launch")
+        except Exception:
+            traffic = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "tri-pairs/s", "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "form": "tuned", "n_nuclei": N_VESSELS * NUCLEI_PER_VESSEL,
+                       "n_vessels": N_VESSELS, "tau": TAU, "seed": SEED, "results": n_results,
+                       "join_seconds": step_ms / 1e3, "tri_pairs_per_join": tri,
+                       "refine_ms": refine_ms, "filter_ms": st_t["filter_ms"],
+                       "l2": "inputs larger than L2 (resident tiles ~37 GB)",
+                       "parallelism": f"{ws} GPU(s), query nuclei sharded by vessel block"},
+            "plain": {"value": plain_value, "unit": "tri-pairs/s", "ms_per_step": plain_ms,
+                      "tuned_over_plain": value / plain_value if plain_value else None},
+            "e2e": {"value": e2e_value, "unit": "tri-pairs/s", "ms_per_step": e2e_step,
+                    "h2d_bytes_per_step": int(nb.size + vb.size), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches_t),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
+                         "kernel": "refine_tuned_kernel",
+                         "peak_source": "measured FP32 FMA probe (tdp_fp32_peak); MEASURED_PEAKS.json has no CUDA-core FP32 figure",
+                         "work": f"full evals x {F_TRI:.0f} + culled pairs x {F_CULL:.0f} FLOPs",
+                         "launches_per_step": launches_refine},
+            "clocks": clocks,
+            "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")} if cpu else None,
+            "stats": {k: st_t[k] for k in ("full_evals", "refine_items", "recheck_pairs", "filter_pairs",
+                                           "filter_voxel_pairs", "kernel_launches")},
+        }
+        print(json.dumps(line))
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -70,6 +70,9 @@ typedef struct {
     long kernel_launches;            /* all kernels launched by the call        */
 } tdp_stats;
 int tdp_last_stats(const tdp_ctx *ctx, tdp_stats *out);
+/* measured FP32 FMA throughput of the context's device in TFLOP/s (CUDA cores,
+ * no tensor cores): the roofline ceiling of the refine kernels. */
+int tdp_fp32_peak(tdp_ctx *ctx, double *tflops);
 
 /* ---- tiles ------------------------------------------------------------------
  * Upload a RAW .dt tile (the bytes of the file, host memory, pinned or not)
@@ -159,6 +162,8 @@ typedef struct {
     int threads;            /* 0 = all hardware threads                         */
     float grid;             /* 1000                                             */
     float shell_min, shell_max; /* 30, 300                                      */
+    long nuclei_begin;      /* emit only nuclei [begin, end) of the full tile   */
+    long nuclei_end;        /* (end <= 0: all); placement is unchanged          */
 } tdp_gen_params;
 void tdp_gen_default_params(tdp_gen_params *p);
 int tdp_gen_tiles(const tdp_gen_params *p, uint8_t *nuclei, size_t nuclei_cap, size_t *nuclei_len,

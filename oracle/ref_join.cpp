@@ -116,7 +116,8 @@ extern "C" long tdr_join(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t
     std::vector<float> box1(6 * n1), xf1(3 * n1), box2(6 * n2), xf2(3 * n2);
     for (long i = 0; i < n1; ++i) { std::memcpy(&box1[6 * i], T1[i].box, 24); std::memcpy(&xf1[3 * i], T1[i].transform, 12); }
     for (long i = 0; i < n2; ++i) { std::memcpy(&box2[6 * i], S[i].box, 24); std::memcpy(&xf2[3 * i], S[i].transform, 12); }
-    // candidates from the reference octree (all queries: the tree is shared), then optionally a prefix
+    // candidates from the reference octree for the (optionally sampled) query prefix
+    if (max_queries > 0 && max_queries < n1) n1 = max_queries;
     std::vector<long> off(n1 + 1);
     std::vector<int> ids;
     long capc = std::max<long>(1024, n1 * 64);
@@ -127,7 +128,6 @@ extern "C" long tdr_join(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t
         if (tot >= 0) { ids.resize(tot); break; }
         capc *= 4;
     }
-    if (max_queries > 0 && max_queries < n1) n1 = max_queries;
     std::vector<Pair> P;
     for (long q = 0; q < n1; ++q)
         for (long k = off[q]; k < off[q + 1]; ++k) { Pair p; p.q = (int)q; p.t = ids[k]; P.push_back(p); }
