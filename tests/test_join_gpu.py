@@ -104,3 +104,23 @@ def test_tile_info(pkg, ctx, gpu_tiles):
     assert i["n_objects"] == 72 and i["n_tris"][4] == 72 * 1280
     assert i["n_tris"][0] == 72 * 256
     assert T2.info()["n_objects"] == 6
+
+
+def test_cli_matches_library(pkg, ctx, gpu_tiles, tmp_path):
+    """`tdbase join ... --print_result` prints the same pairs the C ABI returns."""
+    import subprocess
+    from pathlib import Path
+    nb, vb = tiles(6, 12, 103)
+    p1, p2 = tmp_path / "n.dt", tmp_path / "v.dt"
+    nb.tofile(p1)
+    vb.tofile(p2)
+    exe = Path(pkg.__file__).parent / "bin" / "tdbase"
+    out = subprocess.run([str(exe), "join", "--tile1", str(p1), "--tile2", str(p2), "-q", "within",
+                          "--within_dist", "150", "--print_result", "-g"], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    got = {tuple(map(int, l.split())) for l in out.stdout.splitlines() if l.strip()}
+    T1, T2 = gpu_tiles(6, 12, 103)
+    q, t, _ = ctx.join(T1, T2, query="within", within=150.0)
+    assert got == set(zip(q.tolist(), t.tolist()))
+    assert "results:" in out.stderr
