@@ -281,7 +281,7 @@ def _join(self, tile1: Tile, tile2: Tile | None, query: str = "nn", knn: int = 1
 Context.join = _join
 
 
-EXPORTED += ["tdp_fp32_peak"]
+EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc"]
 
 
 def _fp32_peak(self) -> float:

@@ -145,6 +145,25 @@ enum { TDP_FORM_PLAIN = 0, TDP_FORM_TUNED = 1 };
 int tdp_refine_batch(tdp_ctx *ctx, const float *data, const float *hausdorff, size_t element_num,
                      const size_t *offset_size, uint32_t pair_num, int form, float *out);
 
+/* ---- refine without any device allocation -------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a plugin inside an application that owns the GPU's memory pool, a
+ * process held to a fixed device budget, a latency-critical loop that must not
+ * call cudaMalloc): the same refine as tdp_refine_batch with TDP_FORM_TUNED,
+ * but every pointer is DEVICE memory and the call needs no context and
+ * allocates nothing.  Its working memory is one fixed 14.3 MB __device__ array
+ * inside this library (held by every GPU that loads it until exit), which caps
+ * a call at 262144 triangles and 65536 voxel pairs; larger calls return
+ * TDP_ERR_ARG with a message in err.  The first call on a device looks up that
+ * array's address (make it before any stream capture begins).  All calls on a
+ * device share the array: calls that may overlap on the GPU race, so serialise
+ * them.  Work is enqueued on `stream` (a cudaStream_t, NULL = default stream);
+ * out is valid once the stream reaches it.  Rows of offset_size that point
+ * outside the batch are not read and yield NaN. */
+int tdp_refine_batch_noalloc(const float *data, const float *hausdorff, size_t element_num,
+                             const size_t *offset_size, uint32_t pair_num, float *out, void *stream,
+                             char *err, size_t err_cap);
+
 /* ---- synthetic tiles (host only, no context) --------------------------------
  * Seeded generator of nuclei/vessel tiles in the reference's RAW .dt format.
  * Replaces the CGAL simulator + `tdbase convert` (reference
