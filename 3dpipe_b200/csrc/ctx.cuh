@@ -43,7 +43,7 @@ struct tdp_ctx {
     unsigned* d_counter = nullptr;            // work counters (device)
     unsigned long long* d_stats = nullptr;    // device-side statistics
     tdp::LastStats stats;
-    int tuned_ctas_per_sm = 4;
+    int tuned_ctas_per_sm = 3;
 };
 
 namespace tdp {

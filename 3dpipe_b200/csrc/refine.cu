@@ -106,15 +106,35 @@ __global__ void __launch_bounds__(BLOCK) refine_plain_kernel(const float4* __res
 }
 
 // ------------------------------------------------------------------ tuned form
-// Shared-memory image of one pre-processed triangle, structure-of-arrays so a
-// broadcast read of triangle k by the whole warp is conflict-free.
-constexpr int kPreF = 43;  // 37 PreTri floats + centre(3) + radius + ph + h
-constexpr int kTunedCA = 64;  // A-side triangles per shared-memory chunk
+// One warp per voxel pair, pulled from an atomic work counter by a persistent
+// grid.  Per chunk of (up to 64 A-side x 32 B-side) triangles:
+//   1. both sides are pre-processed once into shared memory (structure of
+//      arrays: a broadcast read of one triangle by the whole warp is one
+//      transaction per field);
+//   2. seed: lane j finds the A triangle whose bounding sphere is nearest to
+//      its B triangle j and evaluates that pair fully, so the three running
+//      minima start close to their final values;
+//   3. cull: for every A triangle i (warp-uniform loop) lane j tests two lower
+//      bounds of d(i, j) against the minima: the bounding-sphere gap and the
+//      gap between the triangles' projections on the axis u joining the two
+//      voxels (projection onto a unit vector never increases a distance, and
+//      for voxels far apart compared with their size this gap is almost the
+//      distance itself); pairs that could still lower a minimum are appended
+//      to a shared-memory queue with a warp ballot;
+//   4. drain: whenever 32 pairs are queued, each lane evaluates one of them
+//      fully, so the expensive test never runs with idle lanes.
+// A pair is skipped only when a lower bound of d(i, j) is >= max(best_d,
+// best_lo + phA + phB, best_hi - hA - hB), so it can lower none of the minima.
+constexpr int kPreF = 44;    // 37 PreTri floats + centre(3) + radius + ph + h + axis projection
+constexpr int kCA = 64;      // A-side triangles per chunk
+constexpr int kCB = 32;      // B-side triangles per chunk
+constexpr int kQueue = 64;   // queued pairs per warp (>= 32 + 31)
+constexpr int kWarpFloats = kPreF * (kCA + kCB) + kQueue / 2;
 
-__device__ __forceinline__ void store_pre(float* s, int k, const PreTri<float>& t, float3 c, float r,
+__device__ __forceinline__ void store_pre(float* s, int ld, int k, const PreTri<float>& t, float3 c, float r,
                                           float ph, float h) {
     float* p = s + k;
-#define PUT(i, v) p[(i) * kTunedCA] = (v)
+#define PUT(i, v) p[(i) * ld] = (v)
     PUT(0, t.v[0].x); PUT(1, t.v[0].y); PUT(2, t.v[0].z);
     PUT(3, t.v[1].x); PUT(4, t.v[1].y); PUT(5, t.v[1].z);
     PUT(6, t.v[2].x); PUT(7, t.v[2].y); PUT(8, t.v[2].z);
@@ -131,9 +151,9 @@ __device__ __forceinline__ void store_pre(float* s, int k, const PreTri<float>& 
 #undef PUT
 }
 
-__device__ __forceinline__ void load_pre(const float* s, int k, PreTri<float>& t) {
+__device__ __forceinline__ void load_pre(const float* s, int ld, int k, PreTri<float>& t) {
     const float* p = s + k;
-#define GET(i) p[(i) * kTunedCA]
+#define GET(i) p[(i) * ld]
     t.v[0] = v3(GET(0), GET(1), GET(2)); t.v[1] = v3(GET(3), GET(4), GET(5)); t.v[2] = v3(GET(6), GET(7), GET(8));
     t.e[0] = v3(GET(9), GET(10), GET(11)); t.e[1] = v3(GET(12), GET(13), GET(14)); t.e[2] = v3(GET(15), GET(16), GET(17));
     t.n = v3(GET(18), GET(19), GET(20)); t.inn = GET(21);
@@ -156,16 +176,62 @@ __device__ __forceinline__ void tri_sphere(const PreTri<float>& t, float3& c, fl
     r = sqrtf(r2) * 1.0001f + 1e-6f;
 }
 
+// Stage n triangles starting at record `off` into a structure-of-arrays block;
+// field 43 gets the triangle's largest (A side, far = false) or smallest
+// (B side, far = true) projection on the axis u.
+__device__ __forceinline__ void stage(const float4* __restrict__ tri, size_t off, int n, float4 o, float* s, int ld,
+                                      int lane, float& rmax, float3 u, bool far) {
+    for (int k = lane; k < n; k += 32) {
+        const float4* t = tri + (off + k) * kTriF4;
+        const float4 t0 = t[0], t1 = t[1], t2 = t[2];
+        PreTri<float> P;
+        pretri(P, v3(t0.x - o.x, t0.y - o.y, t0.z - o.z), v3(t1.x - o.x, t1.y - o.y, t1.z - o.z),
+               v3(t2.x - o.x, t2.y - o.y, t2.z - o.z));
+        float3 c;
+        float r;
+        tri_sphere(P, c, r);
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            rmax = fmaxf(rmax, fmaxf(fabsf(P.v[q].x), fmaxf(fabsf(P.v[q].y), fabsf(P.v[q].z))));
+        store_pre(s, ld, k, P, c, r, t0.w, t1.w);
+        const float p0 = P.v[0].x * u.x + P.v[0].y * u.y + P.v[0].z * u.z;
+        const float p1 = P.v[1].x * u.x + P.v[1].y * u.y + P.v[1].z * u.z;
+        const float p2 = P.v[2].x * u.x + P.v[2].y * u.y + P.v[2].z * u.z;
+        // one ulp-scale margin keeps the bound conservative under FP32 rounding
+        const float mg = 1e-5f * (fabsf(p0) + fabsf(p1) + fabsf(p2)) + 1e-6f;
+        s[43 * ld + k] = far ? fminf(p0, fminf(p1, p2)) - mg : fmaxf(p0, fmaxf(p1, p2)) + mg;
+    }
+}
+
+// the three minima are >= 0, so their bit patterns order like unsigned ints
+__device__ __forceinline__ float warp_min_nonneg(float v) {
+    return __uint_as_float(__reduce_min_sync(0xffffffffu, __float_as_uint(v)));
+}
+
+__device__ __forceinline__ void eval_pair(const float* sA, const float* sB, int i, int j, float& bd, float& bl,
+                                          float& bh) {
+    PreTri<float> A, B;
+    load_pre(sA, kCA, i, A);
+    load_pre(sB, kCB, j, B);
+    const float d = sqrtf(tri_dist2(A, B));
+    bd = fminf(bd, d);
+    bl = fminf(bl, fmaxf(d - sA[41 * kCA + i] - sB[41 * kCB + j], 0.f));
+    bh = fminf(bh, d + sA[42 * kCA + i] + sB[42 * kCB + j]);
+}
+
 template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) refine_tuned_kernel(const float4* __restrict__ triA,
-                                                                  const float4* __restrict__ triB,
-                                                                  const RefineItem* __restrict__ items,
-                                                                  int n_items, float4* __restrict__ out,
-                                                                  unsigned* __restrict__ work_counter,
-                                                                  unsigned long long* __restrict__ n_full) {
+__global__ void __launch_bounds__(WARPS * 32, 3) refine_tuned_kernel(const float4* __restrict__ triA,
+                                                                     const float4* __restrict__ triB,
+                                                                     const RefineItem* __restrict__ items,
+                                                                     int n_items, float4* __restrict__ out,
+                                                                     unsigned* __restrict__ work_counter,
+                                                                     unsigned long long* __restrict__ n_full) {
     extern __shared__ float smem[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float* sA = smem + (size_t)wid * kPreF * kTunedCA;
+    float* sA = smem + (size_t)wid * kWarpFloats;
+    float* sB = sA + kPreF * kCA;
+    unsigned short* queue = reinterpret_cast<unsigned short*>(sB + kPreF * kCB);
+    const unsigned lt_mask = (1u << lane) - 1u;
     unsigned long long full_evals = 0;
 
     while (true) {
@@ -179,66 +245,91 @@ __global__ void __launch_bounds__(WARPS * 32) refine_tuned_kernel(const float4* 
             continue;
         }
         const float4 o4 = triA[(size_t)w.a_off * kTriF4];
+        // separation axis: from the A voxel's first vertex to the B voxel's first vertex
+        float3 u;
+        {
+            const float4 q = triB[(size_t)w.b_off * kTriF4];
+            const float ux = q.x - o4.x, uy = q.y - o4.y, uz = q.z - o4.z;
+            const float n2 = ux * ux + uy * uy + uz * uz;
+            const float inv = n2 > 0.f ? rsqrtf(n2) : 0.f;
+            u = make_float3(ux * inv, uy * inv, uz * inv);
+        }
         float bd = FLT_MAX, bl = FLT_MAX, bh = FLT_MAX, rmax = 0.f;
-
-        for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += 32) {
-            const bool bval = b0 + lane < w.b_cnt;
-            PreTri<float> B;
-            float3 cB = make_float3(0.f, 0.f, 0.f);
-            float rB = 0.f, phB = 0.f, hB = 0.f;
-            if (bval) {
-                const float4* tb = triB + ((size_t)w.b_off + b0 + lane) * kTriF4;
-                float4 t0 = tb[0], t1 = tb[1], t2 = tb[2];
-                pretri(B, v3(t0.x - o4.x, t0.y - o4.y, t0.z - o4.z), v3(t1.x - o4.x, t1.y - o4.y, t1.z - o4.z),
-                       v3(t2.x - o4.x, t2.y - o4.y, t2.z - o4.z));
-                phB = t0.w; hB = t1.w;
-                tri_sphere(B, cB, rB);
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    rmax = fmaxf(rmax, fmaxf(fabsf(B.v[k].x), fmaxf(fabsf(B.v[k].y), fabsf(B.v[k].z))));
-            }
-            for (uint32_t a0 = 0; a0 < w.a_cnt; a0 += kTunedCA) {
-                const int ca = min((uint32_t)kTunedCA, w.a_cnt - a0);
+        for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += kCB) {
+            const int cb = min((uint32_t)kCB, w.b_cnt - b0);
+            __syncwarp();
+            stage(triB, (size_t)w.b_off + b0, cb, o4, sB, kCB, lane, rmax, u, true);
+            for (uint32_t a0 = 0; a0 < w.a_cnt; a0 += kCA) {
+                const int ca = min((uint32_t)kCA, w.a_cnt - a0);
                 __syncwarp();
-                for (int k = lane; k < ca; k += 32) {
-                    const float4* ta = triA + ((size_t)w.a_off + a0 + k) * kTriF4;
-                    float4 t0 = ta[0], t1 = ta[1], t2 = ta[2];
-                    PreTri<float> A;
-                    pretri(A, v3(t0.x - o4.x, t0.y - o4.y, t0.z - o4.z), v3(t1.x - o4.x, t1.y - o4.y, t1.z - o4.z),
-                           v3(t2.x - o4.x, t2.y - o4.y, t2.z - o4.z));
-                    float3 c; float r;
-                    tri_sphere(A, c, r);
-#pragma unroll
-                    for (int q = 0; q < 3; ++q)
-                        rmax = fmaxf(rmax, fmaxf(fabsf(A.v[q].x), fmaxf(fabsf(A.v[q].y), fabsf(A.v[q].z))));
-                    store_pre(sA, k, A, c, r, t0.w, t1.w);
+                stage(triA, (size_t)w.a_off + a0, ca, o4, sA, kCA, lane, rmax, u, false);
+                __syncwarp();
+                const bool bval = lane < cb;
+                float cbx = 0.f, cby = 0.f, cbz = 0.f, rb = 0.f, phb = 0.f, hb = 0.f, pb = 0.f;
+                if (bval) {
+                    cbx = sB[37 * kCB + lane]; cby = sB[38 * kCB + lane]; cbz = sB[39 * kCB + lane];
+                    rb = sB[40 * kCB + lane]; phb = sB[41 * kCB + lane]; hb = sB[42 * kCB + lane];
+                    pb = sB[43 * kCB + lane];
                 }
-                __syncwarp();
-                for (int k = 0; k < ca; ++k) {
-                    if ((k & 7) == 0) { bd = warp_min(bd); bl = warp_min(bl); bh = warp_min(bh); }
-                    if (!bval) continue;
-                    const float* p = sA + k;
-                    const float cx = p[37 * kTunedCA], cy = p[38 * kTunedCA], cz = p[39 * kTunedCA];
-                    const float rA = p[40 * kTunedCA], phA = p[41 * kTunedCA], hA = p[42 * kTunedCA];
-                    const float thr = fmaxf(bd, fmaxf(bl + phA + phB, bh - hA - hB));
-                    const float reach = rA + rB + thr;
-                    const float dx = cx - cB.x, dy = cy - cB.y, dz = cz - cB.z;
-                    const float cc = dx * dx + dy * dy + dz * dz;
-                    if (reach < 0.f || cc > reach * reach) continue;  // cannot lower any minimum
-                    PreTri<float> A;
-                    load_pre(sA, k, A);
-                    const float d = sqrtf(tri_dist2(A, B));
+                // 2. seed: each lane evaluates its own most promising pair
+                int seed = -1;
+                if (bval) {
+                    float best = FLT_MAX;
+                    for (int i = 0; i < ca; ++i) {
+                        const float dx = sA[37 * kCA + i] - cbx, dy = sA[38 * kCA + i] - cby, dz = sA[39 * kCA + i] - cbz;
+                        const float lb = fmaxf(sqrtf(dx * dx + dy * dy + dz * dz) - sA[40 * kCA + i] - rb,
+                                               pb - sA[43 * kCA + i]);
+                        if (lb < best) { best = lb; seed = i; }
+                    }
+                    eval_pair(sA, sB, seed, lane, bd, bl, bh);
                     ++full_evals;
-                    bd = fminf(bd, d);
-                    bl = fminf(bl, fmaxf(d - phA - phB, 0.f));
-                    bh = fminf(bh, d + hA + hB);
                 }
+                bd = warp_min_nonneg(bd);
+                bl = warp_min_nonneg(bl);
+                bh = warp_min_nonneg(bh);
+                // 3./4. cull, queue, drain
+                int qn = 0;
+                for (int i = 0; i < ca; ++i) {
+                    bool keep = false;
+                    if (bval && i != seed) {
+                        const float dx = sA[37 * kCA + i] - cbx, dy = sA[38 * kCA + i] - cby, dz = sA[39 * kCA + i] - cbz;
+                        const float thr = fmaxf(bd, fmaxf(bl + sA[41 * kCA + i] + phb, bh - sA[42 * kCA + i] - hb));
+                        const float reach = sA[40 * kCA + i] + rb + thr;
+                        keep = pb - sA[43 * kCA + i] < thr && reach > 0.f && dx * dx + dy * dy + dz * dz < reach * reach;
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, keep);
+                    if (keep) queue[qn + __popc(m & lt_mask)] = (unsigned short)((i << 8) | lane);
+                    qn += __popc(m);
+                    if (qn >= 32) {
+                        __syncwarp();
+                        const unsigned e = queue[lane];
+                        eval_pair(sA, sB, e >> 8, e & 0xff, bd, bl, bh);
+                        full_evals += 1;
+                        bd = warp_min_nonneg(bd);
+                        bl = warp_min_nonneg(bl);
+                        bh = warp_min_nonneg(bh);
+                        qn -= 32;
+                        const unsigned short moved = lane < qn ? queue[32 + lane] : 0;
+                        __syncwarp();
+                        if (lane < qn) queue[lane] = moved;
+                        __syncwarp();
+                    }
+                }
+                __syncwarp();
+                if (lane < qn) {
+                    const unsigned e = queue[lane];
+                    eval_pair(sA, sB, e >> 8, e & 0xff, bd, bl, bh);
+                    ++full_evals;
+                }
+                bd = warp_min_nonneg(bd);
+                bl = warp_min_nonneg(bl);
+                bh = warp_min_nonneg(bh);
             }
         }
-        bd = warp_min(bd); bl = warp_min(bl); bh = warp_min(bh); rmax = warp_max(rmax);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
         if (lane == 0) out[it] = make_float4(bd, bl, bh, rmax);
     }
-    // per-warp count of full evaluations (the rest were culled)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) full_evals += __shfl_xor_sync(0xffffffffu, full_evals, o);
     if (lane == 0 && n_full) atomicAdd(n_full, full_evals);
@@ -256,7 +347,7 @@ cudaError_t launch_refine_plain(const float4* triA, const float4* triB, const Re
     return cudaGetLastError();
 }
 
-size_t tuned_smem_bytes(int warps) { return (size_t)warps * kPreF * kTunedCA * sizeof(float); }
+size_t tuned_smem_bytes(int warps) { return (size_t)warps * kWarpFloats * sizeof(float); }
 
 cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                 float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,

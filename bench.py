@@ -198,7 +198,15 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1500, help="query nuclei in the CPU-baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--vessels", type=int, default=None, help="smaller workload for profiling captures")
+    ap.add_argument("--nuclei-per-vessel", type=int, default=None)
     a = ap.parse_args()
+    global N_VESSELS, NUCLEI_PER_VESSEL, WORKLOAD
+    if a.vessels or a.nuclei_per_vessel:
+        N_VESSELS = a.vessels or N_VESSELS
+        NUCLEI_PER_VESSEL = a.nuclei_per_vessel or NUCLEI_PER_VESSEL
+        WORKLOAD = (f"within-400 join, {N_VESSELS} vessels x {NUCLEI_PER_VESSEL} nuclei (reduced, profiling), "
+                    "LODs 20-100, hausdorff level 2")
     if a.impl == "reference":
         return run_reference_arm(a)
 
@@ -280,7 +288,7 @@ def main():
         # end to end through the C ABI from pinned host bytes
         e2e_ms = []
         d2h = 0
-        for i in range(a.e2e_steps + 1):
+        for i in range(a.e2e_steps + 1 if a.e2e_steps > 0 else 0):
             barrier()
             t0 = time.perf_counter()
             U1, U2 = pkg.tdp.Tile(ctx, nb), pkg.tdp.Tile(ctx, vb)
@@ -291,8 +299,8 @@ def main():
             d2h = q.nbytes + r.nbytes + d.nbytes
             if i > 0:
                 e2e_ms.append(dt)
-        e2e_step = allmax(statistics.median(e2e_ms))
-        e2e_value = tri / (e2e_step / 1e3)
+        e2e_step = allmax(statistics.median(e2e_ms)) if e2e_ms else float("nan")
+        e2e_value = tri / (e2e_step / 1e3) if e2e_ms else None
 
     pinned.release()
     cpu = None
