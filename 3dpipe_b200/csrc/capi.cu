@@ -92,6 +92,7 @@ int tdp_ctx_create(int device, size_t budget_bytes, unsigned flags, tdp_ctx** ou
     ctx->num_sms = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return TDP_ERR_CUDA; }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
+    for (auto& e : ctx->lod_ev) cudaEventCreate(&e);
     if (dmalloc(ctx, (void**)&ctx->d_counter, 64 * sizeof(unsigned)) != cudaSuccess ||
         dmalloc(ctx, (void**)&ctx->d_stats, 64 * sizeof(unsigned long long)) != cudaSuccess) {
         tdp_ctx_destroy(ctx);
@@ -109,6 +110,7 @@ int tdp_ctx_destroy(tdp_ctx* ctx) {
     for (auto& kv : ctx->allocs) ptrs.push_back(kv.first);
     for (void* p : ptrs) dfree(ctx, p);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->lod_ev) if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return TDP_OK;
@@ -130,6 +132,9 @@ int tdp_last_stats(const tdp_ctx* ctx, tdp_stats* o) {
     o->filter_pairs = s.filter_pairs;
     o->filter_voxel_pairs = s.filter_voxel_pairs;
     o->kernel_launches = s.kernel_launches;
+    o->candidates_ms = s.candidates_ms;
+    o->lod_ms = s.lod_ms;
+    o->host_syncs = s.host_syncs;
     return TDP_OK;
 }
 

@@ -27,6 +27,9 @@ struct LastStats {
     long filter_pairs = 0;           // object pairs through the filter
     double filter_voxel_pairs = 0;   // voxel pairs evaluated by the filter
     long kernel_launches = 0;        // kernels launched by the call
+    double candidates_ms = 0;        // host wall time of object candidate generation
+    double lod_ms = 0;               // device time of the LOD loop
+    long host_syncs = 0;             // host<->device synchronisations in the call
 };
 
 }  // namespace tdp
@@ -37,6 +40,7 @@ struct tdp_ctx {
     size_t budget = 0, in_use = 0, peak = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[8] = {};
+    cudaEvent_t lod_ev[16] = {};  // refine timing per LOD (tuned loop)
     std::string last_error;
     std::unordered_map<void*, size_t> allocs;
     tdp::Buf scratch[64];

@@ -203,8 +203,9 @@ __global__ void k_build_items(JoinDev d, const uint32_t* __restrict__ vt1, const
     }
 }
 
-__global__ void k_apply_results(JoinDev d, const float4* __restrict__ res, const int* __restrict__ item_vp, int W,
-                                int highest, int level, int li, int stamp) {
+__global__ void k_apply_results(JoinDev d, const float4* __restrict__ res, const int* __restrict__ item_vp, int W_host,
+                                const unsigned* W_dev, int highest, int level, int li, int stamp) {
+    const int W = W_dev ? (int)*W_dev : W_host;
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) {
         const int v = item_vp[w];
         const float4 r = res[w];
@@ -247,8 +248,9 @@ __global__ void k_recheck_items(JoinDev d, const uint32_t* __restrict__ vt1, con
     }
 }
 
-__global__ void k_recheck_apply(const double* __restrict__ res, const int* __restrict__ item_vp, int W,
-                                double* __restrict__ vexact) {
+__global__ void k_recheck_apply(const double* __restrict__ res, const int* __restrict__ item_vp, int W_host,
+                                const unsigned* W_dev, double* __restrict__ vexact) {
+    const int W = W_dev ? (int)*W_dev : W_host;
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) vexact[item_vp[w]] = res[w];
 }
 
@@ -392,9 +394,9 @@ cudaError_t launch_build_items(const JoinDev& d, const uint32_t* vt1, const uint
     return cudaGetLastError();
 }
 cudaError_t launch_apply_results(const JoinDev& d, const float4* res, const int* item_vp, int W, int highest,
-                                 int level, int li, int stamp, cudaStream_t s) {
+                                 int level, int li, int stamp, cudaStream_t s, const unsigned* W_dev) {
     if (W <= 0) return cudaSuccess;
-    k_apply_results<<<grid_for(W, 256), 256, 0, s>>>(d, res, item_vp, W, highest, level, li, stamp);
+    k_apply_results<<<grid_for(W, 256), 256, 0, s>>>(d, res, item_vp, W, W_dev, highest, level, li, stamp);
     return cudaGetLastError();
 }
 cudaError_t launch_pair_update(const JoinDev& d, int stamp, int tuned, cudaStream_t s) {
@@ -409,8 +411,8 @@ cudaError_t launch_recheck_items(const JoinDev& d, const uint32_t* vt1, const ui
     return cudaGetLastError();
 }
 cudaError_t launch_recheck_finish(const JoinDev& d, const double* res, const int* item_vp, int W, double* vexact,
-                                  double* pexact, int knn, int K, float tau, cudaStream_t s) {
-    if (W > 0) k_recheck_apply<<<grid_for(W, 256), 256, 0, s>>>(res, item_vp, W, vexact);
+                                  double* pexact, int knn, int K, float tau, cudaStream_t s, const unsigned* W_dev) {
+    if (W > 0) k_recheck_apply<<<grid_for(W, 256), 256, 0, s>>>(res, item_vp, W, W_dev, vexact);
     if (d.P > 0) k_recheck_pairs<<<grid_for(d.P, kBlock / 32), kBlock, 0, s>>>(d, vexact, pexact, !knn, tau);
     if (knn && d.N1 > 0) k_recheck_knn<<<grid_for(d.N1, 128), 128, 0, s>>>(d, K, pexact);
     return cudaGetLastError();

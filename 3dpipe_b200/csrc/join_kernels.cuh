@@ -60,14 +60,16 @@ cudaError_t launch_write_vps(const JoinDev& d, int within, float tau, int tuned,
 // LOD step
 cudaError_t launch_build_items(const JoinDev& d, const uint32_t* vtri1, const uint32_t* vtri2, RefineItem* items,
                                int* item_vp, unsigned* counter, cudaStream_t s);
+// W: item count, or an upper bound when W_dev (the exact count in device memory) is given
 cudaError_t launch_apply_results(const JoinDev& d, const float4* res, const int* item_vp, int W, int highest,
-                                 int level, int lod_idx, int stamp, cudaStream_t s);
+                                 int level, int lod_idx, int stamp, cudaStream_t s, const unsigned* W_dev = nullptr);
 cudaError_t launch_pair_update(const JoinDev& d, int stamp, int tuned, cudaStream_t s);
 // tuned form: FP64 recheck of the pairs left undecided after LOD 100
 cudaError_t launch_recheck_items(const JoinDev& d, const uint32_t* vtri1, const uint32_t* vtri2, RefineItem* items,
                                  int* item_vp, double* vexact, unsigned* counter, cudaStream_t s);
 cudaError_t launch_recheck_finish(const JoinDev& d, const double* res, const int* item_vp, int W, double* vexact,
-                                  double* pexact, int knn, int K, float tau, cudaStream_t s);
+                                  double* pexact, int knn, int K, float tau, cudaStream_t s,
+                                  const unsigned* W_dev = nullptr);
 cudaError_t launch_count_status(const JoinDev& d, unsigned* counters, cudaStream_t s);
 cudaError_t launch_collect(const JoinDev& d, int* out_q, int* out_t, float* out_d, unsigned* counter,
                            cudaStream_t s);

@@ -223,10 +223,13 @@ template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 3) refine_tuned_kernel(const float4* __restrict__ triA,
                                                                      const float4* __restrict__ triB,
                                                                      const RefineItem* __restrict__ items,
-                                                                     int n_items, float4* __restrict__ out,
+                                                                     int n_items_host, const unsigned* n_items_dev,
+                                                                     float4* __restrict__ out,
                                                                      unsigned* __restrict__ work_counter,
                                                                      unsigned long long* __restrict__ n_full) {
     extern __shared__ float smem[];
+    // the item count comes from device memory when the producer ran on the GPU
+    const int n_items = n_items_dev ? (int)*n_items_dev : n_items_host;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float* sA = smem + (size_t)wid * kWarpFloats;
     float* sB = sA + kPreF * kCA;
@@ -351,7 +354,7 @@ size_t tuned_smem_bytes(int warps) { return (size_t)warps * kWarpFloats * sizeof
 
 cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                 float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
-                                int ctas_per_sm, cudaStream_t s) {
+                                int ctas_per_sm, cudaStream_t s, const unsigned* n_items_dev) {
     if (n_items <= 0) return cudaSuccess;
     static bool attr_set = false;
     const size_t smem = tuned_smem_bytes(kTunedWarps);
@@ -367,8 +370,8 @@ cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const Re
     long need = ((long)n_items + kTunedWarps - 1) / kTunedWarps;
     int grid = (int)(want < need ? want : need);
     if (grid < 1) grid = 1;
-    refine_tuned_kernel<kTunedWarps><<<grid, kTunedWarps * 32, smem, s>>>(triA, triB, items, n_items, out,
-                                                                          work_counter, n_full);
+    refine_tuned_kernel<kTunedWarps><<<grid, kTunedWarps * 32, smem, s>>>(triA, triB, items, n_items, n_items_dev,
+                                                                          out, work_counter, n_full);
     return cudaGetLastError();
 }
 
@@ -379,9 +382,10 @@ constexpr int kF64Block = 128;
 
 __global__ void __launch_bounds__(kF64Block) refine_f64_kernel(const float4* __restrict__ triA,
                                                                const float4* __restrict__ triB,
-                                                               const RefineItem* __restrict__ items, int n_items,
-                                                               double* __restrict__ out) {
+                                                               const RefineItem* __restrict__ items, int n_items_host,
+                                                               const unsigned* n_items_dev, double* __restrict__ out) {
     __shared__ double red[kF64Block / 32];
+    const int n_items = n_items_dev ? (int)*n_items_dev : n_items_host;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
         const RefineItem w = items[it];
@@ -419,10 +423,10 @@ __global__ void __launch_bounds__(kF64Block) refine_f64_kernel(const float4* __r
 }
 
 cudaError_t launch_refine_f64(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
-                              double* out, cudaStream_t s) {
+                              double* out, cudaStream_t s, const unsigned* n_items_dev) {
     if (n_items <= 0) return cudaSuccess;
-    int grid = n_items < 148 * 64 ? n_items : 148 * 64;
-    refine_f64_kernel<<<grid, kF64Block, 0, s>>>(triA, triB, items, n_items, out);
+    int grid = n_items < 148 * 16 ? n_items : 148 * 16;
+    refine_f64_kernel<<<grid, kF64Block, 0, s>>>(triA, triB, items, n_items, n_items_dev, out);
     return cudaGetLastError();
 }
 

@@ -1,4 +1,6 @@
-// refine.cuh -- launchers for the refine kernels (see refine.cu).
+// refine.cuh -- launchers for the refine kernels (see refine.cu).  When
+// n_items_dev is given, the kernel reads the exact item count from device
+// memory and n_items is only an upper bound (it sizes the grid).
 #pragma once
 #include <cuda_runtime.h>
 #include "common.cuh"
@@ -9,11 +11,12 @@ cudaError_t launch_refine_plain(const float4* triA, const float4* triB, const Re
                                 float4* out, cudaStream_t s);
 cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                 float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
-                                int ctas_per_sm, cudaStream_t s);
+                                int ctas_per_sm, cudaStream_t s, const unsigned* n_items_dev = nullptr);
 size_t tuned_smem_bytes(int warps);
 // exact FP64 minimum distance per item (recheck of undecided object pairs)
+// n_items is an upper bound when n_items_dev (the exact count, in device memory) is given
 cudaError_t launch_refine_f64(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
-                              double* out, cudaStream_t s);
+                              double* out, cudaStream_t s, const unsigned* n_items_dev = nullptr);
 cudaError_t launch_pack_triangles(const float* data, const float* hd, size_t n, float4* tri, cudaStream_t s);
 
 }  // namespace tdp

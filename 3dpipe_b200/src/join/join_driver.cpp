@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -98,7 +99,9 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
                       t2->host.obj_xf.data(), t2->n_obj, self, knn, knn ? prm->knn : 0, prm->within_dist, 0};
     std::vector<int64_t> qoff;
     std::vector<int32_t> ids;
+    const auto c0 = std::chrono::steady_clock::now();
     generate_candidates(cq, qoff, ids);
+    st.candidates_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - c0).count();
     const long P = (long)ids.size();
     if (P >= (1L << 31) - 1) return fail(ctx, TDP_ERR_ARG, "too many candidate pairs");
     std::vector<int32_t> pq(P);
@@ -176,68 +179,87 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     double tri_total = 0;
     long refine_items = 0;
     unsigned undecided = 0;
-    for (size_t k = 0; k < lods.size() && V > 0; ++k) {
-        const int li = lod_index(lods[k]);
-        const bool highest = (k + 1 == lods.size());
-        CU(cudaMemsetAsync(ctx->d_counter + 8, 0, 32, s));
-        CU(launch_build_items(d, t1->vtri[li], t2->vtri[li], items, item_vp, cnt_items, s)); ++launches;
-        unsigned hc[4];
-        CU(cudaMemcpyAsync(hc, cnt_items, 16, cudaMemcpyDeviceToHost, s));
-        CU(cudaStreamSynchronize(s));
-        const int W = (int)hc[0];
-        unsigned long long trip;
-        std::memcpy(&trip, &hc[2], 8);
-        tri_total += (double)trip;
-        refine_items += W;
-        if (W > 0) {
-            CU(cudaMemsetAsync(ctx->d_stats, 0, 8, s));
-            CU(cudaEventRecord(ctx->ev[2], s));
-            if (tuned)
-                CU(launch_refine_tuned(t1->tri[li], t2->tri[li], items, W, res, ctx->d_counter, ctx->d_stats,
-                                       ctx->num_sms, ctx->tuned_ctas_per_sm, s));
-            else
+    long syncs = 2;  // candidates upload + voxel-pair count
+    unsigned* lod_counts = ctx->d_counter + 24;   // per-LOD item counts (tuned form)
+    unsigned* cnt_recheck = ctx->d_counter + 32;  // pairs left for the FP64 recheck
+    if (!tuned) {
+        // plain form: the host reads every count, like the reference's chunk loop
+        for (size_t k = 0; k < lods.size() && V > 0; ++k) {
+            const int li = lod_index(lods[k]);
+            const bool highest = (k + 1 == lods.size());
+            CU(cudaMemsetAsync(ctx->d_counter + 8, 0, 32, s));
+            CU(launch_build_items(d, t1->vtri[li], t2->vtri[li], items, item_vp, cnt_items, s)); ++launches;
+            unsigned hc[4];
+            CU(cudaMemcpyAsync(hc, cnt_items, 16, cudaMemcpyDeviceToHost, s));
+            CU(cudaStreamSynchronize(s)); ++syncs;
+            const int W = (int)hc[0];
+            unsigned long long trip;
+            std::memcpy(&trip, &hc[2], 8);
+            tri_total += (double)trip;
+            refine_items += W;
+            if (W > 0) {
+                CU(cudaEventRecord(ctx->ev[2], s));
                 CU(launch_refine_plain(t1->tri[li], t2->tri[li], items, W, res, s));
-            CU(cudaEventRecord(ctx->ev[3], s));
+                CU(cudaEventRecord(ctx->ev[3], s));
+                ++launches;
+                st.refine_launches++;
+                CU(launch_apply_results(d, res, item_vp, W, highest, prm->hausdorff_level, li, (int)k, s)); ++launches;
+            }
+            CU(launch_pair_update(d, (int)k, 0, s)); ++launches;
+            if (knn) CU(launch_knn_rank(d, prm->knn, 0, buf<int>(ctx, kRankSt), s));
+            else CU(launch_within_decide(d, prm->within_dist, 0, s));
+            ++launches;
+            CU(cudaMemsetAsync(cnt_status, 0, 8, s));
+            CU(launch_count_status(d, cnt_status, s)); ++launches;
+            unsigned sc[2];
+            CU(cudaMemcpyAsync(sc, cnt_status, 8, cudaMemcpyDeviceToHost, s));
+            CU(cudaStreamSynchronize(s)); ++syncs;
+            if (W > 0) {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+                refine_ms += ms;
+                full_total += trip;
+            }
+            undecided = sc[0];
+            if (sc[0] == 0) break;
+        }
+    } else if (V > 0) {
+        // tuned form: every count stays on the device, so the whole loop (and
+        // the FP64 recheck) is enqueued without a host round trip; kernels with
+        // nothing left to do exit at once
+        ENS(kVexact, Vz * 8); ENS(kPexact, Pz * 8); ENS(kRes64, Vz * 8);
+        CU(cudaMemsetAsync(ctx->d_counter + 8, 0, 26 * sizeof(unsigned), s));
+        CU(cudaMemsetAsync(ctx->d_stats, 0, 8, s));
+        for (size_t k = 0; k < lods.size(); ++k) {
+            const int li = lod_index(lods[k]);
+            const bool highest = (k + 1 == lods.size());
+            CU(cudaMemsetAsync(cnt_items, 0, 4, s));
+            CU(launch_build_items(d, t1->vtri[li], t2->vtri[li], items, item_vp, cnt_items, s)); ++launches;
+            CU(cudaMemcpyAsync(lod_counts + k, cnt_items, 4, cudaMemcpyDeviceToDevice, s));
+            CU(cudaEventRecord(ctx->lod_ev[2 * k], s));
+            CU(launch_refine_tuned(t1->tri[li], t2->tri[li], items, (int)V, res, ctx->d_counter, ctx->d_stats,
+                                   ctx->num_sms, ctx->tuned_ctas_per_sm, s, cnt_items));
+            CU(cudaEventRecord(ctx->lod_ev[2 * k + 1], s));
             ++launches;
             st.refine_launches++;
-            CU(launch_apply_results(d, res, item_vp, W, highest, prm->hausdorff_level, li, (int)k, s)); ++launches;
+            CU(launch_apply_results(d, res, item_vp, (int)V, highest, prm->hausdorff_level, li, (int)k, s, cnt_items));
+            CU(launch_pair_update(d, (int)k, 1, s));
+            if (knn) CU(launch_knn_rank(d, prm->knn, 1, buf<int>(ctx, kRankSt), s));
+            else CU(launch_within_decide(d, prm->within_dist, 1, s));
+            launches += 3;
         }
-        CU(launch_pair_update(d, (int)k, tuned, s)); ++launches;
-        if (knn) CU(launch_knn_rank(d, prm->knn, tuned, buf<int>(ctx, kRankSt), s));
-        else CU(launch_within_decide(d, prm->within_dist, tuned, s));
-        ++launches;
-        CU(cudaMemsetAsync(cnt_status, 0, 8, s));
-        CU(launch_count_status(d, cnt_status, s)); ++launches;
-        unsigned sc[2];
-        unsigned long long fe = 0;
-        CU(cudaMemcpyAsync(sc, cnt_status, 8, cudaMemcpyDeviceToHost, s));
-        if (W > 0 && tuned) CU(cudaMemcpyAsync(&fe, ctx->d_stats, 8, cudaMemcpyDeviceToHost, s));
-        CU(cudaStreamSynchronize(s));
-        if (W > 0) {
-            float ms = 0;
-            cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
-            refine_ms += ms;
-            full_total += tuned ? fe : trip;
+        // ---- 3b. FP64 recheck of pairs whose FP32 ranges stayed inside their
+        // error band through LOD 100 ----
+        if (lods.back() == 100) {
+            double* vexact = buf<double>(ctx, kVexact);
+            CU(launch_count_status(d, cnt_recheck, s));
+            CU(cudaMemsetAsync(cnt_items, 0, 4, s));
+            CU(launch_recheck_items(d, t1->vtri[4], t2->vtri[4], items, item_vp, vexact, cnt_items, s));
+            CU(launch_refine_f64(t1->tri[4], t2->tri[4], items, (int)V, buf<double>(ctx, kRes64), s, cnt_items));
+            CU(launch_recheck_finish(d, buf<double>(ctx, kRes64), item_vp, (int)V, vexact, buf<double>(ctx, kPexact),
+                                     knn, prm->knn, prm->within_dist, s, cnt_items));
+            launches += knn ? 6 : 5;
         }
-        undecided = sc[0];
-        if (sc[0] == 0) break;
-    }
-
-    // ---- 3b. tuned form: FP64 recheck of pairs whose FP32 ranges stayed inside
-    // their error band through LOD 100 ----
-    if (tuned && undecided > 0 && V > 0 && lods.back() == 100) {
-        ENS(kVexact, Vz * 8); ENS(kPexact, Pz * 8); ENS(kRes64, Vz * 8);
-        double* vexact = buf<double>(ctx, kVexact);
-        CU(cudaMemsetAsync(cnt_items, 0, 4, s));
-        CU(launch_recheck_items(d, t1->vtri[4], t2->vtri[4], items, item_vp, vexact, cnt_items, s)); ++launches;
-        unsigned W64 = 0;
-        CU(cudaMemcpyAsync(&W64, cnt_items, 4, cudaMemcpyDeviceToHost, s));
-        CU(cudaStreamSynchronize(s));
-        CU(launch_refine_f64(t1->tri[4], t2->tri[4], items, (int)W64, buf<double>(ctx, kRes64), s)); ++launches;
-        CU(launch_recheck_finish(d, buf<double>(ctx, kRes64), item_vp, (int)W64, vexact, buf<double>(ctx, kPexact),
-                                 knn, prm->knn, prm->within_dist, s));
-        launches += knn ? 3 : 2;
-        st.recheck_pairs = undecided;
     }
 
     // ---- 4. results ----
@@ -245,8 +267,29 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     CU(launch_collect(d, buf<int>(ctx, kOutQ), buf<int>(ctx, kOutT), buf<float>(ctx, kOutD), cnt_collect, s)); ++launches;
     CU(cudaEventRecord(ctx->ev[4], s));
     unsigned nres = 0;
+    unsigned tc[32] = {0};
+    unsigned long long fe = 0;
     CU(cudaMemcpyAsync(&nres, cnt_collect, 4, cudaMemcpyDeviceToHost, s));
+    if (tuned && V > 0) {
+        CU(cudaMemcpyAsync(tc, ctx->d_counter + 8, 32 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        CU(cudaMemcpyAsync(&fe, ctx->d_stats, 8, cudaMemcpyDeviceToHost, s));
+    }
     CU(cudaStreamSynchronize(s));
+    ++syncs;
+    if (tuned && V > 0) {
+        unsigned long long trip;
+        std::memcpy(&trip, &tc[2], 8);  // d_counter[10..11]
+        tri_total = (double)trip;
+        for (size_t k = 0; k < lods.size(); ++k) {
+            refine_items += tc[16 + k];     // d_counter[24 + k]
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ctx->lod_ev[2 * k], ctx->lod_ev[2 * k + 1]);
+            refine_ms += ms;
+        }
+        full_total = fe;
+        undecided = lods.back() == 100 ? tc[24] : 0;  // d_counter[32]
+        st.recheck_pairs = undecided;
+    }
     tdp_result* R = new tdp_result();
     std::vector<int> q(nres), t(nres);
     std::vector<float> dd(nres);
@@ -272,6 +315,12 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     st.full_evals = full_total;
     st.refine_items = refine_items;
     st.kernel_launches = launches;
+    st.host_syncs = syncs;
+    {
+        float lms = 0;
+        cudaEventElapsedTime(&lms, ctx->ev[1], ctx->ev[4]);
+        st.lod_ms = lms;
+    }
     ctx->stats = st;
     *out = R;
 #undef ENS

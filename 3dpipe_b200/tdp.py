@@ -40,7 +40,8 @@ class Stats(C.Structure):
     _fields_ = [("refine_ms", C.c_double), ("filter_ms", C.c_double), ("total_ms", C.c_double),
                 ("full_evals", C.c_ulonglong), ("tri_pairs", C.c_double), ("refine_items", C.c_long),
                 ("refine_launches", C.c_long), ("recheck_pairs", C.c_long), ("filter_pairs", C.c_long),
-                ("filter_voxel_pairs", C.c_double), ("kernel_launches", C.c_long)]
+                ("filter_voxel_pairs", C.c_double), ("kernel_launches", C.c_long),
+                ("candidates_ms", C.c_double), ("lod_ms", C.c_double), ("host_syncs", C.c_long)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -68,6 +68,9 @@ typedef struct {
     long filter_pairs;               /* object pairs through the filter         */
     double filter_voxel_pairs;       /* voxel pairs evaluated by the filter     */
     long kernel_launches;            /* all kernels launched by the call        */
+    double candidates_ms;            /* host wall time of object candidates     */
+    double lod_ms;                   /* device time of the LOD loop             */
+    long host_syncs;                 /* host<->device synchronisations          */
 } tdp_stats;
 int tdp_last_stats(const tdp_ctx *ctx, tdp_stats *out);
 /* measured FP32 FMA throughput of the context's device in TFLOP/s (CUDA cores,
