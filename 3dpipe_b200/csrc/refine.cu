@@ -274,7 +274,8 @@ __global__ void __launch_bounds__(WARPS * 32, 3) refine_tuned_kernel(const float
                     rb = sB[40 * kCB + lane]; phb = sB[41 * kCB + lane]; hb = sB[42 * kCB + lane];
                     pb = sB[43 * kCB + lane];
                 }
-                // 2. seed: each lane evaluates its own most promising pair
+                // 2. seed: each lane queues its own most promising pair; the queue
+                // is drained before any pair is culled, so the minima start tight
                 int seed = -1;
                 if (bval) {
                     float best = FLT_MAX;
@@ -284,49 +285,48 @@ __global__ void __launch_bounds__(WARPS * 32, 3) refine_tuned_kernel(const float
                                                pb - sA[43 * kCA + i]);
                         if (lb < best) { best = lb; seed = i; }
                     }
-                    eval_pair(sA, sB, seed, lane, bd, bl, bh);
-                    ++full_evals;
                 }
-                bd = warp_min_nonneg(bd);
-                bl = warp_min_nonneg(bl);
-                bh = warp_min_nonneg(bh);
-                // 3./4. cull, queue, drain
-                int qn = 0;
-                for (int i = 0; i < ca; ++i) {
-                    bool keep = false;
-                    if (bval && i != seed) {
-                        const float dx = sA[37 * kCA + i] - cbx, dy = sA[38 * kCA + i] - cby, dz = sA[39 * kCA + i] - cbz;
-                        const float thr = fmaxf(bd, fmaxf(bl + sA[41 * kCA + i] + phb, bh - sA[42 * kCA + i] - hb));
-                        const float reach = sA[40 * kCA + i] + rb + thr;
-                        keep = pb - sA[43 * kCA + i] < thr && reach > 0.f && dx * dx + dy * dy + dz * dz < reach * reach;
+                int qn = __popc(__ballot_sync(0xffffffffu, bval));
+                if (bval) queue[lane] = (unsigned short)((seed << 8) | lane);
+                bool flush = true;
+                // 3./4. cull into the queue, drain 32 pairs at a time; the one
+                // evaluation site below keeps the kernel's code small
+                int i = 0;
+                for (;;) {
+                    while (!flush && qn < 32 && i < ca) {
+                        bool keep = false;
+                        if (bval && i != seed) {
+                            const float dx = sA[37 * kCA + i] - cbx, dy = sA[38 * kCA + i] - cby, dz = sA[39 * kCA + i] - cbz;
+                            const float thr = fmaxf(bd, fmaxf(bl + sA[41 * kCA + i] + phb, bh - sA[42 * kCA + i] - hb));
+                            const float reach = sA[40 * kCA + i] + rb + thr;
+                            keep = pb - sA[43 * kCA + i] < thr && reach > 0.f &&
+                                   dx * dx + dy * dy + dz * dz < reach * reach;
+                        }
+                        const unsigned m = __ballot_sync(0xffffffffu, keep);
+                        if (keep) queue[qn + __popc(m & lt_mask)] = (unsigned short)((i << 8) | lane);
+                        qn += __popc(m);
+                        ++i;
                     }
-                    const unsigned m = __ballot_sync(0xffffffffu, keep);
-                    if (keep) queue[qn + __popc(m & lt_mask)] = (unsigned short)((i << 8) | lane);
-                    qn += __popc(m);
-                    if (qn >= 32) {
-                        __syncwarp();
+                    if (qn == 0) break;
+                    const int take = min(qn, 32);
+                    __syncwarp();
+                    if (lane < take) {
                         const unsigned e = queue[lane];
                         eval_pair(sA, sB, e >> 8, e & 0xff, bd, bl, bh);
-                        full_evals += 1;
-                        bd = warp_min_nonneg(bd);
-                        bl = warp_min_nonneg(bl);
-                        bh = warp_min_nonneg(bh);
-                        qn -= 32;
-                        const unsigned short moved = lane < qn ? queue[32 + lane] : 0;
-                        __syncwarp();
-                        if (lane < qn) queue[lane] = moved;
-                        __syncwarp();
+                        ++full_evals;
                     }
+                    bd = warp_min_nonneg(bd);
+                    bl = warp_min_nonneg(bl);
+                    bh = warp_min_nonneg(bh);
+                    qn -= take;
+                    const unsigned short moved = lane < qn ? queue[take + lane] : 0;
+                    __syncwarp();
+                    if (lane < qn) queue[lane] = moved;
+                    __syncwarp();
+                    flush = false;
+                    if (i >= ca && qn == 0) break;
+                    if (i >= ca) flush = true;  // last partial batch
                 }
-                __syncwarp();
-                if (lane < qn) {
-                    const unsigned e = queue[lane];
-                    eval_pair(sA, sB, e >> 8, e & 0xff, bd, bl, bh);
-                    ++full_evals;
-                }
-                bd = warp_min_nonneg(bd);
-                bl = warp_min_nonneg(bl);
-                bh = warp_min_nonneg(bh);
             }
         }
 #pragma unroll
