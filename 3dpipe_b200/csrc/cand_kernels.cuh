@@ -1,0 +1,20 @@
+// cand_kernels.cuh -- object candidate generation on the GPU (the first filter level).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ctx.cuh"
+#include "storage/dev_tile.h"
+
+namespace tdp {
+
+// Candidates of every tile-1 object against tile 2, the same set and order as
+// generate_candidates() (src/index/candidates.cpp) and the reference octree.
+// On success pq/pt (object pairs, grouped by query object) and qoff ([n1+1]
+// CSR) are device buffers owned by the context's scratch, P is the pair count.
+// overflow is set when a kNN ring search exceeded its per-warp buffer; the
+// caller then uses the host path for this join.
+int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool self, bool knn, int K, float tau,
+                      Buf& pq_buf, Buf& pt_buf, Buf& qoff_buf, long& P, bool& overflow);
+
+}  // namespace tdp

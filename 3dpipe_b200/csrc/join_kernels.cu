@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(kBlock) k_pair_bounds(JoinDev d) {
             d.pmx[p] = mx;
             d.perr[p] = kVoxRel * fmaxf(mn, mx);
             d.pstat[p] = kUndecided;
+            if (d.stat_vp) atomicAdd(d.stat_vp, (unsigned long long)(a1 - a0) * (b1 - b0));
         }
     }
 }

@@ -46,6 +46,7 @@ struct JoinDev {
     float* verr;
     uint8_t* valive;
     int* vupd;
+    unsigned long long* stat_vp;  // voxel pairs evaluated by the filter (statistic)
 };
 
 // filter: per object pair, min box gap and min core distance over all voxel pairs

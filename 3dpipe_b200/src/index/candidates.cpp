@@ -30,58 +30,6 @@ float point_dist(const float* a, const float* b) {
     return std::sqrt(dx * dx + dy * dy + dz * dz);
 }
 
-namespace {
-
-struct Grid {
-    float lo[3] = {0, 0, 0};
-    float cell = 1.f;
-    int n[3] = {1, 1, 1};
-    std::vector<int64_t> start;  // CSR over cells
-    std::vector<int32_t> items;
-
-    int ci(float v, int k) const {
-        long c = (long)std::floor((v - lo[k]) / cell);
-        return (int)std::min<long>(std::max<long>(c, 0), n[k] - 1);
-    }
-    size_t id(int x, int y, int z) const { return ((size_t)x * n[1] + y) * n[2] + z; }
-
-    // boxes: 6 floats per object (a point grid passes lo == hi)
-    void build(const float* boxes, long count, int stride_lo, int stride_hi, float cell_) {
-        cell = cell_;
-        float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        lo[0] = lo[1] = lo[2] = INFINITY;
-        for (long i = 0; i < count; ++i)
-            for (int k = 0; k < 3; ++k) {
-                lo[k] = std::min(lo[k], boxes[i * stride_lo + k]);
-                hi[k] = std::max(hi[k], boxes[i * stride_lo + stride_hi + k]);
-            }
-        // keep the number of cells bounded (about 8 per object)
-        const double max_cells = std::max(4096.0, 8.0 * (double)count);
-        auto cells_for = [&](float c) {
-            double p = 1;
-            for (int k = 0; k < 3; ++k) p *= std::ceil((hi[k] - lo[k]) / c) + 1;
-            return p;
-        };
-        while (cells_for(cell) > max_cells) cell *= 1.25f;
-        for (int k = 0; k < 3; ++k) n[k] = std::max(1, (int)std::ceil((hi[k] - lo[k]) / cell) + 1);
-        std::vector<int64_t> cnt(id(n[0] - 1, n[1] - 1, n[2] - 1) + 2, 0);
-        auto each = [&](long i, auto fn) {
-            const float* b = boxes + i * stride_lo;
-            int x0 = ci(b[0], 0), x1 = ci(b[stride_hi + 0], 0), y0 = ci(b[1], 1), y1 = ci(b[stride_hi + 1], 1);
-            int z0 = ci(b[2], 2), z1 = ci(b[stride_hi + 2], 2);
-            for (int x = x0; x <= x1; ++x)
-                for (int y = y0; y <= y1; ++y)
-                    for (int z = z0; z <= z1; ++z) fn(id(x, y, z));
-        };
-        for (long i = 0; i < count; ++i) each(i, [&](size_t c) { cnt[c + 1]++; });
-        for (size_t c = 1; c < cnt.size(); ++c) cnt[c] += cnt[c - 1];
-        start = cnt;
-        items.resize(start.back());
-        std::vector<int64_t> fill(start.begin(), start.end() - 1);
-        for (long i = 0; i < count; ++i) each(i, [&](size_t c) { items[fill[c]++] = (int32_t)i; });
-    }
-};
-
 float pick_cell(const float* box, long n) {
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     std::vector<float> ext;
@@ -102,14 +50,12 @@ float pick_cell(const float* box, long n) {
     return std::max({ext[ext.size() / 2], dens, 1e-3f});
 }
 
-}  // namespace
-
 void generate_candidates(const CandidateQuery& q, std::vector<int64_t>& off, std::vector<int32_t>& ids) {
     off.assign(q.n1 + 1, 0);
     ids.clear();
     if (q.n1 <= 0) return;
     const float cell = pick_cell(q.box2, q.n2);
-    Grid boxes, points;
+    CellGrid boxes, points;
     boxes.build(q.box2, q.n2, 6, 3, cell);
     if (q.is_knn) points.build(q.xf2, q.n2, 3, 0, cell);
 
@@ -169,7 +115,7 @@ void generate_candidates(const CandidateQuery& q, std::vector<int64_t>& off, std
                                         else if (e < heap.top()) { heap.pop(); heap.push(e); }
                                     }
                                 }
-                        if ((int)heap.size() == K && heap.top().first <= (float)r * points.cell) break;
+                        if ((int)heap.size() == K && heap.top().first < (float)r * points.cell - points.slack) break;
                     }
                     const float maxk = (int)heap.size() == K ? heap.top().first : INFINITY;
                     std::vector<int32_t> topk;

@@ -5,7 +5,7 @@
 //   SpatialJoin::within_chunking             src/join/WithinJoin.cpp:644-813
 //   mbb_knn_op_gpu_one_kernel / mbb_within_op_gpu_one_kernel (the filter)
 //                                            KNNJoin.cpp:497-851, WithinJoin.cpp:26-258
-// 1. object candidates (src/index, host), uploaded as a CSR of object pairs;
+// 1. object candidates (GPU grid search, or the host grid in src/index), a CSR of object pairs;
 // 2. filter: object ranges from all voxel pairs, kNN rank rule or within
 //    classification, compaction of the voxel pairs that can still matter;
 // 3. per LOD: refine every live, non-empty voxel pair, update voxel and
@@ -26,6 +26,7 @@
 
 #include "../../csrc/ctx.cuh"
 #include "../../csrc/join_kernels.cuh"
+#include "../../csrc/cand_kernels.cuh"
 #include "../../csrc/refine.cuh"
 #include "index/candidates.h"
 #include "storage/dev_tile.h"
@@ -94,23 +95,37 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     LastStats st;
     if (cudaEventRecord(ctx->ev[0], s) != cudaSuccess) return fail(ctx, TDP_ERR_CUDA, "event record failed");
 
-    // ---- 1. object candidates (host) ----
-    CandidateQuery cq{t1->host.obj_box.data(), t1->host.obj_xf.data(), t1->n_obj, t2->host.obj_box.data(),
-                      t2->host.obj_xf.data(), t2->n_obj, self, knn, knn ? prm->knn : 0, prm->within_dist, 0};
-    std::vector<int64_t> qoff;
-    std::vector<int32_t> ids;
-    const auto c0 = std::chrono::steady_clock::now();
-    generate_candidates(cq, qoff, ids);
-    st.candidates_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - c0).count();
-    const long P = (long)ids.size();
-    if (P >= (1L << 31) - 1) return fail(ctx, TDP_ERR_ARG, "too many candidate pairs");
-    std::vector<int32_t> pq(P);
-    for (long i = 0; i < t1->n_obj; ++i)
-        for (int64_t k = qoff[i]; k < qoff[i + 1]; ++k) pq[k] = (int32_t)i;
-
+    // ---- 1. object candidates ----
+    // The tuned form generates them on the GPU (csrc/cand_kernels.cu); the
+    // plain form, and the tuned form when a kNN ring search overflows its
+    // buffer, use the host grid (src/index).  Both give the same set and order.
     int rc;
 #define ENS(slot, bytes) do { if ((rc = ensure(ctx, ctx->scratch[slot], (bytes)))) return rc; } while (0)
 #define CU(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } while (0)
+    std::vector<int64_t> qoff;
+    std::vector<int32_t> ids, pq;
+    long P = 0;
+    bool on_device = false;
+    const auto c0 = std::chrono::steady_clock::now();
+    if (tuned) {
+        bool overflow = false;
+        if ((rc = device_candidates(ctx, t1, t2, self, knn, knn ? prm->knn : 0, prm->within_dist, ctx->scratch[kPq],
+                                    ctx->scratch[kPt], ctx->scratch[kQoff], P, overflow)))
+            return rc;
+        on_device = !overflow;
+    }
+    if (!on_device) {
+        CandidateQuery cq{t1->host.obj_box.data(), t1->host.obj_xf.data(), t1->n_obj, t2->host.obj_box.data(),
+                          t2->host.obj_xf.data(), t2->n_obj, self, knn, knn ? prm->knn : 0, prm->within_dist, 0};
+        generate_candidates(cq, qoff, ids);
+        P = (long)ids.size();
+        if (P >= (1L << 31) - 1) return fail(ctx, TDP_ERR_ARG, "too many candidate pairs");
+        pq.resize(P);
+        for (long i = 0; i < t1->n_obj; ++i)
+            for (int64_t k = qoff[i]; k < qoff[i + 1]; ++k) pq[k] = (int32_t)i;
+    }
+    st.candidates_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - c0).count();
+
     const size_t Pz = (size_t)std::max<long>(P, 1);
     ENS(kPq, Pz * 4); ENS(kPt, Pz * 4); ENS(kQoff, (t1->n_obj + 1) * 8);
     ENS(kPmn, Pz * 4); ENS(kPmx, Pz * 4); ENS(kPerr, Pz * 4); ENS(kPstat, Pz);
@@ -131,12 +146,16 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     unsigned* cnt_collect = ctx->d_counter + 20;
 
     CU(cudaEventRecord(ctx->ev[5], s));
-    if (P > 0) {
-        CU(cudaMemcpyAsync((void*)d.pq, pq.data(), P * 4, cudaMemcpyHostToDevice, s));
-        CU(cudaMemcpyAsync((void*)d.pt, ids.data(), P * 4, cudaMemcpyHostToDevice, s));
+    if (!on_device) {
+        if (P > 0) {
+            CU(cudaMemcpyAsync((void*)d.pq, pq.data(), P * 4, cudaMemcpyHostToDevice, s));
+            CU(cudaMemcpyAsync((void*)d.pt, ids.data(), P * 4, cudaMemcpyHostToDevice, s));
+        }
+        CU(cudaMemcpyAsync((void*)d.qoff, qoff.data(), qoff.size() * 8, cudaMemcpyHostToDevice, s));
     }
-    CU(cudaMemcpyAsync((void*)d.qoff, qoff.data(), qoff.size() * 8, cudaMemcpyHostToDevice, s));
     CU(cudaMemsetAsync(d.qconf, 0, t1->n_obj * 4, s));
+    CU(cudaMemsetAsync(ctx->d_stats + 1, 0, 8, s));
+    d.stat_vp = ctx->d_stats + 1;
     long launches = 0;
 
     // ---- 2. filter ----
@@ -165,10 +184,6 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     CU(launch_write_vps(d, !knn, prm->within_dist, tuned, s)); ++launches;
     CU(cudaEventRecord(ctx->ev[1], s));
     st.filter_pairs = P;
-    for (long i = 0; i < t1->n_obj; ++i)
-        for (int64_t k = qoff[i]; k < qoff[i + 1]; ++k)
-            st.filter_voxel_pairs += (double)(t1->host.obj_vox_off[i + 1] - t1->host.obj_vox_off[i]) *
-                                     (double)(t2->host.obj_vox_off[ids[k] + 1] - t2->host.obj_vox_off[ids[k]]);
 
     // ---- 3. LOD loop ----
     RefineItem* items = buf<RefineItem>(ctx, kItems);
@@ -270,12 +285,15 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     unsigned tc[32] = {0};
     unsigned long long fe = 0;
     CU(cudaMemcpyAsync(&nres, cnt_collect, 4, cudaMemcpyDeviceToHost, s));
+    unsigned long long fvp = 0;
+    CU(cudaMemcpyAsync(&fvp, ctx->d_stats + 1, 8, cudaMemcpyDeviceToHost, s));
     if (tuned && V > 0) {
         CU(cudaMemcpyAsync(tc, ctx->d_counter + 8, 32 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
         CU(cudaMemcpyAsync(&fe, ctx->d_stats, 8, cudaMemcpyDeviceToHost, s));
     }
     CU(cudaStreamSynchronize(s));
     ++syncs;
+    st.filter_voxel_pairs = (double)fvp;
     if (tuned && V > 0) {
         unsigned long long trip;
         std::memcpy(&trip, &tc[2], 8);  // d_counter[10..11]

@@ -17,8 +17,22 @@
 
 #include "storage/dt_format.h"
 
+namespace tdp {
+// A uniform grid over a tile's object boxes or transform points, resident on
+// the device (built once per tile, on first use by a join).
+struct DevGrid {
+    float lo[3] = {0, 0, 0};
+    float cell = 1.f, slack = 0.f;
+    int n[3] = {1, 1, 1};
+    int64_t* start = nullptr;  // [cells + 1]
+    int32_t* items = nullptr;
+    bool ready = false;
+};
+}  // namespace tdp
+
 struct tdp_tile {
     tdp::TileHost host;
+    mutable tdp::DevGrid box_grid, point_grid;  // object candidate grids (lazily built)
     long n_obj = 0, n_vox = 0;
     float4* vox = nullptr;
     uint32_t* obj_vox = nullptr;

@@ -282,7 +282,27 @@ def _join(self, tile1: Tile, tile2: Tile | None, query: str = "nn", knn: int = 1
 Context.join = _join
 
 
-EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc"]
+EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates"]
+
+
+def tile_candidates(ctx, tile1, tile2=None, knn=0, within=0.0):
+    """Object candidates computed on the GPU from resident tiles: (CSR offsets, ids)."""
+    L = lib()
+    L.tdp_tile_candidates.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p,
+                                      C.c_void_p, C.c_long]
+    L.tdp_tile_candidates.restype = C.c_long
+    n1 = tile1.info()["n_objects"]
+    off = np.zeros(n1 + 1, np.int64)
+    t2 = None if tile2 is None else tile2.handle
+    n = L.tdp_tile_candidates(ctx.handle, tile1.handle, t2, int(knn > 0), max(knn, 1), float(within), _ptr(off), None, 0)
+    if n == -(2 ** 63):
+        raise TdpError(2, L.tdp_last_error(ctx.handle).decode())
+    ids = np.zeros(max(-n, 1), np.int32)
+    n = L.tdp_tile_candidates(ctx.handle, tile1.handle, t2, int(knn > 0), max(knn, 1), float(within), _ptr(off),
+                              _ptr(ids), ids.size)
+    if n < 0:
+        raise TdpError(2, L.tdp_last_error(ctx.handle).decode())
+    return off, ids[:n]
 
 
 def _fp32_peak(self) -> float:

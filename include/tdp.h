@@ -104,6 +104,11 @@ int tdp_tile_get_info(const tdp_tile *tile, tdp_tile_info *out);
  * cap is too small (off is then valid, ids is not), LONG_MIN on bad arguments. */
 long tdp_candidates(const float *box1, const float *xf1, long n1, const float *box2, const float *xf2, long n2,
                     int self_join, int is_knn, int knn, float within, int64_t *off, int32_t *ids, long cap);
+/* The same candidates computed on the GPU for two resident tiles (tile2 NULL or
+ * == tile1: self-join); this is what the tuned join uses.  Same return
+ * convention as tdp_candidates; LONG_MIN on error (see tdp_last_error). */
+long tdp_tile_candidates(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, int is_knn, int knn,
+                         float within, int64_t *off, int32_t *ids, long cap);
 
 /* ---- join ---------------------------------------------------------------------
  * `tdbase join` (reference src/tools/tdbase.cpp:482-549) on device-resident tiles:

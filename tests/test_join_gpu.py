@@ -124,3 +124,36 @@ def test_cli_matches_library(pkg, ctx, gpu_tiles, tmp_path):
     q, t, _ = ctx.join(T1, T2, query="within", within=150.0)
     assert got == set(zip(q.tolist(), t.tolist()))
     assert "results:" in out.stderr
+
+
+@pytest.mark.parametrize("args", [dict(knn=3), dict(knn=1), dict(knn=7), dict(within=150.0), dict(within=400.0)])
+def test_gpu_candidates_match_reference_octree(pkg, ctx, gpu_tiles, ref, args):
+    """The GPU candidate generation (used by the tuned join) returns the reference
+    octree's candidates, same set and same order, and agrees with the host grid."""
+    from rawdt import read_tile
+    nb, vb = tiles(6, 12, 101)
+    T1, T2 = gpu_tiles(6, 12, 101)
+    off, ids = pkg.tdp.tile_candidates(ctx, T1, T2, **args)
+    N, V = read_tile(nb), read_tile(vb)
+    b1 = np.stack([o.box for o in N]); x1 = np.stack([o.transform for o in N])
+    b2 = np.stack([o.box for o in V]); x2 = np.stack([o.transform for o in V])
+    hoff, hids = pkg.tdp.candidates(b1, x1, b2, x2, **args)
+    np.testing.assert_array_equal(off, hoff)
+    np.testing.assert_array_equal(ids, hids)
+    if ref is not None:
+        roff, rids = ref.candidates(b1, x1, b2, x2, False, args.get("knn", 1), args.get("within", 0.0), "knn" in args)
+        np.testing.assert_array_equal(off, roff)
+        np.testing.assert_array_equal(ids, rids)
+
+
+@pytest.mark.parametrize("args", [dict(knn=5), dict(within=60.0)])
+def test_gpu_candidates_self_join(pkg, ctx, gpu_tiles, ref, args):
+    from rawdt import read_tile
+    nb, _ = tiles(4, 16, 105)
+    T1, _ = gpu_tiles(4, 16, 105)
+    off, ids = pkg.tdp.tile_candidates(ctx, T1, None, **args)
+    N = read_tile(nb)
+    b1 = np.stack([o.box for o in N]); x1 = np.stack([o.transform for o in N])
+    hoff, hids = pkg.tdp.candidates(b1, x1, b1, x1, self_join=True, **args)
+    np.testing.assert_array_equal(off, hoff)
+    np.testing.assert_array_equal(ids, hids)
