@@ -159,6 +159,32 @@ int tdp_fp32_peak(tdp_ctx* ctx, double* tflops) {
     return TDP_OK;
 }
 
+int tdp_refine_config_count(void) { return tdp::kTunedConfigs; }
+
+int tdp_refine_config_info(int cfg, int* chunk_a, int* ctas_per_sm) {
+    if (cfg < 0 || cfg >= tdp::kTunedConfigs) return TDP_ERR_ARG;
+    const tdp::TunedConfig c = tdp::tuned_config(cfg);
+    if (chunk_a) *chunk_a = c.chunk_a;
+    if (ctas_per_sm) *ctas_per_sm = c.ctas_per_sm;
+    return TDP_OK;
+}
+
+int tdp_set_refine_config(tdp_ctx* ctx, int cfg) {
+    if (!ctx) return TDP_ERR_ARG;
+    if (cfg < 0 || cfg >= tdp::kTunedConfigs)
+        return tdp::fail(ctx, TDP_ERR_ARG, "refine configuration " + std::to_string(cfg) + " out of range");
+    ctx->tuned_cfg = cfg;
+    return TDP_OK;
+}
+
+int tdp_get_refine_config(const tdp_ctx* ctx, int* cfg) {
+    if (!ctx || !cfg) return TDP_ERR_ARG;
+    *cfg = ctx->tuned_cfg;
+    return TDP_OK;
+}
+
+void* tdp_ctx_stream(const tdp_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
 int tdp_ctx_memory(const tdp_ctx* ctx, size_t* in_use, size_t* peak) {
     if (!ctx) return TDP_ERR_ARG;
     if (in_use) *in_use = ctx->in_use;
@@ -206,7 +232,7 @@ int tdp_refine_batch(tdp_ctx* ctx, const float* data, const float* hausdorff, si
         TDP_CUDA_TRY(launch_refine_plain(d_tri, d_tri, d_items, (int)pair_num, d_out, s));
     } else {
         TDP_CUDA_TRY(launch_refine_tuned(d_tri, d_tri, d_items, (int)pair_num, d_out, ctx->d_counter, ctx->d_stats,
-                                         ctx->num_sms, ctx->tuned_ctas_per_sm, s));
+                                         ctx->num_sms, ctx->tuned_cfg, s));
     }
     TDP_CUDA_TRY(cudaEventRecord(ctx->ev[1], s));
     std::vector<float4> res(pair_num);

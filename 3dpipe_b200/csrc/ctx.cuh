@@ -47,7 +47,7 @@ struct tdp_ctx {
     unsigned* d_counter = nullptr;            // work counters (device)
     unsigned long long* d_stats = nullptr;    // device-side statistics
     tdp::LastStats stats;
-    int tuned_ctas_per_sm = 3;
+    int tuned_cfg = 0;  // tuned refine kernel configuration (tdp_set_refine_config / tdp_autotune)
 };
 
 namespace tdp {

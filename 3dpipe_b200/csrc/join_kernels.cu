@@ -21,6 +21,7 @@
 // The reference's block reductions in the filter assume a power-of-two block
 // (computing_gpu.cu:2027-2033, blockDim = min(max_voxel_size, 1024)); the
 // reductions here are exact for any voxel count.
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <float.h>
 
@@ -38,21 +39,32 @@ __device__ __forceinline__ float wmin(float v) {
     return v;
 }
 
+// Squared box gap and squared core-core distance of two voxels (the terms of
+// voxel_dist_core before its square roots).  Per axis the gap is
+// max(0, alo - bhi, blo - ahi); for boxes with lo <= hi at most one of the two
+// differences is positive, so this is the reference's branch
+// (t2 < 0 ? t2^2 : t1 > 0 ? t1^2 : 0) with the same rounding.
+__device__ __forceinline__ void vox_dist2(const float4 alo, const float4 ahi, const float4 ac, const float4 blo,
+                                          const float4 bhi, const float4 bc, float& m, float& M) {
+    const float gx = fmaxf(fmaxf(alo.x - bhi.x, blo.x - ahi.x), 0.f);
+    const float gy = fmaxf(fmaxf(alo.y - bhi.y, blo.y - ahi.y), 0.f);
+    const float gz = fmaxf(fmaxf(alo.z - bhi.z, blo.z - ahi.z), 0.f);
+    const float dx = ac.x - bc.x, dy = ac.y - bc.y, dz = ac.z - bc.z;
+    m = 0.f;
+    M = 0.f;
+    m += gx * gx;
+    M += dx * dx;
+    m += gy * gy;
+    M += dy * dy;
+    m += gz * gz;
+    M += dz * dz;
+}
+
 // voxel_dist_core: box gap and core-core distance, a = tile-1 voxel, b = tile-2 voxel
 __device__ __forceinline__ void vox_dist(const float4* __restrict__ va, const float4* __restrict__ vb, float& mn,
                                          float& mx) {
-    const float4 alo = va[0], ahi = va[1], ac = va[2];
-    const float4 blo = vb[0], bhi = vb[1], bc = vb[2];
-    float m = 0.f, M = 0.f, t1, t2, dc;
-    t1 = alo.x - bhi.x; t2 = ahi.x - blo.x;
-    if (t2 < 0.f) m += t2 * t2; else if (t1 > 0.f) m += t1 * t1;
-    dc = ac.x - bc.x; M += dc * dc;
-    t1 = alo.y - bhi.y; t2 = ahi.y - blo.y;
-    if (t2 < 0.f) m += t2 * t2; else if (t1 > 0.f) m += t1 * t1;
-    dc = ac.y - bc.y; M += dc * dc;
-    t1 = alo.z - bhi.z; t2 = ahi.z - blo.z;
-    if (t2 < 0.f) m += t2 * t2; else if (t1 > 0.f) m += t1 * t1;
-    dc = ac.z - bc.z; M += dc * dc;
+    float m, M;
+    vox_dist2(va[0], va[1], va[2], vb[0], vb[1], vb[2], m, M);
     mn = sqrtf(m);
     mx = sqrtf(M);
 }
@@ -60,32 +72,79 @@ __device__ __forceinline__ void vox_dist(const float4* __restrict__ va, const fl
 // relative FP32 error of a box gap / core distance: a handful of roundings
 constexpr float kVoxRel = 8.0f * kUnitRoundoff;
 
+constexpr int kPBWarps = kBlock / 32;
+constexpr int kPBCap = 64;    // tile-1 voxels staged per warp and pass
+constexpr int kPBSmall = 24;  // below this many tile-2 voxels, lanes run over (a, b) pairs
+
+// Object-pair bounds: min over voxel pairs of the box gap and of the core
+// distance.  The square root is correctly rounded and so monotone:
+// min_i sqrt(x_i) == sqrt(min_i x_i) exactly, so the minima are taken over the
+// squared values and each object pair takes two square roots.  The query
+// object's voxels are staged in shared memory (one warp per object pair).
 __global__ void __launch_bounds__(kBlock) k_pair_bounds(JoinDev d) {
-    const int lane = threadIdx.x & 31;
+    __shared__ float4 sa[kPBWarps][kPBCap * 3];
+    __shared__ float4 sb[kPBWarps][kPBSmall * 3];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long vp = 0;  // voxel pairs seen by this warp (lane 0)
     for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
         const int q = d.pq[p], t = d.pt[p];
         const uint32_t a0 = d.ovox1[q], a1 = d.ovox1[q + 1], b0 = d.ovox2[t], b1 = d.ovox2[t + 1];
-        float mn = FLT_MAX, mx = FLT_MAX;
-        for (uint32_t b = b0 + lane; b < b1; b += 32) {
-            const float4* vb = d.vox2 + 3 * (size_t)b;
-            for (uint32_t a = a0; a < a1; ++a) {
-                float m, M;
-                vox_dist(d.vox1 + 3 * (size_t)a, vb, m, M);
-                mn = fminf(mn, m);
-                mx = fminf(mx, M);
+        const int nb = (int)(b1 - b0);
+        float m2 = FLT_MAX, M2 = FLT_MAX;
+        if (nb < kPBSmall) {
+            __syncwarp();
+            for (int i = lane; i < nb * 3; i += 32) sb[w][i] = d.vox2[3 * (size_t)b0 + i];
+        }
+        for (uint32_t ac = a0; ac < a1; ac += kPBCap) {
+            const int na = (int)min((uint32_t)kPBCap, a1 - ac);
+            __syncwarp();
+            for (int i = lane; i < na * 3; i += 32) sa[w][i] = d.vox1[3 * (size_t)ac + i];
+            __syncwarp();
+            if (nb >= kPBSmall) {
+                // two tile-2 voxels per lane share every staged tile-1 voxel; a
+                // missing second one repeats the first (harmless for a minimum)
+                for (int b = lane; b < nb; b += 64) {
+                    const float4* v0 = d.vox2 + 3 * ((size_t)b0 + b);
+                    const float4* v1 = b + 32 < nb ? v0 + 96 : v0;
+                    const float4 lo0 = __ldg(v0), hi0 = __ldg(v0 + 1), c0 = __ldg(v0 + 2);
+                    const float4 lo1 = __ldg(v1), hi1 = __ldg(v1 + 1), c1 = __ldg(v1 + 2);
+                    for (int i = 0; i < na; ++i) {
+                        const float4 alo = sa[w][3 * i], ahi = sa[w][3 * i + 1], acr = sa[w][3 * i + 2];
+                        float m, M, m1, M1;
+                        vox_dist2(alo, ahi, acr, lo0, hi0, c0, m, M);
+                        vox_dist2(alo, ahi, acr, lo1, hi1, c1, m1, M1);
+                        m2 = fminf(m2, fminf(m, m1));
+                        M2 = fminf(M2, fminf(M, M1));
+                    }
+                }
+            } else if (nb > 0) {
+                const int n = na * nb;
+                int i = lane / nb, b = lane - i * nb;
+                for (int k = lane; k < n; k += 32) {
+                    float m, M;
+                    vox_dist2(sa[w][3 * i], sa[w][3 * i + 1], sa[w][3 * i + 2], sb[w][3 * b], sb[w][3 * b + 1],
+                              sb[w][3 * b + 2], m, M);
+                    m2 = fminf(m2, m);
+                    M2 = fminf(M2, M);
+                    b += 32;
+                    while (b >= nb) { b -= nb; ++i; }
+                }
             }
         }
-        mn = wmin(mn);
-        mx = wmin(mx);
+        m2 = wmin(m2);
+        M2 = wmin(M2);
         if (lane == 0) {
+            const float mn = m2 == FLT_MAX ? FLT_MAX : sqrtf(m2);
+            const float mx = M2 == FLT_MAX ? FLT_MAX : sqrtf(M2);
             d.pmn[p] = mn;
             d.pmx[p] = mx;
             d.perr[p] = kVoxRel * fmaxf(mn, mx);
             d.pstat[p] = kUndecided;
-            if (d.stat_vp) atomicAdd(d.stat_vp, (unsigned long long)(a1 - a0) * (b1 - b0));
+            vp += (unsigned long long)(a1 - a0) * (b1 - b0);
         }
     }
+    if (lane == 0 && vp && d.stat_vp) atomicAdd(d.stat_vp, vp);
 }
 
 __global__ void k_within_decide(JoinDev d, float tau, int tuned) {
@@ -343,14 +402,33 @@ __global__ void k_count_status(JoinDev d, unsigned* __restrict__ c) {
     }
 }
 
-__global__ void k_collect(JoinDev d, int* __restrict__ oq, int* __restrict__ ot, float* __restrict__ od,
-                          unsigned* __restrict__ counter) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.P; p += gridDim.x * blockDim.x) {
-        if (d.pstat[p] != kReported) continue;
-        const unsigned w = atomicAdd(counter, 1u);
-        oq[w] = d.pq[p];
-        ot[w] = d.pt[p];
-        if (od) od[w] = d.pmx[p];
+// Result keys: query * n2 + result id for reported pairs, `none` (= n1 * n2)
+// for the rest, so one radix sort over every pair puts the reported ones
+// first, ordered by (query, result id).
+__global__ void k_collect_keys(JoinDev d, long long n2, unsigned long long none, unsigned long long* __restrict__ keys,
+                               float* __restrict__ vals, unsigned* __restrict__ counter) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < d.P; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = base + threadIdx.x;
+        const bool rep = p < d.P && d.pstat[p] == kReported;
+        if (p < d.P) {
+            keys[p] = rep ? (unsigned long long)d.pq[p] * (unsigned long long)n2 + (unsigned)d.pt[p] : none;
+            vals[p] = d.pmx[p];
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, rep);
+        if (lane == 0 && m) atomicAdd(counter, (unsigned)__popc(m));
+    }
+}
+
+__global__ void k_split(const unsigned long long* __restrict__ keys, const float* __restrict__ vals, int64_t n,
+                        long long n2, unsigned long long none, int* __restrict__ oq, int* __restrict__ ot,
+                        float* __restrict__ od) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned long long k = keys[i];
+        if (k == none) break;  // sorted: every later key is `none` too
+        oq[i] = (int)(k / (unsigned long long)n2);
+        ot[i] = (int)(k % (unsigned long long)n2);
+        od[i] = vals[i];
     }
 }
 
@@ -423,9 +501,31 @@ cudaError_t launch_count_status(const JoinDev& d, unsigned* c, cudaStream_t s) {
     k_count_status<<<grid_for(d.P, 256, 148 * 8), 256, 0, s>>>(d, c);
     return cudaGetLastError();
 }
-cudaError_t launch_collect(const JoinDev& d, int* oq, int* ot, float* od, unsigned* counter, cudaStream_t s) {
+static int key_bits(unsigned long long none) {
+    int b = 1;
+    while (b < 64 && (none >> b)) ++b;
+    return b;
+}
+cudaError_t collect_sort_bytes(int64_t P, long long n1, long long n2, size_t& bytes) {
+    bytes = 0;
+    if (P <= 0) return cudaSuccess;
+    cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr);
+    cub::DoubleBuffer<float> v(nullptr, nullptr);
+    return cub::DeviceRadixSort::SortPairs(nullptr, bytes, k, v, (int)P, 0,
+                                           key_bits((unsigned long long)n1 * (unsigned long long)n2));
+}
+cudaError_t launch_collect(const JoinDev& d, long long n2, unsigned long long* keys[2], float* vals[2], void* temp,
+                           size_t temp_bytes, unsigned* counter, int* oq, int* ot, float* od, cudaStream_t s) {
     if (d.P <= 0) return cudaSuccess;
-    k_collect<<<grid_for(d.P, 256), 256, 0, s>>>(d, oq, ot, od, counter);
+    const unsigned long long none = (unsigned long long)d.N1 * (unsigned long long)n2;
+    k_collect_keys<<<grid_for(d.P, 256), 256, 0, s>>>(d, n2, none, keys[0], vals[0], counter);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    cub::DoubleBuffer<unsigned long long> k(keys[0], keys[1]);
+    cub::DoubleBuffer<float> v(vals[0], vals[1]);
+    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, k, v, (int)d.P, 0, key_bits(none), s);
+    if (e != cudaSuccess) return e;
+    k_split<<<grid_for(d.P, 256), 256, 0, s>>>(k.Current(), v.Current(), d.P, n2, none, oq, ot, od);
     return cudaGetLastError();
 }
 

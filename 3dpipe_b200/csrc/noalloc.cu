@@ -147,7 +147,7 @@ extern "C" int tdp_refine_batch_noalloc(const float* data, const float* hausdorf
     e = launch_refine_tuned(tri, tri, reinterpret_cast<const RefineItem*>(scratch + kOffItems), (int)pair_num,
                             reinterpret_cast<float4*>(scratch + kOffRes),
                             reinterpret_cast<unsigned*>(scratch + kOffCounters),
-                            reinterpret_cast<unsigned long long*>(scratch + kOffCounters + 8), sms, 4, s);
+                            reinterpret_cast<unsigned long long*>(scratch + kOffCounters + 8), sms, 0, s);
     if (e != cudaSuccess) return report(err, err_cap, TDP_ERR_CUDA, cudaGetErrorString(e));
     blocks = (int)std::min<size_t>(((size_t)pair_num + 255) / 256, (size_t)sms * 8);
     noalloc_finish_kernel<<<blocks, 256, 0, s>>>(reinterpret_cast<const float4*>(scratch + kOffRes), offset_size,

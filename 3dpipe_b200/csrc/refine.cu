@@ -14,11 +14,11 @@
 //                        memory, every triangle pair fully evaluated.  This is the
 //                        "plain GPU form" the tuned form is measured against.
 //   refine_tuned_kernel  persistent, one warp per voxel pair pulled from an atomic
-//                        work counter; A-side triangles are pre-processed once
-//                        into shared memory, each lane owns one B-side triangle
-//                        in registers, and a bounding-sphere test against the
-//                        warp's running minima skips pairs that cannot lower any
-//                        of the three minima.
+//                        work counter; triangles are pre-processed once into
+//                        shared memory, each lane owns one B-side triangle, and
+//                        cluster- then triangle-level lower bounds against the
+//                        warp's running minima skip pairs that cannot lower any
+//                        of the three minima (details above the kernel).
 #include <float.h>
 #include "common.cuh"
 #include "tridist.cuh"
@@ -107,32 +107,57 @@ __global__ void __launch_bounds__(BLOCK) refine_plain_kernel(const float4* __res
 
 // ------------------------------------------------------------------ tuned form
 // One warp per voxel pair, pulled from an atomic work counter by a persistent
-// grid.  Per chunk of (up to 64 A-side x 32 B-side) triangles:
+// grid (the next index is claimed while the current pair is processed).  Per
+// chunk of up to 64 A-side triangles, staged once, and per chunk of 32 B-side
+// triangles (one per lane):
 //   1. both sides are pre-processed once into shared memory (structure of
 //      arrays: a broadcast read of one triangle by the whole warp is one
-//      transaction per field);
-//   2. seed: lane j finds the A triangle whose bounding sphere is nearest to
+//      transaction per field); each triangle also gets a bounding sphere
+//      (cx, cy, cz, r) and (ph, h, axis projection) as two float4 records;
+//   2. the A chunk is cut into clusters of 8 consecutive triangles (a voxel's
+//      triangles are stored in mesh order, so consecutive triangles are
+//      close); a cluster carries a sphere holding its members' spheres, its
+//      largest axis projection, its largest ph and smallest h;
+//   3. seed: lane j picks the cluster, then the member, whose bound is nearest
 //      its B triangle j and evaluates that pair fully, so the three running
 //      minima start close to their final values;
-//   3. cull: for every A triangle i (warp-uniform loop) lane j tests two lower
-//      bounds of d(i, j) against the minima: the bounding-sphere gap and the
-//      gap between the triangles' projections on the axis u joining the two
-//      voxels (projection onto a unit vector never increases a distance, and
-//      for voxels far apart compared with their size this gap is almost the
-//      distance itself); pairs that could still lower a minimum are appended
-//      to a shared-memory queue with a warp ballot;
-//   4. drain: whenever 32 pairs are queued, each lane evaluates one of them
+//   4. cull: for every cluster (warp-uniform loop) lane j tests the cluster's
+//      lower bounds against the minima; a cluster no lane needs is skipped
+//      whole, otherwise its members are tested one by one with the same two
+//      bounds -- the bounding-sphere gap and the gap between the triangles'
+//      projections on the axis u joining the two voxels (projection onto a
+//      unit vector never increases a distance) -- and pairs that could still
+//      lower a minimum are appended to a shared-memory queue with a warp ballot;
+//   5. drain: whenever 32 pairs are queued, each lane evaluates one of them
 //      fully, so the expensive test never runs with idle lanes.
 // A pair is skipped only when a lower bound of d(i, j) is >= max(best_d,
-// best_lo + phA + phB, best_hi - hA - hB), so it can lower none of the minima.
-constexpr int kPreF = 44;    // 37 PreTri floats + centre(3) + radius + ph + h + axis projection
-constexpr int kCA = 64;      // A-side triangles per chunk
-constexpr int kCB = 32;      // B-side triangles per chunk
-constexpr int kQueue = 64;   // queued pairs per warp (>= 32 + 31)
-constexpr int kWarpFloats = kPreF * (kCA + kCB) + kQueue / 2;
+// best_lo + phA + phB, best_hi - hA - hB), so it can lower none of the minima;
+// a cluster only when its bound is >= that threshold taken with the cluster's
+// largest ph and smallest h, which is >= every member's threshold.
+constexpr int kPreF = 37;   // PreTri floats, structure of arrays
+constexpr int kCB = 32;     // B-side triangles per chunk (one per lane)
+constexpr int kCl = 8;      // A-side triangles per cluster
+constexpr int kQueue = 64;  // queued pairs per warp (>= 32 + 31)
 
-__device__ __forceinline__ void store_pre(float* s, int ld, int k, const PreTri<float>& t, float3 c, float r,
-                                          float ph, float h) {
+// Per-warp shared memory of the tuned kernel for CA A-side triangles per
+// chunk, in floats (every float4 array starts 16-byte aligned).
+template <int CA>
+struct TunedLayout {
+    static_assert(CA % kCl == 0 && CA <= 256, "A chunk must be whole clusters and fit the queue's 8-bit index");
+    static constexpr int kNCl = CA / kCl;
+    static constexpr int kOffSphA = kPreF * CA;
+    static constexpr int kOffAuxA = kOffSphA + 4 * CA;
+    static constexpr int kOffClS = kOffAuxA + 4 * CA;
+    static constexpr int kOffClA = kOffClS + 4 * kNCl;
+    static constexpr int kOffPreB = kOffClA + 4 * kNCl;
+    static constexpr int kOffAuxB = kOffPreB + kPreF * kCB;
+    static constexpr int kOffQueue = kOffAuxB + 4 * kCB;
+    static constexpr int kWarpFloats = kOffQueue + kQueue / 2;
+    static_assert(kOffSphA % 4 == 0 && kOffPreB % 4 == 0 && kOffAuxB % 4 == 0 && kWarpFloats % 4 == 0,
+                  "float4 arrays must stay 16-byte aligned");
+};
+
+__device__ __forceinline__ void store_pre(float* s, int ld, int k, const PreTri<float>& t) {
     float* p = s + k;
 #define PUT(i, v) p[(i) * ld] = (v)
     PUT(0, t.v[0].x); PUT(1, t.v[0].y); PUT(2, t.v[0].z);
@@ -147,7 +172,6 @@ __device__ __forceinline__ void store_pre(float* s, int ld, int k, const PreTri<
     PUT(28, t.m[0].x); PUT(29, t.m[0].y); PUT(30, t.m[0].z);
     PUT(31, t.m[1].x); PUT(32, t.m[1].y); PUT(33, t.m[1].z);
     PUT(34, t.m[2].x); PUT(35, t.m[2].y); PUT(36, t.m[2].z);
-    PUT(37, c.x); PUT(38, c.y); PUT(39, c.z); PUT(40, r); PUT(41, ph); PUT(42, h);
 #undef PUT
 }
 
@@ -176,30 +200,73 @@ __device__ __forceinline__ void tri_sphere(const PreTri<float>& t, float3& c, fl
     r = sqrtf(r2) * 1.0001f + 1e-6f;
 }
 
-// Stage n triangles starting at record `off` into a structure-of-arrays block;
-// field 43 gets the triangle's largest (A side, far = false) or smallest
-// (B side, far = true) projection on the axis u.
-__device__ __forceinline__ void stage(const float4* __restrict__ tri, size_t off, int n, float4 o, float* s, int ld,
-                                      int lane, float& rmax, float3 u, bool far) {
-    for (int k = lane; k < n; k += 32) {
-        const float4* t = tri + (off + k) * kTriF4;
-        const float4 t0 = t[0], t1 = t[1], t2 = t[2];
-        PreTri<float> P;
-        pretri(P, v3(t0.x - o.x, t0.y - o.y, t0.z - o.z), v3(t1.x - o.x, t1.y - o.y, t1.z - o.z),
-               v3(t2.x - o.x, t2.y - o.y, t2.z - o.z));
-        float3 c;
-        float r;
-        tri_sphere(P, c, r);
+// Stage triangle record `idx`: its PreTri fields into column k of a structure
+// of arrays (leading dimension ld); returns sphere = (centre, radius) and
+// aux = (ph, h, projection on u).  The projection is the triangle's largest
+// (A side, far = false) or smallest (B side, far = true) one.
+__device__ __forceinline__ void stage_one(const float4* __restrict__ tri, size_t idx, float4 o, float* s, int ld,
+                                          int k, float3 u, bool far, float& rmax, float4& sph, float4& aux) {
+    const float4* t = tri + idx * kTriF4;
+    const float4 t0 = t[0], t1 = t[1], t2 = t[2];
+    PreTri<float> P;
+    pretri(P, v3(t0.x - o.x, t0.y - o.y, t0.z - o.z), v3(t1.x - o.x, t1.y - o.y, t1.z - o.z),
+           v3(t2.x - o.x, t2.y - o.y, t2.z - o.z));
+    float3 c;
+    float r;
+    tri_sphere(P, c, r);
 #pragma unroll
-        for (int q = 0; q < 3; ++q)
-            rmax = fmaxf(rmax, fmaxf(fabsf(P.v[q].x), fmaxf(fabsf(P.v[q].y), fabsf(P.v[q].z))));
-        store_pre(s, ld, k, P, c, r, t0.w, t1.w);
-        const float p0 = P.v[0].x * u.x + P.v[0].y * u.y + P.v[0].z * u.z;
-        const float p1 = P.v[1].x * u.x + P.v[1].y * u.y + P.v[1].z * u.z;
-        const float p2 = P.v[2].x * u.x + P.v[2].y * u.y + P.v[2].z * u.z;
-        // one ulp-scale margin keeps the bound conservative under FP32 rounding
-        const float mg = 1e-5f * (fabsf(p0) + fabsf(p1) + fabsf(p2)) + 1e-6f;
-        s[43 * ld + k] = far ? fminf(p0, fminf(p1, p2)) - mg : fmaxf(p0, fmaxf(p1, p2)) + mg;
+    for (int q = 0; q < 3; ++q)
+        rmax = fmaxf(rmax, fmaxf(fabsf(P.v[q].x), fmaxf(fabsf(P.v[q].y), fabsf(P.v[q].z))));
+    store_pre(s, ld, k, P);
+    const float p0 = P.v[0].x * u.x + P.v[0].y * u.y + P.v[0].z * u.z;
+    const float p1 = P.v[1].x * u.x + P.v[1].y * u.y + P.v[1].z * u.z;
+    const float p2 = P.v[2].x * u.x + P.v[2].y * u.y + P.v[2].z * u.z;
+    // one ulp-scale margin keeps the bound conservative under FP32 rounding
+    const float mg = 1e-5f * (fabsf(p0) + fabsf(p1) + fabsf(p2)) + 1e-6f;
+    sph = make_float4(c.x, c.y, c.z, r);
+    aux = make_float4(t0.w, t1.w, far ? fminf(p0, fminf(p1, p2)) - mg : fmaxf(p0, fmaxf(p1, p2)) + mg, 0.f);
+}
+
+__device__ __forceinline__ float grp8_min(float v) {
+#pragma unroll
+    for (int o = 1; o < kCl; o <<= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float grp8_max(float v) {
+#pragma unroll
+    for (int o = 1; o < kCl; o <<= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Cluster records of a staged A chunk of n triangles: clS[c] = sphere holding
+// the members' spheres (centre at the middle of their centres' box),
+// clA[c] = (largest ph, smallest h, largest projection).
+template <int CA>
+__device__ __forceinline__ void build_clusters(const float4* sph, const float4* aux, int n, float4* clS, float4* clA,
+                                               int lane) {
+    for (int base = 0; base < CA; base += 32) {
+        const int k = base + lane;
+        const bool v = k < n;
+        const float4 c = v ? sph[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 a = v ? aux[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float lx = grp8_min(v ? c.x : FLT_MAX), hx = grp8_max(v ? c.x : -FLT_MAX);
+        const float ly = grp8_min(v ? c.y : FLT_MAX), hy = grp8_max(v ? c.y : -FLT_MAX);
+        const float lz = grp8_min(v ? c.z : FLT_MAX), hz = grp8_max(v ? c.z : -FLT_MAX);
+        const float cx = 0.5f * (lx + hx), cy = 0.5f * (ly + hy), cz = 0.5f * (lz + hz);
+        float reach = 0.f;
+        if (v) {
+            const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
+            reach = sqrtf(dx * dx + dy * dy + dz * dz) + c.w;
+        }
+        reach = grp8_max(reach);
+        const float phx = grp8_max(v ? a.x : 0.f);
+        const float hmn = grp8_min(v ? a.y : FLT_MAX);
+        const float pmx = grp8_max(v ? a.z : -FLT_MAX);
+        if ((lane & (kCl - 1)) == 0 && v) {
+            // inflated like the member spheres so rounding never culls a needed pair
+            clS[k / kCl] = make_float4(cx, cy, cz, reach * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f);
+            clA[k / kCl] = make_float4(phx, hmn, pmx, 0.f);
+        }
     }
 }
 
@@ -208,43 +275,45 @@ __device__ __forceinline__ float warp_min_nonneg(float v) {
     return __uint_as_float(__reduce_min_sync(0xffffffffu, __float_as_uint(v)));
 }
 
-__device__ __forceinline__ void eval_pair(const float* sA, const float* sB, int i, int j, float& bd, float& bl,
-                                          float& bh) {
-    PreTri<float> A, B;
-    load_pre(sA, kCA, i, A);
-    load_pre(sB, kCB, j, B);
-    const float d = sqrtf(tri_dist2(A, B));
-    bd = fminf(bd, d);
-    bl = fminf(bl, fmaxf(d - sA[41 * kCA + i] - sB[41 * kCB + j], 0.f));
-    bh = fminf(bh, d + sA[42 * kCA + i] + sB[42 * kCB + j]);
-}
+__device__ __forceinline__ float approx_len(float d2) { return d2 * rsqrtf(fmaxf(d2, 1e-30f)); }
 
-template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 3) refine_tuned_kernel(const float4* __restrict__ triA,
+template <int WARPS, int CA, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const float4* __restrict__ triA,
                                                                      const float4* __restrict__ triB,
                                                                      const RefineItem* __restrict__ items,
                                                                      int n_items_host, const unsigned* n_items_dev,
                                                                      float4* __restrict__ out,
                                                                      unsigned* __restrict__ work_counter,
                                                                      unsigned long long* __restrict__ n_full) {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     // the item count comes from device memory when the producer ran on the GPU
     const int n_items = n_items_dev ? (int)*n_items_dev : n_items_host;
+    using L = TunedLayout<CA>;
+    constexpr int kCA = CA;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float* sA = smem + (size_t)wid * kWarpFloats;
-    float* sB = sA + kPreF * kCA;
-    unsigned short* queue = reinterpret_cast<unsigned short*>(sB + kPreF * kCB);
+    float* ws = smem + (size_t)wid * L::kWarpFloats;
+    float* sA = ws;
+    float4* sphA = reinterpret_cast<float4*>(ws + L::kOffSphA);
+    float4* auxA = reinterpret_cast<float4*>(ws + L::kOffAuxA);
+    float4* clS = reinterpret_cast<float4*>(ws + L::kOffClS);
+    float4* clA = reinterpret_cast<float4*>(ws + L::kOffClA);
+    float* sB = ws + L::kOffPreB;
+    float4* auxB = reinterpret_cast<float4*>(ws + L::kOffAuxB);
+    unsigned short* queue = reinterpret_cast<unsigned short*>(ws + L::kOffQueue);
     const unsigned lt_mask = (1u << lane) - 1u;
     unsigned long long full_evals = 0;
 
-    while (true) {
-        unsigned it = 0;
-        if (lane == 0) it = atomicAdd(work_counter, 1u);
-        it = __shfl_sync(0xffffffffu, it, 0);
-        if (it >= (unsigned)n_items) break;
+    unsigned it = 0;
+    if (lane == 0) it = atomicAdd(work_counter, 1u);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    while (it < (unsigned)n_items) {
+        // claim the next pair now; the atomic's latency hides behind this one
+        unsigned next = 0;
+        if (lane == 0) next = atomicAdd(work_counter, 1u);
         const RefineItem w = items[it];
         if (w.a_cnt == 0 || w.b_cnt == 0) {
             if (lane == 0) out[it] = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, 0.f);
+            it = __shfl_sync(0xffffffffu, next, 0);
             continue;
         }
         const float4 o4 = triA[(size_t)w.a_off * kTriF4];
@@ -258,49 +327,77 @@ __global__ void __launch_bounds__(WARPS * 32, 3) refine_tuned_kernel(const float
             u = make_float3(ux * inv, uy * inv, uz * inv);
         }
         float bd = FLT_MAX, bl = FLT_MAX, bh = FLT_MAX, rmax = 0.f;
-        for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += kCB) {
-            const int cb = min((uint32_t)kCB, w.b_cnt - b0);
+        for (uint32_t a0 = 0; a0 < w.a_cnt; a0 += kCA) {
+            const int ca = min((uint32_t)kCA, w.a_cnt - a0);
+            const int ncl = (ca + kCl - 1) / kCl;
             __syncwarp();
-            stage(triB, (size_t)w.b_off + b0, cb, o4, sB, kCB, lane, rmax, u, true);
-            for (uint32_t a0 = 0; a0 < w.a_cnt; a0 += kCA) {
-                const int ca = min((uint32_t)kCA, w.a_cnt - a0);
+            for (int k = lane; k < ca; k += 32)
+                stage_one(triA, (size_t)w.a_off + a0 + k, o4, sA, kCA, k, u, false, rmax, sphA[k], auxA[k]);
+            __syncwarp();
+            build_clusters<CA>(sphA, auxA, ca, clS, clA, lane);
+            for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += kCB) {
+                const int cb = min((uint32_t)kCB, w.b_cnt - b0);
                 __syncwarp();
-                stage(triA, (size_t)w.a_off + a0, ca, o4, sA, kCA, lane, rmax, u, false);
-                __syncwarp();
+                // B side: lane j stages triangle j and keeps its bounds in registers
                 const bool bval = lane < cb;
-                float cbx = 0.f, cby = 0.f, cbz = 0.f, rb = 0.f, phb = 0.f, hb = 0.f, pb = 0.f;
+                float4 sb = make_float4(0.f, 0.f, 0.f, 0.f), ab = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (bval) {
-                    cbx = sB[37 * kCB + lane]; cby = sB[38 * kCB + lane]; cbz = sB[39 * kCB + lane];
-                    rb = sB[40 * kCB + lane]; phb = sB[41 * kCB + lane]; hb = sB[42 * kCB + lane];
-                    pb = sB[43 * kCB + lane];
+                    stage_one(triB, (size_t)w.b_off + b0 + lane, o4, sB, kCB, lane, u, true, rmax, sb, ab);
+                    auxB[lane] = ab;
                 }
-                // 2. seed: each lane queues its own most promising pair; the queue
-                // is drained before any pair is culled, so the minima start tight
+                __syncwarp();
+                // seed: the nearest cluster by its bound, then its nearest member;
+                // the seeds are queued and drained before anything is culled
                 int seed = -1;
                 if (bval) {
                     float best = FLT_MAX;
-                    for (int i = 0; i < ca; ++i) {
-                        const float dx = sA[37 * kCA + i] - cbx, dy = sA[38 * kCA + i] - cby, dz = sA[39 * kCA + i] - cbz;
-                        const float lb = fmaxf(sqrtf(dx * dx + dy * dy + dz * dz) - sA[40 * kCA + i] - rb,
-                                               pb - sA[43 * kCA + i]);
+                    int bc = 0;
+                    for (int c = 0; c < ncl; ++c) {
+                        const float4 s = clS[c];
+                        const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
+                        const float lb = fmaxf(approx_len(dx * dx + dy * dy + dz * dz) - s.w - sb.w, ab.z - clA[c].z);
+                        if (lb < best) { best = lb; bc = c; }
+                    }
+                    best = FLT_MAX;
+                    const int mend = min(ca, (bc + 1) * kCl);
+                    for (int i = bc * kCl; i < mend; ++i) {
+                        const float4 s = sphA[i];
+                        const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
+                        const float lb = fmaxf(approx_len(dx * dx + dy * dy + dz * dz) - s.w - sb.w, ab.z - auxA[i].z);
                         if (lb < best) { best = lb; seed = i; }
                     }
+                    if (seed < 0) seed = bc * kCl;
                 }
                 int qn = __popc(__ballot_sync(0xffffffffu, bval));
                 if (bval) queue[lane] = (unsigned short)((seed << 8) | lane);
                 bool flush = true;
-                // 3./4. cull into the queue, drain 32 pairs at a time; the one
-                // evaluation site below keeps the kernel's code small
+                // cull into the queue, drain 32 pairs at a time; the one evaluation
+                // site below keeps the kernel's code small
                 int i = 0;
+                bool kc = false;
                 for (;;) {
                     while (!flush && qn < 32 && i < ca) {
+                        if ((i & (kCl - 1)) == 0) {
+                            kc = false;
+                            if (bval) {
+                                const float4 s = clS[i / kCl], a = clA[i / kCl];
+                                const float thr = fmaxf(bd, fmaxf(bl + a.x + ab.x, bh - a.y - ab.y));
+                                const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
+                                const float reach = s.w + sb.w + thr;
+                                kc = ab.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach;
+                            }
+                            if (!__any_sync(0xffffffffu, kc)) {
+                                i += kCl;
+                                continue;
+                            }
+                        }
                         bool keep = false;
-                        if (bval && i != seed) {
-                            const float dx = sA[37 * kCA + i] - cbx, dy = sA[38 * kCA + i] - cby, dz = sA[39 * kCA + i] - cbz;
-                            const float thr = fmaxf(bd, fmaxf(bl + sA[41 * kCA + i] + phb, bh - sA[42 * kCA + i] - hb));
-                            const float reach = sA[40 * kCA + i] + rb + thr;
-                            keep = pb - sA[43 * kCA + i] < thr && reach > 0.f &&
-                                   dx * dx + dy * dy + dz * dz < reach * reach;
+                        if (kc && i != seed) {
+                            const float4 s = sphA[i], a = auxA[i];
+                            const float thr = fmaxf(bd, fmaxf(bl + a.x + ab.x, bh - a.y - ab.y));
+                            const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
+                            const float reach = s.w + sb.w + thr;
+                            keep = ab.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach;
                         }
                         const unsigned m = __ballot_sync(0xffffffffu, keep);
                         if (keep) queue[qn + __popc(m & lt_mask)] = (unsigned short)((i << 8) | lane);
@@ -312,7 +409,15 @@ __global__ void __launch_bounds__(WARPS * 32, 3) refine_tuned_kernel(const float
                     __syncwarp();
                     if (lane < take) {
                         const unsigned e = queue[lane];
-                        eval_pair(sA, sB, e >> 8, e & 0xff, bd, bl, bh);
+                        const int qi = e >> 8, qj = e & 0xff;
+                        PreTri<float> A, B;
+                        load_pre(sA, kCA, qi, A);
+                        load_pre(sB, kCB, qj, B);
+                        const float d = sqrtf(tri_dist2(A, B));
+                        const float4 xa = auxA[qi], xb = auxB[qj];
+                        bd = fminf(bd, d);
+                        bl = fminf(bl, fmaxf(d - xa.x - xb.x, 0.f));
+                        bh = fminf(bh, d + xa.y + xb.y);
                         ++full_evals;
                     }
                     bd = warp_min_nonneg(bd);
@@ -332,6 +437,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) refine_tuned_kernel(const float
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
         if (lane == 0) out[it] = make_float4(bd, bl, bh, rmax);
+        it = __shfl_sync(0xffffffffu, next, 0);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) full_evals += __shfl_xor_sync(0xffffffffu, full_evals, o);
@@ -350,29 +456,53 @@ cudaError_t launch_refine_plain(const float4* triA, const float4* triB, const Re
     return cudaGetLastError();
 }
 
-size_t tuned_smem_bytes(int warps) { return (size_t)warps * kWarpFloats * sizeof(float); }
+// The tuned kernel's configurations: A-side triangles staged per warp and
+// CTAs per SM (shared memory per warp shrinks with the A chunk, so a smaller
+// chunk admits more resident warps).  All give identical results: every pair
+// is translated to the same origin and every cull is conservative.
+struct TunedCfgDef {
+    int chunk_a, ctas_per_sm;
+};
+constexpr TunedCfgDef kTunedCfgs[kTunedConfigs] = {{64, 3}, {48, 3}, {32, 4}};
 
-cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
-                                float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
-                                int ctas_per_sm, cudaStream_t s, const unsigned* n_items_dev) {
-    if (n_items <= 0) return cudaSuccess;
-    static bool attr_set = false;
-    const size_t smem = tuned_smem_bytes(kTunedWarps);
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(refine_tuned_kernel<kTunedWarps>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+TunedConfig tuned_config(int cfg) {
+    if (cfg < 0 || cfg >= kTunedConfigs) cfg = 0;
+    return TunedConfig{kTunedCfgs[cfg].chunk_a, kTunedCfgs[cfg].ctas_per_sm};
+}
+
+template <int CA, int MINB>
+static cudaError_t launch_tuned_cfg(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
+                                    float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
+                                    cudaStream_t s, const unsigned* n_items_dev) {
+    static bool attr_set[64] = {};  // per device: the attribute belongs to the device's context
+    const size_t smem = (size_t)kTunedWarps * TunedLayout<CA>::kWarpFloats * sizeof(float);
+    auto kern = refine_tuned_kernel<kTunedWarps, CA, MINB>;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
     cudaError_t e = cudaMemsetAsync(work_counter, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
-    long want = (long)num_sms * ctas_per_sm;
+    long want = (long)num_sms * MINB;
     long need = ((long)n_items + kTunedWarps - 1) / kTunedWarps;
     int grid = (int)(want < need ? want : need);
     if (grid < 1) grid = 1;
-    refine_tuned_kernel<kTunedWarps><<<grid, kTunedWarps * 32, smem, s>>>(triA, triB, items, n_items, n_items_dev,
-                                                                          out, work_counter, n_full);
+    kern<<<grid, kTunedWarps * 32, smem, s>>>(triA, triB, items, n_items, n_items_dev, out, work_counter, n_full);
     return cudaGetLastError();
+}
+
+cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
+                                float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
+                                int cfg, cudaStream_t s, const unsigned* n_items_dev) {
+    if (n_items <= 0) return cudaSuccess;
+    switch (cfg) {
+        case 1: return launch_tuned_cfg<48, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev);
+        case 2: return launch_tuned_cfg<32, 4>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev);
+        default: return launch_tuned_cfg<64, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev);
+    }
 }
 
 // ------------------------------------------------------------------ FP64 recheck

@@ -9,10 +9,16 @@ namespace tdp {
 
 cudaError_t launch_refine_plain(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                 float4* out, cudaStream_t s);
+// tuned-kernel configurations (index 0 is the default); see refine.cu
+constexpr int kTunedConfigs = 3;
+struct TunedConfig {
+    int chunk_a;      // A-side triangles staged per warp and chunk
+    int ctas_per_sm;  // resident CTAs per SM the launch is sized for
+};
+TunedConfig tuned_config(int cfg);
 cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                 float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
-                                int ctas_per_sm, cudaStream_t s, const unsigned* n_items_dev = nullptr);
-size_t tuned_smem_bytes(int warps);
+                                int cfg, cudaStream_t s, const unsigned* n_items_dev = nullptr);
 // exact FP64 minimum distance per item (recheck of undecided object pairs)
 // n_items is an upper bound when n_items_dev (the exact count, in device memory) is given
 cudaError_t launch_refine_f64(const float4* triA, const float4* triB, const RefineItem* items, int n_items,

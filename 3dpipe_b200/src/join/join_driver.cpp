@@ -45,6 +45,7 @@ enum Slot {
     kPq = 20, kPt, kQoff, kPmn, kPmx, kPerr, kPstat, kPvp, kQconf, kCnt, kScanTmp, kRankSt,
     kVpa, kVpb, kVpair, kVmn, kVmx, kVerr, kValive, kVupd, kItems, kItemVp, kRes, kOutQ, kOutT, kOutD,
     kVexact, kPexact, kRes64,
+    kKeyA = 60, kKeyB, kValA, kValB,  // result sort (50-59 hold the candidate buffers)
 };
 
 template <typename T>
@@ -253,7 +254,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
             CU(cudaMemcpyAsync(lod_counts + k, cnt_items, 4, cudaMemcpyDeviceToDevice, s));
             CU(cudaEventRecord(ctx->lod_ev[2 * k], s));
             CU(launch_refine_tuned(t1->tri[li], t2->tri[li], items, (int)V, res, ctx->d_counter, ctx->d_stats,
-                                   ctx->num_sms, ctx->tuned_ctas_per_sm, s, cnt_items));
+                                   ctx->num_sms, ctx->tuned_cfg, s, cnt_items));
             CU(cudaEventRecord(ctx->lod_ev[2 * k + 1], s));
             ++launches;
             st.refine_launches++;
@@ -279,7 +280,17 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
 
     // ---- 4. results ----
     CU(cudaMemsetAsync(cnt_collect, 0, 4, s));
-    CU(launch_collect(d, buf<int>(ctx, kOutQ), buf<int>(ctx, kOutT), buf<float>(ctx, kOutD), cnt_collect, s)); ++launches;
+    {
+        size_t sort_bytes = 0;
+        CU(collect_sort_bytes(P, t1->n_obj, t2->n_obj, sort_bytes));
+        ENS(kKeyA, Pz * 8); ENS(kKeyB, Pz * 8); ENS(kValA, Pz * 4); ENS(kValB, Pz * 4);
+        ENS(kScanTmp, sort_bytes + 16);
+        unsigned long long* keys[2] = {buf<unsigned long long>(ctx, kKeyA), buf<unsigned long long>(ctx, kKeyB)};
+        float* vals[2] = {buf<float>(ctx, kValA), buf<float>(ctx, kValB)};
+        CU(launch_collect(d, t2->n_obj, keys, vals, ctx->scratch[kScanTmp].p, sort_bytes, cnt_collect,
+                          buf<int>(ctx, kOutQ), buf<int>(ctx, kOutT), buf<float>(ctx, kOutD), s));
+        launches += 2;
+    }
     CU(cudaEventRecord(ctx->ev[4], s));
     unsigned nres = 0;
     unsigned tc[32] = {0};
@@ -308,21 +319,16 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         undecided = lods.back() == 100 ? tc[24] : 0;  // d_counter[32]
         st.recheck_pairs = undecided;
     }
+    // rows were sorted by (query, result id) on the device
     tdp_result* R = new tdp_result();
-    std::vector<int> q(nres), t(nres);
-    std::vector<float> dd(nres);
+    R->q.resize(nres); R->t.resize(nres); R->d.resize(nres);
     if (nres) {
-        cudaMemcpyAsync(q.data(), buf<int>(ctx, kOutQ), nres * 4, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(t.data(), buf<int>(ctx, kOutT), nres * 4, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(dd.data(), buf<float>(ctx, kOutD), nres * 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(R->q.data(), buf<int>(ctx, kOutQ), nres * 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(R->t.data(), buf<int>(ctx, kOutT), nres * 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(R->d.data(), buf<float>(ctx, kOutD), nres * 4, cudaMemcpyDeviceToHost, s);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) { delete R; return fail(ctx, TDP_ERR_CUDA, cudaGetErrorString(e)); }
     }
-    std::vector<unsigned> order(nres);
-    std::iota(order.begin(), order.end(), 0u);
-    std::sort(order.begin(), order.end(), [&](unsigned a, unsigned b) { return q[a] != q[b] ? q[a] < q[b] : t[a] < t[b]; });
-    R->q.resize(nres); R->t.resize(nres); R->d.resize(nres);
-    for (unsigned i = 0; i < nres; ++i) { R->q[i] = q[order[i]]; R->t[i] = t[order[i]]; R->d[i] = dd[order[i]]; }
     float f_ms = 0, tot_ms = 0;
     cudaEventElapsedTime(&f_ms, ctx->ev[5], ctx->ev[1]);
     cudaEventElapsedTime(&tot_ms, ctx->ev[0], ctx->ev[4]);
@@ -343,6 +349,38 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     *out = R;
 #undef ENS
 #undef CU
+    return TDP_OK;
+}
+
+int tdp_autotune(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_join_params* prm,
+                 double* ms_per_config, int* best) {
+    if (!ctx || !t1 || !prm) return TDP_ERR_ARG;
+    tdp_join_params p = *prm;
+    p.form = TDP_FORM_TUNED;
+    const int keep = ctx->tuned_cfg;
+    int best_cfg = keep;
+    double best_ms = 1e300;
+    for (int cfg = 0; cfg < kTunedConfigs; ++cfg) {
+        ctx->tuned_cfg = cfg;
+        double ms = 0;
+        for (int rep = 0; rep < 2; ++rep) {  // one untimed run, then one timed
+            tdp_result* r = nullptr;
+            const int rc = tdp_join(ctx, t1, t2, &p, &r);
+            if (rc != TDP_OK) {
+                ctx->tuned_cfg = keep;
+                return rc;
+            }
+            tdp_result_free(r);
+            ms = ctx->stats.refine_ms;
+        }
+        if (ms_per_config) ms_per_config[cfg] = ms;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best_cfg = cfg;
+        }
+    }
+    ctx->tuned_cfg = best_cfg;
+    if (best) *best = best_cfg;
     return TDP_OK;
 }
 

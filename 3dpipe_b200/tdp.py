@@ -152,6 +152,13 @@ class Context:
         self.check(lib().tdp_last_stats(self._h, C.byref(s)))
         return s.as_dict()
 
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        L = lib()
+        L.tdp_ctx_stream.argtypes = [C.c_void_p]
+        L.tdp_ctx_stream.restype = C.c_void_p
+        return L.tdp_ctx_stream(self._h) or 0
+
     def memory(self):
         a, b = C.c_size_t(), C.c_size_t()
         self.check(lib().tdp_ctx_memory(self._h, C.byref(a), C.byref(b)))
@@ -251,20 +258,25 @@ def candidates(box1, xf1, box2, xf2, self_join=False, knn=0, within=0.0):
     return off, ids[:n]
 
 
-def _join(self, tile1: Tile, tile2: Tile | None, query: str = "nn", knn: int = 1, within: float = 1000.0,
-          lods=None, hausdorff_level: int = 2, form: int = FORM_TUNED):
-    """tdbase join on resident tiles; returns (query_ids, result_ids, dist) sorted by (query, result)."""
-    L = lib()
+def _join_params(query, knn, within, lods, hausdorff_level, form) -> JoinParams:
     p = JoinParams()
-    L.tdp_join_default_params(C.byref(p))
-    p.query = QUERY_NN if query == "nn" else QUERY_WITHIN
+    lib().tdp_join_default_params(C.byref(p))
     if query not in ("nn", "within"):
         raise ValueError("query must be nn or within")
+    p.query = QUERY_NN if query == "nn" else QUERY_WITHIN
     p.knn, p.within_dist, p.hausdorff_level, p.form = knn, within, hausdorff_level, form
     if lods:
         p.n_lods = len(lods)
         for i, l in enumerate(lods):
             p.lods[i] = l
+    return p
+
+
+def _join(self, tile1: Tile, tile2: Tile | None, query: str = "nn", knn: int = 1, within: float = 1000.0,
+          lods=None, hausdorff_level: int = 2, form: int = FORM_TUNED):
+    """tdbase join on resident tiles; returns (query_ids, result_ids, dist) sorted by (query, result)."""
+    L = lib()
+    p = _join_params(query, knn, within, lods, hausdorff_level, form)
     r = C.c_void_p()
     self.check(L.tdp_join(self._h, tile1.handle, None if tile2 is None else tile2.handle, C.byref(p), C.byref(r)))
     try:
@@ -282,7 +294,51 @@ def _join(self, tile1: Tile, tile2: Tile | None, query: str = "nn", knn: int = 1
 Context.join = _join
 
 
-EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates"]
+EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates", "tdp_ctx_stream",
+             "tdp_refine_config_count", "tdp_refine_config_info", "tdp_set_refine_config", "tdp_get_refine_config",
+             "tdp_autotune"]
+
+
+def refine_configs():
+    """[(chunk_a, ctas_per_sm)] of the tuned refine kernel's configurations."""
+    L = lib()
+    out = []
+    for i in range(L.tdp_refine_config_count()):
+        a, c = C.c_int(), C.c_int()
+        L.tdp_refine_config_info(i, C.byref(a), C.byref(c))
+        out.append((a.value, c.value))
+    return out
+
+
+def _set_refine_config(self, cfg: int):
+    lib().tdp_set_refine_config.argtypes = [C.c_void_p, C.c_int]
+    self.check(lib().tdp_set_refine_config(self._h, int(cfg)))
+
+
+def _get_refine_config(self) -> int:
+    v = C.c_int()
+    lib().tdp_get_refine_config.argtypes = [C.c_void_p, C.c_void_p]
+    self.check(lib().tdp_get_refine_config(self._h, C.byref(v)))
+    return v.value
+
+
+def _autotune(self, tile1, tile2=None, query="within", knn=1, within=1000.0, lods=None, hausdorff_level=2):
+    """Time every tuned-refine configuration on this join and keep the fastest;
+    returns (best index, [refine ms per configuration])."""
+    L = lib()
+    p = _join_params(query, knn, within, lods, hausdorff_level, FORM_TUNED)
+    n = L.tdp_refine_config_count()
+    ms = (C.c_double * n)()
+    best = C.c_int()
+    L.tdp_autotune.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(JoinParams), C.c_void_p, C.c_void_p]
+    self.check(L.tdp_autotune(self._h, tile1.handle, None if tile2 is None else tile2.handle, C.byref(p), ms,
+                              C.byref(best)))
+    return best.value, list(ms)
+
+
+Context.set_refine_config = _set_refine_config
+Context.refine_config = _get_refine_config
+Context.autotune = _autotune
 
 
 def tile_candidates(ctx, tile1, tile2=None, knn=0, within=0.0):

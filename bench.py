@@ -7,10 +7,10 @@ nuclei of 1280 triangles, ~20k-triangle branching tube vessels, LODs
 RAW .dt format.  The reference publishes no numbers, so vs_baseline is null.
 
   value        triangle pairs refined per second by the tuned form, inputs
-               resident in HBM (tiles of ~37 GB: far larger than L2, so no
-               flush is needed between steps); device time of the whole join
-               call (CUDA events on the library's stream, host candidate
-               generation included), max over ranks
+               resident in HBM; the mean over K steps of the device time of the
+               whole join call (CUDA events on the library's stream, host work
+               between its launches included), L2 flushed between steps,
+               max over ranks
   plain        the same join through the plain form (one CTA per voxel pair,
                reference FP32 decision rules): the tuned/plain ratio
   e2e          the same metric through the public C ABI from pinned host tile
@@ -153,8 +153,13 @@ def cpu_reference(nb, vb, steps, warmup, sample_queries, target_s=15.0):
     if r is None:
         return None
     n_total = N_VESSELS * NUCLEI_PER_VESSEL
+    sample = min(sample_queries, n_total)
     sec = max(r[2][0], 1e-3)
-    sample = int(min(n_total, max(sample_queries, sample_queries * target_s / sec)))
+    # grow the prefix until one run lasts about target_s (or covers every query)
+    while sec < 0.5 * target_s and sample < n_total:
+        sample = int(min(n_total, sample * min(8.0, max(2.0, target_s / sec))))
+        _, _, st = ref_join(nb, vb, False, False, tau=TAU, threads=threads, max_queries=sample)
+        sec = max(st[0], 1e-3)
     vals, last = [], None
     for i in range(warmup + steps):
         _, _, st = ref_join(nb, vb, False, False, tau=TAU, threads=threads, max_queries=sample)
@@ -162,9 +167,11 @@ def cpu_reference(nb, vb, steps, warmup, sample_queries, target_s=15.0):
             vals.append(st[1] / st[0])
         last = st
     return {"value": statistics.median(vals), "unit": "tri-pairs/s", "cores": threads, "kind": "reference",
-            "sample": f"first {sample} of {n_total} query nuclei (all their candidate vessels, all LODs); "
-                      f"{last[0]:.1f} s per run, {last[1]:.3g} tri-pairs; join seconds for all nuclei "
-                      f"extrapolate linearly to {last[0] * n_total / sample:.0f} s",
+            "sample": (f"all {n_total} query nuclei (the whole join), " if sample >= n_total else
+                       f"first {sample} of {n_total} query nuclei (all their candidate vessels, all LODs), ")
+                      + f"median of {steps} run(s) of {last[0]:.1f} s, {last[1]:.3g} tri-pairs each"
+                      + ("" if sample >= n_total else
+                         f"; join seconds for all nuclei extrapolate linearly to {last[0] * n_total / sample:.0f} s"),
             "seconds_per_sample": last[0], "tri_pairs_per_sample": last[1]}
 
 
@@ -178,7 +185,9 @@ def run_reference_arm(a):
                                                                "(needs the reference sources at build time)"}))
         return 0
     nb, vb = make_tiles(0, 1)
-    cb = cpu_reference(nb, vb, a.steps, max(0, min(a.warmup, 1)), a.cpu_sample)
+    # each step a bounded sample, sized so the whole run stays within about 3 minutes
+    warm = max(0, min(a.warmup, 1))
+    cb = cpu_reference(nb, vb, a.steps, warm, a.cpu_sample, target_s=max(2.0, 150.0 / (a.steps + warm)))
     line = {"metric": METRIC, "value": cb["value"], "unit": "tri-pairs/s", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": cb["seconds_per_sample"] * 1e3, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -192,8 +201,8 @@ def run_reference_arm(a):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=1500, help="query nuclei in the CPU-baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
@@ -249,6 +258,10 @@ def main():
         t = time.time()
         T1, T2 = pkg.tdp.Tile(ctx, nb), pkg.tdp.Tile(ctx, vb)
         log(f"[rank {rank}] tiles resident in {time.time() - t:.1f}s, {ctx.memory()[0] / 1e9:.1f} GB on device")
+        # pick the tuned refine kernel's configuration on this join (untimed)
+        best_cfg, cfg_ms = ctx.autotune(T1, T2, query="within", within=TAU)
+        cfg_defs = pkg.tdp.refine_configs()
+        log(f"[rank {rank}] autotune: refine ms per configuration {[round(m, 3) for m in cfg_ms]} -> {best_cfg}")
         # the two forms must agree before anything is timed
         qa, ra, _ = ctx.join(T1, T2, query="within", within=TAU, form=pkg.FORM_PLAIN)
         qb, rb, _ = ctx.join(T1, T2, query="within", within=TAU, form=pkg.FORM_TUNED)
@@ -256,56 +269,74 @@ def main():
             raise SystemExit("plain and tuned forms returned different result sets")
         n_results = len(qb)
 
+        # Every join launches on the context's stream; the step events are
+        # recorded on that same stream.  Between steps a 256 MiB buffer (twice
+        # L2) is rewritten on the stream, outside the step's events, so no
+        # step starts with the previous step's lines in L2.
+        stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=torch.device("cuda", local))
+        flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
         def timed(form, steps, warmup):
             for _ in range(warmup):
                 ctx.join(T1, T2, query="within", within=TAU, form=form)
             barrier()
-            ms, st_last, launches = [], None, 0
-            for _ in range(steps):
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(steps)]
+            sts = []
+            for e0, e1 in evs:
+                with torch.cuda.stream(stream):
+                    flush_buf.fill_(len(sts) & 0xff)
+                    e0.record(stream)
                 ctx.join(T1, T2, query="within", within=TAU, form=form)
-                st = ctx.stats()
-                ms.append(st["total_ms"])
-                launches += st["kernel_launches"]
-                st_last = st
+                with torch.cuda.stream(stream):
+                    e1.record(stream)
+                sts.append(ctx.stats())
             barrier()
-            return ms, st_last, launches
+            ms = sum(e0.elapsed_time(e1) for e0, e1 in evs) / steps
+            agg = {k: sum(s[k] for s in sts) / steps for k in ("refine_ms", "full_evals", "tri_pairs")}
+            launches = sum(s["kernel_launches"] for s in sts)
+            return ms, sts[-1], agg, launches
 
         with ClockSampler(local) as clk:
-            ms_t, st_t, launches_t = timed(pkg.FORM_TUNED, a.steps, a.warmup)
+            ms_t, st_t, agg_t, launches_t = timed(pkg.FORM_TUNED, a.steps, a.warmup)
         clocks = clk.summary()
-        ms_p, st_p, _ = timed(pkg.FORM_PLAIN, max(2, a.steps // 2), 1)
+        ms_p, st_p, agg_p, _ = timed(pkg.FORM_PLAIN, max(3, a.steps // 4), 1)
 
-        step_ms = allmax(statistics.median(ms_t))
+        step_ms = allmax(ms_t)
         tri = allsum(st_t["tri_pairs"])
         value = tri / (step_ms / 1e3)
-        plain_ms = allmax(statistics.median(ms_p))
+        plain_ms = allmax(ms_p)
         plain_value = allsum(st_p["tri_pairs"]) / (plain_ms / 1e3)
-        refine_ms = st_t["refine_ms"]
+        refine_ms = agg_t["refine_ms"]
         launches_refine = max(1, st_t["refine_launches"])
-        flops = st_t["full_evals"] * F_TRI + st_t["tri_pairs"] * F_CULL
+        flops = agg_t["full_evals"] * F_TRI + agg_t["tri_pairs"] * F_CULL
         achieved = flops / (refine_ms / 1e3) / 1e12
 
-        # end to end through the C ABI from pinned host bytes
+        # end to end through the C ABI from pinned host bytes: tile upload
+        # (H2D + unpack), join, result read-back and tile release, between two
+        # events on the context's stream
         e2e_ms = []
         d2h = 0
         for i in range(a.e2e_steps + 1 if a.e2e_steps > 0 else 0):
             barrier()
-            t0 = time.perf_counter()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
             U1, U2 = pkg.tdp.Tile(ctx, nb), pkg.tdp.Tile(ctx, vb)
             q, r, d = ctx.join(U1, U2, query="within", within=TAU, form=pkg.FORM_TUNED)
             U1.free(); U2.free()
-            torch.cuda.synchronize()
-            dt = (time.perf_counter() - t0) * 1e3
+            e1.record(stream)
+            e1.synchronize()
             d2h = q.nbytes + r.nbytes + d.nbytes
             if i > 0:
-                e2e_ms.append(dt)
+                e2e_ms.append(e0.elapsed_time(e1))
         e2e_step = allmax(statistics.median(e2e_ms)) if e2e_ms else float("nan")
         e2e_value = tri / (e2e_step / 1e3) if e2e_ms else None
+        del flush_buf
 
     pinned.release()
     cpu = None
     if rank == 0 and not a.no_cpu:
-        cpu = cpu_reference(nb, vb, 1, 0, a.cpu_sample)
+        cpu = cpu_reference(nb, vb, 3, 0, a.cpu_sample, target_s=5.0)
     prof = ROOT / "profiles" / "traffic.json"
     traffic = None
     if prof.exists():
@@ -322,8 +353,10 @@ def main():
                        "n_vessels": N_VESSELS, "tau": TAU, "seed": SEED, "results": n_results,
                        "join_seconds": step_ms / 1e3, "tri_pairs_per_join": tri,
                        "refine_ms": refine_ms, "filter_ms": st_t["filter_ms"],
-                       "l2": "inputs larger than L2 (resident tiles ~37 GB)",
-                       "parallelism": f"{ws} GPU(s), query nuclei sharded by vessel block"},
+                       "l2": "L2 flushed between timed steps (256 MiB rewrite on the join stream, outside the step events)",
+                       "parallelism": f"{ws} GPU(s), query nuclei sharded by vessel block",
+                       "refine_config": {"chunk_a": cfg_defs[best_cfg][0], "ctas_per_sm": cfg_defs[best_cfg][1],
+                                         "autotune_refine_ms": [round(m, 4) for m in cfg_ms]}},
             "plain": {"value": plain_value, "unit": "tri-pairs/s", "ms_per_step": plain_ms,
                       "tuned_over_plain": value / plain_value if plain_value else None},
             "e2e": {"value": e2e_value, "unit": "tri-pairs/s", "ms_per_step": e2e_step,

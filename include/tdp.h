@@ -76,6 +76,23 @@ int tdp_last_stats(const tdp_ctx *ctx, tdp_stats *out);
 /* measured FP32 FMA throughput of the context's device in TFLOP/s (CUDA cores,
  * no tensor cores): the roofline ceiling of the refine kernels. */
 int tdp_fp32_peak(tdp_ctx *ctx, double *tflops);
+/* ---- tuned refine configurations --------------------------------------
+ * The tuned refine kernel exists in a few configurations: A-side triangles
+ * staged per warp and resident CTAs per SM.  All return identical results;
+ * they differ only in speed, which depends on the voxel sizes of the join.
+ * A context starts with configuration 0.  The reference has one fixed launch
+ * shape (one CTA of 512 threads per voxel pair,
+ * MeshDist_batch_gpu_op_shm_flat_stream, src/geometry/computing_gpu.cu:6540-6658)
+ * and no counterpart to these calls. */
+int tdp_refine_config_count(void);
+int tdp_refine_config_info(int cfg, int *chunk_a, int *ctas_per_sm);
+int tdp_set_refine_config(tdp_ctx *ctx, int cfg);
+int tdp_get_refine_config(const tdp_ctx *ctx, int *cfg);
+
+/* The context's CUDA stream (a cudaStream_t), on which every tdp call that
+ * takes this context launches its work: callers order their own work, or
+ * record timing events, against it.  NULL for a NULL context. */
+void *tdp_ctx_stream(const tdp_ctx *ctx);
 
 /* ---- tiles ------------------------------------------------------------------
  * Upload a RAW .dt tile (the bytes of the file, host memory, pinned or not)
@@ -137,6 +154,13 @@ int tdp_result_count(const tdp_result *r, long *n);
  * it was decided (the exact FP32 distance for pairs decided at the last LOD) */
 int tdp_result_copy(const tdp_result *r, int *query_ids, int *result_ids, float *dist);
 int tdp_result_free(tdp_result *r);
+
+/* Autotuner: runs the tuned join of `params` once per configuration untimed
+ * and once timed, keeps the configuration with the least refine time for the
+ * context and returns it in *best (may be NULL).  ms_per_config, if not NULL,
+ * receives tdp_refine_config_count() refine times in milliseconds. */
+int tdp_autotune(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, const tdp_join_params *params,
+                 double *ms_per_config, int *best);
 
 /* ---- refine seam ------------------------------------------------------------
  * Drop-in for the reference's batched refine (MeshDist_batch_gpu_op_shm_flat_stream):

@@ -157,3 +157,28 @@ def test_gpu_candidates_self_join(pkg, ctx, gpu_tiles, ref, args):
     hoff, hids = pkg.tdp.candidates(b1, x1, b1, x1, self_join=True, **args)
     np.testing.assert_array_equal(off, hoff)
     np.testing.assert_array_equal(ids, hids)
+
+
+def test_refine_configs_identical_and_autotune(pkg, ctx, gpu_tiles):
+    """Every tuned-refine configuration returns bit-identical joins; the
+    autotuner times them all and keeps a valid one for the context."""
+    T1, T2 = gpu_tiles(6, 12, 101)
+    cfgs = pkg.tdp.refine_configs()
+    assert len(cfgs) >= 2 and all(a % 8 == 0 and c >= 1 for a, c in cfgs)
+    keep = ctx.refine_config()
+    try:
+        for args in (dict(query="within", within=150.0), dict(query="nn", knn=3)):
+            outs = []
+            for c in range(len(cfgs)):
+                ctx.set_refine_config(c)
+                outs.append(ctx.join(T1, T2, form=pkg.FORM_TUNED, **args))
+            for o in outs[1:]:
+                for a, b in zip(outs[0], o):
+                    np.testing.assert_array_equal(a, b)
+        best, ms = ctx.autotune(T1, T2, query="within", within=150.0)
+        assert 0 <= best < len(cfgs) and ctx.refine_config() == best
+        assert len(ms) == len(cfgs) and all(m > 0 for m in ms)
+        with pytest.raises(pkg.TdpError):
+            ctx.set_refine_config(len(cfgs))
+    finally:
+        ctx.set_refine_config(keep)

@@ -146,3 +146,21 @@ def test_plain_and_tuned_agree(ctx):
     assert (np.abs(a[:, 0] - b[:, 0]) <= 2 * ERR_C * U * R).all()
     st = ctx.stats()
     assert st["full_evals"] <= st["tri_pairs"]
+
+
+def test_tuned_configs_bit_identical(ctx, pkg):
+    """The tuned kernel's configurations (A-chunk size, CTAs per SM) stage,
+    translate and cull the same pairs conservatively: outputs are bit-identical,
+    including voxels larger than every A chunk."""
+    rng = np.random.default_rng(33)
+    tri, hd, osz = make_batch(rng, 200, sizes=(1, 200))
+    keep = ctx.refine_config()
+    try:
+        outs = []
+        for c in range(len(pkg.tdp.refine_configs())):
+            ctx.set_refine_config(c)
+            outs.append(ctx.refine_batch(tri, hd, osz, form=1))
+        for o in outs[1:]:
+            np.testing.assert_array_equal(outs[0], o)
+    finally:
+        ctx.set_refine_config(keep)
