@@ -5,4 +5,5 @@ The package directory name starts with a digit, so import it with
 CUDA library libtdp.so (C ABI in include/tdp.h); this package only binds it.
 """
 from . import tdp  # noqa: F401
+from . import shard  # noqa: F401
 from .tdp import Context, TdpError, FORM_PLAIN, FORM_TUNED, QUERY_NN, QUERY_WITHIN  # noqa: F401
