@@ -135,6 +135,10 @@ int tdp_last_stats(const tdp_ctx* ctx, tdp_stats* o) {
     o->candidates_ms = s.candidates_ms;
     o->lod_ms = s.lod_ms;
     o->host_syncs = s.host_syncs;
+    o->exact_ms = s.exact_ms;
+    o->exact_items = s.exact_items;
+    o->exact_f64_items = s.exact_f64_items;
+    o->fp32_max_rel_err = s.fp32_max_rel_err;
     return TDP_OK;
 }
 

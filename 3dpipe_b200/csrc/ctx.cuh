@@ -30,6 +30,10 @@ struct LastStats {
     double candidates_ms = 0;        // host wall time of object candidate generation
     double lod_ms = 0;               // device time of the LOD loop
     long host_syncs = 0;             // host<->device synchronisations in the call
+    double exact_ms = 0;             // device time of the exact-distance stage
+    long exact_items = 0;            // LOD-100 voxel pairs it refined in FP32
+    long exact_f64_items = 0;        // of those, evaluated in FP64
+    double fp32_max_rel_err = 0;     // max |FP32 minimum - FP64 distance| / max(distance, 1)
 };
 
 }  // namespace tdp
@@ -43,7 +47,7 @@ struct tdp_ctx {
     cudaEvent_t lod_ev[16] = {};  // refine timing per LOD (tuned loop)
     std::string last_error;
     std::unordered_map<void*, size_t> allocs;
-    tdp::Buf scratch[64];
+    tdp::Buf scratch[96];  // slots: refine-batch 0-4, tile upload 12-13, join 20-48, candidates 50-59, result sort 60-63, exact distances 64-81
     unsigned* d_counter = nullptr;            // work counters (device)
     unsigned long long* d_stats = nullptr;    // device-side statistics
     tdp::LastStats stats;

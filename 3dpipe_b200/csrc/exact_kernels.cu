@@ -1,0 +1,412 @@
+// exact_kernels.cu -- exact (FP64) distances of the join's reported pairs.
+//
+// The reference reports result ids only (HiMesh_Wrapper::report_result,
+// src/spatial/himesh_wrapper.cpp:195-202); a pair decided before LOD 100 has
+// only a Hausdorff-widened range.  When tdp_join_params.exact_distances is set,
+// this stage gives every reported pair its LOD-100 distance in FP64:
+//   1. U, an upper bound of the pair's LOD-100 distance D: the smallest
+//      core-to-core distance over its voxel pairs (a core is a vertex of the
+//      LOD-100 surface), and, at Hausdorff level 2, also the pair's upper
+//      bound pmx when it was decided (d + h1 + h2 at a lower LOD bounds D);
+//      each widened by its FP32 error, max(perr, 1e-4 (value + 1));
+//      U is then tightened by refining one voxel pair per object pair in FP32
+//      (the one with the closest cores): its minimum d32 + err_bound(R) is a
+//      distance between two surface points, hence also >= D;
+//   2. every LOD-100 voxel pair whose box gap is <= U is a candidate (the
+//      voxel pair holding the closest points has gap <= D <= U);
+//   3. the tuned FP32 refine, its minimum preset to U plus the candidate's
+//      largest possible FP32 error, gives each candidate that has a triangle
+//      pair below that preset its minimum d32 (error e = err_bound(R)) and
+//      skips the rest after a few cluster tests; per object pair best32 =
+//      min d32 and E = max e;
+//   4. a candidate can hold the minimum only if d32 - E <= best32 + E (its
+//      true minimum is >= d32 - e, and D <= best32 + E): those are evaluated
+//      in FP64, skipping triangle pairs whose (inflated) bounding-sphere gap
+//      exceeds best32 + 2E;
+//   5. D = the smallest FP64 distance over the evaluated candidates.
+// Every filter is conservative, so D is the exact minimum over the stored
+// float coordinates up to the FP64 rounding of one triangle distance.
+#include <cub/device/device_scan.cuh>
+#include <float.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "exact_kernels.cuh"
+#include "refine.cuh"
+#include "tridist.cuh"
+
+namespace tdp {
+namespace {
+
+constexpr int kBlk = 256;
+
+// U of every reported pair: min core-to-core distance over its voxel pairs,
+// and pmx when it is a proven bound (pmx_valid); item1[p] = the voxel pair with
+// the closest cores (an empty item for pairs that are not reported)
+__global__ void __launch_bounds__(kBlk) k_exact_upper(JoinDev d, int pmx_valid, const uint32_t* __restrict__ vt1,
+                                                      const uint32_t* __restrict__ vt2, float* __restrict__ U,
+                                                      RefineItem* __restrict__ item1) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
+        if (d.pstat[p] != kReported) {
+            if (lane == 0) {
+                U[p] = FLT_MAX;
+                item1[p] = RefineItem{0, 0, 0, 0};
+            }
+            continue;
+        }
+        const int q = d.pq[p], t = d.pt[p];
+        const uint32_t a0 = d.ovox1[q], a1 = d.ovox1[q + 1], b0 = d.ovox2[t], b1 = d.ovox2[t + 1];
+        float m2 = FLT_MAX;
+        uint32_t ba = a0, bb = b0;
+        for (uint32_t b = b0 + lane; b < b1; b += 32) {
+            if (vt2[b + 1] == vt2[b]) continue;
+            const float4 cb = d.vox2[3 * (size_t)b + 2];
+            for (uint32_t a = a0; a < a1; ++a) {
+                if (vt1[a + 1] == vt1[a]) continue;
+                const float4 ca = d.vox1[3 * (size_t)a + 2];
+                const float dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;
+                const float v = dx * dx + dy * dy + dz * dz;
+                if (v < m2) { m2 = v; ba = a; bb = b; }
+            }
+        }
+        // warp argmin (ties to the lowest lane)
+        float best = m2;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
+        const unsigned who = __ballot_sync(0xffffffffu, m2 == best);
+        const int src = who ? __ffs(who) - 1 : 0;
+        ba = __shfl_sync(0xffffffffu, ba, src);
+        bb = __shfl_sync(0xffffffffu, bb, src);
+        if (lane == 0) {
+            float u = FLT_MAX;
+            if (best < FLT_MAX) {
+                const float core = sqrtf(best);
+                u = core + fmaxf(1e-4f * (core + 1.f), 8.f * kUnitRoundoff * core);
+                item1[p] = RefineItem{vt1[ba], vt1[ba + 1] - vt1[ba], vt2[bb], vt2[bb + 1] - vt2[bb]};
+            } else {
+                item1[p] = RefineItem{0, 0, 0, 0};
+            }
+            if (pmx_valid) {
+                const float mx = d.pmx[p];
+                u = fminf(u, mx + fmaxf(d.perr[p], 1e-4f * (mx + 1.f)));
+            }
+            U[p] = u;
+        }
+    }
+}
+
+// U = min(U, d32 + err) with the FP32 minimum of the closest-core voxel pair
+__global__ void k_exact_tighten(const float4* __restrict__ res1, int64_t P, float* __restrict__ U) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P; p += (int64_t)gridDim.x * blockDim.x) {
+        const float4 r = res1[p];
+        if (r.x < FLT_MAX) {
+            const float u = r.x + err_bound(r.w) + 1e-5f * r.x + 1e-6f;
+            U[p] = fminf(U[p], u);
+        }
+    }
+}
+
+// squared box gap of two voxels, as vox_dist2 computes it
+__device__ __forceinline__ float box_gap2(const float4* a, const float4* b) {
+    const float4 alo = a[0], ahi = a[1], blo = b[0], bhi = b[1];
+    const float gx = fmaxf(fmaxf(alo.x - bhi.x, blo.x - ahi.x), 0.f);
+    const float gy = fmaxf(fmaxf(alo.y - bhi.y, blo.y - ahi.y), 0.f);
+    const float gz = fmaxf(fmaxf(alo.z - bhi.z, blo.z - ahi.z), 0.f);
+    return gx * gx + gy * gy + gz * gz;
+}
+
+// count (WRITE = false) or write the candidate voxel pairs of every reported pair
+// The preset of a candidate is U plus the largest FP32 error its minimum can
+// carry: err_bound of a coordinate bound R <= gap + both voxel diagonals, as
+// every coordinate is taken relative to a vertex of the A voxel.
+template <bool WRITE>
+__global__ void __launch_bounds__(kBlk) k_exact_vp(JoinDev d, const float* __restrict__ Ub,
+                                                   const uint32_t* __restrict__ vt1,
+                                                   const uint32_t* __restrict__ vt2, int64_t* __restrict__ cnt,
+                                                   const int64_t* __restrict__ off, RefineItem* __restrict__ items,
+                                                   int* __restrict__ item_pair, float* __restrict__ preset) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
+        if (d.pstat[p] != kReported) {
+            if (!WRITE && lane == 0) cnt[p] = 0;
+            continue;
+        }
+        const int q = d.pq[p], t = d.pt[p];
+        const uint32_t a0 = d.ovox1[q], b0 = d.ovox2[t];
+        const uint32_t n1 = d.ovox1[q + 1] - a0, n2 = d.ovox2[t + 1] - b0;
+        const float U = Ub[p];
+        const float lim = U * (1.f + 1e-5f) + 1e-6f;
+        const float lim2 = lim * lim;
+        const uint64_t total = (uint64_t)n1 * n2;
+        int64_t pos = WRITE ? off[p] : 0, count = 0;
+        for (uint64_t base = 0; base < total; base += 32) {
+            const uint64_t k = base + lane;
+            bool keep = false;
+            uint32_t a = 0, b = 0;
+            if (k < total) {
+                a = a0 + (uint32_t)(k / n2);
+                b = b0 + (uint32_t)(k % n2);
+                keep = box_gap2(d.vox1 + 3 * (size_t)a, d.vox2 + 3 * (size_t)b) <= lim2 && vt1[a + 1] > vt1[a] &&
+                       vt2[b + 1] > vt2[b];
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (WRITE && keep) {
+                const int64_t w = pos + __popc(bal & ((1u << lane) - 1u));
+                items[w] = RefineItem{vt1[a], vt1[a + 1] - vt1[a], vt2[b], vt2[b + 1] - vt2[b]};
+                item_pair[w] = p;
+                const float4* va = d.vox1 + 3 * (size_t)a;
+                const float4* vb = d.vox2 + 3 * (size_t)b;
+                const float4 alo = va[0], ahi = va[1], blo = vb[0], bhi = vb[1];
+                const float da = (ahi.x - alo.x) + (ahi.y - alo.y) + (ahi.z - alo.z);
+                const float db = (bhi.x - blo.x) + (bhi.y - blo.y) + (bhi.z - blo.z);
+                const float R = (U + da + db) * 1.001f + 1.f;
+                preset[w] = U + 2.f * err_bound(R) + 1e-6f;
+            }
+            pos += __popc(bal);
+            count += __popc(bal);
+        }
+        if (!WRITE && lane == 0) cnt[p] = count;
+    }
+}
+
+// per object pair: best32 = min d32, emax = max error bound (non-negative
+// floats order like their bit patterns)
+__global__ void k_exact_best(const float4* __restrict__ res, const int* __restrict__ item_pair, int64_t E,
+                             unsigned* __restrict__ best32, unsigned* __restrict__ emax) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+        const float4 r = res[e];
+        if (!(r.x < FLT_MAX)) continue;  // no triangle pair below the preset
+        const int p = item_pair[e];
+        atomicMin(best32 + p, __float_as_uint(fmaxf(r.x, 0.f)));
+        atomicMax(emax + p, __float_as_uint(err_bound(r.w)));
+    }
+}
+
+// candidates that can still hold the minimum, compacted (order is irrelevant)
+__global__ void k_exact_select(const float4* __restrict__ res, const RefineItem* __restrict__ items,
+                               const int* __restrict__ item_pair, int64_t E, const unsigned* __restrict__ best32,
+                               const unsigned* __restrict__ emax, RefineItem* __restrict__ sel,
+                               int* __restrict__ sel_pair, float* __restrict__ sel_thr, unsigned* __restrict__ n_sel) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+        const float x = res[e].x;
+        if (!(x < FLT_MAX)) continue;
+        const int p = item_pair[e];
+        const float b = __uint_as_float(best32[p]), m = __uint_as_float(emax[p]);
+        if (x - m <= b + m) {
+            const unsigned w = atomicAdd(n_sel, 1u);
+            sel[w] = items[e];
+            sel_pair[w] = p;
+            sel_thr[w] = b + 2.f * m;
+        }
+    }
+}
+
+__device__ __forceinline__ void sphere_rel(const float4* t, float4 o, float& cx, float& cy, float& cz, float& r) {
+    const float4 v0 = t[0], v1 = t[1], v2 = t[2];
+    const float x0 = v0.x - o.x, y0 = v0.y - o.y, z0 = v0.z - o.z;
+    const float x1 = v1.x - o.x, y1 = v1.y - o.y, z1 = v1.z - o.z;
+    const float x2 = v2.x - o.x, y2 = v2.y - o.y, z2 = v2.z - o.z;
+    cx = (x0 + x1 + x2) * (1.f / 3.f);
+    cy = (y0 + y1 + y2) * (1.f / 3.f);
+    cz = (z0 + z1 + z2) * (1.f / 3.f);
+    float r2 = (x0 - cx) * (x0 - cx) + (y0 - cy) * (y0 - cy) + (z0 - cz) * (z0 - cz);
+    r2 = fmaxf(r2, (x1 - cx) * (x1 - cx) + (y1 - cy) * (y1 - cy) + (z1 - cz) * (z1 - cz));
+    r2 = fmaxf(r2, (x2 - cx) * (x2 - cx) + (y2 - cy) * (y2 - cy) + (z2 - cz) * (z2 - cz));
+    // inflated so FP32 rounding never drops a pair that could be the minimum
+    r = sqrtf(r2) * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f;
+}
+
+__device__ __forceinline__ void pre64(const float4* t, double ox, double oy, double oz, PreTri<double>& P) {
+    const float4 a = t[0], b = t[1], c = t[2];
+    pretri(P, v3<double>(a.x - ox, a.y - oy, a.z - oz), v3<double>(b.x - ox, b.y - oy, b.z - oz),
+           v3<double>(c.x - ox, c.y - oy, c.z - oz));
+}
+
+constexpr int kExWarps = 4;
+
+// FP64 minimum over the triangle pairs of a selected voxel pair whose FP32
+// bounding-sphere gap is <= the item's threshold; one warp per item, lane j
+// owns B triangle j of the current chunk of 32, A spheres staged per chunk.
+__global__ void __launch_bounds__(kExWarps * 32) k_exact_f64(const float4* __restrict__ triA,
+                                                             const float4* __restrict__ triB,
+                                                             const RefineItem* __restrict__ sel,
+                                                             const int* __restrict__ sel_pair,
+                                                             const float* __restrict__ sel_thr,
+                                                             const unsigned* __restrict__ n_sel,
+                                                             unsigned long long* __restrict__ pexact_bits) {
+    __shared__ float4 sphA[kExWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned n = *n_sel;
+    for (unsigned it = blockIdx.x * kExWarps + w; it < n; it += gridDim.x * kExWarps) {
+        const RefineItem r = sel[it];
+        const float thr = sel_thr[it];
+        const float4 o4 = triA[(size_t)r.a_off * kTriF4];
+        const double ox = o4.x, oy = o4.y, oz = o4.z;
+        double best = 1e300;
+        for (uint32_t b0 = 0; b0 < r.b_cnt; b0 += 32) {
+            const bool bv = b0 + lane < r.b_cnt;
+            const float4* tb = triB + ((size_t)r.b_off + b0 + lane) * kTriF4;
+            float bx = 0.f, by = 0.f, bz = 0.f, br = 0.f;
+            if (bv) sphere_rel(tb, o4, bx, by, bz, br);
+            for (uint32_t a0 = 0; a0 < r.a_cnt; a0 += 32) {
+                const int ca = (int)min(32u, r.a_cnt - a0);
+                __syncwarp();
+                if (lane < ca) {
+                    float cx, cy, cz, rr;
+                    sphere_rel(triA + ((size_t)r.a_off + a0 + lane) * kTriF4, o4, cx, cy, cz, rr);
+                    sphA[w][lane] = make_float4(cx, cy, cz, rr);
+                }
+                __syncwarp();
+                for (int i = 0; i < ca; ++i) {
+                    const float4 s = sphA[w][i];
+                    const float dx = s.x - bx, dy = s.y - by, dz = s.z - bz;
+                    const float reach = s.w + br + thr;
+                    if (bv && dx * dx + dy * dy + dz * dz <= reach * reach) {
+                        PreTri<double> A, B;
+                        pre64(triA + ((size_t)r.a_off + a0 + i) * kTriF4, ox, oy, oz, A);
+                        pre64(tb, ox, oy, oz, B);
+                        const double d2 = tri_dist2(A, B);
+                        best = d2 < best ? d2 : best;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double v = __shfl_xor_sync(0xffffffffu, best, o);
+            best = v < best ? v : best;
+        }
+        // non-negative doubles order like their bit patterns
+        if (lane == 0 && best < 1e300)
+            atomicMin(pexact_bits + sel_pair[it], (unsigned long long)__double_as_longlong(sqrt(best)));
+    }
+}
+
+// largest |best32 - D| / max(D, 1) over the reported pairs: the FP32 refine's
+// error against FP64 on this join
+__global__ void k_exact_err(JoinDev d, const unsigned* __restrict__ best32, const double* __restrict__ pexact,
+                            unsigned* __restrict__ err_bits) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.P; p += gridDim.x * blockDim.x) {
+        if (d.pstat[p] != kReported) continue;
+        const double D = pexact[p];
+        if (!(D < 1e300)) continue;
+        const double b = (double)__uint_as_float(best32[p]);
+        const float rel = (float)(fabs(b - D) / fmax(D, 1.0));
+        atomicMax(err_bits, __float_as_uint(rel));
+    }
+}
+
+int grid(int64_t n, int per_block, int cap) {
+    int64_t g = (n + per_block - 1) / per_block;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(g, cap));
+}
+
+}  // namespace
+
+int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const tdp_tile* t2, bool pmx_valid,
+                    double* pexact, ExactInfo& info) {
+    cudaStream_t s = ctx->stream;
+    info = ExactInfo{};
+    int rc;
+#define CU(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } while (0)
+#define ENS(slot, bytes) do { if ((rc = ensure(ctx, ctx->scratch[slot], (bytes)))) return rc; } while (0)
+    const size_t Pz = (size_t)std::max<int64_t>(d.P, 1);
+    // every byte 0x7f: the double 1.38e306, above any distance, so atomicMin
+    // over the bit patterns of non-negative doubles takes the first real value
+    CU(cudaMemsetAsync(pexact, 0x7f, Pz * 8, s));
+    if (d.P <= 0) return TDP_OK;
+    ENS(64, (Pz + 1) * 8);             // counts
+    ENS(65, (Pz + 1) * 8);             // offsets
+    ENS(78, Pz * 4);                   // U per pair
+    ENS(79, Pz * sizeof(RefineItem));  // phase-1 item per pair
+    ENS(80, Pz * sizeof(float4));      // phase-1 FP32 results
+    ENS(75, 64);                       // counters
+    int64_t* cnt = (int64_t*)ctx->scratch[64].p;
+    int64_t* off = (int64_t*)ctx->scratch[65].p;
+    float* Ub = (float*)ctx->scratch[78].p;
+    RefineItem* item1 = (RefineItem*)ctx->scratch[79].p;
+    float4* res1 = (float4*)ctx->scratch[80].p;
+    unsigned* ctr = (unsigned*)ctx->scratch[75].p;
+    const uint32_t* vt1 = t1->vtri[kNumLods - 1];
+    const uint32_t* vt2 = t2->vtri[kNumLods - 1];
+    const int pg = grid(d.P, kBlk / 32, ctx->num_sms * 32);
+    CU(cudaMemsetAsync(cnt + d.P, 0, 8, s));
+    CU(cudaMemsetAsync(ctr, 0, 64, s));
+    k_exact_upper<<<pg, kBlk, 0, s>>>(d, pmx_valid ? 1 : 0, vt1, vt2, Ub, item1);
+    CU(cudaGetLastError());
+    // phase 1: one FP32 voxel pair per object pair tightens U
+    CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], item1, (int)d.P, res1, ctr, nullptr,
+                           ctx->num_sms, ctx->tuned_cfg, s));
+    k_exact_tighten<<<grid(d.P, 256, ctx->num_sms * 8), 256, 0, s>>>(res1, d.P, Ub);
+    CU(cudaGetLastError());
+    k_exact_vp<false><<<pg, kBlk, 0, s>>>(d, Ub, vt1, vt2, cnt, nullptr, nullptr, nullptr, nullptr);
+    CU(cudaGetLastError());
+    size_t tb = 0;
+    CU(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, (int)d.P + 1, s));
+    ENS(66, tb + 16);
+    CU(cub::DeviceScan::ExclusiveSum(ctx->scratch[66].p, tb, cnt, off, (int)d.P + 1, s));
+    int64_t E = 0;
+    CU(cudaMemcpyAsync(&E, off + d.P, 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    info.launches += 6;
+    info.items = (long)E;
+    if (E >= (1LL << 31)) return fail(ctx, TDP_ERR_ARG, "too many voxel pairs for the exact-distance stage");
+    const size_t Ez = (size_t)std::max<int64_t>(E, 1);
+    ENS(67, Ez * sizeof(RefineItem));  // items
+    ENS(68, Ez * 4);                   // item -> pair
+    ENS(69, Ez * sizeof(float4));      // FP32 results
+    ENS(70, Pz * 4);                   // best32
+    ENS(71, Pz * 4);                   // emax
+    ENS(72, Ez * sizeof(RefineItem));  // selected items
+    ENS(73, Ez * 4);                   // selected -> pair
+    ENS(74, Ez * 4);                   // selected thresholds
+    ENS(81, Ez * 4);                   // presets
+    RefineItem* items = (RefineItem*)ctx->scratch[67].p;
+    int* item_pair = (int*)ctx->scratch[68].p;
+    float4* res = (float4*)ctx->scratch[69].p;
+    unsigned* best32 = (unsigned*)ctx->scratch[70].p;
+    unsigned* emax = (unsigned*)ctx->scratch[71].p;
+    RefineItem* sel = (RefineItem*)ctx->scratch[72].p;
+    int* sel_pair = (int*)ctx->scratch[73].p;
+    float* sel_thr = (float*)ctx->scratch[74].p;
+    float* preset = (float*)ctx->scratch[81].p;
+    ctr = (unsigned*)ctx->scratch[75].p;
+    k_exact_vp<true><<<pg, kBlk, 0, s>>>(d, Ub, vt1, vt2, nullptr, off, items, item_pair, preset);
+    CU(cudaGetLastError());
+    CU(cudaMemsetAsync(best32, 0x7f, Pz * 4, s));  // 0x7f7f7f7f = 3.4e38, above any distance
+    CU(cudaMemsetAsync(emax, 0, Pz * 4, s));
+    CU(cudaMemsetAsync(ctr, 0, 64, s));
+    if (E > 0) {
+        CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], items, (int)E, res, ctr, nullptr,
+                               ctx->num_sms, ctx->tuned_cfg, s, nullptr, preset));
+        const int eg = grid(E, 256, ctx->num_sms * 16);
+        k_exact_best<<<eg, 256, 0, s>>>(res, item_pair, E, best32, emax);
+        CU(cudaGetLastError());
+        k_exact_select<<<eg, 256, 0, s>>>(res, items, item_pair, E, best32, emax, sel, sel_pair, sel_thr, ctr + 4);
+        CU(cudaGetLastError());
+        k_exact_f64<<<ctx->num_sms * 8, kExWarps * 32, 0, s>>>(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], sel,
+                                                              sel_pair, sel_thr, ctr + 4,
+                                                              reinterpret_cast<unsigned long long*>(pexact));
+        CU(cudaGetLastError());
+        k_exact_err<<<grid(d.P, 256, ctx->num_sms * 8), 256, 0, s>>>(d, best32, pexact, ctr + 8);
+        CU(cudaGetLastError());
+        info.launches += 6;
+        unsigned ns[8] = {0};
+        CU(cudaMemcpyAsync(ns, ctr + 4, 32, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        info.f64_items = ns[0];
+        float e32;
+        std::memcpy(&e32, &ns[4], 4);
+        info.max_rel_err32 = e32;
+    }
+#undef ENS
+#undef CU
+    return TDP_OK;
+}
+
+}  // namespace tdp

@@ -1,0 +1,26 @@
+// exact_kernels.cuh -- FP64 LOD-100 distances of the reported object pairs.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ctx.cuh"
+#include "join_kernels.cuh"
+#include "storage/dev_tile.h"
+
+namespace tdp {
+
+struct ExactInfo {
+    long items = 0;      // LOD-100 voxel pairs refined in FP32 (box gap within the pair's upper bound)
+    long f64_items = 0;  // of those, evaluated in FP64 (FP32 minimum within the error band of the best)
+    int launches = 0;
+    double max_rel_err32 = 0;  // max |FP32 object minimum - FP64 distance| / max(distance, 1)
+};
+
+// For every object pair with pstat == kReported: the exact minimum triangle
+// distance at LOD 100, in double, written to pexact[p] (other pairs, and a
+// reported pair without any LOD-100 triangles: values >= 1e300).
+// pmx_valid: the pairs' upper bounds pmx bound the LOD-100 distance (true at
+// Hausdorff level 2; levels 0 and 1 widen by nothing or by proxy-Hausdorff).
+int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const tdp_tile* t2, bool pmx_valid,
+                    double* pexact, ExactInfo& info);
+
+}  // namespace tdp

@@ -404,31 +404,33 @@ __global__ void k_count_status(JoinDev d, unsigned* __restrict__ c) {
 
 // Result keys: query * n2 + result id for reported pairs, `none` (= n1 * n2)
 // for the rest, so one radix sort over every pair puts the reported ones
-// first, ordered by (query, result id).
+// first, ordered by (query, result id); the payload is the pair index.
 __global__ void k_collect_keys(JoinDev d, long long n2, unsigned long long none, unsigned long long* __restrict__ keys,
-                               float* __restrict__ vals, unsigned* __restrict__ counter) {
+                               int* __restrict__ vals, unsigned* __restrict__ counter) {
     const int lane = threadIdx.x & 31;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < d.P; base += (int64_t)gridDim.x * blockDim.x) {
         const int64_t p = base + threadIdx.x;
         const bool rep = p < d.P && d.pstat[p] == kReported;
         if (p < d.P) {
             keys[p] = rep ? (unsigned long long)d.pq[p] * (unsigned long long)n2 + (unsigned)d.pt[p] : none;
-            vals[p] = d.pmx[p];
+            vals[p] = (int)p;
         }
         const unsigned m = __ballot_sync(0xffffffffu, rep);
         if (lane == 0 && m) atomicAdd(counter, (unsigned)__popc(m));
     }
 }
 
-__global__ void k_split(const unsigned long long* __restrict__ keys, const float* __restrict__ vals, int64_t n,
-                        long long n2, unsigned long long none, int* __restrict__ oq, int* __restrict__ ot,
-                        float* __restrict__ od) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+__global__ void k_split(JoinDev d, const unsigned long long* __restrict__ keys, const int* __restrict__ vals,
+                        long long n2, unsigned long long none, const double* __restrict__ pexact,
+                        int* __restrict__ oq, int* __restrict__ ot, float* __restrict__ od, double* __restrict__ od64) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.P; i += (int64_t)gridDim.x * blockDim.x) {
         const unsigned long long k = keys[i];
         if (k == none) break;  // sorted: every later key is `none` too
+        const int p = vals[i];
         oq[i] = (int)(k / (unsigned long long)n2);
         ot[i] = (int)(k % (unsigned long long)n2);
-        od[i] = vals[i];
+        od[i] = d.pmx[p];
+        if (od64) od64[i] = pexact ? pexact[p] : (double)d.pmx[p];
     }
 }
 
@@ -510,22 +512,23 @@ cudaError_t collect_sort_bytes(int64_t P, long long n1, long long n2, size_t& by
     bytes = 0;
     if (P <= 0) return cudaSuccess;
     cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr);
-    cub::DoubleBuffer<float> v(nullptr, nullptr);
+    cub::DoubleBuffer<int> v(nullptr, nullptr);
     return cub::DeviceRadixSort::SortPairs(nullptr, bytes, k, v, (int)P, 0,
                                            key_bits((unsigned long long)n1 * (unsigned long long)n2));
 }
-cudaError_t launch_collect(const JoinDev& d, long long n2, unsigned long long* keys[2], float* vals[2], void* temp,
-                           size_t temp_bytes, unsigned* counter, int* oq, int* ot, float* od, cudaStream_t s) {
+cudaError_t launch_collect(const JoinDev& d, long long n2, unsigned long long* keys[2], int* vals[2], void* temp,
+                           size_t temp_bytes, unsigned* counter, const double* pexact, int* oq, int* ot, float* od,
+                           double* od64, cudaStream_t s) {
     if (d.P <= 0) return cudaSuccess;
     const unsigned long long none = (unsigned long long)d.N1 * (unsigned long long)n2;
     k_collect_keys<<<grid_for(d.P, 256), 256, 0, s>>>(d, n2, none, keys[0], vals[0], counter);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     cub::DoubleBuffer<unsigned long long> k(keys[0], keys[1]);
-    cub::DoubleBuffer<float> v(vals[0], vals[1]);
+    cub::DoubleBuffer<int> v(vals[0], vals[1]);
     e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, k, v, (int)d.P, 0, key_bits(none), s);
     if (e != cudaSuccess) return e;
-    k_split<<<grid_for(d.P, 256), 256, 0, s>>>(k.Current(), v.Current(), d.P, n2, none, oq, ot, od);
+    k_split<<<grid_for(d.P, 256), 256, 0, s>>>(d, k.Current(), v.Current(), n2, none, pexact, oq, ot, od, od64);
     return cudaGetLastError();
 }
 

@@ -73,12 +73,15 @@ cudaError_t launch_recheck_finish(const JoinDev& d, const double* res, const int
                                   const unsigned* W_dev = nullptr);
 cudaError_t launch_count_status(const JoinDev& d, unsigned* counters, cudaStream_t s);
 // Reported pairs as (query, result id, distance) rows sorted by (query,
-// result id) on the device: the first *counter rows of out_q/out_t/out_d.
-// keys[0..1] / vals[0..1] are P-element double buffers for the radix sort,
-// temp its workspace of collect_sort_bytes() bytes; n2 is the tile-2 object count.
+// result id) on the device: the first *counter rows of out_q/out_t/out_d
+// (out_d = the pair's upper bound pmx; out_d64, if not NULL, = pexact when
+// given, else pmx widened).  keys[0..1] / vals[0..1] are P-element double
+// buffers for the radix sort, temp its workspace of collect_sort_bytes()
+// bytes; n2 is the tile-2 object count.
 cudaError_t collect_sort_bytes(int64_t P, long long n1, long long n2, size_t& bytes);
-cudaError_t launch_collect(const JoinDev& d, long long n2, unsigned long long* keys[2], float* vals[2], void* temp,
-                           size_t temp_bytes, unsigned* counter, int* out_q, int* out_t, float* out_d, cudaStream_t s);
+cudaError_t launch_collect(const JoinDev& d, long long n2, unsigned long long* keys[2], int* vals[2], void* temp,
+                           size_t temp_bytes, unsigned* counter, const double* pexact, int* out_q, int* out_t,
+                           float* out_d, double* out_d64, cudaStream_t s);
 // exclusive scan of n int64 counts into out[0..n] (out[n] = total)
 cudaError_t scan_counts(const int64_t* cnt, int64_t* out, int n, void* temp, size_t& temp_bytes, cudaStream_t s);
 

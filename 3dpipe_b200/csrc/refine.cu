@@ -270,6 +270,20 @@ __device__ __forceinline__ void build_clusters(const float4* sph, const float4* 
     }
 }
 
+// bounding sphere of a triangle record relative to o, inflated like
+// tri_sphere (same centre and radius formula, without the PreTri work)
+__device__ __forceinline__ float4 quick_sphere(const float4* __restrict__ t, float4 o) {
+    const float4 t0 = t[0], t1 = t[1], t2 = t[2];
+    const float x0 = t0.x - o.x, y0 = t0.y - o.y, z0 = t0.z - o.z;
+    const float x1 = t1.x - o.x, y1 = t1.y - o.y, z1 = t1.z - o.z;
+    const float x2 = t2.x - o.x, y2 = t2.y - o.y, z2 = t2.z - o.z;
+    const float cx = (x0 + x1 + x2) * (1.f / 3.f), cy = (y0 + y1 + y2) * (1.f / 3.f), cz = (z0 + z1 + z2) * (1.f / 3.f);
+    float r2 = (x0 - cx) * (x0 - cx) + (y0 - cy) * (y0 - cy) + (z0 - cz) * (z0 - cz);
+    r2 = fmaxf(r2, (x1 - cx) * (x1 - cx) + (y1 - cy) * (y1 - cy) + (z1 - cz) * (z1 - cz));
+    r2 = fmaxf(r2, (x2 - cx) * (x2 - cx) + (y2 - cy) * (y2 - cy) + (z2 - cz) * (z2 - cz));
+    return make_float4(cx, cy, cz, sqrtf(r2) * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f);
+}
+
 // the three minima are >= 0, so their bit patterns order like unsigned ints
 __device__ __forceinline__ float warp_min_nonneg(float v) {
     return __uint_as_float(__reduce_min_sync(0xffffffffu, __float_as_uint(v)));
@@ -284,7 +298,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
                                                                      int n_items_host, const unsigned* n_items_dev,
                                                                      float4* __restrict__ out,
                                                                      unsigned* __restrict__ work_counter,
-                                                                     unsigned long long* __restrict__ n_full) {
+                                                                     unsigned long long* __restrict__ n_full,
+                                                                     const float* __restrict__ init_bd) {
     extern __shared__ __align__(16) float smem[];
     // the item count comes from device memory when the producer ran on the GPU
     const int n_items = n_items_dev ? (int)*n_items_dev : n_items_host;
@@ -327,6 +342,48 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
             u = make_float3(ux * inv, uy * inv, uz * inv);
         }
         float bd = FLT_MAX, bl = FLT_MAX, bh = FLT_MAX, rmax = 0.f;
+        // with init_bd (the exact-distance stage) only the minimum distance
+        // matters: it starts at the item's bound, and the two Hausdorff minima
+        // are parked at -FLT_MAX so they never widen a threshold
+        float b_init = FLT_MAX;
+        if (init_bd) {
+            b_init = init_bd[it];
+            bd = b_init;
+            bl = -FLT_MAX;
+            bh = -FLT_MAX;
+            // item-level reject before any PreTri work: bounding spheres of the
+            // A triangles (clustered as below) against each lane's B triangle;
+            // if no pair of spheres is closer than the preset, no triangle pair
+            // is, and the item has nothing below it
+            bool need = false;
+            for (uint32_t a0 = 0; a0 < w.a_cnt && !__any_sync(0xffffffffu, need); a0 += kCA) {
+                const int ca = min((uint32_t)kCA, w.a_cnt - a0);
+                const int ncl = (ca + kCl - 1) / kCl;
+                __syncwarp();
+                for (int k = lane; k < ca; k += 32) {
+                    sphA[k] = quick_sphere(triA + ((size_t)w.a_off + a0 + k) * kTriF4, o4);
+                    auxA[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                __syncwarp();
+                build_clusters<CA>(sphA, auxA, ca, clS, clA, lane);
+                __syncwarp();
+                for (uint32_t b0 = 0; b0 < w.b_cnt && !need; b0 += kCB) {
+                    if (b0 + lane >= w.b_cnt) break;
+                    const float4 sb = quick_sphere(triB + ((size_t)w.b_off + b0 + lane) * kTriF4, o4);
+                    for (int c = 0; c < ncl; ++c) {
+                        const float4 cs = clS[c];
+                        const float dx = cs.x - sb.x, dy = cs.y - sb.y, dz = cs.z - sb.z;
+                        const float reach = cs.w + sb.w + bd;
+                        if (dx * dx + dy * dy + dz * dz < reach * reach) { need = true; break; }
+                    }
+                }
+            }
+            if (!__any_sync(0xffffffffu, need)) {
+                if (lane == 0) out[it] = make_float4(FLT_MAX, -FLT_MAX, -FLT_MAX, 0.f);
+                it = __shfl_sync(0xffffffffu, next, 0);
+                continue;
+            }
+        }
         for (uint32_t a0 = 0; a0 < w.a_cnt; a0 += kCA) {
             const int ca = min((uint32_t)kCA, w.a_cnt - a0);
             const int ncl = (ca + kCl - 1) / kCl;
@@ -349,6 +406,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
                 // seed: the nearest cluster by its bound, then its nearest member;
                 // the seeds are queued and drained before anything is culled
                 int seed = -1;
+                float seed_lb = FLT_MAX;
                 if (bval) {
                     float best = FLT_MAX;
                     int bc = 0;
@@ -367,9 +425,15 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
                         if (lb < best) { best = lb; seed = i; }
                     }
                     if (seed < 0) seed = bc * kCl;
+                    seed_lb = best;
                 }
-                int qn = __popc(__ballot_sync(0xffffffffu, bval));
-                if (bval) queue[lane] = (unsigned short)((seed << 8) | lane);
+                // a seed whose bound cannot beat a preset minimum is not queued;
+                // the cull below then tests that pair like any other
+                const bool sq = bval && (init_bd == nullptr || seed_lb < bd);
+                if (!sq) seed = -1;
+                const unsigned sqm = __ballot_sync(0xffffffffu, sq);
+                int qn = __popc(sqm);
+                if (sq) queue[__popc(sqm & lt_mask)] = (unsigned short)((seed << 8) | lane);
                 bool flush = true;
                 // cull into the queue, drain 32 pairs at a time; the one evaluation
                 // site below keeps the kernel's code small
@@ -436,6 +500,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+        if (init_bd && !(bd < b_init)) bd = FLT_MAX;  // nothing below the preset bound
         if (lane == 0) out[it] = make_float4(bd, bl, bh, rmax);
         it = __shfl_sync(0xffffffffu, next, 0);
     }
@@ -473,7 +538,7 @@ TunedConfig tuned_config(int cfg) {
 template <int CA, int MINB>
 static cudaError_t launch_tuned_cfg(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                     float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
-                                    cudaStream_t s, const unsigned* n_items_dev) {
+                                    cudaStream_t s, const unsigned* n_items_dev, const float* init_bd) {
     static bool attr_set[64] = {};  // per device: the attribute belongs to the device's context
     const size_t smem = (size_t)kTunedWarps * TunedLayout<CA>::kWarpFloats * sizeof(float);
     auto kern = refine_tuned_kernel<kTunedWarps, CA, MINB>;
@@ -490,18 +555,19 @@ static cudaError_t launch_tuned_cfg(const float4* triA, const float4* triB, cons
     long need = ((long)n_items + kTunedWarps - 1) / kTunedWarps;
     int grid = (int)(want < need ? want : need);
     if (grid < 1) grid = 1;
-    kern<<<grid, kTunedWarps * 32, smem, s>>>(triA, triB, items, n_items, n_items_dev, out, work_counter, n_full);
+    kern<<<grid, kTunedWarps * 32, smem, s>>>(triA, triB, items, n_items, n_items_dev, out, work_counter, n_full,
+                                              init_bd);
     return cudaGetLastError();
 }
 
 cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                 float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
-                                int cfg, cudaStream_t s, const unsigned* n_items_dev) {
+                                int cfg, cudaStream_t s, const unsigned* n_items_dev, const float* init_bd) {
     if (n_items <= 0) return cudaSuccess;
     switch (cfg) {
-        case 1: return launch_tuned_cfg<48, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev);
-        case 2: return launch_tuned_cfg<32, 4>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev);
-        default: return launch_tuned_cfg<64, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev);
+        case 1: return launch_tuned_cfg<48, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 2: return launch_tuned_cfg<32, 4>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        default: return launch_tuned_cfg<64, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
     }
 }
 

@@ -18,7 +18,11 @@ struct TunedConfig {
 TunedConfig tuned_config(int cfg);
 cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                 float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
-                                int cfg, cudaStream_t s, const unsigned* n_items_dev = nullptr);
+                                int cfg, cudaStream_t s, const unsigned* n_items_dev = nullptr,
+                                const float* init_bd = nullptr);
+// init_bd (optional, per item): start the minimum distance at this bound and
+// report x = FLT_MAX when no triangle pair lies below it; y and z (the
+// Hausdorff minima) are then meaningless.  Used by the exact-distance stage.
 // exact FP64 minimum distance per item (recheck of undecided object pairs)
 // n_items is an upper bound when n_items_dev (the exact count, in device memory) is given
 cudaError_t launch_refine_f64(const float4* triA, const float4* triB, const RefineItem* items, int n_items,

@@ -27,6 +27,7 @@
 #include "../../csrc/ctx.cuh"
 #include "../../csrc/join_kernels.cuh"
 #include "../../csrc/cand_kernels.cuh"
+#include "../../csrc/exact_kernels.cuh"
 #include "../../csrc/refine.cuh"
 #include "index/candidates.h"
 #include "storage/dev_tile.h"
@@ -35,6 +36,7 @@
 struct tdp_result {
     std::vector<int> q, t;
     std::vector<float> d;
+    std::vector<double> d64;  // exact LOD-100 distances (params.exact_distances)
 };
 
 namespace tdp {
@@ -46,6 +48,7 @@ enum Slot {
     kVpa, kVpb, kVpair, kVmn, kVmx, kVerr, kValive, kVupd, kItems, kItemVp, kRes, kOutQ, kOutT, kOutD,
     kVexact, kPexact, kRes64,
     kKeyA = 60, kKeyB, kValA, kValB,  // result sort (50-59 hold the candidate buffers)
+    kPexOut = 76, kOutD64,            // exact distances (64-75 and 78-81 are the exact stage's own)
 };
 
 template <typename T>
@@ -67,6 +70,7 @@ void tdp_join_default_params(tdp_join_params* p) {
     p->n_lods = 0;
     p->hausdorff_level = 2;
     p->form = TDP_FORM_TUNED;
+    p->exact_distances = 0;
 }
 
 int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_join_params* prm, tdp_result** out) {
@@ -278,7 +282,22 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         }
     }
 
-    // ---- 4. results ----
+    // ---- 4. exact LOD-100 distances of the reported pairs (optional) ----
+    const bool exact = prm->exact_distances != 0;
+    double* pex = nullptr;
+    ExactInfo xi;
+    if (exact) {
+        ENS(kPexOut, Pz * 8);
+        ENS(kOutD64, Pz * 8);
+        pex = buf<double>(ctx, kPexOut);
+        CU(cudaEventRecord(ctx->ev[6], s));
+        if ((rc = exact_distances(ctx, d, t1, t2, prm->hausdorff_level == 2, pex, xi))) return rc;
+        CU(cudaEventRecord(ctx->ev[7], s));
+        launches += xi.launches;
+        syncs += 2;
+    }
+
+    // ---- 5. results ----
     CU(cudaMemsetAsync(cnt_collect, 0, 4, s));
     {
         size_t sort_bytes = 0;
@@ -286,9 +305,10 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         ENS(kKeyA, Pz * 8); ENS(kKeyB, Pz * 8); ENS(kValA, Pz * 4); ENS(kValB, Pz * 4);
         ENS(kScanTmp, sort_bytes + 16);
         unsigned long long* keys[2] = {buf<unsigned long long>(ctx, kKeyA), buf<unsigned long long>(ctx, kKeyB)};
-        float* vals[2] = {buf<float>(ctx, kValA), buf<float>(ctx, kValB)};
-        CU(launch_collect(d, t2->n_obj, keys, vals, ctx->scratch[kScanTmp].p, sort_bytes, cnt_collect,
-                          buf<int>(ctx, kOutQ), buf<int>(ctx, kOutT), buf<float>(ctx, kOutD), s));
+        int* vals[2] = {buf<int>(ctx, kValA), buf<int>(ctx, kValB)};
+        CU(launch_collect(d, t2->n_obj, keys, vals, ctx->scratch[kScanTmp].p, sort_bytes, cnt_collect, pex,
+                          buf<int>(ctx, kOutQ), buf<int>(ctx, kOutT), buf<float>(ctx, kOutD),
+                          exact ? buf<double>(ctx, kOutD64) : nullptr, s));
         launches += 2;
     }
     CU(cudaEventRecord(ctx->ev[4], s));
@@ -326,6 +346,10 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         cudaMemcpyAsync(R->q.data(), buf<int>(ctx, kOutQ), nres * 4, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(R->t.data(), buf<int>(ctx, kOutT), nres * 4, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(R->d.data(), buf<float>(ctx, kOutD), nres * 4, cudaMemcpyDeviceToHost, s);
+        if (exact) {
+            R->d64.resize(nres);
+            cudaMemcpyAsync(R->d64.data(), buf<double>(ctx, kOutD64), nres * 8, cudaMemcpyDeviceToHost, s);
+        }
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) { delete R; return fail(ctx, TDP_ERR_CUDA, cudaGetErrorString(e)); }
     }
@@ -341,9 +365,14 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     st.kernel_launches = launches;
     st.host_syncs = syncs;
     {
-        float lms = 0;
+        float lms = 0, xms = 0;
         cudaEventElapsedTime(&lms, ctx->ev[1], ctx->ev[4]);
-        st.lod_ms = lms;
+        if (exact) cudaEventElapsedTime(&xms, ctx->ev[6], ctx->ev[7]);
+        st.lod_ms = lms - xms;
+        st.exact_ms = xms;
+        st.exact_items = xi.items;
+        st.exact_f64_items = xi.f64_items;
+        st.fp32_max_rel_err = xi.max_rel_err32;
     }
     ctx->stats = st;
     *out = R;
@@ -387,6 +416,13 @@ int tdp_autotune(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp
 int tdp_result_count(const tdp_result* r, long* n) {
     if (!r || !n) return TDP_ERR_ARG;
     *n = (long)r->q.size();
+    return TDP_OK;
+}
+
+int tdp_result_copy_f64(const tdp_result* r, double* dist) {
+    if (!r) return TDP_ERR_ARG;
+    if (r->d64.size() != r->q.size()) return TDP_ERR_STATE;
+    if (dist) std::memcpy(dist, r->d64.data(), r->d64.size() * 8);
     return TDP_OK;
 }
 

@@ -41,7 +41,9 @@ class Stats(C.Structure):
                 ("full_evals", C.c_ulonglong), ("tri_pairs", C.c_double), ("refine_items", C.c_long),
                 ("refine_launches", C.c_long), ("recheck_pairs", C.c_long), ("filter_pairs", C.c_long),
                 ("filter_voxel_pairs", C.c_double), ("kernel_launches", C.c_long),
-                ("candidates_ms", C.c_double), ("lod_ms", C.c_double), ("host_syncs", C.c_long)]
+                ("candidates_ms", C.c_double), ("lod_ms", C.c_double), ("host_syncs", C.c_long),
+                ("exact_ms", C.c_double), ("exact_items", C.c_long), ("exact_f64_items", C.c_long),
+                ("fp32_max_rel_err", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -187,7 +189,8 @@ class TileInfo(C.Structure):
 
 class JoinParams(C.Structure):
     _fields_ = [("query", C.c_int), ("knn", C.c_int), ("within_dist", C.c_float), ("lods", C.c_int * 8),
-                ("n_lods", C.c_int), ("hausdorff_level", C.c_int), ("form", C.c_int)]
+                ("n_lods", C.c_int), ("hausdorff_level", C.c_int), ("form", C.c_int),
+                ("exact_distances", C.c_int)]
 
 
 def _bind_join(L):
@@ -273,10 +276,14 @@ def _join_params(query, knn, within, lods, hausdorff_level, form) -> JoinParams:
 
 
 def _join(self, tile1: Tile, tile2: Tile | None, query: str = "nn", knn: int = 1, within: float = 1000.0,
-          lods=None, hausdorff_level: int = 2, form: int = FORM_TUNED):
-    """tdbase join on resident tiles; returns (query_ids, result_ids, dist) sorted by (query, result)."""
+          lods=None, hausdorff_level: int = 2, form: int = FORM_TUNED, exact_distances: bool = False):
+    """tdbase join on resident tiles; returns (query_ids, result_ids, dist) sorted by (query, result).
+
+    dist is float32 (each pair's upper bound when decided) unless
+    exact_distances is set: then float64 exact LOD-100 distances."""
     L = lib()
     p = _join_params(query, knn, within, lods, hausdorff_level, form)
+    p.exact_distances = int(bool(exact_distances))
     r = C.c_void_p()
     self.check(L.tdp_join(self._h, tile1.handle, None if tile2 is None else tile2.handle, C.byref(p), C.byref(r)))
     try:
@@ -286,6 +293,12 @@ def _join(self, tile1: Tile, tile2: Tile | None, query: str = "nn", knn: int = 1
         t = np.empty(n.value, np.int32)
         d = np.empty(n.value, np.float32)
         L.tdp_result_copy(r, _ptr(q), _ptr(t), _ptr(d))
+        if exact_distances:
+            d = np.empty(n.value, np.float64)
+            L.tdp_result_copy_f64.argtypes = [C.c_void_p, C.c_void_p]
+            rc = L.tdp_result_copy_f64(r, _ptr(d))
+            if rc != TDP_OK:
+                raise TdpError(rc, "exact distances missing")
     finally:
         L.tdp_result_free(r)
     return q, t, d
@@ -296,7 +309,7 @@ Context.join = _join
 
 EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates", "tdp_ctx_stream",
              "tdp_refine_config_count", "tdp_refine_config_info", "tdp_set_refine_config", "tdp_get_refine_config",
-             "tdp_autotune"]
+             "tdp_autotune", "tdp_result_copy_f64"]
 
 
 def refine_configs():

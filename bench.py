@@ -309,6 +309,14 @@ def main():
         flops = agg_t["full_evals"] * F_TRI + agg_t["tri_pairs"] * F_CULL
         achieved = flops / (refine_ms / 1e3) / 1e12
 
+        # one untimed join with the exact-distance stage: its cost and the FP32
+        # refine's error against FP64 on this workload
+        ctx.join(T1, T2, query="within", within=TAU, form=pkg.FORM_TUNED, exact_distances=True)
+        st_x = ctx.stats()
+        exact = {"ms": st_x["exact_ms"], "join_ms": st_x["total_ms"], "voxel_pairs_fp32": st_x["exact_items"],
+                 "voxel_pairs_fp64": st_x["exact_f64_items"], "fp32_max_rel_err": st_x["fp32_max_rel_err"],
+                 "note": "untimed; every result's LOD-100 distance in FP64"}
+
         # end to end through the C ABI from pinned host bytes: tile upload
         # (H2D + unpack), join, result read-back and tile release, between two
         # events on the context's stream
@@ -361,6 +369,7 @@ def main():
                       "tuned_over_plain": value / plain_value if plain_value else None},
             "e2e": {"value": e2e_value, "unit": "tri-pairs/s", "ms_per_step": e2e_step,
                     "h2d_bytes_per_step": int(nb.size + vb.size), "d2h_bytes_per_step": int(d2h)},
+            "exact_distances": exact,
             "gpu_launches": int(launches_t),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,

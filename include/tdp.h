@@ -71,6 +71,11 @@ typedef struct {
     double candidates_ms;            /* host wall time of object candidates     */
     double lod_ms;                   /* device time of the LOD loop             */
     long host_syncs;                 /* host<->device synchronisations          */
+    double exact_ms;                 /* exact-distance stage (device time)      */
+    long exact_items;                /* LOD-100 voxel pairs it refined in FP32  */
+    long exact_f64_items;            /* of those, evaluated in FP64             */
+    double fp32_max_rel_err;         /* exact stage: max |FP32 minimum - FP64
+                                        distance| / max(distance, 1)           */
 } tdp_stats;
 int tdp_last_stats(const tdp_ctx *ctx, tdp_stats *out);
 /* measured FP32 FMA throughput of the context's device in TFLOP/s (CUDA cores,
@@ -145,6 +150,9 @@ typedef struct {
     int form;              /* TDP_FORM_PLAIN (reference decision rules in FP32) or
                               TDP_FORM_TUNED (persistent refine, FP32 with error
                               bands and an FP64 recheck of undecided pairs)        */
+    int exact_distances;   /* 1: give every result its LOD-100 distance in FP64
+                              (tdp_result_copy_f64); the reference reports ids
+                              only, so this stage has no counterpart (default 0) */
 } tdp_join_params;
 void tdp_join_default_params(tdp_join_params *p);
 int tdp_join(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, const tdp_join_params *p,
@@ -153,6 +161,10 @@ int tdp_result_count(const tdp_result *r, long *n);
 /* any output pointer may be NULL; dist = the pair's upper distance bound when
  * it was decided (the exact FP32 distance for pairs decided at the last LOD) */
 int tdp_result_copy(const tdp_result *r, int *query_ids, int *result_ids, float *dist);
+/* the exact LOD-100 distances (double, minimum over the stored float
+ * coordinates up to FP64 rounding), in the same row order; TDP_ERR_STATE when
+ * the join ran without exact_distances */
+int tdp_result_copy_f64(const tdp_result *r, double *dist);
 int tdp_result_free(tdp_result *r);
 
 /* Autotuner: runs the tuned join of `params` once per configuration untimed

@@ -182,3 +182,36 @@ def test_refine_configs_identical_and_autotune(pkg, ctx, gpu_tiles):
             ctx.set_refine_config(len(cfgs))
     finally:
         ctx.set_refine_config(keep)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_exact_distances_match_fp64_oracle(pkg, ctx, gpu_tiles, name):
+    """With exact_distances every result carries its LOD-100 distance in FP64:
+    within 1e-9 relative of the FP64 oracle's exact object distance."""
+    from oracle_bind import join_exact
+    nv, npv, seed, query, knn, tau, self_join, lods, level = CASES[name]
+    nb, vb = tiles(nv, npv, seed)
+    T1, T2 = gpu_tiles(nv, npv, seed)
+    oq, ot, od, _ = join_exact(nb, None if self_join else vb, self_join, query == "nn", knn=knn, tau=tau)
+    truth = {(int(a), int(b)): float(x) for a, b, x in zip(oq, ot, od)}
+    for form in (pkg.FORM_PLAIN, pkg.FORM_TUNED):
+        q, t, d = ctx.join(T1, None if self_join else T2, query=query, knn=knn, within=tau, lods=lods,
+                           hausdorff_level=level, form=form, exact_distances=True)
+        assert d.dtype == np.float64 and len(d) == len(q) > 0
+        ref = np.array([truth[(int(a), int(b))] for a, b in zip(q, t)])
+        err = np.abs(d - ref) / np.maximum(ref, 1.0)
+        assert err.max() <= 1e-9, (name, form, float(err.max()))
+        st = ctx.stats()
+        assert st["exact_items"] >= len(q) and 0 < st["exact_f64_items"] <= st["exact_items"]
+        # the FP32 refine's own error against FP64 stays far inside its 64uR model
+        assert 0.0 <= st["fp32_max_rel_err"] < 1e-4
+        # the ids are those of the join without the exact stage
+        q2, t2, d2 = ctx.join(T1, None if self_join else T2, query=query, knn=knn, within=tau, lods=lods,
+                              hausdorff_level=level, form=form)
+        np.testing.assert_array_equal(q, q2)
+        np.testing.assert_array_equal(t, t2)
+        assert d2.dtype == np.float32
+        # at Hausdorff level 2 every FP32 result distance is an upper bound of
+        # the exact one (within its error band)
+        if level == 2:
+            assert np.all(d2.astype(np.float64) >= d * (1 - 1e-5) - 1e-4)
