@@ -97,7 +97,8 @@ __device__ unsigned long long kth_key(const unsigned long long* keys, int n, int
 }
 
 __global__ void __launch_bounds__(kWarps * 32) k_cand_kth(DG pg, const float* __restrict__ xf1,
-                                                         const float* __restrict__ xf2, int n1, int K, int self,
+                                                         const float* __restrict__ xf2, int n1, int K_all, int self,
+                                                         const int* __restrict__ qk,
                                                          unsigned long long* __restrict__ kth,
                                                          int* __restrict__ overflow) {
     __shared__ unsigned long long keys[kWarps][kCap];
@@ -105,6 +106,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_cand_kth(DG pg, const float* __
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nw = gridDim.x * kWarps;
     for (int q = blockIdx.x * kWarps + w; q < n1; q += nw) {
+        const int K = qk ? qk[q] : K_all;
+        if (K <= 0) continue;  // a within object of a mixed batch (warp-uniform)
         const float* xq = xf1 + 3 * (size_t)q;
         const int cx = dci(xq[0], pg.lo0, pg.cell, pg.n0), cy = dci(xq[1], pg.lo1, pg.cell, pg.n1);
         const int cz = dci(xq[2], pg.lo2, pg.cell, pg.n2);
@@ -150,7 +153,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_cand_kth(DG pg, const float* __
 template <bool WRITE>
 __global__ void __launch_bounds__(256) k_cand_pass(DG bg, const float* __restrict__ box1, const float* __restrict__ xf1,
                                                    const float* __restrict__ box2, const float* __restrict__ xf2,
-                                                   int n1, int self, int knn, float tau,
+                                                   int n1, int self, int knn_all, float tau_all,
+                                                   const int* __restrict__ qk, const float* __restrict__ qtau,
                                                    const unsigned long long* __restrict__ kth,
                                                    int64_t* __restrict__ cnt, const int64_t* __restrict__ off,
                                                    unsigned long long* __restrict__ keys) {
@@ -160,6 +164,8 @@ __global__ void __launch_bounds__(256) k_cand_pass(DG bg, const float* __restric
     for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n1; q += nw) {
         const float* qb = box1 + 6 * (size_t)q;
         const float* xq = xf1 + 3 * (size_t)q;
+        const int knn = qk ? qk[q] > 0 : knn_all;
+        const float tau = qk ? qtau[q] : tau_all;
         unsigned long long kk = 0;
         float T = tau;
         if (knn) {
@@ -244,7 +250,8 @@ struct TileBoxes {
 }  // namespace
 
 int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool self, bool knn, int K, float tau,
-                      Buf& pq_buf, Buf& pt_buf, Buf& qoff_buf, long& P, bool& overflow) {
+                      Buf& pq_buf, Buf& pt_buf, Buf& qoff_buf, long& P, bool& overflow, const int* qk,
+                      const float* qtau) {
     cudaStream_t s = ctx->stream;
     const long n1 = t1->n_obj, n2 = t2->n_obj;
     overflow = false;
@@ -286,17 +293,17 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
     CU(cudaMemsetAsync(d_over, 0, 4, s));
     const DG bg = dg(t2->box_grid), pg = dg(t2->point_grid);
     unsigned long long* kth = (unsigned long long*)kthb.p;
-    if (knn) {
+    if (knn || qk) {
         const int blocks = (int)std::min<long>((n1 + kWarps - 1) / kWarps, (long)ctx->num_sms * 16);
-        k_cand_kth<<<std::max(blocks, 1), kWarps * 32, 0, s>>>(pg, xf1, xf2, (int)n1, K, self, kth, d_over);
+        k_cand_kth<<<std::max(blocks, 1), kWarps * 32, 0, s>>>(pg, xf1, xf2, (int)n1, K, self, qk, kth, d_over);
         CU(cudaGetLastError());
     }
     int64_t* cnt = (int64_t*)cntb.p;
     int64_t* qoff = (int64_t*)qoff_buf.p;
     const int pblocks = (int)std::min<long>((n1 + 7) / 8, (long)ctx->num_sms * 32);
     CU(cudaMemsetAsync(cnt + n1, 0, 8, s));
-    k_cand_pass<false><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, (int)n1, self, knn, tau, kth,
-                                                           cnt, nullptr, nullptr);
+    k_cand_pass<false><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, (int)n1, self, knn, tau, qk,
+                                                           qtau, kth, cnt, nullptr, nullptr);
     CU(cudaGetLastError());
     size_t tb = 0;
     CU(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, qoff, (int)n1 + 1, s));
@@ -319,7 +326,7 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
     if ((rc = ensure(ctx, pq_buf, Pz * 4))) return rc;
     if ((rc = ensure(ctx, pt_buf, Pz * 4))) return rc;
     if (P > 0) {
-        k_cand_pass<true><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, (int)n1, self, knn, tau, kth,
+        k_cand_pass<true><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, (int)n1, self, knn, tau, qk, qtau, kth,
                                                               nullptr, qoff, (unsigned long long*)keys.p);
         CU(cudaGetLastError());
         size_t sb = 0;

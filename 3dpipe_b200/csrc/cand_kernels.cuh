@@ -14,7 +14,10 @@ namespace tdp {
 // CSR) are device buffers owned by the context's scratch, P is the pair count.
 // overflow is set when a kNN ring search exceeded its per-warp buffer; the
 // caller then uses the host path for this join.
+// qk / qtau (device, optional): per tile-1 object K (> 0, kNN) or 0 (within,
+// distance qtau); NULL: every object uses (knn, K, tau).
 int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool self, bool knn, int K, float tau,
-                      Buf& pq_buf, Buf& pt_buf, Buf& qoff_buf, long& P, bool& overflow);
+                      Buf& pq_buf, Buf& pt_buf, Buf& qoff_buf, long& P, bool& overflow, const int* qk = nullptr,
+                      const float* qtau = nullptr);
 
 }  // namespace tdp

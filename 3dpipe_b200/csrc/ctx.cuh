@@ -47,7 +47,7 @@ struct tdp_ctx {
     cudaEvent_t lod_ev[16] = {};  // refine timing per LOD (tuned loop)
     std::string last_error;
     std::unordered_map<void*, size_t> allocs;
-    tdp::Buf scratch[96];  // slots: refine-batch 0-4, tile upload 12-13, join 20-48, candidates 50-59, result sort 60-63, exact distances 64-81
+    tdp::Buf scratch[96];  // slots: refine-batch 0-4, tile upload 12-13, join 20-48, candidates 50-59, result sort 60-63, exact distances 64-81, per-object queries 82-83
     unsigned* d_counter = nullptr;            // work counters (device)
     unsigned long long* d_stats = nullptr;    // device-side statistics
     tdp::LastStats stats;

@@ -147,17 +147,25 @@ __global__ void __launch_bounds__(kBlock) k_pair_bounds(JoinDev d) {
     if (lane == 0 && vp && d.stat_vp) atomicAdd(d.stat_vp, vp);
 }
 
-__global__ void k_within_decide(JoinDev d, float tau, int tuned) {
+__global__ void k_within_decide(JoinDev d, float tau_all, int tuned) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.P; p += gridDim.x * blockDim.x) {
         if (d.pstat[p] != kUndecided) continue;
+        float tau = tau_all;
+        if (d.qk) {
+            const int q = d.pq[p];
+            if (d.qk[q] > 0) continue;  // a kNN object of a mixed batch
+            tau = d.qtau[q];
+        }
         const float e = tuned ? d.perr[p] : 0.f;
         if (d.pmx[p] + e <= tau) d.pstat[p] = kReported;
         else if (d.pmn[p] - e > tau) d.pstat[p] = kDropped;
     }
 }
 
-__global__ void k_knn_rank(JoinDev d, int K, int tuned, int* __restrict__ st) {
+__global__ void k_knn_rank(JoinDev d, int K_all, int tuned, int* __restrict__ st) {
     for (int q = blockIdx.x; q < d.N1; q += gridDim.x) {
+        const int K = d.qk ? d.qk[q] : K_all;
+        if (K <= 0) continue;  // a within object of a mixed batch (uniform over the block)
         const int64_t b = d.qoff[q], e = d.qoff[q + 1];
         int conf = d.qconf[q];
         if (conf < K) {
@@ -196,7 +204,8 @@ __global__ void k_knn_rank(JoinDev d, int K, int tuned, int* __restrict__ st) {
 }
 
 template <bool WRITE>
-__global__ void __launch_bounds__(kBlock) k_vps(JoinDev d, int within, float tau, int tuned, int64_t* __restrict__ cnt) {
+__global__ void __launch_bounds__(kBlock) k_vps(JoinDev d, int within_all, float tau_all, int tuned,
+                                                 int64_t* __restrict__ cnt) {
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
@@ -205,6 +214,8 @@ __global__ void __launch_bounds__(kBlock) k_vps(JoinDev d, int within, float tau
             continue;
         }
         const int q = d.pq[p], t = d.pt[p];
+        const int within = d.qk ? d.qk[q] == 0 : within_all;
+        const float tau = d.qk ? d.qtau[q] : tau_all;
         const uint32_t a0 = d.ovox1[q], b0 = d.ovox2[t];
         const uint32_t n1 = d.ovox1[q + 1] - a0, n2 = d.ovox2[t + 1] - b0;
         const float slack = tuned ? d.perr[p] : 0.f;
@@ -315,7 +326,8 @@ __global__ void k_recheck_apply(const double* __restrict__ res, const int* __res
 }
 
 __global__ void __launch_bounds__(kBlock) k_recheck_pairs(JoinDev d, const double* __restrict__ vexact,
-                                                          double* __restrict__ pexact, int within, float tau) {
+                                                          double* __restrict__ pexact, int within_all,
+                                                          float tau_all) {
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
@@ -329,6 +341,9 @@ __global__ void __launch_bounds__(kBlock) k_recheck_pairs(JoinDev d, const doubl
             D = x < D ? x : D;
         }
         if (lane == 0) {
+            const int q = d.pq[p];
+            const int within = d.qk ? d.qk[q] == 0 : within_all;
+            const float tau = d.qk ? d.qtau[q] : tau_all;
             pexact[p] = D;
             d.pmn[p] = d.pmx[p] = (float)D;
             if (within) d.pstat[p] = D <= (double)tau ? kReported : kDropped;
@@ -337,8 +352,10 @@ __global__ void __launch_bounds__(kBlock) k_recheck_pairs(JoinDev d, const doubl
 }
 
 // kNN: the still-undecided candidates of a query compete for its open slots by exact distance
-__global__ void k_recheck_knn(JoinDev d, int K, const double* __restrict__ pexact) {
+__global__ void k_recheck_knn(JoinDev d, int K_all, const double* __restrict__ pexact) {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < d.N1; q += gridDim.x * blockDim.x) {
+        const int K = d.qk ? d.qk[q] : K_all;
+        if (K <= 0) continue;
         const int64_t b = d.qoff[q], e = d.qoff[q + 1];
         int conf = d.qconf[q];
         while (conf < K) {
@@ -495,7 +512,7 @@ cudaError_t launch_recheck_finish(const JoinDev& d, const double* res, const int
                                   double* pexact, int knn, int K, float tau, cudaStream_t s, const unsigned* W_dev) {
     if (W > 0) k_recheck_apply<<<grid_for(W, 256), 256, 0, s>>>(res, item_vp, W, W_dev, vexact);
     if (d.P > 0) k_recheck_pairs<<<grid_for(d.P, kBlock / 32), kBlock, 0, s>>>(d, vexact, pexact, !knn, tau);
-    if (knn && d.N1 > 0) k_recheck_knn<<<grid_for(d.N1, 128), 128, 0, s>>>(d, K, pexact);
+    if ((knn || d.qk) && d.N1 > 0) k_recheck_knn<<<grid_for(d.N1, 128), 128, 0, s>>>(d, K, pexact);
     return cudaGetLastError();
 }
 cudaError_t launch_count_status(const JoinDev& d, unsigned* c, cudaStream_t s) {

@@ -36,6 +36,11 @@ struct JoinDev {
     int N1;
     const int64_t* qoff;  // [N1+1]
     int* qconf;
+    // per query object query (a batch of different requests), or NULL when
+    // every object uses the call's scalar query: qk[q] = K (> 0, kNN) or 0
+    // (within, distance qtau[q])
+    const int* qk;
+    const float* qtau;
     // voxel pairs kept after the filter
     int64_t V;
     int* vpa;

@@ -19,14 +19,9 @@
 
 #include "ctx.cuh"
 #include "storage/dev_tile.h"
+#include "tile_kernels.cuh"
 
 namespace tdp {
-
-struct UnpackSeg {
-    uint64_t src;      // byte offset of the segment's triangles in the staging buffer
-    uint32_t dst;      // first destination triangle in tri[lod]
-    uint32_t cnt_lod;  // count (low 24 bits) | lod << 24
-};
 
 struct TriPtrs {
     float4* p[kNumLods];
@@ -49,6 +44,16 @@ __global__ void unpack_kernel(const uint8_t* __restrict__ raw, const UnpackSeg* 
             dst[3 * (size_t)i + 2] = make_float4(q[6], q[7], q[8], 0.f);
         }
     }
+}
+
+cudaError_t launch_unpack(const uint8_t* raw, const UnpackSeg* segs, int nseg, float4* const* tri, int num_sms,
+                          cudaStream_t s) {
+    if (nseg <= 0) return cudaSuccess;
+    TriPtrs tp;
+    for (int l = 0; l < kNumLods; ++l) tp.p[l] = tri[l];
+    const int blocks = (int)std::min<size_t>(((size_t)nseg + 7) / 8, (size_t)num_sms * 16);
+    unpack_kernel<<<blocks, 256, 0, s>>>(raw, segs, nseg, tp);
+    return cudaGetLastError();
 }
 
 void tile_release(tdp_ctx* ctx, tdp_tile* t) {

@@ -57,7 +57,7 @@ void generate_candidates(const CandidateQuery& q, std::vector<int64_t>& off, std
     const float cell = pick_cell(q.box2, q.n2);
     CellGrid boxes, points;
     boxes.build(q.box2, q.n2, 6, 3, cell);
-    if (q.is_knn) points.build(q.xf2, q.n2, 3, 0, cell);
+    if (q.is_knn || q.obj_knn) points.build(q.xf2, q.n2, 3, 0, cell);
 
     const int threads = q.threads > 0 ? q.threads : (int)std::max(1u, std::thread::hardware_concurrency());
     const long chunk = 256;
@@ -76,8 +76,10 @@ void generate_candidates(const CandidateQuery& q, std::vector<int64_t>& off, std
                 const float* qb = q.box1 + 6 * i;
                 const float* qx = q.xf1 + 3 * i;
                 found.clear();
-                if (!q.is_knn) {
-                    const float r = q.within;
+                const bool is_knn = q.obj_knn ? q.obj_knn[i] > 0 : q.is_knn;
+                const float within = q.obj_knn ? q.obj_within[i] : q.within;
+                if (!is_knn) {
+                    const float r = within;
                     int x0 = boxes.ci(qb[0] - r, 0), x1 = boxes.ci(qb[3] + r, 0);
                     int y0 = boxes.ci(qb[1] - r, 1), y1 = boxes.ci(qb[4] + r, 1);
                     int z0 = boxes.ci(qb[2] - r, 2), z1 = boxes.ci(qb[5] + r, 2);
@@ -90,13 +92,13 @@ void generate_candidates(const CandidateQuery& q, std::vector<int64_t>& off, std
                                     if (stamp[o] == (int)i) continue;
                                     stamp[o] = (int)i;
                                     if (q.self_join && o == i) continue;
-                                    if (box_gap(q.box2 + 6 * o, qb) <= q.within) found.push_back({0.f, o});
+                                    if (box_gap(q.box2 + 6 * o, qb) <= within) found.push_back({0.f, o});
                                 }
                             }
                     std::sort(found.begin(), found.end(), [](auto& a, auto& b) { return a.second < b.second; });
                 } else {
                     // 1) the K smallest transform distances (ring search on the point grid)
-                    const int K = q.knn;
+                    const int K = q.obj_knn ? q.obj_knn[i] : q.knn;
                     std::priority_queue<std::pair<float, int32_t>> heap;  // max-heap of (dist, id)
                     int cx = points.ci(qx[0], 0), cy = points.ci(qx[1], 1), cz = points.ci(qx[2], 2);
                     int maxr = std::max({points.n[0], points.n[1], points.n[2]});

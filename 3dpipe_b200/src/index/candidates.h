@@ -32,6 +32,10 @@ struct CandidateQuery {
     int knn;
     float within;
     int threads;  // 0 = hardware concurrency
+    // optional per query object query (a batch of different requests):
+    // obj_knn[i] = K (> 0, kNN) or 0 (within, distance obj_within[i])
+    const int* obj_knn = nullptr;
+    const float* obj_within = nullptr;
 };
 
 // off: [n1+1] CSR offsets into ids.

@@ -33,11 +33,7 @@
 #include "storage/dev_tile.h"
 #include "tdp.h"
 
-struct tdp_result {
-    std::vector<int> q, t;
-    std::vector<float> d;
-    std::vector<double> d64;  // exact LOD-100 distances (params.exact_distances)
-};
+#include "join/result.h"
 
 namespace tdp {
 
@@ -49,6 +45,7 @@ enum Slot {
     kVexact, kPexact, kRes64,
     kKeyA = 60, kKeyB, kValA, kValB,  // result sort (50-59 hold the candidate buffers)
     kPexOut = 76, kOutD64,            // exact distances (64-75 and 78-81 are the exact stage's own)
+    kQk = 82, kQtau,                  // per query object queries
 };
 
 template <typename T>
@@ -79,8 +76,21 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     const bool self = (t2 == nullptr || t2 == t1);
     if (!t2) t2 = t1;
     const bool knn = prm->query == TDP_QUERY_NN;
-    if (!knn && prm->query != TDP_QUERY_WITHIN) return fail(ctx, TDP_ERR_ARG, "query must be nn or within");
-    if (knn && prm->knn < 1) return fail(ctx, TDP_ERR_ARG, "knn must be >= 1");
+    const bool mixed = prm->obj_knn != nullptr;  // per query object queries (a batch of requests)
+    bool any_knn = knn, any_within = !knn;
+    if (mixed) {
+        if (!prm->obj_within) return fail(ctx, TDP_ERR_ARG, "obj_knn given without obj_within");
+        any_knn = any_within = false;
+        for (long i = 0; i < t1->n_obj; ++i) {
+            if (prm->obj_knn[i] < 0) return fail(ctx, TDP_ERR_ARG, "obj_knn must be >= 0");
+            if (prm->obj_knn[i] == 0 && !(prm->obj_within[i] >= 0.f))
+                return fail(ctx, TDP_ERR_ARG, "obj_within must be >= 0 for within objects");
+            (prm->obj_knn[i] > 0 ? any_knn : any_within) = true;
+        }
+    } else {
+        if (!knn && prm->query != TDP_QUERY_WITHIN) return fail(ctx, TDP_ERR_ARG, "query must be nn or within");
+        if (knn && prm->knn < 1) return fail(ctx, TDP_ERR_ARG, "knn must be >= 1");
+    }
     if (prm->hausdorff_level < 0 || prm->hausdorff_level > 2) return fail(ctx, TDP_ERR_ARG, "hausdorff_level must be 0, 1 or 2");
     if (prm->form != TDP_FORM_PLAIN && prm->form != TDP_FORM_TUNED) return fail(ctx, TDP_ERR_ARG, "unknown form");
     if (t1->device != ctx->device || t2->device != ctx->device) return fail(ctx, TDP_ERR_ARG, "tile lives on another device");
@@ -112,16 +122,28 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     long P = 0;
     bool on_device = false;
     const auto c0 = std::chrono::steady_clock::now();
+    const int* dqk = nullptr;
+    const float* dqtau = nullptr;
+    if (mixed) {
+        const size_t n1z = (size_t)std::max<long>(t1->n_obj, 1);
+        ENS(kQk, n1z * 4);
+        ENS(kQtau, n1z * 4);
+        dqk = buf<int>(ctx, kQk);
+        dqtau = buf<float>(ctx, kQtau);
+        CU(cudaMemcpyAsync((void*)dqk, prm->obj_knn, t1->n_obj * 4, cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync((void*)dqtau, prm->obj_within, t1->n_obj * 4, cudaMemcpyHostToDevice, s));
+    }
     if (tuned) {
         bool overflow = false;
         if ((rc = device_candidates(ctx, t1, t2, self, knn, knn ? prm->knn : 0, prm->within_dist, ctx->scratch[kPq],
-                                    ctx->scratch[kPt], ctx->scratch[kQoff], P, overflow)))
+                                    ctx->scratch[kPt], ctx->scratch[kQoff], P, overflow, dqk, dqtau)))
             return rc;
         on_device = !overflow;
     }
     if (!on_device) {
         CandidateQuery cq{t1->host.obj_box.data(), t1->host.obj_xf.data(), t1->n_obj, t2->host.obj_box.data(),
-                          t2->host.obj_xf.data(), t2->n_obj, self, knn, knn ? prm->knn : 0, prm->within_dist, 0};
+                          t2->host.obj_xf.data(), t2->n_obj, self, knn, knn ? prm->knn : 0, prm->within_dist, 0,
+                          prm->obj_knn, prm->obj_within};
         generate_candidates(cq, qoff, ids);
         P = (long)ids.size();
         if (P >= (1L << 31) - 1) return fail(ctx, TDP_ERR_ARG, "too many candidate pairs");
@@ -145,6 +167,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     d.pmn = buf<float>(ctx, kPmn); d.pmx = buf<float>(ctx, kPmx); d.perr = buf<float>(ctx, kPerr);
     d.pstat = buf<uint8_t>(ctx, kPstat); d.pvp = buf<int64_t>(ctx, kPvp);
     d.N1 = (int)t1->n_obj; d.qoff = buf<int64_t>(ctx, kQoff); d.qconf = buf<int>(ctx, kQconf);
+    d.qk = dqk; d.qtau = dqtau;
 
     unsigned* cnt_items = ctx->d_counter + 8;    // [0] items, [2..3] tri-pair sum (u64)
     unsigned* cnt_status = ctx->d_counter + 16;  // undecided, reported
@@ -165,8 +188,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
 
     // ---- 2. filter ----
     CU(launch_pair_bounds(d, s)); ++launches;
-    if (knn) { CU(launch_knn_rank(d, prm->knn, tuned, buf<int>(ctx, kRankSt), s)); }
-    else { CU(launch_within_decide(d, prm->within_dist, tuned, s)); }
+    if (any_knn) { CU(launch_knn_rank(d, prm->knn, tuned, buf<int>(ctx, kRankSt), s)); }
+    if (any_within) { CU(launch_within_decide(d, prm->within_dist, tuned, s)); }
     ++launches;
     int64_t* cnt = buf<int64_t>(ctx, kCnt);
     CU(cudaMemsetAsync(cnt + P, 0, 8, s));
@@ -226,8 +249,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
                 CU(launch_apply_results(d, res, item_vp, W, highest, prm->hausdorff_level, li, (int)k, s)); ++launches;
             }
             CU(launch_pair_update(d, (int)k, 0, s)); ++launches;
-            if (knn) CU(launch_knn_rank(d, prm->knn, 0, buf<int>(ctx, kRankSt), s));
-            else CU(launch_within_decide(d, prm->within_dist, 0, s));
+            if (any_knn) CU(launch_knn_rank(d, prm->knn, 0, buf<int>(ctx, kRankSt), s));
+            if (any_within) CU(launch_within_decide(d, prm->within_dist, 0, s));
             ++launches;
             CU(cudaMemsetAsync(cnt_status, 0, 8, s));
             CU(launch_count_status(d, cnt_status, s)); ++launches;
@@ -264,8 +287,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
             st.refine_launches++;
             CU(launch_apply_results(d, res, item_vp, (int)V, highest, prm->hausdorff_level, li, (int)k, s, cnt_items));
             CU(launch_pair_update(d, (int)k, 1, s));
-            if (knn) CU(launch_knn_rank(d, prm->knn, 1, buf<int>(ctx, kRankSt), s));
-            else CU(launch_within_decide(d, prm->within_dist, 1, s));
+            if (any_knn) CU(launch_knn_rank(d, prm->knn, 1, buf<int>(ctx, kRankSt), s));
+            if (any_within) CU(launch_within_decide(d, prm->within_dist, 1, s));
             launches += 3;
         }
         // ---- 3b. FP64 recheck of pairs whose FP32 ranges stayed inside their

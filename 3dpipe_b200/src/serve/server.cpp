@@ -1,0 +1,484 @@
+// server.cpp -- continuous-batching request loop over a resident tile 2
+// (tdp_server_* in include/tdp.h).
+//
+// Two device arenas hold the query objects of the admitted requests.  An
+// arena is a tdp_tile whose device arrays are allocated once at full
+// capacity; a request is appended at the arena's running offsets (objects,
+// voxels, triangles per LOD), on the arena's own stream: its RAW bytes are
+// copied to a device staging buffer and unpacked by the tile-upload kernel.
+//
+//   admitter thread   takes requests in arrival order and appends each to the
+//                     arena being filled while it fits (admission by memory);
+//                     a request that does not fit seals the arena and waits
+//                     for the other one;
+//   executor thread   whenever it is idle, takes the sealed arena or else the
+//                     filling one (if it holds a request), waits on the
+//                     arena's upload event, runs ONE tdp_join over all of its
+//                     objects with per-object queries (obj_knn / obj_within),
+//                     splits the rows by request and frees the arena.
+// While a batch runs, arrivals go into the other arena, so uploads overlap
+// the join and the next batch starts as soon as the GPU is free.
+// The reference has no request loop (one join per `tdbase join` run,
+// src/tools/tdbase.cpp:482-549).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../csrc/ctx.cuh"
+#include "../../csrc/tile_kernels.cuh"
+#include "join/result.h"
+#include "storage/dev_tile.h"
+#include "storage/dt_format.h"
+#include "tdp.h"
+
+namespace tdp {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+struct Request {
+    uint64_t id = 0;
+    const uint8_t* raw = nullptr;
+    size_t len = 0;
+    TileHost host;     // parsed at submit
+    uint64_t base = 0; // byte offset of the first object's record in raw
+    uint64_t span = 0; // bytes from base to the end of the last object's data
+    int knn = 0;       // > 0: kNN; 0: within
+    float within = 0.f;
+    Clock::time_point t_submit, t_start, t_done;
+    long o0 = 0;       // first object in its arena
+    long batch = -1;
+    int batch_requests = 0;
+    int status = TDP_OK;
+    bool done = false;
+    std::unique_ptr<tdp_result> res;
+};
+
+enum class ArenaState { kFree, kFilling, kSealed, kRunning };
+
+struct Arena {
+    tdp_tile tile;                 // device arrays at capacity; counts grow with appends
+    uint32_t n_tri[kNumLods] = {};
+    std::vector<float4> hvox;      // host copy of the voxel records (3 float4 per voxel)
+    std::vector<Request*> reqs;
+    ArenaState state = ArenaState::kFree;
+    bool appending = false;
+    cudaStream_t up = nullptr;
+    cudaEvent_t ready = nullptr;
+    uint8_t* stage = nullptr;      // device staging of one request's RAW bytes
+    UnpackSeg* dsegs = nullptr;
+    std::vector<UnpackSeg> segs;
+};
+
+}  // namespace
+}  // namespace tdp
+
+using namespace tdp;
+
+struct tdp_server {
+    tdp_ctx* ctx = nullptr;
+    const tdp_tile* t2 = nullptr;
+    tdp_server_params p{};
+    long seg_cap = 0;
+    Arena arena[2];
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Request*> pending;
+    std::unordered_map<uint64_t, std::unique_ptr<Request>> table;
+    uint64_t next_id = 1;
+    long batches = 0, completed = 0, failed = 0;
+    double busy_ms = 0;
+    bool stop = false;
+    std::thread admitter, executor;
+};
+
+namespace {
+
+void reset_arena(Arena& a) {
+    TileHost& H = a.tile.host;
+    a.tile.n_obj = a.tile.n_vox = 0;
+    H.n_obj = H.n_vox = 0;
+    H.obj_box.clear(); H.obj_xf.clear(); H.obj_hd.clear(); H.obj_phd.clear(); H.vox_box.clear();
+    H.obj_vox_off.assign(1, 0);
+    for (int l = 0; l < kNumLods; ++l) {
+        a.tile.h_vtri[l].assign(1, 0);
+        a.n_tri[l] = 0;
+        H.n_tris[l] = 0;
+    }
+    a.hvox.clear();
+    a.reqs.clear();
+}
+
+bool fits(const tdp_server* S, const Arena& a, const Request& r) {
+    if (a.tile.n_obj + r.host.n_obj > S->p.arena_objects) return false;
+    if (a.tile.n_vox + r.host.n_vox > S->p.arena_voxels) return false;
+    for (int l = 0; l < kNumLods; ++l)
+        if ((long)a.n_tri[l] + (long)r.host.n_tris[l] > S->p.arena_tris) return false;
+    return true;
+}
+
+// Append one request's objects at the arena's offsets (admitter thread; the
+// arena is not visible to the executor while `appending` is set).
+int append(tdp_server* S, Arena& a, Request& r) {
+    const TileHost& h = r.host;
+    TileHost& H = a.tile.host;
+    const long o0 = a.tile.n_obj, v0 = a.tile.n_vox, n = h.n_obj, nv = h.n_vox;
+    uint32_t t0[kNumLods];
+    for (int l = 0; l < kNumLods; ++l) t0[l] = a.n_tri[l];
+    // host metadata (capacity reserved at creation: no reallocation)
+    H.obj_box.insert(H.obj_box.end(), h.obj_box.begin(), h.obj_box.end());
+    H.obj_xf.insert(H.obj_xf.end(), h.obj_xf.begin(), h.obj_xf.end());
+    H.obj_hd.insert(H.obj_hd.end(), h.obj_hd.begin(), h.obj_hd.end());
+    H.obj_phd.insert(H.obj_phd.end(), h.obj_phd.begin(), h.obj_phd.end());
+    H.vox_box.insert(H.vox_box.end(), h.vox_box.begin(), h.vox_box.end());
+    for (long i = 1; i <= n; ++i) H.obj_vox_off.push_back((uint32_t)(v0 + h.obj_vox_off[i]));
+    for (long v = 0; v < nv; ++v) {
+        const float* b = &h.vox_box[9 * v];
+        a.hvox.push_back(make_float4(b[0], b[1], b[2], 0.f));
+        a.hvox.push_back(make_float4(b[3], b[4], b[5], 0.f));
+        a.hvox.push_back(make_float4(b[6], b[7], b[8], 0.f));
+    }
+    a.segs.clear();
+    for (int l = 0; l < kNumLods; ++l) {
+        std::vector<uint32_t>& vt = a.tile.h_vtri[l];
+        for (long v = 0; v < nv; ++v) {
+            const uint32_t c = h.vox_cnt[l][v];
+            const uint32_t dst = vt.back();
+            vt.push_back(dst + c);
+            if (!c) continue;
+            const uint64_t src = h.vox_byte_off[l][v] - r.base;
+            if ((src & 3u) || src + (uint64_t)c * 44 > r.span) return TDP_ERR_FORMAT;
+            a.segs.push_back(UnpackSeg{src, dst, c | ((uint32_t)l << 24)});
+        }
+        a.n_tri[l] = t0[l] + (uint32_t)h.n_tris[l];
+        H.n_tris[l] = a.n_tri[l];
+    }
+    if ((long)a.segs.size() > S->seg_cap) return TDP_ERR_ARG;
+    cudaStream_t s = a.up;
+    cudaError_t e = cudaSuccess;
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+        if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+    };
+    cp(a.tile.vox + 3 * (size_t)v0, a.hvox.data() + 3 * (size_t)v0, (size_t)nv * 3 * sizeof(float4));
+    cp(a.tile.obj_vox + o0 + 1, H.obj_vox_off.data() + o0 + 1, (size_t)n * 4);
+    cp(a.tile.obj_hd + (size_t)o0 * kNumLods, H.obj_hd.data() + (size_t)o0 * kNumLods, (size_t)n * kNumLods * 4);
+    cp(a.tile.obj_phd + (size_t)o0 * kNumLods, H.obj_phd.data() + (size_t)o0 * kNumLods, (size_t)n * kNumLods * 4);
+    for (int l = 0; l < kNumLods; ++l)
+        cp(a.tile.vtri[l] + v0 + 1, a.tile.h_vtri[l].data() + v0 + 1, (size_t)nv * 4);
+    cp(a.stage, r.raw + r.base, r.span);
+    cp(a.dsegs, a.segs.data(), a.segs.size() * sizeof(UnpackSeg));
+    if (e == cudaSuccess) e = launch_unpack(a.stage, a.dsegs, (int)a.segs.size(), a.tile.tri, S->ctx->num_sms, s);
+    if (e == cudaSuccess) e = cudaEventRecord(a.ready, s);
+    // the staging buffers are reused by the next append: finish this one first
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return TDP_ERR_CUDA;
+    a.tile.n_obj = H.n_obj = o0 + n;
+    a.tile.n_vox = H.n_vox = v0 + nv;
+    return TDP_OK;
+}
+
+void finish(tdp_server* S, Request* r, int status) {
+    r->status = status;
+    r->t_done = Clock::now();
+    r->done = true;
+    ++S->completed;
+    if (status != TDP_OK) ++S->failed;
+}
+
+void admitter_loop(tdp_server* S) {
+    cudaSetDevice(S->ctx->device);
+    std::unique_lock<std::mutex> lk(S->mu);
+    for (;;) {
+        Arena* a = nullptr;
+        S->cv.wait(lk, [&] {
+            if (S->stop) return true;
+            if (S->pending.empty()) return false;
+            for (Arena& x : S->arena)
+                if (x.state == ArenaState::kFilling) { a = &x; return true; }
+            for (Arena& x : S->arena)
+                if (x.state == ArenaState::kFree) { a = &x; return true; }
+            return false;
+        });
+        if (S->stop) return;
+        Request* r = S->pending.front();
+        if (a->state == ArenaState::kFree) a->state = ArenaState::kFilling;
+        if (!fits(S, *a, *r)) {
+            // sealed: the executor takes it next; the request waits for the other arena
+            a->state = ArenaState::kSealed;
+            S->cv.notify_all();
+            continue;
+        }
+        S->pending.pop_front();
+        a->appending = true;
+        r->o0 = a->tile.n_obj;
+        lk.unlock();
+        const int rc = append(S, *a, *r);
+        lk.lock();
+        a->appending = false;
+        if (rc == TDP_OK) a->reqs.push_back(r);
+        else finish(S, r, rc);
+        S->cv.notify_all();
+    }
+}
+
+void executor_loop(tdp_server* S) {
+    tdp_ctx* ctx = S->ctx;
+    cudaSetDevice(ctx->device);
+    std::vector<int> obj_knn;
+    std::vector<float> obj_within;
+    std::unique_lock<std::mutex> lk(S->mu);
+    for (;;) {
+        Arena* a = nullptr;
+        S->cv.wait(lk, [&] {
+            for (Arena& x : S->arena)
+                if (x.state == ArenaState::kSealed && !x.appending) { a = &x; return true; }
+            for (Arena& x : S->arena)
+                if (x.state == ArenaState::kFilling && !x.appending && !x.reqs.empty()) { a = &x; return true; }
+            return S->stop;
+        });
+        if (!a) return;  // stopping with nothing admitted left to run
+        a->state = ArenaState::kRunning;
+        const long batch = S->batches++;
+        const auto t_start = Clock::now();
+        for (Request* r : a->reqs) {
+            r->t_start = t_start;
+            r->batch = batch;
+            r->batch_requests = (int)a->reqs.size();
+        }
+        std::vector<Request*> reqs = a->reqs;
+        lk.unlock();
+        // per-object queries of the batch
+        const long n = a->tile.n_obj;
+        obj_knn.assign(n, 0);
+        obj_within.assign(n, 0.f);
+        for (Request* r : reqs)
+            for (long i = 0; i < r->host.n_obj; ++i) {
+                obj_knn[r->o0 + i] = r->knn;
+                obj_within[r->o0 + i] = r->within;
+            }
+        tdp_join_params jp;
+        tdp_join_default_params(&jp);
+        std::memcpy(jp.lods, S->p.lods, sizeof(jp.lods));
+        jp.n_lods = S->p.n_lods;
+        jp.hausdorff_level = S->p.hausdorff_level;
+        jp.form = S->p.form;
+        jp.obj_knn = obj_knn.data();
+        jp.obj_within = obj_within.data();
+        tdp_result* res = nullptr;
+        int rc = cudaStreamWaitEvent(ctx->stream, a->ready, 0) == cudaSuccess ? TDP_OK : TDP_ERR_CUDA;
+        if (rc == TDP_OK) rc = tdp_join(ctx, &a->tile, S->t2, &jp, &res);
+        // split the rows (sorted by query object) by request
+        if (rc == TDP_OK) {
+            for (Request* r : reqs) {
+                r->res.reset(new tdp_result());
+                const long lo = r->o0, hi = r->o0 + r->host.n_obj;
+                auto b = std::lower_bound(res->q.begin(), res->q.end(), (int)lo);
+                auto e = std::lower_bound(res->q.begin(), res->q.end(), (int)hi);
+                const size_t i0 = b - res->q.begin(), i1 = e - res->q.begin();
+                r->res->q.reserve(i1 - i0);
+                for (size_t i = i0; i < i1; ++i) r->res->q.push_back(res->q[i] - (int)lo);
+                r->res->t.assign(res->t.begin() + i0, res->t.begin() + i1);
+                r->res->d.assign(res->d.begin() + i0, res->d.begin() + i1);
+            }
+        }
+        delete res;
+        const double busy = ms_between(t_start, Clock::now());
+        lk.lock();
+        S->busy_ms += busy;
+        for (Request* r : reqs) finish(S, r, rc);
+        reset_arena(*a);
+        a->state = ArenaState::kFree;
+        S->cv.notify_all();
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void tdp_server_default_params(tdp_server_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->arena_objects = 65536;
+    p->arena_voxels = 1L << 20;
+    p->arena_tris = 1L << 25;
+    p->max_request_bytes = (size_t)1 << 30;
+    p->hausdorff_level = 2;
+    p->form = TDP_FORM_TUNED;
+}
+
+int tdp_server_create(tdp_ctx* ctx, const tdp_tile* t2, const tdp_server_params* p, tdp_server** out) {
+    if (!ctx || !t2 || !p || !out) return TDP_ERR_ARG;
+    *out = nullptr;
+    if (p->arena_objects < 1 || p->arena_voxels < 1 || p->arena_tris < 1 || p->arena_tris >= (1L << 32) ||
+        p->max_request_bytes < 16)
+        return fail(ctx, TDP_ERR_ARG, "server capacities must be positive (arena_tris < 2^32)");
+    cudaSetDevice(ctx->device);
+    std::unique_ptr<tdp_server> S(new tdp_server());
+    S->ctx = ctx;
+    S->t2 = t2;
+    S->p = *p;
+    S->seg_cap = p->arena_voxels * kNumLods;
+    for (Arena& a : S->arena) {
+        tdp_tile& T = a.tile;
+        T.device = ctx->device;
+        auto alloc = [&](void** ptr, size_t bytes) {
+            if (dmalloc(ctx, ptr, bytes) != cudaSuccess) return false;
+            T.device_bytes += bytes;
+            return true;
+        };
+        bool ok = alloc((void**)&T.vox, (size_t)p->arena_voxels * 3 * sizeof(float4)) &&
+                  alloc((void**)&T.obj_vox, (size_t)(p->arena_objects + 1) * 4) &&
+                  alloc((void**)&T.obj_hd, (size_t)p->arena_objects * kNumLods * 4) &&
+                  alloc((void**)&T.obj_phd, (size_t)p->arena_objects * kNumLods * 4) &&
+                  alloc((void**)&a.stage, p->max_request_bytes + 16) &&
+                  alloc((void**)&a.dsegs, (size_t)S->seg_cap * sizeof(UnpackSeg));
+        for (int l = 0; ok && l < kNumLods; ++l)
+            ok = alloc((void**)&T.tri[l], (size_t)p->arena_tris * 3 * sizeof(float4)) &&
+                 alloc((void**)&T.vtri[l], (size_t)(p->arena_voxels + 1) * 4);
+        if (!ok || cudaStreamCreateWithFlags(&a.up, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&a.ready, cudaEventDisableTiming) != cudaSuccess) {
+            tdp_server_destroy(S.release());
+            return fail(ctx, TDP_ERR_NOMEM, "cannot allocate the serving arenas");
+        }
+        // the first entry of each CSR array stays 0
+        cudaMemsetAsync(T.obj_vox, 0, 4, a.up);
+        for (int l = 0; l < kNumLods; ++l) cudaMemsetAsync(T.vtri[l], 0, 4, a.up);
+        cudaEventRecord(a.ready, a.up);
+        TileHost& H = T.host;
+        H.obj_box.reserve((size_t)p->arena_objects * 6);
+        H.obj_xf.reserve((size_t)p->arena_objects * 3);
+        H.obj_hd.reserve((size_t)p->arena_objects * kNumLods);
+        H.obj_phd.reserve((size_t)p->arena_objects * kNumLods);
+        H.vox_box.reserve((size_t)p->arena_voxels * 9);
+        H.obj_vox_off.reserve((size_t)p->arena_objects + 1);
+        for (int l = 0; l < kNumLods; ++l) T.h_vtri[l].reserve((size_t)p->arena_voxels + 1);
+        a.hvox.reserve((size_t)p->arena_voxels * 3);
+        a.segs.reserve((size_t)S->seg_cap);
+        reset_arena(a);
+        if (cudaStreamSynchronize(a.up) != cudaSuccess) {
+            tdp_server_destroy(S.release());
+            return fail(ctx, TDP_ERR_CUDA, "serving arena set-up failed");
+        }
+    }
+    tdp_server* raw = S.release();
+    raw->admitter = std::thread(admitter_loop, raw);
+    raw->executor = std::thread(executor_loop, raw);
+    *out = raw;
+    return TDP_OK;
+}
+
+int tdp_server_submit(tdp_server* S, const void* raw_dt, size_t len, int query, int knn, float within,
+                      uint64_t* id) {
+    if (!S || !raw_dt || !id) return TDP_ERR_ARG;
+    if (query == TDP_QUERY_NN ? knn < 1 : (query != TDP_QUERY_WITHIN || !(within >= 0.f))) return TDP_ERR_ARG;
+    std::unique_ptr<Request> r(new Request());
+    r->t_submit = Clock::now();
+    r->raw = (const uint8_t*)raw_dt;
+    r->len = len;
+    std::string err;
+    int rc = parse_raw_dt(r->raw, len, 0, r->host, err);
+    if (rc != TDP_OK) return rc;
+    const TileHost& h = r->host;
+    if (h.n_obj < 1) return TDP_ERR_FORMAT;
+    r->base = h.obj_data_off[0] - 8;  // the first object's first byte
+    r->span = h.obj_data_off[h.n_obj - 1] + h.obj_data_size[h.n_obj - 1] - r->base;
+    if (h.n_obj > S->p.arena_objects || h.n_vox > S->p.arena_voxels || r->span > S->p.max_request_bytes)
+        return TDP_ERR_ARG;
+    for (int l = 0; l < kNumLods; ++l)
+        if ((long)h.n_tris[l] > S->p.arena_tris) return TDP_ERR_ARG;
+    if ((long)h.n_vox * kNumLods > S->seg_cap) return TDP_ERR_ARG;
+    r->knn = query == TDP_QUERY_NN ? knn : 0;
+    r->within = query == TDP_QUERY_NN ? 0.f : within;
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stop) return TDP_ERR_STATE;
+    r->id = S->next_id++;
+    *id = r->id;
+    S->pending.push_back(r.get());
+    S->table.emplace(r->id, std::move(r));
+    S->cv.notify_all();
+    return TDP_OK;
+}
+
+int tdp_server_wait(tdp_server* S, uint64_t id, int timeout_ms, tdp_result** result, tdp_request_info* info) {
+    if (!S) return TDP_ERR_ARG;
+    if (result) *result = nullptr;
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->table.find(id);
+    if (it == S->table.end()) return TDP_ERR_ARG;
+    Request* r = it->second.get();
+    auto done = [&] { return r->done; };
+    if (timeout_ms < 0) S->cv.wait(lk, done);
+    else if (!S->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), done)) return TDP_ERR_TIMEOUT;
+    if (info) {
+        info->queue_ms = r->batch >= 0 ? ms_between(r->t_submit, r->t_start) : 0.0;
+        info->latency_ms = ms_between(r->t_submit, r->t_done);
+        info->batch = r->batch;
+        info->batch_requests = r->batch_requests;
+        info->status = r->status;
+    }
+    const int status = r->status;
+    if (status == TDP_OK && result) *result = r->res.release();
+    S->table.erase(it);
+    return status;
+}
+
+int tdp_server_get_stats(const tdp_server* S, tdp_server_stats* o) {
+    if (!S || !o) return TDP_ERR_ARG;
+    std::lock_guard<std::mutex> lk(const_cast<tdp_server*>(S)->mu);
+    o->batches = S->batches;
+    o->requests = S->completed;
+    o->failed = S->failed;
+    o->busy_ms = S->busy_ms;
+    return TDP_OK;
+}
+
+int tdp_server_destroy(tdp_server* S) {
+    if (!S) return TDP_ERR_ARG;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        S->cv.notify_all();
+    }
+    if (S->admitter.joinable()) S->admitter.join();
+    if (S->executor.joinable()) S->executor.join();
+    tdp_ctx* ctx = S->ctx;
+    cudaSetDevice(ctx->device);
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        for (Request* r : S->pending)
+            if (!r->done) finish(S, r, TDP_ERR_STATE);
+        for (Arena& a : S->arena)
+            for (Request* r : a.reqs)
+                if (!r->done) finish(S, r, TDP_ERR_STATE);
+        S->cv.notify_all();
+    }
+    for (Arena& a : S->arena) {
+        if (a.up) cudaStreamSynchronize(a.up);
+        tdp_tile& T = a.tile;
+        dfree(ctx, T.vox); dfree(ctx, T.obj_vox); dfree(ctx, T.obj_hd); dfree(ctx, T.obj_phd);
+        for (int l = 0; l < kNumLods; ++l) { dfree(ctx, T.tri[l]); dfree(ctx, T.vtri[l]); }
+        dfree(ctx, a.stage);
+        dfree(ctx, a.dsegs);
+        if (a.ready) cudaEventDestroy(a.ready);
+        if (a.up) cudaStreamDestroy(a.up);
+    }
+    delete S;
+    return TDP_OK;
+}
+
+}  // extern "C"

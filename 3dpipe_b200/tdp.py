@@ -190,7 +190,7 @@ class TileInfo(C.Structure):
 class JoinParams(C.Structure):
     _fields_ = [("query", C.c_int), ("knn", C.c_int), ("within_dist", C.c_float), ("lods", C.c_int * 8),
                 ("n_lods", C.c_int), ("hausdorff_level", C.c_int), ("form", C.c_int),
-                ("exact_distances", C.c_int)]
+                ("exact_distances", C.c_int), ("obj_knn", C.c_void_p), ("obj_within", C.c_void_p)]
 
 
 def _bind_join(L):
@@ -276,14 +276,25 @@ def _join_params(query, knn, within, lods, hausdorff_level, form) -> JoinParams:
 
 
 def _join(self, tile1: Tile, tile2: Tile | None, query: str = "nn", knn: int = 1, within: float = 1000.0,
-          lods=None, hausdorff_level: int = 2, form: int = FORM_TUNED, exact_distances: bool = False):
+          lods=None, hausdorff_level: int = 2, form: int = FORM_TUNED, exact_distances: bool = False,
+          obj_knn=None, obj_within=None):
     """tdbase join on resident tiles; returns (query_ids, result_ids, dist) sorted by (query, result).
 
     dist is float32 (each pair's upper bound when decided) unless
-    exact_distances is set: then float64 exact LOD-100 distances."""
+    exact_distances is set: then float64 exact LOD-100 distances.  obj_knn /
+    obj_within (one entry per tile-1 object) give every query object its own
+    query: K > 0 for kNN, 0 for within at obj_within[i]."""
     L = lib()
     p = _join_params(query, knn, within, lods, hausdorff_level, form)
     p.exact_distances = int(bool(exact_distances))
+    keep = []
+    if obj_knn is not None:
+        ok = np.ascontiguousarray(obj_knn, np.int32)
+        ow = np.ascontiguousarray(np.zeros(len(ok)) if obj_within is None else obj_within, np.float32)
+        if ok.shape != ow.shape:
+            raise ValueError("obj_knn and obj_within need one entry per query object")
+        keep = [ok, ow]
+        p.obj_knn, p.obj_within = ok.ctypes.data, ow.ctypes.data
     r = C.c_void_p()
     self.check(L.tdp_join(self._h, tile1.handle, None if tile2 is None else tile2.handle, C.byref(p), C.byref(r)))
     try:
@@ -309,7 +320,112 @@ Context.join = _join
 
 EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates", "tdp_ctx_stream",
              "tdp_refine_config_count", "tdp_refine_config_info", "tdp_set_refine_config", "tdp_get_refine_config",
-             "tdp_autotune", "tdp_result_copy_f64"]
+             "tdp_autotune", "tdp_result_copy_f64", "tdp_server_default_params", "tdp_server_create",
+             "tdp_server_submit", "tdp_server_wait", "tdp_server_get_stats", "tdp_server_destroy"]
+
+
+class ServerParams(C.Structure):
+    _fields_ = [("arena_objects", C.c_long), ("arena_voxels", C.c_long), ("arena_tris", C.c_long),
+                ("max_request_bytes", C.c_size_t), ("lods", C.c_int * 8), ("n_lods", C.c_int),
+                ("hausdorff_level", C.c_int), ("form", C.c_int)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("latency_ms", C.c_double), ("batch", C.c_long),
+                ("batch_requests", C.c_int), ("status", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("batches", C.c_long), ("requests", C.c_long), ("failed", C.c_long), ("busy_ms", C.c_double)]
+
+
+class Server:
+    """Continuous-batching request loop over a resident tile 2 (tdp_server_*).
+
+    submit() takes a RAW .dt tile of query objects plus its own query and
+    returns at once; wait() returns that request's (query ids, result ids,
+    distances) with the request's own object ids, and its latency record.
+    The context belongs to the server until close()."""
+
+    def __init__(self, ctx: "Context", tile2: "Tile", **params):
+        L = lib()
+        P = C.c_void_p
+        L.tdp_server_default_params.argtypes = [C.POINTER(ServerParams)]
+        L.tdp_server_default_params.restype = None
+        L.tdp_server_create.argtypes = [P, P, C.POINTER(ServerParams), C.POINTER(P)]
+        L.tdp_server_submit.argtypes = [P, P, C.c_size_t, C.c_int, C.c_int, C.c_float, C.POINTER(C.c_uint64)]
+        L.tdp_server_wait.argtypes = [P, C.c_uint64, C.c_int, C.POINTER(P), C.POINTER(RequestInfo)]
+        L.tdp_server_get_stats.argtypes = [P, C.POINTER(ServerStats)]
+        L.tdp_server_destroy.argtypes = [P]
+        p = ServerParams()
+        L.tdp_server_default_params(C.byref(p))
+        for k, v in params.items():
+            if k == "lods":
+                p.n_lods = len(v)
+                for i, l in enumerate(v):
+                    p.lods[i] = l
+            else:
+                setattr(p, k, v)
+        h = C.c_void_p()
+        ctx.check(L.tdp_server_create(ctx.handle, tile2.handle, C.byref(p), C.byref(h)))
+        self._ctx, self._tile2, self._h = ctx, tile2, h
+        self._bufs = {}
+
+    def submit(self, raw: np.ndarray, query: str = "nn", knn: int = 1, within: float = 0.0) -> int:
+        raw = np.ascontiguousarray(raw, np.uint8)
+        rid = C.c_uint64()
+        rc = lib().tdp_server_submit(self._h, _ptr(raw), raw.size, QUERY_NN if query == "nn" else QUERY_WITHIN,
+                                     int(knn), float(within), C.byref(rid))
+        if rc != TDP_OK:
+            raise TdpError(rc, "request rejected")
+        self._bufs[rid.value] = raw  # the bytes must live until the request completes
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: int = -1):
+        """(q, t, d, info) of a finished request; None if timeout_ms ran out."""
+        L = lib()
+        r = C.c_void_p()
+        info = RequestInfo()
+        rc = L.tdp_server_wait(self._h, rid, int(timeout_ms), C.byref(r), C.byref(info))
+        if rc == 5:  # TDP_ERR_TIMEOUT
+            return None
+        self._bufs.pop(rid, None)
+        if rc != TDP_OK:
+            raise TdpError(rc, "request failed")
+        try:
+            n = C.c_long()
+            L.tdp_result_count(r, C.byref(n))
+            q = np.empty(n.value, np.int32)
+            t = np.empty(n.value, np.int32)
+            d = np.empty(n.value, np.float32)
+            L.tdp_result_copy(r, _ptr(q), _ptr(t), _ptr(d))
+        finally:
+            L.tdp_result_free(r)
+        return q, t, d, {"queue_ms": info.queue_ms, "latency_ms": info.latency_ms, "batch": info.batch,
+                         "batch_requests": info.batch_requests}
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        lib().tdp_server_get_stats(self._h, C.byref(s))
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tdp_server_destroy(self._h)
+            self._h = None
+            self._bufs.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def refine_configs():

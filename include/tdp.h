@@ -153,6 +153,12 @@ typedef struct {
     int exact_distances;   /* 1: give every result its LOD-100 distance in FP64
                               (tdp_result_copy_f64); the reference reports ids
                               only, so this stage has no counterpart (default 0) */
+    const int *obj_knn;    /* NULL, or one entry per tile-1 object: K (> 0, that
+                              object is a kNN query) or 0 (a within query at
+                              distance obj_within[i]).  Lets one join carry a
+                              batch of different requests; query/knn/within_dist
+                              are then ignored.  No reference counterpart. */
+    const float *obj_within;
 } tdp_join_params;
 void tdp_join_default_params(tdp_join_params *p);
 int tdp_join(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, const tdp_join_params *p,
@@ -173,6 +179,67 @@ int tdp_result_free(tdp_result *r);
  * receives tdp_refine_config_count() refine times in milliseconds. */
 int tdp_autotune(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, const tdp_join_params *params,
                  double *ms_per_config, int *best);
+
+/* ---- serving ------------------------------------------------------------------
+ * A request loop over one resident tile 2 (for example the vessel tile): each
+ * request is a RAW .dt tile of query objects with its own query (kNN with its
+ * own K, or within with its own distance).  Requests are admitted into one of
+ * two device arenas as long as they fit its capacity (admission by memory);
+ * while the GPU joins one arena, newly arriving requests are copied into the
+ * other on a separate stream, and when the running batch ends the next one
+ * starts with every request admitted meanwhile (continuous batching).  A batch
+ * is one tdp_join whose query objects carry their requests' own queries
+ * (obj_knn / obj_within), so each request's result equals the result of
+ * tdp_join on that request alone.
+ * The reference runs one join per invocation of `tdbase join`
+ * (src/tools/tdbase.cpp:482-549) and has no request loop: no counterpart.
+ *
+ * The server takes over the context: no other call may use `ctx` until
+ * tdp_server_destroy.  The bytes passed to tdp_server_submit must stay valid
+ * until that request completes (tdp_server_wait returned TDP_OK or an error). */
+typedef struct tdp_server tdp_server;
+typedef struct {
+    long arena_objects;        /* query objects one arena holds        (default 65536)    */
+    long arena_voxels;         /* voxels one arena holds               (default 2^20)     */
+    long arena_tris;           /* triangles per LOD one arena holds    (default 2^25)     */
+    size_t max_request_bytes;  /* largest RAW request accepted         (default 1 GiB)    */
+    int lods[8];               /* LOD list as in tdp_join_params (n_lods = 0: all)        */
+    int n_lods;
+    int hausdorff_level;       /* default 2 */
+    int form;                  /* default TDP_FORM_TUNED */
+} tdp_server_params;
+typedef struct {
+    double queue_ms;           /* submit -> its batch started                              */
+    double latency_ms;         /* submit -> result ready                                   */
+    long batch;                /* index of the batch that served it                        */
+    int batch_requests;        /* requests in that batch                                    */
+    int status;                /* TDP_OK, or why the request failed                        */
+} tdp_request_info;
+typedef struct {
+    long batches;
+    long requests;             /* completed (including failed)                             */
+    long failed;
+    double busy_ms;            /* wall time the executor spent in joins                    */
+} tdp_server_stats;
+void tdp_server_default_params(tdp_server_params *p);
+/* allocates both arenas in the context (counted against its budget) */
+int tdp_server_create(tdp_ctx *ctx, const tdp_tile *tile2, const tdp_server_params *p, tdp_server **out);
+/* query: TDP_QUERY_NN (knn >= 1) or TDP_QUERY_WITHIN (within >= 0).  The bytes
+ * are parsed here: TDP_ERR_FORMAT for malformed bytes, TDP_ERR_ARG for a request
+ * larger than an arena or than max_request_bytes. */
+int tdp_server_submit(tdp_server *srv, const void *raw_dt, size_t len, int query, int knn, float within,
+                      uint64_t *request_id);
+/* Waits up to timeout_ms (< 0: no limit) for the request; TDP_ERR_TIMEOUT if it
+ * is not done yet (call again).  On completion returns its status and, when
+ * TDP_OK, the result with the request's own object ids (tdp_result_* calls;
+ * free it with tdp_result_free).  info may be NULL.  A request id can be
+ * waited for successfully once. */
+int tdp_server_wait(tdp_server *srv, uint64_t request_id, int timeout_ms, tdp_result **result,
+                    tdp_request_info *info);
+int tdp_server_get_stats(const tdp_server *srv, tdp_server_stats *out);
+/* Stops admitting, runs the batches already admitted, fails the requests not
+ * yet admitted (TDP_ERR_STATE), frees the arenas and hands the context back. */
+int tdp_server_destroy(tdp_server *srv);
 
 /* ---- refine seam ------------------------------------------------------------
  * Drop-in for the reference's batched refine (MeshDist_batch_gpu_op_shm_flat_stream):

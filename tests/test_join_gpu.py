@@ -215,3 +215,35 @@ def test_exact_distances_match_fp64_oracle(pkg, ctx, gpu_tiles, name):
         # the exact one (within its error band)
         if level == 2:
             assert np.all(d2.astype(np.float64) >= d * (1 - 1e-5) - 1e-4)
+
+
+def test_mixed_queries_equal_separate_joins(pkg, ctx, gpu_tiles):
+    """One join whose query objects carry different queries (kNN with several
+    K, within with several tau) returns, for every object, exactly what a join
+    of that object's own query returns: same ids, same distances."""
+    nb, vb = tiles(6, 12, 101)
+    T1, T2 = gpu_tiles(6, 12, 101)
+    n1 = T1.info()["n_objects"]
+    specs = [("nn", 1, 0.0), ("nn", 3, 0.0), ("nn", 5, 0.0), ("within", 0, 60.0), ("within", 0, 150.0)]
+    rng = np.random.default_rng(7)
+    which = rng.integers(0, len(specs), n1)
+    ok = np.array([specs[w][1] for w in which], np.int32)
+    ow = np.array([specs[w][2] for w in which], np.float32)
+    for form in (pkg.FORM_PLAIN, pkg.FORM_TUNED):
+        q, t, d = ctx.join(T1, T2, form=form, obj_knn=ok, obj_within=ow)
+        want_q, want_t, want_d = [], [], []
+        for k, (query, K, tau) in enumerate(specs):
+            aq, at, ad = ctx.join(T1, T2, query=query, knn=max(K, 1), within=tau, form=form)
+            m = which[aq] == k
+            want_q.append(aq[m]); want_t.append(at[m]); want_d.append(ad[m])
+        wq, wt, wd = (np.concatenate(x) for x in (want_q, want_t, want_d))
+        o = np.lexsort((wt, wq))
+        np.testing.assert_array_equal(q, wq[o])
+        np.testing.assert_array_equal(t, wt[o])
+        np.testing.assert_array_equal(d, wd[o])
+        # every kNN object reports exactly its own K
+        for k, (query, K, tau) in enumerate(specs):
+            if query == "nn":
+                objs = np.nonzero(which == k)[0]
+                counts = np.bincount(q, minlength=n1)[objs]
+                assert np.all(counts == K)
