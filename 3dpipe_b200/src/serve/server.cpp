@@ -3,14 +3,21 @@
 //
 // Two device arenas hold the query objects of the admitted requests.  An
 // arena is a tdp_tile whose device arrays are allocated once at full
-// capacity; a request is appended at the arena's running offsets (objects,
-// voxels, triangles per LOD), on the arena's own stream: its RAW bytes are
-// copied to a device staging buffer and unpacked by the tile-upload kernel.
+// capacity.  A request's RAW bytes, and its metadata in request-local
+// offsets (voxel records, CSR offsets, Hausdorff values, unpack segments,
+// built on the host into a page-locked block), are first copied to one of
+// two device staging areas that belong to no arena (the slow PCIe part; the
+// next request's copy runs while the current one is appended).  Appending is
+// then device work only, on the arena's stream: a commit kernel writes the
+// metadata at the arena's running offsets (objects, voxels, triangles per
+// LOD) and the tile-upload kernel unpacks the triangles from the staging area.
+// No host-to-device copy happens while an arena is being appended to, so an
+// append never queues behind a staging copy on the copy engine.
 //
-//   admitter thread   takes requests in arrival order and appends each to the
-//                     arena being filled while it fits (admission by memory);
-//                     a request that does not fit seals the arena and waits
-//                     for the other one;
+//   admitter thread   takes requests in arrival order, stages each one, then
+//                     appends it to the arena being filled if it fits
+//                     (admission by memory); a request that does not fit
+//                     seals the arena and waits for the other one;
 //   executor thread   whenever it is idle, takes the sealed arena or else the
 //                     filling one (if it holds a request), waits on the
 //                     arena's upload event, runs ONE tdp_join over all of its
@@ -35,6 +42,7 @@
 #include <vector>
 
 #include "../../csrc/ctx.cuh"
+#include "../../csrc/serve_kernels.cuh"
 #include "../../csrc/tile_kernels.cuh"
 #include "join/result.h"
 #include "storage/dev_tile.h"
@@ -73,16 +81,34 @@ enum class ArenaState { kFree, kFilling, kSealed, kRunning };
 struct Arena {
     tdp_tile tile;                 // device arrays at capacity; counts grow with appends
     uint32_t n_tri[kNumLods] = {};
-    std::vector<float4> hvox;      // host copy of the voxel records (3 float4 per voxel)
     std::vector<Request*> reqs;
     ArenaState state = ArenaState::kFree;
     bool appending = false;
     cudaStream_t up = nullptr;
     cudaEvent_t ready = nullptr;
-    uint8_t* stage = nullptr;      // device staging of one request's RAW bytes
-    UnpackSeg* dsegs = nullptr;
-    std::vector<UnpackSeg> segs;
 };
+
+// Byte layout of one request's staged metadata (every section 16-byte aligned).
+struct MetaLayout {
+    size_t vox = 0, obj_vox = 0, obj_hd = 0, obj_phd = 0, vtri[kNumLods] = {}, segs = 0, bytes = 0;
+    long nseg = 0;
+};
+
+size_t up16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+MetaLayout meta_layout(long n, long nv, long nseg) {
+    MetaLayout L;
+    size_t o = 0;
+    L.vox = o; o = up16(o + (size_t)nv * 3 * sizeof(float4));
+    L.obj_vox = o; o = up16(o + (size_t)(n + 1) * 4);
+    L.obj_hd = o; o = up16(o + (size_t)n * kNumLods * 4);
+    L.obj_phd = o; o = up16(o + (size_t)n * kNumLods * 4);
+    for (int l = 0; l < kNumLods; ++l) { L.vtri[l] = o; o = up16(o + (size_t)(nv + 1) * 4); }
+    L.segs = o; o = up16(o + (size_t)nseg * sizeof(UnpackSeg));
+    L.bytes = o;
+    L.nseg = nseg;
+    return L;
+}
 
 }  // namespace
 }  // namespace tdp
@@ -93,15 +119,21 @@ struct tdp_server {
     tdp_ctx* ctx = nullptr;
     const tdp_tile* t2 = nullptr;
     tdp_server_params p{};
-    long seg_cap = 0;
     Arena arena[2];
+    uint8_t* stage[2] = {};           // device staging of RAW bytes (double-buffered)
+    uint8_t* dmeta[2] = {};           // device staging of the metadata
+    uint8_t* hmeta[2] = {};           // page-locked host metadata blocks
+    size_t meta_cap = 0;
+    MetaLayout meta[2];
+    cudaEvent_t staged[2] = {};       // a stage's copies finished
+    cudaStream_t copy = nullptr;      // stream of the staging copies
     std::mutex mu;
     std::condition_variable cv;
     std::deque<Request*> pending;
     std::unordered_map<uint64_t, std::unique_ptr<Request>> table;
     uint64_t next_id = 1;
     long batches = 0, completed = 0, failed = 0;
-    double busy_ms = 0;
+    double busy_ms = 0, upload_ms = 0, upload_bytes = 0;
     bool stop = false;
     std::thread admitter, executor;
 };
@@ -112,14 +144,12 @@ void reset_arena(Arena& a) {
     TileHost& H = a.tile.host;
     a.tile.n_obj = a.tile.n_vox = 0;
     H.n_obj = H.n_vox = 0;
-    H.obj_box.clear(); H.obj_xf.clear(); H.obj_hd.clear(); H.obj_phd.clear(); H.vox_box.clear();
-    H.obj_vox_off.assign(1, 0);
+    H.obj_box.clear();
+    H.obj_xf.clear();
     for (int l = 0; l < kNumLods; ++l) {
-        a.tile.h_vtri[l].assign(1, 0);
         a.n_tri[l] = 0;
         H.n_tris[l] = 0;
     }
-    a.hvox.clear();
     a.reqs.clear();
 }
 
@@ -131,61 +161,84 @@ bool fits(const tdp_server* S, const Arena& a, const Request& r) {
     return true;
 }
 
-// Append one request's objects at the arena's offsets (admitter thread; the
-// arena is not visible to the executor while `appending` is set).
-int append(tdp_server* S, Arena& a, Request& r) {
+// Build r's metadata (request-local offsets) into hmeta[j] and start copying
+// it and r's RAW bytes into staging area j (copy stream, asynchronous).
+// Returns TDP_OK or an error for malformed triangle blocks.
+int start_copy(tdp_server* S, Request* r, int j) {
+    const TileHost& h = r->host;
+    const long n = h.n_obj, nv = h.n_vox;
+    long nseg = 0;
+    for (int l = 0; l < kNumLods; ++l)
+        for (long v = 0; v < nv; ++v) nseg += h.vox_cnt[l][v] != 0;
+    const MetaLayout L = meta_layout(n, nv, nseg);
+    if (L.bytes > S->meta_cap) return TDP_ERR_ARG;
+    uint8_t* m = S->hmeta[j];
+    float4* vox = (float4*)(m + L.vox);
+    for (long v = 0; v < nv; ++v) {
+        const float* b = &h.vox_box[9 * v];
+        vox[3 * v + 0] = make_float4(b[0], b[1], b[2], 0.f);
+        vox[3 * v + 1] = make_float4(b[3], b[4], b[5], 0.f);
+        vox[3 * v + 2] = make_float4(b[6], b[7], b[8], 0.f);
+    }
+    std::memcpy(m + L.obj_vox, h.obj_vox_off.data(), (size_t)(n + 1) * 4);
+    std::memcpy(m + L.obj_hd, h.obj_hd.data(), (size_t)n * kNumLods * 4);
+    std::memcpy(m + L.obj_phd, h.obj_phd.data(), (size_t)n * kNumLods * 4);
+    UnpackSeg* seg = (UnpackSeg*)(m + L.segs);
+    long k = 0;
+    for (int l = 0; l < kNumLods; ++l) {
+        uint32_t* vt = (uint32_t*)(m + L.vtri[l]);
+        vt[0] = 0;
+        for (long v = 0; v < nv; ++v) {
+            const uint32_t c = h.vox_cnt[l][v];
+            vt[v + 1] = vt[v] + c;
+            if (!c) continue;
+            const uint64_t src = h.vox_byte_off[l][v] - r->base;
+            if ((src & 3u) || src + (uint64_t)c * 44 > r->span) return TDP_ERR_FORMAT;
+            seg[k++] = UnpackSeg{src, vt[v], c | ((uint32_t)l << 24)};  // dst local to the request
+        }
+    }
+    S->meta[j] = L;
+    if (cudaMemcpyAsync(S->dmeta[j], m, L.bytes, cudaMemcpyHostToDevice, S->copy) != cudaSuccess ||
+        cudaMemcpyAsync(S->stage[j], r->raw + r->base, r->span, cudaMemcpyHostToDevice, S->copy) != cudaSuccess ||
+        cudaEventRecord(S->staged[j], S->copy) != cudaSuccess)
+        return TDP_ERR_CUDA;
+    return TDP_OK;
+}
+
+// Append the request staged in area j at the arena's offsets: device work on
+// the arena's stream only (admitter thread; the arena is not visible to the
+// executor while `appending` is set).
+int append(tdp_server* S, Arena& a, Request& r, int j) {
     const TileHost& h = r.host;
     TileHost& H = a.tile.host;
     const long o0 = a.tile.n_obj, v0 = a.tile.n_vox, n = h.n_obj, nv = h.n_vox;
     uint32_t t0[kNumLods];
     for (int l = 0; l < kNumLods; ++l) t0[l] = a.n_tri[l];
-    // host metadata (capacity reserved at creation: no reallocation)
+    const MetaLayout& L = S->meta[j];
+    const uint8_t* m = S->dmeta[j];
+    ArenaMeta am{(const float4*)(m + L.vox), (const uint32_t*)(m + L.obj_vox), (const float*)(m + L.obj_hd),
+                 (const float*)(m + L.obj_phd), {}};
+    ArenaDst ad{a.tile.vox, a.tile.obj_vox, a.tile.obj_hd, a.tile.obj_phd, {}};
+    float4* tri_at[kNumLods];
+    for (int l = 0; l < kNumLods; ++l) {
+        am.vtri[l] = (const uint32_t*)(m + L.vtri[l]);
+        ad.vtri[l] = a.tile.vtri[l];
+        tri_at[l] = a.tile.tri[l] + 3 * (size_t)t0[l];  // segments carry request-local destinations
+    }
+    cudaError_t e = launch_arena_commit(am, ad, n, nv, o0, v0, t0, S->ctx->num_sms, a.up);
+    if (e == cudaSuccess)
+        e = launch_unpack(S->stage[j], (const UnpackSeg*)(m + L.segs), (int)L.nseg, tri_at, S->ctx->num_sms, a.up);
+    if (e == cudaSuccess) e = cudaEventRecord(a.ready, a.up);
+    // the staging area is refilled two requests later: finish with it now
+    if (e == cudaSuccess) e = cudaStreamSynchronize(a.up);
+    if (e != cudaSuccess) return TDP_ERR_CUDA;
+    // host side of the arena: what the join reads from the host
     H.obj_box.insert(H.obj_box.end(), h.obj_box.begin(), h.obj_box.end());
     H.obj_xf.insert(H.obj_xf.end(), h.obj_xf.begin(), h.obj_xf.end());
-    H.obj_hd.insert(H.obj_hd.end(), h.obj_hd.begin(), h.obj_hd.end());
-    H.obj_phd.insert(H.obj_phd.end(), h.obj_phd.begin(), h.obj_phd.end());
-    H.vox_box.insert(H.vox_box.end(), h.vox_box.begin(), h.vox_box.end());
-    for (long i = 1; i <= n; ++i) H.obj_vox_off.push_back((uint32_t)(v0 + h.obj_vox_off[i]));
-    for (long v = 0; v < nv; ++v) {
-        const float* b = &h.vox_box[9 * v];
-        a.hvox.push_back(make_float4(b[0], b[1], b[2], 0.f));
-        a.hvox.push_back(make_float4(b[3], b[4], b[5], 0.f));
-        a.hvox.push_back(make_float4(b[6], b[7], b[8], 0.f));
-    }
-    a.segs.clear();
     for (int l = 0; l < kNumLods; ++l) {
-        std::vector<uint32_t>& vt = a.tile.h_vtri[l];
-        for (long v = 0; v < nv; ++v) {
-            const uint32_t c = h.vox_cnt[l][v];
-            const uint32_t dst = vt.back();
-            vt.push_back(dst + c);
-            if (!c) continue;
-            const uint64_t src = h.vox_byte_off[l][v] - r.base;
-            if ((src & 3u) || src + (uint64_t)c * 44 > r.span) return TDP_ERR_FORMAT;
-            a.segs.push_back(UnpackSeg{src, dst, c | ((uint32_t)l << 24)});
-        }
         a.n_tri[l] = t0[l] + (uint32_t)h.n_tris[l];
         H.n_tris[l] = a.n_tri[l];
     }
-    if ((long)a.segs.size() > S->seg_cap) return TDP_ERR_ARG;
-    cudaStream_t s = a.up;
-    cudaError_t e = cudaSuccess;
-    auto cp = [&](void* dst, const void* src, size_t bytes) {
-        if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
-    };
-    cp(a.tile.vox + 3 * (size_t)v0, a.hvox.data() + 3 * (size_t)v0, (size_t)nv * 3 * sizeof(float4));
-    cp(a.tile.obj_vox + o0 + 1, H.obj_vox_off.data() + o0 + 1, (size_t)n * 4);
-    cp(a.tile.obj_hd + (size_t)o0 * kNumLods, H.obj_hd.data() + (size_t)o0 * kNumLods, (size_t)n * kNumLods * 4);
-    cp(a.tile.obj_phd + (size_t)o0 * kNumLods, H.obj_phd.data() + (size_t)o0 * kNumLods, (size_t)n * kNumLods * 4);
-    for (int l = 0; l < kNumLods; ++l)
-        cp(a.tile.vtri[l] + v0 + 1, a.tile.h_vtri[l].data() + v0 + 1, (size_t)nv * 4);
-    cp(a.stage, r.raw + r.base, r.span);
-    cp(a.dsegs, a.segs.data(), a.segs.size() * sizeof(UnpackSeg));
-    if (e == cudaSuccess) e = launch_unpack(a.stage, a.dsegs, (int)a.segs.size(), a.tile.tri, S->ctx->num_sms, s);
-    if (e == cudaSuccess) e = cudaEventRecord(a.ready, s);
-    // the staging buffers are reused by the next append: finish this one first
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return TDP_ERR_CUDA;
     a.tile.n_obj = H.n_obj = o0 + n;
     a.tile.n_vox = H.n_vox = v0 + nv;
     return TDP_OK;
@@ -202,36 +255,88 @@ void finish(tdp_server* S, Request* r, int status) {
 void admitter_loop(tdp_server* S) {
     cudaSetDevice(S->ctx->device);
     std::unique_lock<std::mutex> lk(S->mu);
+    Request* cur = nullptr;  // request whose bytes are in (or on their way to) staging area j
+    int j = 0;
+    Clock::time_point t_cur;
+    int cur_rc = TDP_OK;
     for (;;) {
-        Arena* a = nullptr;
-        S->cv.wait(lk, [&] {
-            if (S->stop) return true;
-            if (S->pending.empty()) return false;
-            for (Arena& x : S->arena)
-                if (x.state == ArenaState::kFilling) { a = &x; return true; }
-            for (Arena& x : S->arena)
-                if (x.state == ArenaState::kFree) { a = &x; return true; }
-            return false;
-        });
-        if (S->stop) return;
-        Request* r = S->pending.front();
-        if (a->state == ArenaState::kFree) a->state = ArenaState::kFilling;
-        if (!fits(S, *a, *r)) {
-            // sealed: the executor takes it next; the request waits for the other arena
-            a->state = ArenaState::kSealed;
-            S->cv.notify_all();
-            continue;
+        if (!cur) {
+            S->cv.wait(lk, [&] { return S->stop || !S->pending.empty(); });
+            if (S->stop) return;
+            cur = S->pending.front();
+            S->pending.pop_front();
+            t_cur = Clock::now();
+            lk.unlock();
+            cur_rc = start_copy(S, cur, j);
+            lk.lock();
         }
-        S->pending.pop_front();
-        a->appending = true;
-        r->o0 = a->tile.n_obj;
+        // 1. the next request's bytes go to the other stage while this one is appended
+        Request* nxt = nullptr;
+        int nxt_rc = TDP_OK;
+        Clock::time_point t_nxt;
+        if (!S->pending.empty()) {
+            nxt = S->pending.front();
+            S->pending.pop_front();
+        }
         lk.unlock();
-        const int rc = append(S, *a, *r);
+        if (nxt) {
+            t_nxt = Clock::now();
+            nxt_rc = start_copy(S, nxt, 1 - j);
+        }
+        if (cur_rc == TDP_OK && cudaEventSynchronize(S->staged[j]) != cudaSuccess) cur_rc = TDP_ERR_CUDA;
         lk.lock();
-        a->appending = false;
-        if (rc == TDP_OK) a->reqs.push_back(r);
-        else finish(S, r, rc);
-        S->cv.notify_all();
+        Request* r = cur;
+        if (cur_rc != TDP_OK) {
+            finish(S, r, cur_rc);
+            S->cv.notify_all();
+        } else {
+            // 2. an arena with room: the one being filled, else a free one
+            Arena* a = nullptr;
+            for (;;) {
+                S->cv.wait(lk, [&] {
+                    if (S->stop) return true;
+                    for (Arena& x : S->arena)
+                        if (x.state == ArenaState::kFilling) { a = &x; return true; }
+                    for (Arena& x : S->arena)
+                        if (x.state == ArenaState::kFree) { a = &x; return true; }
+                    return false;
+                });
+                if (S->stop) break;
+                if (a->state == ArenaState::kFree) a->state = ArenaState::kFilling;
+                if (fits(S, *a, *r)) break;
+                a->state = ArenaState::kSealed;  // the executor takes it next
+                a = nullptr;
+                S->cv.notify_all();
+            }
+            if (!a) {
+                finish(S, r, TDP_ERR_STATE);
+                if (nxt) {
+                    lk.unlock();
+                    cudaEventSynchronize(S->staged[1 - j]);  // its copy may still read the caller's bytes
+                    lk.lock();
+                    finish(S, nxt, TDP_ERR_STATE);
+                }
+                S->cv.notify_all();
+                return;
+            }
+            // 3. metadata and unpack into the arena (short)
+            a->appending = true;
+            r->o0 = a->tile.n_obj;
+            lk.unlock();
+            const int rc = append(S, *a, *r, j);
+            const double up_ms = ms_between(t_cur, Clock::now());
+            lk.lock();
+            S->upload_ms += up_ms;
+            S->upload_bytes += (double)r->span;
+            a->appending = false;
+            if (rc == TDP_OK) a->reqs.push_back(r);
+            else finish(S, r, rc);
+            S->cv.notify_all();
+        }
+        cur = nxt;
+        cur_rc = nxt_rc;
+        t_cur = t_nxt;
+        j = 1 - j;
     }
 }
 
@@ -332,7 +437,7 @@ int tdp_server_create(tdp_ctx* ctx, const tdp_tile* t2, const tdp_server_params*
     S->ctx = ctx;
     S->t2 = t2;
     S->p = *p;
-    S->seg_cap = p->arena_voxels * kNumLods;
+    S->meta_cap = meta_layout(p->arena_objects, p->arena_voxels, p->arena_voxels * kNumLods).bytes;
     for (Arena& a : S->arena) {
         tdp_tile& T = a.tile;
         T.device = ctx->device;
@@ -344,9 +449,7 @@ int tdp_server_create(tdp_ctx* ctx, const tdp_tile* t2, const tdp_server_params*
         bool ok = alloc((void**)&T.vox, (size_t)p->arena_voxels * 3 * sizeof(float4)) &&
                   alloc((void**)&T.obj_vox, (size_t)(p->arena_objects + 1) * 4) &&
                   alloc((void**)&T.obj_hd, (size_t)p->arena_objects * kNumLods * 4) &&
-                  alloc((void**)&T.obj_phd, (size_t)p->arena_objects * kNumLods * 4) &&
-                  alloc((void**)&a.stage, p->max_request_bytes + 16) &&
-                  alloc((void**)&a.dsegs, (size_t)S->seg_cap * sizeof(UnpackSeg));
+                  alloc((void**)&T.obj_phd, (size_t)p->arena_objects * kNumLods * 4);
         for (int l = 0; ok && l < kNumLods; ++l)
             ok = alloc((void**)&T.tri[l], (size_t)p->arena_tris * 3 * sizeof(float4)) &&
                  alloc((void**)&T.vtri[l], (size_t)(p->arena_voxels + 1) * 4);
@@ -362,18 +465,23 @@ int tdp_server_create(tdp_ctx* ctx, const tdp_tile* t2, const tdp_server_params*
         TileHost& H = T.host;
         H.obj_box.reserve((size_t)p->arena_objects * 6);
         H.obj_xf.reserve((size_t)p->arena_objects * 3);
-        H.obj_hd.reserve((size_t)p->arena_objects * kNumLods);
-        H.obj_phd.reserve((size_t)p->arena_objects * kNumLods);
-        H.vox_box.reserve((size_t)p->arena_voxels * 9);
-        H.obj_vox_off.reserve((size_t)p->arena_objects + 1);
-        for (int l = 0; l < kNumLods; ++l) T.h_vtri[l].reserve((size_t)p->arena_voxels + 1);
-        a.hvox.reserve((size_t)p->arena_voxels * 3);
-        a.segs.reserve((size_t)S->seg_cap);
         reset_arena(a);
         if (cudaStreamSynchronize(a.up) != cudaSuccess) {
             tdp_server_destroy(S.release());
             return fail(ctx, TDP_ERR_CUDA, "serving arena set-up failed");
         }
+    }
+    if (dmalloc(ctx, (void**)&S->stage[0], p->max_request_bytes + 16) != cudaSuccess ||
+        dmalloc(ctx, (void**)&S->stage[1], p->max_request_bytes + 16) != cudaSuccess ||
+        dmalloc(ctx, (void**)&S->dmeta[0], S->meta_cap) != cudaSuccess ||
+        dmalloc(ctx, (void**)&S->dmeta[1], S->meta_cap) != cudaSuccess ||
+        cudaHostAlloc((void**)&S->hmeta[0], S->meta_cap, cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc((void**)&S->hmeta[1], S->meta_cap, cudaHostAllocDefault) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->staged[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->staged[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&S->copy, cudaStreamNonBlocking) != cudaSuccess) {
+        tdp_server_destroy(S.release());
+        return fail(ctx, TDP_ERR_NOMEM, "cannot allocate the serving staging buffer");
     }
     tdp_server* raw = S.release();
     raw->admitter = std::thread(admitter_loop, raw);
@@ -401,7 +509,6 @@ int tdp_server_submit(tdp_server* S, const void* raw_dt, size_t len, int query, 
         return TDP_ERR_ARG;
     for (int l = 0; l < kNumLods; ++l)
         if ((long)h.n_tris[l] > S->p.arena_tris) return TDP_ERR_ARG;
-    if ((long)h.n_vox * kNumLods > S->seg_cap) return TDP_ERR_ARG;
     r->knn = query == TDP_QUERY_NN ? knn : 0;
     r->within = query == TDP_QUERY_NN ? 0.f : within;
     std::lock_guard<std::mutex> lk(S->mu);
@@ -444,6 +551,8 @@ int tdp_server_get_stats(const tdp_server* S, tdp_server_stats* o) {
     o->requests = S->completed;
     o->failed = S->failed;
     o->busy_ms = S->busy_ms;
+    o->upload_ms = S->upload_ms;
+    o->upload_bytes = S->upload_bytes;
     return TDP_OK;
 }
 
@@ -472,11 +581,17 @@ int tdp_server_destroy(tdp_server* S) {
         tdp_tile& T = a.tile;
         dfree(ctx, T.vox); dfree(ctx, T.obj_vox); dfree(ctx, T.obj_hd); dfree(ctx, T.obj_phd);
         for (int l = 0; l < kNumLods; ++l) { dfree(ctx, T.tri[l]); dfree(ctx, T.vtri[l]); }
-        dfree(ctx, a.stage);
-        dfree(ctx, a.dsegs);
         if (a.ready) cudaEventDestroy(a.ready);
         if (a.up) cudaStreamDestroy(a.up);
     }
+    if (S->copy) cudaStreamSynchronize(S->copy);
+    for (int k = 0; k < 2; ++k) {
+        dfree(ctx, S->stage[k]);
+        dfree(ctx, S->dmeta[k]);
+        if (S->hmeta[k]) cudaFreeHost(S->hmeta[k]);
+        if (S->staged[k]) cudaEventDestroy(S->staged[k]);
+    }
+    if (S->copy) cudaStreamDestroy(S->copy);
     delete S;
     return TDP_OK;
 }

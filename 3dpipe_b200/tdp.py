@@ -324,6 +324,31 @@ EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates",
              "tdp_server_submit", "tdp_server_wait", "tdp_server_get_stats", "tdp_server_destroy"]
 
 
+def raw_object_offsets(raw: np.ndarray) -> np.ndarray:
+    """Byte offset of every object record of a RAW .dt tile, plus the end:
+    [n+1] int64.  Record layout (reference src/storage/tile_IO.cpp:79-172):
+    u64 data_size, data, u64 vnum, 5 x (hausdorff, proxy) floats, vnum x
+    (9 floats + 5 x (u64 offset, u64 count)), 3 floats of transform."""
+    import struct
+    mv = memoryview(np.ascontiguousarray(raw, np.uint8))
+    off, n = 1, len(mv)
+    out = [off]
+    while off < n:
+        (ds,) = struct.unpack_from("<Q", mv, off)
+        p = off + 8 + ds
+        (vn,) = struct.unpack_from("<Q", mv, p)
+        off = p + 8 + 40 + vn * 116 + 12
+        if off > n:
+            raise ValueError("truncated RAW tile")
+        out.append(off)
+    return np.asarray(out, np.int64)
+
+
+def raw_slice(raw: np.ndarray, offsets: np.ndarray, b: int, e: int) -> np.ndarray:
+    """A RAW .dt tile holding objects [b, e) of `raw` (its type byte first)."""
+    return np.concatenate([raw[:1], raw[offsets[b]:offsets[e]]])
+
+
 class ServerParams(C.Structure):
     _fields_ = [("arena_objects", C.c_long), ("arena_voxels", C.c_long), ("arena_tris", C.c_long),
                 ("max_request_bytes", C.c_size_t), ("lods", C.c_int * 8), ("n_lods", C.c_int),
@@ -336,7 +361,8 @@ class RequestInfo(C.Structure):
 
 
 class ServerStats(C.Structure):
-    _fields_ = [("batches", C.c_long), ("requests", C.c_long), ("failed", C.c_long), ("busy_ms", C.c_double)]
+    _fields_ = [("batches", C.c_long), ("requests", C.c_long), ("failed", C.c_long), ("busy_ms", C.c_double),
+                ("upload_ms", C.c_double), ("upload_bytes", C.c_double)]
 
 
 class Server:

@@ -172,6 +172,99 @@ def cpu_reference(nb, vb, steps, warmup, sample_queries, target_s=15.0):
             "seconds_per_sample": last[0], "tri_pairs_per_sample": last[1]}
 
 
+def run_serving(pkg, ctx, T2, nb, rates, per_rate_cap=600, seconds=3.0, pool_size=48, seed=20260005):
+    """Config 5: a served stream of query batches against the resident vessel
+    tile.  Requests are contiguous runs of 1-5000 nuclei (log-uniform) of the
+    200k-nuclei tile, 60 % kNN with K uniform in 1-50, 40 % within with tau
+    uniform in 50-800, Poisson arrivals at each rate for `seconds` (at most
+    per_rate_cap requests).  The batching server (tdp_server_*) is compared
+    with plain per-request launches (tile upload + tdp_join + free per request,
+    one at a time in arrival order) on the same arrival schedule.  Latency =
+    arrival to result ready, host clock."""
+    import threading
+    rng = np.random.default_rng(seed)
+    off = pkg.tdp.raw_object_offsets(nb)
+    n_total = len(off) - 1
+    pool, sizes = [], []
+    for _ in range(pool_size):
+        n = int(np.clip(np.round(np.exp(rng.uniform(0.0, np.log(5000.0)))), 1, 5000))
+        b = int(rng.integers(0, n_total - n + 1))
+        pool.append(pkg.tdp.raw_slice(nb, off, b, b + n))
+        sizes.append(n)
+    pinned = Pinned(pool)
+
+    def schedule(rate):
+        n = int(min(per_rate_cap, max(1, round(rate * seconds))))
+        t = np.cumsum(rng.exponential(1.0 / rate, n))
+        reqs = []
+        for k in range(n):
+            i = int(rng.integers(0, pool_size))
+            if rng.random() < 0.6:
+                reqs.append((t[k], i, "nn", int(rng.integers(1, 51)), 0.0))
+            else:
+                reqs.append((t[k], i, "within", 1, float(rng.uniform(50.0, 800.0))))
+        return reqs
+
+    def pct(v, q):
+        return float(np.percentile(np.asarray(v), q)) if v else None
+
+    out = []
+    for rate in rates:
+        reqs = schedule(rate)
+        nuclei = sum(sizes[i] for _, i, _, _, _ in reqs)
+        # batching server
+        with pkg.tdp.Server(ctx, T2) as srv:
+            ids = [None] * len(reqs)
+            t0 = time.perf_counter()
+
+            def submitter():
+                for k, (ta, i, query, K, tau) in enumerate(reqs):
+                    dt = t0 + ta - time.perf_counter()
+                    if dt > 0:
+                        time.sleep(dt)
+                    ids[k] = srv.submit(pool[i], query=query, knn=K, within=tau)
+
+            th = threading.Thread(target=submitter)
+            th.start()
+            th.join()
+            lat, batch_sizes = [], []
+            for rid in ids:
+                _, _, _, info = srv.wait(rid)
+                lat.append(info["latency_ms"])
+                batch_sizes.append(info["batch_requests"])
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+        batched = {"p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "requests_per_s": len(reqs) / wall,
+                   "nuclei_per_s": nuclei / wall, "batches": st["batches"],
+                   "mean_requests_per_batch": len(reqs) / max(1, st["batches"]),
+                   "join_busy_frac": st["busy_ms"] / 1e3 / wall, "h2d_gb_per_s": st["upload_bytes"] / wall / 1e9}
+        # plain per-request launches, same schedule
+        lat2 = []
+        t0 = time.perf_counter()
+        for ta, i, query, K, tau in reqs:
+            dt = t0 + ta - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            T1 = pkg.tdp.Tile(ctx, pool[i])
+            ctx.join(T1, T2, query=query, knn=K, within=tau)
+            T1.free()
+            lat2.append((time.perf_counter() - (t0 + ta)) * 1e3)
+        wall2 = time.perf_counter() - t0
+        per_request = {"p50_ms": pct(lat2, 50), "p99_ms": pct(lat2, 99), "requests_per_s": len(reqs) / wall2,
+                       "nuclei_per_s": nuclei / wall2}
+        log(f"serving rate {rate}/s: {len(reqs)} requests; batched p50 {batched['p50_ms']:.1f} p99 "
+            f"{batched['p99_ms']:.1f} ms; per-request p50 {per_request['p50_ms']:.1f} p99 {per_request['p99_ms']:.1f} ms")
+        out.append({"rate_per_s": rate, "requests": len(reqs), "nuclei": nuclei, "batched": batched,
+                    "per_request": per_request})
+    pinned.release()
+    return {"workload": "served stream on the resident 1000-vessel tile: requests of 1-5000 nuclei (log-uniform), "
+                        "60% kNN k~U[1,50], 40% within tau~U[50,800], Poisson arrivals",
+            "pool": f"{pool_size} request tiles sliced from the 200k-nuclei tile (page-locked), reused across arrivals "
+                    "with fresh query parameters",
+            "latency": "arrival to result ready (host clock); throughput over the whole run including the drain",
+            "rates": out}
+
+
 def run_reference_arm(a):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -204,6 +297,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1500, help="query nuclei in the CPU-baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream measurement")
+    ap.add_argument("--serve-rates", type=float, nargs="*", default=[200.0, 500.0, 1000.0, 2000.0])
     ap.add_argument("--vessels", type=int, default=None, help="smaller workload for profiling captures")
     ap.add_argument("--nuclei-per-vessel", type=int, default=None)
     a = ap.parse_args()
@@ -336,6 +431,11 @@ def main():
                 e2e_ms.append(e0.elapsed_time(e1))
         e2e_step = allmax(statistics.median(e2e_ms)) if e2e_ms else float("nan")
         e2e_value = tri / (e2e_step / 1e3) if e2e_ms else None
+
+        serving = None
+        if not a.no_serve and ws == 1:
+            T1.free()  # the serving arenas replace the resident query tile
+            serving = run_serving(pkg, ctx, T2, nb, a.serve_rates)
         del flush_buf
 
     pinned.release()
@@ -370,6 +470,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "tri-pairs/s", "ms_per_step": e2e_step,
                     "h2d_bytes_per_step": int(nb.size + vb.size), "d2h_bytes_per_step": int(d2h)},
             "exact_distances": exact,
+            "serving": serving,
             "gpu_launches": int(launches_t),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,

@@ -220,6 +220,9 @@ typedef struct {
     long requests;             /* completed (including failed)                             */
     long failed;
     double busy_ms;            /* wall time the executor spent in joins                    */
+    double upload_ms;          /* per request, staging copy start to arena append done,
+                                  summed (the copies of two requests overlap)              */
+    double upload_bytes;       /* RAW bytes staged                                           */
 } tdp_server_stats;
 void tdp_server_default_params(tdp_server_params *p);
 /* allocates both arenas in the context (counted against its budget) */
