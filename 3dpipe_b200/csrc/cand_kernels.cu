@@ -74,6 +74,11 @@ __device__ __forceinline__ float d_point_dist(const float* a, const float* b) {
     return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
 }
 
+// aab::intersect of the reference: the boxes overlap strictly on every axis
+__device__ __forceinline__ bool strict_overlap(const float* b, const float* a) {
+    return !(b[0] >= a[3] || b[3] <= a[0] || b[1] >= a[4] || b[4] <= a[1] || b[2] >= a[5] || b[5] <= a[2]);
+}
+
 __device__ __forceinline__ unsigned long long key_of(float d, int id) {
     return ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)id;
 }
@@ -155,7 +160,7 @@ __global__ void __launch_bounds__(256) k_cand_pass(DG bg, const float* __restric
                                                    const float* __restrict__ box2, const float* __restrict__ xf2,
                                                    int n1, int self, int knn_all, float tau_all,
                                                    const int* __restrict__ qk, const float* __restrict__ qtau,
-                                                   const unsigned long long* __restrict__ kth,
+                                                   int isect, const unsigned long long* __restrict__ kth,
                                                    int64_t* __restrict__ cnt, const int64_t* __restrict__ off,
                                                    unsigned long long* __restrict__ keys) {
     const int lane = threadIdx.x & 31;
@@ -201,7 +206,7 @@ __global__ void __launch_bounds__(256) k_cand_pass(DG bg, const float* __restric
                                     keep = gap < T || key <= kk;
                                 } else {
                                     key = (unsigned)o;
-                                    keep = gap <= tau;
+                                    keep = isect ? strict_overlap(ob, qb) : gap <= tau;
                                 }
                             }
                         }
@@ -251,7 +256,7 @@ struct TileBoxes {
 
 int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool self, bool knn, int K, float tau,
                       Buf& pq_buf, Buf& pt_buf, Buf& qoff_buf, long& P, bool& overflow, const int* qk,
-                      const float* qtau) {
+                      const float* qtau, bool isect) {
     cudaStream_t s = ctx->stream;
     const long n1 = t1->n_obj, n2 = t2->n_obj;
     overflow = false;
@@ -303,7 +308,7 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
     const int pblocks = (int)std::min<long>((n1 + 7) / 8, (long)ctx->num_sms * 32);
     CU(cudaMemsetAsync(cnt + n1, 0, 8, s));
     k_cand_pass<false><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, (int)n1, self, knn, tau, qk,
-                                                           qtau, kth, cnt, nullptr, nullptr);
+                                                           qtau, isect ? 1 : 0, kth, cnt, nullptr, nullptr);
     CU(cudaGetLastError());
     size_t tb = 0;
     CU(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, qoff, (int)n1 + 1, s));
@@ -326,7 +331,7 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
     if ((rc = ensure(ctx, pq_buf, Pz * 4))) return rc;
     if ((rc = ensure(ctx, pt_buf, Pz * 4))) return rc;
     if (P > 0) {
-        k_cand_pass<true><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, (int)n1, self, knn, tau, qk, qtau, kth,
+        k_cand_pass<true><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, (int)n1, self, knn, tau, qk, qtau, isect ? 1 : 0, kth,
                                                               nullptr, qoff, (unsigned long long*)keys.p);
         CU(cudaGetLastError());
         size_t sb = 0;

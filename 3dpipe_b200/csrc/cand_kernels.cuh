@@ -18,6 +18,6 @@ namespace tdp {
 // distance qtau); NULL: every object uses (knn, K, tau).
 int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool self, bool knn, int K, float tau,
                       Buf& pq_buf, Buf& pt_buf, Buf& qoff_buf, long& P, bool& overflow, const int* qk = nullptr,
-                      const float* qtau = nullptr);
+                      const float* qtau = nullptr, bool isect = false);
 
 }  // namespace tdp

@@ -231,8 +231,17 @@ __global__ void __launch_bounds__(kBlock) k_vps(JoinDev d, int within_all, float
             if (k < total) {
                 a = (uint32_t)(k / n2);
                 bb = (uint32_t)(k - (uint64_t)a * n2);
-                vox_dist(d.vox1 + 3 * (size_t)(a0 + a), d.vox2 + 3 * (size_t)(b0 + bb), m, M);
-                keep = (m - slack <= lim) && (!within || m - slack <= tau);
+                const float4* va = d.vox1 + 3 * (size_t)(a0 + a);
+                const float4* vb = d.vox2 + 3 * (size_t)(b0 + bb);
+                vox_dist(va, vb, m, M);
+                if (d.isect) {
+                    // aab::intersect: strict overlap on every axis
+                    const float4 alo = va[0], ahi = va[1], blo = vb[0], bhi = vb[1];
+                    keep = !(blo.x >= ahi.x || bhi.x <= alo.x || blo.y >= ahi.y || bhi.y <= alo.y ||
+                             blo.z >= ahi.z || bhi.z <= alo.z);
+                } else {
+                    keep = (m - slack <= lim) && (!within || m - slack <= tau);
+                }
             }
             const unsigned bal = __ballot_sync(0xffffffffu, keep);
             if (WRITE && keep) {

@@ -41,6 +41,8 @@ struct JoinDev {
     // (within, distance qtau[q])
     const int* qk;
     const float* qtau;
+    // intersect query: voxel pairs are kept when their boxes overlap strictly
+    int isect;
     // voxel pairs kept after the filter
     int64_t V;
     int* vpa;

@@ -92,7 +92,13 @@ void generate_candidates(const CandidateQuery& q, std::vector<int64_t>& off, std
                                     if (stamp[o] == (int)i) continue;
                                     stamp[o] = (int)i;
                                     if (q.self_join && o == i) continue;
-                                    if (box_gap(q.box2 + 6 * o, qb) <= within) found.push_back({0.f, o});
+                                    const float* ob = q.box2 + 6 * o;
+                                    const bool hit =
+                                        q.strict_overlap
+                                            ? !(ob[0] >= qb[3] || ob[3] <= qb[0] || ob[1] >= qb[4] || ob[4] <= qb[1] ||
+                                                ob[2] >= qb[5] || ob[5] <= qb[2])
+                                            : box_gap(ob, qb) <= within;
+                                    if (hit) found.push_back({0.f, o});
                                 }
                             }
                     std::sort(found.begin(), found.end(), [](auto& a, auto& b) { return a.second < b.second; });

@@ -36,6 +36,8 @@ struct CandidateQuery {
     // obj_knn[i] = K (> 0, kNN) or 0 (within, distance obj_within[i])
     const int* obj_knn = nullptr;
     const float* obj_within = nullptr;
+    // intersect query: candidates are objects whose boxes overlap strictly
+    bool strict_overlap = false;
 };
 
 // off: [n1+1] CSR offsets into ids.

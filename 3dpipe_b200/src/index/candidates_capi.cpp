@@ -8,8 +8,12 @@
 extern "C" long tdp_candidates(const float* box1, const float* xf1, long n1, const float* box2, const float* xf2,
                                long n2, int self_join, int is_knn, int knn, float within, int64_t* off, int32_t* ids,
                                long cap) {
-    if (!box1 || !xf1 || !box2 || !xf2 || !off || n1 < 0 || n2 < 0 || (is_knn && knn < 1)) return LONG_MIN;
-    tdp::CandidateQuery q{box1, xf1, n1, box2, xf2, n2, self_join != 0, is_knn != 0, knn, within, 0};
+    if (!box1 || !xf1 || !box2 || !xf2 || !off || n1 < 0 || n2 < 0 || (is_knn == 1 && knn < 1) || is_knn < 0 ||
+        is_knn > 2)
+        return LONG_MIN;
+    // is_knn: 1 kNN, 0 within, 2 intersect (strict box overlap, ordered by id)
+    tdp::CandidateQuery q{box1, xf1, n1, box2, xf2, n2, self_join != 0, is_knn == 1, knn, within, 0};
+    q.strict_overlap = is_knn == 2;
     std::vector<int64_t> o;
     std::vector<int32_t> i;
     tdp::generate_candidates(q, o, i);

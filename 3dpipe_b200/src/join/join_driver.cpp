@@ -76,6 +76,9 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     const bool self = (t2 == nullptr || t2 == t1);
     if (!t2) t2 = t1;
     const bool knn = prm->query == TDP_QUERY_NN;
+    const bool isect = prm->query == TDP_QUERY_INTERSECT;
+    // an intersect join takes the decisions of a within join at distance 0
+    const float within_dist = isect ? 0.f : prm->within_dist;
     const bool mixed = prm->obj_knn != nullptr;  // per query object queries (a batch of requests)
     bool any_knn = knn, any_within = !knn;
     if (mixed) {
@@ -88,7 +91,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
             (prm->obj_knn[i] > 0 ? any_knn : any_within) = true;
         }
     } else {
-        if (!knn && prm->query != TDP_QUERY_WITHIN) return fail(ctx, TDP_ERR_ARG, "query must be nn or within");
+        if (!knn && !isect && prm->query != TDP_QUERY_WITHIN)
+            return fail(ctx, TDP_ERR_ARG, "query must be nn, within or intersect");
         if (knn && prm->knn < 1) return fail(ctx, TDP_ERR_ARG, "knn must be >= 1");
     }
     if (prm->hausdorff_level < 0 || prm->hausdorff_level > 2) return fail(ctx, TDP_ERR_ARG, "hausdorff_level must be 0, 1 or 2");
@@ -135,15 +139,15 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     }
     if (tuned) {
         bool overflow = false;
-        if ((rc = device_candidates(ctx, t1, t2, self, knn, knn ? prm->knn : 0, prm->within_dist, ctx->scratch[kPq],
-                                    ctx->scratch[kPt], ctx->scratch[kQoff], P, overflow, dqk, dqtau)))
+        if ((rc = device_candidates(ctx, t1, t2, self, knn, knn ? prm->knn : 0, within_dist, ctx->scratch[kPq],
+                                    ctx->scratch[kPt], ctx->scratch[kQoff], P, overflow, dqk, dqtau, isect)))
             return rc;
         on_device = !overflow;
     }
     if (!on_device) {
         CandidateQuery cq{t1->host.obj_box.data(), t1->host.obj_xf.data(), t1->n_obj, t2->host.obj_box.data(),
-                          t2->host.obj_xf.data(), t2->n_obj, self, knn, knn ? prm->knn : 0, prm->within_dist, 0,
-                          prm->obj_knn, prm->obj_within};
+                          t2->host.obj_xf.data(), t2->n_obj, self, knn, knn ? prm->knn : 0, within_dist, 0,
+                          prm->obj_knn, prm->obj_within, isect};
         generate_candidates(cq, qoff, ids);
         P = (long)ids.size();
         if (P >= (1L << 31) - 1) return fail(ctx, TDP_ERR_ARG, "too many candidate pairs");
@@ -167,7 +171,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     d.pmn = buf<float>(ctx, kPmn); d.pmx = buf<float>(ctx, kPmx); d.perr = buf<float>(ctx, kPerr);
     d.pstat = buf<uint8_t>(ctx, kPstat); d.pvp = buf<int64_t>(ctx, kPvp);
     d.N1 = (int)t1->n_obj; d.qoff = buf<int64_t>(ctx, kQoff); d.qconf = buf<int>(ctx, kQconf);
-    d.qk = dqk; d.qtau = dqtau;
+    d.qk = dqk; d.qtau = dqtau; d.isect = isect ? 1 : 0;
 
     unsigned* cnt_items = ctx->d_counter + 8;    // [0] items, [2..3] tri-pair sum (u64)
     unsigned* cnt_status = ctx->d_counter + 16;  // undecided, reported
@@ -189,11 +193,11 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     // ---- 2. filter ----
     CU(launch_pair_bounds(d, s)); ++launches;
     if (any_knn) { CU(launch_knn_rank(d, prm->knn, tuned, buf<int>(ctx, kRankSt), s)); }
-    if (any_within) { CU(launch_within_decide(d, prm->within_dist, tuned, s)); }
+    if (any_within) { CU(launch_within_decide(d, within_dist, tuned, s)); }
     ++launches;
     int64_t* cnt = buf<int64_t>(ctx, kCnt);
     CU(cudaMemsetAsync(cnt + P, 0, 8, s));
-    CU(launch_count_vps(d, !knn, prm->within_dist, tuned, cnt, s)); ++launches;
+    CU(launch_count_vps(d, !knn, within_dist, tuned, cnt, s)); ++launches;
     size_t tmp_bytes = 0;
     CU(scan_counts(cnt, d.pvp, (int)P, nullptr, tmp_bytes, s));
     ENS(kScanTmp, tmp_bytes + 16);
@@ -209,7 +213,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     d.vpa = buf<int>(ctx, kVpa); d.vpb = buf<int>(ctx, kVpb); d.vpair = buf<int>(ctx, kVpair);
     d.vmn = buf<float>(ctx, kVmn); d.vmx = buf<float>(ctx, kVmx); d.verr = buf<float>(ctx, kVerr);
     d.valive = buf<uint8_t>(ctx, kValive); d.vupd = buf<int>(ctx, kVupd);
-    CU(launch_write_vps(d, !knn, prm->within_dist, tuned, s)); ++launches;
+    CU(launch_write_vps(d, !knn, within_dist, tuned, s)); ++launches;
     CU(cudaEventRecord(ctx->ev[1], s));
     st.filter_pairs = P;
 
@@ -250,7 +254,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
             }
             CU(launch_pair_update(d, (int)k, 0, s)); ++launches;
             if (any_knn) CU(launch_knn_rank(d, prm->knn, 0, buf<int>(ctx, kRankSt), s));
-            if (any_within) CU(launch_within_decide(d, prm->within_dist, 0, s));
+            if (any_within) CU(launch_within_decide(d, within_dist, 0, s));
             ++launches;
             CU(cudaMemsetAsync(cnt_status, 0, 8, s));
             CU(launch_count_status(d, cnt_status, s)); ++launches;
@@ -288,7 +292,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
             CU(launch_apply_results(d, res, item_vp, (int)V, highest, prm->hausdorff_level, li, (int)k, s, cnt_items));
             CU(launch_pair_update(d, (int)k, 1, s));
             if (any_knn) CU(launch_knn_rank(d, prm->knn, 1, buf<int>(ctx, kRankSt), s));
-            if (any_within) CU(launch_within_decide(d, prm->within_dist, 1, s));
+            if (any_within) CU(launch_within_decide(d, within_dist, 1, s));
             launches += 3;
         }
         // ---- 3b. FP64 recheck of pairs whose FP32 ranges stayed inside their
@@ -300,7 +304,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
             CU(launch_recheck_items(d, t1->vtri[4], t2->vtri[4], items, item_vp, vexact, cnt_items, s));
             CU(launch_refine_f64(t1->tri[4], t2->tri[4], items, (int)V, buf<double>(ctx, kRes64), s, cnt_items));
             CU(launch_recheck_finish(d, buf<double>(ctx, kRes64), item_vp, (int)V, vexact, buf<double>(ctx, kPexact),
-                                     knn, prm->knn, prm->within_dist, s, cnt_items));
+                                     knn, prm->knn, within_dist, s, cnt_items));
             launches += knn ? 6 : 5;
         }
     }

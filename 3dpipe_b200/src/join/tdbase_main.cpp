@@ -74,6 +74,7 @@ int main(int argc, char** argv) {
     if (t1.empty() || q.empty()) return usage();
     if (q == "nn") p.query = TDP_QUERY_NN;
     else if (q == "within") p.query = TDP_QUERY_WITHIN;
+    else if (q == "intersect") p.query = TDP_QUERY_INTERSECT;
     else { std::fprintf(stderr, "error query type: %s\n", q.c_str()); return 2; }
 
     auto t0 = std::chrono::steady_clock::now();

@@ -21,7 +21,7 @@ TDP_OK = 0
 ERRORS = {1: "TDP_ERR_ARG", 2: "TDP_ERR_CUDA", 3: "TDP_ERR_NOMEM", 4: "TDP_ERR_FORMAT",
           5: "TDP_ERR_TIMEOUT", 6: "TDP_ERR_STATE", 7: "TDP_ERR_NODEV"}
 FORM_PLAIN, FORM_TUNED = 0, 1
-QUERY_NN, QUERY_WITHIN = 1, 2
+QUERY_NN, QUERY_WITHIN, QUERY_INTERSECT = 1, 2, 3
 
 # Every symbol include/tdp.h declares; tests check the library exports them all.
 EXPORTED = [
@@ -243,19 +243,21 @@ class Tile:
             pass
 
 
-def candidates(box1, xf1, box2, xf2, self_join=False, knn=0, within=0.0):
-    """Object candidates (CSR offsets, ids); knn > 0 selects the kNN query."""
+def candidates(box1, xf1, box2, xf2, self_join=False, knn=0, within=0.0, intersect=False):
+    """Object candidates (CSR offsets, ids); knn > 0 selects the kNN query,
+    intersect the strict box-overlap query."""
     L = lib()
     box1 = np.ascontiguousarray(box1, np.float32).reshape(-1, 6)
     box2 = np.ascontiguousarray(box2, np.float32).reshape(-1, 6)
     xf1 = np.ascontiguousarray(xf1, np.float32).reshape(-1, 3)
     xf2 = np.ascontiguousarray(xf2, np.float32).reshape(-1, 3)
     off = np.zeros(len(box1) + 1, np.int64)
+    mode = 2 if intersect else int(knn > 0)
     n = L.tdp_candidates(_ptr(box1), _ptr(xf1), len(box1), _ptr(box2), _ptr(xf2), len(box2), int(self_join),
-                         int(knn > 0), max(knn, 1), float(within), _ptr(off), None, 0)
+                         mode, max(knn, 1), float(within), _ptr(off), None, 0)
     ids = np.zeros(max(-n, 1), np.int32)
     n = L.tdp_candidates(_ptr(box1), _ptr(xf1), len(box1), _ptr(box2), _ptr(xf2), len(box2), int(self_join),
-                         int(knn > 0), max(knn, 1), float(within), _ptr(off), _ptr(ids), ids.size)
+                         mode, max(knn, 1), float(within), _ptr(off), _ptr(ids), ids.size)
     if n < 0:
         raise TdpError(1, "tdp_candidates failed")
     return off, ids[:n]
@@ -264,9 +266,9 @@ def candidates(box1, xf1, box2, xf2, self_join=False, knn=0, within=0.0):
 def _join_params(query, knn, within, lods, hausdorff_level, form) -> JoinParams:
     p = JoinParams()
     lib().tdp_join_default_params(C.byref(p))
-    if query not in ("nn", "within"):
-        raise ValueError("query must be nn or within")
-    p.query = QUERY_NN if query == "nn" else QUERY_WITHIN
+    if query not in ("nn", "within", "intersect"):
+        raise ValueError("query must be nn, within or intersect")
+    p.query = {"nn": QUERY_NN, "within": QUERY_WITHIN, "intersect": QUERY_INTERSECT}[query]
     p.knn, p.within_dist, p.hausdorff_level, p.form = knn, within, hausdorff_level, form
     if lods:
         p.n_lods = len(lods)

@@ -298,6 +298,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream measurement")
+    ap.add_argument("--no-self", action="store_true", help="skip the 10-NN self-join measurement")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[200.0, 500.0, 1000.0, 2000.0])
     ap.add_argument("--vessels", type=int, default=None, help="smaller workload for profiling captures")
     ap.add_argument("--nuclei-per-vessel", type=int, default=None)
@@ -404,6 +405,21 @@ def main():
         flops = agg_t["full_evals"] * F_TRI + agg_t["tri_pairs"] * F_CULL
         achieved = flops / (refine_ms / 1e3) / 1e12
 
+        # config 3: the 10-NN self-join over the same 200k nuclei (tuned form;
+        # one run to build the grids, one measured by the library's events)
+        knn_self = None
+        if not a.no_self and ws == 1:
+            ctx.join(T1, None, query="nn", knn=10, form=pkg.FORM_TUNED)
+            qs, _, _ = ctx.join(T1, None, query="nn", knn=10, form=pkg.FORM_TUNED)
+            st_s = ctx.stats()
+            knn_self = {"workload": f"10-NN self-join over the {N_VESSELS * NUCLEI_PER_VESSEL} nuclei, LODs 20-100",
+                        "join_ms": st_s["total_ms"], "tri_pairs": st_s["tri_pairs"],
+                        "tri_pairs_per_s": st_s["tri_pairs"] / (st_s["total_ms"] / 1e3),
+                        "refine_ms": st_s["refine_ms"], "voxel_pairs_refined": st_s["refine_items"],
+                        "results": int(len(qs)), "recheck_pairs": st_s["recheck_pairs"]}
+            log(f"[rank {rank}] knn self-join: {st_s['total_ms']:.0f} ms, "
+                f"{knn_self['tri_pairs_per_s'] / 1e9:.1f} G tri-pairs/s")
+
         # one untimed join with the exact-distance stage: its cost and the FP32
         # refine's error against FP64 on this workload
         ctx.join(T1, T2, query="within", within=TAU, form=pkg.FORM_TUNED, exact_distances=True)
@@ -471,6 +487,7 @@ def main():
                     "h2d_bytes_per_step": int(nb.size + vb.size), "d2h_bytes_per_step": int(d2h)},
             "exact_distances": exact,
             "serving": serving,
+            "knn_self_join": knn_self,
             "gpu_launches": int(launches_t),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,

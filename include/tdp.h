@@ -118,10 +118,13 @@ int tdp_tile_get_info(const tdp_tile *tile, tdp_tile_info *out);
  * The object-level filter: replaces OctreeNode::query_knn_fast / query_within
  * over Tile::build_octree (reference src/index/octree.cpp:215-330,
  * src/storage/tile.cpp:76-85).  Boxes are 6 floats (low xyz, high xyz),
- * transforms 3 floats.  kNN (is_knn != 0): the knn objects with the smallest
+ * transforms 3 floats.  kNN (is_knn == 1): the knn objects with the smallest
  * transform distance plus every object whose box gap is below the knn-th of
- * those distances, ordered by (transform distance, id).  within: every object
- * with box gap <= within, ordered by id.  self_join excludes the query object.
+ * those distances, ordered by (transform distance, id).  within (is_knn == 0):
+ * every object with box gap <= within, ordered by id.  intersect (is_knn == 2,
+ * OctreeNode::query_intersect, src/index/octree.cpp:332-349): every object
+ * whose box overlaps strictly, ordered by id.  self_join excludes the query
+ * object.
  * off: [n1+1] CSR offsets.  Returns the number of candidates, or -(needed) when
  * cap is too small (off is then valid, ids is not), LONG_MIN on bad arguments. */
 long tdp_candidates(const float *box1, const float *xf1, long n1, const float *box2, const float *xf2, long n2,
@@ -139,9 +142,17 @@ long tdp_tile_candidates(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *ti
  * tile2 == tile1 is a self-join (query object excluded from its own candidates;
  * within results then hold both (a,b) and (b,a), as in the reference).
  * Results are (query id, result id) pairs sorted by query then result id. */
-enum { TDP_QUERY_NN = 1, TDP_QUERY_WITHIN = 2 };
+/* TDP_QUERY_INTERSECT (-q intersect, SpatialJoin::intersect,
+ * src/join/IntersectionJoin.cpp:12-140 with TriInt_cuda,
+ * src/geometry/computing_gpu.cu:1441-1511): candidates are objects whose boxes
+ * overlap strictly (aab::intersect, src/spatial/himesh_box.cpp:95-99), voxel
+ * pairs likewise; a pair is reported when a voxel pair's max_dist = min(d + h1
+ * + h2) is 0 and dropped when every voxel pair's min_dist is above 0 -- the
+ * decisions of a within join at distance 0, with LOD 100 deciding. */
+enum { TDP_QUERY_NN = 1, TDP_QUERY_WITHIN = 2, TDP_QUERY_INTERSECT = 3 };
 typedef struct {
-    int query;             /* TDP_QUERY_NN (-q nn) or TDP_QUERY_WITHIN (-q within)   */
+    int query;             /* TDP_QUERY_NN (-q nn), TDP_QUERY_WITHIN (-q within) or
+                              TDP_QUERY_INTERSECT (-q intersect; within_dist unused) */
     int knn;               /* --knn K                      (default 1)             */
     float within_dist;     /* --within_dist tau            (default 1000)          */
     int lods[8];           /* -l/--lods, ascending; n_lods = 0 -> 20,40,60,80,100  */

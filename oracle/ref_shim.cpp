@@ -10,6 +10,7 @@
  * This file is new code; it only adapts plain arrays to the reference's types
  * so the oracle and the CUDA path can be pinned against the reference itself.
  */
+#include <algorithm>
 #include <vector>
 #include <utility>
 #include <cstring>
@@ -90,7 +91,18 @@ long tdr_candidates(const float *box1, const float *xf1, long n1,
         }
         std::vector<std::pair<int, range>> cand;
         float xf[3] = {xf1[3 * i], xf1[3 * i + 1], xf1[3 * i + 2]};
-        if (is_knn) {
+        if (is_knn == 2) {
+            // intersect: SpatialJoin::mbb_intersect (IntersectionJoin.cpp:12-60)
+            // sorts the octree's ids and skips duplicates
+            std::vector<int> hit;
+            tree->query_intersect(q, hit);
+            std::sort(hit.begin(), hit.end());
+            int former = -1;
+            for (int id : hit) {
+                if (id != former) cand.push_back({id, range()});
+                former = id;
+            }
+        } else if (is_knn) {
             float mm = 3.4e38f;
             tree->query_knn_fast(q, xf, cand, mm, knn);
         } else {

@@ -102,3 +102,31 @@ def test_reference_rules_agree_with_exact_oracle(name):
     truth, margin = exact_truth(nb, vb, self_join, query, knn, tau)
     assert margin > 1e-3
     assert set(zip(rq.tolist(), rt.tolist())) == truth
+
+
+def _overlapping_nuclei(pkg):
+    """Two nuclei tiles of different seeds around the same vessel grid, in a
+    tight shell, so that many nuclei boxes (and some nuclei) overlap."""
+    a, _ = pkg.tdp.gen_tiles(3, 100, seed=301, shell_min=12.0, shell_max=30.0)
+    b, _ = pkg.tdp.gen_tiles(3, 100, seed=302, shell_min=12.0, shell_max=30.0)
+    return a, b
+
+
+def test_intersect_candidates_match_reference_octree(pkg, ref):
+    """Intersect candidates (strict box overlap, OctreeNode::query_intersect)
+    equal the reference octree's, compiled from source, set and order."""
+    if ref is None:
+        pytest.skip("reference CPU code not built")
+    a, b = _overlapping_nuclei(pkg)
+    A, B = read_tile(a), read_tile(b)
+    b1 = np.stack([o.box for o in A]); x1 = np.stack([o.transform for o in A])
+    b2 = np.stack([o.box for o in B]); x2 = np.stack([o.transform for o in B])
+    off, ids = pkg.tdp.candidates(b1, x1, b2, x2, intersect=True)
+    roff, rids = ref.candidates(b1, x1, b2, x2, False, 1, 0.0, 2)
+    np.testing.assert_array_equal(off, roff)
+    np.testing.assert_array_equal(ids, rids)
+    assert len(ids) >= 10
+    off, ids = pkg.tdp.candidates(b1, x1, b1, x1, self_join=True, intersect=True)
+    roff, rids = ref.candidates(b1, x1, b1, x1, True, 1, 0.0, 2)
+    np.testing.assert_array_equal(off, roff)
+    np.testing.assert_array_equal(ids, rids)

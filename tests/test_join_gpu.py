@@ -247,3 +247,25 @@ def test_mixed_queries_equal_separate_joins(pkg, ctx, gpu_tiles):
                 objs = np.nonzero(which == k)[0]
                 counts = np.bincount(q, minlength=n1)[objs]
                 assert np.all(counts == K)
+
+
+def test_intersect_join_matches_fp64_truth(pkg, ctx):
+    """-q intersect: the pairs whose boxes overlap strictly and whose LOD-100
+    meshes touch or cross (exact FP64 distance 0); both forms."""
+    from oracle_bind import join_exact
+    from rawdt import read_tile
+    a, _ = pkg.tdp.gen_tiles(3, 100, seed=301, shell_min=12.0, shell_max=30.0)
+    b, _ = pkg.tdp.gen_tiles(3, 100, seed=302, shell_min=12.0, shell_max=30.0)
+    oq, ot, od, _ = join_exact(a, b, False, False, tau=0.0)
+    A, B = read_tile(a), read_tile(b)
+
+    def strict(x, y):
+        return not any(y[i] >= x[i + 3] or y[i + 3] <= x[i] for i in range(3))
+
+    truth = {(int(q), int(t)) for q, t, d in zip(oq, ot, od) if d == 0.0 and strict(A[q].box, B[t].box)}
+    assert len(truth) > 0
+    T1, T2 = pkg.tdp.Tile(ctx, a), pkg.tdp.Tile(ctx, b)
+    for form in (pkg.FORM_PLAIN, pkg.FORM_TUNED):
+        q, t, d = ctx.join(T1, T2, query="intersect", form=form)
+        assert set(zip(q.tolist(), t.tolist())) == truth, form
+        assert np.all(d == 0.0)
