@@ -323,7 +323,42 @@ Context.join = _join
 EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates", "tdp_ctx_stream",
              "tdp_refine_config_count", "tdp_refine_config_info", "tdp_set_refine_config", "tdp_get_refine_config",
              "tdp_autotune", "tdp_result_copy_f64", "tdp_server_default_params", "tdp_server_create",
-             "tdp_server_submit", "tdp_server_wait", "tdp_server_get_stats", "tdp_server_destroy"]
+             "tdp_server_submit", "tdp_server_wait", "tdp_server_get_stats", "tdp_server_destroy",
+             "tdp_join_chunked"]
+
+
+class ChunkedInfo(C.Structure):
+    _fields_ = [("chunks", C.c_long), ("h2d_bytes", C.c_double), ("tri_pairs", C.c_double),
+                ("join_ms", C.c_double), ("device_peak_bytes", C.c_double)]
+
+
+def _join_chunked(self, raw1: np.ndarray, raw2: np.ndarray, chunk_objects: int, query: str = "nn", knn: int = 1,
+                  within: float = 1000.0, lods=None, hausdorff_level: int = 2, form: int = FORM_TUNED):
+    """A join of host RAW tiles in chunks of query objects (tdp_join_chunked);
+    returns (q, t, d, info) with global ids, equal to the whole join."""
+    L = lib()
+    raw1 = np.ascontiguousarray(raw1, np.uint8)
+    raw2 = np.ascontiguousarray(raw2, np.uint8)
+    p = _join_params(query, knn, within, lods, hausdorff_level, form)
+    r = C.c_void_p()
+    inf = ChunkedInfo()
+    L.tdp_join_chunked.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                   C.POINTER(JoinParams), C.c_long, C.POINTER(ChunkedInfo), C.POINTER(C.c_void_p)]
+    self.check(L.tdp_join_chunked(self._h, _ptr(raw1), raw1.size, _ptr(raw2), raw2.size, C.byref(p),
+                                  int(chunk_objects), C.byref(inf), C.byref(r)))
+    try:
+        n = C.c_long()
+        L.tdp_result_count(r, C.byref(n))
+        q = np.empty(n.value, np.int32)
+        t = np.empty(n.value, np.int32)
+        d = np.empty(n.value, np.float32)
+        L.tdp_result_copy(r, _ptr(q), _ptr(t), _ptr(d))
+    finally:
+        L.tdp_result_free(r)
+    return q, t, d, {k: getattr(inf, k) for k, _ in inf._fields_}
+
+
+Context.join_chunked = _join_chunked
 
 
 def raw_object_offsets(raw: np.ndarray) -> np.ndarray:

@@ -191,6 +191,27 @@ int tdp_result_free(tdp_result *r);
 int tdp_autotune(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, const tdp_join_params *params,
                  double *ms_per_config, int *best);
 
+/* ---- joins larger than the device ------------------------------------------
+ * Joins host RAW tiles that need not fit on the device (config 4: a device
+ * budget below the tiles' size).  The candidates are computed on the host for
+ * the whole tiles; tile 1 is joined in chunks of chunk_objects query objects,
+ * each against a sub-tile of tile 2 holding exactly that chunk's candidates.
+ * The result equals tdp_join on the whole tiles (ids and distances).  Device
+ * memory is bounded by one chunk, its sub-tile and the join's scratch: pick
+ * chunk_objects so that fits the context's budget.  No per-object queries;
+ * tile 2 must be a different tile (no self-join).  No reference counterpart
+ * (the reference keeps both tiles decoded in host memory and sizes its device
+ * scratch for the whole tile, src/geometry/computing_gpu.cu:4538-4626). */
+typedef struct {
+    long chunks;
+    double h2d_bytes;          /* RAW bytes uploaded (chunks and sub-tiles)               */
+    double tri_pairs;          /* refined triangle pairs, all chunks                      */
+    double join_ms;            /* device time of the chunk joins                          */
+    double device_peak_bytes;  /* the context's device-memory high-water mark             */
+} tdp_chunked_info;
+int tdp_join_chunked(tdp_ctx *ctx, const void *raw1, size_t len1, const void *raw2, size_t len2,
+                     const tdp_join_params *p, long chunk_objects, tdp_chunked_info *info, tdp_result **out);
+
 /* ---- serving ------------------------------------------------------------------
  * A request loop over one resident tile 2 (for example the vessel tile): each
  * request is a RAW .dt tile of query objects with its own query (kNN with its

@@ -269,3 +269,40 @@ def test_intersect_join_matches_fp64_truth(pkg, ctx):
         q, t, d = ctx.join(T1, T2, query="intersect", form=form)
         assert set(zip(q.tolist(), t.tolist())) == truth, form
         assert np.all(d == 0.0)
+
+
+@pytest.mark.parametrize("args", [dict(query="nn", knn=3), dict(query="within", within=150.0)])
+@pytest.mark.parametrize("chunk", [1, 7, 1000])
+def test_chunked_join_equals_whole_join(pkg, ctx, gpu_tiles, args, chunk):
+    """tdp_join_chunked (tiles in host memory, tile 1 in chunks against
+    sub-tiles of tile 2) returns the whole join's result, ids and distances."""
+    nb, vb = tiles(6, 12, 101)
+    T1, T2 = gpu_tiles(6, 12, 101)
+    q, t, d = ctx.join(T1, T2, **args)
+    cq, ct, cd, info = ctx.join_chunked(nb, vb, chunk, **args)
+    np.testing.assert_array_equal(cq, q)
+    np.testing.assert_array_equal(ct, t)
+    np.testing.assert_array_equal(cd, d)
+    assert info["chunks"] == -(-T1.info()["n_objects"] // chunk)
+
+
+def test_chunked_join_fits_a_budget_the_whole_join_exceeds(pkg):
+    """Config 4 in small: under a device budget below the two tiles' size the
+    whole join fails with TDP_ERR_NOMEM; the chunked join succeeds within the
+    same budget (a fresh context: the failed upload may keep scratch)."""
+    nb, vb = tiles(2, 60, 107)
+    budget = int(0.7 * (nb.size + vb.size))
+    assert nb.size > budget  # the query tile alone does not fit
+    with pkg.Context(0, budget) as small:
+        with pytest.raises(pkg.TdpError) as e:
+            pkg.tdp.Tile(small, nb)
+        assert e.value.code == 3
+    with pkg.Context(0, budget) as small:
+        q, t, d, info = small.join_chunked(nb, vb, 10, query="nn", knn=2)
+        assert info["device_peak_bytes"] <= budget and info["chunks"] == 12
+        assert len(q) == 2 * 120
+    with pkg.Context(0) as big:
+        wq, wt, wd = big.join(pkg.tdp.Tile(big, nb), pkg.tdp.Tile(big, vb), query="nn", knn=2)
+    np.testing.assert_array_equal(q, wq)
+    np.testing.assert_array_equal(t, wt)
+    np.testing.assert_array_equal(d, wd)
