@@ -16,10 +16,18 @@
 // needs both tiles decoded in host memory and its filter scratch on the
 // device for the whole tile (src/geometry/computing_gpu.cu:4538-4626).
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
+#include <thread>
+#include <tuple>
 #include <cstring>
+#include <functional>
 #include <future>
+#include <memory>
 #include <string>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 #include "../../csrc/ctx.cuh"
 #include "index/candidates.h"
@@ -38,33 +46,83 @@ inline uint64_t rec_end(const TileHost& h, long i) {
     return h.obj_data_off[i] + h.obj_data_size[i] + 8 + kNumLods * 8 + nv * (9 * 4 + kNumLods * 16) + 12;
 }
 
-struct Chunk {
-    long q0 = 0, q1 = 0;           // query objects [q0, q1)
-    std::vector<int32_t> sub;       // global tile-2 ids in the sub-tile, increasing
-    std::vector<uint8_t> raw1, raw2;
+// A host staging buffer, page-locked when possible (uploads then run at the
+// full host-to-device rate), reused by every chunk assembled into it.
+struct HostBuf {
+    uint8_t* p = nullptr;
+    size_t cap = 0;
+    bool pinned = false;
+    bool alloc(size_t bytes) {
+        cap = bytes;
+        pinned = cudaHostAlloc((void**)&p, bytes, cudaHostAllocDefault) == cudaSuccess;
+        if (!pinned) p = (uint8_t*)std::malloc(bytes);
+        return p != nullptr;
+    }
+    ~HostBuf() {
+        if (!p) return;
+        if (pinned) cudaFreeHost(p);
+        else std::free(p);
+    }
 };
 
+struct Chunk {
+    long q0 = 0, q1 = 0;       // query objects [q0, q1)
+    std::vector<int32_t> sub;  // global tile-2 ids in the sub-tile, increasing
+    uint8_t* raw1 = nullptr;   // in the chunk's HostBuf: RAW chunk of tile 1, then the sub-tile
+    uint8_t* raw2 = nullptr;
+    size_t len1 = 0, len2 = 0;
+};
+
+// copy (dst, src, len) pieces with a few threads, split by bytes
+void parallel_copy(std::vector<std::tuple<uint8_t*, const uint8_t*, size_t>>& pieces) {
+    size_t total = 0;
+    for (auto& x : pieces) total += std::get<2>(x);
+    const unsigned T = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (T == 1 || total < ((size_t)64 << 20)) {
+        for (auto& x : pieces) std::memcpy(std::get<0>(x), std::get<1>(x), std::get<2>(x));
+        return;
+    }
+    // cut big pieces so that every thread gets about total / T bytes
+    std::vector<std::tuple<uint8_t*, const uint8_t*, size_t>> cut;
+    const size_t part = total / T + 1;
+    for (auto& x : pieces)
+        for (size_t o = 0; o < std::get<2>(x); o += part)
+            cut.emplace_back(std::get<0>(x) + o, std::get<1>(x) + o, std::min(part, std::get<2>(x) - o));
+    std::vector<std::thread> th;
+    std::atomic<size_t> next{0};
+    for (unsigned t = 0; t < T; ++t)
+        th.emplace_back([&] {
+            for (size_t i; (i = next.fetch_add(1)) < cut.size();)
+                std::memcpy(std::get<0>(cut[i]), std::get<1>(cut[i]), std::get<2>(cut[i]));
+        });
+    for (auto& x : th) x.join();
+}
+
 void build_chunk(const uint8_t* b1, const TileHost& h1, const uint8_t* b2, const TileHost& h2,
-                 const std::vector<int64_t>& off, const std::vector<int32_t>& ids, long q0, long q1, Chunk& c) {
+                 const std::vector<int64_t>& off, const std::vector<int32_t>& ids, long q0, long q1, HostBuf& buf,
+                 Chunk& c) {
     c.q0 = q0;
     c.q1 = q1;
     c.sub.assign(ids.begin() + off[q0], ids.begin() + off[q1]);
     std::sort(c.sub.begin(), c.sub.end());
     c.sub.erase(std::unique(c.sub.begin(), c.sub.end()), c.sub.end());
     const uint64_t s1 = rec_begin(h1, q0), e1 = rec_end(h1, q1 - 1);
-    c.raw1.resize(1 + (e1 - s1));
+    c.len1 = 1 + (e1 - s1);
+    c.len2 = 1;
+    for (int32_t o : c.sub) c.len2 += rec_end(h2, o) - rec_begin(h2, o);
+    c.raw1 = buf.p;
+    c.raw2 = buf.p + c.len1;
     c.raw1[0] = b1[0];
-    std::memcpy(c.raw1.data() + 1, b1 + s1, e1 - s1);
-    size_t bytes = 1;
-    for (int32_t o : c.sub) bytes += rec_end(h2, o) - rec_begin(h2, o);
-    c.raw2.resize(bytes);
     c.raw2[0] = b2[0];
+    std::vector<std::tuple<uint8_t*, const uint8_t*, size_t>> pieces;
+    pieces.emplace_back(c.raw1 + 1, b1 + s1, e1 - s1);
     size_t p = 1;
     for (int32_t o : c.sub) {
         const uint64_t s = rec_begin(h2, o), n = rec_end(h2, o) - s;
-        std::memcpy(c.raw2.data() + p, b2 + s, n);
+        pieces.emplace_back(c.raw2 + p, b2 + s, n);
         p += n;
     }
+    parallel_copy(pieces);
 }
 
 }  // namespace
@@ -96,39 +154,95 @@ extern "C" int tdp_join_chunked(tdp_ctx* ctx, const void* raw1, size_t len1, con
     generate_candidates(cq, off, ids);
     tdp_chunked_info inf{};
     std::unique_ptr<tdp_result> R(new tdp_result());
-    auto next_chunk = [&](long q0) {
+    // chunk plan: grow each chunk object by object while the chunk, its
+    // candidates' sub-tile and the join's scratch fit the context's budget
+    // (about 2.5x their RAW bytes on the device: tiles, upload staging, join
+    // state), at most chunk_objects per chunk
+    std::vector<std::pair<long, long>> plan;
+    double max_chunk_bytes = 0;
+    {
+        const double reserve = std::min(512.0 * (1 << 20), 0.25 * (double)ctx->budget);
+        const double limit = ctx->budget ? ((double)ctx->budget - reserve) / 2.5 : 1e300;
+        std::vector<char> mark((size_t)h2.n_obj, 0);
+        std::vector<int32_t> touched;
+        double bytes = 0;
+        long q0 = 0;
+        for (long q = 0; q < h1.n_obj; ++q) {
+            double add = (double)(rec_end(h1, q) - rec_begin(h1, q));
+            for (int64_t k = off[q]; k < off[q + 1]; ++k)
+                if (!mark[ids[k]]) add += (double)(rec_end(h2, ids[k]) - rec_begin(h2, ids[k]));
+            if (q > q0 && (q - q0 >= chunk_objects || bytes + add > limit)) {
+                plan.push_back({q0, q});
+                max_chunk_bytes = std::max(max_chunk_bytes, bytes);
+                for (int32_t o : touched) mark[o] = 0;
+                touched.clear();
+                bytes = 0;
+                q0 = q;
+                add = (double)(rec_end(h1, q) - rec_begin(h1, q));
+                for (int64_t k = off[q]; k < off[q + 1]; ++k)
+                    if (!mark[ids[k]]) add += (double)(rec_end(h2, ids[k]) - rec_begin(h2, ids[k]));
+            }
+            for (int64_t k = off[q]; k < off[q + 1]; ++k)
+                if (!mark[ids[k]]) { mark[ids[k]] = 1; touched.push_back(ids[k]); }
+            bytes += add;
+        }
+        if (h1.n_obj > q0) plan.push_back({q0, h1.n_obj});
+        max_chunk_bytes = std::max(max_chunk_bytes, bytes);
+    }
+    HostBuf bufs[2];
+    for (HostBuf& b : bufs)
+        if (!b.alloc((size_t)max_chunk_bytes + 64)) return fail(ctx, TDP_ERR_NOMEM, "cannot allocate host chunk buffers");
+    auto make = [&](long q0, long q1, int slot) {
         auto c = std::make_unique<Chunk>();
-        build_chunk(b1, h1, b2, h2, off, ids, q0, std::min(h1.n_obj, q0 + chunk_objects), *c);
+        build_chunk(b1, h1, b2, h2, off, ids, q0, q1, bufs[slot], *c);
         return c;
     };
-    std::future<std::unique_ptr<Chunk>> fut;
-    if (h1.n_obj > 0) fut = std::async(std::launch::async, next_chunk, 0L);
-    for (long q0 = 0; q0 < h1.n_obj; q0 += chunk_objects) {
-        std::unique_ptr<Chunk> c = fut.get();
-        const long q1n = q0 + chunk_objects;
-        if (q1n < h1.n_obj) fut = std::async(std::launch::async, next_chunk, q1n);  // overlaps this chunk's join
+    // one chunk on the device; a chunk that exceeds the budget is split in two
+    std::function<int(Chunk&, int)> run = [&](Chunk& c, int slot) -> int {
         ++inf.chunks;
-        inf.h2d_bytes += (double)(c->raw1.size() + c->raw2.size());
-        if (c->sub.empty()) continue;  // no candidates: nothing to report
+        inf.h2d_bytes += (double)(c.len1 + c.len2);
+        if (c.sub.empty()) return TDP_OK;  // no candidates: nothing to report
         tdp_tile *t1 = nullptr, *t2 = nullptr;
         tdp_result* r = nullptr;
-        rc = tdp_tile_upload(ctx, c->raw1.data(), c->raw1.size(), 0, &t1);
-        if (rc == TDP_OK) rc = tdp_tile_upload(ctx, c->raw2.data(), c->raw2.size(), 0, &t2);
+        int rc = tdp_tile_upload(ctx, c.raw1, c.len1, 0, &t1);
+        if (rc == TDP_OK) rc = tdp_tile_upload(ctx, c.raw2, c.len2, 0, &t2);
         if (rc == TDP_OK) rc = tdp_join(ctx, t1, t2, prm, &r);
         if (t1) tdp_tile_free(ctx, t1);
         if (t2) tdp_tile_free(ctx, t2);
+        if (rc == TDP_ERR_NOMEM && c.q1 - c.q0 > 1) {
+            --inf.chunks;
+            inf.h2d_bytes -= (double)(c.len1 + c.len2);
+            ++inf.splits;
+            // the halves reuse this chunk's buffer one after the other
+            const long q0 = c.q0, mid = c.q0 + (c.q1 - c.q0) / 2, q1 = c.q1;
+            auto lo = make(q0, mid, slot);
+            if ((rc = run(*lo, slot)) != TDP_OK) return rc;
+            auto hi = make(mid, q1, slot);
+            return run(*hi, slot);
+        }
+        if (rc != TDP_OK) return rc;
+        inf.tri_pairs += ctx->stats.tri_pairs;
+        inf.join_ms += ctx->stats.total_ms;
+        for (size_t i = 0; i < r->q.size(); ++i) {
+            R->q.push_back(r->q[i] + (int)c.q0);
+            R->t.push_back(c.sub[r->t[i]]);
+            R->d.push_back(r->d[i]);
+        }
+        tdp_result_free(r);
+        return TDP_OK;
+    };
+    std::future<std::unique_ptr<Chunk>> fut;
+    if (!plan.empty()) fut = std::async(std::launch::async, make, plan[0].first, plan[0].second, 0);
+    for (size_t k = 0; k < plan.size(); ++k) {
+        std::unique_ptr<Chunk> c = fut.get();
+        const int slot = (int)(k & 1);
+        if (k + 1 < plan.size())  // the next chunk is assembled into the other buffer meanwhile
+            fut = std::async(std::launch::async, make, plan[k + 1].first, plan[k + 1].second, 1 - slot);
+        rc = run(*c, slot);
         if (rc != TDP_OK) {
             if (fut.valid()) fut.wait();
             return rc;
         }
-        inf.tri_pairs += ctx->stats.tri_pairs;
-        inf.join_ms += ctx->stats.total_ms;
-        for (size_t i = 0; i < r->q.size(); ++i) {
-            R->q.push_back(r->q[i] + (int)c->q0);
-            R->t.push_back(c->sub[r->t[i]]);
-            R->d.push_back(r->d[i]);
-        }
-        tdp_result_free(r);
     }
     size_t in_use = 0, peak = 0;
     tdp_ctx_memory(ctx, &in_use, &peak);

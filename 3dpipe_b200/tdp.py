@@ -328,7 +328,7 @@ EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates",
 
 
 class ChunkedInfo(C.Structure):
-    _fields_ = [("chunks", C.c_long), ("h2d_bytes", C.c_double), ("tri_pairs", C.c_double),
+    _fields_ = [("chunks", C.c_long), ("splits", C.c_long), ("h2d_bytes", C.c_double), ("tri_pairs", C.c_double),
                 ("join_ms", C.c_double), ("device_peak_bytes", C.c_double)]
 
 

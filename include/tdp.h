@@ -196,14 +196,17 @@ int tdp_autotune(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, con
  * budget below the tiles' size).  The candidates are computed on the host for
  * the whole tiles; tile 1 is joined in chunks of chunk_objects query objects,
  * each against a sub-tile of tile 2 holding exactly that chunk's candidates.
- * The result equals tdp_join on the whole tiles (ids and distances).  Device
- * memory is bounded by one chunk, its sub-tile and the join's scratch: pick
- * chunk_objects so that fits the context's budget.  No per-object queries;
+ * The result equals tdp_join on the whole tiles (ids and distances).  Chunks
+ * hold at most chunk_objects query objects and, when the context has a
+ * budget, are cut so that the chunk, its sub-tile and the join's scratch fit
+ * it (estimated from their RAW bytes; a chunk that still runs out of device
+ * memory is split in two and retried).  No per-object queries;
  * tile 2 must be a different tile (no self-join).  No reference counterpart
  * (the reference keeps both tiles decoded in host memory and sizes its device
  * scratch for the whole tile, src/geometry/computing_gpu.cu:4538-4626). */
 typedef struct {
     long chunks;
+    long splits;               /* chunks split in two after running out of memory        */
     double h2d_bytes;          /* RAW bytes uploaded (chunks and sub-tiles)               */
     double tri_pairs;          /* refined triangle pairs, all chunks                      */
     double join_ms;            /* device time of the chunk joins                          */
