@@ -427,9 +427,15 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
                     if (seed < 0) seed = bc * kCl;
                     seed_lb = best;
                 }
-                // a seed whose bound cannot beat a preset minimum is not queued;
-                // the cull below then tests that pair like any other
-                const bool sq = bval && (init_bd == nullptr || seed_lb < bd);
+                // a seed whose bound cannot lower any of the running minima is not
+                // queued (after the first chunk pair the minima are usually tight);
+                // the cull below then tests that pair exactly like any other
+                bool sq = bval;
+                if (bval && seed >= 0) {
+                    const float4 xs = auxA[seed];
+                    const float thr = fmaxf(bd, fmaxf(bl + xs.x + ab.x, bh - xs.y - ab.y));
+                    sq = seed_lb < thr;
+                }
                 if (!sq) seed = -1;
                 const unsigned sqm = __ballot_sync(0xffffffffu, sq);
                 int qn = __popc(sqm);
@@ -468,7 +474,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
                         qn += __popc(m);
                         ++i;
                     }
-                    if (qn == 0) break;
+                    if (qn == 0) {
+                        if (i >= ca) break;  // culled the whole chunk
+                        flush = false;       // nothing queued yet (no seed): cull first
+                        continue;
+                    }
                     const int take = min(qn, 32);
                     __syncwarp();
                     if (lane < take) {
