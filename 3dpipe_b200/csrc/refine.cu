@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
                 int i = 0;
                 bool kc = false;
                 for (;;) {
-                    while (!flush && qn < 32 && i < ca) {
+                    while (!flush && qn < 16 && i < ca) {
                         if ((i & (kCl - 1)) == 0) {
                             kc = false;
                             if (bval) {
@@ -479,15 +479,24 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
                         flush = false;       // nothing queued yet (no seed): cull first
                         continue;
                     }
-                    const int take = min(qn, 32);
+                    // up to 16 pairs per round, two lanes per pair (one half each)
+                    const int take = min(qn, 16);
                     __syncwarp();
-                    if (lane < take) {
-                        const unsigned e = queue[lane];
-                        const int qi = e >> 8, qj = e & 0xff;
-                        PreTri<float> A, B;
-                        load_pre(sA, kCA, qi, A);
-                        load_pre(sB, kCB, qj, B);
-                        const float d = sqrtf(tri_dist2(A, B));
+                    const int pl = lane & 15, part = lane >> 4;
+                    float d2 = FLT_MAX;
+                    int qi = 0, qj = 0;
+                    if (pl < take) {
+                        const unsigned e = queue[pl];
+                        qi = e >> 8;
+                        qj = e & 0xff;
+                        PreTri<float> X, Y;
+                        load_pre(part ? sB : sA, part ? kCB : kCA, part ? qj : qi, X);
+                        load_pre(part ? sA : sB, part ? kCA : kCB, part ? qi : qj, Y);
+                        d2 = tri_dist2_half(X, Y, part);
+                    }
+                    d2 = fminf(d2, __shfl_xor_sync(0xffffffffu, d2, 16));
+                    if (pl < take && part == 0) {
+                        const float d = sqrtf(d2);
                         const float4 xa = auxA[qi], xb = auxB[qj];
                         bd = fminf(bd, d);
                         bl = fminf(bl, fmaxf(d - xa.x - xb.x, 0.f));

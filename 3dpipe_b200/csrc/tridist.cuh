@@ -176,4 +176,48 @@ __host__ __device__ __forceinline__ R tri_dist2(const PreTri<R>& A, const PreTri
     return best;
 }
 
+// One half of tri_dist2, for two lanes that evaluate one pair together: the
+// lane with part 0 holds (X, Y) = (A, B), the lane with part 1 holds (B, A).
+// Each half covers X's three vertex heights, X's edges crossing Y, X's
+// vertices onto Y's face and onto Y's edges, and five (part 0) or four (part
+// 1) of the nine edge pairs, always evaluated with A's edge first exactly as
+// tri_dist2 does; the operands are picked by selects on the part, so both
+// halves run the same instructions (no divergence) and the minimum of the two
+// halves is bit-identical to tri_dist2(A, B).
+template <typename R>
+__host__ __device__ __forceinline__ R tri_dist2_half(const PreTri<R>& X, const PreTri<R>& Y, int part) {
+    R hX[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) hX[k] = dot(X.v[k] - Y.v[0], Y.n);
+    const bool sepX =
+        (hX[0] > R(0) && hX[1] > R(0) && hX[2] > R(0)) || (hX[0] < R(0) && hX[1] < R(0) && hX[2] < R(0));
+    if (!sepX) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (edge_crosses(Y, X, hX, k)) return R(0);
+    }
+    R best = R(3.0e38);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        if (Y.inn > R(0) && foot_inside(Y, X.v[k])) best = fminf_t(best, hX[k] * hX[k] * Y.inn);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) best = fminf_t(best, pt_seg2(X.v[i], Y.v[j], Y.e[j], Y.iee[j]));
+    // edge pairs p = 3 i + j (A's edge i, B's edge j): part 0 takes p = 0..4,
+    // part 1 takes p = 5..8 (its fifth slot repeats p = 8)
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int p0 = k, p1 = k + 5 < 9 ? k + 5 : 8;
+        const int i0 = p0 / 3, j0 = p0 % 3, i1 = p1 / 3, j1 = p1 % 3;
+        // A = X for part 0, A = Y for part 1 (and B the other one)
+        const V3<R> a = part ? Y.v[i1] : X.v[i0], e = part ? Y.e[i1] : X.e[i0];
+        const R ee = part ? Y.ee[i1] : X.ee[i0];
+        const V3<R> b = part ? X.v[j1] : Y.v[j0], f = part ? X.e[j1] : Y.e[j0];
+        const R ff = part ? X.ee[j1] : Y.ee[j0];
+        best = fminf_t(best, edge_pair_interior2(a, e, ee, b, f, ff));
+    }
+    return best;
+}
+
 }  // namespace tdp
