@@ -407,7 +407,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
                 // the seeds are queued and drained before anything is culled
                 int seed = -1;
                 float seed_lb = FLT_MAX;
-                if (bval) {
+                // only while the distance minimum is still unset (the first chunk
+                // pair of an item, or a preset bound): later chunk pairs start from
+                // tight minima and go straight to the cull
+                const bool want_seed = bd == FLT_MAX || init_bd != nullptr;
+                if (bval && want_seed) {
                     float best = FLT_MAX;
                     int bc = 0;
                     for (int c = 0; c < ncl; ++c) {
@@ -430,8 +434,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
                 // a seed whose bound cannot lower any of the running minima is not
                 // queued (after the first chunk pair the minima are usually tight);
                 // the cull below then tests that pair exactly like any other
-                bool sq = bval;
-                if (bval && seed >= 0) {
+                bool sq = bval && want_seed;
+                if (sq && seed >= 0) {
                     const float4 xs = auxA[seed];
                     const float thr = fmaxf(bd, fmaxf(bl + xs.x + ab.x, bh - xs.y - ab.y));
                     sq = seed_lb < thr;
