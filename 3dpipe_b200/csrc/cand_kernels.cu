@@ -273,27 +273,31 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
         if ((rc = upload_grid(ctx, t2->point_grid, hp))) return rc;
     }
     // device copies of both tiles' boxes and transforms
-    Buf& b1 = ctx->scratch[50];
-    Buf& b2 = ctx->scratch[51];
     Buf& kthb = ctx->scratch[52];
     Buf& cntb = ctx->scratch[53];
     Buf& keys = ctx->scratch[54];
     Buf& keys2 = ctx->scratch[55];
     Buf& tmp = ctx->scratch[56];
-    if ((rc = ensure(ctx, b1, (size_t)n1 * 9 * 4 + 64))) return rc;
-    if ((rc = ensure(ctx, b2, (size_t)n2 * 9 * 4 + 64))) return rc;
     if ((rc = ensure(ctx, kthb, (size_t)(n1 + 1) * 8))) return rc;
     if ((rc = ensure(ctx, cntb, (size_t)(n1 + 1) * 8))) return rc;
     if ((rc = ensure(ctx, qoff_buf, (size_t)(n1 + 1) * 8))) return rc;
-    float* box1 = (float*)b1.p;
-    float* xf1 = box1 + 6 * n1;
-    float* box2 = (float*)b2.p;
-    float* xf2 = box2 + 6 * n2;
 #define CU(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } while (0)
-    CU(cudaMemcpyAsync(box1, t1->host.obj_box.data(), n1 * 24, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(xf1, t1->host.obj_xf.data(), n1 * 12, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(box2, t2->host.obj_box.data(), n2 * 24, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(xf2, t2->host.obj_xf.data(), n2 * 12, cudaMemcpyHostToDevice, s));
+    // the tiles' boxes and transforms stay on the device between joins
+    for (const tdp_tile* t : {t1, t2}) {
+        if (t->d_boxes && t->boxes_n == t->n_obj) continue;
+        dfree(ctx, t->d_boxes);
+        t->d_boxes = nullptr;
+        if (dmalloc(ctx, (void**)&t->d_boxes, (size_t)std::max<long>(t->n_obj, 1) * 9 * 4) != cudaSuccess)
+            return fail(ctx, TDP_ERR_NOMEM, "cannot allocate the candidate boxes");
+        CU(cudaMemcpyAsync(t->d_boxes, t->host.obj_box.data(), t->n_obj * 24, cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(t->d_boxes + 6 * t->n_obj, t->host.obj_xf.data(), t->n_obj * 12, cudaMemcpyHostToDevice,
+                           s));
+        t->boxes_n = t->n_obj;
+    }
+    const float* box1 = t1->d_boxes;
+    const float* xf1 = box1 + 6 * n1;
+    const float* box2 = t2->d_boxes;
+    const float* xf2 = box2 + 6 * n2;
     int* d_over = (int*)(ctx->d_counter + 40);
     CU(cudaMemsetAsync(d_over, 0, 4, s));
     const DG bg = dg(t2->box_grid), pg = dg(t2->point_grid);

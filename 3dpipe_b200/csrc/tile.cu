@@ -66,6 +66,7 @@ void tile_release(tdp_ctx* ctx, tdp_tile* t) {
         dfree(ctx, t->tri[l]);
         dfree(ctx, t->vtri[l]);
     }
+    dfree(ctx, t->d_boxes);
     dfree(ctx, t->box_grid.start);
     dfree(ctx, t->box_grid.items);
     dfree(ctx, t->point_grid.start);

@@ -142,6 +142,7 @@ namespace {
 
 void reset_arena(Arena& a) {
     TileHost& H = a.tile.host;
+    a.tile.boxes_n = 0;
     a.tile.n_obj = a.tile.n_vox = 0;
     H.n_obj = H.n_vox = 0;
     H.obj_box.clear();
@@ -241,6 +242,7 @@ int append(tdp_server* S, Arena& a, Request& r, int j) {
     }
     a.tile.n_obj = H.n_obj = o0 + n;
     a.tile.n_vox = H.n_vox = v0 + nv;
+    a.tile.boxes_n = 0;  // the device copy of the boxes is stale
     return TDP_OK;
 }
 
@@ -580,6 +582,7 @@ int tdp_server_destroy(tdp_server* S) {
         if (a.up) cudaStreamSynchronize(a.up);
         tdp_tile& T = a.tile;
         dfree(ctx, T.vox); dfree(ctx, T.obj_vox); dfree(ctx, T.obj_hd); dfree(ctx, T.obj_phd);
+        dfree(ctx, T.d_boxes);
         for (int l = 0; l < kNumLods; ++l) { dfree(ctx, T.tri[l]); dfree(ctx, T.vtri[l]); }
         if (a.ready) cudaEventDestroy(a.ready);
         if (a.up) cudaStreamDestroy(a.up);

@@ -33,6 +33,11 @@ struct DevGrid {
 struct tdp_tile {
     tdp::TileHost host;
     mutable tdp::DevGrid box_grid, point_grid;  // object candidate grids (lazily built)
+    // device copy of the objects' boxes (6 floats each) then transforms (3
+    // each), made on first use by candidate generation; boxes_n != n_obj
+    // (or 0 after a serving-arena append) means stale
+    mutable float* d_boxes = nullptr;
+    mutable long boxes_n = 0;
     long n_obj = 0, n_vox = 0;
     float4* vox = nullptr;
     uint32_t* obj_vox = nullptr;
