@@ -532,6 +532,250 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
     if (lane == 0 && n_full) atomicAdd(n_full, full_evals);
 }
 
+// ------------------------------------------------------------------ tuned form, lazy staging
+// The same algorithm as refine_tuned_kernel (clusters, seed, cull, two-lane
+// drain), but only the bounds are staged: per triangle a bounding sphere and
+// (ph, h, axis projection), 32 bytes instead of the 37-float PreTri.  A lane
+// that evaluates a queued pair loads the pair's two raw triangle records (L1 /
+// L2 hits: the staging just read them) and builds both PreTri in registers,
+// relative to the same origin as the staging would have -- so the distances,
+// and with them the three minima, are bit-identical.  Shared memory per warp
+// drops to about 5 KB, so the A side is staged up to 128 triangles at a time
+// and an item needs far fewer chunk pairs (each of which restages B).
+template <int CA>
+struct LazyLayout {
+    static_assert(CA % kCl == 0 && CA <= 256, "A chunk must be whole clusters and fit the queue's 8-bit index");
+    static constexpr int kNCl = CA / kCl;
+    static constexpr int kOffAuxA = 4 * CA;
+    static constexpr int kOffClS = 8 * CA;
+    static constexpr int kOffClA = kOffClS + 4 * kNCl;
+    static constexpr int kOffAuxB = kOffClA + 4 * kNCl;
+    static constexpr int kOffQueue = kOffAuxB + 4 * kCB;
+    static constexpr int kWarpFloats = kOffQueue + kQueue / 2;
+    static_assert(kWarpFloats % 4 == 0, "float4 arrays must stay 16-byte aligned");
+};
+
+// Bounds of raw triangle record idx relative to o (the formulas of stage_one /
+// tri_sphere): sphere = (centre, radius), aux = (ph, h, projection on u).
+__device__ __forceinline__ void lazy_bounds(const float4* __restrict__ tri, size_t idx, float4 o, float3 u,
+                                            bool far, float& rmax, float4& sph, float4& aux) {
+    const float4* t = tri + idx * kTriF4;
+    const float4 t0 = t[0], t1 = t[1], t2 = t[2];
+    const V3<float> v[3] = {v3(t0.x - o.x, t0.y - o.y, t0.z - o.z), v3(t1.x - o.x, t1.y - o.y, t1.z - o.z),
+                            v3(t2.x - o.x, t2.y - o.y, t2.z - o.z)};
+    const float3 c = make_float3((v[0].x + v[1].x + v[2].x) * (1.f / 3.f), (v[0].y + v[1].y + v[2].y) * (1.f / 3.f),
+                                 (v[0].z + v[1].z + v[2].z) * (1.f / 3.f));
+    float r2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float dx = v[k].x - c.x, dy = v[k].y - c.y, dz = v[k].z - c.z;
+        r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
+        rmax = fmaxf(rmax, fmaxf(fabsf(v[k].x), fmaxf(fabsf(v[k].y), fabsf(v[k].z))));
+    }
+    const float p0 = v[0].x * u.x + v[0].y * u.y + v[0].z * u.z;
+    const float p1 = v[1].x * u.x + v[1].y * u.y + v[1].z * u.z;
+    const float p2 = v[2].x * u.x + v[2].y * u.y + v[2].z * u.z;
+    const float mg = 1e-5f * (fabsf(p0) + fabsf(p1) + fabsf(p2)) + 1e-6f;
+    sph = make_float4(c.x, c.y, c.z, sqrtf(r2) * 1.0001f + 1e-6f);
+    aux = make_float4(t0.w, t1.w, far ? fminf(p0, fminf(p1, p2)) - mg : fmaxf(p0, fmaxf(p1, p2)) + mg, 0.f);
+}
+
+__device__ __forceinline__ void lazy_pre(const float4* __restrict__ t, float4 o, PreTri<float>& P) {
+    const float4 t0 = t[0], t1 = t[1], t2 = t[2];
+    pretri(P, v3(t0.x - o.x, t0.y - o.y, t0.z - o.z), v3(t1.x - o.x, t1.y - o.y, t1.z - o.z),
+           v3(t2.x - o.x, t2.y - o.y, t2.z - o.z));
+}
+
+template <int WARPS, int CA, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const float4* __restrict__ triA,
+                                                                    const float4* __restrict__ triB,
+                                                                    const RefineItem* __restrict__ items,
+                                                                    int n_items_host, const unsigned* n_items_dev,
+                                                                    float4* __restrict__ out,
+                                                                    unsigned* __restrict__ work_counter,
+                                                                    unsigned long long* __restrict__ n_full,
+                                                                    const float* __restrict__ init_bd) {
+    extern __shared__ __align__(16) float smem[];
+    const int n_items = n_items_dev ? (int)*n_items_dev : n_items_host;
+    using L = LazyLayout<CA>;
+    constexpr int kCA = CA;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float* ws = smem + (size_t)wid * L::kWarpFloats;
+    float4* sphA = reinterpret_cast<float4*>(ws);
+    float4* auxA = reinterpret_cast<float4*>(ws + L::kOffAuxA);
+    float4* clS = reinterpret_cast<float4*>(ws + L::kOffClS);
+    float4* clA = reinterpret_cast<float4*>(ws + L::kOffClA);
+    float4* auxB = reinterpret_cast<float4*>(ws + L::kOffAuxB);
+    unsigned short* queue = reinterpret_cast<unsigned short*>(ws + L::kOffQueue);
+    const unsigned lt_mask = (1u << lane) - 1u;
+    unsigned long long full_evals = 0;
+
+    unsigned it = 0;
+    if (lane == 0) it = atomicAdd(work_counter, 1u);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    while (it < (unsigned)n_items) {
+        unsigned next = 0;
+        if (lane == 0) next = atomicAdd(work_counter, 1u);
+        const RefineItem w = items[it];
+        if (w.a_cnt == 0 || w.b_cnt == 0) {
+            if (lane == 0) out[it] = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, 0.f);
+            it = __shfl_sync(0xffffffffu, next, 0);
+            continue;
+        }
+        const float4 o4 = triA[(size_t)w.a_off * kTriF4];
+        float3 u;
+        {
+            const float4 q = triB[(size_t)w.b_off * kTriF4];
+            const float ux = q.x - o4.x, uy = q.y - o4.y, uz = q.z - o4.z;
+            const float n2 = ux * ux + uy * uy + uz * uz;
+            const float inv = n2 > 0.f ? rsqrtf(n2) : 0.f;
+            u = make_float3(ux * inv, uy * inv, uz * inv);
+        }
+        float bd = FLT_MAX, bl = FLT_MAX, bh = FLT_MAX, rmax = 0.f;
+        float b_init = FLT_MAX;
+        if (init_bd) {
+            b_init = init_bd[it];
+            bd = b_init;
+            bl = -FLT_MAX;
+            bh = -FLT_MAX;
+        }
+        for (uint32_t a0 = 0; a0 < w.a_cnt; a0 += kCA) {
+            const int ca = min((uint32_t)kCA, w.a_cnt - a0);
+            const int ncl = (ca + kCl - 1) / kCl;
+            const float4* tA = triA + ((size_t)w.a_off + a0) * kTriF4;
+            __syncwarp();
+            for (int k = lane; k < ca; k += 32) lazy_bounds(tA, k, o4, u, false, rmax, sphA[k], auxA[k]);
+            __syncwarp();
+            build_clusters<CA>(sphA, auxA, ca, clS, clA, lane);
+            for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += kCB) {
+                const int cb = min((uint32_t)kCB, w.b_cnt - b0);
+                const float4* tB = triB + ((size_t)w.b_off + b0) * kTriF4;
+                __syncwarp();
+                const bool bval = lane < cb;
+                float4 sb = make_float4(0.f, 0.f, 0.f, 0.f), ab = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (bval) {
+                    lazy_bounds(tB, lane, o4, u, true, rmax, sb, ab);
+                    auxB[lane] = ab;
+                }
+                __syncwarp();
+                int seed = -1;
+                float seed_lb = FLT_MAX;
+                const bool want_seed = bd == FLT_MAX || init_bd != nullptr;
+                if (bval && want_seed) {
+                    float best = FLT_MAX;
+                    int bc = 0;
+                    for (int c = 0; c < ncl; ++c) {
+                        const float4 s = clS[c];
+                        const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
+                        const float lb = fmaxf(approx_len(dx * dx + dy * dy + dz * dz) - s.w - sb.w, ab.z - clA[c].z);
+                        if (lb < best) { best = lb; bc = c; }
+                    }
+                    best = FLT_MAX;
+                    const int mend = min(ca, (bc + 1) * kCl);
+                    for (int i = bc * kCl; i < mend; ++i) {
+                        const float4 s = sphA[i];
+                        const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
+                        const float lb = fmaxf(approx_len(dx * dx + dy * dy + dz * dz) - s.w - sb.w, ab.z - auxA[i].z);
+                        if (lb < best) { best = lb; seed = i; }
+                    }
+                    if (seed < 0) seed = bc * kCl;
+                    seed_lb = best;
+                }
+                bool sq = bval && want_seed;
+                if (sq && seed >= 0) {
+                    const float4 xs = auxA[seed];
+                    const float thr = fmaxf(bd, fmaxf(bl + xs.x + ab.x, bh - xs.y - ab.y));
+                    sq = seed_lb < thr;
+                }
+                if (!sq) seed = -1;
+                const unsigned sqm = __ballot_sync(0xffffffffu, sq);
+                int qn = __popc(sqm);
+                if (sq) queue[__popc(sqm & lt_mask)] = (unsigned short)((seed << 8) | lane);
+                bool flush = true;
+                int i = 0;
+                bool kc = false;
+                for (;;) {
+                    while (!flush && qn < 16 && i < ca) {
+                        if ((i & (kCl - 1)) == 0) {
+                            kc = false;
+                            if (bval) {
+                                const float4 s = clS[i / kCl], a = clA[i / kCl];
+                                const float thr = fmaxf(bd, fmaxf(bl + a.x + ab.x, bh - a.y - ab.y));
+                                const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
+                                const float reach = s.w + sb.w + thr;
+                                kc = ab.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach;
+                            }
+                            if (!__any_sync(0xffffffffu, kc)) {
+                                i += kCl;
+                                continue;
+                            }
+                        }
+                        bool keep = false;
+                        if (kc && i != seed) {
+                            const float4 s = sphA[i], a = auxA[i];
+                            const float thr = fmaxf(bd, fmaxf(bl + a.x + ab.x, bh - a.y - ab.y));
+                            const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
+                            const float reach = s.w + sb.w + thr;
+                            keep = ab.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach;
+                        }
+                        const unsigned m = __ballot_sync(0xffffffffu, keep);
+                        if (keep) queue[qn + __popc(m & lt_mask)] = (unsigned short)((i << 8) | lane);
+                        qn += __popc(m);
+                        ++i;
+                    }
+                    if (qn == 0) {
+                        if (i >= ca) break;
+                        flush = false;
+                        continue;
+                    }
+                    const int take = min(qn, 16);
+                    __syncwarp();
+                    const int pl = lane & 15, part = lane >> 4;
+                    float d2 = FLT_MAX;
+                    int qi = 0, qj = 0;
+                    if (pl < take) {
+                        const unsigned e = queue[pl];
+                        qi = e >> 8;
+                        qj = e & 0xff;
+                        PreTri<float> X, Y;
+                        lazy_pre(part ? tB + (size_t)qj * kTriF4 : tA + (size_t)qi * kTriF4, o4, X);
+                        lazy_pre(part ? tA + (size_t)qi * kTriF4 : tB + (size_t)qj * kTriF4, o4, Y);
+                        d2 = tri_dist2_half(X, Y, part);
+                    }
+                    d2 = fminf(d2, __shfl_xor_sync(0xffffffffu, d2, 16));
+                    if (pl < take && part == 0) {
+                        const float d = sqrtf(d2);
+                        const float4 xa = auxA[qi], xb = auxB[qj];
+                        bd = fminf(bd, d);
+                        bl = fminf(bl, fmaxf(d - xa.x - xb.x, 0.f));
+                        bh = fminf(bh, d + xa.y + xb.y);
+                        ++full_evals;
+                    }
+                    bd = warp_min_nonneg(bd);
+                    bl = warp_min_nonneg(bl);
+                    bh = warp_min_nonneg(bh);
+                    qn -= take;
+                    const unsigned short moved = lane < qn ? queue[take + lane] : 0;
+                    __syncwarp();
+                    if (lane < qn) queue[lane] = moved;
+                    __syncwarp();
+                    flush = false;
+                    if (i >= ca && qn == 0) break;
+                    if (i >= ca) flush = true;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+        if (init_bd && !(bd < b_init)) bd = FLT_MAX;
+        if (lane == 0) out[it] = make_float4(bd, bl, bh, rmax);
+        it = __shfl_sync(0xffffffffu, next, 0);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) full_evals += __shfl_xor_sync(0xffffffffu, full_evals, o);
+    if (lane == 0 && n_full) atomicAdd(n_full, full_evals);
+}
+
 // ------------------------------------------------------------------ launchers
 constexpr int kPlainBlock = 256;
 constexpr int kTunedWarps = 4;
@@ -551,7 +795,9 @@ cudaError_t launch_refine_plain(const float4* triA, const float4* triB, const Re
 struct TunedCfgDef {
     int chunk_a, ctas_per_sm;
 };
-constexpr TunedCfgDef kTunedCfgs[kTunedConfigs] = {{64, 3}, {48, 3}, {32, 4}};
+// 0-2: PreTri staged in shared memory (refine_tuned_kernel); 3-5: bounds
+// staged, PreTri built per evaluated pair (refine_lazy_kernel)
+constexpr TunedCfgDef kTunedCfgs[kTunedConfigs] = {{64, 3}, {48, 3}, {32, 4}, {128, 3}, {128, 4}, {64, 4}};
 
 TunedConfig tuned_config(int cfg) {
     if (cfg < 0 || cfg >= kTunedConfigs) cfg = 0;
@@ -583,6 +829,23 @@ static cudaError_t launch_tuned_cfg(const float4* triA, const float4* triB, cons
     return cudaGetLastError();
 }
 
+template <int CA, int MINB>
+static cudaError_t launch_lazy_cfg(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
+                                   float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
+                                   cudaStream_t s, const unsigned* n_items_dev, const float* init_bd) {
+    const size_t smem = (size_t)kTunedWarps * LazyLayout<CA>::kWarpFloats * sizeof(float);
+    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB>;
+    cudaError_t e = cudaMemsetAsync(work_counter, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    long want = (long)num_sms * MINB;
+    long need = ((long)n_items + kTunedWarps - 1) / kTunedWarps;
+    int grid = (int)(want < need ? want : need);
+    if (grid < 1) grid = 1;
+    kern<<<grid, kTunedWarps * 32, smem, s>>>(triA, triB, items, n_items, n_items_dev, out, work_counter, n_full,
+                                              init_bd);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                 float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
                                 int cfg, cudaStream_t s, const unsigned* n_items_dev, const float* init_bd) {
@@ -590,6 +853,9 @@ cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const Re
     switch (cfg) {
         case 1: return launch_tuned_cfg<48, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 2: return launch_tuned_cfg<32, 4>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 3: return launch_lazy_cfg<128, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 4: return launch_lazy_cfg<128, 4>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 5: return launch_lazy_cfg<64, 4>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         default: return launch_tuned_cfg<64, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
     }
 }

@@ -83,7 +83,9 @@ int tdp_last_stats(const tdp_ctx *ctx, tdp_stats *out);
 int tdp_fp32_peak(tdp_ctx *ctx, double *tflops);
 /* ---- tuned refine configurations --------------------------------------
  * The tuned refine kernel exists in a few configurations: A-side triangles
- * staged per warp and resident CTAs per SM.  All return identical results;
+ * staged per warp and resident CTAs per SM (configurations 0-2 stage each
+ * triangle's full pre-processed record in shared memory; 3-5 stage only its
+ * bounds and pre-process the triangles of each evaluated pair in registers).  All return identical results;
  * they differ only in speed, which depends on the voxel sizes of the join.
  * A context starts with configuration 0.  The reference has one fixed launch
  * shape (one CTA of 512 threads per voxel pair,
