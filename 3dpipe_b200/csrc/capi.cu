@@ -112,6 +112,7 @@ int tdp_ctx_destroy(tdp_ctx* ctx) {
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->lod_ev) if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->hres) cudaFreeHost(ctx->hres);
     delete ctx;
     return TDP_OK;
 }

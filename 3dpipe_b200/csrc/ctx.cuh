@@ -51,7 +51,9 @@ struct tdp_ctx {
     unsigned* d_counter = nullptr;            // work counters (device)
     unsigned long long* d_stats = nullptr;    // device-side statistics
     tdp::LastStats stats;
-    int tuned_cfg = 0;  // tuned refine kernel configuration (tdp_set_refine_config / tdp_autotune)
+    int tuned_cfg = 0;
+    void* hres = nullptr;  // page-locked staging of join results (grow-only)
+    size_t hres_cap = 0;  // tuned refine kernel configuration (tdp_set_refine_config / tdp_autotune)
 };
 
 namespace tdp {

@@ -92,11 +92,13 @@ __global__ void __launch_bounds__(kBlock) k_pair_bounds(JoinDev d) {
         const uint32_t a0 = d.ovox1[q], a1 = d.ovox1[q + 1], b0 = d.ovox2[t], b1 = d.ovox2[t + 1];
         const int nb = (int)(b1 - b0);
         float m2 = FLT_MAX, M2 = FLT_MAX;
+        bool early = false;  // reported before every voxel pair was seen
+        const float etau = d.early_mixed ? (d.qk[q] == 0 ? d.qtau[q] : -1.f) : d.early_tau;
         if (nb < kPBSmall) {
             __syncwarp();
             for (int i = lane; i < nb * 3; i += 32) sb[w][i] = d.vox2[3 * (size_t)b0 + i];
         }
-        for (uint32_t ac = a0; ac < a1; ac += kPBCap) {
+        for (uint32_t ac = a0; ac < a1 && !early; ac += kPBCap) {
             const int na = (int)min((uint32_t)kPBCap, a1 - ac);
             __syncwarp();
             for (int i = lane; i < na * 3; i += 32) sa[w][i] = d.vox1[3 * (size_t)ac + i];
@@ -104,18 +106,28 @@ __global__ void __launch_bounds__(kBlock) k_pair_bounds(JoinDev d) {
             if (nb >= kPBSmall) {
                 // two tile-2 voxels per lane share every staged tile-1 voxel; a
                 // missing second one repeats the first (harmless for a minimum)
-                for (int b = lane; b < nb; b += 64) {
-                    const float4* v0 = d.vox2 + 3 * ((size_t)b0 + b);
-                    const float4* v1 = b + 32 < nb ? v0 + 96 : v0;
-                    const float4 lo0 = __ldg(v0), hi0 = __ldg(v0 + 1), c0 = __ldg(v0 + 2);
-                    const float4 lo1 = __ldg(v1), hi1 = __ldg(v1 + 1), c1 = __ldg(v1 + 2);
-                    for (int i = 0; i < na; ++i) {
-                        const float4 alo = sa[w][3 * i], ahi = sa[w][3 * i + 1], acr = sa[w][3 * i + 2];
-                        float m, M, m1, M1;
-                        vox_dist2(alo, ahi, acr, lo0, hi0, c0, m, M);
-                        vox_dist2(alo, ahi, acr, lo1, hi1, c1, m1, M1);
-                        m2 = fminf(m2, fminf(m, m1));
-                        M2 = fminf(M2, fminf(M, M1));
+                for (int bb = 0; bb < nb && !early; bb += 64) {
+                    const int b = bb + lane;
+                    if (b < nb) {
+                        const float4* v0 = d.vox2 + 3 * ((size_t)b0 + b);
+                        const float4* v1 = b + 32 < nb ? v0 + 96 : v0;
+                        const float4 lo0 = __ldg(v0), hi0 = __ldg(v0 + 1), c0 = __ldg(v0 + 2);
+                        const float4 lo1 = __ldg(v1), hi1 = __ldg(v1 + 1), c1 = __ldg(v1 + 2);
+                        for (int i = 0; i < na; ++i) {
+                            const float4 alo = sa[w][3 * i], ahi = sa[w][3 * i + 1], acr = sa[w][3 * i + 2];
+                            float m, M, m1, M1;
+                            vox_dist2(alo, ahi, acr, lo0, hi0, c0, m, M);
+                            vox_dist2(alo, ahi, acr, lo1, hi1, c1, m1, M1);
+                            m2 = fminf(m2, fminf(m, m1));
+                            M2 = fminf(M2, fminf(M, M1));
+                        }
+                    }
+                    if (etau >= 0.f) {
+                        // a core distance is a distance between two surface points,
+                        // so it bounds the pair's distance from above: the tuned
+                        // within decision (max + error band <= tau) is final
+                        const float mx = sqrtf(M2);
+                        early = __any_sync(0xffffffffu, mx + kVoxRel * mx <= etau);
                     }
                 }
             } else if (nb > 0) {
@@ -134,6 +146,17 @@ __global__ void __launch_bounds__(kBlock) k_pair_bounds(JoinDev d) {
         }
         m2 = wmin(m2);
         M2 = wmin(M2);
+        if (early) {
+            if (lane == 0) {
+                const float mx = sqrtf(M2);
+                d.pmn[p] = 0.f;  // not computed: the pair is decided
+                d.pmx[p] = mx;
+                d.perr[p] = kVoxRel * mx;
+                d.pstat[p] = kReported;
+                vp += (unsigned long long)(a1 - a0) * (b1 - b0);
+            }
+            continue;
+        }
         if (lane == 0) {
             const float mn = m2 == FLT_MAX ? FLT_MAX : sqrtf(m2);
             const float mx = M2 == FLT_MAX ? FLT_MAX : sqrtf(M2);

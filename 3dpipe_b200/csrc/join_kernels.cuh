@@ -43,6 +43,12 @@ struct JoinDev {
     const float* qtau;
     // intersect query: voxel pairs are kept when their boxes overlap strictly
     int isect;
+    // tuned form: the filter reports a within pair as soon as one voxel pair's
+    // core distance (plus its error band) is within its distance -- early_tau
+    // for a single within query (< 0: off), qtau[q] of within objects when
+    // early_mixed is set
+    float early_tau;
+    int early_mixed;
     // voxel pairs kept after the filter
     int64_t V;
     int* vpa;

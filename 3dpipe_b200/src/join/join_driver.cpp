@@ -172,6 +172,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     d.pstat = buf<uint8_t>(ctx, kPstat); d.pvp = buf<int64_t>(ctx, kPvp);
     d.N1 = (int)t1->n_obj; d.qoff = buf<int64_t>(ctx, kQoff); d.qconf = buf<int>(ctx, kQconf);
     d.qk = dqk; d.qtau = dqtau; d.isect = isect ? 1 : 0;
+    d.early_tau = (tuned && !knn && !mixed && !isect) ? within_dist : -1.f;
+    d.early_mixed = (tuned && mixed) ? 1 : 0;
 
     unsigned* cnt_items = ctx->d_counter + 8;    // [0] items, [2..3] tri-pair sum (u64)
     unsigned* cnt_status = ctx->d_counter + 16;  // undecided, reported
@@ -368,16 +370,47 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     }
     // rows were sorted by (query, result id) on the device
     tdp_result* R = new tdp_result();
-    R->q.resize(nres); R->t.resize(nres); R->d.resize(nres);
     if (nres) {
-        cudaMemcpyAsync(R->q.data(), buf<int>(ctx, kOutQ), nres * 4, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(R->t.data(), buf<int>(ctx, kOutT), nres * 4, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(R->d.data(), buf<float>(ctx, kOutD), nres * 4, cudaMemcpyDeviceToHost, s);
-        if (exact) {
-            R->d64.resize(nres);
-            cudaMemcpyAsync(R->d64.data(), buf<double>(ctx, kOutD64), nres * 8, cudaMemcpyDeviceToHost, s);
+        // through a page-locked staging buffer: a fast copy, then one pass
+        // into the result (no zero-fill of the vectors first)
+        const size_t need = (size_t)nres * (exact ? 20 : 12);
+        if (need > ctx->hres_cap) {
+            if (ctx->hres) cudaFreeHost(ctx->hres);
+            ctx->hres = nullptr;
+            ctx->hres_cap = 0;
+            const size_t cap = need + need / 4 + 4096;
+            if (cudaHostAlloc(&ctx->hres, cap, cudaHostAllocDefault) == cudaSuccess) ctx->hres_cap = cap;
+            else ctx->hres = nullptr;
         }
-        cudaError_t e = cudaStreamSynchronize(s);
+        cudaError_t e;
+        if (ctx->hres) {
+            uint8_t* h = (uint8_t*)ctx->hres;
+            double* h64 = (double*)h;  // 8-byte aligned first
+            int* hq = (int*)(h + (exact ? (size_t)nres * 8 : 0));
+            int* ht = hq + nres;
+            float* hd = (float*)(ht + nres);
+            if (exact) cudaMemcpyAsync(h64, buf<double>(ctx, kOutD64), nres * 8, cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(hq, buf<int>(ctx, kOutQ), nres * 4, cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(ht, buf<int>(ctx, kOutT), nres * 4, cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(hd, buf<float>(ctx, kOutD), nres * 4, cudaMemcpyDeviceToHost, s);
+            e = cudaStreamSynchronize(s);
+            if (e == cudaSuccess) {
+                R->q.assign(hq, hq + nres);
+                R->t.assign(ht, ht + nres);
+                R->d.assign(hd, hd + nres);
+                if (exact) R->d64.assign(h64, h64 + nres);
+            }
+        } else {
+            R->q.resize(nres); R->t.resize(nres); R->d.resize(nres);
+            cudaMemcpyAsync(R->q.data(), buf<int>(ctx, kOutQ), nres * 4, cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(R->t.data(), buf<int>(ctx, kOutT), nres * 4, cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(R->d.data(), buf<float>(ctx, kOutD), nres * 4, cudaMemcpyDeviceToHost, s);
+            if (exact) {
+                R->d64.resize(nres);
+                cudaMemcpyAsync(R->d64.data(), buf<double>(ctx, kOutD64), nres * 8, cudaMemcpyDeviceToHost, s);
+            }
+            e = cudaStreamSynchronize(s);
+        }
         if (e != cudaSuccess) { delete R; return fail(ctx, TDP_ERR_CUDA, cudaGetErrorString(e)); }
     }
     float f_ms = 0, tot_ms = 0;

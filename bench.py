@@ -546,7 +546,7 @@ def main():
             "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")} if cpu else None,
             "stats": {k: st_t[k] for k in ("full_evals", "refine_items", "recheck_pairs", "filter_pairs",
                                            "filter_voxel_pairs", "kernel_launches", "candidates_ms", "lod_ms",
-                                           "host_syncs")},
+                                           "host_syncs", "total_ms")},
         }
         print(json.dumps(line))
     if ws > 1:
