@@ -330,6 +330,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream measurement")
     ap.add_argument("--no-self", action="store_true", help="skip the 10-NN self-join measurement")
+    ap.add_argument("--refine-config", type=int, default=-1,
+                    help="tuned refine configuration (default: autotuned in the warm-up)")
     ap.add_argument("--out-of-core", action="store_true",
                     help="config 4 instead: the chunked 10-NN join under a device budget (its own JSON line)")
     ap.add_argument("--ooc-vessels", type=int, default=10000)
@@ -390,8 +392,13 @@ def main():
         t = time.time()
         T1, T2 = pkg.tdp.Tile(ctx, nb), pkg.tdp.Tile(ctx, vb)
         log(f"[rank {rank}] tiles resident in {time.time() - t:.1f}s, {ctx.memory()[0] / 1e9:.1f} GB on device")
-        # pick the tuned refine kernel's configuration on this join (untimed)
-        best_cfg, cfg_ms = ctx.autotune(T1, T2, query="within", within=TAU)
+        # pick the tuned refine kernel's configuration on this join (untimed),
+        # or take the one given on the command line
+        if a.refine_config >= 0:
+            ctx.set_refine_config(a.refine_config)
+            best_cfg, cfg_ms = a.refine_config, []
+        else:
+            best_cfg, cfg_ms = ctx.autotune(T1, T2, query="within", within=TAU)
         cfg_defs = pkg.tdp.refine_configs()
         log(f"[rank {rank}] autotune: refine ms per configuration {[round(m, 3) for m in cfg_ms]} -> {best_cfg}")
         # the two forms must agree before anything is timed
@@ -499,7 +506,7 @@ def main():
         cpu = cpu_reference(nb, vb, 3, 0, a.cpu_sample, target_s=5.0)
     # DRAM bytes per refine launch from the committed ncu capture of this workload
     traffic = None
-    prof = ROOT / "profiles" / "refine_tuned_within400.md"
+    prof = ROOT / "profiles" / "refine_within400.md"
     if prof.exists():
         for ln in prof.read_text().splitlines():
             if ln.startswith("traffic_bytes_per_launch:"):
@@ -531,8 +538,8 @@ def main():
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
                          "traffic_source": "DRAM read+write bytes per launch, ncu 1-pass capture of this workload "
-                                           "(profiles/refine_tuned_within400.md)",
-                         "kernel": "refine_tuned_kernel",
+                                           "(profiles/refine_within400.md)",
+                         "kernel": "refine_lazy_kernel" if best_cfg >= 3 else "refine_tuned_kernel",
                          "peak_source": "measured FP32 FMA probe (tdp_fp32_peak); MEASURED_PEAKS.json has no CUDA-core FP32 figure",
                          "work": f"full evals x {F_TRI:.0f} + culled pairs x {F_CULL:.0f} FLOPs",
                          "tri_pair_equivalent": {
