@@ -111,6 +111,7 @@ int tdp_ctx_destroy(tdp_ctx* ctx) {
     for (void* p : ptrs) dfree(ctx, p);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->lod_ev) if (e) cudaEventDestroy(e);
+    if (ctx->lod_graph) cudaGraphExecDestroy(ctx->lod_graph);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->hres) cudaFreeHost(ctx->hres);
     delete ctx;
@@ -140,6 +141,14 @@ int tdp_last_stats(const tdp_ctx* ctx, tdp_stats* o) {
     o->exact_items = s.exact_items;
     o->exact_f64_items = s.exact_f64_items;
     o->fp32_max_rel_err = s.fp32_max_rel_err;
+    o->lod_graph = s.lod_graph;
+    return TDP_OK;
+}
+
+int tdp_set_lod_graph(tdp_ctx* ctx, int mode) {
+    if (!ctx) return TDP_ERR_ARG;
+    if (mode < TDP_LOD_GRAPH_OFF || mode > TDP_LOD_GRAPH_ALWAYS) return fail(ctx, TDP_ERR_ARG, "LOD graph mode must be 0, 1 or 2");
+    ctx->lod_graph_mode = mode;
     return TDP_OK;
 }
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <string>
 #include <unordered_map>
+#include <vector>
 #include "common.cuh"
 #include "../../include/tdp.h"
 
@@ -34,6 +35,7 @@ struct LastStats {
     long exact_items = 0;            // LOD-100 voxel pairs it refined in FP32
     long exact_f64_items = 0;        // of those, evaluated in FP64
     double fp32_max_rel_err = 0;     // max |FP32 minimum - FP64 distance| / max(distance, 1)
+    long lod_graph = 0;              // tuned LOD loop: 0 direct launches, 1 graph replayed, 2 graph captured
 };
 
 }  // namespace tdp
@@ -51,9 +53,15 @@ struct tdp_ctx {
     unsigned* d_counter = nullptr;            // work counters (device)
     unsigned long long* d_stats = nullptr;    // device-side statistics
     tdp::LastStats stats;
-    int tuned_cfg = 0;
+    int tuned_cfg = 0;  // tuned refine kernel configuration (tdp_set_refine_config / tdp_autotune)
     void* hres = nullptr;  // page-locked staging of join results (grow-only)
-    size_t hres_cap = 0;  // tuned refine kernel configuration (tdp_set_refine_config / tdp_autotune)
+    size_t hres_cap = 0;
+    // CUDA graph of the tuned form's LOD loop (tdp_set_lod_graph): the
+    // executable, the launch arguments it was captured with, and the last
+    // arguments launched directly (auto mode captures a key on its second use)
+    int lod_graph_mode = TDP_LOD_GRAPH_AUTO;
+    cudaGraphExec_t lod_graph = nullptr;
+    std::vector<unsigned char> lod_key, lod_seen;
 };
 
 namespace tdp {

@@ -795,9 +795,10 @@ cudaError_t launch_refine_plain(const float4* triA, const float4* triB, const Re
 struct TunedCfgDef {
     int chunk_a, ctas_per_sm;
 };
-// 0-2: PreTri staged in shared memory (refine_tuned_kernel); 3-5: bounds
+// 0-2: PreTri staged in shared memory (refine_tuned_kernel); 3-7: bounds
 // staged, PreTri built per evaluated pair (refine_lazy_kernel)
-constexpr TunedCfgDef kTunedCfgs[kTunedConfigs] = {{64, 3}, {48, 3}, {32, 4}, {128, 3}, {128, 4}, {64, 4}};
+constexpr TunedCfgDef kTunedCfgs[kTunedConfigs] = {{64, 3}, {48, 3}, {32, 4}, {128, 3}, {128, 4}, {64, 4},
+                                                    {128, 5}, {128, 6}};
 
 TunedConfig tuned_config(int cfg) {
     if (cfg < 0 || cfg >= kTunedConfigs) cfg = 0;
@@ -855,6 +856,8 @@ cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const Re
         case 2: return launch_tuned_cfg<32, 4>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 3: return launch_lazy_cfg<128, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 4: return launch_lazy_cfg<128, 4>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 6: return launch_lazy_cfg<128, 5>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 7: return launch_lazy_cfg<128, 6>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 5: return launch_lazy_cfg<64, 4>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         default: return launch_tuned_cfg<64, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
     }

@@ -51,6 +51,125 @@ enum Slot {
 template <typename T>
 T* buf(tdp_ctx* ctx, int slot) { return (T*)ctx->scratch[slot].p; }
 
+// Everything the tuned form's LOD loop (and the FP64 recheck after it) hands
+// to its launches.  The loop's launches are a pure function of these bytes, so
+// they are also the key of the context's cached CUDA graph of the loop: an
+// equal key replays the graph, any difference (a grown scratch buffer, another
+// tile, V, the LOD list, the refine configuration) captures it again.
+struct LodLoop {
+    JoinDev d;
+    int nl, li[8], highest_k;
+    const float4 *tri1[8], *tri2[8];
+    const uint32_t *vt1[8], *vt2[8];
+    const float4 *tri1_100, *tri2_100;
+    const uint32_t *vt1_100, *vt2_100;
+    RefineItem* items;
+    int* item_vp;
+    float4* res;
+    unsigned* counter;
+    unsigned long long* dstats;
+    int num_sms, cfg, hlevel, any_knn, any_within, K, knn, recheck;
+    int64_t V;
+    float tau;
+    int* rankst;
+    double *vexact, *res64, *pexact;
+    cudaEvent_t ev[16];
+};
+
+// Enqueue the loop on s.  While s is being captured, the per-LOD timing events
+// become event-record nodes of the graph (cudaEventRecordExternal), so that
+// a replay still times every refine launch.
+int enqueue_lod_loop(tdp_ctx* ctx, const LodLoop& L, cudaStream_t s, bool capturing) {
+#define CUL(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } while (0)
+    auto rec = [&](cudaEvent_t e) {
+        return capturing ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal) : cudaEventRecord(e, s);
+    };
+    unsigned* cnt_items = L.counter + 8;     // [0] items, [2..3] tri-pair sum (u64)
+    unsigned* lod_counts = L.counter + 24;   // per-LOD item counts
+    unsigned* cnt_recheck = L.counter + 32;  // pairs left for the FP64 recheck
+    const int V = (int)L.V;
+    CUL(cudaMemsetAsync(L.counter + 8, 0, 26 * sizeof(unsigned), s));
+    CUL(cudaMemsetAsync(L.dstats, 0, 8, s));
+    for (int k = 0; k < L.nl; ++k) {
+        const int highest = k == L.highest_k;
+        CUL(cudaMemsetAsync(cnt_items, 0, 4, s));
+        CUL(launch_build_items(L.d, L.vt1[k], L.vt2[k], L.items, L.item_vp, cnt_items, s));
+        CUL(cudaMemcpyAsync(lod_counts + k, cnt_items, 4, cudaMemcpyDeviceToDevice, s));
+        CUL(rec(L.ev[2 * k]));
+        CUL(launch_refine_tuned(L.tri1[k], L.tri2[k], L.items, V, L.res, L.counter, L.dstats, L.num_sms, L.cfg, s,
+                                cnt_items));
+        CUL(rec(L.ev[2 * k + 1]));
+        CUL(launch_apply_results(L.d, L.res, L.item_vp, V, highest, L.hlevel, L.li[k], k, s, cnt_items));
+        CUL(launch_pair_update(L.d, k, 1, s));
+        if (L.any_knn) CUL(launch_knn_rank(L.d, L.K, 1, L.rankst, s));
+        if (L.any_within) CUL(launch_within_decide(L.d, L.tau, 1, s));
+    }
+    if (L.recheck) {
+        CUL(launch_count_status(L.d, cnt_recheck, s));
+        CUL(cudaMemsetAsync(cnt_items, 0, 4, s));
+        CUL(launch_recheck_items(L.d, L.vt1_100, L.vt2_100, L.items, L.item_vp, L.vexact, cnt_items, s));
+        CUL(launch_refine_f64(L.tri1_100, L.tri2_100, L.items, V, L.res64, s, cnt_items));
+        CUL(launch_recheck_finish(L.d, L.res64, L.item_vp, V, L.vexact, L.pexact, L.knn, L.K, L.tau, s, cnt_items));
+    }
+#undef CUL
+    return TDP_OK;
+}
+
+// Run the loop directly or through the context's graph (tdp_set_lod_graph).
+// *how: 0 launched directly, 1 replayed the cached graph, 2 captured it now.
+int run_lod_loop(tdp_ctx* ctx, const LodLoop& L, cudaStream_t s, long* how) {
+    *how = 0;
+    const unsigned char* kb = reinterpret_cast<const unsigned char*>(&L);
+    auto equal = [&](const std::vector<unsigned char>& v) {
+        return v.size() == sizeof(LodLoop) && std::memcmp(v.data(), kb, sizeof(LodLoop)) == 0;
+    };
+    const int mode = ctx->lod_graph_mode;
+    if (mode == TDP_LOD_GRAPH_OFF) return enqueue_lod_loop(ctx, L, s, false);
+    if (ctx->lod_graph && equal(ctx->lod_key)) {
+        *how = 1;
+        const cudaError_t e = cudaGraphLaunch(ctx->lod_graph, s);
+        return e == cudaSuccess ? TDP_OK : fail(ctx, TDP_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+    }
+    if (mode == TDP_LOD_GRAPH_AUTO && !equal(ctx->lod_seen)) {
+        // a key seen for the first time runs directly: one-off joins (a served
+        // batch) never pay for a capture
+        ctx->lod_seen.assign(kb, kb + sizeof(LodLoop));
+        return enqueue_lod_loop(ctx, L, s, false);
+    }
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return fail(ctx, TDP_ERR_CUDA, std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e));
+    const int rc = enqueue_lod_loop(ctx, L, s, true);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(s, &g);
+    if (rc != TDP_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return rc != TDP_OK ? rc : fail(ctx, TDP_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+    }
+    ctx->lod_key.clear();
+    if (ctx->lod_graph) {
+        // same launch sequence with other arguments: update the executable in place
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(ctx->lod_graph, g, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(ctx->lod_graph);
+            ctx->lod_graph = nullptr;
+        }
+    }
+    if (!ctx->lod_graph) {
+        e = cudaGraphInstantiate(&ctx->lod_graph, g, 0);
+        if (e != cudaSuccess) {
+            ctx->lod_graph = nullptr;
+            cudaGraphDestroy(g);
+            return fail(ctx, TDP_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+        }
+    }
+    cudaGraphDestroy(g);
+    ctx->lod_key.assign(kb, kb + sizeof(LodLoop));
+    *how = 2;
+    e = cudaGraphLaunch(ctx->lod_graph, s);
+    return e == cudaSuccess ? TDP_OK : fail(ctx, TDP_ERR_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+}
+
 }  // namespace
 }  // namespace tdp
 
@@ -163,7 +282,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     ENS(kPvp, (Pz + 1) * 8); ENS(kQconf, (t1->n_obj + 1) * 4); ENS(kCnt, (Pz + 1) * 8); ENS(kRankSt, Pz * 4);
     ENS(kOutQ, Pz * 4); ENS(kOutT, Pz * 4); ENS(kOutD, Pz * 4);
 
-    JoinDev d{};
+    JoinDev d;
+    std::memset(&d, 0, sizeof d);  // padding too: the LOD loop's graph key holds these bytes
     d.vox1 = t1->vox; d.ovox1 = t1->obj_vox; d.vox2 = t2->vox; d.ovox2 = t2->obj_vox;
     d.ohd1 = t1->obj_hd; d.ophd1 = t1->obj_phd; d.ohd2 = t2->obj_hd; d.ophd2 = t2->obj_phd;
     d.P = (int)P;
@@ -229,8 +349,6 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     long refine_items = 0;
     unsigned undecided = 0;
     long syncs = 2;  // candidates upload + voxel-pair count
-    unsigned* lod_counts = ctx->d_counter + 24;   // per-LOD item counts (tuned form)
-    unsigned* cnt_recheck = ctx->d_counter + 32;  // pairs left for the FP64 recheck
     if (!tuned) {
         // plain form: the host reads every count, like the reference's chunk loop
         for (size_t k = 0; k < lods.size() && V > 0; ++k) {
@@ -277,38 +395,34 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         // the FP64 recheck) is enqueued without a host round trip; kernels with
         // nothing left to do exit at once
         ENS(kVexact, Vz * 8); ENS(kPexact, Pz * 8); ENS(kRes64, Vz * 8);
-        CU(cudaMemsetAsync(ctx->d_counter + 8, 0, 26 * sizeof(unsigned), s));
-        CU(cudaMemsetAsync(ctx->d_stats, 0, 8, s));
-        for (size_t k = 0; k < lods.size(); ++k) {
+        // 3b. after LOD 100, the FP64 recheck of pairs whose FP32 ranges
+        // stayed inside their error band
+        LodLoop L;
+        std::memset(&L, 0, sizeof L);  // padding included: the bytes are the graph's key
+        L.d = d;
+        L.nl = (int)lods.size();
+        L.highest_k = L.nl - 1;
+        for (int k = 0; k < L.nl; ++k) {
             const int li = lod_index(lods[k]);
-            const bool highest = (k + 1 == lods.size());
-            CU(cudaMemsetAsync(cnt_items, 0, 4, s));
-            CU(launch_build_items(d, t1->vtri[li], t2->vtri[li], items, item_vp, cnt_items, s)); ++launches;
-            CU(cudaMemcpyAsync(lod_counts + k, cnt_items, 4, cudaMemcpyDeviceToDevice, s));
-            CU(cudaEventRecord(ctx->lod_ev[2 * k], s));
-            CU(launch_refine_tuned(t1->tri[li], t2->tri[li], items, (int)V, res, ctx->d_counter, ctx->d_stats,
-                                   ctx->num_sms, ctx->tuned_cfg, s, cnt_items));
-            CU(cudaEventRecord(ctx->lod_ev[2 * k + 1], s));
-            ++launches;
-            st.refine_launches++;
-            CU(launch_apply_results(d, res, item_vp, (int)V, highest, prm->hausdorff_level, li, (int)k, s, cnt_items));
-            CU(launch_pair_update(d, (int)k, 1, s));
-            if (any_knn) CU(launch_knn_rank(d, prm->knn, 1, buf<int>(ctx, kRankSt), s));
-            if (any_within) CU(launch_within_decide(d, within_dist, 1, s));
-            launches += 3;
+            L.li[k] = li;
+            L.tri1[k] = t1->tri[li]; L.tri2[k] = t2->tri[li];
+            L.vt1[k] = t1->vtri[li]; L.vt2[k] = t2->vtri[li];
+            L.ev[2 * k] = ctx->lod_ev[2 * k];
+            L.ev[2 * k + 1] = ctx->lod_ev[2 * k + 1];
         }
-        // ---- 3b. FP64 recheck of pairs whose FP32 ranges stayed inside their
-        // error band through LOD 100 ----
-        if (lods.back() == 100) {
-            double* vexact = buf<double>(ctx, kVexact);
-            CU(launch_count_status(d, cnt_recheck, s));
-            CU(cudaMemsetAsync(cnt_items, 0, 4, s));
-            CU(launch_recheck_items(d, t1->vtri[4], t2->vtri[4], items, item_vp, vexact, cnt_items, s));
-            CU(launch_refine_f64(t1->tri[4], t2->tri[4], items, (int)V, buf<double>(ctx, kRes64), s, cnt_items));
-            CU(launch_recheck_finish(d, buf<double>(ctx, kRes64), item_vp, (int)V, vexact, buf<double>(ctx, kPexact),
-                                     knn, prm->knn, within_dist, s, cnt_items));
-            launches += knn ? 6 : 5;
-        }
+        L.recheck = lods.back() == 100;
+        L.tri1_100 = t1->tri[4]; L.tri2_100 = t2->tri[4];
+        L.vt1_100 = t1->vtri[4]; L.vt2_100 = t2->vtri[4];
+        L.items = items; L.item_vp = item_vp; L.res = res;
+        L.counter = ctx->d_counter; L.dstats = ctx->d_stats;
+        L.num_sms = ctx->num_sms; L.cfg = ctx->tuned_cfg; L.hlevel = prm->hausdorff_level;
+        L.any_knn = any_knn; L.any_within = any_within; L.K = prm->knn; L.knn = knn;
+        L.V = V; L.tau = within_dist;
+        L.rankst = buf<int>(ctx, kRankSt);
+        L.vexact = buf<double>(ctx, kVexact); L.res64 = buf<double>(ctx, kRes64); L.pexact = buf<double>(ctx, kPexact);
+        if ((rc = run_lod_loop(ctx, L, s, &st.lod_graph))) return rc;
+        launches += 5 * L.nl + (L.recheck ? (knn ? 6 : 5) : 0);
+        st.refine_launches += L.nl;
     }
 
     // ---- 4. exact LOD-100 distances of the reported pairs (optional) ----

@@ -43,7 +43,7 @@ class Stats(C.Structure):
                 ("filter_voxel_pairs", C.c_double), ("kernel_launches", C.c_long),
                 ("candidates_ms", C.c_double), ("lod_ms", C.c_double), ("host_syncs", C.c_long),
                 ("exact_ms", C.c_double), ("exact_items", C.c_long), ("exact_f64_items", C.c_long),
-                ("fp32_max_rel_err", C.c_double)]
+                ("fp32_max_rel_err", C.c_double), ("lod_graph", C.c_long)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -160,6 +160,14 @@ class Context:
         L.tdp_ctx_stream.argtypes = [C.c_void_p]
         L.tdp_ctx_stream.restype = C.c_void_p
         return L.tdp_ctx_stream(self._h) or 0
+
+    def set_lod_graph(self, mode: int):
+        """How the tuned LOD loop launches: LOD_GRAPH_OFF (directly), LOD_GRAPH_AUTO
+        (default: a CUDA graph captured on the second join with the same launch
+        arguments, replayed after that) or LOD_GRAPH_ALWAYS."""
+        L = lib()
+        L.tdp_set_lod_graph.argtypes = [C.c_void_p, C.c_int]
+        self.check(L.tdp_set_lod_graph(self._h, int(mode)))
 
     def memory(self):
         a, b = C.c_size_t(), C.c_size_t()
@@ -324,7 +332,9 @@ EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates",
              "tdp_refine_config_count", "tdp_refine_config_info", "tdp_set_refine_config", "tdp_get_refine_config",
              "tdp_autotune", "tdp_result_copy_f64", "tdp_server_default_params", "tdp_server_create",
              "tdp_server_submit", "tdp_server_wait", "tdp_server_get_stats", "tdp_server_destroy",
-             "tdp_join_chunked"]
+             "tdp_join_chunked", "tdp_set_lod_graph"]
+
+LOD_GRAPH_OFF, LOD_GRAPH_AUTO, LOD_GRAPH_ALWAYS = 0, 1, 2
 
 
 class ChunkedInfo(C.Structure):

@@ -76,6 +76,9 @@ typedef struct {
     long exact_f64_items;            /* of those, evaluated in FP64             */
     double fp32_max_rel_err;         /* exact stage: max |FP32 minimum - FP64
                                         distance| / max(distance, 1)           */
+    long lod_graph;                  /* tuned LOD loop: 0 launched directly,
+                                        1 replayed the context's CUDA graph,
+                                        2 captured (or updated) it in this call */
 } tdp_stats;
 int tdp_last_stats(const tdp_ctx *ctx, tdp_stats *out);
 /* measured FP32 FMA throughput of the context's device in TFLOP/s (CUDA cores,
@@ -84,7 +87,7 @@ int tdp_fp32_peak(tdp_ctx *ctx, double *tflops);
 /* ---- tuned refine configurations --------------------------------------
  * The tuned refine kernel exists in a few configurations: A-side triangles
  * staged per warp and resident CTAs per SM (configurations 0-2 stage each
- * triangle's full pre-processed record in shared memory; 3-5 stage only its
+ * triangle's full pre-processed record in shared memory; 3-7 stage only its
  * bounds and pre-process the triangles of each evaluated pair in registers).  All return identical results;
  * they differ only in speed, which depends on the voxel sizes of the join.
  * A context starts with configuration 0.  The reference has one fixed launch
@@ -95,6 +98,23 @@ int tdp_refine_config_count(void);
 int tdp_refine_config_info(int cfg, int *chunk_a, int *ctas_per_sm);
 int tdp_set_refine_config(tdp_ctx *ctx, int cfg);
 int tdp_get_refine_config(const tdp_ctx *ctx, int *cfg);
+
+/* ---- CUDA graph of the LOD loop --------------------------------------
+ * The tuned form's LOD loop (per LOD: item build, refine, bound update,
+ * decision; then the FP64 recheck) is a fixed sequence of about 30 launches
+ * whose counts stay in device memory.  A context can capture it as a CUDA
+ * graph and replay it while the loop's launch arguments (tiles, buffers,
+ * voxel-pair count, LOD list, query, refine configuration) stay the same:
+ *   TDP_LOD_GRAPH_OFF     launch directly, always;
+ *   TDP_LOD_GRAPH_AUTO    (default) capture arguments on their second use, so
+ *                         one-off joins (served batches) launch directly and
+ *                         repeated joins replay the graph;
+ *   TDP_LOD_GRAPH_ALWAYS  capture whenever the arguments change.
+ * Results are identical in every mode.  No reference counterpart: the
+ * reference launches and synchronises per chunk and per LOD
+ * (src/join/KNNJoin.cpp:1596-1714). */
+enum { TDP_LOD_GRAPH_OFF = 0, TDP_LOD_GRAPH_AUTO = 1, TDP_LOD_GRAPH_ALWAYS = 2 };
+int tdp_set_lod_graph(tdp_ctx *ctx, int mode);
 
 /* The context's CUDA stream (a cudaStream_t), on which every tdp call that
  * takes this context launches its work: callers order their own work, or

@@ -249,6 +249,58 @@ def test_mixed_queries_equal_separate_joins(pkg, ctx, gpu_tiles):
                 assert np.all(counts == K)
 
 
+def test_lod_graph_modes_identical(pkg):
+    """The tuned LOD loop launched directly, captured as a CUDA graph, and
+    replayed from the graph returns the same ids and distances.  Auto mode
+    launches new arguments directly, captures them on their second use and
+    replays them after that; a change of arguments (query, distance, LOD list,
+    self-join) captures or updates the graph again; the per-LOD refine timing
+    still works in a replay.  A join whose filter decides every pair has no
+    LOD loop (no refine launch) and so no graph."""
+    c = pkg.Context(0)
+    try:
+        nb, vb = tiles(6, 12, 101)
+        T1, T2 = pkg.tdp.Tile(c, nb), pkg.tdp.Tile(c, vb)
+        runs = [(T2, dict(query="nn", knn=3)), (T2, dict(query="within", within=150.0)),
+                (T2, dict(query="nn", knn=1, lods=[40, 100])), (T2, dict(query="within", within=60.0, lods=[40, 100])),
+                (T2, dict(query="nn", knn=2, lods=[20, 60, 100])), (None, dict(query="within", within=60.0)),
+                (None, dict(query="nn", knn=4)), (T2, dict(query="nn", knn=3, lods=[20, 40]))]
+        want, looped = {}, {}
+        for i, (t2, args) in enumerate(runs):
+            nl = len(args.get("lods") or [20, 40, 60, 80, 100])
+            c.set_lod_graph(pkg.tdp.LOD_GRAPH_OFF)
+            want[i] = c.join(T1, t2, **args)
+            st = c.stats()
+            assert st["lod_graph"] == 0
+            looped[i] = st["refine_launches"] > 0
+            c.set_lod_graph(pkg.tdp.LOD_GRAPH_AUTO)
+            how = []
+            for _ in range(3):
+                got = c.join(T1, t2, **args)
+                st = c.stats()
+                how.append(st["lod_graph"])
+                assert st["refine_launches"] == (nl if looped[i] else 0)
+                if looped[i]:
+                    assert st["refine_ms"] > 0
+                for a, b in zip(got, want[i]):
+                    np.testing.assert_array_equal(a, b)
+            assert how == ([0, 2, 1] if looped[i] else [0, 0, 0]), (args, how)
+        assert sum(looped.values()) >= 4
+        c.set_lod_graph(pkg.tdp.LOD_GRAPH_ALWAYS)
+        for i, (t2, args) in enumerate(runs):
+            for expect in ((2, 1) if looped[i] else (0, 0)):
+                got = c.join(T1, t2, **args)
+                assert c.stats()["lod_graph"] == expect
+                for a, b in zip(got, want[i]):
+                    np.testing.assert_array_equal(a, b)
+        with pytest.raises(pkg.TdpError):
+            c.set_lod_graph(3)
+        T1.free()
+        T2.free()
+    finally:
+        c.close()
+
+
 def test_intersect_join_matches_fp64_truth(pkg, ctx):
     """-q intersect: the pairs whose boxes overlap strictly and whose LOD-100
     meshes touch or cross (exact FP64 distance 0); both forms."""
