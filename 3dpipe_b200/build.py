@@ -28,6 +28,9 @@ CXX = shutil.which("g++") or "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                      "--expt-relaxed-constexpr", "-I", str(ROOT / "include"), "-I", str(PKG / "src")]
+# bounds_kernels.cu: no contraction of a*b+c into an FMA, so its FP64 values are
+# those of the same expressions rounded one operation at a time (as on the host)
+PER_FILE_FLAGS = {"bounds_kernels.cu": ["-fmad=false"]}
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-Wall", "-Wno-unused-function",
              "-I", str(ROOT / "include"), "-I", str(PKG / "src"),
              "-I", "/usr/local/cuda/include"]
@@ -55,7 +58,7 @@ def _compile(src: Path, force: bool, hdr_time: float) -> Path:
         return obj
     obj.parent.mkdir(parents=True, exist_ok=True)
     if src.suffix == ".cu":
-        cmd = [NVCC, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+        cmd = [NVCC, *NVCC_FLAGS, *PER_FILE_FLAGS.get(src.name, []), "-c", str(src), "-o", str(obj)]
     else:
         cmd = [CXX, *CXX_FLAGS, "-c", str(src), "-o", str(obj)]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -336,6 +336,44 @@ EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates",
 
 LOD_GRAPH_OFF, LOD_GRAPH_AUTO, LOD_GRAPH_ALWAYS = 0, 1, 2
 
+EXPORTED += ["tdp_tile_compute_bounds", "tdp_raw_compute_bounds"]
+
+
+class BoundsInfo(C.Structure):
+    _fields_ = [("ms", C.c_double), ("objects", C.c_long), ("triangles", C.c_long), ("facet_queries", C.c_long),
+                ("pieces", C.c_long), ("dist_evals", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def _compute_bounds(self, tile: "Tile") -> dict:
+    """Recompute the per-triangle (proxy, hausdorff) bounds and the object-level
+    values of a resident tile on the GPU, in place; returns the kernel stats."""
+    L = lib()
+    L.tdp_tile_compute_bounds.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(BoundsInfo)]
+    info = BoundsInfo()
+    self.check(L.tdp_tile_compute_bounds(self._h, tile.handle, C.byref(info)))
+    return info.as_dict()
+
+
+def _raw_compute_bounds(self, raw, out=None):
+    """RAW tile bytes -> (the same bytes with GPU-computed bounds, stats).  `out`
+    (uint8, raw's size) receives the result; it may be `raw` itself."""
+    L = lib()
+    L.tdp_raw_compute_bounds.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.POINTER(BoundsInfo)]
+    src = np.ascontiguousarray(raw, np.uint8)
+    dst = np.empty_like(src) if out is None else out
+    if dst.nbytes != src.nbytes or not dst.flags.c_contiguous:
+        raise ValueError("out must be a contiguous buffer of the tile's size")
+    info = BoundsInfo()
+    self.check(L.tdp_raw_compute_bounds(self._h, _ptr(src), src.nbytes, _ptr(dst), C.byref(info)))
+    return dst, info.as_dict()
+
+
+Context.compute_bounds = _compute_bounds
+Context.raw_compute_bounds = _raw_compute_bounds
+
 
 class ChunkedInfo(C.Structure):
     _fields_ = [("chunks", C.c_long), ("splits", C.c_long), ("h2d_bytes", C.c_double), ("tri_pairs", C.c_double),

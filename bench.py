@@ -265,6 +265,51 @@ def run_serving(pkg, ctx, T2, nb, rates, per_rate_cap=600, seconds=3.0, pool_siz
             "rates": out}
 
 
+def run_bounds_prep(pkg, ctx, nb, vb, n_nuclei=20000):
+    """GPU preparation of the per-triangle bounds (tdp_tile_compute_bounds) on
+    the first n_nuclei objects of the query tile and on the whole vessel tile,
+    each on its own resident copy (the joined tiles keep their bounds), beside
+    the FP64 CPU restatement of the same rule (oracle/bounds_oracle.cpp, all
+    host cores) on a few objects of each."""
+    import ctypes
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_bind import oracle
+    L = oracle().L
+    L.tdo_tile_bounds.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_double)]
+    cores = os.cpu_count() or 1
+    cpu_nuclei, cpu_vessels = 4 * cores, cores  # a few objects per host core
+    offn, offv = pkg.tdp.raw_object_offsets(nb), pkg.tdp.raw_object_offsets(vb)
+    n_nuc = min(n_nuclei, len(offn) - 1)
+    parts = {"nuclei": (pkg.tdp.raw_slice(nb, offn, 0, n_nuc), pkg.tdp.raw_slice(nb, offn, 0, min(cpu_nuclei, n_nuc))),
+             "vessels": (vb, pkg.tdp.raw_slice(vb, offv, 0, min(cpu_vessels, len(offv) - 1)))}
+    out = {"workload": f"bounds of the first {n_nuc} nuclei and of all {len(offv) - 1} vessels of the join's tiles "
+                       "(LODs 20-80 from each object's LOD-100 surface)"}
+    for name, (raw, sample) in parts.items():
+        T = pkg.tdp.Tile(ctx, raw)
+        ctx.compute_bounds(T)  # untimed first run
+        info = ctx.compute_bounds(T)
+        T.free()
+        smp = np.ascontiguousarray(sample)
+        res = np.empty_like(smp)
+        ev = ctypes.c_double()
+        n_cpu = len(pkg.tdp.raw_object_offsets(smp)) - 1
+        t0 = time.perf_counter()
+        L.tdo_tile_bounds(smp.ctypes.data, smp.size, res.ctypes.data, 1, cores, ctypes.byref(ev))
+        cpu_s = time.perf_counter() - t0
+        gpu_rate = info["objects"] / (info["ms"] / 1e3)
+        out[name] = {"objects": info["objects"], "triangles": info["triangles"], "gpu_ms": info["ms"],
+                     "objects_per_s": gpu_rate, "dist_evals": info["dist_evals"],
+                     "dist_evals_per_s": info["dist_evals"] / (info["ms"] / 1e3),
+                     "facet_queries": info["facet_queries"], "pieces": info["pieces"],
+                     "cpu_objects_per_s": n_cpu / cpu_s, "cpu_cores": cores,
+                     "cpu_sample": f"first {n_cpu} {name}, FP64 restatement, one run of {cpu_s:.2f} s",
+                     "gpu_over_cpu": gpu_rate / (n_cpu / cpu_s)}
+        log(f"bounds {name}: {info['objects']} objects in {info['ms']:.0f} ms on the GPU "
+            f"({gpu_rate:.0f}/s), CPU {n_cpu / cpu_s:.1f}/s on {cores} cores")
+    return out
+
+
 def run_out_of_core(a):
     """Config 4 scaled to the host: a 10-NN join of nuclei against 10,000
     vessels under a 16 GB device budget, both tiles in host memory (the vessel
@@ -330,6 +375,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream measurement")
     ap.add_argument("--no-self", action="store_true", help="skip the 10-NN self-join measurement")
+    ap.add_argument("--no-bounds", action="store_true", help="skip the GPU bound-preparation measurement")
     ap.add_argument("--refine-config", type=int, default=-1,
                     help="tuned refine configuration (default: autotuned in the warm-up)")
     ap.add_argument("--out-of-core", action="store_true",
@@ -498,6 +544,11 @@ def main():
         if not a.no_serve and ws == 1:
             T1.free()  # the serving arenas replace the resident query tile
             serving = run_serving(pkg, ctx, T2, nb, a.serve_rates)
+        bounds_prep = None
+        if not a.no_bounds and ws == 1:
+            T1.free()
+            T2.free()
+            bounds_prep = run_bounds_prep(pkg, ctx, nb, vb)
         del flush_buf
 
     pinned.release()
@@ -533,6 +584,7 @@ def main():
                     "h2d_bytes_per_step": int(nb.size + vb.size), "d2h_bytes_per_step": int(d2h)},
             "exact_distances": exact,
             "serving": serving,
+            "bounds_prep": bounds_prep,
             "knn_self_join": knn_self,
             "gpu_launches": int(launches_t),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",

@@ -136,6 +136,35 @@ int tdp_tile_upload(tdp_ctx *ctx, const void *raw_dt, size_t len, long max_objec
 int tdp_tile_free(tdp_ctx *ctx, tdp_tile *tile);
 int tdp_tile_get_info(const tdp_tile *tile, tdp_tile_info *out);
 
+/* ---- bound preparation (GPU) ------------------------------------------------
+ * Replaces the reference's CGAL preparation of the per-triangle bounds the join
+ * reads (sampled in src/spatial/himesh_hausdorff.cpp:197-270, stored as
+ * (proxy, hausdorff) per triangle at src/spatial/himesh_retrieve.cpp:131-151,
+ * written by tdbase convert through src/storage/tile_IO.cpp:79-172) with a
+ * conservative rule computed on the GPU in FP64 from each object's own LOD-100
+ * surface S:
+ *   proxy ph(t): every LOD-100 facet goes to the LOD triangle nearest its
+ *     barycentre; ph(t) = the largest distance of an assigned facet's vertex
+ *     to t, so every point of S lies within ph of its triangle;
+ *   hausdorff h(t): t cut into up to 64 pieces about one LOD-100 edge long;
+ *     h(t) = the largest over pieces of the smallest over facets of the
+ *     largest corner distance, so every point of t lies within h of S;
+ * rounded up to float; the object-level values are the per-LOD maxima (LOD
+ * 100: 0).  The triangles, voxels and LODs themselves are the input's.
+ * tdp_tile_compute_bounds rewrites the bounds of a resident tile in place (a
+ * join may use it at once); tdp_raw_compute_bounds maps RAW bytes to RAW
+ * bytes (out: len bytes, may equal raw) through a temporary resident tile. */
+typedef struct {
+    double ms;           /* device time of the bound kernels (CUDA events) */
+    long objects;        /* objects of the tile */
+    long triangles;      /* LOD 20-80 triangles bounded */
+    long facet_queries;  /* (LOD-100 facet, LOD) nearest-triangle searches */
+    long pieces;         /* triangle pieces searched for their nearest facet */
+    double dist_evals;   /* FP64 point-to-triangle distances evaluated */
+} tdp_bounds_info;
+int tdp_tile_compute_bounds(tdp_ctx *ctx, tdp_tile *tile, tdp_bounds_info *info);
+int tdp_raw_compute_bounds(tdp_ctx *ctx, const void *raw, size_t len, void *out, tdp_bounds_info *info);
+
 /* ---- object candidates (host only) ------------------------------------------
  * The object-level filter: replaces OctreeNode::query_knn_fast / query_within
  * over Tile::build_octree (reference src/index/octree.cpp:215-330,

@@ -19,6 +19,12 @@ void tdo_tri_dist_batch(const double *S, const double *T, size_t n, double *out_
 void tdo_voxel_pair(const float *tri1, const float *hd1, size_t n1,
                     const float *tri2, const float *hd2, size_t n2, double out[3]);
 
+/* per-triangle Hausdorff bounds of a RAW tile (bounds_oracle.cpp): out = a
+ * copy of the tile with the bounds replaced; prune 0 = brute force */
+int tdo_tile_bounds(const uint8_t *raw, size_t len, uint8_t *out, int prune, int threads, double *evals);
+/* largest violation of a tile's bounds over sampled points, see bounds_oracle.cpp */
+int tdo_bounds_violation(const uint8_t *raw, size_t len, int samples, uint64_t seed, double out[2]);
+
 #ifdef __cplusplus
 }
 #endif
