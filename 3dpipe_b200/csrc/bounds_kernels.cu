@@ -37,6 +37,7 @@
 
 #include "ctx.cuh"
 #include "bounds_kernels.cuh"
+#include "fetch_kernels.cuh"
 #include "ptdist.cuh"
 #include "storage/dev_tile.h"
 
@@ -380,6 +381,9 @@ extern "C" int tdp_tile_compute_bounds(tdp_ctx* ctx, tdp_tile* tile, tdp_bounds_
     b.n_obj = no;
     b.counters = (unsigned long long*)ctx->scratch[kBoundCounters].p;
 #define CU(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } while (0)
+    // an attached tile first fetches every voxel: the bounds are written into
+    // the device records, which later fetches must not overwrite
+    CU(launch_fetch_all(lazy_view(tile), ctx->num_sms, s));
     CU(cudaEventRecord(ctx->ev[0], s));
     CU(cudaMemsetAsync(b.counters, 0, 4 * sizeof(unsigned long long), s));
     const int small_grid = ctx->num_sms * 8;

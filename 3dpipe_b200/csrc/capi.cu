@@ -13,16 +13,54 @@ int fail(tdp_ctx* ctx, int code, const std::string& msg) {
     return code;
 }
 
+void cache_trim(tdp_ctx* ctx) {
+    for (auto& kv : ctx->block_cache) cudaFree(kv.second);
+    ctx->block_cache.clear();
+    ctx->cached_bytes = 0;
+}
+
 cudaError_t dmalloc(tdp_ctx* ctx, void** p, size_t bytes) {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
     if (ctx->budget && ctx->in_use + bytes > ctx->budget) return cudaErrorMemoryAllocation;
+    if (ctx->budget && ctx->in_use + ctx->cached_bytes + bytes > ctx->budget) cache_trim(ctx);
     cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess && !ctx->block_cache.empty()) {  // the cache holds the memory: give it back, retry
+        cudaGetLastError();
+        cache_trim(ctx);
+        e = cudaMalloc(p, bytes);
+    }
     if (e != cudaSuccess) { *p = nullptr; return e; }
     ctx->allocs[*p] = bytes;
     ctx->in_use += bytes;
-    if (ctx->in_use > ctx->peak) ctx->peak = ctx->in_use;
+    if (ctx->in_use + ctx->cached_bytes > ctx->peak) ctx->peak = ctx->in_use + ctx->cached_bytes;
     return cudaSuccess;
+}
+
+cudaError_t block_alloc(tdp_ctx* ctx, void** p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    auto it = ctx->block_cache.lower_bound(bytes);
+    if (it != ctx->block_cache.end() && it->first <= bytes + bytes / 4) {
+        if (ctx->budget && ctx->in_use + it->first > ctx->budget) return cudaErrorMemoryAllocation;
+        *p = it->second;
+        ctx->allocs[*p] = it->first;
+        ctx->in_use += it->first;
+        ctx->cached_bytes -= it->first;
+        ctx->block_cache.erase(it);
+        return cudaSuccess;
+    }
+    return dmalloc(ctx, p, bytes);
+}
+
+void block_release(tdp_ctx* ctx, void* p) {
+    if (!p) return;
+    auto it = ctx->allocs.find(p);
+    if (it == ctx->allocs.end() || it->second < kCachedBlockMin) { dfree(ctx, p); return; }
+    ctx->in_use -= it->second;
+    ctx->cached_bytes += it->second;
+    ctx->block_cache.emplace(it->second, p);
+    ctx->allocs.erase(it);
 }
 
 void dfree(tdp_ctx* ctx, void* p) {
@@ -76,8 +114,8 @@ using namespace tdp;
 extern "C" {
 
 int tdp_ctx_create(int device, size_t budget_bytes, unsigned flags, tdp_ctx** out) {
-    (void)flags;
     if (!out) return TDP_ERR_ARG;
+    if (flags & ~(unsigned)TDP_CTX_POISON) return TDP_ERR_ARG;
     *out = nullptr;
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return TDP_ERR_NODEV;
@@ -89,6 +127,7 @@ int tdp_ctx_create(int device, size_t budget_bytes, unsigned flags, tdp_ctx** ou
     tdp_ctx* ctx = new tdp_ctx();
     ctx->device = device;
     ctx->budget = budget_bytes;
+    ctx->flags = flags;
     ctx->num_sms = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return TDP_ERR_CUDA; }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
@@ -111,6 +150,7 @@ int tdp_ctx_destroy(tdp_ctx* ctx) {
     for (void* p : ptrs) dfree(ctx, p);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->lod_ev) if (e) cudaEventDestroy(e);
+    cache_trim(ctx);
     if (ctx->lod_graph) cudaGraphExecDestroy(ctx->lod_graph);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->hres) cudaFreeHost(ctx->hres);
@@ -141,6 +181,7 @@ int tdp_last_stats(const tdp_ctx* ctx, tdp_stats* o) {
     o->exact_items = s.exact_items;
     o->exact_f64_items = s.exact_f64_items;
     o->fp32_max_rel_err = s.fp32_max_rel_err;
+    o->fetch_bytes = s.fetch_bytes;
     o->lod_graph = s.lod_graph;
     return TDP_OK;
 }
@@ -201,7 +242,7 @@ void* tdp_ctx_stream(const tdp_ctx* ctx) { return ctx ? (void*)ctx->stream : nul
 
 int tdp_ctx_memory(const tdp_ctx* ctx, size_t* in_use, size_t* peak) {
     if (!ctx) return TDP_ERR_ARG;
-    if (in_use) *in_use = ctx->in_use;
+    if (in_use) *in_use = ctx->in_use + ctx->cached_bytes;  // idle cached tile blocks are held too
     if (peak) *peak = ctx->peak;
     return TDP_OK;
 }

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <string>
 #include <unordered_map>
+#include <map>
 #include <vector>
 #include "common.cuh"
 #include "../../include/tdp.h"
@@ -35,6 +36,7 @@ struct LastStats {
     long exact_items = 0;            // LOD-100 voxel pairs it refined in FP32
     long exact_f64_items = 0;        // of those, evaluated in FP64
     double fp32_max_rel_err = 0;     // max |FP32 minimum - FP64 distance| / max(distance, 1)
+    double fetch_bytes = 0;          // RAW bytes fetched from attached tiles
     long lod_graph = 0;              // tuned LOD loop: 0 direct launches, 1 graph replayed, 2 graph captured
 };
 
@@ -42,6 +44,7 @@ struct LastStats {
 
 struct tdp_ctx {
     int device = 0;
+    unsigned flags = 0;  // TDP_CTX_* flags given to tdp_ctx_create
     int num_sms = 148;
     size_t budget = 0, in_use = 0, peak = 0;
     cudaStream_t stream = nullptr;
@@ -62,6 +65,13 @@ struct tdp_ctx {
     int lod_graph_mode = TDP_LOD_GRAPH_AUTO;
     cudaGraphExec_t lod_graph = nullptr;
     std::vector<unsigned char> lod_key, lod_seen;
+    // idle device blocks of released tiles' triangle arrays, by size, handed
+    // back to the next tile of (about) the same size: re-attaching or
+    // re-uploading a tile costs no cudaMalloc / cudaFree of tens of GB.  Not
+    // counted in in_use; trimmed when an allocation would fail or exceed the
+    // budget, and on destroy.
+    std::multimap<size_t, void*> block_cache;
+    size_t cached_bytes = 0;
 };
 
 namespace tdp {
@@ -71,6 +81,14 @@ cudaError_t dmalloc(tdp_ctx* ctx, void** p, size_t bytes);
 void dfree(tdp_ctx* ctx, void* p);
 // grow-only scratch buffer; returns TDP_OK or an error status (recorded in ctx)
 int ensure(tdp_ctx* ctx, Buf& b, size_t bytes);
+// large blocks for tile triangle arrays: block_alloc reuses an idle cached
+// block of the size (or up to 25 % larger); block_release caches blocks of
+// at least kCachedBlockMin bytes (the caller has synchronised the context's
+// stream, so the block is idle) and frees smaller ones
+constexpr size_t kCachedBlockMin = (size_t)16 << 20;
+cudaError_t block_alloc(tdp_ctx* ctx, void** p, size_t bytes);
+void block_release(tdp_ctx* ctx, void* p);
+void cache_trim(tdp_ctx* ctx);
 
 enum ScratchSlot {
     kSlotRawData = 0, kSlotRawHd, kSlotTris, kSlotItems, kSlotOut,

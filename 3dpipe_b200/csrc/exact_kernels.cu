@@ -309,7 +309,7 @@ int grid(int64_t n, int per_block, int cap) {
 }  // namespace
 
 int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const tdp_tile* t2, bool pmx_valid,
-                    double* pexact, ExactInfo& info) {
+                    double* pexact, ExactInfo& info, const LazyTile& lz1, const LazyTile& lz2) {
     cudaStream_t s = ctx->stream;
     info = ExactInfo{};
     int rc;
@@ -340,6 +340,7 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     k_exact_upper<<<pg, kBlk, 0, s>>>(d, pmx_valid ? 1 : 0, vt1, vt2, Ub, item1);
     CU(cudaGetLastError());
     // phase 1: one FP32 voxel pair per object pair tightens U
+    CU(launch_fetch_items(item1, nullptr, d.P, kNumLods - 1, lz1, lz2, ctx->num_sms, s));
     CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], item1, (int)d.P, res1, ctr, nullptr,
                            ctx->num_sms, ctx->tuned_cfg, s));
     k_exact_tighten<<<grid(d.P, 256, ctx->num_sms * 8), 256, 0, s>>>(res1, d.P, Ub);
@@ -382,6 +383,7 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     CU(cudaMemsetAsync(emax, 0, Pz * 4, s));
     CU(cudaMemsetAsync(ctr, 0, 64, s));
     if (E > 0) {
+        CU(launch_fetch_items(items, nullptr, E, kNumLods - 1, lz1, lz2, ctx->num_sms, s));
         CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], items, (int)E, res, ctr, nullptr,
                                ctx->num_sms, ctx->tuned_cfg, s, nullptr, preset));
         const int eg = grid(E, 256, ctx->num_sms * 16);

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "ctx.cuh"
+#include "fetch_kernels.cuh"
 #include "join_kernels.cuh"
 #include "storage/dev_tile.h"
 
@@ -20,7 +21,9 @@ struct ExactInfo {
 // reported pair without any LOD-100 triangles: values >= 1e300).
 // pmx_valid: the pairs' upper bounds pmx bound the LOD-100 distance (true at
 // Hausdorff level 2; levels 0 and 1 widen by nothing or by proxy-Hausdorff).
+// lz1 / lz2: the tiles' fetch views (attached tiles fetch the LOD-100 voxels
+// that the stage refines; resident tiles: raw == nullptr).
 int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const tdp_tile* t2, bool pmx_valid,
-                    double* pexact, ExactInfo& info);
+                    double* pexact, ExactInfo& info, const LazyTile& lz1, const LazyTile& lz2);
 
 }  // namespace tdp

@@ -1,0 +1,138 @@
+// fetch_kernels.cu -- on-demand triangle fetch for attached tiles (see
+// fetch_kernels.cuh).
+//
+// A voxel's bytes at one LOD sit in its object's data block in the RAW layout
+// that the reference's writer produces (src/storage/tile_IO.cpp:79-172): for
+// each LOD, for each voxel, 9 floats per triangle, then (proxy, hausdorff) per
+// triangle.  tdp_tile_attach accepts only tiles in that layout, so the offset
+// of (voxel v, LOD l) inside object o's block is 44 bytes times the triangles
+// the object holds at the LODs before l plus those of o's voxels before v at
+// l -- all read from the tile's resident prefix arrays, nothing extra is
+// uploaded.  Every float of a RAW object sits a multiple of 4 bytes after the
+// object's first byte, but the objects follow a one-byte header, so the host
+// floats are read as aligned 32-bit words and realigned with a funnel shift
+// (the word after the last float still lies inside the object's record: the
+// voxel table and the transform follow the data block).  A warp moves 32
+// triangles at a time: coalesced word reads from host memory into shared
+// memory, then one 48-byte record per lane.
+#include "fetch_kernels.cuh"
+
+#include <algorithm>
+
+#include "storage/dev_tile.h"
+
+namespace tdp {
+
+namespace {
+
+constexpr int kFetchWarps = 8;
+constexpr int kStageWords = 32 * 11 + 1;
+
+// last index i in [0, n) with a[i] <= x (a ascending, a[0] <= x)
+__device__ inline long last_le(const uint32_t* a, long n, uint32_t x) {
+    long lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const long mid = (lo + hi + 1) >> 1;
+        if (a[mid] <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// copy voxel v's n triangles at LOD index lod (first record off) from the host
+// bytes into the tile's records, if this warp is the first to claim the voxel
+__device__ void fetch_voxel(const LazyTile& L, int lod, long v, uint32_t off, uint32_t n, uint32_t* stage) {
+    const int lane = threadIdx.x & 31;
+    unsigned prev = 1;
+    if (lane == 0) prev = atomicCAS(L.state + (size_t)lod * L.n_vox + v, 0u, 1u);
+    prev = __shfl_sync(0xffffffffu, prev, 0);
+    if (prev != 0u) return;
+    const long o = last_le(L.obj_vox, L.n_obj + 1, (uint32_t)v);
+    const uint32_t vb = L.obj_vox[o], ve = L.obj_vox[o + 1];
+    uint64_t before = off - L.vtri[lod][vb];
+    for (int l = 0; l < lod; ++l) before += L.vtri[l][ve] - L.vtri[l][vb];
+    const uintptr_t base = reinterpret_cast<uintptr_t>(L.raw) + L.data_off[o] + 44 * before;
+    const uint32_t* W = reinterpret_cast<const uint32_t*>(base & ~uintptr_t(3));
+    const unsigned sh = (unsigned)(base & 3) * 8;
+    auto word = [&](uint64_t k) -> uint32_t { return sh ? __funnelshift_r(W[k], W[k + 1], sh) : W[k]; };
+    float4* dst = L.tri[lod] + 3 * (size_t)off;
+    for (uint32_t c0 = 0; c0 < n; c0 += 32) {
+        const uint32_t m = min(32u, n - c0);
+        for (uint32_t k = lane; k < 9 * m; k += 32) stage[k] = word(9 * (uint64_t)c0 + k);
+        for (uint32_t k = lane; k < 2 * m; k += 32) stage[9 * m + k] = word(9 * (uint64_t)n + 2 * (uint64_t)c0 + k);
+        __syncwarp();
+        if (lane < m) {
+            const float* f = reinterpret_cast<const float*>(stage + 9 * lane);
+            const float* h = reinterpret_cast<const float*>(stage + 9 * m + 2 * lane);
+            float4* r = dst + 3 * (size_t)(c0 + lane);
+            r[0] = make_float4(f[0], f[1], f[2], h[0]);
+            r[1] = make_float4(f[3], f[4], f[5], h[1]);
+            r[2] = make_float4(f[6], f[7], f[8], 0.f);
+        }
+        __syncwarp();
+    }
+    if (lane == 0) atomicAdd(L.bytes, 44ull * n);
+}
+
+__global__ void __launch_bounds__(kFetchWarps * 32) k_fetch_items(const RefineItem* __restrict__ items,
+                                                                  const unsigned* n_dev, long n_host, int lod,
+                                                                  LazyTile A, LazyTile B) {
+    __shared__ uint32_t stage[kFetchWarps][kStageWords];
+    uint32_t* st = stage[threadIdx.x >> 5];
+    const long n = n_dev ? (long)*n_dev : n_host;
+    const long warps = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const RefineItem it = items[i];
+        if (A.raw && it.a_cnt) fetch_voxel(A, lod, last_le(A.vtri[lod], A.n_vox + 1, it.a_off), it.a_off, it.a_cnt, st);
+        if (B.raw && it.b_cnt) fetch_voxel(B, lod, last_le(B.vtri[lod], B.n_vox + 1, it.b_off), it.b_off, it.b_cnt, st);
+    }
+}
+
+__global__ void __launch_bounds__(kFetchWarps * 32) k_fetch_all(LazyTile L) {
+    __shared__ uint32_t stage[kFetchWarps][kStageWords];
+    uint32_t* st = stage[threadIdx.x >> 5];
+    const long warps = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < kNumLods * L.n_vox; i += warps) {
+        const int lod = (int)(i / L.n_vox);
+        const long v = i - (long)lod * L.n_vox;
+        const uint32_t off = L.vtri[lod][v], n = L.vtri[lod][v + 1] - off;
+        if (n) fetch_voxel(L, lod, v, off, n, st);
+    }
+}
+
+}  // namespace
+
+LazyTile lazy_view(const tdp_tile* t) {
+    LazyTile L;
+    if (!t || !t->lazy_raw) return L;
+    L.raw = t->lazy_raw;
+    L.data_off = t->lazy_data_off;
+    L.obj_vox = t->obj_vox;
+    for (int l = 0; l < kNumLods; ++l) {
+        L.vtri[l] = t->vtri[l];
+        L.tri[l] = t->tri[l];
+    }
+    L.state = t->lazy_state;
+    L.bytes = t->lazy_bytes;
+    L.n_vox = t->n_vox;
+    L.n_obj = t->n_obj;
+    return L;
+}
+
+cudaError_t launch_fetch_items(const RefineItem* items, const unsigned* n_dev, long n_host, int lod,
+                               const LazyTile& a, const LazyTile& b, int num_sms, cudaStream_t s) {
+    if (!a.raw && !b.raw) return cudaSuccess;
+    if (!n_dev && n_host <= 0) return cudaSuccess;
+    const long blocks_needed = n_dev ? (long)num_sms * 8 : (n_host + kFetchWarps - 1) / kFetchWarps;
+    const int blocks = (int)std::max(1L, std::min<long>(blocks_needed, (long)num_sms * 8));
+    k_fetch_items<<<blocks, kFetchWarps * 32, 0, s>>>(items, n_dev, n_host, lod, a, b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fetch_all(const LazyTile& t, int num_sms, cudaStream_t s) {
+    if (!t.raw || t.n_vox == 0) return cudaSuccess;
+    k_fetch_all<<<num_sms * 8, kFetchWarps * 32, 0, s>>>(t);
+    return cudaGetLastError();
+}
+
+}  // namespace tdp

@@ -13,6 +13,7 @@
 // at an object's first byte into a 256-byte aligned staging buffer, which makes
 // every float 4-byte aligned on the device (checked on the host per segment).
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -63,9 +64,12 @@ void tile_release(tdp_ctx* ctx, tdp_tile* t) {
     dfree(ctx, t->obj_hd);
     dfree(ctx, t->obj_phd);
     for (int l = 0; l < kNumLods; ++l) {
-        dfree(ctx, t->tri[l]);
+        block_release(ctx, t->tri[l]);  // kept for the next tile of the size
         dfree(ctx, t->vtri[l]);
     }
+    dfree(ctx, (void*)t->lazy_data_off);
+    dfree(ctx, t->lazy_state);
+    dfree(ctx, t->lazy_bytes);
     dfree(ctx, t->d_boxes);
     dfree(ctx, t->box_grid.start);
     dfree(ctx, t->box_grid.items);
@@ -74,22 +78,39 @@ void tile_release(tdp_ctx* ctx, tdp_tile* t) {
     delete t;
 }
 
-}  // namespace tdp
-
-using namespace tdp;
-
-extern "C" {
-
-int tdp_tile_upload(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, tdp_tile** out) {
+// Parse, validate and make a tile resident (attach == false), or attach it:
+// voxel and object metadata resident, triangle records allocated but filled
+// by the joins that need them, straight from the page-locked host bytes.
+int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bool attach, tdp_tile** out) {
     if (!ctx || !out) return TDP_ERR_ARG;
     *out = nullptr;
     if (!raw_dt) return fail(ctx, TDP_ERR_ARG, "null tile buffer");
     cudaSetDevice(ctx->device);
     const uint8_t* buf = (const uint8_t*)raw_dt;
+    const uint8_t* dev_view = nullptr;
+    if (attach) {
+        // the bytes must be page-locked (cudaHostRegister / cudaHostAlloc), so
+        // that kernels can read them, from the first byte to the last
+        cudaPointerAttributes a0{}, a1{};
+        void* dp = nullptr;
+        if (len == 0 || cudaPointerGetAttributes(&a0, buf) != cudaSuccess || a0.type != cudaMemoryTypeHost ||
+            cudaPointerGetAttributes(&a1, buf + len - 1) != cudaSuccess || a1.type != cudaMemoryTypeHost ||
+            cudaHostGetDevicePointer(&dp, (void*)buf, 0) != cudaSuccess || !dp) {
+            cudaGetLastError();
+            return fail(ctx, TDP_ERR_ARG, "tdp_tile_attach needs page-locked host memory (cudaHostRegister or "
+                                          "cudaHostAlloc) covering the whole tile; use tdp_tile_upload otherwise");
+        }
+        dev_view = (const uint8_t*)dp;
+    }
     tdp_tile* T = new tdp_tile();
     T->device = ctx->device;
     std::string err;
+    const auto t0 = std::chrono::steady_clock::now();
+    auto ms_since = [](std::chrono::steady_clock::time_point a) {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+    };
     int rc = parse_raw_dt(buf, len, max_objects, T->host, err);
+    T->parse_ms = ms_since(t0);
     if (rc != TDP_OK) {
         delete T;
         return fail(ctx, rc, err);
@@ -105,6 +126,26 @@ int tdp_tile_upload(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objec
         T->h_vtri[l][0] = 0;
         for (long v = 0; v < H.n_vox; ++v) T->h_vtri[l][v + 1] = T->h_vtri[l][v] + H.vox_cnt[l][v];
     }
+    if (attach) {
+        // fetches locate a voxel's bytes from the prefix arrays: the data
+        // block must hold, LOD by LOD and voxel by voxel, each voxel's
+        // triangles then its bounds, with nothing in between (the layout the
+        // reference's writer produces, src/storage/tile_IO.cpp:79-172)
+        for (long o = 0; o < H.n_obj; ++o) {
+            uint64_t expect = H.obj_data_off[o];
+            for (int l = 0; l < kNumLods; ++l)
+                for (uint32_t v = H.obj_vox_off[o]; v < H.obj_vox_off[o + 1]; ++v) {
+                    if (H.vox_byte_off[l][v] != expect) {
+                        delete T;
+                        return fail(ctx, TDP_ERR_FORMAT, "object " + std::to_string(o) +
+                                                             " does not keep its voxels' triangles in LOD and voxel "
+                                                             "order; use tdp_tile_upload for this tile");
+                    }
+                    expect += 44ull * H.vox_cnt[l][v];
+                }
+        }
+    }
+    const auto ta = std::chrono::steady_clock::now();
     auto alloc = [&](void** p, size_t bytes) -> int {
         if (dmalloc(ctx, p, bytes) != cudaSuccess)
             return fail(ctx, TDP_ERR_NOMEM, "tile upload: cannot allocate " + std::to_string(bytes) + " bytes" +
@@ -119,10 +160,18 @@ int tdp_tile_upload(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objec
     TRY(alloc((void**)&T->obj_vox, (size_t)(H.n_obj + 1) * sizeof(uint32_t)));
     TRY(alloc((void**)&T->obj_hd, (size_t)H.n_obj * kNumLods * sizeof(float)));
     TRY(alloc((void**)&T->obj_phd, (size_t)H.n_obj * kNumLods * sizeof(float)));
+    auto alloc_block = [&](void** p, size_t bytes) -> int {
+        if (block_alloc(ctx, p, bytes) != cudaSuccess)
+            return fail(ctx, TDP_ERR_NOMEM, "tile upload: cannot allocate " + std::to_string(bytes) + " bytes" +
+                                                (ctx->budget ? " within the context budget" : ""));
+        T->device_bytes += bytes;
+        return TDP_OK;
+    };
     for (int l = 0; l < kNumLods; ++l) {
-        TRY(alloc((void**)&T->tri[l], (size_t)H.n_tris[l] * 3 * sizeof(float4)));
+        TRY(alloc_block((void**)&T->tri[l], (size_t)H.n_tris[l] * 3 * sizeof(float4)));
         TRY(alloc((void**)&T->vtri[l], (size_t)(H.n_vox + 1) * sizeof(uint32_t)));
     }
+    T->alloc_ms = ms_since(ta);
     {
         std::vector<float4> v4((size_t)H.n_vox * 3);
         for (long v = 0; v < H.n_vox; ++v) {
@@ -137,7 +186,26 @@ int tdp_tile_upload(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objec
         CTRY(cudaMemcpyAsync(T->obj_phd, H.obj_phd.data(), H.obj_phd.size() * 4, cudaMemcpyHostToDevice, s));
         for (int l = 0; l < kNumLods; ++l)
             CTRY(cudaMemcpyAsync(T->vtri[l], T->h_vtri[l].data(), T->h_vtri[l].size() * 4, cudaMemcpyHostToDevice, s));
+        T->h2d_bytes += v4.size() * sizeof(float4) + H.obj_vox_off.size() * 4 + H.obj_hd.size() * 8;
+        for (int l = 0; l < kNumLods; ++l) T->h2d_bytes += T->h_vtri[l].size() * 4;
         CTRY(cudaStreamSynchronize(s));
+    }
+    if (attach) {
+        TRY(alloc((void**)&T->lazy_data_off, (size_t)std::max<long>(H.n_obj, 1) * sizeof(uint64_t)));
+        TRY(alloc((void**)&T->lazy_state, (size_t)kNumLods * std::max<long>(H.n_vox, 1) * sizeof(unsigned)));
+        TRY(alloc((void**)&T->lazy_bytes, sizeof(unsigned long long)));
+        CTRY(cudaMemcpyAsync(T->lazy_data_off, H.obj_data_off.data(), H.n_obj * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+        CTRY(cudaMemsetAsync(T->lazy_state, 0, (size_t)kNumLods * H.n_vox * sizeof(unsigned), s));
+        CTRY(cudaMemsetAsync(T->lazy_bytes, 0, sizeof(unsigned long long), s));
+        if (ctx->flags & TDP_CTX_POISON)
+            for (int l = 0; l < kNumLods; ++l)
+                CTRY(cudaMemsetAsync(T->tri[l], 0xff, (size_t)H.n_tris[l] * 3 * sizeof(float4), s));
+        CTRY(cudaStreamSynchronize(s));
+        T->h2d_bytes += H.n_obj * sizeof(uint64_t);
+        T->lazy_raw = dev_view;
+        T->load_ms = ms_since(t0);
+        *out = T;
+        return TDP_OK;
     }
     // chunked copy + unpack of the triangle data, whole objects per chunk
     const size_t kChunk = (size_t)1 << 30;
@@ -171,6 +239,7 @@ int tdp_tile_upload(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objec
                 }
         TRY(ensure(ctx, segbuf, std::max<size_t>(segs.size(), 1) * sizeof(UnpackSeg)));
         CTRY(cudaMemcpyAsync(stage.p, buf + base, bytes, cudaMemcpyHostToDevice, s));
+        T->h2d_bytes += bytes + segs.size() * sizeof(UnpackSeg);
         CTRY(cudaMemcpyAsync(segbuf.p, segs.data(), segs.size() * sizeof(UnpackSeg), cudaMemcpyHostToDevice, s));
         if (!segs.empty()) {
             int blocks = (int)std::min<size_t>((segs.size() + 7) / 8, (size_t)ctx->num_sms * 16);
@@ -182,8 +251,40 @@ int tdp_tile_upload(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objec
     }
 #undef TRY
 #undef CTRY
+    T->load_ms = ms_since(t0);
     *out = T;
     return TDP_OK;
+}
+
+}  // namespace tdp
+
+using namespace tdp;
+
+extern "C" {
+
+int tdp_tile_upload(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, tdp_tile** out) {
+    return tile_load(ctx, raw_dt, len, max_objects, false, out);
+}
+
+int tdp_tile_attach(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, tdp_tile** out) {
+    return tile_load(ctx, raw_dt, len, max_objects, true, out);
+}
+
+int tdp_host_alloc(size_t bytes, void** out) {
+    if (!out) return TDP_ERR_ARG;
+    *out = nullptr;
+    if (bytes == 0) return TDP_ERR_ARG;
+    if (cudaHostAlloc(out, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return TDP_ERR_NOMEM;
+    }
+    return TDP_OK;
+}
+
+int tdp_host_free(void* p) {
+    if (!p) return TDP_ERR_ARG;
+    return cudaFreeHost(p) == cudaSuccess ? TDP_OK : TDP_ERR_CUDA;
 }
 
 int tdp_tile_free(tdp_ctx* ctx, tdp_tile* tile) {
@@ -200,6 +301,11 @@ int tdp_tile_get_info(const tdp_tile* t, tdp_tile_info* o) {
     o->n_voxels = t->n_vox;
     for (int l = 0; l < kNumLods; ++l) o->n_tris[l] = (long)t->host.n_tris[l];
     o->device_bytes = t->device_bytes;
+    o->h2d_bytes = t->h2d_bytes;
+    o->attached = t->lazy_raw != nullptr;
+    o->parse_ms = t->parse_ms;
+    o->alloc_ms = t->alloc_ms;
+    o->load_ms = t->load_ms;
     return TDP_OK;
 }
 

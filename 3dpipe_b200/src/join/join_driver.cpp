@@ -28,6 +28,7 @@
 #include "../../csrc/join_kernels.cuh"
 #include "../../csrc/cand_kernels.cuh"
 #include "../../csrc/exact_kernels.cuh"
+#include "../../csrc/fetch_kernels.cuh"
 #include "../../csrc/refine.cuh"
 #include "index/candidates.h"
 #include "storage/dev_tile.h"
@@ -74,6 +75,7 @@ struct LodLoop {
     int* rankst;
     double *vexact, *res64, *pexact;
     cudaEvent_t ev[16];
+    LazyTile lz1, lz2;  // attached tiles: fetch each LOD's voxels before its refine
 };
 
 // Enqueue the loop on s.  While s is being captured, the per-LOD timing events
@@ -94,6 +96,7 @@ int enqueue_lod_loop(tdp_ctx* ctx, const LodLoop& L, cudaStream_t s, bool captur
         const int highest = k == L.highest_k;
         CUL(cudaMemsetAsync(cnt_items, 0, 4, s));
         CUL(launch_build_items(L.d, L.vt1[k], L.vt2[k], L.items, L.item_vp, cnt_items, s));
+        CUL(launch_fetch_items(L.items, cnt_items, 0, L.li[k], L.lz1, L.lz2, L.num_sms, s));
         CUL(cudaMemcpyAsync(lod_counts + k, cnt_items, 4, cudaMemcpyDeviceToDevice, s));
         CUL(rec(L.ev[2 * k]));
         CUL(launch_refine_tuned(L.tri1[k], L.tri2[k], L.items, V, L.res, L.counter, L.dstats, L.num_sms, L.cfg, s,
@@ -108,6 +111,7 @@ int enqueue_lod_loop(tdp_ctx* ctx, const LodLoop& L, cudaStream_t s, bool captur
         CUL(launch_count_status(L.d, cnt_recheck, s));
         CUL(cudaMemsetAsync(cnt_items, 0, 4, s));
         CUL(launch_recheck_items(L.d, L.vt1_100, L.vt2_100, L.items, L.item_vp, L.vexact, cnt_items, s));
+        CUL(launch_fetch_items(L.items, cnt_items, 0, kNumLods - 1, L.lz1, L.lz2, L.num_sms, s));
         CUL(launch_refine_f64(L.tri1_100, L.tri2_100, L.items, V, L.res64, s, cnt_items));
         CUL(launch_recheck_finish(L.d, L.res64, L.item_vp, V, L.vexact, L.pexact, L.knn, L.K, L.tau, s, cnt_items));
     }
@@ -309,6 +313,12 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     }
     CU(cudaMemsetAsync(d.qconf, 0, t1->n_obj * 4, s));
     CU(cudaMemsetAsync(ctx->d_stats + 1, 0, 8, s));
+    // attached tiles: voxels fetched on demand, bytes counted per join
+    LazyTile lz1 = lazy_view(t1), lz2 = lazy_view(t2);
+    unsigned long long* fetch_ctr = ctx->d_stats + 8;
+    if (lz1.raw) lz1.bytes = fetch_ctr;
+    if (lz2.raw) lz2.bytes = fetch_ctr;
+    CU(cudaMemsetAsync(fetch_ctr, 0, 8, s));
     d.stat_vp = ctx->d_stats + 1;
     long launches = 0;
 
@@ -365,6 +375,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
             tri_total += (double)trip;
             refine_items += W;
             if (W > 0) {
+                CU(launch_fetch_items(items, nullptr, W, li, lz1, lz2, ctx->num_sms, s));
                 CU(cudaEventRecord(ctx->ev[2], s));
                 CU(launch_refine_plain(t1->tri[li], t2->tri[li], items, W, res, s));
                 CU(cudaEventRecord(ctx->ev[3], s));
@@ -420,6 +431,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         L.V = V; L.tau = within_dist;
         L.rankst = buf<int>(ctx, kRankSt);
         L.vexact = buf<double>(ctx, kVexact); L.res64 = buf<double>(ctx, kRes64); L.pexact = buf<double>(ctx, kPexact);
+        L.lz1 = lz1; L.lz2 = lz2;
         if ((rc = run_lod_loop(ctx, L, s, &st.lod_graph))) return rc;
         launches += 5 * L.nl + (L.recheck ? (knn ? 6 : 5) : 0);
         st.refine_launches += L.nl;
@@ -434,7 +446,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         ENS(kOutD64, Pz * 8);
         pex = buf<double>(ctx, kPexOut);
         CU(cudaEventRecord(ctx->ev[6], s));
-        if ((rc = exact_distances(ctx, d, t1, t2, prm->hausdorff_level == 2, pex, xi))) return rc;
+        if ((rc = exact_distances(ctx, d, t1, t2, prm->hausdorff_level == 2, pex, xi, lz1, lz2))) return rc;
         CU(cudaEventRecord(ctx->ev[7], s));
         launches += xi.launches;
         syncs += 2;
@@ -459,8 +471,9 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     unsigned tc[32] = {0};
     unsigned long long fe = 0;
     CU(cudaMemcpyAsync(&nres, cnt_collect, 4, cudaMemcpyDeviceToHost, s));
-    unsigned long long fvp = 0;
+    unsigned long long fvp = 0, fetched = 0;
     CU(cudaMemcpyAsync(&fvp, ctx->d_stats + 1, 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&fetched, fetch_ctr, 8, cudaMemcpyDeviceToHost, s));
     if (tuned && V > 0) {
         CU(cudaMemcpyAsync(tc, ctx->d_counter + 8, 32 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
         CU(cudaMemcpyAsync(&fe, ctx->d_stats, 8, cudaMemcpyDeviceToHost, s));
@@ -468,6 +481,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     CU(cudaStreamSynchronize(s));
     ++syncs;
     st.filter_voxel_pairs = (double)fvp;
+    st.fetch_bytes = (double)fetched;
     if (tuned && V > 0) {
         unsigned long long trip;
         std::memcpy(&trip, &tc[2], 8);  // d_counter[10..11]

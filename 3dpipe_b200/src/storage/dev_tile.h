@@ -47,5 +47,13 @@ struct tdp_tile {
     uint32_t* vtri[tdp::kNumLods] = {};
     std::vector<uint32_t> h_vtri[tdp::kNumLods];  // host copy of vtri
     size_t device_bytes = 0;
+    size_t h2d_bytes = 0;  // bytes copied host -> device by the upload or attach itself
+    double parse_ms = 0, alloc_ms = 0, load_ms = 0;  // host time of the upload or attach
     int device = 0;
+    // attached tiles (tdp_tile_attach): the triangles stay in page-locked host
+    // memory and joins fetch the voxels they refine (csrc/fetch_kernels.cu)
+    const uint8_t* lazy_raw = nullptr;          // device view of the host bytes; nullptr: resident tile
+    uint64_t* lazy_data_off = nullptr;          // [n_obj] byte offset of each object's data block
+    unsigned* lazy_state = nullptr;             // [kNumLods * n_vox] 1 once the voxel's LOD is fetched
+    unsigned long long* lazy_bytes = nullptr;   // RAW bytes fetched so far
 };

@@ -1,8 +1,11 @@
 // dt_format.cpp -- bounds-checked parser of the RAW tile format (see dt_format.h).
 #include "storage/dt_format.h"
 
+#include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 #include "tdp.h"
 
@@ -26,7 +29,11 @@ size_t raw_object_bytes(uint32_t nvox, const uint32_t* counts) {
            (size_t)nvox * (9 * sizeof(float) + kNumLods * 2 * sizeof(size_t)) + 3 * sizeof(float);
 }
 
-int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, std::string& err) {
+namespace {
+
+// One object after another: the reference reader's order.  Used as is for the
+// exact first error of a malformed tile.
+int parse_sequential(const uint8_t* buf, size_t len, long max_objects, TileHost& T, std::string& err) {
     T = TileHost();
     if (!buf || len < 1) { err = "empty tile buffer"; return TDP_ERR_FORMAT; }
     if (buf[0] != kRawType) {
@@ -91,4 +98,142 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
     return TDP_OK;
 }
 
+}  // namespace
+
+// Two passes: a walk over the size fields finds every object's record (a
+// structural problem hands the tile to the sequential parser, which reports
+// the first error in file order); then the objects' voxel tables are read in
+// parallel into arrays sized from the walk.  Content errors are reported for
+// the lowest object that has one, the error the sequential parser would meet
+// first, with the same message.
+int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, std::string& err) {
+    T = TileHost();
+    if (!buf || len < 1) { err = "empty tile buffer"; return TDP_ERR_FORMAT; }
+    if (buf[0] != kRawType) return parse_sequential(buf, len, max_objects, T, err);
+    struct Rec {
+        uint64_t data_off, data_size, meta, vnum;
+    };
+    std::vector<Rec> recs;
+    size_t pos = 1;
+    uint64_t nvox = 0;
+    constexpr size_t kVoxBytes = 9 * sizeof(float) + kNumLods * 2 * sizeof(uint64_t);
+    while (pos < len && (max_objects <= 0 || (long)recs.size() < max_objects)) {
+        uint64_t data_size = 0, vnum = 0;
+        if (!rd(buf, len, pos, data_size) || data_size > len - pos || data_size % 4)
+            return parse_sequential(buf, len, max_objects, T, err);
+        const uint64_t data_off = pos;
+        pos += data_size;
+        if (!rd(buf, len, pos, vnum) || vnum == 0 || vnum > (1u << 24))
+            return parse_sequential(buf, len, max_objects, T, err);
+        const uint64_t rec = 2 * kNumLods * sizeof(float) + vnum * kVoxBytes + 3 * sizeof(float);
+        if (rec > len - pos) return parse_sequential(buf, len, max_objects, T, err);
+        recs.push_back({data_off, data_size, pos, vnum});
+        pos += rec;
+        nvox += vnum;
+        if (nvox >= 0xffffffffull) return parse_sequential(buf, len, max_objects, T, err);
+    }
+    const long n = (long)recs.size();
+    if (n == 0) { err = "tile holds no objects"; return TDP_ERR_FORMAT; }
+    T.n_obj = n;
+    T.n_vox = (long)nvox;
+    T.obj_vox_off.resize(n + 1);
+    T.obj_vox_off[0] = 0;
+    for (long o = 0; o < n; ++o) T.obj_vox_off[o + 1] = T.obj_vox_off[o] + (uint32_t)recs[o].vnum;
+    T.obj_data_off.resize(n);
+    T.obj_data_size.resize(n);
+    T.obj_box.resize(6 * n);
+    T.obj_xf.resize(3 * n);
+    T.obj_hd.resize((size_t)kNumLods * n);
+    T.obj_phd.resize((size_t)kNumLods * n);
+    T.vox_box.resize(9 * nvox);
+    for (int l = 0; l < kNumLods; ++l) {
+        T.vox_byte_off[l].resize(nvox);
+        T.vox_cnt[l].resize(nvox);
+    }
+    const int nt = (int)std::max<long>(1, std::min<long>((long)std::thread::hardware_concurrency(), n / 256));
+    std::vector<long> bad(nt, -1);
+    std::vector<std::string> msg(nt);
+    std::vector<std::array<uint64_t, kNumLods>> tris(nt);
+    auto work = [&](int k) {
+        tris[k].fill(0);
+        for (long o = n * k / nt; o < n * (k + 1) / nt; ++o) {
+            const Rec& r = recs[o];
+            const uint8_t* p = buf + r.meta;
+            float hp[2 * kNumLods];
+            std::memcpy(hp, p, sizeof(hp));
+            p += sizeof(hp);
+            for (int l = 0; l < kNumLods; ++l) {
+                T.obj_hd[(size_t)o * kNumLods + l] = hp[2 * l];
+                T.obj_phd[(size_t)o * kNumLods + l] = hp[2 * l + 1];
+            }
+            float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            const uint32_t v0 = T.obj_vox_off[o];
+            for (uint64_t v = 0; v < r.vnum; ++v) {
+                float* b = &T.vox_box[9 * (size_t)(v0 + v)];
+                std::memcpy(b, p, 9 * sizeof(float));
+                p += 9 * sizeof(float);
+                for (int c = 0; c < 3; ++c) {
+                    if (!(b[c] <= b[3 + c])) {
+                        bad[k] = o;
+                        msg[k] = "inverted voxel box in object " + std::to_string(o);
+                        return;
+                    }
+                    lo[c] = std::fmin(lo[c], b[c]);
+                    hi[c] = std::fmax(hi[c], b[3 + c]);
+                }
+                uint64_t oc[2 * kNumLods];
+                std::memcpy(oc, p, sizeof(oc));
+                p += sizeof(oc);
+                for (int l = 0; l < kNumLods; ++l) {
+                    const uint64_t off = oc[2 * l], cnt = oc[2 * l + 1];
+                    if (cnt > (1u << 24) || off % 4 || off > r.data_size || cnt * 44 > r.data_size - off) {
+                        bad[k] = o;
+                        msg[k] = "voxel lod range outside data block in object " + std::to_string(o);
+                        return;
+                    }
+                    T.vox_byte_off[l][v0 + v] = r.data_off + off;
+                    T.vox_cnt[l][v0 + v] = (uint32_t)cnt;
+                    tris[k][l] += cnt;
+                }
+            }
+            std::memcpy(&T.obj_xf[3 * o], p, 3 * sizeof(float));
+            T.obj_data_off[o] = r.data_off;
+            T.obj_data_size[o] = r.data_size;
+            float* ob = &T.obj_box[6 * o];
+            ob[0] = lo[0]; ob[1] = lo[1]; ob[2] = lo[2];
+            ob[3] = hi[0]; ob[4] = hi[1]; ob[5] = hi[2];
+        }
+    };
+    if (nt == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> pool;
+        for (int k = 0; k < nt; ++k) pool.emplace_back(work, k);
+        for (auto& th : pool) th.join();
+    }
+    for (int k = 0; k < nt; ++k)
+        if (bad[k] >= 0) {  // chunks are in object order: the first failing chunk holds the lowest object
+            err = msg[k];
+            T = TileHost();
+            return TDP_ERR_FORMAT;
+        }
+    for (int k = 0; k < nt; ++k)
+        for (int l = 0; l < kNumLods; ++l) T.n_tris[l] += tris[k][l];
+    return TDP_OK;
+}
+
 }  // namespace tdp
+
+extern "C" int tdp_raw_check(const void* raw, size_t len, long* n_objects, long* n_voxels, char* err, size_t err_len) {
+    tdp::TileHost T;
+    std::string e;
+    const int rc = tdp::parse_raw_dt((const uint8_t*)raw, len, 0, T, e);
+    if (n_objects) *n_objects = rc == TDP_OK ? T.n_obj : 0;
+    if (n_voxels) *n_voxels = rc == TDP_OK ? T.n_vox : 0;
+    if (err && err_len) {
+        const size_t k = std::min(err_len - 1, e.size());
+        std::memcpy(err, e.data(), k);
+        err[k] = 0;
+    }
+    return rc;
+}

@@ -43,7 +43,7 @@ class Stats(C.Structure):
                 ("filter_voxel_pairs", C.c_double), ("kernel_launches", C.c_long),
                 ("candidates_ms", C.c_double), ("lod_ms", C.c_double), ("host_syncs", C.c_long),
                 ("exact_ms", C.c_double), ("exact_items", C.c_long), ("exact_f64_items", C.c_long),
-                ("fp32_max_rel_err", C.c_double), ("lod_graph", C.c_long)]
+                ("fp32_max_rel_err", C.c_double), ("fetch_bytes", C.c_double), ("lod_graph", C.c_long)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -116,10 +116,10 @@ def gen_tiles(n_vessels: int = 10, nuclei_per_vessel: int = 20, seed: int = 2026
 class Context:
     """A device context: stream, memory budget, scratch buffers."""
 
-    def __init__(self, device: int = 0, budget_bytes: int = 0):
+    def __init__(self, device: int = 0, budget_bytes: int = 0, flags: int = 0):
         L = lib()
         h = C.c_void_p()
-        rc = L.tdp_ctx_create(device, budget_bytes, 0, C.byref(h))
+        rc = L.tdp_ctx_create(device, budget_bytes, flags, C.byref(h))
         if rc != TDP_OK:
             raise TdpError(rc, "tdp_ctx_create failed (device %d)" % device)
         self._h = h
@@ -192,7 +192,8 @@ class Context:
 
 class TileInfo(C.Structure):
     _fields_ = [("n_objects", C.c_long), ("n_voxels", C.c_long), ("n_tris", C.c_long * 5),
-                ("device_bytes", C.c_size_t)]
+                ("device_bytes", C.c_size_t), ("h2d_bytes", C.c_size_t), ("attached", C.c_int),
+                ("parse_ms", C.c_double), ("alloc_ms", C.c_double), ("load_ms", C.c_double)]
 
 
 class JoinParams(C.Structure):
@@ -204,6 +205,7 @@ class JoinParams(C.Structure):
 def _bind_join(L):
     P = C.c_void_p
     L.tdp_tile_upload.argtypes = [P, P, C.c_size_t, C.c_long, C.POINTER(P)]
+    L.tdp_tile_attach.argtypes = [P, P, C.c_size_t, C.c_long, C.POINTER(P)]
     L.tdp_tile_free.argtypes = [P, P]
     L.tdp_tile_get_info.argtypes = [P, C.POINTER(TileInfo)]
     L.tdp_candidates.argtypes = [P, P, C.c_long, P, P, C.c_long, C.c_int, C.c_int, C.c_int, C.c_float, P, P, C.c_long]
@@ -221,13 +223,23 @@ EXPORTED += ["tdp_tile_upload", "tdp_tile_free", "tdp_tile_get_info", "tdp_candi
 
 
 class Tile:
-    """A RAW .dt tile resident in HBM (Tile::load + decode to every LOD)."""
+    """A RAW .dt tile resident in HBM (Tile::load + decode to every LOD), or,
+    with attach=True, attached: `raw` stays in page-locked host memory (it must
+    be registered, e.g. with cudaHostRegister, or come from pinned_empty, and it
+    must outlive the tile) and joins fetch the voxels they refine
+    (tdp_tile_attach)."""
 
-    def __init__(self, ctx: "Context", raw: np.ndarray, max_objects: int = 0):
-        raw = np.ascontiguousarray(raw, np.uint8)
+    def __init__(self, ctx: "Context", raw: np.ndarray, max_objects: int = 0, attach: bool = False):
+        if attach:
+            if not (isinstance(raw, np.ndarray) and raw.dtype == np.uint8 and raw.flags.c_contiguous):
+                raise ValueError("attach needs the tile's own contiguous uint8 buffer (page-locked)")
+        else:
+            raw = np.ascontiguousarray(raw, np.uint8)
         h = C.c_void_p()
-        ctx.check(lib().tdp_tile_upload(ctx.handle, _ptr(raw), raw.size, max_objects, C.byref(h)))
+        fn = lib().tdp_tile_attach if attach else lib().tdp_tile_upload
+        ctx.check(fn(ctx.handle, _ptr(raw), raw.size, max_objects, C.byref(h)))
         self._ctx, self._h = ctx, h
+        self._raw = raw if attach else None  # the host bytes an attached tile reads
 
     @property
     def handle(self):
@@ -237,7 +249,8 @@ class Tile:
         i = TileInfo()
         lib().tdp_tile_get_info(self._h, C.byref(i))
         return {"n_objects": i.n_objects, "n_voxels": i.n_voxels, "n_tris": list(i.n_tris),
-                "device_bytes": i.device_bytes}
+                "device_bytes": i.device_bytes, "h2d_bytes": i.h2d_bytes, "attached": bool(i.attached),
+                "parse_ms": i.parse_ms, "alloc_ms": i.alloc_ms, "load_ms": i.load_ms}
 
     def free(self):
         if getattr(self, "_h", None):
@@ -336,7 +349,49 @@ EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates",
 
 LOD_GRAPH_OFF, LOD_GRAPH_AUTO, LOD_GRAPH_ALWAYS = 0, 1, 2
 
-EXPORTED += ["tdp_tile_compute_bounds", "tdp_raw_compute_bounds"]
+EXPORTED += ["tdp_tile_compute_bounds", "tdp_raw_compute_bounds", "tdp_tile_attach", "tdp_host_alloc",
+             "tdp_host_free", "tdp_raw_check"]
+
+CTX_POISON = 1  # tdp_ctx_create flag: unfetched records of attached tiles read as NaN
+
+
+def raw_check(raw):
+    """Validate RAW tile bytes on the host: (n_objects, n_voxels), or TdpError
+    (TDP_ERR_FORMAT) naming the first problem in file order."""
+    L = lib()
+    L.tdp_raw_check.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_long), C.POINTER(C.c_long), C.c_char_p,
+                                C.c_size_t]
+    raw = np.ascontiguousarray(raw, np.uint8)
+    no, nv = C.c_long(), C.c_long()
+    err = C.create_string_buffer(512)
+    rc = L.tdp_raw_check(_ptr(raw), raw.size, C.byref(no), C.byref(nv), err, 512)
+    if rc != TDP_OK:
+        raise TdpError(rc, err.value.decode())
+    return no.value, nv.value
+
+
+def pinned_empty(nbytes: int) -> np.ndarray:
+    """A uint8 array in page-locked host memory (tdp_host_alloc), freed when the
+    array is collected: the buffer to read a tile into before attaching it."""
+    import weakref
+    L = lib()
+    L.tdp_host_alloc.argtypes = [C.c_size_t, C.POINTER(C.c_void_p)]
+    L.tdp_host_free.argtypes = [C.c_void_p]
+    p = C.c_void_p()
+    rc = L.tdp_host_alloc(int(nbytes), C.byref(p))
+    if rc != TDP_OK:
+        raise TdpError(rc, f"tdp_host_alloc({nbytes}) failed")
+    buf = (C.c_uint8 * int(nbytes)).from_address(p.value)
+    arr = np.frombuffer(buf, np.uint8)
+    weakref.finalize(buf, L.tdp_host_free, p.value)
+    return arr
+
+
+def pinned_copy(raw: np.ndarray) -> np.ndarray:
+    """`raw` copied into page-locked host memory (see pinned_empty)."""
+    out = pinned_empty(raw.size)
+    out[:] = np.asarray(raw, np.uint8).ravel()
+    return out
 
 
 class BoundsInfo(C.Structure):

@@ -13,8 +13,11 @@ RAW .dt format.  The reference publishes no numbers, so vs_baseline is null.
                max over ranks
   plain        the same join through the plain form (one CTA per voxel pair,
                reference FP32 decision rules): the tuned/plain ratio
-  e2e          the same metric through the public C ABI from pinned host tile
-               bytes: tile upload (H2D + unpack) + join + result read-back
+  e2e          the same metric through the public C ABI from page-locked host
+               tile bytes: both tiles attached (metadata copied), the join
+               fetching each LOD's refined voxels from the host bytes, result
+               read-back, tiles released; fresh tiles every step (the whole
+               upload path is reported beside it)
   roofline     the dominant kernel (tuned refine), FP32 CUDA-core bound
   cpu_baseline the reference's own CPU code (MeshDist, octree; compiled from
                source into oracle/_ref) on a bounded sample of query nuclei,
@@ -372,7 +375,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=1500, help="query nuclei in the CPU-baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream measurement")
     ap.add_argument("--no-self", action="store_true", help="skip the 10-NN self-join measurement")
     ap.add_argument("--no-bounds", action="store_true", help="skip the GPU bound-preparation measurement")
@@ -520,25 +523,48 @@ def main():
                  "voxel_pairs_fp64": st_x["exact_f64_items"], "fp32_max_rel_err": st_x["fp32_max_rel_err"],
                  "note": "untimed; every result's LOD-100 distance in FP64"}
 
-        # end to end through the C ABI from pinned host bytes: tile upload
-        # (H2D + unpack), join, result read-back and tile release, between two
-        # events on the context's stream
-        e2e_ms = []
-        d2h = 0
-        for i in range(a.e2e_steps + 1 if a.e2e_steps > 0 else 0):
-            barrier()
+        # end to end through the C ABI from the page-locked host tile bytes:
+        # attach both tiles (voxel metadata up), join (each LOD fetches the
+        # triangles of the voxels it refines from the host bytes), result
+        # read-back, tile release -- between two events on the context's
+        # stream, every step on freshly attached tiles.  The same with whole
+        # uploads (every byte of both tiles copied and unpacked) is measured
+        # once beside it.
+        def e2e_step_run(attach):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            U1, U2 = pkg.tdp.Tile(ctx, nb), pkg.tdp.Tile(ctx, vb)
+            h0 = time.perf_counter()
+            U1, U2 = pkg.tdp.Tile(ctx, nb, attach=attach), pkg.tdp.Tile(ctx, vb, attach=attach)
+            h1 = time.perf_counter()
             q, r, d = ctx.join(U1, U2, query="within", within=TAU, form=pkg.FORM_TUNED)
+            h2 = time.perf_counter()
+            fetched = ctx.stats()["fetch_bytes"]
+            i1, i2 = U1.info(), U2.info()
+            h2d_b = i1["h2d_bytes"] + i2["h2d_bytes"] + int(fetched)
             U1.free(); U2.free()
             e1.record(stream)
             e1.synchronize()
-            d2h = q.nbytes + r.nbytes + d.nbytes
+            h3 = time.perf_counter()
+            return (e0.elapsed_time(e1), h2d_b, q.nbytes + r.nbytes + d.nbytes,
+                    {"tiles_ms": 1e3 * (h1 - h0), "parse_ms": i1["parse_ms"] + i2["parse_ms"],
+                     "alloc_ms": i1["alloc_ms"] + i2["alloc_ms"], "join_ms": 1e3 * (h2 - h1),
+                     "fetch_bytes": fetched, "release_ms": 1e3 * (h3 - h2)})
+
+        e2e_ms, h2d, d2h, e2e_parts = [], 0, 0, None
+        for i in range(a.e2e_steps + 1 if a.e2e_steps > 0 else 0):
+            barrier()
+            ms, h2d, d2h, e2e_parts = e2e_step_run(True)
             if i > 0:
-                e2e_ms.append(e0.elapsed_time(e1))
+                e2e_ms.append(ms)
         e2e_step = allmax(statistics.median(e2e_ms)) if e2e_ms else float("nan")
         e2e_value = tri / (e2e_step / 1e3) if e2e_ms else None
+        e2e_upload = None
+        if a.e2e_steps > 0:
+            barrier()
+            ms_u, h2d_u, _, parts_u = e2e_step_run(False)
+            e2e_upload = {"value": tri / (allmax(ms_u) / 1e3), "unit": "tri-pairs/s", "ms_per_step": allmax(ms_u),
+                          "h2d_bytes_per_step": int(h2d_u), "host_ms": parts_u,
+                          "note": "tiles uploaded whole (every LOD of every object copied and unpacked), one step"}
 
         serving = None
         if not a.no_serve and ws == 1:
@@ -581,7 +607,10 @@ def main():
             "plain": {"value": plain_value, "unit": "tri-pairs/s", "ms_per_step": plain_ms,
                       "tuned_over_plain": value / plain_value if plain_value else None},
             "e2e": {"value": e2e_value, "unit": "tri-pairs/s", "ms_per_step": e2e_step,
-                    "h2d_bytes_per_step": int(nb.size + vb.size), "d2h_bytes_per_step": int(d2h)},
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "path": "tdp_tile_attach x2 (page-locked host tiles, 36.8 GB) + tdp_join (per-LOD fetch of the "
+                            "voxels refined) + result read-back + tdp_tile_free, fresh tiles every step",
+                    "host_ms": e2e_parts, "upload_path": e2e_upload},
             "exact_distances": exact,
             "serving": serving,
             "bounds_prep": bounds_prep,

@@ -47,7 +47,11 @@ typedef struct tdp_result tdp_result;
 
 /* ---- context --------------------------------------------------------------
  * device: CUDA ordinal.  budget_bytes: cap on device memory this context may
- * hold (0 = no cap beyond what the device has).  flags: reserved, pass 0. */
+ * hold (0 = no cap beyond what the device has).  flags: 0, or TDP_CTX_POISON:
+ * the triangle records of attached tiles start as NaN instead of whatever the
+ * allocation held, so that a read of a record no fetch filled shows in the
+ * results (for tests; it costs a memset of the records per attach). */
+#define TDP_CTX_POISON 1u
 int tdp_ctx_create(int device, size_t budget_bytes, unsigned flags, tdp_ctx **out);
 int tdp_ctx_destroy(tdp_ctx *ctx);
 const char *tdp_last_error(const tdp_ctx *ctx);
@@ -76,6 +80,8 @@ typedef struct {
     long exact_f64_items;            /* of those, evaluated in FP64             */
     double fp32_max_rel_err;         /* exact stage: max |FP32 minimum - FP64
                                         distance| / max(distance, 1)           */
+    double fetch_bytes;              /* RAW bytes fetched from attached tiles
+                                        (tdp_tile_attach) during the call     */
     long lod_graph;                  /* tuned LOD loop: 0 launched directly,
                                         1 replayed the context's CUDA graph,
                                         2 captured (or updated) it in this call */
@@ -131,8 +137,32 @@ typedef struct {
     long n_voxels;
     long n_tris[5];        /* per LOD 20,40,60,80,100 */
     size_t device_bytes;
+    size_t h2d_bytes;      /* bytes the upload / attach itself copied host -> device */
+    int attached;          /* 1 for a tile made by tdp_tile_attach */
+    double parse_ms;       /* host time of the upload / attach: parsing the bytes, */
+    double alloc_ms;       /* allocating the device arrays,                       */
+    double load_ms;        /* and in total                                        */
 } tdp_tile_info;
 int tdp_tile_upload(tdp_ctx *ctx, const void *raw_dt, size_t len, long max_objects, tdp_tile **out);
+/* Attach a RAW tile that stays in page-locked host memory (cudaHostRegister or
+ * cudaHostAlloc covering all len bytes; it must outlive the tile): only the
+ * voxel and object metadata are copied now; each join copies, LOD by LOD, the
+ * triangles of the voxels its refine touches, straight from the host bytes,
+ * and keeps them for later joins on the tile.  This is the reference's
+ * per-LOD staging of the voxels a chunk needs (build_chunks_by_pair /
+ * packing_data_stream, src/join/KNNJoin.cpp:1473-1521,
+ * src/join/SpatialJoin.cpp:169-248) done by the GPU.  Results equal those of
+ * an uploaded tile.  The tile must be in the writer's layout (each object's
+ * data block LOD by LOD, voxel by voxel: src/storage/tile_IO.cpp:79-172),
+ * else TDP_ERR_FORMAT; unlocked memory is TDP_ERR_ARG. */
+int tdp_tile_attach(tdp_ctx *ctx, const void *raw_dt, size_t len, long max_objects, tdp_tile **out);
+/* Validate RAW tile bytes on the host (no device needed): the same
+ * bounds-checked parser the uploads use.  TDP_ERR_FORMAT with the first
+ * problem in file order described in err (NUL-terminated, err_len bytes). */
+int tdp_raw_check(const void *raw, size_t len, long *n_objects, long *n_voxels, char *err, size_t err_len);
+/* page-locked host memory (cudaHostAlloc) to read tiles into for attaching */
+int tdp_host_alloc(size_t bytes, void **out);
+int tdp_host_free(void *p);
 int tdp_tile_free(tdp_ctx *ctx, tdp_tile *tile);
 int tdp_tile_get_info(const tdp_tile *tile, tdp_tile_info *out);
 

@@ -65,3 +65,27 @@ def read_tile(buf, max_objects=None):
             hds.append(hl)
         objs.append(Obj(vox, tris, hds, hp[:, 0].copy(), hp[:, 1].copy(), xf))
     return objs
+
+
+def write_tile(objects, lod_order=(0, 1, 2, 3, 4)):
+    """RAW tile bytes (uint8 array) from objects given as [lod][voxel] -> float32
+    array [n, 9]; bounds written as zeros, voxel boxes from the triangles, core =
+    the first vertex.  lod_order: the order in which the LOD blocks are laid out
+    in each object's data block (the writer's order is 20, 40, ..., 100)."""
+    out = bytearray([1])
+    for obj in objects:
+        nv = len(obj[4])
+        data = bytearray()
+        offc = np.zeros((nv, 5, 2), np.uint64)
+        for li in lod_order:
+            for v in range(nv):
+                t = np.asarray(obj[li][v], np.float32).reshape(-1, 9)
+                offc[v, li] = (len(data), len(t))
+                data += t.tobytes() + np.zeros((len(t), 2), np.float32).tobytes()
+        out += struct.pack("<Q", len(data)) + data + struct.pack("<Q", nv) + np.zeros(10, np.float32).tobytes()
+        for v in range(nv):
+            pts = np.concatenate([np.asarray(obj[li][v], np.float32).reshape(-1, 3) for li in range(5)])
+            lo, hi = pts.min(0), pts.max(0)
+            out += np.concatenate([lo, hi, pts[0]]).astype(np.float32).tobytes() + offc[v].tobytes()
+        out += np.zeros(3, np.float32).tobytes()
+    return np.frombuffer(bytes(out), np.uint8).copy()

@@ -1,0 +1,125 @@
+"""Attached tiles (tdp_tile_attach): the triangles stay in page-locked host
+memory and each join fetches the voxels its refine touches.  Every join on
+attached tiles must return exactly what the same join on uploaded tiles
+returns (ids, distances, exact FP64 distances), fetch only part of the tile,
+and fetch nothing the second time; attach refuses unlocked memory and tiles
+not in the writer's layout.  The context poisons attached records with NaN,
+so a record that no fetch filled would change the results."""
+import numpy as np
+import pytest
+
+from join_cases import CASES, tiles
+from rawdt import read_tile, write_tile
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pctx(pkg):
+    c = pkg.Context(0, 0, pkg.tdp.CTX_POISON)
+    yield c
+    c.close()
+
+
+def both(pkg, ctx, nb, vb):
+    up = (pkg.tdp.Tile(ctx, nb), pkg.tdp.Tile(ctx, vb))
+    pn, pv = pkg.tdp.pinned_copy(nb), pkg.tdp.pinned_copy(vb)
+    at = (pkg.tdp.Tile(ctx, pn, attach=True), pkg.tdp.Tile(ctx, pv, attach=True))
+    return up, at
+
+
+def same(a, b):
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_attached_join_equals_uploaded(pkg, pctx, name):
+    nv, npv, seed, query, knn, tau, self_join, lods, level = CASES[name]
+    nb, vb = tiles(nv, npv, seed)
+    U1, U2 = pkg.tdp.Tile(pctx, nb), pkg.tdp.Tile(pctx, vb)
+    pn, pv = pkg.tdp.pinned_copy(nb), pkg.tdp.pinned_copy(vb)
+    for form in (pkg.FORM_PLAIN, pkg.FORM_TUNED):
+        args = dict(query=query, knn=knn, within=tau, lods=lods, hausdorff_level=level, form=form)
+        want = pctx.join(U1, None if self_join else U2, **args)
+        assert pctx.stats()["fetch_bytes"] == 0
+        # freshly attached tiles per form: nothing fetched yet
+        A1, A2 = pkg.tdp.Tile(pctx, pn, attach=True), pkg.tdp.Tile(pctx, pv, attach=True)
+        got = pctx.join(A1, None if self_join else A2, **args)
+        st = pctx.stats()
+        assert st["refine_items"] == 0 or st["fetch_bytes"] > 0
+        same(got, want)
+        A1.free()
+        A2.free()
+    U1.free()
+    U2.free()
+
+
+def test_attached_fetches_part_once(pkg, pctx):
+    nb, vb = tiles(6, 12, 101)
+    (U1, U2), (A1, A2) = both(pkg, pctx, nb, vb)
+    info = A1.info()
+    assert info["attached"] and not U1.info()["attached"]
+    assert info["h2d_bytes"] < nb.size // 10
+    args = dict(query="within", within=400.0, exact_distances=True)
+    want = pctx.join(U1, U2, **args)
+    got = pctx.join(A1, A2, **args)
+    same(got, want)
+    st = pctx.stats()
+    assert 0 < st["fetch_bytes"] < (nb.size + vb.size) / 2, st["fetch_bytes"]
+    again = pctx.join(A1, A2, **args)
+    same(again, want)
+    assert pctx.stats()["fetch_bytes"] == 0          # every voxel it needs is resident now
+    # other queries on the same attached tiles still agree
+    same(pctx.join(A1, A2, query="within", within=150.0), pctx.join(U1, U2, query="within", within=150.0))
+    same(pctx.join(A1, A2, query="nn", knn=5), pctx.join(U1, U2, query="nn", knn=5))
+    for T in (U1, U2, A1, A2):
+        T.free()
+
+
+def test_attached_exact_mixed_and_graph(pkg, pctx):
+    nb, vb = tiles(6, 12, 101)
+    (U1, U2), (A1, A2) = both(pkg, pctx, nb, vb)
+    want = pctx.join(U1, U2, query="within", within=400.0, exact_distances=True)
+    got = pctx.join(A1, A2, query="within", within=400.0, exact_distances=True)
+    same(got, want)
+    n1 = U1.info()["n_objects"]
+    rng = np.random.default_rng(3)
+    ok = rng.integers(0, 4, n1).astype(np.int32)
+    ow = np.where(ok == 0, 120.0, 0.0).astype(np.float32)
+    same(pctx.join(A1, A2, obj_knn=ok, obj_within=ow), pctx.join(U1, U2, obj_knn=ok, obj_within=ow))
+    # repeated joins replay the LOD graph with the fetch step inside it
+    pctx.set_lod_graph(pkg.tdp.LOD_GRAPH_ALWAYS)
+    try:
+        for _ in range(2):
+            same(pctx.join(A1, A2, query="nn", knn=2), pctx.join(U1, U2, query="nn", knn=2))
+    finally:
+        pctx.set_lod_graph(pkg.tdp.LOD_GRAPH_AUTO)
+    for T in (U1, U2, A1, A2):
+        T.free()
+
+
+def test_attached_bounds_equal_uploaded(pkg, pctx):
+    nb, vb = pkg.tdp.gen_tiles(1, 5, seed=13)
+    U = pkg.tdp.Tile(pctx, nb)
+    A = pkg.tdp.Tile(pctx, pkg.tdp.pinned_copy(nb), attach=True)
+    pctx.compute_bounds(U)
+    pctx.compute_bounds(A)
+    V = pkg.tdp.Tile(pctx, vb)
+    same(pctx.join(A, V, query="nn", knn=1), pctx.join(U, V, query="nn", knn=1))
+    for T in (U, A, V):
+        T.free()
+
+
+def test_attach_refusals(pkg, pctx):
+    nb, _ = tiles(2, 4, 7)
+    with pytest.raises(pkg.TdpError) as e:
+        pkg.tdp.Tile(pctx, np.array(nb), attach=True)          # pageable memory
+    assert e.value.code == 1
+    N = read_tile(nb)
+    objs = [[list(o.tris[li]) for li in range(5)] for o in N[:2]]
+    shuffled = write_tile(objs, lod_order=(4, 3, 2, 1, 0))     # valid RAW, not the writer's layout
+    pkg.tdp.Tile(pctx, shuffled).free()
+    with pytest.raises(pkg.TdpError) as e:
+        pkg.tdp.Tile(pctx, pkg.tdp.pinned_copy(shuffled), attach=True)
+    assert e.value.code == 4

@@ -10,14 +10,12 @@ bytes compared whole), including hand-made edge cases, and a join on tiles
 whose bounds came from the GPU to return the FP64 exact result set.
 """
 import ctypes as C
-import struct
-
 import numpy as np
 import pytest
 
 from join_cases import exact_truth
 from oracle_bind import oracle
-from rawdt import read_tile
+from rawdt import read_tile, write_tile as make_raw
 
 P = C.c_void_p
 
@@ -46,28 +44,6 @@ def violation(raw, samples=3, seed=5):
 
 def small_tiles(pkg, seed=11):
     return pkg.tdp.gen_tiles(1, 4, seed=seed, tube_sides=8, tube_rings=12)
-
-
-def make_raw(objects):
-    """RAW tile bytes from objects given as [lod][voxel] -> float32 array [n, 9]
-    (bounds written as zeros; voxel boxes from the triangles, core = first vertex)."""
-    out = bytearray([1])
-    for obj in objects:
-        nv = len(obj[4])
-        data = bytearray()
-        offc = np.zeros((nv, 5, 2), np.uint64)
-        for li in range(5):
-            for v in range(nv):
-                t = np.asarray(obj[li][v], np.float32).reshape(-1, 9)
-                offc[v, li] = (len(data), len(t))
-                data += t.tobytes() + np.zeros((len(t), 2), np.float32).tobytes()
-        out += struct.pack("<Q", len(data)) + data + struct.pack("<Q", nv) + np.zeros(10, np.float32).tobytes()
-        for v in range(nv):
-            pts = np.concatenate([np.asarray(obj[li][v], np.float32).reshape(-1, 3) for li in range(5)])
-            lo, hi = pts.min(0), pts.max(0)
-            out += np.concatenate([lo, hi, pts[0]]).astype(np.float32).tobytes() + offc[v].tobytes()
-        out += np.zeros(3, np.float32).tobytes()
-    return np.frombuffer(bytes(out), np.uint8).copy()
 
 
 def edge_case_tile(pkg):
