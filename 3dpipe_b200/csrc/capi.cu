@@ -154,6 +154,7 @@ int tdp_ctx_destroy(tdp_ctx* ctx) {
     if (ctx->lod_graph) cudaGraphExecDestroy(ctx->lod_graph);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->hres) cudaFreeHost(ctx->hres);
+    if (ctx->hstage) cudaFreeHost(ctx->hstage);
     delete ctx;
     return TDP_OK;
 }

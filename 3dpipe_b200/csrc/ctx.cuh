@@ -72,6 +72,8 @@ struct tdp_ctx {
     // budget, and on destroy.
     std::multimap<size_t, void*> block_cache;
     size_t cached_bytes = 0;
+    void* hstage = nullptr;  // page-locked staging of tile metadata uploads (grow-only)
+    size_t hstage_cap = 0;
 };
 
 namespace tdp {

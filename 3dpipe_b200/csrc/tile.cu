@@ -13,6 +13,9 @@
 // at an object's first byte into a 256-byte aligned staging buffer, which makes
 // every float 4-byte aligned on the device (checked on the host per segment).
 #include <algorithm>
+#include <atomic>
+#include <climits>
+#include <thread>
 #include <chrono>
 #include <cstring>
 #include <string>
@@ -55,6 +58,16 @@ cudaError_t launch_unpack(const uint8_t* raw, const UnpackSeg* segs, int nseg, f
     const int blocks = (int)std::min<size_t>(((size_t)nseg + 7) / 8, (size_t)num_sms * 16);
     unpack_kernel<<<blocks, 256, 0, s>>>(raw, segs, nseg, tp);
     return cudaGetLastError();
+}
+
+// fn(b, e) over [0, n) in a few host threads (one for small n)
+template <typename Fn>
+static void host_parallel(long n, Fn fn) {
+    const long nt = std::max(1L, std::min<long>((long)std::thread::hardware_concurrency(), n / 65536));
+    if (nt == 1) { fn(0L, n); return; }
+    std::vector<std::thread> pool;
+    for (long k = 0; k < nt; ++k) pool.emplace_back([&, k] { fn(n * k / nt, n * (k + 1) / nt); });
+    for (auto& th : pool) th.join();
 }
 
 void tile_release(tdp_ctx* ctx, tdp_tile* t) {
@@ -118,31 +131,57 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
     TileHost& H = T->host;
     T->n_obj = H.n_obj;
     T->n_vox = H.n_vox;
-    for (int l = 0; l < kNumLods; ++l) {
+    for (int l = 0; l < kNumLods; ++l)
         if (H.n_tris[l] >= 0xffffffffull) { delete T; return fail(ctx, TDP_ERR_FORMAT, "more than 2^32 triangles in one LOD"); }
-        for (long v = 0; v < H.n_vox; ++v)
-            if ((H.vox_byte_off[l][v] & 3u) != 1u) { delete T; return fail(ctx, TDP_ERR_FORMAT, "misaligned triangle data"); }
-        T->h_vtri[l].resize(H.n_vox + 1);
-        T->h_vtri[l][0] = 0;
-        for (long v = 0; v < H.n_vox; ++v) T->h_vtri[l][v + 1] = T->h_vtri[l][v] + H.vox_cnt[l][v];
+    // per LOD (one host thread each): alignment of every voxel's floats and
+    // the prefix of triangle counts
+    {
+        bool misaligned[kNumLods] = {false, false, false, false, false};
+        std::vector<std::thread> pool;
+        for (int l = 0; l < kNumLods; ++l)
+            pool.emplace_back([&, l] {
+                std::vector<uint32_t>& vt = T->h_vtri[l];
+                vt.resize(H.n_vox + 1);
+                vt[0] = 0;
+                const uint64_t* off = H.vox_byte_off[l].data();
+                const uint32_t* cnt = H.vox_cnt[l].data();
+                for (long v = 0; v < H.n_vox; ++v) {
+                    misaligned[l] |= (off[v] & 3u) != 1u;
+                    vt[v + 1] = vt[v] + cnt[v];
+                }
+            });
+        for (auto& th : pool) th.join();
+        for (int l = 0; l < kNumLods; ++l)
+            if (misaligned[l]) { delete T; return fail(ctx, TDP_ERR_FORMAT, "misaligned triangle data"); }
     }
     if (attach) {
         // fetches locate a voxel's bytes from the prefix arrays: the data
         // block must hold, LOD by LOD and voxel by voxel, each voxel's
         // triangles then its bounds, with nothing in between (the layout the
         // reference's writer produces, src/storage/tile_IO.cpp:79-172)
-        for (long o = 0; o < H.n_obj; ++o) {
-            uint64_t expect = H.obj_data_off[o];
-            for (int l = 0; l < kNumLods; ++l)
-                for (uint32_t v = H.obj_vox_off[o]; v < H.obj_vox_off[o + 1]; ++v) {
-                    if (H.vox_byte_off[l][v] != expect) {
-                        delete T;
-                        return fail(ctx, TDP_ERR_FORMAT, "object " + std::to_string(o) +
-                                                             " does not keep its voxels' triangles in LOD and voxel "
-                                                             "order; use tdp_tile_upload for this tile");
+        std::atomic<long> first_bad{LONG_MAX};
+        host_parallel(H.n_obj, [&](long b, long e) {
+            for (long o = b; o < e; ++o) {
+                uint64_t expect = H.obj_data_off[o];
+                bool ok = true;
+                for (int l = 0; l < kNumLods && ok; ++l)
+                    for (uint32_t v = H.obj_vox_off[o]; v < H.obj_vox_off[o + 1]; ++v) {
+                        if (H.vox_byte_off[l][v] != expect) { ok = false; break; }
+                        expect += 44ull * H.vox_cnt[l][v];
                     }
-                    expect += 44ull * H.vox_cnt[l][v];
+                if (!ok) {
+                    long cur = first_bad.load();
+                    while (o < cur && !first_bad.compare_exchange_weak(cur, o)) {}
+                    return;
                 }
+            }
+        });
+        if (first_bad.load() != LONG_MAX) {
+            const long o = first_bad.load();
+            delete T;
+            return fail(ctx, TDP_ERR_FORMAT, "object " + std::to_string(o) +
+                                                 " does not keep its voxels' triangles in LOD and voxel "
+                                                 "order; use tdp_tile_upload for this tile");
         }
     }
     const auto ta = std::chrono::steady_clock::now();
@@ -173,21 +212,58 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
     }
     T->alloc_ms = ms_since(ta);
     {
-        std::vector<float4> v4((size_t)H.n_vox * 3);
-        for (long v = 0; v < H.n_vox; ++v) {
-            const float* b = &H.vox_box[9 * v];
-            v4[3 * v + 0] = make_float4(b[0], b[1], b[2], 0.f);
-            v4[3 * v + 1] = make_float4(b[3], b[4], b[5], 0.f);
-            v4[3 * v + 2] = make_float4(b[6], b[7], b[8], 0.f);
+        // the metadata go up through the context's page-locked staging buffer
+        // (assembled by host threads), so the copies run at full PCIe rate
+        const size_t v4_bytes = (size_t)H.n_vox * 3 * sizeof(float4);
+        const size_t vt_bytes = (size_t)(H.n_vox + 1) * sizeof(uint32_t);
+        const size_t ov_bytes = H.obj_vox_off.size() * 4, hd_bytes = H.obj_hd.size() * 4;
+        const size_t need = v4_bytes + kNumLods * vt_bytes + ov_bytes + 2 * hd_bytes + 64;
+        if (need > ctx->hstage_cap) {
+            if (ctx->hstage) cudaFreeHost(ctx->hstage);
+            ctx->hstage = nullptr;
+            ctx->hstage_cap = 0;
+            if (cudaHostAlloc(&ctx->hstage, need + need / 4, cudaHostAllocDefault) == cudaSuccess)
+                ctx->hstage_cap = need + need / 4;
+            else { cudaGetLastError(); ctx->hstage = nullptr; }
         }
-        CTRY(cudaMemcpyAsync(T->vox, v4.data(), v4.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
-        CTRY(cudaMemcpyAsync(T->obj_vox, H.obj_vox_off.data(), H.obj_vox_off.size() * 4, cudaMemcpyHostToDevice, s));
-        CTRY(cudaMemcpyAsync(T->obj_hd, H.obj_hd.data(), H.obj_hd.size() * 4, cudaMemcpyHostToDevice, s));
-        CTRY(cudaMemcpyAsync(T->obj_phd, H.obj_phd.data(), H.obj_phd.size() * 4, cudaMemcpyHostToDevice, s));
+        std::vector<float4> v4_pageable;
+        float4* v4 = nullptr;
+        if (ctx->hstage) v4 = (float4*)ctx->hstage;
+        else { v4_pageable.resize((size_t)H.n_vox * 3); v4 = v4_pageable.data(); }
+        host_parallel(H.n_vox, [&](long b, long e) {
+            for (long v = b; v < e; ++v) {
+                const float* x = &H.vox_box[9 * v];
+                v4[3 * v + 0] = make_float4(x[0], x[1], x[2], 0.f);
+                v4[3 * v + 1] = make_float4(x[3], x[4], x[5], 0.f);
+                v4[3 * v + 2] = make_float4(x[6], x[7], x[8], 0.f);
+            }
+        });
+        const void* src_vt[kNumLods];
+        const void* src_ov = H.obj_vox_off.data();
+        const void* src_hd = H.obj_hd.data();
+        const void* src_phd = H.obj_phd.data();
+        if (ctx->hstage) {
+            uint8_t* p = (uint8_t*)ctx->hstage + v4_bytes;
+            std::vector<std::thread> pool;
+            for (int l = 0; l < kNumLods; ++l) {
+                src_vt[l] = p;
+                pool.emplace_back([&, l, p] { std::memcpy(p, T->h_vtri[l].data(), vt_bytes); });
+                p += vt_bytes;
+            }
+            for (auto& th : pool) th.join();
+            std::memcpy(p, src_ov, ov_bytes); src_ov = p; p += ov_bytes;
+            std::memcpy(p, src_hd, hd_bytes); src_hd = p; p += hd_bytes;
+            std::memcpy(p, src_phd, hd_bytes); src_phd = p;
+        } else {
+            for (int l = 0; l < kNumLods; ++l) src_vt[l] = T->h_vtri[l].data();
+        }
+        CTRY(cudaMemcpyAsync(T->vox, v4, v4_bytes, cudaMemcpyHostToDevice, s));
+        CTRY(cudaMemcpyAsync(T->obj_vox, src_ov, ov_bytes, cudaMemcpyHostToDevice, s));
+        CTRY(cudaMemcpyAsync(T->obj_hd, src_hd, hd_bytes, cudaMemcpyHostToDevice, s));
+        CTRY(cudaMemcpyAsync(T->obj_phd, src_phd, hd_bytes, cudaMemcpyHostToDevice, s));
         for (int l = 0; l < kNumLods; ++l)
-            CTRY(cudaMemcpyAsync(T->vtri[l], T->h_vtri[l].data(), T->h_vtri[l].size() * 4, cudaMemcpyHostToDevice, s));
-        T->h2d_bytes += v4.size() * sizeof(float4) + H.obj_vox_off.size() * 4 + H.obj_hd.size() * 8;
-        for (int l = 0; l < kNumLods; ++l) T->h2d_bytes += T->h_vtri[l].size() * 4;
+            CTRY(cudaMemcpyAsync(T->vtri[l], src_vt[l], vt_bytes, cudaMemcpyHostToDevice, s));
+        T->h2d_bytes += v4_bytes + ov_bytes + 2 * hd_bytes + kNumLods * vt_bytes;
         CTRY(cudaStreamSynchronize(s));
     }
     if (attach) {
