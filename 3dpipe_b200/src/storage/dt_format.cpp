@@ -117,7 +117,22 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
     size_t pos = 1;
     uint64_t nvox = 0;
     constexpr size_t kVoxBytes = 9 * sizeof(float) + kNumLods * 2 * sizeof(uint64_t);
+    // Every object's position depends on the sizes read at the previous one,
+    // so the walk is a chain of dependent loads.  Objects of one tile are
+    // mostly the same size (instances of one mesh), so the headers of the
+    // next few objects are prefetched at the last record's stride; a wrong
+    // guess only wastes a prefetch.
+    uint64_t stride = 0, last_ds = 0;
+    constexpr int kAhead = 8;
     while (pos < len && (max_objects <= 0 || (long)recs.size() < max_objects)) {
+        if (stride)
+            for (int k = 1; k <= kAhead; ++k) {
+                const uint64_t q = pos + k * stride;
+                if (q + 8 + last_ds + 8 > len) break;
+                __builtin_prefetch(buf + q);
+                __builtin_prefetch(buf + q + 8 + last_ds);
+            }
+        const size_t start = pos;
         uint64_t data_size = 0, vnum = 0;
         if (!rd(buf, len, pos, data_size) || data_size > len - pos || data_size % 4)
             return parse_sequential(buf, len, max_objects, T, err);
@@ -129,6 +144,8 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
         if (rec > len - pos) return parse_sequential(buf, len, max_objects, T, err);
         recs.push_back({data_off, data_size, pos, vnum});
         pos += rec;
+        stride = pos - start;
+        last_ds = data_size;
         nvox += vnum;
         if (nvox >= 0xffffffffull) return parse_sequential(buf, len, max_objects, T, err);
     }
@@ -156,8 +173,14 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
     std::vector<std::array<uint64_t, kNumLods>> tris(nt);
     auto work = [&](int k) {
         tris[k].fill(0);
-        for (long o = n * k / nt; o < n * (k + 1) / nt; ++o) {
+        const long o_end = n * (k + 1) / nt;
+        for (long o = n * k / nt; o < o_end; ++o) {
             const Rec& r = recs[o];
+            if (o + 4 < o_end) {  // the metadata of a later object, ahead of its turn
+                const Rec& f = recs[o + 4];
+                const uint64_t bytes = 2 * kNumLods * sizeof(float) + f.vnum * kVoxBytes;
+                for (uint64_t b = 0; b < bytes; b += 64) __builtin_prefetch(buf + f.meta + b);
+            }
             const uint8_t* p = buf + r.meta;
             float hp[2 * kNumLods];
             std::memcpy(hp, p, sizeof(hp));

@@ -20,6 +20,8 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <memory>
+#include <utility>
 #include <vector>
 
 namespace tdp {
@@ -34,20 +36,45 @@ inline int lod_index(int lod) {
     return -1;
 }
 
+// An allocator whose resize() leaves new elements of plain types
+// uninitialised: the parser writes every element from its own threads, so a
+// tile's arrays are touched first there (in parallel) instead of being
+// zeroed by one thread beforehand.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U* p) noexcept {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <typename U, typename... A>
+    void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+template <typename T>
+using HostVec = std::vector<T, NoInitAlloc<T>>;
+
 // Host-side view of a parsed RAW tile.  Offsets point into the caller's byte buffer.
 struct TileHost {
     long n_obj = 0;
     long n_vox = 0;
-    std::vector<uint64_t> obj_data_off;     // byte offset of each object's data block
-    std::vector<uint64_t> obj_data_size;
-    std::vector<uint32_t> obj_vox_off;      // [n_obj+1]
-    std::vector<float> obj_box;             // 6 per object: low xyz, high xyz
-    std::vector<float> obj_xf;              // 3 per object
-    std::vector<float> obj_hd;              // kNumLods per object (hausdorff)
-    std::vector<float> obj_phd;             // kNumLods per object (proxy hausdorff)
-    std::vector<float> vox_box;             // 9 per voxel: low xyz, high xyz, core xyz
-    std::vector<uint64_t> vox_byte_off[kNumLods];  // absolute byte offset of the voxel's triangles
-    std::vector<uint32_t> vox_cnt[kNumLods];
+    HostVec<uint64_t> obj_data_off;     // byte offset of each object's data block
+    HostVec<uint64_t> obj_data_size;
+    HostVec<uint32_t> obj_vox_off;      // [n_obj+1]
+    HostVec<float> obj_box;             // 6 per object: low xyz, high xyz
+    HostVec<float> obj_xf;              // 3 per object
+    HostVec<float> obj_hd;              // kNumLods per object (hausdorff)
+    HostVec<float> obj_phd;             // kNumLods per object (proxy hausdorff)
+    HostVec<float> vox_box;             // 9 per voxel: low xyz, high xyz, core xyz
+    HostVec<uint64_t> vox_byte_off[kNumLods];  // absolute byte offset of the voxel's triangles
+    HostVec<uint32_t> vox_cnt[kNumLods];
     uint64_t n_tris[kNumLods] = {0, 0, 0, 0, 0};
 };
 
