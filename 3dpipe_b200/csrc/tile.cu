@@ -140,7 +140,7 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
         std::vector<std::thread> pool;
         for (int l = 0; l < kNumLods; ++l)
             pool.emplace_back([&, l] {
-                std::vector<uint32_t>& vt = T->h_vtri[l];
+                HostVec<uint32_t>& vt = T->h_vtri[l];
                 vt.resize(H.n_vox + 1);
                 vt[0] = 0;
                 const uint64_t* off = H.vox_byte_off[l].data();

@@ -45,7 +45,7 @@ struct tdp_tile {
     float* obj_phd = nullptr;
     float4* tri[tdp::kNumLods] = {};
     uint32_t* vtri[tdp::kNumLods] = {};
-    std::vector<uint32_t> h_vtri[tdp::kNumLods];  // host copy of vtri
+    tdp::HostVec<uint32_t> h_vtri[tdp::kNumLods];  // host copy of vtri
     size_t device_bytes = 0;
     size_t h2d_bytes = 0;  // bytes copied host -> device by the upload or attach itself
     double parse_ms = 0, alloc_ms = 0, load_ms = 0;  // host time of the upload or attach
