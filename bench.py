@@ -71,8 +71,15 @@ class ClockSampler:
         try:
             self.f = tempfile.TemporaryFile(mode="w+")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            # the timed loop starts only once the sampler is producing lines
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and self.proc.poll() is None:
+                self.f.flush()
+                if os.fstat(self.f.fileno()).st_size > 0:
+                    break
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
@@ -370,7 +377,7 @@ def run_reference_arm(a):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=1500, help="query nuclei in the CPU-baseline sample")
