@@ -155,14 +155,30 @@ __global__ void __launch_bounds__(kWarps * 32) k_cand_kth(DG pg, const float* __
     }
 }
 
+// first box-grid cell (the cell of its low corner) of every object of tile 2
+__global__ void k_first_cells(DG bg, const float* __restrict__ box2, int n2, int4* __restrict__ fc) {
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n2; o += gridDim.x * blockDim.x) {
+        const float* ob = box2 + 6 * (size_t)o;
+        fc[o] = make_int4(dci(ob[0], bg.lo0, bg.cell, bg.n0), dci(ob[1], bg.lo1, bg.cell, bg.n1),
+                          dci(ob[2], bg.lo2, bg.cell, bg.n2), 0);
+    }
+}
+
+// The cells of the scan range are taken 32 at a time, one per lane; their
+// item counts are prefix-summed across the warp and the lanes then stride
+// over the items of all 32 cells together (each lane finds its item's cell by
+// a binary search over the prefix), so a range of many sparse cells costs a
+// few warp iterations instead of one per cell.
 template <bool WRITE>
 __global__ void __launch_bounds__(256) k_cand_pass(DG bg, const float* __restrict__ box1, const float* __restrict__ xf1,
                                                    const float* __restrict__ box2, const float* __restrict__ xf2,
-                                                   int n1, int self, int knn_all, float tau_all,
-                                                   const int* __restrict__ qk, const float* __restrict__ qtau,
-                                                   int isect, const unsigned long long* __restrict__ kth,
+                                                   const int4* __restrict__ fc, int n1, int self, int knn_all,
+                                                   float tau_all, const int* __restrict__ qk,
+                                                   const float* __restrict__ qtau, int isect,
+                                                   const unsigned long long* __restrict__ kth,
                                                    int64_t* __restrict__ cnt, const int64_t* __restrict__ off,
                                                    unsigned long long* __restrict__ keys) {
+    constexpr unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -181,41 +197,63 @@ __global__ void __launch_bounds__(256) k_cand_pass(DG bg, const float* __restric
         const int x0 = dci(__fsub_rn(qb[0], r), bg.lo0, bg.cell, bg.n0), x1 = dci(__fadd_rn(qb[3], r), bg.lo0, bg.cell, bg.n0);
         const int y0 = dci(__fsub_rn(qb[1], r), bg.lo1, bg.cell, bg.n1), y1 = dci(__fadd_rn(qb[4], r), bg.lo1, bg.cell, bg.n1);
         const int z0 = dci(__fsub_rn(qb[2], r), bg.lo2, bg.cell, bg.n2), z1 = dci(__fadd_rn(qb[5], r), bg.lo2, bg.cell, bg.n2);
+        const int ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+        const int64_t ncell = (int64_t)(x1 - x0 + 1) * ny * nz;
         int64_t pos = WRITE ? off[q] : 0, count = 0;
-        for (int x = x0; x <= x1; ++x)
-            for (int y = y0; y <= y1; ++y)
-                for (int z = z0; z <= z1; ++z) {
-                    const size_t c = ((size_t)x * bg.n1 + y) * bg.n2 + z;
-                    const int64_t b = bg.start[c], e = bg.start[c + 1];
-                    for (int64_t base = b; base < e; base += 32) {
-                        const int64_t k = base + lane;
-                        bool keep = false;
-                        unsigned long long key = 0;
-                        if (k < e) {
-                            const int o = bg.items[k];
-                            const float* ob = box2 + 6 * (size_t)o;
-                            // count an object only in its first cell inside the scan range
-                            const int hx = max(dci(ob[0], bg.lo0, bg.cell, bg.n0), x0);
-                            const int hy = max(dci(ob[1], bg.lo1, bg.cell, bg.n1), y0);
-                            const int hz = max(dci(ob[2], bg.lo2, bg.cell, bg.n2), z0);
-                            if (hx == x && hy == y && hz == z && !(self && o == q)) {
-                                const float gap = d_box_gap(ob, qb);
-                                if (knn) {
-                                    const float md = d_point_dist(xq, xf2 + 3 * (size_t)o);
-                                    key = key_of(md, o);
-                                    keep = gap < T || key <= kk;
-                                } else {
-                                    key = (unsigned)o;
-                                    keep = isect ? strict_overlap(ob, qb) : gap <= tau;
-                                }
-                            }
+        for (int64_t cb = 0; cb < ncell; cb += 32) {
+            const int64_t L = cb + lane;
+            int cx = 0, cy = 0, cz = 0;
+            int64_t b = 0, n = 0;
+            if (L < ncell) {
+                cz = z0 + (int)(L % nz);
+                const int64_t t = L / nz;
+                cy = y0 + (int)(t % ny);
+                cx = x0 + (int)(t / ny);
+                const size_t c = ((size_t)cx * bg.n1 + cy) * bg.n2 + cz;
+                b = bg.start[c];
+                n = bg.start[c + 1] - b;
+            }
+            int64_t inc = n;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t t = __shfl_up_sync(kFull, inc, o);
+                if (lane >= o) inc += t;
+            }
+            const int64_t ex = inc - n;
+            const int64_t tot = __shfl_sync(kFull, inc, 31);
+            for (int64_t j0 = 0; j0 < tot; j0 += 32) {
+                const int64_t j = j0 + lane;
+                int k = 0;  // the last lane whose cell starts at or before item j
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1)
+                    if (__shfl_sync(kFull, ex, k + step) <= j) k += step;
+                const int64_t bk = __shfl_sync(kFull, b, k), ek = __shfl_sync(kFull, ex, k);
+                const int xk = __shfl_sync(kFull, cx, k), yk = __shfl_sync(kFull, cy, k), zk = __shfl_sync(kFull, cz, k);
+                bool keep = false;
+                unsigned long long key = 0;
+                if (j < tot) {
+                    const int o = bg.items[bk + (j - ek)];
+                    const float* ob = box2 + 6 * (size_t)o;
+                    const int4 f = fc[o];
+                    // count an object only in its first cell inside the scan range
+                    if (max(f.x, x0) == xk && max(f.y, y0) == yk && max(f.z, z0) == zk && !(self && o == q)) {
+                        const float gap = d_box_gap(ob, qb);
+                        if (knn) {
+                            const float md = d_point_dist(xq, xf2 + 3 * (size_t)o);
+                            key = key_of(md, o);
+                            keep = gap < T || key <= kk;
+                        } else {
+                            key = (unsigned)o;
+                            keep = isect ? strict_overlap(ob, qb) : gap <= tau;
                         }
-                        const unsigned m = __ballot_sync(0xffffffffu, keep);
-                        if (WRITE && keep) keys[pos + __popc(m & lt)] = key;
-                        pos += __popc(m);
-                        count += __popc(m);
                     }
                 }
+                const unsigned m = __ballot_sync(kFull, keep);
+                if (WRITE && keep) keys[pos + __popc(m & lt)] = key;
+                pos += __popc(m);
+                count += __popc(m);
+            }
+        }
         if (!WRITE && lane == 0) cnt[q] = count;
     }
 }
@@ -307,11 +345,18 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
         k_cand_kth<<<std::max(blocks, 1), kWarps * 32, 0, s>>>(pg, xf1, xf2, (int)n1, K, self, qk, kth, d_over);
         CU(cudaGetLastError());
     }
+    // first cell of every tile-2 object (the dedupe test of the scan)
+    Buf& fcb = ctx->scratch[88];
+    if ((rc = ensure(ctx, fcb, (size_t)std::max<long>(n2, 1) * sizeof(int4)))) return rc;
+    const int4* fc = (const int4*)fcb.p;
+    k_first_cells<<<(int)std::max<long>(1, std::min<long>((n2 + 255) / 256, (long)ctx->num_sms * 8)), 256, 0, s>>>(
+        bg, box2, (int)n2, (int4*)fcb.p);
+    CU(cudaGetLastError());
     int64_t* cnt = (int64_t*)cntb.p;
     int64_t* qoff = (int64_t*)qoff_buf.p;
     const int pblocks = (int)std::min<long>((n1 + 7) / 8, (long)ctx->num_sms * 32);
     CU(cudaMemsetAsync(cnt + n1, 0, 8, s));
-    k_cand_pass<false><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, (int)n1, self, knn, tau, qk,
+    k_cand_pass<false><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, fc, (int)n1, self, knn, tau, qk,
                                                            qtau, isect ? 1 : 0, kth, cnt, nullptr, nullptr);
     CU(cudaGetLastError());
     size_t tb = 0;
@@ -335,7 +380,7 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
     if ((rc = ensure(ctx, pq_buf, Pz * 4))) return rc;
     if ((rc = ensure(ctx, pt_buf, Pz * 4))) return rc;
     if (P > 0) {
-        k_cand_pass<true><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, (int)n1, self, knn, tau, qk, qtau, isect ? 1 : 0, kth,
+        k_cand_pass<true><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, fc, (int)n1, self, knn, tau, qk, qtau, isect ? 1 : 0, kth,
                                                               nullptr, qoff, (unsigned long long*)keys.p);
         CU(cudaGetLastError());
         size_t sb = 0;
