@@ -183,6 +183,7 @@ int tdp_last_stats(const tdp_ctx* ctx, tdp_stats* o) {
     o->exact_f64_items = s.exact_f64_items;
     o->fp32_max_rel_err = s.fp32_max_rel_err;
     o->fetch_bytes = s.fetch_bytes;
+    for (int l = 0; l < tdp::kNumLods; ++l) o->refine_ms_lod[l] = s.refine_ms_lod[l];
     o->lod_graph = s.lod_graph;
     return TDP_OK;
 }
@@ -230,6 +231,15 @@ int tdp_set_refine_config(tdp_ctx* ctx, int cfg) {
     if (cfg < 0 || cfg >= tdp::kTunedConfigs)
         return tdp::fail(ctx, TDP_ERR_ARG, "refine configuration " + std::to_string(cfg) + " out of range");
     ctx->tuned_cfg = cfg;
+    for (int& c : ctx->lod_cfg) c = -1;
+    return TDP_OK;
+}
+
+int tdp_get_refine_config_lod(const tdp_ctx* ctx, int lod, int* cfg) {
+    if (!ctx || !cfg) return TDP_ERR_ARG;
+    const int li = tdp::lod_index(lod);
+    if (li < 0) return TDP_ERR_ARG;
+    *cfg = ctx->lod_cfg[li] >= 0 ? ctx->lod_cfg[li] : ctx->tuned_cfg;
     return TDP_OK;
 }
 

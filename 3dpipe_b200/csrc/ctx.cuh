@@ -7,6 +7,7 @@
 #include <map>
 #include <vector>
 #include "common.cuh"
+#include "storage/dt_format.h"
 #include "../../include/tdp.h"
 
 namespace tdp {
@@ -37,6 +38,7 @@ struct LastStats {
     long exact_f64_items = 0;        // of those, evaluated in FP64
     double fp32_max_rel_err = 0;     // max |FP32 minimum - FP64 distance| / max(distance, 1)
     double fetch_bytes = 0;          // RAW bytes fetched from attached tiles
+    double refine_ms_lod[kNumLods] = {0, 0, 0, 0, 0};  // tuned refine time per LOD index
     long lod_graph = 0;              // tuned LOD loop: 0 direct launches, 1 graph replayed, 2 graph captured
 };
 
@@ -57,6 +59,9 @@ struct tdp_ctx {
     unsigned long long* d_stats = nullptr;    // device-side statistics
     tdp::LastStats stats;
     int tuned_cfg = 0;  // tuned refine kernel configuration (tdp_set_refine_config / tdp_autotune)
+    // per LOD index (20..100): the configuration the autotuner found fastest
+    // at that LOD (-1: tuned_cfg); tdp_set_refine_config clears them
+    int lod_cfg[tdp::kNumLods] = {-1, -1, -1, -1, -1};
     void* hres = nullptr;  // page-locked staging of join results (grow-only)
     size_t hres_cap = 0;
     // CUDA graph of the tuned form's LOD loop (tdp_set_lod_graph): the

@@ -342,7 +342,7 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     // phase 1: one FP32 voxel pair per object pair tightens U
     CU(launch_fetch_items(item1, nullptr, d.P, kNumLods - 1, lz1, lz2, ctx->num_sms, s));
     CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], item1, (int)d.P, res1, ctr, nullptr,
-                           ctx->num_sms, ctx->tuned_cfg, s));
+                           ctx->num_sms, ctx->lod_cfg[kNumLods - 1] >= 0 ? ctx->lod_cfg[kNumLods - 1] : ctx->tuned_cfg, s));
     k_exact_tighten<<<grid(d.P, 256, ctx->num_sms * 8), 256, 0, s>>>(res1, d.P, Ub);
     CU(cudaGetLastError());
     k_exact_vp<false><<<pg, kBlk, 0, s>>>(d, Ub, vt1, vt2, cnt, nullptr, nullptr, nullptr, nullptr);
@@ -385,7 +385,7 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     if (E > 0) {
         CU(launch_fetch_items(items, nullptr, E, kNumLods - 1, lz1, lz2, ctx->num_sms, s));
         CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], items, (int)E, res, ctr, nullptr,
-                               ctx->num_sms, ctx->tuned_cfg, s, nullptr, preset));
+                               ctx->num_sms, ctx->lod_cfg[kNumLods - 1] >= 0 ? ctx->lod_cfg[kNumLods - 1] : ctx->tuned_cfg, s, nullptr, preset));
         const int eg = grid(E, 256, ctx->num_sms * 16);
         k_exact_best<<<eg, 256, 0, s>>>(res, item_pair, E, best32, emax);
         CU(cudaGetLastError());

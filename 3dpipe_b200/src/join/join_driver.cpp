@@ -69,7 +69,7 @@ struct LodLoop {
     float4* res;
     unsigned* counter;
     unsigned long long* dstats;
-    int num_sms, cfg, hlevel, any_knn, any_within, K, knn, recheck;
+    int num_sms, cfg[8], hlevel, any_knn, any_within, K, knn, recheck;
     int64_t V;
     float tau;
     int* rankst;
@@ -99,7 +99,7 @@ int enqueue_lod_loop(tdp_ctx* ctx, const LodLoop& L, cudaStream_t s, bool captur
         CUL(launch_fetch_items(L.items, cnt_items, 0, L.li[k], L.lz1, L.lz2, L.num_sms, s));
         CUL(cudaMemcpyAsync(lod_counts + k, cnt_items, 4, cudaMemcpyDeviceToDevice, s));
         CUL(rec(L.ev[2 * k]));
-        CUL(launch_refine_tuned(L.tri1[k], L.tri2[k], L.items, V, L.res, L.counter, L.dstats, L.num_sms, L.cfg, s,
+        CUL(launch_refine_tuned(L.tri1[k], L.tri2[k], L.items, V, L.res, L.counter, L.dstats, L.num_sms, L.cfg[k], s,
                                 cnt_items));
         CUL(rec(L.ev[2 * k + 1]));
         CUL(launch_apply_results(L.d, L.res, L.item_vp, V, highest, L.hlevel, L.li[k], k, s, cnt_items));
@@ -426,7 +426,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         L.vt1_100 = t1->vtri[4]; L.vt2_100 = t2->vtri[4];
         L.items = items; L.item_vp = item_vp; L.res = res;
         L.counter = ctx->d_counter; L.dstats = ctx->d_stats;
-        L.num_sms = ctx->num_sms; L.cfg = ctx->tuned_cfg; L.hlevel = prm->hausdorff_level;
+        L.num_sms = ctx->num_sms; L.hlevel = prm->hausdorff_level;
+        for (int k = 0; k < L.nl; ++k) L.cfg[k] = ctx->lod_cfg[L.li[k]] >= 0 ? ctx->lod_cfg[L.li[k]] : ctx->tuned_cfg;
         L.any_knn = any_knn; L.any_within = any_within; L.K = prm->knn; L.knn = knn;
         L.V = V; L.tau = within_dist;
         L.rankst = buf<int>(ctx, kRankSt);
@@ -491,6 +492,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
             float ms = 0;
             cudaEventElapsedTime(&ms, ctx->lod_ev[2 * k], ctx->lod_ev[2 * k + 1]);
             refine_ms += ms;
+            st.refine_ms_lod[lod_index(lods[k])] = ms;
         }
         full_total = fe;
         undecided = lods.back() == 100 ? tc[24] : 0;  // d_counter[32]
@@ -575,8 +577,14 @@ int tdp_autotune(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp
     tdp_join_params p = *prm;
     p.form = TDP_FORM_TUNED;
     const int keep = ctx->tuned_cfg;
+    int keep_lod[kNumLods];
+    std::memcpy(keep_lod, ctx->lod_cfg, sizeof(keep_lod));
+    for (int& c : ctx->lod_cfg) c = -1;
     int best_cfg = keep;
     double best_ms = 1e300;
+    double lod_best[kNumLods];
+    int lod_arg[kNumLods];
+    for (int l = 0; l < kNumLods; ++l) { lod_best[l] = 1e300; lod_arg[l] = -1; }
     for (int cfg = 0; cfg < kTunedConfigs; ++cfg) {
         ctx->tuned_cfg = cfg;
         double ms = 0;
@@ -585,6 +593,7 @@ int tdp_autotune(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp
             const int rc = tdp_join(ctx, t1, t2, &p, &r);
             if (rc != TDP_OK) {
                 ctx->tuned_cfg = keep;
+                std::memcpy(ctx->lod_cfg, keep_lod, sizeof(keep_lod));
                 return rc;
             }
             tdp_result_free(r);
@@ -595,8 +604,14 @@ int tdp_autotune(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp
             best_ms = ms;
             best_cfg = cfg;
         }
+        // the fastest configuration at each LOD the join refined
+        for (int l = 0; l < kNumLods; ++l) {
+            const double m = ctx->stats.refine_ms_lod[l];
+            if (m > 0 && m < lod_best[l]) { lod_best[l] = m; lod_arg[l] = cfg; }
+        }
     }
     ctx->tuned_cfg = best_cfg;
+    for (int l = 0; l < kNumLods; ++l) ctx->lod_cfg[l] = lod_arg[l];
     if (best) *best = best_cfg;
     return TDP_OK;
 }

@@ -43,10 +43,13 @@ class Stats(C.Structure):
                 ("filter_voxel_pairs", C.c_double), ("kernel_launches", C.c_long),
                 ("candidates_ms", C.c_double), ("lod_ms", C.c_double), ("host_syncs", C.c_long),
                 ("exact_ms", C.c_double), ("exact_items", C.c_long), ("exact_f64_items", C.c_long),
-                ("fp32_max_rel_err", C.c_double), ("fetch_bytes", C.c_double), ("lod_graph", C.c_long)]
+                ("fp32_max_rel_err", C.c_double), ("fetch_bytes", C.c_double), ("lod_graph", C.c_long),
+                ("refine_ms_lod", C.c_double * 5)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["refine_ms_lod"] = list(self.refine_ms_lod)
+        return d
 
 
 _lib = None
@@ -350,7 +353,7 @@ EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates",
 LOD_GRAPH_OFF, LOD_GRAPH_AUTO, LOD_GRAPH_ALWAYS = 0, 1, 2
 
 EXPORTED += ["tdp_tile_compute_bounds", "tdp_raw_compute_bounds", "tdp_tile_attach", "tdp_host_alloc",
-             "tdp_host_free", "tdp_raw_check"]
+             "tdp_host_free", "tdp_raw_check", "tdp_get_refine_config_lod"]
 
 CTX_POISON = 1  # tdp_ctx_create flag: unfetched records of attached tiles read as NaN
 
@@ -631,8 +634,21 @@ def _autotune(self, tile1, tile2=None, query="within", knn=1, within=1000.0, lod
     return best.value, list(ms)
 
 
+def _refine_configs_by_lod(self) -> dict:
+    """{LOD: configuration} the tuned form uses at each LOD."""
+    L = lib()
+    L.tdp_get_refine_config_lod.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    out = {}
+    for lod in (20, 40, 60, 80, 100):
+        v = C.c_int()
+        self.check(L.tdp_get_refine_config_lod(self._h, lod, C.byref(v)))
+        out[lod] = v.value
+    return out
+
+
 Context.set_refine_config = _set_refine_config
 Context.refine_config = _get_refine_config
+Context.refine_configs_by_lod = _refine_configs_by_lod
 Context.autotune = _autotune
 
 

@@ -456,7 +456,9 @@ def main():
         else:
             best_cfg, cfg_ms = ctx.autotune(T1, T2, query="within", within=TAU)
         cfg_defs = pkg.tdp.refine_configs()
-        log(f"[rank {rank}] autotune: refine ms per configuration {[round(m, 3) for m in cfg_ms]} -> {best_cfg}")
+        cfg_by_lod = ctx.refine_configs_by_lod()
+        log(f"[rank {rank}] autotune: refine ms per configuration {[round(m, 3) for m in cfg_ms]} -> {best_cfg}, "
+            f"per LOD {cfg_by_lod}")
         # the two forms must agree before anything is timed
         qa, ra, _ = ctx.join(T1, T2, query="within", within=TAU, form=pkg.FORM_PLAIN)
         qb, rb, _ = ctx.join(T1, T2, query="within", within=TAU, form=pkg.FORM_TUNED)
@@ -610,7 +612,10 @@ def main():
                        "l2": "L2 flushed between timed steps (256 MiB rewrite on the join stream, outside the step events)",
                        "parallelism": f"{ws} GPU(s), query nuclei sharded by vessel block",
                        "refine_config": {"chunk_a": cfg_defs[best_cfg][0], "ctas_per_sm": cfg_defs[best_cfg][1],
-                                         "autotune_refine_ms": [round(m, 4) for m in cfg_ms]}},
+                                         "autotune_refine_ms": [round(m, 4) for m in cfg_ms],
+                                         "by_lod": {str(k): {"config": v, "chunk_a": cfg_defs[v][0],
+                                                             "ctas_per_sm": cfg_defs[v][1]}
+                                                    for k, v in cfg_by_lod.items()}}},
             "plain": {"value": plain_value, "unit": "tri-pairs/s", "ms_per_step": plain_ms,
                       "tuned_over_plain": value / plain_value if plain_value else None},
             "e2e": {"value": e2e_value, "unit": "tri-pairs/s", "ms_per_step": e2e_step,
@@ -627,7 +632,7 @@ def main():
                          "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
                          "traffic_source": "DRAM read+write bytes per launch, ncu 1-pass capture of this workload "
                                            "(profiles/refine_within400.md)",
-                         "kernel": "refine_lazy_kernel" if best_cfg >= 3 else "refine_tuned_kernel",
+                         "kernel": "refine_lazy_kernel" if cfg_by_lod[100] >= 3 else "refine_tuned_kernel",
                          "peak_source": "measured FP32 FMA probe (tdp_fp32_peak); MEASURED_PEAKS.json has no CUDA-core FP32 figure",
                          "work": f"full evals x {F_TRI:.0f} + culled pairs x {F_CULL:.0f} FLOPs",
                          "tri_pair_equivalent": {

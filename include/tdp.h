@@ -85,6 +85,7 @@ typedef struct {
     long lod_graph;                  /* tuned LOD loop: 0 launched directly,
                                         1 replayed the context's CUDA graph,
                                         2 captured (or updated) it in this call */
+    double refine_ms_lod[5];         /* tuned refine time per LOD 20..100      */
 } tdp_stats;
 int tdp_last_stats(const tdp_ctx *ctx, tdp_stats *out);
 /* measured FP32 FMA throughput of the context's device in TFLOP/s (CUDA cores,
@@ -104,6 +105,11 @@ int tdp_refine_config_count(void);
 int tdp_refine_config_info(int cfg, int *chunk_a, int *ctas_per_sm);
 int tdp_set_refine_config(tdp_ctx *ctx, int cfg);
 int tdp_get_refine_config(const tdp_ctx *ctx, int *cfg);
+/* The configuration the tuned form uses at one LOD (20, 40, 60, 80, 100):
+ * tdp_autotune keeps, besides the fastest configuration over the whole join
+ * (its *best), the fastest one at each LOD, and the LOD loop launches each
+ * LOD's own; tdp_set_refine_config sets one configuration for every LOD. */
+int tdp_get_refine_config_lod(const tdp_ctx *ctx, int lod, int *cfg);
 
 /* ---- CUDA graph of the LOD loop --------------------------------------
  * The tuned form's LOD loop (per LOD: item build, refine, bound update,

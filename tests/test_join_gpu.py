@@ -166,8 +166,10 @@ def test_refine_configs_identical_and_autotune(pkg, ctx, gpu_tiles):
     cfgs = pkg.tdp.refine_configs()
     assert len(cfgs) >= 2 and all(a % 8 == 0 and c >= 1 for a, c in cfgs)
     keep = ctx.refine_config()
+    queries = (dict(query="within", within=150.0), dict(query="nn", knn=3))
+    first = []
     try:
-        for args in (dict(query="within", within=150.0), dict(query="nn", knn=3)):
+        for args in queries:
             outs = []
             for c in range(len(cfgs)):
                 ctx.set_refine_config(c)
@@ -175,9 +177,18 @@ def test_refine_configs_identical_and_autotune(pkg, ctx, gpu_tiles):
             for o in outs[1:]:
                 for a, b in zip(outs[0], o):
                     np.testing.assert_array_equal(a, b)
+            first.append(outs[0])
         best, ms = ctx.autotune(T1, T2, query="within", within=150.0)
         assert 0 <= best < len(cfgs) and ctx.refine_config() == best
         assert len(ms) == len(cfgs) and all(m > 0 for m in ms)
+        # each LOD runs the configuration fastest at that LOD; results unchanged
+        by_lod = ctx.refine_configs_by_lod()
+        assert sorted(by_lod) == [20, 40, 60, 80, 100] and all(0 <= c < len(cfgs) for c in by_lod.values())
+        for args, want in zip(queries, first):
+            for a, b in zip(ctx.join(T1, T2, form=pkg.FORM_TUNED, **args), want):
+                np.testing.assert_array_equal(a, b)
+        ctx.set_refine_config(0)
+        assert set(ctx.refine_configs_by_lod().values()) == {0}
         with pytest.raises(pkg.TdpError):
             ctx.set_refine_config(len(cfgs))
     finally:
