@@ -5,7 +5,8 @@
 // the reference octree).  Tile 1 is then processed in contiguous chunks of
 // query objects; for each chunk a RAW sub-tile of tile 2 is assembled from
 // exactly the tile-2 objects that are candidates of the chunk, in increasing
-// id, and both are uploaded, joined and freed.  Because the sub-tile holds
+// id, and both are attached (their triangles fetched by the join as it
+// refines them), joined and freed.  Because the sub-tile holds
 // every candidate of the chunk's queries and keeps their id order, each
 // query's candidate list (set and order), and with it every filter decision,
 // refine result and reported pair, is the one of the whole join; the result
@@ -200,18 +201,28 @@ extern "C" int tdp_join_chunked(tdp_ctx* ctx, const void* raw1, size_t len1, con
     // one chunk on the device; a chunk that exceeds the budget is split in two
     std::function<int(Chunk&, int)> run = [&](Chunk& c, int slot) -> int {
         ++inf.chunks;
-        inf.h2d_bytes += (double)(c.len1 + c.len2);
         if (c.sub.empty()) return TDP_OK;  // no candidates: nothing to report
         tdp_tile *t1 = nullptr, *t2 = nullptr;
         tdp_result* r = nullptr;
-        int rc = tdp_tile_upload(ctx, c.raw1, c.len1, 0, &t1);
-        if (rc == TDP_OK) rc = tdp_tile_upload(ctx, c.raw2, c.len2, 0, &t2);
+        // a page-locked chunk buffer is attached: the join fetches only the
+        // voxels it refines (and the buffer is not rewritten before the
+        // chunk's tiles are freed); otherwise the chunk is uploaded whole
+        auto load = [&](const uint8_t* raw, size_t len, tdp_tile** t) {
+            return bufs[slot].pinned ? tdp_tile_attach(ctx, raw, len, 0, t) : tdp_tile_upload(ctx, raw, len, 0, t);
+        };
+        int rc = load(c.raw1, c.len1, &t1);
+        if (rc == TDP_OK) rc = load(c.raw2, c.len2, &t2);
         if (rc == TDP_OK) rc = tdp_join(ctx, t1, t2, prm, &r);
+        if (rc == TDP_OK) {
+            tdp_tile_info i1{}, i2{};
+            tdp_tile_get_info(t1, &i1);
+            tdp_tile_get_info(t2, &i2);
+            inf.h2d_bytes += (double)(i1.h2d_bytes + i2.h2d_bytes) + ctx->stats.fetch_bytes;
+        }
         if (t1) tdp_tile_free(ctx, t1);
         if (t2) tdp_tile_free(ctx, t2);
         if (rc == TDP_ERR_NOMEM && c.q1 - c.q0 > 1) {
             --inf.chunks;
-            inf.h2d_bytes -= (double)(c.len1 + c.len2);
             ++inf.splits;
             // the halves reuse this chunk's buffer one after the other
             const long q0 = c.q0, mid = c.q0 + (c.q1 - c.q0) / 2, q1 = c.q1;

@@ -294,7 +294,10 @@ int tdp_autotune(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, con
 typedef struct {
     long chunks;
     long splits;               /* chunks split in two after running out of memory        */
-    double h2d_bytes;          /* RAW bytes uploaded (chunks and sub-tiles)               */
+    double h2d_bytes;          /* bytes copied host -> device: chunk and sub-tile
+                                  metadata plus the triangles the joins fetched (chunks
+                                  are assembled in page-locked buffers and attached;
+                                  whole uploads when page-locking is unavailable)     */
     double tri_pairs;          /* refined triangle pairs, all chunks                      */
     double join_ms;            /* device time of the chunk joins                          */
     double device_peak_bytes;  /* the context's device-memory high-water mark             */
