@@ -325,7 +325,7 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
         if (t->d_boxes && t->boxes_n == t->n_obj) continue;
         dfree(ctx, t->d_boxes);
         t->d_boxes = nullptr;
-        if (dmalloc(ctx, (void**)&t->d_boxes, (size_t)std::max<long>(t->n_obj, 1) * 9 * 4) != cudaSuccess)
+        if (block_alloc(ctx, (void**)&t->d_boxes, (size_t)std::max<long>(t->n_obj, 1) * 9 * 4) != cudaSuccess)
             return fail(ctx, TDP_ERR_NOMEM, "cannot allocate the candidate boxes");
         CU(cudaMemcpyAsync(t->d_boxes, t->host.obj_box.data(), t->n_obj * 24, cudaMemcpyHostToDevice, s));
         CU(cudaMemcpyAsync(t->d_boxes + 6 * t->n_obj, t->host.obj_xf.data(), t->n_obj * 12, cudaMemcpyHostToDevice,

@@ -88,11 +88,11 @@ cudaError_t dmalloc(tdp_ctx* ctx, void** p, size_t bytes);
 void dfree(tdp_ctx* ctx, void* p);
 // grow-only scratch buffer; returns TDP_OK or an error status (recorded in ctx)
 int ensure(tdp_ctx* ctx, Buf& b, size_t bytes);
-// large blocks for tile triangle arrays: block_alloc reuses an idle cached
+// large blocks for tile arrays: block_alloc reuses an idle cached
 // block of the size (or up to 25 % larger); block_release caches blocks of
 // at least kCachedBlockMin bytes (the caller has synchronised the context's
 // stream, so the block is idle) and frees smaller ones
-constexpr size_t kCachedBlockMin = (size_t)16 << 20;
+constexpr size_t kCachedBlockMin = (size_t)1 << 20;
 cudaError_t block_alloc(tdp_ctx* ctx, void** p, size_t bytes);
 void block_release(tdp_ctx* ctx, void* p);
 void cache_trim(tdp_ctx* ctx);

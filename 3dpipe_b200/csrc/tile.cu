@@ -70,20 +70,22 @@ static void host_parallel(long n, Fn fn) {
     for (auto& th : pool) th.join();
 }
 
+// Device arrays go back to the context's block cache: every caller has
+// synchronised the context's stream, or queued the arrays' pending work on it.
 void tile_release(tdp_ctx* ctx, tdp_tile* t) {
     if (!t) return;
-    dfree(ctx, t->vox);
-    dfree(ctx, t->obj_vox);
-    dfree(ctx, t->obj_hd);
-    dfree(ctx, t->obj_phd);
+    block_release(ctx, t->vox);
+    block_release(ctx, t->obj_vox);
+    block_release(ctx, t->obj_hd);
+    block_release(ctx, t->obj_phd);
     for (int l = 0; l < kNumLods; ++l) {
         block_release(ctx, t->tri[l]);  // kept for the next tile of the size
-        dfree(ctx, t->vtri[l]);
+        block_release(ctx, t->vtri[l]);
     }
-    dfree(ctx, (void*)t->lazy_data_off);
-    dfree(ctx, t->lazy_state);
-    dfree(ctx, t->lazy_bytes);
-    dfree(ctx, t->d_boxes);
+    block_release(ctx, (void*)t->lazy_data_off);
+    block_release(ctx, t->lazy_state);
+    block_release(ctx, t->lazy_bytes);
+    block_release(ctx, t->d_boxes);
     dfree(ctx, t->box_grid.start);
     dfree(ctx, t->box_grid.items);
     dfree(ctx, t->point_grid.start);
@@ -186,7 +188,7 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
     }
     const auto ta = std::chrono::steady_clock::now();
     auto alloc = [&](void** p, size_t bytes) -> int {
-        if (dmalloc(ctx, p, bytes) != cudaSuccess)
+        if (block_alloc(ctx, p, bytes) != cudaSuccess)
             return fail(ctx, TDP_ERR_NOMEM, "tile upload: cannot allocate " + std::to_string(bytes) + " bytes" +
                                                 (ctx->budget ? " within the context budget" : ""));
         T->device_bytes += bytes;
@@ -211,6 +213,7 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
         TRY(alloc((void**)&T->vtri[l], (size_t)(H.n_vox + 1) * sizeof(uint32_t)));
     }
     T->alloc_ms = ms_since(ta);
+    const auto tm = std::chrono::steady_clock::now();
     {
         // the metadata go up through the context's page-locked staging buffer
         // (assembled by host threads), so the copies run at full PCIe rate
@@ -266,6 +269,7 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
         T->h2d_bytes += v4_bytes + ov_bytes + 2 * hd_bytes + kNumLods * vt_bytes;
         CTRY(cudaStreamSynchronize(s));
     }
+    T->meta_ms = ms_since(tm);
     if (attach) {
         TRY(alloc((void**)&T->lazy_data_off, (size_t)std::max<long>(H.n_obj, 1) * sizeof(uint64_t)));
         TRY(alloc((void**)&T->lazy_state, (size_t)kNumLods * std::max<long>(H.n_vox, 1) * sizeof(unsigned)));
@@ -382,6 +386,7 @@ int tdp_tile_get_info(const tdp_tile* t, tdp_tile_info* o) {
     o->parse_ms = t->parse_ms;
     o->alloc_ms = t->alloc_ms;
     o->load_ms = t->load_ms;
+    o->meta_ms = t->meta_ms;
     return TDP_OK;
 }
 

@@ -48,7 +48,7 @@ struct tdp_tile {
     tdp::HostVec<uint32_t> h_vtri[tdp::kNumLods];  // host copy of vtri
     size_t device_bytes = 0;
     size_t h2d_bytes = 0;  // bytes copied host -> device by the upload or attach itself
-    double parse_ms = 0, alloc_ms = 0, load_ms = 0;  // host time of the upload or attach
+    double parse_ms = 0, alloc_ms = 0, meta_ms = 0, load_ms = 0;  // host time of the upload or attach
     int device = 0;
     // attached tiles (tdp_tile_attach): the triangles stay in page-locked host
     // memory and joins fetch the voxels they refine (csrc/fetch_kernels.cu)

@@ -196,7 +196,8 @@ class Context:
 class TileInfo(C.Structure):
     _fields_ = [("n_objects", C.c_long), ("n_voxels", C.c_long), ("n_tris", C.c_long * 5),
                 ("device_bytes", C.c_size_t), ("h2d_bytes", C.c_size_t), ("attached", C.c_int),
-                ("parse_ms", C.c_double), ("alloc_ms", C.c_double), ("load_ms", C.c_double)]
+                ("parse_ms", C.c_double), ("alloc_ms", C.c_double), ("load_ms", C.c_double),
+                ("meta_ms", C.c_double)]
 
 
 class JoinParams(C.Structure):
@@ -253,7 +254,7 @@ class Tile:
         lib().tdp_tile_get_info(self._h, C.byref(i))
         return {"n_objects": i.n_objects, "n_voxels": i.n_voxels, "n_tris": list(i.n_tris),
                 "device_bytes": i.device_bytes, "h2d_bytes": i.h2d_bytes, "attached": bool(i.attached),
-                "parse_ms": i.parse_ms, "alloc_ms": i.alloc_ms, "load_ms": i.load_ms}
+                "parse_ms": i.parse_ms, "alloc_ms": i.alloc_ms, "load_ms": i.load_ms, "meta_ms": i.meta_ms}
 
     def free(self):
         if getattr(self, "_h", None):

@@ -556,7 +556,8 @@ def main():
             h3 = time.perf_counter()
             return (e0.elapsed_time(e1), h2d_b, q.nbytes + r.nbytes + d.nbytes,
                     {"tiles_ms": 1e3 * (h1 - h0), "parse_ms": i1["parse_ms"] + i2["parse_ms"],
-                     "alloc_ms": i1["alloc_ms"] + i2["alloc_ms"], "join_ms": 1e3 * (h2 - h1),
+                     "alloc_ms": i1["alloc_ms"] + i2["alloc_ms"], "meta_ms": i1["meta_ms"] + i2["meta_ms"],
+                     "load_ms": i1["load_ms"] + i2["load_ms"], "join_ms": 1e3 * (h2 - h1),
                      "fetch_bytes": fetched, "release_ms": 1e3 * (h3 - h2)})
 
         e2e_ms, h2d, d2h, e2e_parts = [], 0, 0, None

@@ -148,6 +148,8 @@ typedef struct {
     double parse_ms;       /* host time of the upload / attach: parsing the bytes, */
     double alloc_ms;       /* allocating the device arrays,                       */
     double load_ms;        /* and in total                                        */
+    double meta_ms;        /* of which staging and copying the voxel and object
+                              metadata to the device                              */
 } tdp_tile_info;
 int tdp_tile_upload(tdp_ctx *ctx, const void *raw_dt, size_t len, long max_objects, tdp_tile **out);
 /* Attach a RAW tile that stays in page-locked host memory (cudaHostRegister or
