@@ -63,7 +63,7 @@ cudaError_t launch_unpack(const uint8_t* raw, const UnpackSeg* segs, int nseg, f
 // fn(b, e) over [0, n) in a few host threads (one for small n)
 template <typename Fn>
 static void host_parallel(long n, Fn fn) {
-    const long nt = std::max(1L, std::min<long>((long)std::thread::hardware_concurrency(), n / 65536));
+    const long nt = std::max(1L, std::min<long>((long)std::thread::hardware_concurrency(), n / 4096));
     if (nt == 1) { fn(0L, n); return; }
     std::vector<std::thread> pool;
     for (long k = 0; k < nt; ++k) pool.emplace_back([&, k] { fn(n * k / nt, n * (k + 1) / nt); });
