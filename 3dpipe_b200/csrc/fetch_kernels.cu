@@ -14,7 +14,9 @@
 // (the word after the last float still lies inside the object's record: the
 // voxel table and the transform follow the data block).  A warp moves 32
 // triangles at a time: coalesced word reads from host memory into shared
-// memory, then one 48-byte record per lane.
+// memory, then one 48-byte record per lane.  Serving arenas use the same
+// fetch with absolute addresses: each object's data block lives in its own
+// request's page-locked buffer.
 #include "fetch_kernels.cuh"
 
 #include <algorithm>
@@ -44,7 +46,7 @@ __device__ inline long last_le(const uint32_t* a, long n, uint32_t x) {
 __device__ void fetch_voxel(const LazyTile& L, int lod, long v, uint32_t off, uint32_t n, uint32_t* stage) {
     const int lane = threadIdx.x & 31;
     unsigned prev = 1;
-    if (lane == 0) prev = atomicCAS(L.state + (size_t)lod * L.n_vox + v, 0u, 1u);
+    if (lane == 0) prev = atomicCAS(L.state + (size_t)lod * L.stride + v, 0u, 1u);
     prev = __shfl_sync(0xffffffffu, prev, 0);
     if (prev != 0u) return;
     const long o = last_le(L.obj_vox, L.n_obj + 1, (uint32_t)v);
@@ -83,8 +85,8 @@ __global__ void __launch_bounds__(kFetchWarps * 32) k_fetch_items(const RefineIt
     const long warps = ((long)gridDim.x * blockDim.x) >> 5;
     for (long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
         const RefineItem it = items[i];
-        if (A.raw && it.a_cnt) fetch_voxel(A, lod, last_le(A.vtri[lod], A.n_vox + 1, it.a_off), it.a_off, it.a_cnt, st);
-        if (B.raw && it.b_cnt) fetch_voxel(B, lod, last_le(B.vtri[lod], B.n_vox + 1, it.b_off), it.b_off, it.b_cnt, st);
+        if (A.on && it.a_cnt) fetch_voxel(A, lod, last_le(A.vtri[lod], A.n_vox + 1, it.a_off), it.a_off, it.a_cnt, st);
+        if (B.on && it.b_cnt) fetch_voxel(B, lod, last_le(B.vtri[lod], B.n_vox + 1, it.b_off), it.b_off, it.b_cnt, st);
     }
 }
 
@@ -104,7 +106,8 @@ __global__ void __launch_bounds__(kFetchWarps * 32) k_fetch_all(LazyTile L) {
 
 LazyTile lazy_view(const tdp_tile* t) {
     LazyTile L;
-    if (!t || !t->lazy_raw) return L;
+    if (!t || !t->lazy_on) return L;
+    L.on = true;
     L.raw = t->lazy_raw;
     L.data_off = t->lazy_data_off;
     L.obj_vox = t->obj_vox;
@@ -113,6 +116,7 @@ LazyTile lazy_view(const tdp_tile* t) {
         L.tri[l] = t->tri[l];
     }
     L.state = t->lazy_state;
+    L.stride = t->lazy_stride;
     L.bytes = t->lazy_bytes;
     L.n_vox = t->n_vox;
     L.n_obj = t->n_obj;
@@ -121,7 +125,7 @@ LazyTile lazy_view(const tdp_tile* t) {
 
 cudaError_t launch_fetch_items(const RefineItem* items, const unsigned* n_dev, long n_host, int lod,
                                const LazyTile& a, const LazyTile& b, int num_sms, cudaStream_t s) {
-    if (!a.raw && !b.raw) return cudaSuccess;
+    if (!a.on && !b.on) return cudaSuccess;
     if (!n_dev && n_host <= 0) return cudaSuccess;
     const long blocks_needed = n_dev ? (long)num_sms * 8 : (n_host + kFetchWarps - 1) / kFetchWarps;
     const int blocks = (int)std::max(1L, std::min<long>(blocks_needed, (long)num_sms * 8));
@@ -130,7 +134,7 @@ cudaError_t launch_fetch_items(const RefineItem* items, const unsigned* n_dev, l
 }
 
 cudaError_t launch_fetch_all(const LazyTile& t, int num_sms, cudaStream_t s) {
-    if (!t.raw || t.n_vox == 0) return cudaSuccess;
+    if (!t.on || t.n_vox == 0) return cudaSuccess;
     k_fetch_all<<<num_sms * 8, kFetchWarps * 32, 0, s>>>(t);
     return cudaGetLastError();
 }

@@ -22,17 +22,20 @@ struct tdp_tile;
 namespace tdp {
 
 struct LazyTile {
-    const uint8_t* raw = nullptr;           // device view of the page-locked RAW bytes (nullptr: resident tile)
-    const uint64_t* data_off = nullptr;     // [n_obj] byte offset of each object's data block
+    bool on = false;                        // false: a resident tile, nothing to fetch
+    const uint8_t* raw = nullptr;           // device view of the page-locked RAW bytes (or nullptr
+                                            // when data_off holds absolute device-view addresses)
+    const uint64_t* data_off = nullptr;     // [n_obj] where each object's data block starts
     const uint32_t* obj_vox = nullptr;      // [n_obj + 1]
     const uint32_t* vtri[kNumLods] = {};    // [n_vox + 1] first triangle of each voxel
     float4* tri[kNumLods] = {};             // device records
-    unsigned* state = nullptr;              // [kNumLods * n_vox] 0 = not fetched, 1 = fetched
+    unsigned* state = nullptr;              // [kNumLods * stride] 0 = not fetched, 1 = fetched (or resident)
+    long stride = 0;                        // state entries per LOD (>= n_vox)
     unsigned long long* bytes = nullptr;    // RAW bytes fetched (counter)
     long n_vox = 0, n_obj = 0;
 };
 
-// the device view of a tile (raw == nullptr for a resident tile)
+// the device view of a tile (on == false for a resident tile)
 LazyTile lazy_view(const tdp_tile* t);
 
 // fetch, for every item of `items` (n_dev: count in device memory, else

@@ -16,6 +16,8 @@ struct ArenaMeta {
     const float* obj_hd;        // [n * kNumLods]
     const float* obj_phd;       // [n * kNumLods]
     const uint32_t* vtri[kNumLods];  // [nv + 1] local first triangle of each voxel
+    const uint64_t* data_abs;   // [n] device-view address of each object's data block (fetched requests)
+    unsigned fetched;           // 1: the join fetches the request's triangles from its own buffer
 };
 
 struct ArenaDst {
@@ -24,6 +26,9 @@ struct ArenaDst {
     float* obj_hd;
     float* obj_phd;
     uint32_t* vtri[kNumLods];
+    uint64_t* data_off;  // the arena's per-object data-block addresses
+    unsigned* state;     // the arena's fetch state, kNumLods planes of `stride` voxels
+    long stride;
 };
 
 // Write n objects / nv voxels of `m` at object o0, voxel v0, triangle t0[l].

@@ -283,6 +283,8 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
         CTRY(cudaStreamSynchronize(s));
         T->h2d_bytes += H.n_obj * sizeof(uint64_t);
         T->lazy_raw = dev_view;
+        T->lazy_on = true;
+        T->lazy_stride = H.n_vox;
         T->load_ms = ms_since(t0);
         *out = T;
         return TDP_OK;

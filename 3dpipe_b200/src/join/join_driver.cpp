@@ -316,8 +316,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     // attached tiles: voxels fetched on demand, bytes counted per join
     LazyTile lz1 = lazy_view(t1), lz2 = lazy_view(t2);
     unsigned long long* fetch_ctr = ctx->d_stats + 8;
-    if (lz1.raw) lz1.bytes = fetch_ctr;
-    if (lz2.raw) lz2.bytes = fetch_ctr;
+    if (lz1.on) lz1.bytes = fetch_ctr;
+    if (lz2.on) lz2.bytes = fetch_ctr;
     CU(cudaMemsetAsync(fetch_ctr, 0, 8, s));
     d.stat_vp = ctx->d_stats + 1;
     long launches = 0;

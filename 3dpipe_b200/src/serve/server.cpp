@@ -65,6 +65,9 @@ struct Request {
     TileHost host;     // parsed at submit
     uint64_t base = 0; // byte offset of the first object's record in raw
     uint64_t span = 0; // bytes from base to the end of the last object's data
+    const uint8_t* dev = nullptr;  // device view of raw when it is page-locked
+    bool fetched = false;          // the join fetches its triangles from raw (else staged whole)
+    double staged_bytes = 0;       // bytes its staging copies moved
     int knn = 0;       // > 0: kNN; 0: within
     float within = 0.f;
     Clock::time_point t_submit, t_start, t_done;
@@ -90,7 +93,7 @@ struct Arena {
 
 // Byte layout of one request's staged metadata (every section 16-byte aligned).
 struct MetaLayout {
-    size_t vox = 0, obj_vox = 0, obj_hd = 0, obj_phd = 0, vtri[kNumLods] = {}, segs = 0, bytes = 0;
+    size_t vox = 0, obj_vox = 0, obj_hd = 0, obj_phd = 0, vtri[kNumLods] = {}, data_abs = 0, segs = 0, bytes = 0;
     long nseg = 0;
 };
 
@@ -104,6 +107,7 @@ MetaLayout meta_layout(long n, long nv, long nseg) {
     L.obj_hd = o; o = up16(o + (size_t)n * kNumLods * 4);
     L.obj_phd = o; o = up16(o + (size_t)n * kNumLods * 4);
     for (int l = 0; l < kNumLods; ++l) { L.vtri[l] = o; o = up16(o + (size_t)(nv + 1) * 4); }
+    L.data_abs = o; o = up16(o + (size_t)n * 8);
     L.segs = o; o = up16(o + (size_t)nseg * sizeof(UnpackSeg));
     L.bytes = o;
     L.nseg = nseg;
@@ -133,7 +137,7 @@ struct tdp_server {
     std::unordered_map<uint64_t, std::unique_ptr<Request>> table;
     uint64_t next_id = 1;
     long batches = 0, completed = 0, failed = 0;
-    double busy_ms = 0, upload_ms = 0, upload_bytes = 0;
+    double busy_ms = 0, upload_ms = 0, upload_bytes = 0, fetch_bytes = 0;
     bool stop = false;
     std::thread admitter, executor;
 };
@@ -169,8 +173,9 @@ int start_copy(tdp_server* S, Request* r, int j) {
     const TileHost& h = r->host;
     const long n = h.n_obj, nv = h.n_vox;
     long nseg = 0;
-    for (int l = 0; l < kNumLods; ++l)
-        for (long v = 0; v < nv; ++v) nseg += h.vox_cnt[l][v] != 0;
+    if (!r->fetched)
+        for (int l = 0; l < kNumLods; ++l)
+            for (long v = 0; v < nv; ++v) nseg += h.vox_cnt[l][v] != 0;
     const MetaLayout L = meta_layout(n, nv, nseg);
     if (L.bytes > S->meta_cap) return TDP_ERR_ARG;
     uint8_t* m = S->hmeta[j];
@@ -184,6 +189,8 @@ int start_copy(tdp_server* S, Request* r, int j) {
     std::memcpy(m + L.obj_vox, h.obj_vox_off.data(), (size_t)(n + 1) * 4);
     std::memcpy(m + L.obj_hd, h.obj_hd.data(), (size_t)n * kNumLods * 4);
     std::memcpy(m + L.obj_phd, h.obj_phd.data(), (size_t)n * kNumLods * 4);
+    uint64_t* abs = (uint64_t*)(m + L.data_abs);
+    for (long o = 0; o < n; ++o) abs[o] = r->fetched ? (uint64_t)(uintptr_t)(r->dev + h.obj_data_off[o]) : 0;
     UnpackSeg* seg = (UnpackSeg*)(m + L.segs);
     long k = 0;
     for (int l = 0; l < kNumLods; ++l) {
@@ -192,15 +199,19 @@ int start_copy(tdp_server* S, Request* r, int j) {
         for (long v = 0; v < nv; ++v) {
             const uint32_t c = h.vox_cnt[l][v];
             vt[v + 1] = vt[v] + c;
-            if (!c) continue;
+            if (!c || r->fetched) continue;
             const uint64_t src = h.vox_byte_off[l][v] - r->base;
             if ((src & 3u) || src + (uint64_t)c * 44 > r->span) return TDP_ERR_FORMAT;
             seg[k++] = UnpackSeg{src, vt[v], c | ((uint32_t)l << 24)};  // dst local to the request
         }
     }
     S->meta[j] = L;
+    // a page-locked request moves only its metadata now; its triangles are
+    // fetched by the join, voxel by voxel, from the caller's buffer
+    r->staged_bytes = (double)L.bytes + (r->fetched ? 0.0 : (double)r->span);
     if (cudaMemcpyAsync(S->dmeta[j], m, L.bytes, cudaMemcpyHostToDevice, S->copy) != cudaSuccess ||
-        cudaMemcpyAsync(S->stage[j], r->raw + r->base, r->span, cudaMemcpyHostToDevice, S->copy) != cudaSuccess ||
+        (!r->fetched &&
+         cudaMemcpyAsync(S->stage[j], r->raw + r->base, r->span, cudaMemcpyHostToDevice, S->copy) != cudaSuccess) ||
         cudaEventRecord(S->staged[j], S->copy) != cudaSuccess)
         return TDP_ERR_CUDA;
     return TDP_OK;
@@ -218,8 +229,9 @@ int append(tdp_server* S, Arena& a, Request& r, int j) {
     const MetaLayout& L = S->meta[j];
     const uint8_t* m = S->dmeta[j];
     ArenaMeta am{(const float4*)(m + L.vox), (const uint32_t*)(m + L.obj_vox), (const float*)(m + L.obj_hd),
-                 (const float*)(m + L.obj_phd), {}};
-    ArenaDst ad{a.tile.vox, a.tile.obj_vox, a.tile.obj_hd, a.tile.obj_phd, {}};
+                 (const float*)(m + L.obj_phd), {}, (const uint64_t*)(m + L.data_abs), r.fetched ? 1u : 0u};
+    ArenaDst ad{a.tile.vox, a.tile.obj_vox, a.tile.obj_hd, a.tile.obj_phd, {},
+                a.tile.lazy_data_off, a.tile.lazy_state, a.tile.lazy_stride};
     float4* tri_at[kNumLods];
     for (int l = 0; l < kNumLods; ++l) {
         am.vtri[l] = (const uint32_t*)(m + L.vtri[l]);
@@ -227,7 +239,7 @@ int append(tdp_server* S, Arena& a, Request& r, int j) {
         tri_at[l] = a.tile.tri[l] + 3 * (size_t)t0[l];  // segments carry request-local destinations
     }
     cudaError_t e = launch_arena_commit(am, ad, n, nv, o0, v0, t0, S->ctx->num_sms, a.up);
-    if (e == cudaSuccess)
+    if (e == cudaSuccess && L.nseg > 0)
         e = launch_unpack(S->stage[j], (const UnpackSeg*)(m + L.segs), (int)L.nseg, tri_at, S->ctx->num_sms, a.up);
     if (e == cudaSuccess) e = cudaEventRecord(a.ready, a.up);
     // the staging area is refilled two requests later: finish with it now
@@ -244,6 +256,30 @@ int append(tdp_server* S, Arena& a, Request& r, int j) {
     a.tile.n_vox = H.n_vox = v0 + nv;
     a.tile.boxes_n = 0;  // the device copy of the boxes is stale
     return TDP_OK;
+}
+
+// A request can be fetched from by the join when its bytes are page-locked
+// from the first to the last and every object keeps its voxels' triangles LOD
+// by LOD and voxel by voxel (the writer's layout, src/storage/tile_IO.cpp:79-172).
+bool fetchable(const uint8_t* raw, size_t len, const TileHost& h, const uint8_t** dev) {
+    cudaPointerAttributes a0{}, a1{};
+    void* dp = nullptr;
+    if (len == 0 || cudaPointerGetAttributes(&a0, raw) != cudaSuccess || a0.type != cudaMemoryTypeHost ||
+        cudaPointerGetAttributes(&a1, raw + len - 1) != cudaSuccess || a1.type != cudaMemoryTypeHost ||
+        cudaHostGetDevicePointer(&dp, (void*)raw, 0) != cudaSuccess || !dp) {
+        cudaGetLastError();
+        return false;
+    }
+    for (long o = 0; o < h.n_obj; ++o) {
+        uint64_t expect = h.obj_data_off[o];
+        for (int l = 0; l < kNumLods; ++l)
+            for (uint32_t v = h.obj_vox_off[o]; v < h.obj_vox_off[o + 1]; ++v) {
+                if (h.vox_byte_off[l][v] != expect) return false;
+                expect += 44ull * h.vox_cnt[l][v];
+            }
+    }
+    *dev = (const uint8_t*)dp;
+    return true;
 }
 
 void finish(tdp_server* S, Request* r, int status) {
@@ -329,7 +365,7 @@ void admitter_loop(tdp_server* S) {
             const double up_ms = ms_between(t_cur, Clock::now());
             lk.lock();
             S->upload_ms += up_ms;
-            S->upload_bytes += (double)r->span;
+            S->upload_bytes += r->staged_bytes;
             a->appending = false;
             if (rc == TDP_OK) a->reqs.push_back(r);
             else finish(S, r, rc);
@@ -388,6 +424,7 @@ void executor_loop(tdp_server* S) {
         tdp_result* res = nullptr;
         int rc = cudaStreamWaitEvent(ctx->stream, a->ready, 0) == cudaSuccess ? TDP_OK : TDP_ERR_CUDA;
         if (rc == TDP_OK) rc = tdp_join(ctx, &a->tile, S->t2, &jp, &res);
+        const double fetched = rc == TDP_OK ? ctx->stats.fetch_bytes : 0.0;
         // split the rows (sorted by query object) by request
         if (rc == TDP_OK) {
             for (Request* r : reqs) {
@@ -406,6 +443,7 @@ void executor_loop(tdp_server* S) {
         const double busy = ms_between(t_start, Clock::now());
         lk.lock();
         S->busy_ms += busy;
+        S->fetch_bytes += fetched;
         for (Request* r : reqs) finish(S, r, rc);
         reset_arena(*a);
         a->state = ArenaState::kFree;
@@ -455,6 +493,14 @@ int tdp_server_create(tdp_ctx* ctx, const tdp_tile* t2, const tdp_server_params*
         for (int l = 0; ok && l < kNumLods; ++l)
             ok = alloc((void**)&T.tri[l], (size_t)p->arena_tris * 3 * sizeof(float4)) &&
                  alloc((void**)&T.vtri[l], (size_t)(p->arena_voxels + 1) * 4);
+        // fetch state of the arena: requests in page-locked memory are fetched
+        // by the join, the others are unpacked from staging (state 1)
+        ok = ok && alloc((void**)&T.lazy_data_off, (size_t)p->arena_objects * 8) &&
+             alloc((void**)&T.lazy_state, (size_t)kNumLods * p->arena_voxels * sizeof(unsigned)) &&
+             alloc((void**)&T.lazy_bytes, sizeof(unsigned long long));
+        T.lazy_on = true;
+        T.lazy_raw = nullptr;  // lazy_data_off holds absolute addresses
+        T.lazy_stride = p->arena_voxels;
         if (!ok || cudaStreamCreateWithFlags(&a.up, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&a.ready, cudaEventDisableTiming) != cudaSuccess) {
             tdp_server_destroy(S.release());
@@ -513,6 +559,7 @@ int tdp_server_submit(tdp_server* S, const void* raw_dt, size_t len, int query, 
         if ((long)h.n_tris[l] > S->p.arena_tris) return TDP_ERR_ARG;
     r->knn = query == TDP_QUERY_NN ? knn : 0;
     r->within = query == TDP_QUERY_NN ? 0.f : within;
+    r->fetched = fetchable(r->raw, len, h, &r->dev);
     std::lock_guard<std::mutex> lk(S->mu);
     if (S->stop) return TDP_ERR_STATE;
     r->id = S->next_id++;
@@ -555,6 +602,7 @@ int tdp_server_get_stats(const tdp_server* S, tdp_server_stats* o) {
     o->busy_ms = S->busy_ms;
     o->upload_ms = S->upload_ms;
     o->upload_bytes = S->upload_bytes;
+    o->fetch_bytes = S->fetch_bytes;
     return TDP_OK;
 }
 
@@ -583,6 +631,7 @@ int tdp_server_destroy(tdp_server* S) {
         tdp_tile& T = a.tile;
         dfree(ctx, T.vox); dfree(ctx, T.obj_vox); dfree(ctx, T.obj_hd); dfree(ctx, T.obj_phd);
         dfree(ctx, T.d_boxes);
+        dfree(ctx, (void*)T.lazy_data_off); dfree(ctx, T.lazy_state); dfree(ctx, T.lazy_bytes);
         for (int l = 0; l < kNumLods; ++l) { dfree(ctx, T.tri[l]); dfree(ctx, T.vtri[l]); }
         if (a.ready) cudaEventDestroy(a.ready);
         if (a.up) cudaStreamDestroy(a.up);

@@ -52,8 +52,11 @@ struct tdp_tile {
     int device = 0;
     // attached tiles (tdp_tile_attach): the triangles stay in page-locked host
     // memory and joins fetch the voxels they refine (csrc/fetch_kernels.cu)
-    const uint8_t* lazy_raw = nullptr;          // device view of the host bytes; nullptr: resident tile
+    bool lazy_on = false;                       // joins fetch triangles (attached tiles, serving arenas)
+    const uint8_t* lazy_raw = nullptr;          // device view of the host bytes (attached tiles; an arena's
+                                                // lazy_data_off holds absolute device-view addresses)
     uint64_t* lazy_data_off = nullptr;          // [n_obj] byte offset of each object's data block
-    unsigned* lazy_state = nullptr;             // [kNumLods * n_vox] 1 once the voxel's LOD is fetched
+    unsigned* lazy_state = nullptr;             // [kNumLods * lazy_stride] 1 once the voxel's LOD is on the device
+    long lazy_stride = 0;
     unsigned long long* lazy_bytes = nullptr;   // RAW bytes fetched so far
 };

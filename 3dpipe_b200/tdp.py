@@ -506,7 +506,7 @@ class RequestInfo(C.Structure):
 
 class ServerStats(C.Structure):
     _fields_ = [("batches", C.c_long), ("requests", C.c_long), ("failed", C.c_long), ("busy_ms", C.c_double),
-                ("upload_ms", C.c_double), ("upload_bytes", C.c_double)]
+                ("upload_ms", C.c_double), ("upload_bytes", C.c_double), ("fetch_bytes", C.c_double)]
 
 
 class Server:

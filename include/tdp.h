@@ -323,7 +323,11 @@ int tdp_join_chunked(tdp_ctx *ctx, const void *raw1, size_t len1, const void *ra
  *
  * The server takes over the context: no other call may use `ctx` until
  * tdp_server_destroy.  The bytes passed to tdp_server_submit must stay valid
- * until that request completes (tdp_server_wait returned TDP_OK or an error). */
+ * until that request completes (tdp_server_wait returned TDP_OK or an error).
+ * Requests in page-locked memory (cudaHostRegister / cudaHostAlloc, e.g.
+ * tdp_host_alloc) stage only their metadata: the batch join fetches, per
+ * LOD, the triangles of the voxels it refines straight from their bytes;
+ * other requests are copied whole. */
 typedef struct tdp_server tdp_server;
 typedef struct {
     long arena_objects;        /* query objects one arena holds        (default 65536)    */
@@ -349,7 +353,10 @@ typedef struct {
     double busy_ms;            /* wall time the executor spent in joins                    */
     double upload_ms;          /* per request, staging copy start to arena append done,
                                   summed (the copies of two requests overlap)              */
-    double upload_bytes;       /* RAW bytes staged                                           */
+    double upload_bytes;       /* bytes staged: every request's metadata, and the RAW bytes
+                                  of requests not in page-locked memory                    */
+    double fetch_bytes;        /* RAW bytes the batch joins fetched from page-locked
+                                  requests (only the voxels they refined)                  */
 } tdp_server_stats;
 void tdp_server_default_params(tdp_server_params *p);
 /* allocates both arenas in the context (counted against its budget) */

@@ -34,15 +34,19 @@ def setup(pkg, ctx):
 
 
 @pytest.mark.parametrize("arena_objects", [40, 100000])
-def test_each_request_equals_its_join_alone(pkg, ctx, setup, arena_objects):
+@pytest.mark.parametrize("pinned", [False, True])
+def test_each_request_equals_its_join_alone(pkg, ctx, setup, arena_objects, pinned):
+    """pinned: requests in page-locked memory, whose triangles the batch joins
+    fetch from the caller's bytes instead of staging them whole."""
     T2, reqs, alone = setup
+    bufs = [pkg.tdp.pinned_copy(r[0]) if pinned else r[0] for r in reqs]
     with pkg.tdp.Server(ctx, T2, arena_objects=arena_objects, arena_voxels=1 << 16, arena_tris=1 << 20,
                         max_request_bytes=64 << 20) as srv:
         ids = [None] * len(reqs)
 
         def client(k):
-            raw, query, K, tau = reqs[k]
-            ids[k] = srv.submit(raw, query=query, knn=max(K, 1), within=tau)
+            _, query, K, tau = reqs[k]
+            ids[k] = srv.submit(bufs[k], query=query, knn=max(K, 1), within=tau)
 
         threads = [threading.Thread(target=client, args=(k,)) for k in range(len(reqs))]
         for th in threads:
@@ -60,6 +64,11 @@ def test_each_request_equals_its_join_alone(pkg, ctx, setup, arena_objects):
             infos.append(info)
         st = srv.stats()
         assert st["requests"] == len(reqs) and st["failed"] == 0
+        raw_bytes = sum(r[0].size for r in reqs)
+        if pinned:
+            assert 0 < st["fetch_bytes"] < raw_bytes and st["upload_bytes"] < raw_bytes / 4, st
+        else:
+            assert st["fetch_bytes"] == 0 and st["upload_bytes"] >= raw_bytes / 2, st
         if arena_objects == 40:
             assert st["batches"] >= 4  # 128 objects of requests, at most 40 per batch
         assert max(i["batch_requests"] for i in infos) >= 2  # requests were mixed in a batch
