@@ -144,13 +144,18 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
             pool.emplace_back([&, l] {
                 HostVec<uint32_t>& vt = T->h_vtri[l];
                 vt.resize(H.n_vox + 1);
-                vt[0] = 0;
+                uint32_t* out = vt.data();
                 const uint64_t* off = H.vox_byte_off[l].data();
                 const uint32_t* cnt = H.vox_cnt[l].data();
+                uint64_t bad = 0;  // kept in a register: the five threads' flags share a cache line
+                uint32_t run = 0;
+                out[0] = 0;
                 for (long v = 0; v < H.n_vox; ++v) {
-                    misaligned[l] |= (off[v] & 3u) != 1u;
-                    vt[v + 1] = vt[v] + cnt[v];
+                    bad |= (off[v] & 3u) ^ 1u;
+                    run += cnt[v];
+                    out[v + 1] = run;
                 }
+                misaligned[l] = bad != 0;
             });
         for (auto& th : pool) th.join();
         for (int l = 0; l < kNumLods; ++l)

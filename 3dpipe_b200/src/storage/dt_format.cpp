@@ -172,7 +172,12 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
     std::vector<std::string> msg(nt);
     std::vector<std::array<uint64_t, kNumLods>> tris(nt);
     auto work = [&](int k) {
-        tris[k].fill(0);
+        uint64_t nt_l[kNumLods] = {0, 0, 0, 0, 0};  // per thread, in registers (no shared cache line)
+        struct Flush {
+            std::array<uint64_t, kNumLods>& dst;
+            const uint64_t* src;
+            ~Flush() { for (int l = 0; l < kNumLods; ++l) dst[l] = src[l]; }
+        } flush{tris[k], nt_l};
         const long o_end = n * (k + 1) / nt;
         for (long o = n * k / nt; o < o_end; ++o) {
             const Rec& r = recs[o];
@@ -216,7 +221,7 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
                     }
                     T.vox_byte_off[l][v0 + v] = r.data_off + off;
                     T.vox_cnt[l][v0 + v] = (uint32_t)cnt;
-                    tris[k][l] += cnt;
+                    nt_l[l] += cnt;
                 }
             }
             std::memcpy(&T.obj_xf[3 * o], p, 3 * sizeof(float));
