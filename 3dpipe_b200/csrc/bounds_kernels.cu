@@ -24,7 +24,10 @@
 // plus a margin far above FP64 rounding, lanes striding over the voxel's
 // triangles, a lexicographic (distance, index) warp minimum after each voxel.
 // The pieces' nearest facets are searched the same way with each lane cutting a
-// facet short once its running maximum reaches the best value.  Both searches
+// facet short once its running maximum reaches the best value.  Distances are
+// compared squared and rooted once per result (sqrt is monotone and correctly
+// rounded, so this changes no bound); the nearest-triangle assignment breaks
+// ties on the squared distance.  Both searches
 // return exactly what a scan of every triangle returns.  This file is built
 // with -fmad=false: each product and sum is rounded on its own, so the FP64
 // values equal a host evaluation of the same expressions.
@@ -150,11 +153,11 @@ __global__ void __launch_bounds__(kBoundsThreads, kBoundsBlocksPerSm) k_proxy(Bo
             const D3 q{(a.x + c1.x + c2.x) * (1.0 / 3.0), (a.y + c1.y + c2.y) * (1.0 / 3.0),
                        (a.z + c1.z + c2.z) * (1.0 / 3.0)};
             const double eps = pd::margin(q);
-            double bd = INFINITY;
+            double bd = INFINITY;  // squared distance of the nearest triangle so far
             unsigned bi = UINT_MAX;
             auto visit = [&](uint32_t u) {
                 for (uint32_t t = VT[u] + lane; t < VT[u + 1]; t += 32) {
-                    const double d = pd::tri(q, vert(T, t, 0), vert(T, t, 1), vert(T, t, 2));
+                    const double d = pd::tri2(q, vert(T, t, 0), vert(T, t, 1), vert(T, t, 2));
                     ++evals;
                     if (d < bd || (d == bd && t < bi)) { bd = d; bi = t; }
                 }
@@ -165,26 +168,26 @@ __global__ void __launch_bounds__(kBoundsThreads, kBoundsBlocksPerSm) k_proxy(Bo
                 const uint32_t u = base + lane;
                 const bool cand = u < ve && u != (uint32_t)v;
                 const double lb = cand ? pd::box_gap(q, box[2 * (size_t)u], box[2 * (size_t)u + 1]) : INFINITY;
-                unsigned mask = __ballot_sync(0xffffffffu, cand && lb <= bd + eps);
+                unsigned mask = __ballot_sync(0xffffffffu, cand && lb <= sqrt(bd) + eps);
                 while (mask) {
                     const int k = __ffs(mask) - 1;
                     mask &= mask - 1;
                     const double lbk = __shfl_sync(0xffffffffu, lb, k);
-                    if (lbk <= bd + eps) visit(base + k);
+                    if (lbk <= sqrt(bd) + eps) visit(base + k);
                 }
             }
             if (lane == 0) ++queries;
             if (bi == UINT_MAX) continue;
             double m = 0;
             if (lane < 3) {
-                m = pd::tri(vert(S, s, lane), vert(T, bi, 0), vert(T, bi, 1), vert(T, bi, 2));
+                m = pd::tri2(vert(S, s, lane), vert(T, bi, 0), vert(T, bi, 1), vert(T, bi, 2));
                 ++evals;
             }
             m = pd::dmax(m, __shfl_down_sync(0xffffffffu, m, 1));
             m = pd::dmax(m, __shfl_down_sync(0xffffffffu, m, 2));
             if (lane == 0)
                 atomicMax(reinterpret_cast<unsigned*>(const_cast<float*>(&T[3 * (size_t)bi].w)),
-                          __float_as_uint(__double2float_ru(m)));
+                          __float_as_uint(__double2float_ru(sqrt(m))));
         }
     }
     evals = warp_sum(evals);
@@ -247,7 +250,7 @@ __global__ void __launch_bounds__(kBoundsThreads, kBoundsBlocksPerSm) k_hausdorf
                     double dk = 0;
                     if (lane < 3) {
                         const D3 qk = lane == 0 ? q[0] : (lane == 1 ? q[1] : q[2]);
-                        dk = pd::tri(qk, vert(S, seed, 0), vert(S, seed, 1), vert(S, seed, 2));
+                        dk = pd::tri2(qk, vert(S, seed, 0), vert(S, seed, 1), vert(S, seed, 2));
                         ++evals;
                     }
                     dk = pd::dmax(dk, __shfl_down_sync(0xffffffffu, dk, 1));
@@ -264,7 +267,7 @@ __global__ void __launch_bounds__(kBoundsThreads, kBoundsBlocksPerSm) k_hausdorf
                         bool whole = true;
 #pragma unroll 1
                         for (int k = 0; k < 3; ++k) {
-                            acc = pd::dmax(acc, pd::tri(q[k], sa, sb, sc));
+                            acc = pd::dmax(acc, pd::tri2(q[k], sa, sb, sc));
                             ++evals;
                             if (acc >= mine) { whole = k == 2; break; }
                         }
@@ -283,19 +286,19 @@ __global__ void __launch_bounds__(kBoundsThreads, kBoundsBlocksPerSm) k_hausdorf
                         const float4 lo = box[2 * (size_t)u], hi = box[2 * (size_t)u + 1];
                         lb = pd::dmax(pd::box_gap(q[0], lo, hi), pd::dmax(pd::box_gap(q[1], lo, hi), pd::box_gap(q[2], lo, hi)));
                     }
-                    unsigned mask = __ballot_sync(0xffffffffu, cand && lb <= best + eps);
+                    unsigned mask = __ballot_sync(0xffffffffu, cand && lb <= sqrt(best) + eps);
                     while (mask) {
                         const int k = __ffs(mask) - 1;
                         mask &= mask - 1;
                         const double lbk = __shfl_sync(0xffffffffu, lb, k);
-                        if (lbk <= best + eps) visit(base + k);
+                        if (lbk <= sqrt(best) + eps) visit(base + k);
                     }
                 }
                 h = pd::dmax(h, best);
                 seed = best_i;
             }
             if (lane == 0) {
-                const_cast<float4*>(T)[3 * (size_t)t + 1].w = __double2float_ru(h);
+                const_cast<float4*>(T)[3 * (size_t)t + 1].w = __double2float_ru(sqrt(h));
                 npieces += np;
             }
         }

@@ -10,7 +10,7 @@
 // For an object with LOD-100 facets S (all voxels, stored order) and LOD-l
 // triangles T (l = 20..80):
 //   ph: every facet s goes to target(s) = the triangle t of T minimising
-//       (dist(bary(s), t), index of t); ph(t) = max over s with target t and
+//       (dist(bary(s), t)^2, index of t); ph(t) = max over s with target t and
 //       over the vertices q of s of dist(q, t)  (0 if no facet targets t).
 //   h:  e0 = mean edge length of S (edges (0,1),(1,2),(2,0) summed in stored
 //       order); t's depth d is the least d < 3 with L / 2^d <= 1.5 e0 (else 3),
@@ -50,44 +50,52 @@ inline double vdist(V3 a, V3 b) {
     return std::sqrt(vdot(d, d));
 }
 
-double seg_dist(V3 p, V3 a, V3 b) {
+inline double vdist2(V3 a, V3 b) {
+    const V3 d = vsub(a, b);
+    return vdot(d, d);
+}
+
+double seg_dist2(V3 p, V3 a, V3 b) {
     const V3 ab = vsub(b, a);
     const double den = vdot(ab, ab);
     double t = den > 0 ? vdot(vsub(p, a), ab) / den : 0.0;
     t = t < 0 ? 0.0 : (t > 1 ? 1.0 : t);
-    return vdist(p, vmad(a, t, ab));
+    return vdist2(p, vmad(a, t, ab));
 }
 
-double tri_dist(V3 p, V3 a, V3 b, V3 c) {
+// squared distance; the searches root it once per result
+double tri_dist2(V3 p, V3 a, V3 b, V3 c) {
     const V3 ab = vsub(b, a), ac = vsub(c, a), ap = vsub(p, a);
     const double d1 = vdot(ab, ap), d2 = vdot(ac, ap);
-    if (d1 <= 0 && d2 <= 0) return vdist(p, a);
+    if (d1 <= 0 && d2 <= 0) return vdist2(p, a);
     const V3 bp = vsub(p, b);
     const double d3 = vdot(ab, bp), d4 = vdot(ac, bp);
-    if (d3 >= 0 && d4 <= d3) return vdist(p, b);
+    if (d3 >= 0 && d4 <= d3) return vdist2(p, b);
     const double vc = d1 * d4 - d3 * d2;
     if (vc <= 0 && d1 >= 0 && d3 <= 0) {
         const double den = d1 - d3;
-        return vdist(p, vmad(a, den > 0 ? d1 / den : 0.0, ab));
+        return vdist2(p, vmad(a, den > 0 ? d1 / den : 0.0, ab));
     }
     const V3 cp = vsub(p, c);
     const double d5 = vdot(ab, cp), d6 = vdot(ac, cp);
-    if (d6 >= 0 && d5 <= d6) return vdist(p, c);
+    if (d6 >= 0 && d5 <= d6) return vdist2(p, c);
     const double vb = d5 * d2 - d1 * d6;
     if (vb <= 0 && d2 >= 0 && d6 <= 0) {
         const double den = d2 - d6;
-        return vdist(p, vmad(a, den > 0 ? d2 / den : 0.0, ac));
+        return vdist2(p, vmad(a, den > 0 ? d2 / den : 0.0, ac));
     }
     const double va = d3 * d6 - d5 * d4;
     if (va <= 0 && d4 - d3 >= 0 && d5 - d6 >= 0) {
         const double den = (d4 - d3) + (d5 - d6);
-        return vdist(p, vmad(b, den > 0 ? (d4 - d3) / den : 0.0, vsub(c, b)));
+        return vdist2(p, vmad(b, den > 0 ? (d4 - d3) / den : 0.0, vsub(c, b)));
     }
     const double s = va + vb + vc;
-    if (!(s > 0)) return std::min(seg_dist(p, a, b), std::min(seg_dist(p, b, c), seg_dist(p, c, a)));
+    if (!(s > 0)) return std::min(seg_dist2(p, a, b), std::min(seg_dist2(p, b, c), seg_dist2(p, c, a)));
     const double v = vb / s, w = vc / s;
-    return vdist(p, V3{a.x + ab.x * v + ac.x * w, a.y + ab.y * v + ac.y * w, a.z + ab.z * v + ac.z * w});
+    return vdist2(p, V3{a.x + ab.x * v + ac.x * w, a.y + ab.y * v + ac.y * w, a.z + ab.z * v + ac.z * w});
 }
+
+double tri_dist(V3 p, V3 a, V3 b, V3 c) { return std::sqrt(tri_dist2(p, a, b, c)); }
 
 double box_gap(V3 q, const float* lo, const float* hi) {
     const double gx = std::max(std::max((double)lo[0] - q.x, q.x - (double)hi[0]), 0.0);
@@ -144,13 +152,13 @@ struct Counter {
     double evals = 0;
 };
 
-// nearest triangle of T (lexicographic (distance, index)) to q; `home` is visited first
+// nearest triangle of T (lexicographic (squared distance, index)) to q; `home` is visited first
 size_t nearest(const Level& T, V3 q, size_t home, bool prune, Counter& C) {
     double bd = INFINITY;
     size_t bi = SIZE_MAX;
     auto visit = [&](size_t k) {
         for (size_t i = T.off[k]; i < T.off[k + 1]; ++i) {
-            const double d = tri_dist(q, T.v[3 * i], T.v[3 * i + 1], T.v[3 * i + 2]);
+            const double d = tri_dist2(q, T.v[3 * i], T.v[3 * i + 1], T.v[3 * i + 2]);
             C.evals += 1;
             if (d < bd || (d == bd && i < bi)) { bd = d; bi = i; }
         }
@@ -163,18 +171,18 @@ size_t nearest(const Level& T, V3 q, size_t home, bool prune, Counter& C) {
     const double eps = margin(q);
     visit(home);
     for (size_t k = 0; k < nv; ++k)
-        if (k != home && box_gap(q, &T.box[6 * k], &T.box[6 * k + 3]) <= bd + eps) visit(k);
+        if (k != home && box_gap(q, &T.box[6 * k], &T.box[6 * k + 3]) <= std::sqrt(bd) + eps) visit(k);
     return bi;
 }
 
-// min over facets s of S of max over the corners of dist(corner, s)
+// min over facets s of S of max over the corners of dist(corner, s)^2
 double piece_min(const Level& S, const V3 q[3], size_t home, bool prune, Counter& C) {
     double best = INFINITY;
     auto visit = [&](size_t k) {
         for (size_t i = S.off[k]; i < S.off[k + 1]; ++i) {
             double acc = 0;
             for (int c = 0; c < 3; ++c) {
-                const double d = tri_dist(q[c], S.v[3 * i], S.v[3 * i + 1], S.v[3 * i + 2]);
+                const double d = tri_dist2(q[c], S.v[3 * i], S.v[3 * i + 1], S.v[3 * i + 2]);
                 C.evals += 1;
                 acc = d > acc ? d : acc;
                 if (acc >= best) break;
@@ -194,7 +202,7 @@ double piece_min(const Level& S, const V3 q[3], size_t home, bool prune, Counter
         if (k == home) continue;
         double lb = 0;
         for (int c = 0; c < 3; ++c) lb = std::max(lb, box_gap(q[c], &S.box[6 * k], &S.box[6 * k + 3]));
-        if (lb <= best + eps) visit(k);
+        if (lb <= std::sqrt(best) + eps) visit(k);
     }
     return best;
 }
@@ -251,7 +259,7 @@ void object_bounds(const oracle::RObject& o, const uint8_t* base, uint8_t* out, 
                 if (t == SIZE_MAX) continue;
                 double m = 0;
                 for (int k = 0; k < 3; ++k) {
-                    const double d = tri_dist(S.v[3 * s + k], T.v[3 * t], T.v[3 * t + 1], T.v[3 * t + 2]);
+                    const double d = tri_dist2(S.v[3 * s + k], T.v[3 * t], T.v[3 * t + 1], T.v[3 * t + 2]);
                     C.evals += 1;
                     m = d > m ? d : m;
                 }
@@ -274,8 +282,8 @@ void object_bounds(const oracle::RObject& o, const uint8_t* base, uint8_t* out, 
                             h = m > h ? m : h;
                         }
                     }
-                    ph[t] = up(phd[t]);
-                    hh[t] = up(h);
+                    ph[t] = up(std::sqrt(phd[t]));
+                    hh[t] = up(std::sqrt(h));
                     obj_ph[li] = std::max(obj_ph[li], ph[t]);
                     obj_h[li] = std::max(obj_h[li], hh[t]);
                 }
