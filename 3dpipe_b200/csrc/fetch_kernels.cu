@@ -41,6 +41,29 @@ __device__ inline long last_le(const uint32_t* a, long n, uint32_t x) {
     return lo;
 }
 
+// stage[k] = the float that starts sh/8 bytes into word k of src, k < cnt
+// (cnt <= 32 * R - 1): lane j holds words j, j + 32, ...; word k + 1, which
+// the realignment needs, is the next lane's (lane 0's next round for lane 31).
+// Reads exactly words 0..cnt of src.
+template <int R>
+__device__ __forceinline__ void copy_words(const uint32_t* src, uint32_t cnt, unsigned sh, int lane,
+                                           uint32_t* stage) {
+    uint32_t w[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint32_t k = 32 * r + lane;
+        w[r] = k <= cnt && (sh || k < cnt) ? src[k] : 0u;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint32_t up = __shfl_down_sync(0xffffffffu, w[r], 1);
+        const uint32_t wrap = __shfl_sync(0xffffffffu, r + 1 < R ? w[r + 1 < R ? r + 1 : r] : 0u, 0);
+        const uint32_t next = lane < 31 ? up : wrap;
+        const uint32_t k = 32 * r + lane;
+        if (k < cnt) stage[k] = sh ? __funnelshift_r(w[r], next, sh) : w[r];
+    }
+}
+
 // copy voxel v's n triangles at LOD index lod (first record off) from the host
 // bytes into the tile's records, if this warp is the first to claim the voxel
 __device__ void fetch_voxel(const LazyTile& L, int lod, long v, uint32_t off, uint32_t n, uint32_t* stage) {
@@ -56,12 +79,14 @@ __device__ void fetch_voxel(const LazyTile& L, int lod, long v, uint32_t off, ui
     const uintptr_t base = reinterpret_cast<uintptr_t>(L.raw) + L.data_off[o] + 44 * before;
     const uint32_t* W = reinterpret_cast<const uint32_t*>(base & ~uintptr_t(3));
     const unsigned sh = (unsigned)(base & 3) * 8;
-    auto word = [&](uint64_t k) -> uint32_t { return sh ? __funnelshift_r(W[k], W[k + 1], sh) : W[k]; };
     float4* dst = L.tri[lod] + 3 * (size_t)off;
     for (uint32_t c0 = 0; c0 < n; c0 += 32) {
         const uint32_t m = min(32u, n - c0);
-        for (uint32_t k = lane; k < 9 * m; k += 32) stage[k] = word(9 * (uint64_t)c0 + k);
-        for (uint32_t k = lane; k < 2 * m; k += 32) stage[9 * m + k] = word(9 * (uint64_t)n + 2 * (uint64_t)c0 + k);
+        // the 9m triangle words and 2m bound words of these m triangles, plus
+        // the word after each run (for the realignment): every load issued
+        // before any is used; the next word comes from the next lane
+        copy_words<10>(W + 9 * (uint64_t)c0, 9 * m, sh, lane, stage);
+        copy_words<3>(W + 9 * (uint64_t)n + 2 * (uint64_t)c0, 2 * m, sh, lane, stage + 9 * m);
         __syncwarp();
         if (lane < m) {
             const float* f = reinterpret_cast<const float*>(stage + 9 * lane);
