@@ -13,8 +13,6 @@
 // at an object's first byte into a 256-byte aligned staging buffer, which makes
 // every float 4-byte aligned on the device (checked on the host per segment).
 #include <algorithm>
-#include <atomic>
-#include <climits>
 #include <thread>
 #include <chrono>
 #include <cstring>
@@ -58,6 +56,32 @@ cudaError_t launch_unpack(const uint8_t* raw, const UnpackSeg* segs, int nseg, f
     const int blocks = (int)std::min<size_t>(((size_t)nseg + 7) / 8, (size_t)num_sms * 16);
     unpack_kernel<<<blocks, 256, 0, s>>>(raw, segs, nseg, tp);
     return cudaGetLastError();
+}
+
+// out[v + 1] = sum of cnt[0..v] (out[0] = 0), also into stage when given.
+// Returns true when a voxel's triangles do not start 1 byte past a 4-byte
+// boundary of the tile buffer: every field of an object is 4 or 8 bytes and
+// the objects follow the 1-byte type, so the kernels' 4-byte reads rely on it.
+static bool vtri_prefix(const uint64_t* off, const uint32_t* cnt, long n, uint32_t* out, uint32_t* stage) {
+    uint64_t bad = 0;  // in a register: the five LOD threads' flags share a cache line
+    uint32_t run = 0;
+    out[0] = 0;
+    if (stage) {
+        stage[0] = 0;
+        for (long v = 0; v < n; ++v) {
+            bad |= (off[v] & 3u) ^ 1u;
+            run += cnt[v];
+            out[v + 1] = run;
+            stage[v + 1] = run;
+        }
+    } else {
+        for (long v = 0; v < n; ++v) {
+            bad |= (off[v] & 3u) ^ 1u;
+            run += cnt[v];
+            out[v + 1] = run;
+        }
+    }
+    return bad != 0;
 }
 
 // fn(b, e) over [0, n) in a few host threads (one for small n)
@@ -135,61 +159,14 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
     T->n_vox = H.n_vox;
     for (int l = 0; l < kNumLods; ++l)
         if (H.n_tris[l] >= 0xffffffffull) { delete T; return fail(ctx, TDP_ERR_FORMAT, "more than 2^32 triangles in one LOD"); }
-    // per LOD (one host thread each): alignment of every voxel's floats and
-    // the prefix of triangle counts
-    {
-        bool misaligned[kNumLods] = {false, false, false, false, false};
-        std::vector<std::thread> pool;
-        for (int l = 0; l < kNumLods; ++l)
-            pool.emplace_back([&, l] {
-                HostVec<uint32_t>& vt = T->h_vtri[l];
-                vt.resize(H.n_vox + 1);
-                uint32_t* out = vt.data();
-                const uint64_t* off = H.vox_byte_off[l].data();
-                const uint32_t* cnt = H.vox_cnt[l].data();
-                uint64_t bad = 0;  // kept in a register: the five threads' flags share a cache line
-                uint32_t run = 0;
-                out[0] = 0;
-                for (long v = 0; v < H.n_vox; ++v) {
-                    bad |= (off[v] & 3u) ^ 1u;
-                    run += cnt[v];
-                    out[v + 1] = run;
-                }
-                misaligned[l] = bad != 0;
-            });
-        for (auto& th : pool) th.join();
-        for (int l = 0; l < kNumLods; ++l)
-            if (misaligned[l]) { delete T; return fail(ctx, TDP_ERR_FORMAT, "misaligned triangle data"); }
-    }
-    if (attach) {
-        // fetches locate a voxel's bytes from the prefix arrays: the data
-        // block must hold, LOD by LOD and voxel by voxel, each voxel's
-        // triangles then its bounds, with nothing in between (the layout the
-        // reference's writer produces, src/storage/tile_IO.cpp:79-172)
-        std::atomic<long> first_bad{LONG_MAX};
-        host_parallel(H.n_obj, [&](long b, long e) {
-            for (long o = b; o < e; ++o) {
-                uint64_t expect = H.obj_data_off[o];
-                bool ok = true;
-                for (int l = 0; l < kNumLods && ok; ++l)
-                    for (uint32_t v = H.obj_vox_off[o]; v < H.obj_vox_off[o + 1]; ++v) {
-                        if (H.vox_byte_off[l][v] != expect) { ok = false; break; }
-                        expect += 44ull * H.vox_cnt[l][v];
-                    }
-                if (!ok) {
-                    long cur = first_bad.load();
-                    while (o < cur && !first_bad.compare_exchange_weak(cur, o)) {}
-                    return;
-                }
-            }
-        });
-        if (first_bad.load() != LONG_MAX) {
-            const long o = first_bad.load();
-            delete T;
-            return fail(ctx, TDP_ERR_FORMAT, "object " + std::to_string(o) +
-                                                 " does not keep its voxels' triangles in LOD and voxel "
-                                                 "order; use tdp_tile_upload for this tile");
-        }
+    if (attach && H.first_noncanonical >= 0) {
+        // fetches locate a voxel's bytes from the prefix arrays, which needs
+        // the layout the reference's writer produces (checked by the parser)
+        const long o = H.first_noncanonical;
+        delete T;
+        return fail(ctx, TDP_ERR_FORMAT, "object " + std::to_string(o) +
+                                             " does not keep its voxels' triangles in LOD and voxel "
+                                             "order; use tdp_tile_upload for this tile");
     }
     const auto ta = std::chrono::steady_clock::now();
     auto alloc = [&](void** p, size_t bytes) -> int {
@@ -201,31 +178,34 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
     };
     cudaStream_t s = ctx->stream;
 #define TRY(x) do { int _r = (x); if (_r) { tile_release(ctx, T); return _r; } } while (0)
-#define CTRY(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { tile_release(ctx, T); return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } } while (0)
+#define CTRY(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { cudaStreamSynchronize(s); tile_release(ctx, T); return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } } while (0)
     TRY(alloc((void**)&T->vox, (size_t)H.n_vox * 3 * sizeof(float4)));
     TRY(alloc((void**)&T->obj_vox, (size_t)(H.n_obj + 1) * sizeof(uint32_t)));
     TRY(alloc((void**)&T->obj_hd, (size_t)H.n_obj * kNumLods * sizeof(float)));
     TRY(alloc((void**)&T->obj_phd, (size_t)H.n_obj * kNumLods * sizeof(float)));
-    auto alloc_block = [&](void** p, size_t bytes) -> int {
-        if (block_alloc(ctx, p, bytes) != cudaSuccess)
-            return fail(ctx, TDP_ERR_NOMEM, "tile upload: cannot allocate " + std::to_string(bytes) + " bytes" +
-                                                (ctx->budget ? " within the context budget" : ""));
-        T->device_bytes += bytes;
-        return TDP_OK;
-    };
     for (int l = 0; l < kNumLods; ++l) {
-        TRY(alloc_block((void**)&T->tri[l], (size_t)H.n_tris[l] * 3 * sizeof(float4)));
+        TRY(alloc((void**)&T->tri[l], (size_t)H.n_tris[l] * 3 * sizeof(float4)));
         TRY(alloc((void**)&T->vtri[l], (size_t)(H.n_vox + 1) * sizeof(uint32_t)));
+    }
+    if (attach) {
+        TRY(alloc((void**)&T->lazy_data_off, (size_t)std::max<long>(H.n_obj, 1) * sizeof(uint64_t)));
+        TRY(alloc((void**)&T->lazy_state, (size_t)kNumLods * std::max<long>(H.n_vox, 1) * sizeof(unsigned)));
+        TRY(alloc((void**)&T->lazy_bytes, sizeof(unsigned long long)));
     }
     T->alloc_ms = ms_since(ta);
     const auto tm = std::chrono::steady_clock::now();
     {
-        // the metadata go up through the context's page-locked staging buffer
-        // (assembled by host threads), so the copies run at full PCIe rate
+        // The metadata go up through the context's page-locked staging
+        // buffer, laid out [voxel records][data-block offsets][vtri x 5]
+        // [obj_vox][obj_hd][obj_phd].  Host threads write it directly: one
+        // per LOD computes the prefix of triangle counts (into the tile's
+        // host copy and the staging slot at once) while the others assemble
+        // the voxel records, whose copy then starts while the prefixes finish.
         const size_t v4_bytes = (size_t)H.n_vox * 3 * sizeof(float4);
+        const size_t do_bytes = attach ? (size_t)H.n_obj * sizeof(uint64_t) : 0;
         const size_t vt_bytes = (size_t)(H.n_vox + 1) * sizeof(uint32_t);
         const size_t ov_bytes = H.obj_vox_off.size() * 4, hd_bytes = H.obj_hd.size() * 4;
-        const size_t need = v4_bytes + kNumLods * vt_bytes + ov_bytes + 2 * hd_bytes + 64;
+        const size_t need = v4_bytes + do_bytes + kNumLods * vt_bytes + ov_bytes + 2 * hd_bytes + 64;
         if (need > ctx->hstage_cap) {
             if (ctx->hstage) cudaFreeHost(ctx->hstage);
             ctx->hstage = nullptr;
@@ -234,9 +214,22 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
                 ctx->hstage_cap = need + need / 4;
             else { cudaGetLastError(); ctx->hstage = nullptr; }
         }
+        uint8_t* stg = (uint8_t*)ctx->hstage;  // nullptr: copy from pageable memory
+        uint32_t* vt_stage[kNumLods] = {};
+        if (stg)
+            for (int l = 0; l < kNumLods; ++l) vt_stage[l] = (uint32_t*)(stg + v4_bytes + do_bytes + l * vt_bytes);
+        bool misaligned[kNumLods] = {false, false, false, false, false};
+        std::vector<std::thread> pool;
+        for (int l = 0; l < kNumLods; ++l)
+            pool.emplace_back([&, l] {
+                HostVec<uint32_t>& vt = T->h_vtri[l];
+                vt.resize(H.n_vox + 1);
+                misaligned[l] = vtri_prefix(H.vox_byte_off[l].data(), H.vox_cnt[l].data(), H.n_vox, vt.data(),
+                                            vt_stage[l]);
+            });
         std::vector<float4> v4_pageable;
         float4* v4 = nullptr;
-        if (ctx->hstage) v4 = (float4*)ctx->hstage;
+        if (stg) v4 = (float4*)stg;
         else { v4_pageable.resize((size_t)H.n_vox * 3); v4 = v4_pageable.data(); }
         host_parallel(H.n_vox, [&](long b, long e) {
             for (long v = b; v < e; ++v) {
@@ -246,47 +239,54 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
                 v4[3 * v + 2] = make_float4(x[6], x[7], x[8], 0.f);
             }
         });
+        const void* src_do = H.obj_data_off.data();
+        if (stg && attach) {
+            std::memcpy(stg + v4_bytes, src_do, do_bytes);
+            src_do = stg + v4_bytes;
+        }
+        // no early return while the prefix threads run
+        cudaError_t e = cudaMemcpyAsync(T->vox, v4, v4_bytes, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && attach)
+            e = cudaMemcpyAsync(T->lazy_data_off, src_do, do_bytes, cudaMemcpyHostToDevice, s);
+        for (auto& th : pool) th.join();
+        CTRY(e);
+        for (int l = 0; l < kNumLods; ++l)
+            if (misaligned[l]) {
+                cudaStreamSynchronize(s);
+                tile_release(ctx, T);
+                return fail(ctx, TDP_ERR_FORMAT, "misaligned triangle data");
+            }
         const void* src_vt[kNumLods];
         const void* src_ov = H.obj_vox_off.data();
         const void* src_hd = H.obj_hd.data();
         const void* src_phd = H.obj_phd.data();
-        if (ctx->hstage) {
-            uint8_t* p = (uint8_t*)ctx->hstage + v4_bytes;
-            std::vector<std::thread> pool;
-            for (int l = 0; l < kNumLods; ++l) {
-                src_vt[l] = p;
-                pool.emplace_back([&, l, p] { std::memcpy(p, T->h_vtri[l].data(), vt_bytes); });
-                p += vt_bytes;
-            }
-            for (auto& th : pool) th.join();
+        if (stg) {
+            uint8_t* p = stg + v4_bytes + do_bytes + kNumLods * vt_bytes;
+            for (int l = 0; l < kNumLods; ++l) src_vt[l] = vt_stage[l];
             std::memcpy(p, src_ov, ov_bytes); src_ov = p; p += ov_bytes;
             std::memcpy(p, src_hd, hd_bytes); src_hd = p; p += hd_bytes;
             std::memcpy(p, src_phd, hd_bytes); src_phd = p;
         } else {
             for (int l = 0; l < kNumLods; ++l) src_vt[l] = T->h_vtri[l].data();
         }
-        CTRY(cudaMemcpyAsync(T->vox, v4, v4_bytes, cudaMemcpyHostToDevice, s));
+        for (int l = 0; l < kNumLods; ++l)
+            CTRY(cudaMemcpyAsync(T->vtri[l], src_vt[l], vt_bytes, cudaMemcpyHostToDevice, s));
         CTRY(cudaMemcpyAsync(T->obj_vox, src_ov, ov_bytes, cudaMemcpyHostToDevice, s));
         CTRY(cudaMemcpyAsync(T->obj_hd, src_hd, hd_bytes, cudaMemcpyHostToDevice, s));
         CTRY(cudaMemcpyAsync(T->obj_phd, src_phd, hd_bytes, cudaMemcpyHostToDevice, s));
-        for (int l = 0; l < kNumLods; ++l)
-            CTRY(cudaMemcpyAsync(T->vtri[l], src_vt[l], vt_bytes, cudaMemcpyHostToDevice, s));
-        T->h2d_bytes += v4_bytes + ov_bytes + 2 * hd_bytes + kNumLods * vt_bytes;
+        T->h2d_bytes += v4_bytes + do_bytes + ov_bytes + 2 * hd_bytes + kNumLods * vt_bytes;
+        if (attach) {
+            CTRY(cudaMemsetAsync(T->lazy_state, 0, (size_t)kNumLods * H.n_vox * sizeof(unsigned), s));
+            CTRY(cudaMemsetAsync(T->lazy_bytes, 0, sizeof(unsigned long long), s));
+            if (ctx->flags & TDP_CTX_POISON)
+                for (int l = 0; l < kNumLods; ++l)
+                    CTRY(cudaMemsetAsync(T->tri[l], 0xff, (size_t)H.n_tris[l] * 3 * sizeof(float4), s));
+        }
+        // the staging buffer is free for the next tile once this returns
         CTRY(cudaStreamSynchronize(s));
     }
     T->meta_ms = ms_since(tm);
     if (attach) {
-        TRY(alloc((void**)&T->lazy_data_off, (size_t)std::max<long>(H.n_obj, 1) * sizeof(uint64_t)));
-        TRY(alloc((void**)&T->lazy_state, (size_t)kNumLods * std::max<long>(H.n_vox, 1) * sizeof(unsigned)));
-        TRY(alloc((void**)&T->lazy_bytes, sizeof(unsigned long long)));
-        CTRY(cudaMemcpyAsync(T->lazy_data_off, H.obj_data_off.data(), H.n_obj * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-        CTRY(cudaMemsetAsync(T->lazy_state, 0, (size_t)kNumLods * H.n_vox * sizeof(unsigned), s));
-        CTRY(cudaMemsetAsync(T->lazy_bytes, 0, sizeof(unsigned long long), s));
-        if (ctx->flags & TDP_CTX_POISON)
-            for (int l = 0; l < kNumLods; ++l)
-                CTRY(cudaMemsetAsync(T->tri[l], 0xff, (size_t)H.n_tris[l] * 3 * sizeof(float4), s));
-        CTRY(cudaStreamSynchronize(s));
-        T->h2d_bytes += H.n_obj * sizeof(uint64_t);
         T->lazy_raw = dev_view;
         T->lazy_on = true;
         T->lazy_stride = H.n_vox;

@@ -4,12 +4,88 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
 #include <thread>
+#include <unordered_map>
 
 #include "tdp.h"
 
 namespace tdp {
+
+namespace {
+
+struct HostBlockCache {
+    std::mutex mu;
+    std::multimap<size_t, void*> free_blocks;  // capacity -> freed block
+    std::unordered_map<void*, size_t> cap;     // capacity of every block the cache made
+    size_t cached = 0;                         // bytes in free_blocks
+};
+
+// never destroyed: tiles may release their arrays during static destruction
+HostBlockCache& host_cache() {
+    static HostBlockCache* c = new HostBlockCache();
+    return *c;
+}
+
+// free cached blocks (smallest first) until at most `keep` bytes stay; the
+// caller holds the lock
+void host_cache_shrink(HostBlockCache& c, size_t keep) {
+    while (c.cached > keep && !c.free_blocks.empty()) {
+        auto it = c.free_blocks.begin();
+        c.cached -= it->first;
+        c.cap.erase(it->second);
+        std::free(it->second);
+        c.free_blocks.erase(it);
+    }
+}
+
+}  // namespace
+
+void* host_block_get(size_t bytes) {
+    HostBlockCache& c = host_cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    auto it = c.free_blocks.lower_bound(bytes);
+    if (it != c.free_blocks.end() && it->first - bytes <= bytes / 8) {
+        void* p = it->second;
+        c.cached -= it->first;
+        c.free_blocks.erase(it);
+        return p;
+    }
+    void* p = std::malloc(bytes);
+    if (!p) {
+        host_cache_shrink(c, 0);
+        p = std::malloc(bytes);
+        if (!p) throw std::bad_alloc();
+    }
+    c.cap[p] = bytes;
+    return p;
+}
+
+void host_block_put(void* p, size_t bytes) {
+    if (!p) return;
+    HostBlockCache& c = host_cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    auto it = c.cap.find(p);
+    const size_t cap = it != c.cap.end() ? it->second : bytes;
+    if (cap > kHostCacheMax) {
+        if (it != c.cap.end()) c.cap.erase(it);
+        std::free(p);
+        return;
+    }
+    host_cache_shrink(c, kHostCacheMax - cap);
+    c.free_blocks.emplace(cap, p);
+    c.cached += cap;
+}
+
+size_t host_cache_bytes() {
+    HostBlockCache& c = host_cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    return c.cached;
+}
 
 namespace {
 template <typename T>
@@ -30,6 +106,18 @@ size_t raw_object_bytes(uint32_t nvox, const uint32_t* counts) {
 }
 
 namespace {
+
+// object o's data block holds, LOD by LOD and voxel by voxel, each voxel's
+// triangles then their bounds, with nothing in between
+bool object_canonical(const TileHost& T, long o, uint32_t v0, uint32_t v1) {
+    uint64_t expect = T.obj_data_off[o];
+    for (int l = 0; l < kNumLods; ++l)
+        for (uint32_t v = v0; v < v1; ++v) {
+            if (T.vox_byte_off[l][v] != expect) return false;
+            expect += 44ull * T.vox_cnt[l][v];
+        }
+    return true;
+}
 
 // One object after another: the reference reader's order.  Used as is for the
 // exact first error of a malformed tile.
@@ -95,6 +183,8 @@ int parse_sequential(const uint8_t* buf, size_t len, long max_objects, TileHost&
     }
     T.n_vox = T.obj_vox_off.back();
     if (T.n_obj == 0) { err = "tile holds no objects"; return TDP_ERR_FORMAT; }
+    for (long o = 0; o < T.n_obj && T.first_noncanonical < 0; ++o)
+        if (!object_canonical(T, o, T.obj_vox_off[o], T.obj_vox_off[o + 1])) T.first_noncanonical = o;
     return TDP_OK;
 }
 
@@ -113,7 +203,7 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
     struct Rec {
         uint64_t data_off, data_size, meta, vnum;
     };
-    std::vector<Rec> recs;
+    HostVec<Rec> recs;
     size_t pos = 1;
     uint64_t nvox = 0;
     constexpr size_t kVoxBytes = 9 * sizeof(float) + kNumLods * 2 * sizeof(uint64_t);
@@ -171,7 +261,14 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
     std::vector<long> bad(nt, -1);
     std::vector<std::string> msg(nt);
     std::vector<std::array<uint64_t, kNumLods>> tris(nt);
+    std::vector<long> noncanon(nt, -1);
     auto work = [&](int k) {
+        long nc = -1;  // this chunk's lowest non-canonical object, in a register
+        struct FlushNc {
+            long& dst;
+            const long& src;
+            ~FlushNc() { dst = src; }
+        } flush_nc{noncanon[k], nc};
         uint64_t nt_l[kNumLods] = {0, 0, 0, 0, 0};  // per thread, in registers (no shared cache line)
         struct Flush {
             std::array<uint64_t, kNumLods>& dst;
@@ -226,6 +323,7 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
             }
             std::memcpy(&T.obj_xf[3 * o], p, 3 * sizeof(float));
             T.obj_data_off[o] = r.data_off;
+            if (nc < 0 && !object_canonical(T, o, v0, v0 + (uint32_t)r.vnum)) nc = o;
             T.obj_data_size[o] = r.data_size;
             float* ob = &T.obj_box[6 * o];
             ob[0] = lo[0]; ob[1] = lo[1]; ob[2] = lo[2];
@@ -247,6 +345,7 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
         }
     for (int k = 0; k < nt; ++k)
         for (int l = 0; l < kNumLods; ++l) T.n_tris[l] += tris[k][l];
+    for (int k = 0; k < nt && T.first_noncanonical < 0; ++k) T.first_noncanonical = noncanon[k];
     return TDP_OK;
 }
 

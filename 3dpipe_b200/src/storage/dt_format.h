@@ -36,12 +36,26 @@ inline int lod_index(int lod) {
     return -1;
 }
 
+// Large host arrays (kHostBlockMin bytes and up) are recycled through a
+// process-wide cache of freed blocks.  A block fresh from the system arrives
+// as untouched pages, every first touch of one costs a page fault, and handing
+// it back costs an munmap: for a 100k-object tile that was about half of the
+// parse.  The cache keeps at most kHostCacheMax bytes of freed blocks and
+// serves a request from a cached block at most 1/8 larger.
+constexpr size_t kHostBlockMin = size_t(1) << 20;
+constexpr size_t kHostCacheMax = size_t(4) << 30;
+void* host_block_get(size_t bytes);  // throws std::bad_alloc
+void host_block_put(void* p, size_t bytes);
+size_t host_cache_bytes();           // freed bytes held by the cache now
+
 // An allocator whose resize() leaves new elements of plain types
 // uninitialised: the parser writes every element from its own threads, so a
 // tile's arrays are touched first there (in parallel) instead of being
-// zeroed by one thread beforehand.
+// zeroed by one thread beforehand.  Large arrays come from the host block
+// cache.
 template <typename T>
 struct NoInitAlloc : std::allocator<T> {
+    using value_type = T;
     template <typename U>
     struct rebind {
         using other = NoInitAlloc<U>;
@@ -49,6 +63,14 @@ struct NoInitAlloc : std::allocator<T> {
     NoInitAlloc() = default;
     template <typename U>
     NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    T* allocate(size_t n) {
+        if (n * sizeof(T) >= kHostBlockMin) return static_cast<T*>(host_block_get(n * sizeof(T)));
+        return std::allocator<T>::allocate(n);
+    }
+    void deallocate(T* p, size_t n) {
+        if (n * sizeof(T) >= kHostBlockMin) host_block_put(p, n * sizeof(T));
+        else std::allocator<T>::deallocate(p, n);
+    }
     template <typename U>
     void construct(U* p) noexcept {
         ::new (static_cast<void*>(p)) U;
@@ -76,6 +98,11 @@ struct TileHost {
     HostVec<uint64_t> vox_byte_off[kNumLods];  // absolute byte offset of the voxel's triangles
     HostVec<uint32_t> vox_cnt[kNumLods];
     uint64_t n_tris[kNumLods] = {0, 0, 0, 0, 0};
+    // lowest object whose data block does not hold, LOD by LOD and voxel by
+    // voxel, each voxel's triangles then their bounds with nothing in between
+    // (the layout the reference's writer produces, src/storage/tile_IO.cpp:79-172); -1
+    // when every object does
+    long first_noncanonical = -1;
 };
 
 // Parse `len` bytes; at most max_objects objects (<= 0: all).  Returns 0 or a
