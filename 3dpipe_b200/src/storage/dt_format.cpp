@@ -190,6 +190,58 @@ int parse_sequential(const uint8_t* buf, size_t len, long max_objects, TileHost&
 
 }  // namespace
 
+namespace {
+
+struct Rec {
+    uint64_t data_off, data_size, meta, vnum;
+};
+constexpr size_t kVoxBytes = 9 * sizeof(float) + kNumLods * 2 * sizeof(uint64_t);
+
+// the record of the object whose first byte is at pos; false on a structural
+// problem (the sequential parser then reports it)
+inline bool walk_one(const uint8_t* buf, size_t len, size_t& pos, Rec& r) {
+    uint64_t data_size = 0, vnum = 0;
+    if (!rd(buf, len, pos, data_size) || data_size > len - pos || data_size % 4) return false;
+    r.data_off = pos;
+    r.data_size = data_size;
+    pos += data_size;
+    if (!rd(buf, len, pos, vnum) || vnum == 0 || vnum > (1u << 24)) return false;
+    const uint64_t rec = 2 * kNumLods * sizeof(float) + vnum * kVoxBytes + 3 * sizeof(float);
+    if (rec > len - pos) return false;
+    r.meta = pos;
+    r.vnum = vnum;
+    pos += rec;
+    return true;
+}
+
+// up to `limit` records from pos into out (count in n, pos past the last);
+// false on a structural problem.  Every object's position depends on the
+// sizes read at the previous one, so this is a chain of dependent loads: the
+// headers of the next few objects are prefetched at the last record's stride
+// (a wrong guess only wastes a prefetch).
+bool walk_chain(const uint8_t* buf, size_t len, size_t& pos, long limit, Rec* out, long& n) {
+    constexpr int kAhead = 8;
+    uint64_t stride = 0, last_ds = 0;
+    n = 0;
+    while (pos < len && n < limit) {
+        if (stride)
+            for (int k = 1; k <= kAhead; ++k) {
+                const uint64_t q = pos + k * stride;
+                if (q + 8 + last_ds + 8 > len) break;
+                __builtin_prefetch(buf + q);
+                __builtin_prefetch(buf + q + 8 + last_ds);
+            }
+        const size_t start = pos;
+        if (!walk_one(buf, len, pos, out[n])) return false;
+        stride = pos - start;
+        last_ds = out[n].data_size;
+        ++n;
+    }
+    return true;
+}
+
+}  // namespace
+
 // Two passes: a walk over the size fields finds every object's record (a
 // structural problem hands the tile to the sequential parser, which reports
 // the first error in file order); then the objects' voxel tables are read in
@@ -200,45 +252,68 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
     T = TileHost();
     if (!buf || len < 1) { err = "empty tile buffer"; return TDP_ERR_FORMAT; }
     if (buf[0] != kRawType) return parse_sequential(buf, len, max_objects, T, err);
-    struct Rec {
-        uint64_t data_off, data_size, meta, vnum;
-    };
     HostVec<Rec> recs;
     size_t pos = 1;
-    uint64_t nvox = 0;
-    constexpr size_t kVoxBytes = 9 * sizeof(float) + kNumLods * 2 * sizeof(uint64_t);
-    // Every object's position depends on the sizes read at the previous one,
-    // so the walk is a chain of dependent loads.  Objects of one tile are
-    // mostly the same size (instances of one mesh), so the headers of the
-    // next few objects are prefetched at the last record's stride; a wrong
-    // guess only wastes a prefetch.
-    uint64_t stride = 0, last_ds = 0;
-    constexpr int kAhead = 8;
-    while (pos < len && (max_objects <= 0 || (long)recs.size() < max_objects)) {
-        if (stride)
-            for (int k = 1; k <= kAhead; ++k) {
-                const uint64_t q = pos + k * stride;
-                if (q + 8 + last_ds + 8 > len) break;
-                __builtin_prefetch(buf + q);
-                __builtin_prefetch(buf + q + 8 + last_ds);
+    // Objects of one tile are mostly the same size (instances of one mesh):
+    // with many objects, threads walk chunks from guessed starts at the
+    // first object's stride.  A chunk counts only when the walk before it
+    // ends exactly on its start, so what is kept is what the serial walk
+    // would find; the walk continues serially from the last verified
+    // position (a wrong guess, a structural problem, the tile's end).
+    if (max_objects <= 0) {
+        size_t p1 = 1;
+        Rec r0;
+        const long hw = (long)std::thread::hardware_concurrency();
+        if (walk_one(buf, len, p1, r0)) {
+            const uint64_t stride = p1 - 1;
+            const long n_est = (long)((len - 1) / stride);
+            const long nt = std::min(hw, n_est / 4096);
+            if (nt >= 2) {
+                const long per = (n_est + nt - 1) / nt;
+                recs.resize((size_t)(nt * per));
+                std::vector<long> got(nt, 0);
+                std::vector<size_t> end(nt, 0);
+                std::vector<char> clean(nt, 0);
+                std::vector<std::thread> pool;
+                for (long k = 0; k < nt; ++k)
+                    pool.emplace_back([&, k] {
+                        size_t q = 1 + (size_t)(k * per) * stride;
+                        if (q >= len) return;
+                        long c = 0;
+                        clean[k] = walk_chain(buf, len, q, per, &recs[(size_t)(k * per)], c);
+                        got[k] = c;
+                        end[k] = q;
+                    });
+                for (auto& th : pool) th.join();
+                long kept = 0;
+                for (long k = 0; k < nt; ++k) {
+                    if (!clean[k] || 1 + (size_t)(k * per) * stride != pos) break;
+                    kept += got[k];
+                    pos = end[k];
+                    if (got[k] != per) break;
+                }
+                recs.resize((size_t)kept);
             }
-        const size_t start = pos;
-        uint64_t data_size = 0, vnum = 0;
-        if (!rd(buf, len, pos, data_size) || data_size > len - pos || data_size % 4)
-            return parse_sequential(buf, len, max_objects, T, err);
-        const uint64_t data_off = pos;
-        pos += data_size;
-        if (!rd(buf, len, pos, vnum) || vnum == 0 || vnum > (1u << 24))
-            return parse_sequential(buf, len, max_objects, T, err);
-        const uint64_t rec = 2 * kNumLods * sizeof(float) + vnum * kVoxBytes + 3 * sizeof(float);
-        if (rec > len - pos) return parse_sequential(buf, len, max_objects, T, err);
-        recs.push_back({data_off, data_size, pos, vnum});
-        pos += rec;
-        stride = pos - start;
-        last_ds = data_size;
-        nvox += vnum;
-        if (nvox >= 0xffffffffull) return parse_sequential(buf, len, max_objects, T, err);
+        }
     }
+    {
+        size_t q = pos;
+        long c = 0;
+        const long room = max_objects <= 0 ? -1 : max_objects;
+        while (q < len && (room < 0 || (long)recs.size() < room)) {
+            // serial walk in blocks (the block's records land in place)
+            const long block = room < 0 ? 65536 : std::min<long>(65536, room - (long)recs.size());
+            const size_t at = recs.size();
+            recs.resize(at + (size_t)block);
+            c = 0;
+            const bool ok = walk_chain(buf, len, q, block, &recs[at], c);
+            recs.resize(at + (size_t)c);
+            if (!ok) return parse_sequential(buf, len, max_objects, T, err);
+        }
+    }
+    uint64_t nvox = 0;
+    for (const Rec& r : recs) nvox += r.vnum;
+    if (nvox >= 0xffffffffull) return parse_sequential(buf, len, max_objects, T, err);
     const long n = (long)recs.size();
     if (n == 0) { err = "tile holds no objects"; return TDP_ERR_FORMAT; }
     T.n_obj = n;

@@ -81,3 +81,79 @@ def test_structural_errors(pkg):
         assert str(e.value).endswith(want), (str(e.value), want)
     with pytest.raises(pkg.TdpError):
         pkg.tdp.raw_check(np.array([2, 0, 0], np.uint8))   # not RAW
+
+
+# Tiles of many equal-size records: the parser's threads walk chunks from
+# starts guessed at the first record's stride.  Two record kinds share one
+# size -- A: one voxel with 29 triangles (5+5+6+6+7 over the LODs), B: twelve
+# voxels without triangles (44 * 29 + 116 == 116 * 12) -- so the voxel count
+# tells whether every record was found where the serial walk finds it.
+def _record(kind, extra_voxels=0):
+    if kind == "A":
+        counts, nv = (5, 5, 6, 6, 7), 1
+    else:
+        counts, nv = (0, 0, 0, 0, 0), 12
+    nv += extra_voxels
+    data = bytearray(44 * sum(counts))
+    for i in range(0, len(data), 4):
+        struct.pack_into("<f", data, i, float(i % 97))
+    rec = bytearray(struct.pack("<Q", len(data))) + data + struct.pack("<Q", nv)
+    rec += struct.pack("<10f", *([1.0] * 10))
+    off = 0
+    for v in range(nv):
+        rec += struct.pack("<9f", 0, 0, 0, 1, 1, 1, 0.5, 0.5, 0.5)
+        for li in range(5):
+            c = counts[li] if v == 0 else 0
+            rec += struct.pack("<QQ", off, c)
+            off += 44 * c
+    rec += struct.pack("<3f", 0, 0, 0)
+    return bytes(rec)
+
+
+def _uniform_tile(n, seed, odd=None):
+    """(bytes, voxels per record, record offsets); record `odd` gets one more voxel"""
+    rng = np.random.default_rng(seed)
+    kinds = rng.integers(0, 2, n)
+    recs = {"A": _record("A"), "B": _record("B")}
+    parts, nvox, offs = [b"\x01"], [], []
+    pos = 1
+    for i, k in enumerate(kinds):
+        r = _record("AB"[k], 1) if odd == i else recs["AB"[k]]
+        offs.append(pos)
+        parts.append(r)
+        pos += len(r)
+        nvox.append((1 if k == 0 else 12) + (1 if odd == i else 0))
+    return np.frombuffer(b"".join(parts), np.uint8).copy(), np.array(nvox), np.array(offs)
+
+
+def test_uniform_records_found_by_the_parallel_walk(pkg):
+    assert len(_record("A")) == len(_record("B"))
+    raw, nvox, offs = _uniform_tile(20000, 3)
+    assert pkg.tdp.raw_check(raw) == (20000, nvox.sum())
+    # the tile ends 77 records early: the last chunk stops at the end
+    assert pkg.tdp.raw_check(raw[:offs[-77]]) == (20000 - 77, nvox[:-77].sum())
+
+
+@pytest.mark.parametrize("odd", [1, 7000, 19999])
+def test_a_longer_record_breaks_the_guessed_starts(pkg, odd):
+    raw, nvox, _ = _uniform_tile(20000, 4, odd=odd)
+    assert pkg.tdp.raw_check(raw) == (20000, nvox.sum())
+
+
+def test_errors_inside_guessed_chunks(pkg):
+    raw, _, offs = _uniform_tile(20000, 5)
+    b = raw.copy()
+    p = int(offs[17000])
+    (ds,) = struct.unpack_from("<Q", b, p)
+    struct.pack_into("<Q", b, p + 8 + ds, 0)                 # a zero voxel count
+    with pytest.raises(pkg.TdpError) as e:
+        pkg.tdp.raw_check(b)
+    assert str(e.value).endswith("bad voxel count of object 17000")
+    b = raw.copy()
+    for o in (19000, 12345):                                   # inverted boxes: the lowest is named
+        p = int(offs[o])
+        (ds,) = struct.unpack_from("<Q", b, p)
+        struct.pack_into("<f", b, p + 8 + ds + 8 + 40 + 12, -1.0)
+    with pytest.raises(pkg.TdpError) as e:
+        pkg.tdp.raw_check(b)
+    assert str(e.value).endswith("inverted voxel box in object 12345")
