@@ -58,30 +58,23 @@ cudaError_t launch_unpack(const uint8_t* raw, const UnpackSeg* segs, int nseg, f
     return cudaGetLastError();
 }
 
-// out[v + 1] = sum of cnt[0..v] (out[0] = 0), also into stage when given.
-// Returns true when a voxel's triangles do not start 1 byte past a 4-byte
-// boundary of the tile buffer: every field of an object is 4 or 8 bytes and
-// the objects follow the 1-byte type, so the kernels' 4-byte reads rely on it.
-static bool vtri_prefix(const uint64_t* off, const uint32_t* cnt, long n, uint32_t* out, uint32_t* stage) {
-    uint64_t bad = 0;  // in a register: the five LOD threads' flags share a cache line
+// out[v + 1] = sum of cnt[0..v] (out[0] = 0), also into stage when given
+static void vtri_prefix(const uint32_t* cnt, long n, uint32_t* out, uint32_t* stage) {
     uint32_t run = 0;
     out[0] = 0;
     if (stage) {
         stage[0] = 0;
         for (long v = 0; v < n; ++v) {
-            bad |= (off[v] & 3u) ^ 1u;
             run += cnt[v];
             out[v + 1] = run;
             stage[v + 1] = run;
         }
     } else {
         for (long v = 0; v < n; ++v) {
-            bad |= (off[v] & 3u) ^ 1u;
             run += cnt[v];
             out[v + 1] = run;
         }
     }
-    return bad != 0;
 }
 
 // fn(b, e) over [0, n) in a few host threads (one for small n)
@@ -148,7 +141,27 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
     auto ms_since = [](std::chrono::steady_clock::time_point a) {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
     };
-    int rc = parse_raw_dt(buf, len, max_objects, T->host, err);
+    // The metadata go up through the context's page-locked staging buffer,
+    // laid out [voxel records][data-block offsets][vtri x 5][obj_vox][obj_hd]
+    // [obj_phd]; the parser writes the voxel records into it directly.
+    auto stage_bytes = [attach](long n_vox, long n_obj) {
+        return (size_t)n_vox * 3 * sizeof(float4) + (attach ? (size_t)n_obj * sizeof(uint64_t) : 0) +
+               kNumLods * (size_t)(n_vox + 1) * sizeof(uint32_t) + (size_t)(n_obj + 1) * sizeof(uint32_t) +
+               2 * (size_t)n_obj * kNumLods * sizeof(float) + 64;
+    };
+    auto grow_stage = [&](size_t need) {
+        if (need <= ctx->hstage_cap) return;
+        if (ctx->hstage) cudaFreeHost(ctx->hstage);
+        ctx->hstage = nullptr;
+        ctx->hstage_cap = 0;
+        if (cudaHostAlloc(&ctx->hstage, need + need / 4, cudaHostAllocDefault) == cudaSuccess)
+            ctx->hstage_cap = need + need / 4;
+        else { cudaGetLastError(); ctx->hstage = nullptr; }
+    };
+    int rc = parse_raw_dt(buf, len, max_objects, T->host, err, [&](long n_vox, long n_obj) -> float* {
+        grow_stage(stage_bytes(n_vox, n_obj));
+        return (float*)ctx->hstage;  // nullptr when page-locked memory is short
+    });
     T->parse_ms = ms_since(t0);
     if (rc != TDP_OK) {
         delete T;
@@ -195,50 +208,39 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
     T->alloc_ms = ms_since(ta);
     const auto tm = std::chrono::steady_clock::now();
     {
-        // The metadata go up through the context's page-locked staging
-        // buffer, laid out [voxel records][data-block offsets][vtri x 5]
-        // [obj_vox][obj_hd][obj_phd].  Host threads write it directly: one
-        // per LOD computes the prefix of triangle counts (into the tile's
-        // host copy and the staging slot at once) while the others assemble
-        // the voxel records, whose copy then starts while the prefixes finish.
+        // One host thread per LOD writes the prefix of triangle counts (into
+        // the tile's host copy and the staging slot at once) while the voxel
+        // records, already staged by the parser, are copied.
         const size_t v4_bytes = (size_t)H.n_vox * 3 * sizeof(float4);
         const size_t do_bytes = attach ? (size_t)H.n_obj * sizeof(uint64_t) : 0;
         const size_t vt_bytes = (size_t)(H.n_vox + 1) * sizeof(uint32_t);
         const size_t ov_bytes = H.obj_vox_off.size() * 4, hd_bytes = H.obj_hd.size() * 4;
-        const size_t need = v4_bytes + do_bytes + kNumLods * vt_bytes + ov_bytes + 2 * hd_bytes + 64;
-        if (need > ctx->hstage_cap) {
-            if (ctx->hstage) cudaFreeHost(ctx->hstage);
-            ctx->hstage = nullptr;
-            ctx->hstage_cap = 0;
-            if (cudaHostAlloc(&ctx->hstage, need + need / 4, cudaHostAllocDefault) == cudaSuccess)
-                ctx->hstage_cap = need + need / 4;
-            else { cudaGetLastError(); ctx->hstage = nullptr; }
-        }
+        const bool staged = H.vox_box.empty();  // the parser wrote the voxel records into the staging buffer
+        if (!staged) grow_stage(stage_bytes(H.n_vox, H.n_obj));
         uint8_t* stg = (uint8_t*)ctx->hstage;  // nullptr: copy from pageable memory
         uint32_t* vt_stage[kNumLods] = {};
         if (stg)
             for (int l = 0; l < kNumLods; ++l) vt_stage[l] = (uint32_t*)(stg + v4_bytes + do_bytes + l * vt_bytes);
-        bool misaligned[kNumLods] = {false, false, false, false, false};
         std::vector<std::thread> pool;
         for (int l = 0; l < kNumLods; ++l)
             pool.emplace_back([&, l] {
                 HostVec<uint32_t>& vt = T->h_vtri[l];
                 vt.resize(H.n_vox + 1);
-                misaligned[l] = vtri_prefix(H.vox_byte_off[l].data(), H.vox_cnt[l].data(), H.n_vox, vt.data(),
-                                            vt_stage[l]);
+                vtri_prefix(H.vox_cnt[l].data(), H.n_vox, vt.data(), vt_stage[l]);
             });
         std::vector<float4> v4_pageable;
         float4* v4 = nullptr;
         if (stg) v4 = (float4*)stg;
         else { v4_pageable.resize((size_t)H.n_vox * 3); v4 = v4_pageable.data(); }
-        host_parallel(H.n_vox, [&](long b, long e) {
-            for (long v = b; v < e; ++v) {
-                const float* x = &H.vox_box[9 * v];
-                v4[3 * v + 0] = make_float4(x[0], x[1], x[2], 0.f);
-                v4[3 * v + 1] = make_float4(x[3], x[4], x[5], 0.f);
-                v4[3 * v + 2] = make_float4(x[6], x[7], x[8], 0.f);
-            }
-        });
+        if (!staged)
+            host_parallel(H.n_vox, [&](long b, long e) {
+                for (long v = b; v < e; ++v) {
+                    const float* x = &H.vox_box[9 * v];
+                    v4[3 * v + 0] = make_float4(x[0], x[1], x[2], 0.f);
+                    v4[3 * v + 1] = make_float4(x[3], x[4], x[5], 0.f);
+                    v4[3 * v + 2] = make_float4(x[6], x[7], x[8], 0.f);
+                }
+            });
         const void* src_do = H.obj_data_off.data();
         if (stg && attach) {
             std::memcpy(stg + v4_bytes, src_do, do_bytes);
@@ -250,12 +252,6 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
             e = cudaMemcpyAsync(T->lazy_data_off, src_do, do_bytes, cudaMemcpyHostToDevice, s);
         for (auto& th : pool) th.join();
         CTRY(e);
-        for (int l = 0; l < kNumLods; ++l)
-            if (misaligned[l]) {
-                cudaStreamSynchronize(s);
-                tile_release(ctx, T);
-                return fail(ctx, TDP_ERR_FORMAT, "misaligned triangle data");
-            }
         const void* src_vt[kNumLods];
         const void* src_ov = H.obj_vox_off.data();
         const void* src_hd = H.obj_hd.data();

@@ -270,14 +270,7 @@ bool fetchable(const uint8_t* raw, size_t len, const TileHost& h, const uint8_t*
         cudaGetLastError();
         return false;
     }
-    for (long o = 0; o < h.n_obj; ++o) {
-        uint64_t expect = h.obj_data_off[o];
-        for (int l = 0; l < kNumLods; ++l)
-            for (uint32_t v = h.obj_vox_off[o]; v < h.obj_vox_off[o + 1]; ++v) {
-                if (h.vox_byte_off[l][v] != expect) return false;
-                expect += 44ull * h.vox_cnt[l][v];
-            }
-    }
+    if (h.first_noncanonical >= 0) return false;  // checked by the parser
     *dev = (const uint8_t*)dp;
     return true;
 }

@@ -248,7 +248,8 @@ bool walk_chain(const uint8_t* buf, size_t len, size_t& pos, long limit, Rec* ou
 // parallel into arrays sized from the walk.  Content errors are reported for
 // the lowest object that has one, the error the sequential parser would meet
 // first, with the same message.
-int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, std::string& err) {
+int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, std::string& err,
+                 const VoxSink& sink) {
     T = TileHost();
     if (!buf || len < 1) { err = "empty tile buffer"; return TDP_ERR_FORMAT; }
     if (buf[0] != kRawType) return parse_sequential(buf, len, max_objects, T, err);
@@ -327,12 +328,20 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
     T.obj_xf.resize(3 * n);
     T.obj_hd.resize((size_t)kNumLods * n);
     T.obj_phd.resize((size_t)kNumLods * n);
-    T.vox_box.resize(9 * nvox);
+    float* vrec = sink ? sink((long)nvox, n) : nullptr;  // device-layout voxel records
+    if (!vrec) T.vox_box.resize(9 * nvox);
     for (int l = 0; l < kNumLods; ++l) {
         T.vox_byte_off[l].resize(nvox);
         T.vox_cnt[l].resize(nvox);
     }
-    const int nt = (int)std::max<long>(1, std::min<long>((long)std::thread::hardware_concurrency(), n / 256));
+    // chunks of whole objects with about equal voxel counts (a vessel tile
+    // has few objects of many voxels each)
+    const int nt = (int)std::max<long>(
+        1, std::min<long>({(long)std::thread::hardware_concurrency(), (long)(nvox / 2048), n}));
+    std::vector<long> first(nt + 1, n);
+    for (int k = 0; k < nt; ++k)
+        first[k] = std::lower_bound(T.obj_vox_off.begin(), T.obj_vox_off.begin() + n, (uint32_t)(nvox * k / nt)) -
+                   T.obj_vox_off.begin();
     std::vector<long> bad(nt, -1);
     std::vector<std::string> msg(nt);
     std::vector<std::array<uint64_t, kNumLods>> tris(nt);
@@ -350,8 +359,8 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
             const uint64_t* src;
             ~Flush() { for (int l = 0; l < kNumLods; ++l) dst[l] = src[l]; }
         } flush{tris[k], nt_l};
-        const long o_end = n * (k + 1) / nt;
-        for (long o = n * k / nt; o < o_end; ++o) {
+        const long o_end = first[k + 1];
+        for (long o = first[k]; o < o_end; ++o) {
             const Rec& r = recs[o];
             if (o + 4 < o_end) {  // the metadata of a later object, ahead of its turn
                 const Rec& f = recs[o + 4];
@@ -369,8 +378,14 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
             float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
             const uint32_t v0 = T.obj_vox_off[o];
             for (uint64_t v = 0; v < r.vnum; ++v) {
-                float* b = &T.vox_box[9 * (size_t)(v0 + v)];
+                float box[9];
+                float* b = vrec ? box : &T.vox_box[9 * (size_t)(v0 + v)];
                 std::memcpy(b, p, 9 * sizeof(float));
+                if (vrec) {
+                    float* d = vrec + 12 * (size_t)(v0 + v);
+                    const float rec[12] = {b[0], b[1], b[2], 0.f, b[3], b[4], b[5], 0.f, b[6], b[7], b[8], 0.f};
+                    std::memcpy(d, rec, sizeof(rec));
+                }
                 p += 9 * sizeof(float);
                 for (int c = 0; c < 3; ++c) {
                     if (!(b[c] <= b[3 + c])) {

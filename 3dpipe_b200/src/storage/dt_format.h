@@ -19,6 +19,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <memory>
 #include <utility>
@@ -105,9 +106,17 @@ struct TileHost {
     long first_noncanonical = -1;
 };
 
+// Optional destination of the voxel records in the device layout, 12 floats
+// per voxel (low xyz, 0, high xyz, 0, core xyz, 0): called once with the
+// voxel and object counts before the voxel tables are read.  When it returns
+// a pointer, the records go there and vox_box stays empty; when it returns
+// nullptr (or the tile takes the sequential parser), vox_box is filled.
+using VoxSink = std::function<float*(long n_vox, long n_obj)>;
+
 // Parse `len` bytes; at most max_objects objects (<= 0: all).  Returns 0 or a
 // TDP_ERR_* code with a message in `err`.
-int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& out, std::string& err);
+int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& out, std::string& err,
+                 const VoxSink& sink = {});
 
 // Size in bytes of one object's record given its voxel count and per-(lod,voxel)
 // triangle counts (counts[l * nvox + v]).

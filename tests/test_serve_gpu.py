@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from join_cases import tiles
+from rawdt import read_tile, write_tile
 
 pytestmark = pytest.mark.gpu
 
@@ -93,3 +94,27 @@ def test_rejected_requests(pkg, ctx, setup):
         rid = srv.submit(reqs[0][0], query="nn", knn=3)
         q, t, d, _ = srv.wait(rid)
         assert len(q) == 3 * 5
+
+
+def test_page_locked_request_outside_the_writer_layout_is_staged(pkg, ctx, setup):
+    """A page-locked request whose objects keep their LOD blocks in another
+    order cannot be fetched (the fetch computes offsets in the writer's
+    layout): the server stages its triangles, and the result equals the same
+    objects in the writer's layout, which are fetched."""
+    T2, reqs, _ = setup
+    objs = [[list(o.tris[li]) for li in range(5)] for o in read_tile(reqs[5][0])]
+    canonical = pkg.tdp.pinned_copy(write_tile(objs))
+    shuffled = pkg.tdp.pinned_copy(write_tile(objs, lod_order=(4, 3, 2, 1, 0)))
+    out = []
+    for raw in (canonical, shuffled):
+        with pkg.tdp.Server(ctx, T2, arena_objects=100, arena_voxels=1 << 16, arena_tris=1 << 20,
+                            max_request_bytes=64 << 20) as srv:
+            rid = srv.submit(raw, query="within", within=400.0)
+            out.append(srv.wait(rid, timeout_ms=60000)[:3])
+            out.append(srv.stats())
+    (a, st_a, b, st_b) = out
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    assert len(a[0]) > 0
+    assert st_a["fetch_bytes"] > 0 and st_b["fetch_bytes"] == 0, (st_a, st_b)
+    assert st_b["upload_bytes"] > st_a["upload_bytes"]
