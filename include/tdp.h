@@ -145,11 +145,13 @@ typedef struct {
     size_t device_bytes;
     size_t h2d_bytes;      /* bytes the upload / attach itself copied host -> device */
     int attached;          /* 1 for a tile made by tdp_tile_attach */
-    double parse_ms;       /* host time of the upload / attach: parsing the bytes, */
+    double parse_ms;       /* host time of the upload / attach: parsing the bytes
+                              (the parser writes the voxel records into the
+                              page-locked staging buffer),                        */
     double alloc_ms;       /* allocating the device arrays,                       */
     double load_ms;        /* and in total                                        */
-    double meta_ms;        /* of which staging and copying the voxel and object
-                              metadata to the device                              */
+    double meta_ms;        /* of which the prefix sums, the rest of the staging
+                              and the copies of the metadata to the device        */
 } tdp_tile_info;
 int tdp_tile_upload(tdp_ctx *ctx, const void *raw_dt, size_t len, long max_objects, tdp_tile **out);
 /* Attach a RAW tile that stays in page-locked host memory (cudaHostRegister or
