@@ -58,25 +58,6 @@ cudaError_t launch_unpack(const uint8_t* raw, const UnpackSeg* segs, int nseg, f
     return cudaGetLastError();
 }
 
-// out[v + 1] = sum of cnt[0..v] (out[0] = 0), also into stage when given
-static void vtri_prefix(const uint32_t* cnt, long n, uint32_t* out, uint32_t* stage) {
-    uint32_t run = 0;
-    out[0] = 0;
-    if (stage) {
-        stage[0] = 0;
-        for (long v = 0; v < n; ++v) {
-            run += cnt[v];
-            out[v + 1] = run;
-            stage[v + 1] = run;
-        }
-    } else {
-        for (long v = 0; v < n; ++v) {
-            run += cnt[v];
-            out[v + 1] = run;
-        }
-    }
-}
-
 // fn(b, e) over [0, n) in a few host threads (one for small n)
 template <typename Fn>
 static void host_parallel(long n, Fn fn) {
@@ -208,9 +189,9 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
     T->alloc_ms = ms_since(ta);
     const auto tm = std::chrono::steady_clock::now();
     {
-        // One host thread per LOD writes the prefix of triangle counts (into
-        // the tile's host copy and the staging slot at once) while the voxel
-        // records, already staged by the parser, are copied.
+        // The voxel records (staged by the parser) start their copy, then
+        // host threads write the prefix of triangle counts per LOD into the
+        // tile's host copy and the staging slot at once.
         const size_t v4_bytes = (size_t)H.n_vox * 3 * sizeof(float4);
         const size_t do_bytes = attach ? (size_t)H.n_obj * sizeof(uint64_t) : 0;
         const size_t vt_bytes = (size_t)(H.n_vox + 1) * sizeof(uint32_t);
@@ -219,15 +200,12 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
         if (!staged) grow_stage(stage_bytes(H.n_vox, H.n_obj));
         uint8_t* stg = (uint8_t*)ctx->hstage;  // nullptr: copy from pageable memory
         uint32_t* vt_stage[kNumLods] = {};
-        if (stg)
-            for (int l = 0; l < kNumLods; ++l) vt_stage[l] = (uint32_t*)(stg + v4_bytes + do_bytes + l * vt_bytes);
-        std::vector<std::thread> pool;
-        for (int l = 0; l < kNumLods; ++l)
-            pool.emplace_back([&, l] {
-                HostVec<uint32_t>& vt = T->h_vtri[l];
-                vt.resize(H.n_vox + 1);
-                vtri_prefix(H.vox_cnt[l].data(), H.n_vox, vt.data(), vt_stage[l]);
-            });
+        uint32_t* vt_host[kNumLods] = {};
+        for (int l = 0; l < kNumLods; ++l) {
+            T->h_vtri[l].resize(H.n_vox + 1);
+            vt_host[l] = T->h_vtri[l].data();
+            if (stg) vt_stage[l] = (uint32_t*)(stg + v4_bytes + do_bytes + l * vt_bytes);
+        }
         std::vector<float4> v4_pageable;
         float4* v4 = nullptr;
         if (stg) v4 = (float4*)stg;
@@ -246,12 +224,9 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
             std::memcpy(stg + v4_bytes, src_do, do_bytes);
             src_do = stg + v4_bytes;
         }
-        // no early return while the prefix threads run
-        cudaError_t e = cudaMemcpyAsync(T->vox, v4, v4_bytes, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess && attach)
-            e = cudaMemcpyAsync(T->lazy_data_off, src_do, do_bytes, cudaMemcpyHostToDevice, s);
-        for (auto& th : pool) th.join();
-        CTRY(e);
+        CTRY(cudaMemcpyAsync(T->vox, v4, v4_bytes, cudaMemcpyHostToDevice, s));
+        if (attach) CTRY(cudaMemcpyAsync(T->lazy_data_off, src_do, do_bytes, cudaMemcpyHostToDevice, s));
+        vtri_prefix(H, vt_host, vt_stage);
         const void* src_vt[kNumLods];
         const void* src_ov = H.obj_vox_off.data();
         const void* src_hd = H.obj_hd.data();

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -185,6 +186,9 @@ int parse_sequential(const uint8_t* buf, size_t len, long max_objects, TileHost&
     if (T.n_obj == 0) { err = "tile holds no objects"; return TDP_ERR_FORMAT; }
     for (long o = 0; o < T.n_obj && T.first_noncanonical < 0; ++o)
         if (!object_canonical(T, o, T.obj_vox_off[o], T.obj_vox_off[o + 1])) T.first_noncanonical = o;
+    T.chunk_vox = {0, (uint64_t)T.n_vox};
+    T.chunk_tris.assign(1, {});
+    for (int l = 0; l < kNumLods; ++l) T.chunk_tris[0][l] = T.n_tris[l];
     return TDP_OK;
 }
 
@@ -436,7 +440,54 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
     for (int k = 0; k < nt; ++k)
         for (int l = 0; l < kNumLods; ++l) T.n_tris[l] += tris[k][l];
     for (int k = 0; k < nt && T.first_noncanonical < 0; ++k) T.first_noncanonical = noncanon[k];
+    T.chunk_vox.resize(nt + 1);
+    for (int k = 0; k <= nt; ++k) T.chunk_vox[k] = T.obj_vox_off[first[k]];
+    T.chunk_tris = std::move(tris);
     return TDP_OK;
+}
+
+void vtri_prefix(const TileHost& T, uint32_t* const out[kNumLods], uint32_t* const stage[kNumLods]) {
+    const long nk = (long)T.chunk_tris.size();
+    const long tasks = nk * kNumLods;
+    auto run = [&](long task) {
+        const int l = (int)(task % kNumLods);
+        const long k = task / kNumLods;
+        uint64_t base = 0;
+        for (long j = 0; j < k; ++j) base += T.chunk_tris[j][l];
+        const uint32_t* cnt = T.vox_cnt[l].data();
+        uint32_t* o = out[l];
+        uint32_t* st = stage[l];
+        uint32_t run_sum = (uint32_t)base;
+        const uint64_t vb = T.chunk_vox[k], ve = T.chunk_vox[k + 1];
+        if (k == 0) {
+            o[0] = 0;
+            if (st) st[0] = 0;
+        }
+        if (st) {
+            for (uint64_t v = vb; v < ve; ++v) {
+                run_sum += cnt[v];
+                o[v + 1] = run_sum;
+                st[v + 1] = run_sum;
+            }
+        } else {
+            for (uint64_t v = vb; v < ve; ++v) {
+                run_sum += cnt[v];
+                o[v + 1] = run_sum;
+            }
+        }
+    };
+    const long nt = std::min<long>(tasks, std::max<long>(1, (long)std::thread::hardware_concurrency()));
+    if (nt <= 1) {
+        for (long t = 0; t < tasks; ++t) run(t);
+        return;
+    }
+    std::atomic<long> next{0};
+    std::vector<std::thread> pool;
+    for (long i = 0; i < nt; ++i)
+        pool.emplace_back([&] {
+            for (long t = next++; t < tasks; t = next++) run(t);
+        });
+    for (auto& th : pool) th.join();
 }
 
 }  // namespace tdp

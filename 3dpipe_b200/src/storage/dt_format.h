@@ -17,6 +17,7 @@
 //
 // The object's box is the union of its voxel boxes (himesh_wrapper.cpp:40, :80).
 #pragma once
+#include <array>
 #include <cstddef>
 #include <cstdint>
 #include <functional>
@@ -104,7 +105,17 @@ struct TileHost {
     // (the layout the reference's writer produces, src/storage/tile_IO.cpp:79-172); -1
     // when every object does
     long first_noncanonical = -1;
+    // the parser's chunks: chunk k holds voxels [chunk_vox[k], chunk_vox[k + 1])
+    // and chunk_tris[k][l] triangles at LOD index l
+    std::vector<uint64_t> chunk_vox;
+    std::vector<std::array<uint64_t, kNumLods>> chunk_tris;
 };
+
+// out[l][v] = triangles at LOD index l in voxels [0, v), for v in [0, n_vox]
+// (out[l] holds n_vox + 1 entries), written also to stage[l] where that is
+// not null: host threads over (LOD, parser chunk) tasks, each chunk starting
+// from the triangle totals of the chunks before it.
+void vtri_prefix(const TileHost& T, uint32_t* const out[kNumLods], uint32_t* const stage[kNumLods]);
 
 // Optional destination of the voxel records in the device layout, 12 floats
 // per voxel (low xyz, 0, high xyz, 0, core xyz, 0): called once with the
