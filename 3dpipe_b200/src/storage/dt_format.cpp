@@ -92,6 +92,12 @@ size_t host_cache_bytes() {
     return c.cached;
 }
 
+void host_cache_trim() {
+    HostBlockCache& c = host_cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    host_cache_shrink(c, 0);
+}
+
 namespace {
 template <typename T>
 bool rd(const uint8_t* buf, size_t len, size_t& pos, T& v) {
@@ -533,3 +539,6 @@ extern "C" int tdp_raw_check(const void* raw, size_t len, long* n_objects, long*
     }
     return rc;
 }
+
+extern "C" size_t tdp_host_cache_bytes(void) { return tdp::host_cache_bytes(); }
+extern "C" void tdp_host_cache_trim(void) { tdp::host_cache_trim(); }

@@ -49,6 +49,7 @@ constexpr size_t kHostCacheMax = size_t(4) << 30;
 void* host_block_get(size_t bytes);  // throws std::bad_alloc
 void host_block_put(void* p, size_t bytes);
 size_t host_cache_bytes();           // freed bytes held by the cache now
+void host_cache_trim();              // free every cached block
 
 // An allocator whose resize() leaves new elements of plain types
 // uninitialised: the parser writes every element from its own threads, so a

@@ -354,7 +354,8 @@ EXPORTED += ["tdp_fp32_peak", "tdp_refine_batch_noalloc", "tdp_tile_candidates",
 LOD_GRAPH_OFF, LOD_GRAPH_AUTO, LOD_GRAPH_ALWAYS = 0, 1, 2
 
 EXPORTED += ["tdp_tile_compute_bounds", "tdp_raw_compute_bounds", "tdp_tile_attach", "tdp_host_alloc",
-             "tdp_host_free", "tdp_raw_check", "tdp_get_refine_config_lod"]
+             "tdp_host_free", "tdp_raw_check", "tdp_get_refine_config_lod", "tdp_host_cache_bytes",
+             "tdp_host_cache_trim"]
 
 CTX_POISON = 1  # tdp_ctx_create flag: unfetched records of attached tiles read as NaN
 
@@ -372,6 +373,22 @@ def raw_check(raw):
     if rc != TDP_OK:
         raise TdpError(rc, err.value.decode())
     return no.value, nv.value
+
+
+def host_cache_bytes() -> int:
+    """Freed host bytes the parser's process-wide block cache holds now."""
+    L = lib()
+    L.tdp_host_cache_bytes.restype = C.c_size_t
+    L.tdp_host_cache_bytes.argtypes = []
+    return int(L.tdp_host_cache_bytes())
+
+
+def host_cache_trim() -> None:
+    """Hand every block of the parser's host block cache back to the system."""
+    L = lib()
+    L.tdp_host_cache_trim.restype = None
+    L.tdp_host_cache_trim.argtypes = []
+    L.tdp_host_cache_trim()
 
 
 def pinned_empty(nbytes: int) -> np.ndarray:

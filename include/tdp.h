@@ -173,6 +173,13 @@ int tdp_raw_check(const void *raw, size_t len, long *n_objects, long *n_voxels, 
 /* page-locked host memory (cudaHostAlloc) to read tiles into for attaching */
 int tdp_host_alloc(size_t bytes, void **out);
 int tdp_host_free(void *p);
+/* The parser's large host arrays (1 MiB and up) are recycled through a
+ * process-wide cache of freed blocks, at most 4 GiB: repeated uploads and
+ * attaches then pay no page faults on fresh memory.  No reference
+ * counterpart.  tdp_host_cache_bytes: freed bytes the cache holds now;
+ * tdp_host_cache_trim: hand them all back to the system. */
+size_t tdp_host_cache_bytes(void);
+void tdp_host_cache_trim(void);
 int tdp_tile_free(tdp_ctx *ctx, tdp_tile *tile);
 int tdp_tile_get_info(const tdp_tile *tile, tdp_tile_info *out);
 

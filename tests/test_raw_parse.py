@@ -157,3 +157,19 @@ def test_errors_inside_guessed_chunks(pkg):
     with pytest.raises(pkg.TdpError) as e:
         pkg.tdp.raw_check(b)
     assert str(e.value).endswith("inverted voxel box in object 12345")
+
+
+def test_host_block_cache_recycles_and_trims(pkg):
+    """The parser's arrays of 1 MiB and up go back to the process-wide block
+    cache when a parse ends, are reused by the next parse of the same tile,
+    and are handed back to the system on request."""
+    raw, nvox, _ = _uniform_tile(40000, 6)      # ~260k voxels: the per-voxel offset arrays exceed 1 MiB
+    pkg.tdp.host_cache_trim()
+    assert pkg.tdp.host_cache_bytes() == 0
+    assert pkg.tdp.raw_check(raw) == (40000, nvox.sum())
+    held = pkg.tdp.host_cache_bytes()
+    assert held > 0
+    assert pkg.tdp.raw_check(raw) == (40000, nvox.sum())
+    assert pkg.tdp.host_cache_bytes() == held    # the second parse took its blocks from the cache and gave them back
+    pkg.tdp.host_cache_trim()
+    assert pkg.tdp.host_cache_bytes() == 0
