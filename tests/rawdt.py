@@ -89,3 +89,61 @@ def write_tile(objects, lod_order=(0, 1, 2, 3, 4)):
             out += np.concatenate([lo, hi, pts[0]]).astype(np.float32).tobytes() + offc[v].tobytes()
         out += np.zeros(3, np.float32).tobytes()
     return np.frombuffer(bytes(out), np.uint8).copy()
+
+
+def first_problem(b, pos=1, obj=0, resume=None):
+    """Restatement of a sequential read of RAW tile bytes (the order and the
+    messages of the reader the C++ parser reports for, after the reference's
+    HiMesh_Wrapper(char*, id, RAW), src/spatial/himesh_wrapper.cpp:17-83),
+    starting at byte `pos` with object id `obj`.  `resume` maps byte offsets
+    to the ids of records known to be intact from there to the end: reaching
+    one ends the read.  Returns ("error", message) or ("ok", objects read,
+    voxels read, id of the intact record reached or None)."""
+    mv = memoryview(b)
+    n = len(mv)
+    nvox = 0
+    start = obj
+
+    def u64(p):
+        return struct.unpack_from("<Q", mv, p)[0] if p + 8 <= n else None
+
+    while pos < n:
+        if resume is not None and pos in resume:
+            return ("ok", obj - start, nvox, resume[pos])
+        ds = u64(pos)
+        if ds is None:
+            return ("error", f"truncated data_size of object {obj}")
+        pos += 8
+        if ds > n - pos or ds % 4:
+            return ("error", f"bad data_size of object {obj}")
+        pos += ds
+        vn = u64(pos)
+        if vn is None or vn == 0 or vn > (1 << 24):
+            return ("error", f"bad voxel count of object {obj}")
+        pos += 8
+        if pos + 40 > n:
+            return ("error", "truncated object hausdorff")
+        pos += 40
+        for _ in range(vn):
+            if pos + 36 > n:
+                return ("error", f"truncated voxel record of object {obj}")
+            box = struct.unpack_from("<9f", mv, pos)
+            pos += 36
+            for k in range(3):
+                if not (box[k] <= box[3 + k]):
+                    return ("error", f"inverted voxel box in object {obj}")
+            for _ in range(5):
+                if pos + 16 > n:
+                    return ("error", "truncated voxel lod table")
+                off, cnt = struct.unpack_from("<QQ", mv, pos)
+                pos += 16
+                if cnt > (1 << 24) or off % 4 or off > ds or cnt * 44 > ds - off:
+                    return ("error", f"voxel lod range outside data block in object {obj}")
+        if pos + 12 > n:
+            return ("error", f"truncated transform of object {obj}")
+        pos += 12
+        nvox += vn
+        obj += 1
+    if obj == 0:
+        return ("error", "tile holds no objects")
+    return ("ok", obj - start, nvox, None)

@@ -173,3 +173,43 @@ def test_host_block_cache_recycles_and_trims(pkg):
     assert pkg.tdp.host_cache_bytes() == held    # the second parse took its blocks from the cache and gave them back
     pkg.tdp.host_cache_trim()
     assert pkg.tdp.host_cache_bytes() == 0
+
+
+def test_random_corruptions_report_what_a_sequential_read_finds(pkg):
+    """Random byte changes in a tile of equal-size records (walked by the
+    parser's threads from guessed starts): the parser reports the first
+    problem a sequential read meets, or the counts it reads."""
+    from rawdt import first_problem
+    n = 12000
+    raw, nvox, offs = _uniform_tile(n, 7)
+    rec_len = len(_record("A"))
+    rng = np.random.default_rng(11)
+    for trial in range(200):
+        b = raw.copy()
+        r = int(rng.integers(0, n))
+        p = int(offs[r])
+        (ds,) = struct.unpack_from("<Q", b, p)
+        if trial % 2:   # a header field: sizes, bounds, voxel records, lod tables, transform
+            at = p + int(rng.choice([0, 8 + ds + int(rng.integers(0, rec_len - 8 - ds))]))
+        else:
+            at = p + int(rng.integers(0, rec_len))
+        b[at] = (int(b[at]) + int(rng.integers(1, 256))) % 256
+        if trial % 5 == 4:                      # also cut the tile short somewhere after it
+            b = b[: int(rng.integers(at + 1, len(b) + 1))]
+        resume = {int(o): i for i, o in enumerate(offs) if o > at and o + rec_len <= len(b)}
+        want = first_problem(b, p, r, resume)
+        if want[0] == "ok":
+            k = want[3]
+            tail_objs = (n - k) if k is not None else 0
+            tail_vox = int(nvox[k:].sum()) if k is not None else 0
+            if k is not None and int(offs[-1]) + rec_len > len(b):   # the cut reaches the intact records
+                want = first_problem(b, p, r)
+                tail_objs, tail_vox = 0, 0
+        if want[0] == "error":
+            with pytest.raises(pkg.TdpError) as e:
+                pkg.tdp.raw_check(b)
+            assert e.value.code == 4
+            assert str(e.value).endswith(want[1]), (trial, str(e.value), want)
+        else:
+            got = pkg.tdp.raw_check(b)
+            assert got == (r + want[1] + tail_objs, int(nvox[:r].sum()) + want[2] + tail_vox), (trial, got, want)
