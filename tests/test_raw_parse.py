@@ -175,41 +175,57 @@ def test_host_block_cache_recycles_and_trims(pkg):
     assert pkg.tdp.host_cache_bytes() == 0
 
 
-def test_random_corruptions_report_what_a_sequential_read_finds(pkg):
-    """Random byte changes in a tile of equal-size records (walked by the
-    parser's threads from guessed starts): the parser reports the first
-    problem a sequential read meets, or the counts it reads."""
+def _record_table(raw):
+    """(record offsets plus the end, voxels per record) of RAW tile bytes"""
+    offs, pos = [], 1
+    nvox = []
+    while pos < len(raw):
+        offs.append(pos)
+        (ds,) = struct.unpack_from("<Q", raw, pos)
+        (vn,) = struct.unpack_from("<Q", raw, pos + 8 + ds)
+        nvox.append(vn)
+        pos += 8 + ds + 8 + 40 + 116 * vn + 12
+    return np.array(offs + [pos]), np.array(nvox)
+
+
+@pytest.mark.parametrize("tile", ["equal-size records", "generated nuclei"])
+def test_random_corruptions_report_what_a_sequential_read_finds(pkg, tile):
+    """Random byte changes, some with the tile cut short after them: the
+    parser reports the first problem a sequential read meets, or the counts
+    it reads.  Equal-size records are walked by the parser's threads from
+    guessed starts; the generated tile's records differ in size."""
     from rawdt import first_problem
-    n = 12000
-    raw, nvox, offs = _uniform_tile(n, 7)
-    rec_len = len(_record("A"))
+    if tile == "equal-size records":
+        raw, _, _ = _uniform_tile(12000, 7)
+    else:
+        raw, _ = pkg.tdp.gen_tiles(3, 200, seed=8)
+        raw = np.array(raw)
+    ends, nvox = _record_table(raw)
+    offs, n = ends[:-1], len(ends) - 1
     rng = np.random.default_rng(11)
     for trial in range(200):
-        b = raw.copy()
         r = int(rng.integers(0, n))
-        p = int(offs[r])
-        (ds,) = struct.unpack_from("<Q", b, p)
-        if trial % 2:   # a header field: sizes, bounds, voxel records, lod tables, transform
-            at = p + int(rng.choice([0, 8 + ds + int(rng.integers(0, rec_len - 8 - ds))]))
+        p, q = int(offs[r]), int(ends[r + 1])
+        (ds,) = struct.unpack_from("<Q", raw, p)
+        if trial % 2:   # a field outside the data block: sizes, bounds, voxel records, lod tables, transform
+            at = p + int(rng.choice([0, 8 + ds + int(rng.integers(0, q - p - 8 - ds))]))
         else:
-            at = p + int(rng.integers(0, rec_len))
-        b[at] = (int(b[at]) + int(rng.integers(1, 256))) % 256
-        if trial % 5 == 4:                      # also cut the tile short somewhere after it
-            b = b[: int(rng.integers(at + 1, len(b) + 1))]
-        resume = {int(o): i for i, o in enumerate(offs) if o > at and o + rec_len <= len(b)}
+            at = p + int(rng.integers(0, q - p))
+        old = int(raw[at])
+        raw[at] = (old + int(rng.integers(1, 256))) % 256   # changed in place, restored below
+        cut = trial % 5 == 4
+        b = raw[: int(rng.integers(at + 1, len(raw) + 1))] if cut else raw
+        # records after the changed byte are intact up to the end (or the cut)
+        resume = None if cut else {int(o): i for i, o in enumerate(offs) if o > at}
         want = first_problem(b, p, r, resume)
-        if want[0] == "ok":
-            k = want[3]
-            tail_objs = (n - k) if k is not None else 0
-            tail_vox = int(nvox[k:].sum()) if k is not None else 0
-            if k is not None and int(offs[-1]) + rec_len > len(b):   # the cut reaches the intact records
-                want = first_problem(b, p, r)
-                tail_objs, tail_vox = 0, 0
         if want[0] == "error":
             with pytest.raises(pkg.TdpError) as e:
                 pkg.tdp.raw_check(b)
             assert e.value.code == 4
             assert str(e.value).endswith(want[1]), (trial, str(e.value), want)
         else:
-            got = pkg.tdp.raw_check(b)
-            assert got == (r + want[1] + tail_objs, int(nvox[:r].sum()) + want[2] + tail_vox), (trial, got, want)
+            k = want[3]
+            objs = r + want[1] + (n - k if k is not None else 0)
+            vox = int(nvox[:r].sum()) + want[2] + (int(nvox[k:].sum()) if k is not None else 0)
+            assert pkg.tdp.raw_check(b) == (objs, vox), (trial, want)
+        raw[at] = old
