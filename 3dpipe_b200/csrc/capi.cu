@@ -154,7 +154,10 @@ int tdp_ctx_destroy(tdp_ctx* ctx) {
     if (ctx->lod_graph) cudaGraphExecDestroy(ctx->lod_graph);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->hres) cudaFreeHost(ctx->hres);
-    if (ctx->hstage) cudaFreeHost(ctx->hstage);
+    for (int k = 0; k < 2; ++k) {
+        if (ctx->hstage[k]) cudaFreeHost(ctx->hstage[k]);
+        if (ctx->hstage_ev[k]) cudaEventDestroy(ctx->hstage_ev[k]);
+    }
     delete ctx;
     return TDP_OK;
 }

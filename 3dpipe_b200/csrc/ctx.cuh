@@ -77,8 +77,13 @@ struct tdp_ctx {
     // budget, and on destroy.
     std::multimap<size_t, void*> block_cache;
     size_t cached_bytes = 0;
-    void* hstage = nullptr;  // page-locked staging of tile metadata uploads (grow-only)
-    size_t hstage_cap = 0;
+    // page-locked staging of tile metadata (grow-only): two buffers taken in
+    // turn, each with an event recorded after its last copy, so an attach
+    // returns while its copies run and the next attach stages into the other
+    void* hstage[2] = {nullptr, nullptr};
+    size_t hstage_cap[2] = {0, 0};
+    cudaEvent_t hstage_ev[2] = {nullptr, nullptr};
+    int hstage_next = 0;
 };
 
 namespace tdp {

@@ -122,26 +122,33 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
     auto ms_since = [](std::chrono::steady_clock::time_point a) {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
     };
-    // The metadata go up through the context's page-locked staging buffer,
-    // laid out [voxel records][data-block offsets][vtri x 5][obj_vox][obj_hd]
-    // [obj_phd]; the parser writes the voxel records into it directly.
+    // The metadata go up through one of the context's two page-locked staging
+    // buffers, laid out [voxel records][data-block offsets][vtri x 5]
+    // [obj_vox][obj_hd][obj_phd]; the parser writes the voxel records into it
+    // directly.  The buffer is written only once its previous copies are done.
+    const int slot = ctx->hstage_next;
+    ctx->hstage_next ^= 1;
+    auto wait_slot = [&] {
+        if (ctx->hstage_ev[slot]) cudaEventSynchronize(ctx->hstage_ev[slot]);
+    };
     auto stage_bytes = [attach](long n_vox, long n_obj) {
         return (size_t)n_vox * 3 * sizeof(float4) + (attach ? (size_t)n_obj * sizeof(uint64_t) : 0) +
                kNumLods * (size_t)(n_vox + 1) * sizeof(uint32_t) + (size_t)(n_obj + 1) * sizeof(uint32_t) +
                2 * (size_t)n_obj * kNumLods * sizeof(float) + 64;
     };
     auto grow_stage = [&](size_t need) {
-        if (need <= ctx->hstage_cap) return;
-        if (ctx->hstage) cudaFreeHost(ctx->hstage);
-        ctx->hstage = nullptr;
-        ctx->hstage_cap = 0;
-        if (cudaHostAlloc(&ctx->hstage, need + need / 4, cudaHostAllocDefault) == cudaSuccess)
-            ctx->hstage_cap = need + need / 4;
-        else { cudaGetLastError(); ctx->hstage = nullptr; }
+        wait_slot();
+        if (need <= ctx->hstage_cap[slot]) return;
+        if (ctx->hstage[slot]) cudaFreeHost(ctx->hstage[slot]);
+        ctx->hstage[slot] = nullptr;
+        ctx->hstage_cap[slot] = 0;
+        if (cudaHostAlloc(&ctx->hstage[slot], need + need / 4, cudaHostAllocDefault) == cudaSuccess)
+            ctx->hstage_cap[slot] = need + need / 4;
+        else { cudaGetLastError(); ctx->hstage[slot] = nullptr; }
     };
     int rc = parse_raw_dt(buf, len, max_objects, T->host, err, [&](long n_vox, long n_obj) -> float* {
         grow_stage(stage_bytes(n_vox, n_obj));
-        return (float*)ctx->hstage;  // nullptr when page-locked memory is short
+        return (float*)ctx->hstage[slot];  // nullptr when page-locked memory is short
     });
     T->parse_ms = ms_since(t0);
     if (rc != TDP_OK) {
@@ -198,7 +205,7 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
         const size_t ov_bytes = H.obj_vox_off.size() * 4, hd_bytes = H.obj_hd.size() * 4;
         const bool staged = H.vox_box.empty();  // the parser wrote the voxel records into the staging buffer
         if (!staged) grow_stage(stage_bytes(H.n_vox, H.n_obj));
-        uint8_t* stg = (uint8_t*)ctx->hstage;  // nullptr: copy from pageable memory
+        uint8_t* stg = (uint8_t*)ctx->hstage[slot];  // nullptr: copy from pageable memory
         uint32_t* vt_stage[kNumLods] = {};
         uint32_t* vt_host[kNumLods] = {};
         for (int l = 0; l < kNumLods; ++l) {
@@ -253,8 +260,12 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
                 for (int l = 0; l < kNumLods; ++l)
                     CTRY(cudaMemsetAsync(T->tri[l], 0xff, (size_t)H.n_tris[l] * 3 * sizeof(float4), s));
         }
-        // the staging buffer is free for the next tile once this returns
-        CTRY(cudaStreamSynchronize(s));
+        // An attach returns with its copies queued: every later use of the
+        // tile is ordered after them on the context's stream, and the event
+        // keeps this staging buffer from being rewritten before they finish.
+        if (!ctx->hstage_ev[slot]) CTRY(cudaEventCreateWithFlags(&ctx->hstage_ev[slot], cudaEventDisableTiming));
+        CTRY(cudaEventRecord(ctx->hstage_ev[slot], s));
+        if (!attach || !stg) CTRY(cudaStreamSynchronize(s));
     }
     T->meta_ms = ms_since(tm);
     if (attach) {
