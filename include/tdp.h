@@ -151,12 +151,15 @@ typedef struct {
     double alloc_ms;       /* allocating the device arrays,                       */
     double load_ms;        /* and in total                                        */
     double meta_ms;        /* of which the prefix sums, the rest of the staging
-                              and the copies of the metadata to the device        */
+                              and the copies of the metadata to the device (for
+                              an attach: queuing them, not their completion)      */
 } tdp_tile_info;
 int tdp_tile_upload(tdp_ctx *ctx, const void *raw_dt, size_t len, long max_objects, tdp_tile **out);
 /* Attach a RAW tile that stays in page-locked host memory (cudaHostRegister or
  * cudaHostAlloc covering all len bytes; it must outlive the tile): only the
- * voxel and object metadata are copied now; each join copies, LOD by LOD, the
+ * voxel and object metadata are copied now (the call may return with those
+ * copies still queued on the context's stream, tdp_ctx_stream, which every
+ * later call on the context is ordered after); each join copies, LOD by LOD, the
  * triangles of the voxels its refine touches, straight from the host bytes,
  * and keeps them for later joins on the tile.  This is the reference's
  * per-LOD staging of the voxels a chunk needs (build_chunks_by_pair /
