@@ -65,7 +65,9 @@ int main(int argc, char** argv) {
         else if (a == "--max_objects2") max2 = std::atol(val());
         else if (a == "--form") {
             std::string f = val();
-            p.form = f == "plain" ? TDP_FORM_PLAIN : TDP_FORM_TUNED;
+            if (f == "plain") p.form = TDP_FORM_PLAIN;
+            else if (f == "tuned") p.form = TDP_FORM_TUNED;
+            else { std::fprintf(stderr, "unknown form %s (plain or tuned)\n", f.c_str()); return 2; }
         } else if (a == "--device") device = std::atoi(val());
         else if (a == "-g" || a == "--gpu" || a == "--aabb") {
         } else if (a == "-t" || a == "--threads" || a == "--cn" || a == "-v" || a == "--verbose") val();
