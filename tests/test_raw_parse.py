@@ -229,3 +229,32 @@ def test_random_corruptions_report_what_a_sequential_read_finds(pkg, tile):
             vox = int(nvox[:r].sum()) + want[2] + (int(nvox[k:].sum()) if k is not None else 0)
             assert pkg.tdp.raw_check(b) == (objs, vox), (trial, want)
         raw[at] = old
+
+
+def test_concurrent_parses_share_the_block_cache(pkg):
+    """Parses on several threads at once (as request submissions to a server
+    run): each returns its own tile's counts while they take blocks from,
+    and give them back to, the one process-wide cache."""
+    import threading
+    tiles = [_uniform_tile(n, seed) for n, seed in ((9000, 31), (12000, 32), (3000, 33), (20000, 34))]
+    want = [(len(offs), int(nvox.sum())) for _, nvox, offs in tiles]
+    errors = []
+
+    def worker(k):
+        try:
+            for i in range(6):
+                j = (k + i) % len(tiles)
+                got = pkg.tdp.raw_check(tiles[j][0])
+                if got != want[j]:
+                    errors.append((k, j, got))
+        except Exception as e:  # noqa: BLE001 -- reported below
+            errors.append((k, repr(e)))
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(8)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    assert not errors, errors[:3]
+    pkg.tdp.host_cache_trim()
+    assert pkg.tdp.host_cache_bytes() == 0
