@@ -105,6 +105,13 @@ def build_oracle(with_reference: bool = True) -> None:
                            capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"reference build failed:\n{r.stdout}\n{r.stderr}")
+        # the reference's own GPU join (a comparison baseline, never on a test
+        # or product path): a failure here is reported, not fatal
+        r = subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "refgpu", f"REF={ref}"],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            print(f"note: the reference GPU join (oracle/_ref/tdbase_ref_gpu) did not build:\n{r.stderr[-2000:]}",
+                  file=sys.stderr)
 
 
 if __name__ == "__main__":
