@@ -99,7 +99,12 @@ def build_oracle(with_reference: bool = True) -> None:
     r = subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
-    ref = Path(os.environ.get("TDP_REFERENCE", "/root/reference"))
+    ref_env = os.environ.get("TDP_REFERENCE")
+    if not ref_env:
+        # the oracle recipe names the reference tree it reads by default
+        r = subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "print-ref"], capture_output=True, text=True)
+        ref_env = r.stdout.strip() if r.returncode == 0 else ""
+    ref = Path(ref_env) if ref_env else Path("/nonexistent")
     if with_reference and (ref / "src" / "geometry" / "computing_cpu.cpp").exists():
         r = subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", f"REF={ref}"],
                            capture_output=True, text=True)

@@ -21,7 +21,7 @@ constexpr int kTriF4 = 3;
 // FP32 forward-error model for one voxel-pair distance: |d32 - d| <= kErrC * u * R,
 // u = 2^-24, R = largest |coordinate| after translation to the pair's origin
 // (the .w of the refine output).  kErrC is 8x the largest ratio measured
-// against the FP64 oracle (tests/test_tridist_gpu.py records the measurement).
+// against the FP64 oracle (tests/test_refine_gpu.py prints the measured ratio).
 constexpr float kErrC = 64.0f;
 constexpr float kUnitRoundoff = 5.9604645e-8f;
 

@@ -13,14 +13,21 @@
 // cudaFree or any allocating library routine.
 //
 // Limits: at most kNoAllocMaxTris triangles and kNoAllocMaxPairs voxel pairs
-// per call (the array holds 14.3 MB; every GPU that loads this library keeps
-// it until the process exits).  Larger batches are rejected with an error.
+// per call (the array holds kScratchBytes = 14,680,320 bytes, 14.0 MiB; every
+// GPU that loads this library keeps it until the process exits).  Larger
+// batches are rejected with an error.
+//
+// Kernel: the tuned refine in its configuration 0 (eager staging, A chunk of
+// 64 triangles, 3 CTAs per SM) -- a call has no context, so no autotuner pick
+// applies.  Its minima equal those of every other tuned configuration.
 //
 // Set-up: the first call on each device looks up the array's device address
-// with cudaGetSymbolAddress while that device is current, and caches it; make
-// that first call before any stream capture begins.  All calls on a device
-// share the one array and each call overwrites it, so calls whose work can
-// overlap on the GPU (other streams, other host threads) race: serialise them.
+// with cudaGetSymbolAddress while that device is current, and caches it; the
+// first launch of the tuned kernel in a process also raises its dynamic
+// shared-memory limit (cudaFuncSetAttribute).  Make that first call before any
+// stream capture begins.  All calls on a device share the one array and each
+// call overwrites it, so calls whose work can overlap on the GPU (other
+// streams, other host threads) race: serialise them.
 #include <float.h>
 
 #include <algorithm>

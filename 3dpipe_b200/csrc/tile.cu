@@ -178,6 +178,10 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
         return TDP_OK;
     };
     cudaStream_t s = ctx->stream;
+    // CTRY synchronises the stream before it returns an error: copies already
+    // queued from the staging slot have finished by then, so the slot's event
+    // (recorded only on success) cannot let a later attach rewrite page-locked
+    // memory that a queued copy still reads.
 #define TRY(x) do { int _r = (x); if (_r) { tile_release(ctx, T); return _r; } } while (0)
 #define CTRY(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { cudaStreamSynchronize(s); tile_release(ctx, T); return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } } while (0)
     TRY(alloc((void**)&T->vox, (size_t)H.n_vox * 3 * sizeof(float4)));

@@ -150,6 +150,42 @@ def make_tiles(rank, ws):
     return nb, vb
 
 
+def base_config():
+    """The workload keys both arms print in `config`."""
+    return {"workload": WORKLOAD, "n_nuclei": N_VESSELS * NUCLEI_PER_VESSEL, "n_vessels": N_VESSELS, "tau": TAU,
+            "seed": SEED, "query": "within", "lods": [20, 40, 60, 80, 100], "hausdorff_level": 2}
+
+
+def make_tiles_isolated():
+    """Generate the tiles in a child process and read their bytes through a
+    pipe, so that the reference arm's own process never loads this
+    repository's library."""
+    code = ("import sys, importlib; sys.path.insert(0, %r); pkg = importlib.import_module('3dpipe_b200'); "
+            "nb, vb, _ = pkg.shard.gen_shard_tiles(0, 1, %d, %d, %d); o = sys.stdout.buffer; "
+            "o.write(int(nb.size).to_bytes(8, 'little')); o.write(int(vb.size).to_bytes(8, 'little')); "
+            "o.write(memoryview(nb)); o.write(memoryview(vb)); o.flush()"
+            % (str(ROOT), N_VESSELS, NUCLEI_PER_VESSEL, SEED))
+    t = time.time()
+    p = subprocess.Popen([sys.executable, "-c", code], stdout=subprocess.PIPE)
+    hdr = p.stdout.read(16)
+    if len(hdr) != 16:
+        p.wait()
+        raise SystemExit(f"tile generator exited with {p.returncode}")
+    bufs = [np.empty(int.from_bytes(hdr[:8], "little"), np.uint8), np.empty(int.from_bytes(hdr[8:], "little"), np.uint8)]
+    for b in bufs:
+        mv, off = memoryview(b), 0
+        while off < b.size:
+            n = p.stdout.readinto(mv[off:off + (1 << 26)])
+            if not n:
+                raise SystemExit("tile generator pipe closed early")
+            off += n
+    if p.wait() != 0:
+        raise SystemExit(f"tile generator exited with {p.returncode}")
+    log(f"[reference] generated {bufs[0].size / 1e9:.2f} + {bufs[1].size / 1e9:.2f} GB in a child process "
+        f"in {time.time() - t:.1f}s")
+    return bufs[0], bufs[1]
+
+
 def cpu_reference(nb, vb, steps, warmup, sample_queries, target_s=15.0):
     """The reference's CPU implementation (oracle/_ref) on a bounded sample of
     query nuclei, sized so one run takes about target_s seconds."""
@@ -180,6 +216,52 @@ def cpu_reference(nb, vb, steps, warmup, sample_queries, target_s=15.0):
                       + ("" if sample >= n_total else
                          f"; join seconds for all nuclei extrapolate linearly to {last[0] * n_total / sample:.0f} s"),
             "seconds_per_sample": last[0], "tri_pairs_per_sample": last[1]}
+
+
+def check_parity(nb, vb, q, t):
+    """The tuned form's within-400 result set against the reference's join
+    rules (oracle/_ref: its octree and FP32 MeshDist, all host cores) on the
+    whole join; exits when they differ."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_bind import ref_join
+    r = ref_join(nb, vb, False, False, tau=TAU, threads=os.cpu_count() or 1)
+    if r is None:
+        return {"checked": False, "why": "oracle/_ref was not built"}
+    got = set(zip(q.tolist(), t.tolist()))
+    ref = set(zip(r[0].tolist(), r[1].tolist()))
+    out = {"checked": True, "ref_rules_equal": got == ref, "results": len(got), "ref_results": len(ref),
+           "only_ours": len(got - ref), "only_ref": len(ref - got), "queries": "all",
+           "ref_seconds": r[2][0]}
+    log(f"parity within-{TAU:g}: {out}")
+    if got != ref:
+        print(json.dumps({"parity_failure": out}), file=sys.stderr)
+        raise SystemExit("the tuned result set differs from the reference rules' set")
+    return out
+
+
+def check_parity_self_sample(nb, q, t, n_sample):
+    """The 10-NN self-join's lists for a stratified sample of query nuclei
+    (every n/n_sample-th, from 137) against the reference rules run for
+    exactly those queries; exits when they differ."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_bind import ref_join
+    n = int(q.max()) + 1 if len(q) else 0
+    step = max(1, n // max(1, n_sample))
+    sample = np.arange(137 % step, n, step, dtype=np.int32)
+    r = ref_join(nb, None, True, True, knn=10, threads=os.cpu_count() or 1, queries=sample)
+    if r is None:
+        return {"checked": False, "why": "oracle/_ref was not built"}
+    sel = np.isin(q, sample)
+    got = set(zip(q[sel].tolist(), t[sel].tolist()))
+    ref = set(zip(r[0].tolist(), r[1].tolist()))
+    out = {"checked": True, "ref_rules_equal": got == ref, "sample_queries": int(len(sample)),
+           "sample": f"every {step}th query nucleus from {137 % step}", "results": len(got),
+           "ref_results": len(ref), "ref_seconds": r[2][0]}
+    log(f"parity 10-NN self-join sample: {out}")
+    if got != ref:
+        print(json.dumps({"parity_failure": out}), file=sys.stderr)
+        raise SystemExit("the 10-NN self-join lists differ from the reference rules' on the sample")
+    return out
 
 
 def run_serving(pkg, ctx, T2, nb, rates, per_rate_cap=600, seconds=3.0, pool_size=48, seed=20260005):
@@ -360,14 +442,14 @@ def run_reference_arm(a):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtdp_ref.so was not built "
                                                                "(needs the reference sources at build time)"}))
         return 0
-    nb, vb = make_tiles(0, 1)
+    nb, vb = make_tiles_isolated()
     # each step a bounded sample, sized so the whole run stays within about 3 minutes
     warm = max(0, min(a.warmup, 1))
     cb = cpu_reference(nb, vb, a.steps, warm, a.cpu_sample, target_s=max(2.0, 150.0 / (a.steps + warm)))
     line = {"metric": METRIC, "value": cb["value"], "unit": "tri-pairs/s", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": cb["seconds_per_sample"] * 1e3, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "impl": "reference CPU (MeshDist + octree compiled from source)"},
+            "config": {**base_config(), "impl": "reference CPU (MeshDist + octree compiled from source)"},
             "impl": "reference", "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": "tri-pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -382,6 +464,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=1500, help="query nuclei in the CPU-baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the reference-rule result-set checks")
+    ap.add_argument("--self-sample", type=int, default=500,
+                    help="query nuclei (stratified) whose 10-NN self-join lists are checked against the reference")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream measurement")
     ap.add_argument("--no-self", action="store_true", help="skip the 10-NN self-join measurement")
@@ -465,6 +550,11 @@ def main():
         if not (np.array_equal(qa, qb) and np.array_equal(ra, rb)):
             raise SystemExit("plain and tuned forms returned different result sets")
         n_results = len(qb)
+        # and the reference's own join rules (its octree and FP32 MeshDist,
+        # compiled from source, all host cores) must give the same set
+        parity = {"within400": None, "knn10_self_sample": None}
+        if rank == 0 and not a.no_parity:
+            parity["within400"] = check_parity(nb, vb, qb, rb)
 
         # Every join launches on the context's stream; the step events are
         # recorded on that same stream.  Between steps a 256 MiB buffer (twice
@@ -514,8 +604,10 @@ def main():
         knn_self = None
         if not a.no_self and ws == 1:
             ctx.join(T1, None, query="nn", knn=10, form=pkg.FORM_TUNED)
-            qs, _, _ = ctx.join(T1, None, query="nn", knn=10, form=pkg.FORM_TUNED)
+            qs, ts, _ = ctx.join(T1, None, query="nn", knn=10, form=pkg.FORM_TUNED)
             st_s = ctx.stats()
+            if not a.no_parity:
+                parity["knn10_self_sample"] = check_parity_self_sample(nb, qs, ts, a.self_sample)
             knn_self = {"workload": f"10-NN self-join over the {N_VESSELS * NUCLEI_PER_VESSEL} nuclei, LODs 20-100",
                         "join_ms": st_s["total_ms"], "tri_pairs": st_s["tri_pairs"],
                         "tri_pairs_per_s": st_s["tri_pairs"] / (st_s["total_ms"] / 1e3),
@@ -606,8 +698,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "tri-pairs/s", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "form": "tuned", "n_nuclei": N_VESSELS * NUCLEI_PER_VESSEL,
-                       "n_vessels": N_VESSELS, "tau": TAU, "seed": SEED, "results": n_results,
+            "config": {**base_config(), "form": "tuned", "results": n_results,
                        "join_seconds": step_ms / 1e3, "tri_pairs_per_join": tri,
                        "refine_ms": refine_ms, "filter_ms": st_t["filter_ms"],
                        "l2": "L2 flushed between timed steps (256 MiB rewrite on the join stream, outside the step events)",
@@ -624,6 +715,7 @@ def main():
                     "path": "tdp_tile_attach x2 (page-locked host tiles, 36.8 GB) + tdp_join (per-LOD fetch of the "
                             "voxels refined) + result read-back + tdp_tile_free, fresh tiles every step",
                     "host_ms": e2e_parts, "upload_path": e2e_upload},
+            "parity": parity,
             "exact_distances": exact,
             "serving": serving,
             "bounds_prep": bounds_prep,

@@ -411,11 +411,14 @@ int tdp_refine_batch(tdp_ctx *ctx, const float *data, const float *hausdorff, si
  * process held to a fixed device budget, a latency-critical loop that must not
  * call cudaMalloc): the same refine as tdp_refine_batch with TDP_FORM_TUNED,
  * but every pointer is DEVICE memory and the call needs no context and
- * allocates nothing.  Its working memory is one fixed 14.3 MB __device__ array
- * inside this library (held by every GPU that loads it until exit), which caps
- * a call at 262144 triangles and 65536 voxel pairs; larger calls return
- * TDP_ERR_ARG with a message in err.  The first call on a device looks up that
- * array's address (make it before any stream capture begins).  All calls on a
+ * allocates nothing.  It runs the tuned kernel's configuration 0 (no
+ * autotuner pick applies without a context).  Its working memory is one fixed
+ * __device__ array of 14,680,320 bytes (14.0 MiB) inside this library (held by
+ * every GPU that loads it until exit), which caps a call at 262144 triangles
+ * and 65536 voxel pairs; larger calls return TDP_ERR_ARG with a message in
+ * err.  The first call on a device looks up that array's address, and the
+ * first launch in a process raises the kernel's dynamic shared-memory limit
+ * (make that first call before any stream capture begins).  All calls on a
  * device share the array: calls that may overlap on the GPU race, so serialise
  * them.  Work is enqueued on `stream` (a cudaStream_t, NULL = default stream);
  * out is valid once the stream reaches it.  Rows of offset_size that point

@@ -29,9 +29,9 @@
 #include "geometry.h"
 #include "rawdt.hpp"
 
-extern "C" long tdr_candidates(const float* box1, const float* xf1, long n1, const float* box2, const float* xf2,
-                               long n2, int self_join, int knn, float within, int is_knn, long* off, int* ids,
-                               long cap);
+extern "C" long tdr_candidates_sel(const float* box1, const float* xf1, long n1, const float* box2,
+                                   const float* xf2, long n2, int self_join, int knn, float within, int is_knn,
+                                   const int* qmap, long* off, int* ids, long cap);
 
 namespace {
 
@@ -101,36 +101,45 @@ void knn_rank(std::vector<Pair>& P, long b, long e, int K, int& conf) {
             if (!P[i].stat) P[i].stat = 2;
 }
 
-}  // namespace
-
-// stats (optional, 4 doubles): seconds, triangle pairs refined, voxel pairs refined, candidates
-extern "C" long tdr_join(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t l2, int self_join, int is_knn,
-                         int knn, float tau, const int* lods, int nlods, int level, int threads, long max_queries,
-                         int* oq, int* ot, long cap, double* stats) {
+// The join for the query objects qsel (ids into tile 1); when qsel is empty,
+// for the first max_queries objects of tile 1, or all of them when
+// max_queries <= 0.  Results are (tile-1 id, tile-2 id) pairs.
+long join_impl(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t l2, int self_join, int is_knn, int knn,
+               float tau, const int* lods, int nlods, int level, int threads, long max_queries, std::vector<int> qsel,
+               int* oq, int* ot, long cap, double* stats) {
     auto t0 = std::chrono::steady_clock::now();
     std::vector<RObject> T1 = oracle::read_tile(b1, l1);
     std::vector<RObject> T2 = self_join ? std::vector<RObject>() : oracle::read_tile(b2, l2);
     const std::vector<RObject>& S = self_join ? T1 : T2;
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
-    long n1 = (long)T1.size(), n2 = (long)S.size();
+    if (qsel.empty()) {
+        long n = (long)T1.size();
+        if (max_queries > 0 && max_queries < n) n = max_queries;
+        for (long i = 0; i < n; ++i) qsel.push_back((int)i);
+    }
+    for (int q : qsel)
+        if (q < 0 || q >= (long)T1.size()) return 0;
+    long n1 = (long)qsel.size(), n2 = (long)S.size();
     std::vector<float> box1(6 * n1), xf1(3 * n1), box2(6 * n2), xf2(3 * n2);
-    for (long i = 0; i < n1; ++i) { std::memcpy(&box1[6 * i], T1[i].box, 24); std::memcpy(&xf1[3 * i], T1[i].transform, 12); }
+    for (long i = 0; i < n1; ++i) {
+        std::memcpy(&box1[6 * i], T1[qsel[i]].box, 24);
+        std::memcpy(&xf1[3 * i], T1[qsel[i]].transform, 12);
+    }
     for (long i = 0; i < n2; ++i) { std::memcpy(&box2[6 * i], S[i].box, 24); std::memcpy(&xf2[3 * i], S[i].transform, 12); }
-    // candidates from the reference octree for the (optionally sampled) query prefix
-    if (max_queries > 0 && max_queries < n1) n1 = max_queries;
+    // candidates from the reference octree for the chosen query objects
     std::vector<long> off(n1 + 1);
     std::vector<int> ids;
     long capc = std::max<long>(1024, n1 * 64);
     for (;;) {
         ids.assign(capc, 0);
-        long tot = tdr_candidates(box1.data(), xf1.data(), n1, box2.data(), xf2.data(), n2, self_join, knn, tau, is_knn,
-                                  off.data(), ids.data(), capc);
+        long tot = tdr_candidates_sel(box1.data(), xf1.data(), n1, box2.data(), xf2.data(), n2, self_join, knn, tau,
+                                      is_knn, qsel.data(), off.data(), ids.data(), capc);
         if (tot >= 0) { ids.resize(tot); break; }
         capc *= 4;
     }
     std::vector<Pair> P;
     for (long q = 0; q < n1; ++q)
-        for (long k = off[q]; k < off[q + 1]; ++k) { Pair p; p.q = (int)q; p.t = ids[k]; P.push_back(p); }
+        for (long k = off[q]; k < off[q + 1]; ++k) { Pair p; p.q = qsel[q]; p.t = ids[k]; P.push_back(p); }
     std::vector<long> qoff(off.begin(), off.begin() + n1 + 1);
     std::vector<int> conf(n1, 0);
     // filter
@@ -233,4 +242,26 @@ extern "C" long tdr_join(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t
         stats[3] = (double)P.size();
     }
     return n <= cap ? n : -n;
+}
+
+}  // namespace
+
+// stats (optional, 4 doubles): seconds, triangle pairs refined, voxel pairs refined, candidates.
+// max_queries > 0 joins only the first max_queries objects of tile 1.
+extern "C" long tdr_join(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t l2, int self_join, int is_knn,
+                         int knn, float tau, const int* lods, int nlods, int level, int threads, long max_queries,
+                         int* oq, int* ot, long cap, double* stats) {
+    return join_impl(b1, l1, b2, l2, self_join, is_knn, knn, tau, lods, nlods, level, threads, max_queries, {}, oq, ot,
+                     cap, stats);
+}
+
+// The same join for the query objects qids[0..nq) of tile 1 (a sample of
+// queries: per-object candidate lists never mix query objects, so each
+// query's result is the one the whole join gives it).  Ids must be in range.
+extern "C" long tdr_join_sel(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t l2, int self_join, int is_knn,
+                             int knn, float tau, const int* lods, int nlods, int level, int threads, const int* qids,
+                             long nq, int* oq, int* ot, long cap, double* stats) {
+    if (nq <= 0) return 0;
+    return join_impl(b1, l1, b2, l2, self_join, is_knn, knn, tau, lods, nlods, level, threads, 0,
+                     std::vector<int>(qids, qids + nq), oq, ot, cap, stats);
 }

@@ -50,10 +50,10 @@ void tdr_mesh_dist(const float *d1, const float *d2, size_t n1, size_t n2,
  * object itself, as the pointer test at octree.cpp:253/299 does.
  * Output: CSR offsets [n1+1] and ids in the reference's candidate order.
  * Returns the total number of candidates, or -1 if cap is too small. */
-long tdr_candidates(const float *box1, const float *xf1, long n1,
-                    const float *box2, const float *xf2, long n2,
-                    int self_join, int knn, float within, int is_knn,
-                    long *off, int *ids, long cap)
+static long candidates_impl(const float *box1, const float *xf1, long n1,
+                            const float *box2, const float *xf2, long n2,
+                            int self_join, int knn, float within, int is_knn,
+                            const int *qmap, long *off, int *ids, long cap)
 {
     std::vector<weighted_aab> b2((size_t)n2);
     std::vector<weighted_aab *> ptr2((size_t)n2);
@@ -79,7 +79,7 @@ long tdr_candidates(const float *box1, const float *xf1, long n1,
     for (long i = 0; i < n1; ++i) {
         weighted_aab *q;
         if (self_join) {
-            q = ptr2[(size_t)i];
+            q = ptr2[(size_t)(qmap ? qmap[i] : i)];
         } else {
             q = &b1[(size_t)i];
             q->set_box(box1[6 * i], box1[6 * i + 1], box1[6 * i + 2],
@@ -116,6 +116,25 @@ long tdr_candidates(const float *box1, const float *xf1, long n1,
     }
     delete tree;
     return total;
+}
+
+long tdr_candidates(const float *box1, const float *xf1, long n1,
+                    const float *box2, const float *xf2, long n2,
+                    int self_join, int knn, float within, int is_knn,
+                    long *off, int *ids, long cap)
+{
+    return candidates_impl(box1, xf1, n1, box2, xf2, n2, self_join, knn, within, is_knn, nullptr, off, ids, cap);
+}
+
+/* The same for a chosen set of query objects: query i is tile-1 object
+ * qmap[i] (its box and transform are box1[6 i..], xf1[3 i..]); in a self-join
+ * the octree's pointer test excludes tile-2 object qmap[i]. */
+long tdr_candidates_sel(const float *box1, const float *xf1, long n1,
+                        const float *box2, const float *xf2, long n2,
+                        int self_join, int knn, float within, int is_knn,
+                        const int *qmap, long *off, int *ids, long cap)
+{
+    return candidates_impl(box1, xf1, n1, box2, xf2, n2, self_join, knn, within, is_knn, qmap, off, ids, cap);
 }
 
 } /* extern "C" */

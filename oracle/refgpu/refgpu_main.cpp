@@ -8,11 +8,20 @@
  * reference's GPU path, compiled for sm_100a, beside this repository's on the
  * same tiles.  Prints the join's wall time on stderr as "join seconds: S".
  *
+ * With TDP_REFGPU_RESULTS=PATH set, every result the join recorded is written
+ * to PATH as one "qid rid" line per pair, read from each query object's result
+ * list after the join.  The reference's --print_result prints only the
+ * results that pass through HiMesh_Wrapper::report_result
+ * (src/spatial/himesh_wrapper.cpp:195-202); within_chunking appends its
+ * per-LOD results to the list directly (src/join/WithinJoin.cpp:781), so the
+ * lists are the complete result set.
+ *
  *   tdbase_ref_gpu --tile1 N.dt --tile2 V.dt -q within --within_dist 400 -g [--print_result]
  */
 #include <sys/time.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <utility>
 #include <vector>
 
@@ -59,6 +68,23 @@ int main(int argc, char** argv) {
     joiner->join(pairs);
     const double j1 = now_s();
     std::fprintf(stderr, "load seconds: %f\njoin seconds: %f\n", l1 - l0, j1 - j0);
+    if (const char* path = std::getenv("TDP_REFGPU_RESULTS")) {
+        FILE* f = std::fopen(path, "w");
+        if (!f) {
+            std::fprintf(stderr, "cannot write %s\n", path);
+            return 2;
+        }
+        size_t n = 0;
+        for (size_t i = 0; i < t1->num_objects(); ++i) {
+            HiMesh_Wrapper* w = t1->get_mesh_wrapper(i);
+            for (HiMesh_Wrapper* r : w->results) {
+                std::fprintf(f, "%ld %ld\n", (long)w->id, (long)r->id);
+                ++n;
+            }
+        }
+        std::fclose(f);
+        std::fprintf(stderr, "results: %zu\n", n);
+    }
     if (t2 != t1) delete t2;
     delete t1;
     delete joiner;

@@ -120,8 +120,12 @@ def join_exact(tile1, tile2, self_join, is_knn, knn=1, tau=0.0, threads=0):
         cap = -n
 
 
-def ref_join(tile1, tile2, self_join, is_knn, knn=1, tau=0.0, lods=None, level=2, threads=0, max_queries=0):
+def ref_join(tile1, tile2, self_join, is_knn, knn=1, tau=0.0, lods=None, level=2, threads=0, max_queries=0,
+             queries=None):
     """The reference's join rules on the CPU with the reference's own MeshDist/octree.
+    max_queries > 0 joins only the first max_queries query objects; `queries`
+    (ids into tile 1) joins only those (each query's candidate list and result
+    are the ones the whole join gives it).
     Returns (q, t, stats) with stats = (seconds, tri_pairs, voxel_pairs_refined, candidates)."""
     R = reference()
     if R is None:
@@ -130,14 +134,25 @@ def ref_join(tile1, tile2, self_join, is_knn, knn=1, tau=0.0, lods=None, level=2
     L.tdr_join.argtypes = [P, C.c_size_t, P, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_float, P, C.c_int, C.c_int,
                            C.c_int, C.c_long, P, P, C.c_long, P]
     L.tdr_join.restype = C.c_long
+    L.tdr_join_sel.argtypes = [P, C.c_size_t, P, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_float, P, C.c_int,
+                               C.c_int, C.c_int, P, C.c_long, P, P, C.c_long, P]
+    L.tdr_join_sel.restype = C.c_long
     t1 = np.ascontiguousarray(tile1, np.uint8)
     t2 = t1 if tile2 is None else np.ascontiguousarray(tile2, np.uint8)
     lods = np.array(lods or [20, 40, 60, 80, 100], np.int32)
+    qsel = None if queries is None else np.ascontiguousarray(queries, np.int32)
+    if qsel is not None and len(qsel) == 0:
+        return np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(4)
     cap = 1 << 16
     while True:
         q = np.empty(cap, np.int32); t = np.empty(cap, np.int32); st = np.zeros(4)
-        n = L.tdr_join(_p(t1), t1.size, _p(t2), t2.size, int(self_join), int(is_knn), int(knn), float(tau), _p(lods),
-                       len(lods), int(level), int(threads), int(max_queries), _p(q), _p(t), cap, _p(st))
+        if qsel is None:
+            n = L.tdr_join(_p(t1), t1.size, _p(t2), t2.size, int(self_join), int(is_knn), int(knn), float(tau),
+                           _p(lods), len(lods), int(level), int(threads), int(max_queries), _p(q), _p(t), cap, _p(st))
+        else:
+            n = L.tdr_join_sel(_p(t1), t1.size, _p(t2), t2.size, int(self_join), int(is_knn), int(knn), float(tau),
+                               _p(lods), len(lods), int(level), int(threads), _p(qsel), len(qsel), _p(q), _p(t), cap,
+                               _p(st))
         if n >= 0:
             o = np.lexsort((t[:n], q[:n]))
             return q[:n][o], t[:n][o], st

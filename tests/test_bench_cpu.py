@@ -1,7 +1,9 @@
 """bench.py's reference arm on the host: the JSON line of the reference's CPU
 path (oracle/_ref, the reference's MeshDist and octree compiled from source)
 on a reduced workload (10 vessels x 40 nuclei, where the join refines some
-2e5 triangle pairs) carries every key of the line the GPU arm prints."""
+2e5 triangle pairs) carries every key of the line the GPU arm prints, the
+same workload keys in `config`, and its process never maps this
+repository's library (the tiles are generated in a child process)."""
 import json
 import subprocess
 import sys
@@ -15,9 +17,13 @@ ROOT = Path(__file__).resolve().parents[1]
 def test_reference_arm_line(pkg):
     if not (ROOT / "oracle" / "_ref" / "libtdp_ref.so").exists():
         pytest.skip("the reference library is built from the reference sources")
-    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "2",
-                          "--warmup", "1", "--vessels", "10", "--nuclei-per-vessel", "40"],
-                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    argv = ["bench.py", "--impl", "reference", "--steps", "2", "--warmup", "1", "--vessels", "10",
+            "--nuclei-per-vessel", "40"]
+    # run bench.py in a process that reports, at exit, whether libtdp.so was mapped
+    code = ("import atexit, runpy, sys; "
+            "atexit.register(lambda: sys.stderr.write('LIBTDP_MAPPED=%d\\n' % ('libtdp.so' in open('/proc/self/maps').read()))); "
+            f"sys.argv = {argv!r}; runpy.run_path('bench.py', run_name='__main__')")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1, out.stdout
@@ -32,3 +38,6 @@ def test_reference_arm_line(pkg):
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"]
     assert "10 vessels x 40 nuclei" in d["config"]["workload"]
+    c = d["config"]
+    assert c["n_nuclei"] == 400 and c["n_vessels"] == 10 and c["tau"] == 400.0 and c["seed"] == 20260002
+    assert "LIBTDP_MAPPED=0" in out.stderr, out.stderr[-2000:]

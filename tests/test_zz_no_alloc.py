@@ -4,15 +4,17 @@ It serves callers that cannot allocate device memory, so the test hands it
 device buffers it allocated itself and checks, on two calls in a row with
 different batches (the second call must not see the first one's leftovers),
 that it returns what the ordinary entry point tdp_refine_batch returns for the
-same inputs, within the refine tests' FP32 tolerance.  This file is collected
-last so a failure here never hides the other tests.
+same inputs and what the FP64 oracle gives, both within the refine tests'
+FP32 tolerance; that an empty row starting at the end of the batch is valid;
+and that batches over its fixed limits are rejected with the limit named.
+This file is collected last so a failure here never hides the other tests.
 """
 import ctypes as C
 
 import numpy as np
 import pytest
 
-from test_refine_gpu import ERR_C, U, local_scale, make_batch
+from test_refine_gpu import ERR_C, U, check, local_scale, make_batch, oracle_batch
 
 pytestmark = pytest.mark.gpu
 
@@ -44,6 +46,8 @@ def test_noalloc_matches_refine_batch_on_two_calls(pkg, ctx):
         tol = ERR_C * U * np.maximum(local_scale(tri, osz), 1e-30)
         assert (np.abs(got[:, 0] - want[:, 0]) <= tol).all(), call
         assert (np.abs(got[:, 1:] - want[:, 1:]) <= tol[:, None] + 1e-5 * np.abs(want[:, 1:])).all(), call
+        # and directly against the FP64 oracle
+        check(got, oracle_batch(tri, hd, osz), tri, hd, osz)
 
 
 def test_noalloc_without_hausdorff_and_bad_rows(pkg, ctx):
@@ -66,3 +70,22 @@ def test_noalloc_rejects_oversized_batches(pkg):
     osz = np.array([[0, 1, 1, 1]], np.uint64)
     rc, msg, _ = call_noalloc(pkg, tri, None, osz)
     assert rc == 1 and "262144" in msg
+
+
+def test_noalloc_empty_row_at_the_end_of_the_batch(pkg, ctx):
+    rng = np.random.default_rng(11)
+    tri, hd, osz = make_batch(rng, 12)
+    osz = np.concatenate([osz, np.array([[len(tri), 0, 0, 5]], np.uint64)])  # n1 = 0 at offset == element_num
+    rc, msg, got = call_noalloc(pkg, tri, hd, osz)
+    assert rc == 0, msg
+    want = ctx.refine_batch(tri, hd, osz, form=pkg.FORM_TUNED)
+    assert not np.isnan(got[-1]).any()
+    np.testing.assert_array_equal(got[-1], want[-1])
+    check(got[:-1], oracle_batch(tri, hd, osz[:-1]), tri, hd, osz[:-1])
+
+
+def test_noalloc_rejects_too_many_pairs(pkg):
+    tri = np.zeros((4, 9), np.float32)
+    osz = np.tile(np.array([[0, 1, 1, 1]], np.uint64), (65537, 1))
+    rc, msg, _ = call_noalloc(pkg, tri, None, osz)
+    assert rc == 1 and "65536" in msg
