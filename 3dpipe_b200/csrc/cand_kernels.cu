@@ -101,11 +101,63 @@ __device__ unsigned long long kth_key(const unsigned long long* keys, int n, int
     return lo;
 }
 
+// Ring search of one query (one warp): the K-th smallest (transform
+// distance, id) key, ~0 when tile 2 holds fewer than K candidates.  The keys
+// of the points seen so far go to keys[0, cap); returns false when a ring
+// brought more than cap points (the result is then unusable).  Every point of
+// tile 2 lies in exactly one grid cell and every cell is visited by exactly
+// one ring, so cap >= n2 can never overflow.
+__device__ bool kth_search(const DG& pg, const float* xq, const float* __restrict__ xf2, int q, int K, int self,
+                           unsigned long long* keys, int cap, int* cnt, int lane, unsigned long long& result) {
+    const int cx = dci(xq[0], pg.lo0, pg.cell, pg.n0), cy = dci(xq[1], pg.lo1, pg.cell, pg.n1);
+    const int cz = dci(xq[2], pg.lo2, pg.cell, pg.n2);
+    if (lane == 0) *cnt = 0;
+    __syncwarp();
+    const int maxr = max(pg.n0, max(pg.n1, pg.n2));
+    result = ~0ull;  // fewer than K objects: every object is a candidate
+    bool over = false;
+    for (int r = 0; r <= maxr; ++r) {
+        const int side = 2 * r + 1;
+        const int total = side * side * side;
+        for (int t = lane; t < total; t += 32) {
+            const int dx = t % side - r, dy = (t / side) % side - r, dz = t / (side * side) - r;
+            if (max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
+            const int x = cx + dx, y = cy + dy, z = cz + dz;
+            if (x < 0 || y < 0 || z < 0 || x >= pg.n0 || y >= pg.n1 || z >= pg.n2) continue;
+            const size_t c = ((size_t)x * pg.n1 + y) * pg.n2 + z;
+            for (int64_t k = pg.start[c]; k < pg.start[c + 1]; ++k) {
+                const int o = pg.items[k];
+                if (self && o == q) continue;
+                const int pos = atomicAdd(cnt, 1);
+                if (pos < cap) keys[pos] = key_of(d_point_dist(xq, xf2 + 3 * (size_t)o), o);
+            }
+        }
+        __syncwarp();
+        const int seen = *cnt;
+        if (seen > cap) {
+            over = true;
+            break;
+        }
+        if (seen >= K) {
+            const unsigned long long kk = kth_key(keys, seen, K, lane);
+            const float kd = __uint_as_float((unsigned)(kk >> 32));
+            result = kk;  // best so far; the loop ends after the last ring anyway
+            if (kd < __fsub_rn(__fmul_rn((float)r, pg.cell), pg.slack)) break;
+        }
+        __syncwarp();
+    }
+    __syncwarp();
+    return !over;
+}
+
+// Pass 1: every kNN query with its keys in shared memory (kCap per warp); a
+// query whose rings bring more points than that is appended to ovlist and
+// redone by k_cand_kth_global.
 __global__ void __launch_bounds__(kWarps * 32) k_cand_kth(DG pg, const float* __restrict__ xf1,
                                                          const float* __restrict__ xf2, int n1, int K_all, int self,
                                                          const int* __restrict__ qk,
                                                          unsigned long long* __restrict__ kth,
-                                                         int* __restrict__ overflow) {
+                                                         int* __restrict__ n_over, int* __restrict__ ovlist) {
     __shared__ unsigned long long keys[kWarps][kCap];
     __shared__ int cnt[kWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -113,43 +165,34 @@ __global__ void __launch_bounds__(kWarps * 32) k_cand_kth(DG pg, const float* __
     for (int q = blockIdx.x * kWarps + w; q < n1; q += nw) {
         const int K = qk ? qk[q] : K_all;
         if (K <= 0) continue;  // a within object of a mixed batch (warp-uniform)
-        const float* xq = xf1 + 3 * (size_t)q;
-        const int cx = dci(xq[0], pg.lo0, pg.cell, pg.n0), cy = dci(xq[1], pg.lo1, pg.cell, pg.n1);
-        const int cz = dci(xq[2], pg.lo2, pg.cell, pg.n2);
-        if (lane == 0) cnt[w] = 0;
-        __syncwarp();
-        const int maxr = max(pg.n0, max(pg.n1, pg.n2));
-        unsigned long long result = ~0ull;  // fewer than K objects: every object is a candidate
-        for (int r = 0; r <= maxr; ++r) {
-            const int side = 2 * r + 1;
-            const int total = side * side * side;
-            for (int t = lane; t < total; t += 32) {
-                const int dx = t % side - r, dy = (t / side) % side - r, dz = t / (side * side) - r;
-                if (max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
-                const int x = cx + dx, y = cy + dy, z = cz + dz;
-                if (x < 0 || y < 0 || z < 0 || x >= pg.n0 || y >= pg.n1 || z >= pg.n2) continue;
-                const size_t c = ((size_t)x * pg.n1 + y) * pg.n2 + z;
-                for (int64_t k = pg.start[c]; k < pg.start[c + 1]; ++k) {
-                    const int o = pg.items[k];
-                    if (self && o == q) continue;
-                    const int pos = atomicAdd(&cnt[w], 1);
-                    if (pos < kCap) keys[w][pos] = key_of(d_point_dist(xq, xf2 + 3 * (size_t)o), o);
-                    else atomicOr(overflow, 1);
-                }
-            }
-            __syncwarp();
-            const int n = min(cnt[w], kCap);
-            if (n >= K) {
-                const unsigned long long kk = kth_key(keys[w], n, K, lane);
-                const float kd = __uint_as_float((unsigned)(kk >> 32));
-                if (kd < __fsub_rn(__fmul_rn((float)r, pg.cell), pg.slack)) {
-                    result = kk;
-                    break;
-                }
-                result = kk;  // best so far; the loop ends after the last ring anyway
-            }
-            __syncwarp();
+        unsigned long long result;
+        const bool ok = kth_search(pg, xf1 + 3 * (size_t)q, xf2, q, K, self, keys[w], kCap, &cnt[w], lane, result);
+        if (lane == 0) {
+            kth[q] = result;
+            if (!ok) ovlist[atomicAdd(n_over, 1)] = q;
         }
+        __syncwarp();
+    }
+}
+
+// Pass 2, only when pass 1 overflowed: the queries of ovlist, one warp each,
+// with a global-memory key buffer of cap (>= the points of tile 2) per warp.
+__global__ void __launch_bounds__(kWarps * 32) k_cand_kth_global(DG pg, const float* __restrict__ xf1,
+                                                                const float* __restrict__ xf2, int K_all, int self,
+                                                                const int* __restrict__ qk,
+                                                                unsigned long long* __restrict__ kth,
+                                                                const int* __restrict__ n_over,
+                                                                const int* __restrict__ ovlist,
+                                                                unsigned long long* __restrict__ gkeys, int cap) {
+    __shared__ int cnt[kWarps];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int gw = blockIdx.x * kWarps + w, nw = gridDim.x * kWarps;
+    unsigned long long* keys = gkeys + (size_t)gw * cap;
+    for (int i = gw; i < *n_over; i += nw) {
+        const int q = ovlist[i];
+        const int K = qk ? qk[q] : K_all;
+        unsigned long long result;
+        kth_search(pg, xf1 + 3 * (size_t)q, xf2, q, K, self, keys, cap, &cnt[w], lane, result);
         if (lane == 0) kth[q] = result;
         __syncwarp();
     }
@@ -293,11 +336,11 @@ struct TileBoxes {
 }  // namespace
 
 int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool self, bool knn, int K, float tau,
-                      Buf& pq_buf, Buf& pt_buf, Buf& qoff_buf, long& P, bool& overflow, const int* qk,
+                      Buf& pq_buf, Buf& pt_buf, Buf& qoff_buf, long& P, long& n_redone, const int* qk,
                       const float* qtau, bool isect) {
     cudaStream_t s = ctx->stream;
     const long n1 = t1->n_obj, n2 = t2->n_obj;
-    overflow = false;
+    n_redone = 0;
     P = 0;
     int rc;
     // grids over tile 2, built once per tile
@@ -337,12 +380,16 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
     const float* box2 = t2->d_boxes;
     const float* xf2 = box2 + 6 * n2;
     int* d_over = (int*)(ctx->d_counter + 40);
+    Buf& ovb = ctx->scratch[89];
+    if ((rc = ensure(ctx, ovb, (size_t)(n1 + 1) * 4))) return rc;
     CU(cudaMemsetAsync(d_over, 0, 4, s));
     const DG bg = dg(t2->box_grid), pg = dg(t2->point_grid);
     unsigned long long* kth = (unsigned long long*)kthb.p;
-    if (knn || qk) {
+    const bool any_knn = knn || qk;
+    if (any_knn) {
         const int blocks = (int)std::min<long>((n1 + kWarps - 1) / kWarps, (long)ctx->num_sms * 16);
-        k_cand_kth<<<std::max(blocks, 1), kWarps * 32, 0, s>>>(pg, xf1, xf2, (int)n1, K, self, qk, kth, d_over);
+        k_cand_kth<<<std::max(blocks, 1), kWarps * 32, 0, s>>>(pg, xf1, xf2, (int)n1, K, self, qk, kth, d_over,
+                                                              (int*)ovb.p);
         CU(cudaGetLastError());
     }
     // first cell of every tile-2 object (the dedupe test of the scan)
@@ -355,22 +402,34 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
     int64_t* cnt = (int64_t*)cntb.p;
     int64_t* qoff = (int64_t*)qoff_buf.p;
     const int pblocks = (int)std::min<long>((n1 + 7) / 8, (long)ctx->num_sms * 32);
-    CU(cudaMemsetAsync(cnt + n1, 0, 8, s));
-    k_cand_pass<false><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, fc, (int)n1, self, knn, tau, qk,
-                                                           qtau, isect ? 1 : 0, kth, cnt, nullptr, nullptr);
-    CU(cudaGetLastError());
-    size_t tb = 0;
-    CU(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, qoff, (int)n1 + 1, s));
-    if ((rc = ensure(ctx, tmp, tb + 16))) return rc;
-    CU(cub::DeviceScan::ExclusiveSum(tmp.p, tb, cnt, qoff, (int)n1 + 1, s));
     int64_t total = 0;
     int over = 0;
-    CU(cudaMemcpyAsync(&total, qoff + n1, 8, cudaMemcpyDeviceToHost, s));
-    CU(cudaMemcpyAsync(&over, d_over, 4, cudaMemcpyDeviceToHost, s));
-    CU(cudaStreamSynchronize(s));
-    if (over) {
-        overflow = true;
-        return TDP_OK;
+    for (int pass = 0;; ++pass) {
+        CU(cudaMemsetAsync(cnt + n1, 0, 8, s));
+        k_cand_pass<false><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, fc, (int)n1, self, knn, tau,
+                                                               qk, qtau, isect ? 1 : 0, kth, cnt, nullptr, nullptr);
+        CU(cudaGetLastError());
+        size_t tb = 0;
+        CU(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, qoff, (int)n1 + 1, s));
+        if ((rc = ensure(ctx, tmp, tb + 16))) return rc;
+        CU(cub::DeviceScan::ExclusiveSum(tmp.p, tb, cnt, qoff, (int)n1 + 1, s));
+        CU(cudaMemcpyAsync(&total, qoff + n1, 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaMemcpyAsync(&over, d_over, 4, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (!over || pass > 0) break;
+        // Some kNN ring searches saw more points than a warp's shared-memory
+        // buffer holds: redo just those on the device with a global buffer of
+        // n2 + 1 keys per warp (which no ring search can overflow), then count
+        // again.  At most 256 MiB of keys, at least one warp.
+        const long cap = n2 + 1;
+        const long warps = std::max<long>(1, std::min<long>({(long)over, (long)ctx->num_sms * kWarps,
+                                                             (256L << 20) / (cap * 8)}));
+        Buf& gk = ctx->scratch[90];
+        if ((rc = ensure(ctx, gk, (size_t)warps * cap * 8))) return rc;
+        k_cand_kth_global<<<(int)((warps + kWarps - 1) / kWarps), kWarps * 32, 0, s>>>(
+            pg, xf1, xf2, K, self, qk, kth, d_over, (const int*)ovb.p, (unsigned long long*)gk.p, (int)cap);
+        CU(cudaGetLastError());
+        n_redone = over;
     }
     if (total >= (1LL << 31) - 1) return fail(ctx, TDP_ERR_ARG, "too many candidate pairs");
     P = (long)total;
@@ -407,17 +466,13 @@ extern "C" long tdp_tile_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_
     const bool self = (t2 == nullptr || t2 == t1);
     if (!t2) t2 = t1;
     cudaSetDevice(ctx->device);
-    long P = 0;
-    bool overflow = false;
+    long P = 0, redone = 0;
     Buf& pq = ctx->scratch[57];
     Buf& pt = ctx->scratch[58];
     Buf& qo = ctx->scratch[59];
-    if (device_candidates(ctx, t1, t2, self, is_knn != 0, is_knn ? knn : 0, within, pq, pt, qo, P, overflow))
+    if (device_candidates(ctx, t1, t2, self, is_knn != 0, is_knn ? knn : 0, within, pq, pt, qo, P, redone))
         return LONG_MIN;
-    if (overflow) {
-        fail(ctx, TDP_ERR_STATE, "kNN ring search overflowed its buffer; use tdp_candidates");
-        return LONG_MIN;
-    }
+    ctx->stats.candidate_redone = redone;
     cudaMemcpyAsync(off, qo.p, (t1->n_obj + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream);
     if (ids && P <= cap && P > 0) cudaMemcpyAsync(ids, pt.p, P * 4, cudaMemcpyDeviceToHost, ctx->stream);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return LONG_MIN;

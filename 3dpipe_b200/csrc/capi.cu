@@ -188,6 +188,8 @@ int tdp_last_stats(const tdp_ctx* ctx, tdp_stats* o) {
     o->fetch_bytes = s.fetch_bytes;
     for (int l = 0; l < tdp::kNumLods; ++l) o->refine_ms_lod[l] = s.refine_ms_lod[l];
     o->lod_graph = s.lod_graph;
+    o->candidates_on_device = s.candidates_on_device;
+    o->candidate_redone = s.candidate_redone;
     return TDP_OK;
 }
 

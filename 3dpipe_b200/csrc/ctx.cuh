@@ -40,6 +40,8 @@ struct LastStats {
     double fetch_bytes = 0;          // RAW bytes fetched from attached tiles
     double refine_ms_lod[kNumLods] = {0, 0, 0, 0, 0};  // tuned refine time per LOD index
     long lod_graph = 0;              // tuned LOD loop: 0 direct launches, 1 graph replayed, 2 graph captured
+    long candidates_on_device = 0;   // 1: object candidates came from the GPU (the tuned form)
+    long candidate_redone = 0;       // kNN queries redone with the global ring-search buffer
 };
 
 }  // namespace tdp

@@ -238,9 +238,12 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     if (cudaEventRecord(ctx->ev[0], s) != cudaSuccess) return fail(ctx, TDP_ERR_CUDA, "event record failed");
 
     // ---- 1. object candidates ----
-    // The tuned form generates them on the GPU (csrc/cand_kernels.cu); the
-    // plain form, and the tuned form when a kNN ring search overflows its
-    // buffer, use the host grid (src/index).  Both give the same set and order.
+    // The tuned form generates them on the GPU (csrc/cand_kernels.cu; a kNN
+    // ring search that overflows its shared-memory buffer is redone there with
+    // a global one).  The plain form keeps the reference's arrangement, where
+    // the host builds the candidate lists (its OpenMP octree queries,
+    // KNNJoin.cpp:552-573), with the host grid of src/index.  Both give the
+    // same set and order.
     int rc;
 #define ENS(slot, bytes) do { if ((rc = ensure(ctx, ctx->scratch[slot], (bytes)))) return rc; } while (0)
 #define CU(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } while (0)
@@ -261,11 +264,12 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         CU(cudaMemcpyAsync((void*)dqtau, prm->obj_within, t1->n_obj * 4, cudaMemcpyHostToDevice, s));
     }
     if (tuned) {
-        bool overflow = false;
         if ((rc = device_candidates(ctx, t1, t2, self, knn, knn ? prm->knn : 0, within_dist, ctx->scratch[kPq],
-                                    ctx->scratch[kPt], ctx->scratch[kQoff], P, overflow, dqk, dqtau, isect)))
+                                    ctx->scratch[kPt], ctx->scratch[kQoff], P, st.candidate_redone, dqk, dqtau,
+                                    isect)))
             return rc;
-        on_device = !overflow;
+        on_device = true;
+        st.candidates_on_device = 1;
     }
     if (!on_device) {
         CandidateQuery cq{t1->host.obj_box.data(), t1->host.obj_xf.data(), t1->n_obj, t2->host.obj_box.data(),

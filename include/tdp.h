@@ -86,6 +86,11 @@ typedef struct {
                                         1 replayed the context's CUDA graph,
                                         2 captured (or updated) it in this call */
     double refine_ms_lod[5];         /* tuned refine time per LOD 20..100      */
+    long candidates_on_device;       /* 1: object candidates were computed on
+                                        the GPU (tuned form), 0: on the host   */
+    long candidate_redone;           /* kNN queries whose ring search outgrew a
+                                        warp's shared-memory buffer and were
+                                        redone on the GPU with a global one    */
 } tdp_stats;
 int tdp_last_stats(const tdp_ctx *ctx, tdp_stats *out);
 /* measured FP32 FMA throughput of the context's device in TFLOP/s (CUDA cores,
@@ -231,8 +236,11 @@ int tdp_raw_compute_bounds(tdp_ctx *ctx, const void *raw, size_t len, void *out,
 long tdp_candidates(const float *box1, const float *xf1, long n1, const float *box2, const float *xf2, long n2,
                     int self_join, int is_knn, int knn, float within, int64_t *off, int32_t *ids, long cap);
 /* The same candidates computed on the GPU for two resident tiles (tile2 NULL or
- * == tile1: self-join); this is what the tuned join uses.  Same return
- * convention as tdp_candidates; LONG_MIN on error (see tdp_last_error). */
+ * == tile1: self-join); this is what the tuned join uses.  A kNN query whose
+ * ring search outgrows a warp's shared-memory buffer (large K, dense cells) is
+ * redone on the GPU with a global buffer; the number of such queries is then
+ * tdp_last_stats().candidate_redone.  Same return convention as
+ * tdp_candidates; LONG_MIN on error (see tdp_last_error). */
 long tdp_tile_candidates(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, int is_knn, int knn,
                          float within, int64_t *off, int32_t *ids, long cap);
 
