@@ -157,12 +157,13 @@ __global__ void __launch_bounds__(kWarps * 32) k_cand_kth(DG pg, const float* __
                                                          const float* __restrict__ xf2, int n1, int K_all, int self,
                                                          const int* __restrict__ qk,
                                                          unsigned long long* __restrict__ kth,
-                                                         int* __restrict__ n_over, int* __restrict__ ovlist) {
+                                                         int* __restrict__ n_over, int* __restrict__ ovlist,
+                                                         int qb0) {
     __shared__ unsigned long long keys[kWarps][kCap];
     __shared__ int cnt[kWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nw = gridDim.x * kWarps;
-    for (int q = blockIdx.x * kWarps + w; q < n1; q += nw) {
+    for (int q = qb0 + blockIdx.x * kWarps + w; q < n1; q += nw) {
         const int K = qk ? qk[q] : K_all;
         if (K <= 0) continue;  // a within object of a mixed batch (warp-uniform)
         unsigned long long result;
@@ -220,12 +221,16 @@ __global__ void __launch_bounds__(256) k_cand_pass(DG bg, const float* __restric
                                                    const float* __restrict__ qtau, int isect,
                                                    const unsigned long long* __restrict__ kth,
                                                    int64_t* __restrict__ cnt, const int64_t* __restrict__ off,
-                                                   unsigned long long* __restrict__ keys) {
+                                                   unsigned long long* __restrict__ keys, int qb0, int qe0) {
     constexpr unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const unsigned lt = (1u << lane) - 1u;
     for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n1; q += nw) {
+        if (q < qb0 || q >= qe0) {  // outside the joined query range: no candidates
+            if (!WRITE && lane == 0) cnt[q] = 0;
+            continue;
+        }
         const float* qb = box1 + 6 * (size_t)q;
         const float* xq = xf1 + 3 * (size_t)q;
         const int knn = qk ? qk[q] > 0 : knn_all;
@@ -337,9 +342,10 @@ struct TileBoxes {
 
 int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool self, bool knn, int K, float tau,
                       Buf& pq_buf, Buf& pt_buf, Buf& qoff_buf, long& P, long& n_redone, const int* qk,
-                      const float* qtau, bool isect) {
+                      const float* qtau, bool isect, long q_begin, long q_end) {
     cudaStream_t s = ctx->stream;
     const long n1 = t1->n_obj, n2 = t2->n_obj;
+    const long qb0 = std::max(0L, q_begin), qe0 = q_end < 0 ? n1 : std::min(n1, q_end);
     n_redone = 0;
     P = 0;
     int rc;
@@ -387,9 +393,10 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
     unsigned long long* kth = (unsigned long long*)kthb.p;
     const bool any_knn = knn || qk;
     if (any_knn) {
-        const int blocks = (int)std::min<long>((n1 + kWarps - 1) / kWarps, (long)ctx->num_sms * 16);
-        k_cand_kth<<<std::max(blocks, 1), kWarps * 32, 0, s>>>(pg, xf1, xf2, (int)n1, K, self, qk, kth, d_over,
-                                                              (int*)ovb.p);
+        const long nq = std::max(0L, qe0 - qb0);
+        const int blocks = (int)std::min<long>((nq + kWarps - 1) / kWarps, (long)ctx->num_sms * 16);
+        k_cand_kth<<<std::max(blocks, 1), kWarps * 32, 0, s>>>(pg, xf1, xf2, (int)qe0, K, self, qk, kth, d_over,
+                                                              (int*)ovb.p, (int)qb0);
         CU(cudaGetLastError());
     }
     // first cell of every tile-2 object (the dedupe test of the scan)
@@ -407,7 +414,8 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
     for (int pass = 0;; ++pass) {
         CU(cudaMemsetAsync(cnt + n1, 0, 8, s));
         k_cand_pass<false><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, fc, (int)n1, self, knn, tau,
-                                                               qk, qtau, isect ? 1 : 0, kth, cnt, nullptr, nullptr);
+                                                               qk, qtau, isect ? 1 : 0, kth, cnt, nullptr, nullptr,
+                                                               (int)qb0, (int)qe0);
         CU(cudaGetLastError());
         size_t tb = 0;
         CU(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, qoff, (int)n1 + 1, s));
@@ -440,7 +448,8 @@ int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool
     if ((rc = ensure(ctx, pt_buf, Pz * 4))) return rc;
     if (P > 0) {
         k_cand_pass<true><<<std::max(pblocks, 1), 256, 0, s>>>(bg, box1, xf1, box2, xf2, fc, (int)n1, self, knn, tau, qk, qtau, isect ? 1 : 0, kth,
-                                                              nullptr, qoff, (unsigned long long*)keys.p);
+                                                              nullptr, qoff, (unsigned long long*)keys.p, (int)qb0,
+                                                              (int)qe0);
         CU(cudaGetLastError());
         size_t sb = 0;
         CU(cub::DeviceSegmentedSort::SortKeys(nullptr, sb, (const unsigned long long*)keys.p,

@@ -17,8 +17,9 @@ namespace tdp {
 // buffer that cannot overflow, so the result is always complete.
 // qk / qtau (device, optional): per tile-1 object K (> 0, kNN) or 0 (within,
 // distance qtau); NULL: every object uses (knn, K, tau).
+// Only tile-1 objects [q_begin, q_end) get candidates (q_end < 0: all).
 int device_candidates(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, bool self, bool knn, int K, float tau,
                       Buf& pq_buf, Buf& pt_buf, Buf& qoff_buf, long& P, long& n_redone, const int* qk = nullptr,
-                      const float* qtau = nullptr, bool isect = false);
+                      const float* qtau = nullptr, bool isect = false, long q_begin = 0, long q_end = -1);
 
 }  // namespace tdp

@@ -76,6 +76,10 @@ void generate_candidates(const CandidateQuery& q, std::vector<int64_t>& off, std
                 const float* qb = q.box1 + 6 * i;
                 const float* qx = q.xf1 + 3 * i;
                 found.clear();
+                if (i < q.q_begin || (q.q_end >= 0 && i >= q.q_end)) {
+                    cnts.push_back(0);
+                    continue;
+                }
                 const bool is_knn = q.obj_knn ? q.obj_knn[i] > 0 : q.is_knn;
                 const float within = q.obj_knn ? q.obj_within[i] : q.within;
                 if (!is_knn) {

@@ -38,6 +38,10 @@ struct CandidateQuery {
     const float* obj_within = nullptr;
     // intersect query: candidates are objects whose boxes overlap strictly
     bool strict_overlap = false;
+    // only query objects [q_begin, q_end) get candidates (q_end < 0: to n1);
+    // the others get empty lists
+    long q_begin = 0;
+    long q_end = -1;
 };
 
 // off: [n1+1] CSR offsets into ids.

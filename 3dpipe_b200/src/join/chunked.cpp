@@ -137,6 +137,8 @@ extern "C" int tdp_join_chunked(tdp_ctx* ctx, const void* raw1, size_t len1, con
     if (!ctx || !raw1 || !raw2 || !prm || !out || chunk_objects < 1) return TDP_ERR_ARG;
     *out = nullptr;
     if (prm->obj_knn) return fail(ctx, TDP_ERR_ARG, "per-object queries are not supported by the chunked join");
+    if (prm->query_begin != 0 || prm->query_end >= 0)
+        return fail(ctx, TDP_ERR_ARG, "a query range is not supported by the chunked join (it chunks the queries itself)");
     const uint8_t* b1 = (const uint8_t*)raw1;
     const uint8_t* b2 = (const uint8_t*)raw2;
     TileHost h1, h2;

@@ -191,6 +191,8 @@ void tdp_join_default_params(tdp_join_params* p) {
     p->hausdorff_level = 2;
     p->form = TDP_FORM_TUNED;
     p->exact_distances = 0;
+    p->query_begin = 0;
+    p->query_end = -1;
 }
 
 int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_join_params* prm, tdp_result** out) {
@@ -219,6 +221,12 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         if (knn && prm->knn < 1) return fail(ctx, TDP_ERR_ARG, "knn must be >= 1");
     }
     if (prm->hausdorff_level < 0 || prm->hausdorff_level > 2) return fail(ctx, TDP_ERR_ARG, "hausdorff_level must be 0, 1 or 2");
+    // a shard of a join split over GPUs: only tile-1 objects [q_begin, q_end) are queries
+    const long q_begin = prm->query_begin, q_end = prm->query_end < 0 ? t1->n_obj : prm->query_end;
+    if (q_begin < 0 || q_begin > q_end || q_end > t1->n_obj)
+        return fail(ctx, TDP_ERR_ARG, "query range [" + std::to_string(prm->query_begin) + ", " +
+                                          std::to_string(prm->query_end) + ") is not inside tile 1's " +
+                                          std::to_string(t1->n_obj) + " objects");
     if (prm->form != TDP_FORM_PLAIN && prm->form != TDP_FORM_TUNED) return fail(ctx, TDP_ERR_ARG, "unknown form");
     if (t1->device != ctx->device || t2->device != ctx->device) return fail(ctx, TDP_ERR_ARG, "tile lives on another device");
     const bool tuned = prm->form == TDP_FORM_TUNED;
@@ -266,7 +274,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     if (tuned) {
         if ((rc = device_candidates(ctx, t1, t2, self, knn, knn ? prm->knn : 0, within_dist, ctx->scratch[kPq],
                                     ctx->scratch[kPt], ctx->scratch[kQoff], P, st.candidate_redone, dqk, dqtau,
-                                    isect)))
+                                    isect, q_begin, q_end)))
             return rc;
         on_device = true;
         st.candidates_on_device = 1;
@@ -274,7 +282,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
     if (!on_device) {
         CandidateQuery cq{t1->host.obj_box.data(), t1->host.obj_xf.data(), t1->n_obj, t2->host.obj_box.data(),
                           t2->host.obj_xf.data(), t2->n_obj, self, knn, knn ? prm->knn : 0, within_dist, 0,
-                          prm->obj_knn, prm->obj_within, isect};
+                          prm->obj_knn, prm->obj_within, isect, q_begin, q_end};
         generate_candidates(cq, qoff, ids);
         P = (long)ids.size();
         if (P >= (1L << 31) - 1) return fail(ctx, TDP_ERR_ARG, "too many candidate pairs");

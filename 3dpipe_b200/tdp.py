@@ -204,7 +204,8 @@ class TileInfo(C.Structure):
 class JoinParams(C.Structure):
     _fields_ = [("query", C.c_int), ("knn", C.c_int), ("within_dist", C.c_float), ("lods", C.c_int * 8),
                 ("n_lods", C.c_int), ("hausdorff_level", C.c_int), ("form", C.c_int),
-                ("exact_distances", C.c_int), ("obj_knn", C.c_void_p), ("obj_within", C.c_void_p)]
+                ("exact_distances", C.c_int), ("obj_knn", C.c_void_p), ("obj_within", C.c_void_p),
+                ("query_begin", C.c_long), ("query_end", C.c_long)]
 
 
 def _bind_join(L):
@@ -305,16 +306,20 @@ def _join_params(query, knn, within, lods, hausdorff_level, form) -> JoinParams:
 
 def _join(self, tile1: Tile, tile2: Tile | None, query: str = "nn", knn: int = 1, within: float = 1000.0,
           lods=None, hausdorff_level: int = 2, form: int = FORM_TUNED, exact_distances: bool = False,
-          obj_knn=None, obj_within=None):
+          obj_knn=None, obj_within=None, query_range=None):
     """tdbase join on resident tiles; returns (query_ids, result_ids, dist) sorted by (query, result).
 
     dist is float32 (each pair's upper bound when decided) unless
     exact_distances is set: then float64 exact LOD-100 distances.  obj_knn /
     obj_within (one entry per tile-1 object) give every query object its own
-    query: K > 0 for kNN, 0 for within at obj_within[i]."""
+    query: K > 0 for kNN, 0 for within at obj_within[i].  query_range = (b, e)
+    joins only tile-1 objects [b, e) (one shard of a split join; ids stay
+    tile-1 ids)."""
     L = lib()
     p = _join_params(query, knn, within, lods, hausdorff_level, form)
     p.exact_distances = int(bool(exact_distances))
+    if query_range is not None:
+        p.query_begin, p.query_end = int(query_range[0]), int(query_range[1])
     keep = []
     if obj_knn is not None:
         ok = np.ascontiguousarray(obj_knn, np.int32)
@@ -356,7 +361,27 @@ LOD_GRAPH_OFF, LOD_GRAPH_AUTO, LOD_GRAPH_ALWAYS = 0, 1, 2
 
 EXPORTED += ["tdp_tile_compute_bounds", "tdp_raw_compute_bounds", "tdp_tile_attach", "tdp_host_alloc",
              "tdp_host_free", "tdp_raw_check", "tdp_get_refine_config_lod", "tdp_host_cache_bytes",
-             "tdp_host_cache_trim"]
+             "tdp_host_cache_trim", "tdp_partition_queries", "tdp_raw_partition"]
+
+
+def partition_queries(raw1, raw2=None, n_shards=2, knn=0, within=0.0, intersect=False):
+    """Split the query objects of RAW tile raw1 (raw2 None: a self-join) into
+    n_shards contiguous ranges of about equal estimated work (tdp_raw_partition,
+    host only).  Returns (bounds[n_shards + 1], work[n_shards])."""
+    L = lib()
+    L.tdp_raw_partition.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_float,
+                                    C.c_int, C.c_void_p, C.c_void_p, C.c_char_p, C.c_size_t]
+    r1 = np.ascontiguousarray(raw1, np.uint8)
+    r2 = None if raw2 is None else np.ascontiguousarray(raw2, np.uint8)
+    bounds = np.zeros(int(n_shards) + 1, np.int64)
+    work = np.zeros(int(n_shards), np.float64)
+    err = C.create_string_buffer(512)
+    mode = 2 if intersect else int(knn > 0)
+    rc = L.tdp_raw_partition(_ptr(r1), r1.size, None if r2 is None else _ptr(r2), 0 if r2 is None else r2.size,
+                             mode, max(int(knn), 1), float(within), int(n_shards), _ptr(bounds), _ptr(work), err, 512)
+    if rc != TDP_OK:
+        raise TdpError(rc, err.value.decode() or "tdp_raw_partition failed")
+    return bounds, work
 
 CTX_POISON = 1  # tdp_ctx_create flag: unfetched records of attached tiles read as NaN
 

@@ -141,13 +141,36 @@ class Pinned:
 
 
 def make_tiles(rank, ws):
-    """Generate the tiles.  With N ranks each rank takes the nuclei of its own
-    contiguous block of vessels (all vessels are replicated): strong scaling."""
+    """Generate the tiles.  One rank: the whole workload.  N ranks: rank 0
+    generates the whole nuclei tile and splits the query nuclei with the
+    product's partitioner (contiguous ranges of about equal estimated work,
+    tdp_raw_partition); every rank then generates the nuclei of its own range
+    (the generator places them as in the whole tile) and all vessels, so no
+    rank holds more than its share of the query tile.  Returns (nuclei tile,
+    vessel tile, first global nucleus id, the split bounds, rank 0's whole
+    nuclei tile or None)."""
     pkg = importlib.import_module("3dpipe_b200")
     t = time.time()
-    nb, vb, _ = pkg.shard.gen_shard_tiles(rank, ws, N_VESSELS, NUCLEI_PER_VESSEL, SEED)
-    log(f"[rank {rank}] generated {nb.size / 1e9:.2f} + {vb.size / 1e9:.2f} GB in {time.time() - t:.1f}s")
-    return nb, vb
+    if ws == 1:
+        nb, vb = pkg.tdp.gen_tiles(N_VESSELS, NUCLEI_PER_VESSEL, seed=SEED)
+        log(f"[rank {rank}] generated {nb.size / 1e9:.2f} + {vb.size / 1e9:.2f} GB in {time.time() - t:.1f}s")
+        return nb, vb, 0, [0, N_VESSELS * NUCLEI_PER_VESSEL], None
+    import torch.distributed as dist
+    whole, box = None, [None]
+    if rank == 0:
+        whole, vb0 = pkg.tdp.gen_tiles(N_VESSELS, NUCLEI_PER_VESSEL, seed=SEED)
+        bounds, work = pkg.shard.partition(whole, vb0, ws, within=TAU)
+        box = [bounds.tolist()]
+        log(f"[rank 0] split {N_VESSELS * NUCLEI_PER_VESSEL} query nuclei into {ws} ranges {box[0]} "
+            f"(estimated voxel pairs {[int(w) for w in work]})")
+        del vb0
+    dist.broadcast_object_list(box, src=0)
+    bounds = box[0]
+    b, e = pkg.shard.shard_range(bounds, rank)
+    nb, vb = pkg.shard.gen_shard_tiles(b, e, N_VESSELS, NUCLEI_PER_VESSEL, SEED)
+    log(f"[rank {rank}] nuclei [{b}, {e}): generated {nb.size / 1e9:.2f} + {vb.size / 1e9:.2f} GB "
+        f"in {time.time() - t:.1f}s")
+    return nb, vb, b, bounds, whole
 
 
 def base_config():
@@ -161,7 +184,7 @@ def make_tiles_isolated():
     pipe, so that the reference arm's own process never loads this
     repository's library."""
     code = ("import sys, importlib; sys.path.insert(0, %r); pkg = importlib.import_module('3dpipe_b200'); "
-            "nb, vb, _ = pkg.shard.gen_shard_tiles(0, 1, %d, %d, %d); o = sys.stdout.buffer; "
+            "nb, vb = pkg.tdp.gen_tiles(%d, %d, seed=%d); o = sys.stdout.buffer; "
             "o.write(int(nb.size).to_bytes(8, 'little')); o.write(int(vb.size).to_bytes(8, 'little')); "
             "o.write(memoryview(nb)); o.write(memoryview(vb)); o.flush()"
             % (str(ROOT), N_VESSELS, NUCLEI_PER_VESSEL, SEED))
@@ -503,7 +526,7 @@ def main():
                                 device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
     pkg = importlib.import_module("3dpipe_b200")
-    nb, vb = make_tiles(rank, ws)
+    nb, vb, first, bounds, whole = make_tiles(rank, ws)
     t = time.time()
     pinned = Pinned([nb, vb])
     log(f"[rank {rank}] page-locked {len(pinned.ptrs)} tile buffers in {time.time() - t:.1f}s")
@@ -553,8 +576,13 @@ def main():
         # and the reference's own join rules (its octree and FP32 MeshDist,
         # compiled from source, all host cores) must give the same set
         parity = {"within400": None, "knn10_self_sample": None}
-        if rank == 0 and not a.no_parity:
+        if ws == 1 and not a.no_parity:
             parity["within400"] = check_parity(nb, vb, qb, rb)
+        elif ws > 1:
+            # every rank's result, ids mapped to global ones, gathered on rank
+            # 0; there the union must equal the reference rules' set of the
+            # whole join (after the timed steps: the check takes host cores)
+            merged = pkg.shard.gather_results(pkg.shard.to_global(qb, first), rb, np.zeros(len(qb)), dst=0)
 
         # Every join launches on the context's stream; the step events are
         # recorded on that same stream.  Between steps a 256 MiB buffer (twice
@@ -680,8 +708,14 @@ def main():
         del flush_buf
 
     pinned.release()
+    if ws > 1 and rank == 0 and not a.no_parity:
+        gq, gt, _ = merged
+        parity["within400"] = check_parity(whole, vb, gq, gt)
+        parity["within400"]["shards"] = bounds
+    if ws > 1:
+        n_results = len(merged[0]) if rank == 0 else n_results
     cpu = None
-    if rank == 0 and not a.no_cpu:
+    if rank == 0 and ws == 1 and not a.no_cpu:
         cpu = cpu_reference(nb, vb, 3, 0, a.cpu_sample, target_s=5.0)
     # DRAM bytes per refine launch from the committed ncu capture of this workload
     traffic = None
@@ -702,7 +736,9 @@ def main():
                        "join_seconds": step_ms / 1e3, "tri_pairs_per_join": tri,
                        "refine_ms": refine_ms, "filter_ms": st_t["filter_ms"],
                        "l2": "L2 flushed between timed steps (256 MiB rewrite on the join stream, outside the step events)",
-                       "parallelism": f"{ws} GPU(s), query nuclei sharded by vessel block",
+                       "parallelism": f"{ws} GPU(s)" + ("" if ws == 1 else
+                                       ", query nuclei split into contiguous ranges of equal estimated work "
+                                       "(tdp_raw_partition), results gathered on rank 0"),
                        "refine_config": {"chunk_a": cfg_defs[best_cfg][0], "ctas_per_sm": cfg_defs[best_cfg][1],
                                          "autotune_refine_ms": [round(m, 4) for m in cfg_ms],
                                          "by_lod": {str(k): {"config": v, "chunk_a": cfg_defs[v][0],

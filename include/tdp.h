@@ -244,6 +244,32 @@ long tdp_candidates(const float *box1, const float *xf1, long n1, const float *b
 long tdp_tile_candidates(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, int is_knn, int knn,
                          float within, int64_t *off, int32_t *ids, long cap);
 
+/* ---- splitting a join over GPUs ------------------------------------------------
+ * No reference counterpart (the reference pins itself to one GPU,
+ * src/geometry/cuda_common.cu:20).  A join's query objects are independent
+ * given tile 2: each query object's candidate list, filter and LOD refine read
+ * only that object and tile 2 (per-object candidate lists,
+ * src/join/KNNJoin.cpp:552-600).  So N processes, one per GPU, can each join a
+ * contiguous range of tile-1 objects (tdp_join_params.query_begin/query_end)
+ * against the whole tile 2 and concatenate their results, with no exchange
+ * during the join.  tdp_partition_queries splits [0, n1) into n_shards
+ * contiguous ranges of about equal estimated work: per query object, the sum
+ * over its object candidates (as tdp_candidates returns them) of
+ * n_voxels(query) x n_voxels(candidate) -- the voxel pairs the filter
+ * evaluates -- plus one.  bounds receives n_shards + 1 entries (bounds[0] = 0,
+ * bounds[n_shards] = n1; shard s is [bounds[s], bounds[s+1]), possibly
+ * empty); work (optional) each shard's estimate.  is_knn: 0 within, 1 kNN,
+ * 2 intersect.  Host only, deterministic: every process computes the same
+ * split from the same inputs. */
+int tdp_partition_queries(const float *box1, const float *xf1, const uint32_t *nvox1, long n1,
+                          const float *box2, const float *xf2, const uint32_t *nvox2, long n2,
+                          int self_join, int is_knn, int knn, float within, int n_shards,
+                          long *bounds, double *work);
+/* The same from RAW tiles in host memory, parsed on the host (raw2 NULL: a
+ * self-join of raw1).  err (optional) receives a message. */
+int tdp_raw_partition(const void *raw1, size_t len1, const void *raw2, size_t len2, int is_knn, int knn,
+                      float within, int n_shards, long *bounds, double *work, char *err, size_t err_cap);
+
 /* ---- join ---------------------------------------------------------------------
  * `tdbase join` (reference src/tools/tdbase.cpp:482-549) on device-resident tiles:
  * object candidates (grid restatement of the octree queries), voxel-pair filter,
@@ -279,6 +305,13 @@ typedef struct {
                               batch of different requests; query/knn/within_dist
                               are then ignored.  No reference counterpart. */
     const float *obj_within;
+    long query_begin;      /* join only tile-1 objects [query_begin, query_end)     */
+    long query_end;        /* (query_end < 0: to the last one; default 0, -1); result
+                              ids stay tile-1 ids and a self-join still excludes
+                              each object itself.  One shard of a join split over
+                              GPUs (tdp_partition_queries).  No reference
+                              counterpart: the reference runs on one GPU
+                              (src/geometry/cuda_common.cu:20). */
 } tdp_join_params;
 void tdp_join_default_params(tdp_join_params *p);
 int tdp_join(tdp_ctx *ctx, const tdp_tile *tile1, const tdp_tile *tile2, const tdp_join_params *p,

@@ -70,6 +70,9 @@ calls = {
     "tdp_server_destroy": (None,),
     "tdp_refine_batch": (None, None, None, z, None, C.c_uint32(0), i0, None),
     "tdp_gen_tiles": (None, None, z, None, None, z, None, None, z),
+    "tdp_partition_queries": (None, None, None, C.c_long(0), None, None, None, C.c_long(0), i0, i0, i1, f0,
+                              C.c_int(2), None, None),
+    "tdp_raw_partition": (None, z, None, z, i0, i1, f0, C.c_int(2), None, None, None, z),
 }
 for name, args in calls.items():
     print(name, getattr(L, name)(*args))
