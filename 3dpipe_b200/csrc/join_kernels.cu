@@ -8,7 +8,8 @@
 //   k_within_decide    filter-time classification (src/join/WithinJoin.cpp:164-252)
 //                      and the per-LOD within decision (WithinJoin.cpp:769-792)
 //   k_knn_rank         evaluate_knn_kernel (computing_gpu.cu:105-151) + the confirm
-//                      cap in candidate order (src/join/KNNJoin.cpp:133-202)
+//                      cap in candidate order (src/join/KNNJoin.cpp:133-202), a
+//                      warp per query with the cap taken by ballot
 //   k_count/write_vps  record_valid_voxel_pairs_streaming_{knn,within}
 //                      (computing_gpu.cu:2604-2812): voxel pairs with
 //                      min <= object min-max (and <= tau for within), in (i,j) order
@@ -185,15 +186,26 @@ __global__ void k_within_decide(JoinDev d, float tau_all, int tuned) {
     }
 }
 
-__global__ void k_knn_rank(JoinDev d, int K_all, int tuned, int* __restrict__ st) {
-    for (int q = blockIdx.x; q < d.N1; q += gridDim.x) {
+// One warp per query object.  Pass 1: each lane takes candidates lane,
+// lane + 32, ... and applies the bulk rule against every other undecided
+// candidate (CONFIRMED if fewer than K - confirmed candidates may be closer,
+// REMOVED if at least that many are surely closer).  Pass 2: the cap in
+// candidate order, 32 candidates at a time: a candidate is acted on while the
+// confirmations before it (a ballot and a prefix count) leave an open slot,
+// which is what the reference's sequential loop does (it stops at the first
+// candidate that finds the K slots full).
+__global__ void __launch_bounds__(kBlock) k_knn_rank(JoinDev d, int K_all, int tuned, int* __restrict__ st) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < d.N1; q += nw) {
         const int K = d.qk ? d.qk[q] : K_all;
-        if (K <= 0) continue;  // a within object of a mixed batch (uniform over the block)
+        if (K <= 0) continue;  // a within object of a mixed batch (warp-uniform)
         const int64_t b = d.qoff[q], e = d.qoff[q + 1];
         int conf = d.qconf[q];
         if (conf < K) {
             const int cand_left = K - conf;
-            for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+            for (int64_t i = b + lane; i < e; i += 32) {
                 if (d.pstat[i] != kUndecided) continue;
                 const float ei = tuned ? d.perr[i] : 0.f;
                 const float lo = d.pmn[i] - ei, hi = d.pmx[i] + ei;
@@ -206,23 +218,24 @@ __global__ void k_knn_rank(JoinDev d, int K_all, int tuned, int* __restrict__ st
                 }
                 st[i] = maybe < cand_left ? 1 : (sure >= cand_left ? 2 : 0);
             }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                for (int64_t i = b; i < e; ++i) {
-                    if (d.pstat[i] != kUndecided) continue;
-                    if (conf >= K) break;
-                    if (st[i] == 1) { d.pstat[i] = kReported; ++conf; }
-                    else if (st[i] == 2) d.pstat[i] = kDropped;
+            __syncwarp();
+            for (int64_t base = b; base < e && conf < K; base += 32) {
+                const int64_t i = base + lane;
+                const bool und = i < e && d.pstat[i] == kUndecided;
+                const int s = und ? st[i] : 0;
+                const unsigned cm = __ballot_sync(0xffffffffu, s == 1);
+                if (und && conf + __popc(cm & lt) < K) {
+                    if (s == 1) d.pstat[i] = kReported;
+                    else if (s == 2) d.pstat[i] = kDropped;
                 }
-                d.qconf[q] = conf;
+                conf = min(K, conf + __popc(cm));
             }
-            __syncthreads();
-            conf = d.qconf[q];
+            if (lane == 0) d.qconf[q] = conf;
         }
         if (conf >= K)  // query complete: nothing left to refine for it
-            for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x)
+            for (int64_t i = b + lane; i < e; i += 32)
                 if (d.pstat[i] == kUndecided) d.pstat[i] = kDropped;
-        __syncthreads();
+        __syncwarp();
     }
 }
 
@@ -285,11 +298,19 @@ __global__ void __launch_bounds__(kBlock) k_vps(JoinDev d, int within_all, float
     }
 }
 
+// One slot claim and one triangle-pair sum per warp: lane 0 adds the warp's
+// item count and n1*n2 sum to the counters, the lanes write at the claimed
+// base plus their rank among the warp's items.  (The items form a set: their
+// order never changes a result.)
 __global__ void k_build_items(JoinDev d, const uint32_t* __restrict__ vt1, const uint32_t* __restrict__ vt2,
                               RefineItem* __restrict__ items, int* __restrict__ item_vp, unsigned* __restrict__ counter) {
     // counter[0] = items, counter[2..3] = sum n1*n2 (u64)
-    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < d.V; v += (int64_t)gridDim.x * blockDim.x) {
-        bool ok = d.valive[v] && d.pstat[d.vpair[v]] == kUndecided;
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    // every lane of a warp runs the same number of iterations (the bound is rounded up to whole warps)
+    const int64_t vend = (d.V + 31) & ~(int64_t)31;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < vend; v += stride) {
+        bool ok = v < d.V && d.valive[v] && d.pstat[d.vpair[v]] == kUndecided;
         uint32_t o1 = 0, n1 = 0, o2 = 0, n2 = 0;
         if (ok) {
             const int a = d.vpa[v], b = d.vpb[v];
@@ -297,11 +318,21 @@ __global__ void k_build_items(JoinDev d, const uint32_t* __restrict__ vt1, const
             o2 = vt2[b]; n2 = vt2[b + 1] - o2;
             ok = n1 > 0 && n2 > 0;
         }
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        if (!m) continue;
+        unsigned long long tp = ok ? (unsigned long long)n1 * n2 : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tp += __shfl_xor_sync(0xffffffffu, tp, o);
+        unsigned base = 0;
+        if (lane == 0) {
+            base = atomicAdd(counter, (unsigned)__popc(m));
+            atomicAdd(reinterpret_cast<unsigned long long*>(counter + 2), tp);
+        }
+        base = __shfl_sync(0xffffffffu, base, 0);
         if (ok) {
-            const unsigned w = atomicAdd(counter, 1u);
+            const unsigned w = base + __popc(m & ((1u << lane) - 1u));
             items[w] = RefineItem{o1, n1, o2, n2};
             item_vp[w] = (int)v;
-            atomicAdd(reinterpret_cast<unsigned long long*>(counter + 2), (unsigned long long)n1 * n2);
         }
     }
 }
@@ -504,7 +535,7 @@ cudaError_t launch_within_decide(const JoinDev& d, float tau, int tuned, cudaStr
 }
 cudaError_t launch_knn_rank(const JoinDev& d, int K, int tuned, int* st, cudaStream_t s) {
     if (d.N1 <= 0) return cudaSuccess;
-    k_knn_rank<<<grid_for(d.N1, 1, 148 * 64), 128, 0, s>>>(d, K, tuned, st);
+    k_knn_rank<<<grid_for(d.N1, kBlock / 32, 148 * 32), kBlock, 0, s>>>(d, K, tuned, st);
     return cudaGetLastError();
 }
 cudaError_t launch_count_vps(const JoinDev& d, int within, float tau, int tuned, int64_t* cnt, cudaStream_t s) {
