@@ -132,6 +132,7 @@ int tdp_ctx_create(int device, size_t budget_bytes, unsigned flags, tdp_ctx** ou
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return TDP_ERR_CUDA; }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
     for (auto& e : ctx->lod_ev) cudaEventCreate(&e);
+    for (auto& e : ctx->xev) cudaEventCreate(&e);
     if (dmalloc(ctx, (void**)&ctx->d_counter, 64 * sizeof(unsigned)) != cudaSuccess ||
         dmalloc(ctx, (void**)&ctx->d_stats, 64 * sizeof(unsigned long long)) != cudaSuccess) {
         tdp_ctx_destroy(ctx);
@@ -150,6 +151,7 @@ int tdp_ctx_destroy(tdp_ctx* ctx) {
     for (void* p : ptrs) dfree(ctx, p);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->lod_ev) if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->xev) if (e) cudaEventDestroy(e);
     cache_trim(ctx);
     if (ctx->lod_graph) cudaGraphExecDestroy(ctx->lod_graph);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -188,6 +190,8 @@ int tdp_last_stats(const tdp_ctx* ctx, tdp_stats* o) {
     o->fetch_bytes = s.fetch_bytes;
     for (int l = 0; l < tdp::kNumLods; ++l) o->refine_ms_lod[l] = s.refine_ms_lod[l];
     o->lod_graph = s.lod_graph;
+    for (int k = 0; k < 4; ++k) o->exact_phase_ms[k] = s.exact_phase_ms[k];
+    o->exact_full_evals = s.exact_full_evals;
     o->candidates_on_device = s.candidates_on_device;
     o->candidate_redone = s.candidate_redone;
     return TDP_OK;

@@ -40,6 +40,8 @@ struct LastStats {
     double fetch_bytes = 0;          // RAW bytes fetched from attached tiles
     double refine_ms_lod[kNumLods] = {0, 0, 0, 0, 0};  // tuned refine time per LOD index
     long lod_graph = 0;              // tuned LOD loop: 0 direct launches, 1 graph replayed, 2 graph captured
+    double exact_phase_ms[4] = {0, 0, 0, 0};  // exact stage: upper bounds, candidates, FP32 pass, FP64 pass
+    unsigned long long exact_full_evals = 0;   // exact stage: triangle pairs fully evaluated in FP32
     long candidates_on_device = 0;   // 1: object candidates came from the GPU (the tuned form)
     long candidate_redone = 0;       // kNN queries redone with the global ring-search buffer
 };
@@ -54,6 +56,7 @@ struct tdp_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[8] = {};
     cudaEvent_t lod_ev[16] = {};  // refine timing per LOD (tuned loop)
+    cudaEvent_t xev[5] = {};      // phases of the exact-distance stage
     std::string last_error;
     std::unordered_map<void*, size_t> allocs;
     tdp::Buf scratch[96];  // slots: refine-batch 0-4, tile upload 12-13, join 20-48, candidates 50-59, result sort 60-63, exact distances 64-81, per-object queries 82-83

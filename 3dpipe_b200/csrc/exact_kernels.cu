@@ -9,9 +9,9 @@
 //      LOD-100 surface), and, at Hausdorff level 2, also the pair's upper
 //      bound pmx when it was decided (d + h1 + h2 at a lower LOD bounds D);
 //      each widened by its FP32 error, max(perr, 1e-4 (value + 1));
-//      U is then tightened by refining one voxel pair per object pair in FP32
-//      (the one with the closest cores): its minimum d32 + err_bound(R) is a
-//      distance between two surface points, hence also >= D;
+//      U is then tightened by refining kExK = 8 voxel pairs per object pair in
+//      FP32 (the ones with the closest cores): each minimum d32 + err_bound(R)
+//      is a distance between two surface points, hence also >= D;
 //   2. every LOD-100 voxel pair whose box gap is <= U is a candidate (the
 //      voxel pair holding the closest points has gap <= D <= U);
 //   3. the tuned FP32 refine, its minimum preset to U plus the candidate's
@@ -42,26 +42,33 @@ namespace {
 
 constexpr int kBlk = 256;
 
+// Voxel pairs per object pair refined in FP32 to tighten U (the ones with
+// the closest cores).
+constexpr int kExK = 8;
+
 // U of every reported pair: min core-to-core distance over its voxel pairs,
-// and pmx when it is a proven bound (pmx_valid); item1[p] = the voxel pair with
-// the closest cores (an empty item for pairs that are not reported)
+// and pmx when it is a proven bound (pmx_valid); item1[kExK p + k] = the voxel
+// pairs with the kExK closest cores (empty items for the rest and for pairs
+// that are not reported).  Each lane keeps a sorted top kExK of its own
+// (strided) voxel pairs; the warp then takes the kExK smallest heads.
 __global__ void __launch_bounds__(kBlk) k_exact_upper(JoinDev d, int pmx_valid, const uint32_t* __restrict__ vt1,
                                                       const uint32_t* __restrict__ vt2, float* __restrict__ U,
                                                       RefineItem* __restrict__ item1) {
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
+        RefineItem* it1 = item1 + (size_t)kExK * p;
         if (d.pstat[p] != kReported) {
-            if (lane == 0) {
-                U[p] = FLT_MAX;
-                item1[p] = RefineItem{0, 0, 0, 0};
-            }
+            if (lane == 0) U[p] = FLT_MAX;
+            if (lane < kExK) it1[lane] = RefineItem{0, 0, 0, 0};
             continue;
         }
         const int q = d.pq[p], t = d.pt[p];
         const uint32_t a0 = d.ovox1[q], a1 = d.ovox1[q + 1], b0 = d.ovox2[t], b1 = d.ovox2[t + 1];
-        float m2 = FLT_MAX;
-        uint32_t ba = a0, bb = b0;
+        float kv[kExK];
+        uint32_t ka[kExK], kb[kExK];
+#pragma unroll
+        for (int k = 0; k < kExK; ++k) { kv[k] = FLT_MAX; ka[k] = a0; kb[k] = b0; }
         for (uint32_t b = b0 + lane; b < b1; b += 32) {
             if (vt2[b + 1] == vt2[b]) continue;
             const float4 cb = d.vox2[3 * (size_t)b + 2];
@@ -69,26 +76,45 @@ __global__ void __launch_bounds__(kBlk) k_exact_upper(JoinDev d, int pmx_valid, 
                 if (vt1[a + 1] == vt1[a]) continue;
                 const float4 ca = d.vox1[3 * (size_t)a + 2];
                 const float dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;
-                const float v = dx * dx + dy * dy + dz * dz;
-                if (v < m2) { m2 = v; ba = a; bb = b; }
+                float v = dx * dx + dy * dy + dz * dz;
+                if (!(v < kv[kExK - 1])) continue;
+                // insert into the lane's sorted list (unrolled, registers only)
+                uint32_t ia = a, ib = b;
+#pragma unroll
+                for (int k = 0; k < kExK; ++k) {
+                    if (v < kv[k]) {
+                        const float tv = kv[k];
+                        const uint32_t ta = ka[k], tb = kb[k];
+                        kv[k] = v; ka[k] = ia; kb[k] = ib;
+                        v = tv; ia = ta; ib = tb;
+                    }
+                }
             }
         }
-        // warp argmin (ties to the lowest lane)
-        float best = m2;
+        // the warp's kExK smallest: each round takes the smallest lane head
+        float best = FLT_MAX;
+        for (int k = 0; k < kExK; ++k) {
+            float h = kv[0];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
-        const unsigned who = __ballot_sync(0xffffffffu, m2 == best);
-        const int src = who ? __ffs(who) - 1 : 0;
-        ba = __shfl_sync(0xffffffffu, ba, src);
-        bb = __shfl_sync(0xffffffffu, bb, src);
+            for (int o = 16; o > 0; o >>= 1) h = fminf(h, __shfl_xor_sync(0xffffffffu, h, o));
+            const unsigned who = __ballot_sync(0xffffffffu, kv[0] == h);
+            const int src = __ffs(who) - 1;
+            const uint32_t wa = __shfl_sync(0xffffffffu, ka[0], src), wb = __shfl_sync(0xffffffffu, kb[0], src);
+            if (k == 0) best = h;
+            if (lane == 0)
+                it1[k] = h < FLT_MAX ? RefineItem{vt1[wa], vt1[wa + 1] - vt1[wa], vt2[wb], vt2[wb + 1] - vt2[wb]}
+                                     : RefineItem{0, 0, 0, 0};
+            if (lane == src) {  // pop the head
+#pragma unroll
+                for (int j = 0; j + 1 < kExK; ++j) { kv[j] = kv[j + 1]; ka[j] = ka[j + 1]; kb[j] = kb[j + 1]; }
+                kv[kExK - 1] = FLT_MAX;
+            }
+        }
         if (lane == 0) {
             float u = FLT_MAX;
             if (best < FLT_MAX) {
                 const float core = sqrtf(best);
                 u = core + fmaxf(1e-4f * (core + 1.f), 8.f * kUnitRoundoff * core);
-                item1[p] = RefineItem{vt1[ba], vt1[ba + 1] - vt1[ba], vt2[bb], vt2[bb + 1] - vt2[bb]};
-            } else {
-                item1[p] = RefineItem{0, 0, 0, 0};
             }
             if (pmx_valid) {
                 const float mx = d.pmx[p];
@@ -99,14 +125,15 @@ __global__ void __launch_bounds__(kBlk) k_exact_upper(JoinDev d, int pmx_valid, 
     }
 }
 
-// U = min(U, d32 + err) with the FP32 minimum of the closest-core voxel pair
+// U = min(U, d32 + err) over the FP32 minima of the kExK closest-core voxel pairs
 __global__ void k_exact_tighten(const float4* __restrict__ res1, int64_t P, float* __restrict__ U) {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P; p += (int64_t)gridDim.x * blockDim.x) {
-        const float4 r = res1[p];
-        if (r.x < FLT_MAX) {
-            const float u = r.x + err_bound(r.w) + 1e-5f * r.x + 1e-6f;
-            U[p] = fminf(U[p], u);
+        float u = U[p];
+        for (int k = 0; k < kExK; ++k) {
+            const float4 r = res1[(size_t)kExK * p + k];
+            if (r.x < FLT_MAX) u = fminf(u, r.x + err_bound(r.w) + 1e-5f * r.x + 1e-6f);
         }
+        U[p] = u;
     }
 }
 
@@ -323,8 +350,8 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     ENS(64, (Pz + 1) * 8);             // counts
     ENS(65, (Pz + 1) * 8);             // offsets
     ENS(78, Pz * 4);                   // U per pair
-    ENS(79, Pz * sizeof(RefineItem));  // phase-1 item per pair
-    ENS(80, Pz * sizeof(float4));      // phase-1 FP32 results
+    ENS(79, Pz * kExK * sizeof(RefineItem));  // phase-1 items, kExK per pair
+    ENS(80, Pz * kExK * sizeof(float4));      // phase-1 FP32 results
     ENS(75, 64);                       // counters
     int64_t* cnt = (int64_t*)ctx->scratch[64].p;
     int64_t* off = (int64_t*)ctx->scratch[65].p;
@@ -337,14 +364,18 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     const int pg = grid(d.P, kBlk / 32, ctx->num_sms * 32);
     CU(cudaMemsetAsync(cnt + d.P, 0, 8, s));
     CU(cudaMemsetAsync(ctr, 0, 64, s));
+    CU(cudaEventRecord(ctx->xev[0], s));
     k_exact_upper<<<pg, kBlk, 0, s>>>(d, pmx_valid ? 1 : 0, vt1, vt2, Ub, item1);
     CU(cudaGetLastError());
-    // phase 1: one FP32 voxel pair per object pair tightens U
-    CU(launch_fetch_items(item1, nullptr, d.P, kNumLods - 1, lz1, lz2, ctx->num_sms, s));
-    CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], item1, (int)d.P, res1, ctr, nullptr,
+    // phase 1: the kExK closest-core voxel pairs of every object pair in FP32 tighten U
+    const int64_t n1 = d.P * kExK;
+    if (n1 >= (1LL << 31)) return fail(ctx, TDP_ERR_ARG, "too many object pairs for the exact-distance stage");
+    CU(launch_fetch_items(item1, nullptr, n1, kNumLods - 1, lz1, lz2, ctx->num_sms, s));
+    CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], item1, (int)n1, res1, ctr, nullptr,
                            ctx->num_sms, ctx->lod_cfg[kNumLods - 1] >= 0 ? ctx->lod_cfg[kNumLods - 1] : ctx->tuned_cfg, s));
     k_exact_tighten<<<grid(d.P, 256, ctx->num_sms * 8), 256, 0, s>>>(res1, d.P, Ub);
     CU(cudaGetLastError());
+    CU(cudaEventRecord(ctx->xev[1], s));
     k_exact_vp<false><<<pg, kBlk, 0, s>>>(d, Ub, vt1, vt2, cnt, nullptr, nullptr, nullptr, nullptr);
     CU(cudaGetLastError());
     size_t tb = 0;
@@ -382,29 +413,38 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     CU(cudaMemsetAsync(best32, 0x7f, Pz * 4, s));  // 0x7f7f7f7f = 3.4e38, above any distance
     CU(cudaMemsetAsync(emax, 0, Pz * 4, s));
     CU(cudaMemsetAsync(ctr, 0, 64, s));
+    CU(cudaEventRecord(ctx->xev[2], s));
+    // ctr: [0] work counter, [4] selected items, [8] FP32 error bits, [12..13] full evaluations (u64)
+    unsigned long long* n_full = reinterpret_cast<unsigned long long*>(ctr + 12);
     if (E > 0) {
         CU(launch_fetch_items(items, nullptr, E, kNumLods - 1, lz1, lz2, ctx->num_sms, s));
-        CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], items, (int)E, res, ctr, nullptr,
+        CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], items, (int)E, res, ctr, n_full,
                                ctx->num_sms, ctx->lod_cfg[kNumLods - 1] >= 0 ? ctx->lod_cfg[kNumLods - 1] : ctx->tuned_cfg, s, nullptr, preset));
         const int eg = grid(E, 256, ctx->num_sms * 16);
         k_exact_best<<<eg, 256, 0, s>>>(res, item_pair, E, best32, emax);
         CU(cudaGetLastError());
         k_exact_select<<<eg, 256, 0, s>>>(res, items, item_pair, E, best32, emax, sel, sel_pair, sel_thr, ctr + 4);
         CU(cudaGetLastError());
+        CU(cudaEventRecord(ctx->xev[3], s));
         k_exact_f64<<<ctx->num_sms * 8, kExWarps * 32, 0, s>>>(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], sel,
                                                               sel_pair, sel_thr, ctr + 4,
                                                               reinterpret_cast<unsigned long long*>(pexact));
         CU(cudaGetLastError());
         k_exact_err<<<grid(d.P, 256, ctx->num_sms * 8), 256, 0, s>>>(d, best32, pexact, ctr + 8);
         CU(cudaGetLastError());
+        CU(cudaEventRecord(ctx->xev[4], s));
         info.launches += 6;
-        unsigned ns[8] = {0};
-        CU(cudaMemcpyAsync(ns, ctr + 4, 32, cudaMemcpyDeviceToHost, s));
+        unsigned ns[12] = {0};
+        CU(cudaMemcpyAsync(ns, ctr + 4, 48, cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
         info.f64_items = ns[0];
         float e32;
         std::memcpy(&e32, &ns[4], 4);
         info.max_rel_err32 = e32;
+        std::memcpy(&info.full_evals, &ns[8], 8);
+        float ms[4] = {0, 0, 0, 0};
+        for (int k = 0; k < 4; ++k) cudaEventElapsedTime(&ms[k], ctx->xev[k], ctx->xev[k + 1]);
+        for (int k = 0; k < 4; ++k) info.phase_ms[k] = ms[k];
     }
 #undef ENS
 #undef CU

@@ -14,6 +14,8 @@ struct ExactInfo {
     long f64_items = 0;  // of those, evaluated in FP64 (FP32 minimum within the error band of the best)
     int launches = 0;
     double max_rel_err32 = 0;  // max |FP32 object minimum - FP64 distance| / max(distance, 1)
+    double phase_ms[4] = {0, 0, 0, 0};  // upper bounds, candidates, FP32 pass, FP64 pass (device time)
+    unsigned long long full_evals = 0;  // triangle pairs the FP32 pass evaluated fully
 };
 
 // For every object pair with pstat == kReported: the exact minimum triangle

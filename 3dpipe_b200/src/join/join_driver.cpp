@@ -575,6 +575,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         st.exact_items = xi.items;
         st.exact_f64_items = xi.f64_items;
         st.fp32_max_rel_err = xi.max_rel_err32;
+        for (int k = 0; k < 4; ++k) st.exact_phase_ms[k] = xi.phase_ms[k];
+        st.exact_full_evals = xi.full_evals;
     }
     ctx->stats = st;
     *out = R;

@@ -44,12 +44,14 @@ class Stats(C.Structure):
                 ("candidates_ms", C.c_double), ("lod_ms", C.c_double), ("host_syncs", C.c_long),
                 ("exact_ms", C.c_double), ("exact_items", C.c_long), ("exact_f64_items", C.c_long),
                 ("fp32_max_rel_err", C.c_double), ("fetch_bytes", C.c_double), ("lod_graph", C.c_long),
-                ("refine_ms_lod", C.c_double * 5), ("candidates_on_device", C.c_long),
+                ("refine_ms_lod", C.c_double * 5), ("exact_phase_ms", C.c_double * 4),
+                ("exact_full_evals", C.c_ulonglong), ("candidates_on_device", C.c_long),
                 ("candidate_redone", C.c_long)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
         d["refine_ms_lod"] = list(self.refine_ms_lod)
+        d["exact_phase_ms"] = list(self.exact_phase_ms)
         return d
 
 

@@ -86,6 +86,12 @@ typedef struct {
                                         1 replayed the context's CUDA graph,
                                         2 captured (or updated) it in this call */
     double refine_ms_lod[5];         /* tuned refine time per LOD 20..100      */
+    double exact_phase_ms[4];        /* exact stage, device time of: upper
+                                        bounds (with their FP32 refine),
+                                        candidate voxel pairs, the FP32 pass,
+                                        the FP64 pass                          */
+    unsigned long long exact_full_evals; /* exact stage: triangle pairs fully
+                                        evaluated by its FP32 pass             */
     long candidates_on_device;       /* 1: object candidates were computed on
                                         the GPU (tuned form), 0: on the host   */
     long candidate_redone;           /* kNN queries whose ring search outgrew a
