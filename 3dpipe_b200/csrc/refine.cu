@@ -586,7 +586,12 @@ __device__ __forceinline__ void lazy_pre(const float4* __restrict__ t, float4 o,
            v3(t2.x - o.x, t2.y - o.y, t2.z - o.z));
 }
 
-template <int WARPS, int CA, int MINB>
+// ONE: a drain round gives each lane a whole queued pair (32 per round) and
+// the lane evaluates both halves of it, X = A and X = B, one after the other:
+// the same code as the two-lane rounds, so the minima are bit-identical, but
+// each pair's two PreTri are built once instead of once per half, and the two
+// halves are independent dependency chains the scheduler can interleave.
+template <int WARPS, int CA, int MINB, bool ONE = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const float4* __restrict__ triA,
                                                                     const float4* __restrict__ triB,
                                                                     const RefineItem* __restrict__ items,
@@ -695,7 +700,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                 int i = 0;
                 bool kc = false;
                 for (;;) {
-                    while (!flush && qn < 16 && i < ca) {
+                    while (!flush && qn < (ONE ? 32 : 16) && i < ca) {
                         if ((i & (kCl - 1)) == 0) {
                             kc = false;
                             if (bval) {
@@ -728,9 +733,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                         flush = false;
                         continue;
                     }
-                    const int take = min(qn, 16);
+                    const int take = min(qn, ONE ? 32 : 16);
                     __syncwarp();
-                    const int pl = lane & 15, part = lane >> 4;
+                    const int pl = ONE ? lane : lane & 15, part = ONE ? 0 : lane >> 4;
                     float d2 = FLT_MAX;
                     int qi = 0, qj = 0;
                     if (pl < take) {
@@ -738,11 +743,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                         qi = e >> 8;
                         qj = e & 0xff;
                         PreTri<float> X, Y;
-                        lazy_pre(part ? tB + (size_t)qj * kTriF4 : tA + (size_t)qi * kTriF4, o4, X);
-                        lazy_pre(part ? tA + (size_t)qi * kTriF4 : tB + (size_t)qj * kTriF4, o4, Y);
-                        d2 = tri_dist2_half(X, Y, part);
+                        if (ONE) {
+                            lazy_pre(tA + (size_t)qi * kTriF4, o4, X);
+                            lazy_pre(tB + (size_t)qj * kTriF4, o4, Y);
+                            d2 = fminf(tri_dist2_half(X, Y, 0), tri_dist2_half(Y, X, 1));
+                        } else {
+                            lazy_pre(part ? tB + (size_t)qj * kTriF4 : tA + (size_t)qi * kTriF4, o4, X);
+                            lazy_pre(part ? tA + (size_t)qi * kTriF4 : tB + (size_t)qj * kTriF4, o4, Y);
+                            d2 = tri_dist2_half(X, Y, part);
+                        }
                     }
-                    d2 = fminf(d2, __shfl_xor_sync(0xffffffffu, d2, 16));
+                    if (!ONE) d2 = fminf(d2, __shfl_xor_sync(0xffffffffu, d2, 16));
                     if (pl < take && part == 0) {
                         const float d = sqrtf(d2);
                         const float4 xa = auxA[qi], xb = auxB[qj];
@@ -796,9 +807,10 @@ struct TunedCfgDef {
     int chunk_a, ctas_per_sm;
 };
 // 0-2: PreTri staged in shared memory (refine_tuned_kernel); 3-7: bounds
-// staged, PreTri built per evaluated pair (refine_lazy_kernel)
+// staged, PreTri built per evaluated pair (refine_lazy_kernel); 8-9: the lazy
+// kernel with one lane per queued pair (both halves in the lane)
 constexpr TunedCfgDef kTunedCfgs[kTunedConfigs] = {{64, 3}, {48, 3}, {32, 4}, {128, 3}, {128, 4}, {64, 4},
-                                                    {128, 5}, {128, 6}};
+                                                    {128, 5}, {128, 6}, {128, 4}, {128, 5}};
 
 TunedConfig tuned_config(int cfg) {
     if (cfg < 0 || cfg >= kTunedConfigs) cfg = 0;
@@ -830,12 +842,12 @@ static cudaError_t launch_tuned_cfg(const float4* triA, const float4* triB, cons
     return cudaGetLastError();
 }
 
-template <int CA, int MINB>
+template <int CA, int MINB, bool ONE = false>
 static cudaError_t launch_lazy_cfg(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                    float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
                                    cudaStream_t s, const unsigned* n_items_dev, const float* init_bd) {
     const size_t smem = (size_t)kTunedWarps * LazyLayout<CA>::kWarpFloats * sizeof(float);
-    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB>;
+    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB, ONE>;
     cudaError_t e = cudaMemsetAsync(work_counter, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     long want = (long)num_sms * MINB;
@@ -859,6 +871,8 @@ cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const Re
         case 6: return launch_lazy_cfg<128, 5>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 7: return launch_lazy_cfg<128, 6>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 5: return launch_lazy_cfg<64, 4>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 8: return launch_lazy_cfg<128, 4, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 9: return launch_lazy_cfg<128, 5, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         default: return launch_tuned_cfg<64, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
     }
 }
