@@ -133,6 +133,11 @@ int tdp_ctx_create(int device, size_t budget_bytes, unsigned flags, tdp_ctx** ou
     for (auto& e : ctx->ev) cudaEventCreate(&e);
     for (auto& e : ctx->lod_ev) cudaEventCreate(&e);
     for (auto& e : ctx->xev) cudaEventCreate(&e);
+    for (auto& e : ctx->pf_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    if (cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess) {
+        tdp_ctx_destroy(ctx);
+        return TDP_ERR_CUDA;
+    }
     if (dmalloc(ctx, (void**)&ctx->d_counter, 64 * sizeof(unsigned)) != cudaSuccess ||
         dmalloc(ctx, (void**)&ctx->d_stats, 64 * sizeof(unsigned long long)) != cudaSuccess) {
         tdp_ctx_destroy(ctx);
@@ -152,6 +157,11 @@ int tdp_ctx_destroy(tdp_ctx* ctx) {
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->lod_ev) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->xev) if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->pf_ev) if (e) cudaEventDestroy(e);
+    if (ctx->side) {
+        cudaStreamSynchronize(ctx->side);
+        cudaStreamDestroy(ctx->side);
+    }
     cache_trim(ctx);
     if (ctx->lod_graph) cudaGraphExecDestroy(ctx->lod_graph);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

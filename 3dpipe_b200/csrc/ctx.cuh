@@ -57,6 +57,8 @@ struct tdp_ctx {
     cudaEvent_t ev[8] = {};
     cudaEvent_t lod_ev[16] = {};  // refine timing per LOD (tuned loop)
     cudaEvent_t xev[5] = {};      // phases of the exact-distance stage
+    cudaStream_t side = nullptr;  // second stream: the next LOD's prefetch (attached tiles)
+    cudaEvent_t pf_ev[16] = {};   // fork / join of the prefetches (no timing)
     std::string last_error;
     std::unordered_map<void*, size_t> allocs;
     tdp::Buf scratch[96];  // slots: refine-batch 0-4, tile upload 12-13, join 20-48, candidates 50-59, result sort 60-63, exact distances 64-81, per-object queries 82-83

@@ -127,7 +127,52 @@ __global__ void __launch_bounds__(kFetchWarps * 32) k_fetch_all(LazyTile L) {
     }
 }
 
+// lanes test 32 voxel pairs at once; the warp then fetches the flagged ones'
+// voxels one pair at a time (fetch_voxel is warp-cooperative and claims each
+// voxel once, so voxels shared by many pairs cost one state-word read each)
+__global__ void __launch_bounds__(kFetchWarps * 32) k_prefetch_pairs(const uint8_t* __restrict__ valive,
+                                                                     const int* __restrict__ vpair,
+                                                                     const uint8_t* pstat,
+                                                                     const int* __restrict__ vpa,
+                                                                     const int* __restrict__ vpb, int64_t V, int lod,
+                                                                     LazyTile A, LazyTile B) {
+    __shared__ uint32_t stage[kFetchWarps][kStageWords];
+    uint32_t* st = stage[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < V; base += warps * 32) {
+        const int64_t v = base + lane;
+        const bool want = v < V && valive[v] && pstat[vpair[v]] == 0;
+        unsigned m = __ballot_sync(0xffffffffu, want);
+        while (m) {
+            const int src = __ffs(m) - 1;
+            m &= m - 1;
+            const int64_t u = base + src;
+            if (A.on) {
+                const long a = vpa[u];
+                const uint32_t off = A.vtri[lod][a], n = A.vtri[lod][a + 1] - off;
+                if (n) fetch_voxel(A, lod, a, off, n, st);
+            }
+            if (B.on) {
+                const long b = vpb[u];
+                const uint32_t off = B.vtri[lod][b], n = B.vtri[lod][b + 1] - off;
+                if (n) fetch_voxel(B, lod, b, off, n, st);
+            }
+        }
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_prefetch_pairs(const uint8_t* valive, const int* vpair, const uint8_t* pstat, const int* vpa,
+                                  const int* vpb, int64_t V, int lod, const LazyTile& a, const LazyTile& b,
+                                  int num_sms, cudaStream_t s) {
+    if ((!a.on && !b.on) || V <= 0) return cudaSuccess;
+    const int64_t blocks_needed = (V + 32 * kFetchWarps - 1) / (32 * kFetchWarps);
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(blocks_needed, (int64_t)num_sms * 8));
+    k_prefetch_pairs<<<blocks, kFetchWarps * 32, 0, s>>>(valive, vpair, pstat, vpa, vpb, V, lod, a, b);
+    return cudaGetLastError();
+}
 
 LazyTile lazy_view(const tdp_tile* t) {
     LazyTile L;

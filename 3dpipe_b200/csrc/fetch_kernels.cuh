@@ -44,5 +44,13 @@ cudaError_t launch_fetch_items(const RefineItem* items, const unsigned* n_dev, l
                                const LazyTile& a, const LazyTile& b, int num_sms, cudaStream_t s);
 // fetch every voxel of every LOD of an attached tile
 cudaError_t launch_fetch_all(const LazyTile& t, int num_sms, cudaStream_t s);
+// prefetch, at LOD index lod, both voxels of every voxel pair v < V that is
+// alive and whose object pair is undecided (valive[v], pstat[vpair[v]] == 0):
+// a superset of the next LOD's refine items, run on a second stream beside
+// the current LOD's refine.  The flags may change meanwhile; a voxel that is
+// missed here is fetched by that LOD's own launch_fetch_items.
+cudaError_t launch_prefetch_pairs(const uint8_t* valive, const int* vpair, const uint8_t* pstat, const int* vpa,
+                                  const int* vpb, int64_t V, int lod, const LazyTile& a, const LazyTile& b,
+                                  int num_sms, cudaStream_t s);
 
 }  // namespace tdp

@@ -76,6 +76,8 @@ struct LodLoop {
     double *vexact, *res64, *pexact;
     cudaEvent_t ev[16];
     LazyTile lz1, lz2;  // attached tiles: fetch each LOD's voxels before its refine
+    cudaStream_t side;  // attached tiles: the next LOD's prefetch runs here
+    cudaEvent_t pf[16];
 };
 
 // Enqueue the loop on s.  While s is being captured, the per-LOD timing events
@@ -92,11 +94,24 @@ int enqueue_lod_loop(tdp_ctx* ctx, const LodLoop& L, cudaStream_t s, bool captur
     const int V = (int)L.V;
     CUL(cudaMemsetAsync(L.counter + 8, 0, 26 * sizeof(unsigned), s));
     CUL(cudaMemsetAsync(L.dstats, 0, 8, s));
+    // Attached tiles: once LOD k's own voxels are fetched, a second stream
+    // prefetches LOD k+1 for every live voxel pair of an undecided object pair
+    // (a superset of LOD k+1's items) while LOD k refines; LOD k+1's fetch
+    // waits for it first and then copies only what the prefetch missed.
+    const bool prefetch = (L.lz1.on || L.lz2.on) && L.side;
     for (int k = 0; k < L.nl; ++k) {
         const int highest = k == L.highest_k;
         CUL(cudaMemsetAsync(cnt_items, 0, 4, s));
         CUL(launch_build_items(L.d, L.vt1[k], L.vt2[k], L.items, L.item_vp, cnt_items, s));
+        if (prefetch && k > 0) CUL(cudaStreamWaitEvent(s, L.pf[2 * (k - 1) + 1], 0));
         CUL(launch_fetch_items(L.items, cnt_items, 0, L.li[k], L.lz1, L.lz2, L.num_sms, s));
+        if (prefetch && k + 1 < L.nl) {
+            CUL(cudaEventRecord(L.pf[2 * k], s));
+            CUL(cudaStreamWaitEvent(L.side, L.pf[2 * k], 0));
+            CUL(launch_prefetch_pairs(L.d.valive, L.d.vpair, L.d.pstat, L.d.vpa, L.d.vpb, L.V, L.li[k + 1], L.lz1,
+                                      L.lz2, L.num_sms, L.side));
+            CUL(cudaEventRecord(L.pf[2 * k + 1], L.side));
+        }
         CUL(cudaMemcpyAsync(lod_counts + k, cnt_items, 4, cudaMemcpyDeviceToDevice, s));
         CUL(rec(L.ev[2 * k]));
         CUL(launch_refine_tuned(L.tri1[k], L.tri2[k], L.items, V, L.res, L.counter, L.dstats, L.num_sms, L.cfg[k], s,
@@ -445,6 +460,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         L.rankst = buf<int>(ctx, kRankSt);
         L.vexact = buf<double>(ctx, kVexact); L.res64 = buf<double>(ctx, kRes64); L.pexact = buf<double>(ctx, kPexact);
         L.lz1 = lz1; L.lz2 = lz2;
+        L.side = ctx->side;
+        for (int k = 0; k < 16; ++k) L.pf[k] = ctx->pf_ev[k];
         if ((rc = run_lod_loop(ctx, L, s, &st.lod_graph))) return rc;
         launches += 5 * L.nl + (L.recheck ? (knn ? 6 : 5) : 0);
         st.refine_launches += L.nl;
