@@ -75,10 +75,13 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         objs = list(ex.map(lambda s: _compile(s, force, hdr_time), cu + cpp))
     newest = max(o.stat().st_mtime for o in objs)
     if force or not LIB.exists() or LIB.stat().st_mtime < newest:
-        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread"]
+        # link beside the library and rename over it, so a reader never sees a half-written file
+        tmp = LIB.with_name(LIB.name + ".tmp")
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+        os.replace(tmp, LIB)
     main = PKG / "src" / "join" / "tdbase_main.cpp"
     if main.exists():
         BIN.parent.mkdir(parents=True, exist_ok=True)
