@@ -591,7 +591,11 @@ __device__ __forceinline__ void lazy_pre(const float4* __restrict__ t, float4 o,
 // the same code as the two-lane rounds, so the minima are bit-identical, but
 // each pair's two PreTri are built once instead of once per half, and the two
 // halves are independent dependency chains the scheduler can interleave.
-template <int WARPS, int CA, int MINB, bool ONE = false>
+// SEEDS: only the SEEDS lanes whose seed bound is smallest queue their seed
+// (ties by lane); the other lanes' seed pairs go through the cull like any
+// other pair, against minima the first seeds have already tightened.  Every
+// cull is conservative, so the minima are the same for any SEEDS.
+template <int WARPS, int CA, int MINB, bool ONE = false, int SEEDS = 32>
 __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const float4* __restrict__ triA,
                                                                     const float4* __restrict__ triB,
                                                                     const RefineItem* __restrict__ items,
@@ -691,6 +695,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                     const float4 xs = auxA[seed];
                     const float thr = fmaxf(bd, fmaxf(bl + xs.x + ab.x, bh - xs.y - ab.y));
                     sq = seed_lb < thr;
+                }
+                if (SEEDS < 32) {
+                    // this lane's rank among the queued seeds by (bound, lane)
+                    const float key = sq ? seed_lb : FLT_MAX;
+                    int rank = 0;
+#pragma unroll 8
+                    for (int o = 0; o < 32; ++o) {
+                        const float k2 = __shfl_sync(0xffffffffu, key, o);
+                        rank += (k2 < key) || (k2 == key && o < lane);
+                    }
+                    sq = sq && rank < SEEDS;
                 }
                 if (!sq) seed = -1;
                 const unsigned sqm = __ballot_sync(0xffffffffu, sq);
@@ -808,9 +823,10 @@ struct TunedCfgDef {
 };
 // 0-2: PreTri staged in shared memory (refine_tuned_kernel); 3-7: bounds
 // staged, PreTri built per evaluated pair (refine_lazy_kernel); 8-9: the lazy
-// kernel with one lane per queued pair (both halves in the lane)
+// kernel with one lane per queued pair (both halves in the lane); 10-11: the
+// lazy kernel, two lanes and one lane per pair, queuing 8 seeds first
 constexpr TunedCfgDef kTunedCfgs[kTunedConfigs] = {{64, 3}, {48, 3}, {32, 4}, {128, 3}, {128, 4}, {64, 4},
-                                                    {128, 5}, {128, 6}, {128, 4}, {128, 5}};
+                                                    {128, 5}, {128, 6}, {128, 4}, {128, 5}, {128, 5}, {128, 5}};
 
 TunedConfig tuned_config(int cfg) {
     if (cfg < 0 || cfg >= kTunedConfigs) cfg = 0;
@@ -842,12 +858,12 @@ static cudaError_t launch_tuned_cfg(const float4* triA, const float4* triB, cons
     return cudaGetLastError();
 }
 
-template <int CA, int MINB, bool ONE = false>
+template <int CA, int MINB, bool ONE = false, int SEEDS = 32>
 static cudaError_t launch_lazy_cfg(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                    float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
                                    cudaStream_t s, const unsigned* n_items_dev, const float* init_bd) {
     const size_t smem = (size_t)kTunedWarps * LazyLayout<CA>::kWarpFloats * sizeof(float);
-    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB, ONE>;
+    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB, ONE, SEEDS>;
     cudaError_t e = cudaMemsetAsync(work_counter, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     long want = (long)num_sms * MINB;
@@ -873,6 +889,8 @@ cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const Re
         case 5: return launch_lazy_cfg<64, 4>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 8: return launch_lazy_cfg<128, 4, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 9: return launch_lazy_cfg<128, 5, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 10: return launch_lazy_cfg<128, 5, false, 8>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 11: return launch_lazy_cfg<128, 5, true, 8>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         default: return launch_tuned_cfg<64, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
     }
 }

@@ -107,7 +107,8 @@ int tdp_fp32_peak(tdp_ctx *ctx, double *tflops);
  * staged per warp and resident CTAs per SM (configurations 0-2 stage each
  * triangle's full pre-processed record in shared memory; 3-7 stage only its
  * bounds and pre-process the triangles of each evaluated pair in registers;
- * 8-9 do the same with one lane per evaluated pair).  All return identical results;
+ * 8-9 do the same with one lane per evaluated pair; 10-11 are 6 and 9 queuing
+ * only the 8 most promising first pairs before the cull).  All return identical results;
  * they differ only in speed, which depends on the voxel sizes of the join.
  * A context starts with configuration 0.  The reference has one fixed launch
  * shape (one CTA of 512 threads per voxel pair,
