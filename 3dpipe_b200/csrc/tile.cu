@@ -19,6 +19,7 @@
 #include <string>
 #include <vector>
 
+#include "attach_kernels.cuh"
 #include "ctx.cuh"
 #include "storage/dev_tile.h"
 #include "tile_kernels.cuh"
@@ -91,6 +92,154 @@ void tile_release(tdp_ctx* ctx, tdp_tile* t) {
     delete t;
 }
 
+constexpr int kUseHostParse = -1000;
+
+// The attach path with the voxel tables read on the GPU.  Returns TDP_OK (T
+// attached) or, with T released in both cases, kUseHostParse (parse on the
+// host instead) or an error.
+template <typename GrowStage>
+static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const uint8_t* dev_view, size_t len,
+                         long max_objects, int slot, GrowStage& grow_stage, std::chrono::steady_clock::time_point t0) {
+    auto ms_since = [](std::chrono::steady_clock::time_point a) {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+    };
+    HostVec<RawRec> recs;
+    if (!walk_raw_dt(buf, len, max_objects, recs) || recs.empty()) {
+        tile_release(ctx, T);
+        return kUseHostParse;
+    }
+    const long n = (long)recs.size();
+    uint64_t nvox = 0, meta_bytes = 0;
+    for (const RawRec& r : recs) {
+        nvox += r.vnum;
+        meta_bytes += 2 * kNumLods * 4 + r.vnum * 116 + 12;
+    }
+    if (nvox >= 0xffffffffull) {
+        tile_release(ctx, T);
+        return kUseHostParse;
+    }
+    TileHost& H = T->host;
+    H.n_obj = n;
+    H.n_vox = (long)nvox;
+    H.obj_vox_off.resize(n + 1);
+    H.obj_data_off.resize(n);
+    H.obj_data_size.resize(n);
+    // the object records go up through the staging slot, obj_vox[n] after them
+    grow_stage((size_t)(n + 1) * sizeof(AttachRec) + 64);
+    AttachRec* ar = (AttachRec*)ctx->hstage[slot];
+    std::vector<AttachRec> ar_pageable;
+    if (!ar) {
+        ar_pageable.resize(n + 1);
+        ar = ar_pageable.data();
+    }
+    uint32_t v0 = 0;
+    for (long o = 0; o < n; ++o) {
+        const RawRec& r = recs[o];
+        ar[o] = AttachRec{r.data_off, r.data_size, r.meta, (uint32_t)r.vnum, v0};
+        H.obj_vox_off[o] = v0;
+        H.obj_data_off[o] = r.data_off;
+        H.obj_data_size[o] = r.data_size;
+        v0 += (uint32_t)r.vnum;
+    }
+    H.obj_vox_off[n] = v0;
+    uint32_t* nvox_src = reinterpret_cast<uint32_t*>(ar + n);
+    *nvox_src = v0;
+    T->parse_ms = ms_since(t0);
+    const auto ta = std::chrono::steady_clock::now();
+    T->n_obj = n;
+    T->n_vox = (long)nvox;
+    cudaStream_t s = ctx->stream;
+    auto alloc = [&](void** p, size_t bytes) -> int {
+        if (block_alloc(ctx, p, bytes) != cudaSuccess)
+            return fail(ctx, TDP_ERR_NOMEM, "tile attach: cannot allocate " + std::to_string(bytes) + " bytes" +
+                                                (ctx->budget ? " within the context budget" : ""));
+        T->device_bytes += bytes;
+        return TDP_OK;
+    };
+#define GTRY(x) do { int _r = (x); if (_r) { cudaStreamSynchronize(s); tile_release(ctx, T); return _r; } } while (0)
+#define GCTRY(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) { cudaStreamSynchronize(s); tile_release(ctx, T); return fail(ctx, TDP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); } } while (0)
+    GTRY(alloc((void**)&T->vox, (size_t)nvox * 3 * sizeof(float4)));
+    GTRY(alloc((void**)&T->obj_vox, (size_t)(n + 1) * sizeof(uint32_t)));
+    GTRY(alloc((void**)&T->obj_hd, (size_t)n * kNumLods * sizeof(float)));
+    GTRY(alloc((void**)&T->obj_phd, (size_t)n * kNumLods * sizeof(float)));
+    for (int l = 0; l < kNumLods; ++l) GTRY(alloc((void**)&T->vtri[l], (size_t)(nvox + 1) * sizeof(uint32_t)));
+    GTRY(alloc((void**)&T->lazy_data_off, (size_t)n * sizeof(uint64_t)));
+    GTRY(alloc((void**)&T->lazy_state, (size_t)kNumLods * std::max<uint64_t>(nvox, 1) * sizeof(unsigned)));
+    GTRY(alloc((void**)&T->lazy_bytes, sizeof(unsigned long long)));
+    GTRY(alloc((void**)&T->d_boxes, (size_t)n * 9 * sizeof(float)));
+    T->boxes_n = n;
+    Buf& recs_d = ctx->scratch[96];
+    Buf& off4 = ctx->scratch[97];
+    Buf& vobj = ctx->scratch[98];
+    Buf& tmp = ctx->scratch[99];
+    Buf& ctr = ctx->scratch[100];
+    GTRY(ensure(ctx, recs_d, (size_t)(n + 1) * sizeof(AttachRec)));
+    GTRY(ensure(ctx, off4, (size_t)kNumLods * std::max<uint64_t>(nvox, 1) * sizeof(uint32_t)));
+    GTRY(ensure(ctx, vobj, (size_t)std::max<uint64_t>(nvox, 1) * sizeof(uint32_t)));
+    GTRY(ensure(ctx, ctr, 16 * sizeof(unsigned long long)));
+    AttachOut o{};
+    o.vox = T->vox;
+    o.obj_vox = T->obj_vox;
+    o.obj_hd = T->obj_hd;
+    o.obj_phd = T->obj_phd;
+    o.boxes = T->d_boxes;
+    o.data_off = T->lazy_data_off;
+    for (int l = 0; l < kNumLods; ++l) {
+        o.vtri[l] = T->vtri[l];
+        o.off4[l] = (uint32_t*)off4.p + (size_t)l * nvox;
+    }
+    o.vobj = (uint32_t*)vobj.p;
+    o.n_tris = (unsigned long long*)ctr.p;
+    o.first_bad = (unsigned long long*)ctr.p + 8;
+    size_t scan_bytes = 0;
+    GCTRY(launch_attach_tables(dev_view, nullptr, n, (long)nvox, o, nullptr, scan_bytes, ctx->num_sms, s));
+    GTRY(ensure(ctx, tmp, scan_bytes + 16));
+    T->alloc_ms = ms_since(ta);
+    const auto tm = std::chrono::steady_clock::now();
+    GCTRY(cudaMemcpyAsync(recs_d.p, ar, (size_t)n * sizeof(AttachRec), cudaMemcpyHostToDevice, s));
+    GCTRY(cudaMemcpyAsync(T->obj_vox + n, nvox_src, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    GCTRY(cudaMemsetAsync(ctr.p, 0, 8 * sizeof(unsigned long long), s));
+    GCTRY(cudaMemsetAsync((unsigned long long*)ctr.p + 8, 0xff, sizeof(unsigned long long), s));
+    GCTRY(launch_attach_tables(dev_view, (const AttachRec*)recs_d.p, n, (long)nvox, o, tmp.p, scan_bytes,
+                               ctx->num_sms, s));
+    unsigned long long res[9] = {0};
+    GCTRY(cudaMemcpyAsync(res, ctr.p, 9 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    H.obj_box.resize((size_t)6 * n);
+    H.obj_xf.resize((size_t)3 * n);
+    GCTRY(cudaMemcpyAsync(H.obj_box.data(), T->d_boxes, (size_t)6 * n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    GCTRY(cudaMemcpyAsync(H.obj_xf.data(), T->d_boxes + 6 * n, (size_t)3 * n * sizeof(float),
+                          cudaMemcpyDeviceToHost, s));
+    if (!ctx->hstage_ev[slot]) GCTRY(cudaEventCreateWithFlags(&ctx->hstage_ev[slot], cudaEventDisableTiming));
+    GCTRY(cudaEventRecord(ctx->hstage_ev[slot], s));
+    GCTRY(cudaStreamSynchronize(s));
+    if (res[8] != ~0ull) {  // a check failed: the host parser reports it
+        tile_release(ctx, T);
+        return kUseHostParse;
+    }
+    for (int l = 0; l < kNumLods; ++l) {
+        if (res[l] >= 0xffffffffull) {
+            tile_release(ctx, T);
+            return fail(ctx, TDP_ERR_FORMAT, "more than 2^32 triangles in one LOD");
+        }
+        H.n_tris[l] = res[l];
+    }
+    for (int l = 0; l < kNumLods; ++l) GTRY(alloc((void**)&T->tri[l], (size_t)H.n_tris[l] * 3 * sizeof(float4)));
+    GCTRY(cudaMemsetAsync(T->lazy_state, 0, (size_t)kNumLods * nvox * sizeof(unsigned), s));
+    GCTRY(cudaMemsetAsync(T->lazy_bytes, 0, sizeof(unsigned long long), s));
+    if (ctx->flags & TDP_CTX_POISON)
+        for (int l = 0; l < kNumLods; ++l)
+            GCTRY(cudaMemsetAsync(T->tri[l], 0xff, (size_t)H.n_tris[l] * 3 * sizeof(float4), s));
+#undef GTRY
+#undef GCTRY
+    T->h2d_bytes = (size_t)n * sizeof(AttachRec) + meta_bytes;  // the records, and the tables the GPU read
+    T->meta_ms = ms_since(tm);
+    T->lazy_raw = dev_view;
+    T->lazy_on = true;
+    T->lazy_stride = (long)nvox;
+    T->load_ms = ms_since(t0);
+    return TDP_OK;
+}
+
 // Parse, validate and make a tile resident (attach == false), or attach it:
 // voxel and object metadata resident, triangle records allocated but filled
 // by the joins that need them, straight from the page-locked host bytes.
@@ -146,6 +295,20 @@ int tile_load(tdp_ctx* ctx, const void* raw_dt, size_t len, long max_objects, bo
             ctx->hstage_cap[slot] = need + need / 4;
         else { cudaGetLastError(); ctx->hstage[slot] = nullptr; }
     };
+    // ---- attach: the host walks the size fields, the GPU reads the voxel tables ----
+    // (csrc/attach_kernels.cu).  A tile the walk cannot take, or whose tables
+    // fail a check, goes through the host parser below, which reports the
+    // first error in file order.
+    if (attach) {
+        const int grc = attach_on_gpu(ctx, T, buf, dev_view, len, max_objects, slot, grow_stage, t0);
+        if (grc == TDP_OK) {
+            *out = T;
+            return TDP_OK;
+        }
+        if (grc != kUseHostParse) return grc;  // T released
+        T = new tdp_tile();
+        T->device = ctx->device;
+    }
     int rc = parse_raw_dt(buf, len, max_objects, T->host, err, [&](long n_vox, long n_obj) -> float* {
         grow_stage(stage_bytes(n_vox, n_obj));
         return (float*)ctx->hstage[slot];  // nullptr when page-locked memory is short

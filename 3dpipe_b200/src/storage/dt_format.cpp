@@ -206,9 +206,7 @@ int parse_sequential(const uint8_t* buf, size_t len, long max_objects, TileHost&
 
 namespace {
 
-struct Rec {
-    uint64_t data_off, data_size, meta, vnum;
-};
+using Rec = RawRec;
 
 // One voxel record in the device layout (low xyz, 0, high xyz, 0, core xyz,
 // 0).  The records are read again only by the copy to the device, so on x86
@@ -288,12 +286,9 @@ bool walk_chain(const uint8_t* buf, size_t len, size_t& pos, long limit, Rec* ou
 // parallel into arrays sized from the walk.  Content errors are reported for
 // the lowest object that has one, the error the sequential parser would meet
 // first, with the same message.
-int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, std::string& err,
-                 const VoxSink& sink) {
-    T = TileHost();
-    if (!buf || len < 1) { err = "empty tile buffer"; return TDP_ERR_FORMAT; }
-    if (buf[0] != kRawType) return parse_sequential(buf, len, max_objects, T, err);
-    HostVec<Rec> recs;
+bool walk_raw_dt(const uint8_t* buf, size_t len, long max_objects, HostVec<RawRec>& recs) {
+    recs.clear();
+    if (!buf || len < 1 || buf[0] != kRawType) return false;
     size_t pos = 1;
     // Objects of one tile are mostly the same size (instances of one mesh):
     // with many objects, threads walk chunks from guessed starts at the
@@ -349,9 +344,19 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
             c = 0;
             const bool ok = walk_chain(buf, len, q, block, &recs[at], c);
             recs.resize(at + (size_t)c);
-            if (!ok) return parse_sequential(buf, len, max_objects, T, err);
+            if (!ok) return false;
         }
     }
+    return true;
+}
+
+int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, std::string& err,
+                 const VoxSink& sink) {
+    T = TileHost();
+    if (!buf || len < 1) { err = "empty tile buffer"; return TDP_ERR_FORMAT; }
+    if (buf[0] != kRawType) return parse_sequential(buf, len, max_objects, T, err);
+    HostVec<Rec> recs;
+    if (!walk_raw_dt(buf, len, max_objects, recs)) return parse_sequential(buf, len, max_objects, T, err);
     uint64_t nvox = 0;
     for (const Rec& r : recs) nvox += r.vnum;
     if (nvox >= 0xffffffffull) return parse_sequential(buf, len, max_objects, T, err);

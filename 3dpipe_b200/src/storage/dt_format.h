@@ -125,6 +125,19 @@ void vtri_prefix(const TileHost& T, uint32_t* const out[kNumLods], uint32_t* con
 // nullptr (or the tile takes the sequential parser), vox_box is filled.
 using VoxSink = std::function<float*(long n_vox, long n_obj)>;
 
+// One object's record as the walk over the size fields finds it: where its
+// data block starts and how long it is, where its metadata start (the
+// per-LOD object Hausdorff values, after vnum) and how many voxels it has.
+struct RawRec {
+    uint64_t data_off, data_size, meta, vnum;
+};
+
+// The walk alone (the first pass of parse_raw_dt): the records of at most
+// max_objects objects (<= 0: all).  Returns false on a structural problem
+// (parse_raw_dt then reports it) or when the tile does not start with the RAW
+// type byte; the voxel tables are not read.
+bool walk_raw_dt(const uint8_t* buf, size_t len, long max_objects, HostVec<RawRec>& recs);
+
 // Parse `len` bytes; at most max_objects objects (<= 0: all).  Returns 0 or a
 // TDP_ERR_* code with a message in `err`.
 int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& out, std::string& err,

@@ -123,3 +123,48 @@ def test_attach_refusals(pkg, pctx):
     with pytest.raises(pkg.TdpError) as e:
         pkg.tdp.Tile(pctx, pkg.tdp.pinned_copy(shuffled), attach=True)
     assert e.value.code == 4
+
+
+def test_attach_reports_content_errors_like_the_host_parser(pkg, pctx):
+    """The attach's metadata pass runs on the GPU; a voxel table it finds
+    wrong sends the tile to the host parser, so the error is the one a
+    sequential read meets first, with the host parser's message."""
+    import struct
+    from test_raw_parse import corrupt_box
+    nb, _ = pkg.tdp.gen_tiles(10, 200, seed=5)
+    off = pkg.tdp.raw_object_offsets(nb)
+    for bad in ([7], [1500, 40]):
+        b = nb
+        for o in bad:
+            b = corrupt_box(b, off, o)
+        with pytest.raises(pkg.TdpError) as e:
+            pkg.tdp.Tile(pctx, pkg.tdp.pinned_copy(b), attach=True)
+        assert e.value.code == 4
+        assert str(e.value).endswith("inverted voxel box in object %d" % min(bad))
+    b = nb.copy()
+    p = int(off[321])
+    (ds,) = struct.unpack_from("<Q", b, p)
+    struct.pack_into("<Q", b, p + 8 + ds + 8 + 40 + 36, ds + 4)  # first voxel's LOD-20 offset past the data block
+    with pytest.raises(pkg.TdpError) as e:
+        pkg.tdp.Tile(pctx, pkg.tdp.pinned_copy(b), attach=True)
+    assert str(e.value).endswith("voxel lod range outside data block in object 321")
+
+
+def test_attached_metadata_equal_uploaded(pkg, pctx):
+    """Counts, boxes and transforms the GPU pass derives equal the host parser's."""
+    nb, vb = tiles(8, 10, 104)
+    for raw in (nb, vb):
+        U = pkg.tdp.Tile(pctx, raw)
+        A = pkg.tdp.Tile(pctx, pkg.tdp.pinned_copy(raw), attach=True)
+        iu, ia = U.info(), A.info()
+        for k in ("n_objects", "n_voxels", "n_tris"):
+            assert iu[k] == ia[k], k
+        assert ia["attached"] == 1
+        # the GPU candidates read the attached tile's boxes and transforms
+        for kw in (dict(knn=3), dict(within=200.0)):
+            o1, i1 = pkg.tdp.tile_candidates(pctx, U, None, **kw)
+            o2, i2 = pkg.tdp.tile_candidates(pctx, A, None, **kw)
+            np.testing.assert_array_equal(o1, o2)
+            np.testing.assert_array_equal(i1, i2)
+        U.free()
+        A.free()
