@@ -553,7 +553,49 @@ struct LazyLayout {
     static constexpr int kOffQueue = kOffAuxB + 4 * kCB;
     static constexpr int kWarpFloats = kOffQueue + kQueue / 2;
     static_assert(kWarpFloats % 4 == 0, "float4 arrays must stay 16-byte aligned");
+    // bulk-copy staging (TMA configurations): the raw 48-byte records of the
+    // A chunk and of the B chunk, and the warp's mbarrier
+    static constexpr int kOffRawA = kWarpFloats;
+    static constexpr int kOffRawB = kOffRawA + 4 * kTriF4 * CA;
+    static constexpr int kOffBar = kOffRawB + 4 * kTriF4 * kCB;
+    static constexpr int kWarpFloatsTma = kOffBar + 4;
+    static_assert(kOffRawA % 4 == 0 && kOffRawB % 4 == 0 && kOffBar % 2 == 0 && kWarpFloatsTma % 4 == 0,
+                  "staging must stay 16-byte aligned, the mbarrier 8-byte aligned");
 };
+
+// ---- 1-D bulk copies (TMA) into shared memory, completion on an mbarrier ----
+// Plain global-to-shared copies of this GPU's own memory: no cluster, no
+// multicast.  The size and both addresses are multiples of 16 bytes (whole
+// 48-byte triangle records of 16-byte aligned arrays).
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// lane 0: the one arrival of this phase, expecting `bytes`, then the copy
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+// wait for phase `parity` of the barrier, at most kMbarTries polls; false on
+// giving up (the caller flags it; a copy of valid memory always completes)
+constexpr int kMbarTries = 1 << 16;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    for (int i = 0; i < kMbarTries; ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
 
 // Bounds of raw triangle record idx relative to o (the formulas of stage_one /
 // tri_sphere): sphere = (centre, radius), aux = (ph, h, projection on u).
@@ -595,7 +637,11 @@ __device__ __forceinline__ void lazy_pre(const float4* __restrict__ t, float4 o,
 // (ties by lane); the other lanes' seed pairs go through the cull like any
 // other pair, against minima the first seeds have already tightened.  Every
 // cull is conservative, so the minima are the same for any SEEDS.
-template <int WARPS, int CA, int MINB, bool ONE = false, int SEEDS = 32>
+// TMA: each A chunk and each B chunk is first brought into shared memory by
+// one 1-D bulk copy (cp.async.bulk, completion on the warp's mbarrier); the
+// bounds pass and the evaluations then read the records from shared memory.
+// A wait that gives up sets work_counter[1] and leaves the item's results NaN.
+template <int WARPS, int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const float4* __restrict__ triA,
                                                                     const float4* __restrict__ triB,
                                                                     const RefineItem* __restrict__ items,
@@ -609,7 +655,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
     using L = LazyLayout<CA>;
     constexpr int kCA = CA;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float* ws = smem + (size_t)wid * L::kWarpFloats;
+    float* ws = smem + (size_t)wid * (TMA ? L::kWarpFloatsTma : L::kWarpFloats);
+    float4* rawA = reinterpret_cast<float4*>(ws + L::kOffRawA);
+    float4* rawB = reinterpret_cast<float4*>(ws + L::kOffRawB);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(ws + L::kOffBar);
+    unsigned phase = 0;
+    bool stalled = false;
+    if (TMA) {
+        if (lane == 0) mbar_init(bar);
+        fence_async_shared();
+        __syncwarp();
+    }
     float4* sphA = reinterpret_cast<float4*>(ws);
     float4* auxA = reinterpret_cast<float4*>(ws + L::kOffAuxA);
     float4* clS = reinterpret_cast<float4*>(ws + L::kOffClS);
@@ -653,6 +709,16 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
             const int ncl = (ca + kCl - 1) / kCl;
             const float4* tA = triA + ((size_t)w.a_off + a0) * kTriF4;
             __syncwarp();
+            if (TMA) {
+                // every lane is done with the previous chunk's records
+                if (lane == 0) {
+                    fence_async_shared();
+                    bulk_load(rawA, tA, (unsigned)ca * kTriF4 * 16u, bar);
+                }
+                stalled |= !mbar_wait(bar, phase);
+                phase ^= 1u;
+                tA = rawA;
+            }
             for (int k = lane; k < ca; k += 32) lazy_bounds(tA, k, o4, u, false, rmax, sphA[k], auxA[k]);
             __syncwarp();
             build_clusters<CA>(sphA, auxA, ca, clS, clA, lane);
@@ -660,6 +726,15 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                 const int cb = min((uint32_t)kCB, w.b_cnt - b0);
                 const float4* tB = triB + ((size_t)w.b_off + b0) * kTriF4;
                 __syncwarp();
+                if (TMA) {
+                    if (lane == 0) {
+                        fence_async_shared();
+                        bulk_load(rawB, tB, (unsigned)cb * kTriF4 * 16u, bar);
+                    }
+                    stalled |= !mbar_wait(bar, phase);
+                    phase ^= 1u;
+                    tB = rawB;
+                }
                 const bool bval = lane < cb;
                 float4 sb = make_float4(0.f, 0.f, 0.f, 0.f), ab = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (bval) {
@@ -794,6 +869,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
         if (init_bd && !(bd < b_init)) bd = FLT_MAX;
+        if (TMA && __any_sync(0xffffffffu, stalled)) {
+            const float nan = __int_as_float(0x7fc00000);
+            bd = bl = bh = nan;
+            if (lane == 0) atomicOr(work_counter + 1, 1u);
+        }
         if (lane == 0) out[it] = make_float4(bd, bl, bh, rmax);
         it = __shfl_sync(0xffffffffu, next, 0);
     }
@@ -824,9 +904,11 @@ struct TunedCfgDef {
 // 0-2: PreTri staged in shared memory (refine_tuned_kernel); 3-7: bounds
 // staged, PreTri built per evaluated pair (refine_lazy_kernel); 8-9: the lazy
 // kernel with one lane per queued pair (both halves in the lane); 10-11: the
-// lazy kernel, two lanes and one lane per pair, queuing 8 seeds first
+// lazy kernel, two lanes and one lane per pair, queuing 8 seeds first;
+// 12-13: the lazy kernel staging its raw records by 1-D bulk copies (TMA)
 constexpr TunedCfgDef kTunedCfgs[kTunedConfigs] = {{64, 3}, {48, 3}, {32, 4}, {128, 3}, {128, 4}, {64, 4},
-                                                    {128, 5}, {128, 6}, {128, 4}, {128, 5}, {128, 5}, {128, 5}};
+                                                    {128, 5}, {128, 6}, {128, 4}, {128, 5}, {128, 5}, {128, 5},
+                                                    {128, 4}, {64, 5}};
 
 TunedConfig tuned_config(int cfg) {
     if (cfg < 0 || cfg >= kTunedConfigs) cfg = 0;
@@ -858,12 +940,23 @@ static cudaError_t launch_tuned_cfg(const float4* triA, const float4* triB, cons
     return cudaGetLastError();
 }
 
-template <int CA, int MINB, bool ONE = false, int SEEDS = 32>
+template <int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false>
 static cudaError_t launch_lazy_cfg(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                    float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
                                    cudaStream_t s, const unsigned* n_items_dev, const float* init_bd) {
-    const size_t smem = (size_t)kTunedWarps * LazyLayout<CA>::kWarpFloats * sizeof(float);
-    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB, ONE, SEEDS>;
+    const size_t smem = (size_t)kTunedWarps *
+                        (TMA ? LazyLayout<CA>::kWarpFloatsTma : LazyLayout<CA>::kWarpFloats) * sizeof(float);
+    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB, ONE, SEEDS, TMA>;
+    if (smem > 48 * 1024) {
+        static bool attr_set[64] = {};  // per device
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+            const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            if (dev >= 0 && dev < 64) attr_set[dev] = true;
+        }
+    }
     cudaError_t e = cudaMemsetAsync(work_counter, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     long want = (long)num_sms * MINB;
@@ -891,6 +984,8 @@ cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const Re
         case 9: return launch_lazy_cfg<128, 5, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 10: return launch_lazy_cfg<128, 5, false, 8>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 11: return launch_lazy_cfg<128, 5, true, 8>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 12: return launch_lazy_cfg<128, 4, false, 32, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 13: return launch_lazy_cfg<64, 5, false, 32, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         default: return launch_tuned_cfg<64, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
     }
 }
