@@ -715,8 +715,12 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                     fence_async_shared();
                     bulk_load(rawA, tA, (unsigned)ca * kTriF4 * 16u, bar);
                 }
-                stalled |= !mbar_wait(bar, phase);
+                const bool ok = mbar_wait(bar, phase);
                 phase ^= 1u;
+                if (__any_sync(0xffffffffu, !ok)) {
+                    stalled = true;
+                    break;
+                }
                 tA = rawA;
             }
             for (int k = lane; k < ca; k += 32) lazy_bounds(tA, k, o4, u, false, rmax, sphA[k], auxA[k]);
@@ -731,8 +735,12 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                         fence_async_shared();
                         bulk_load(rawB, tB, (unsigned)cb * kTriF4 * 16u, bar);
                     }
-                    stalled |= !mbar_wait(bar, phase);
+                    const bool ok = mbar_wait(bar, phase);
                     phase ^= 1u;
+                    if (__any_sync(0xffffffffu, !ok)) {
+                        stalled = true;
+                        break;
+                    }
                     tB = rawB;
                 }
                 const bool bval = lane < cb;
@@ -865,14 +873,20 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                     if (i >= ca) flush = true;
                 }
             }
+            if (TMA && stalled) break;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) rmax = fmaxf(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
         if (init_bd && !(bd < b_init)) bd = FLT_MAX;
-        if (TMA && __any_sync(0xffffffffu, stalled)) {
-            const float nan = __int_as_float(0x7fc00000);
-            bd = bl = bh = nan;
-            if (lane == 0) atomicOr(work_counter + 1, 1u);
+        if (TMA && stalled) {
+            // a bulk copy did not complete in time: flag it, mark the item
+            // NaN and end this warp (its later items are never claimed)
+            if (lane == 0) {
+                atomicOr(work_counter + 1, 1u);
+                const float nan = __int_as_float(0x7fc00000);
+                out[it] = make_float4(nan, nan, nan, rmax);
+            }
+            return;
         }
         if (lane == 0) out[it] = make_float4(bd, bl, bh, rmax);
         it = __shfl_sync(0xffffffffu, next, 0);
