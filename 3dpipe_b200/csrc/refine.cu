@@ -703,6 +703,37 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
             bd = b_init;
             bl = -FLT_MAX;
             bh = -FLT_MAX;
+            // item-level reject, as in refine_tuned_kernel: if no pair of
+            // (cluster, triangle) bounding spheres is closer than the preset,
+            // no triangle pair is, and the item has nothing below it
+            bool need = false;
+            for (uint32_t a0 = 0; a0 < w.a_cnt && !__any_sync(0xffffffffu, need); a0 += kCA) {
+                const int ca = min((uint32_t)kCA, w.a_cnt - a0);
+                const int ncl = (ca + kCl - 1) / kCl;
+                __syncwarp();
+                for (int k = lane; k < ca; k += 32) {
+                    sphA[k] = quick_sphere(triA + ((size_t)w.a_off + a0 + k) * kTriF4, o4);
+                    auxA[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                __syncwarp();
+                build_clusters<CA>(sphA, auxA, ca, clS, clA, lane);
+                __syncwarp();
+                for (uint32_t b0 = 0; b0 < w.b_cnt && !need; b0 += kCB) {
+                    if (b0 + lane >= w.b_cnt) break;
+                    const float4 sb = quick_sphere(triB + ((size_t)w.b_off + b0 + lane) * kTriF4, o4);
+                    for (int c = 0; c < ncl; ++c) {
+                        const float4 cs = clS[c];
+                        const float dx = cs.x - sb.x, dy = cs.y - sb.y, dz = cs.z - sb.z;
+                        const float reach = cs.w + sb.w + bd;
+                        if (dx * dx + dy * dy + dz * dz < reach * reach) { need = true; break; }
+                    }
+                }
+            }
+            if (!__any_sync(0xffffffffu, need)) {
+                if (lane == 0) out[it] = make_float4(FLT_MAX, -FLT_MAX, -FLT_MAX, 0.f);
+                it = __shfl_sync(0xffffffffu, next, 0);
+                continue;
+            }
         }
         for (uint32_t a0 = 0; a0 < w.a_cnt; a0 += kCA) {
             const int ca = min((uint32_t)kCA, w.a_cnt - a0);
