@@ -10,10 +10,9 @@
 // KB for a nucleus, every 170 KB of the file -- straight from the mapped host
 // bytes, instead of a host pass over them followed by copies of its results.
 // The blocks follow a one-byte header, so they are read as aligned 32-bit
-// words and realigned with a funnel shift (every field is 4 or 8 bytes from
-// its object's first byte).  A value's second word always holds some of the
-// value's own bytes, so no read leaves the page of a byte inside the record,
-// and every record lies inside the buffer (the walk checks it).
+// words, each once, and realigned with a funnel shift against the next word
+// (from the neighbouring lane); every word read holds bytes of the record,
+// which the walk checked lies inside the buffer.
 //
 // Validation: every check the host parser makes on these fields (voxel boxes
 // not inverted, each LOD range inside the object's data block, 4-byte
@@ -35,16 +34,30 @@ namespace {
 constexpr int kWarps = 8;
 constexpr int kVoxWords = 29;  // 9 floats + 5 x (offset, count) as u64
 constexpr int kChunkVox = 32;  // voxels per warp and round (one per lane)
+constexpr int kHdWords = 2 * kNumLods;
+constexpr int kStage = kHdWords + kChunkVox * kVoxWords + 3;  // words staged per window
 
-// the 32-bit value that starts sh/8 bytes into word k
-__device__ __forceinline__ uint32_t word_at(const uint32_t* W, uint64_t k, unsigned sh) {
-    return sh ? __funnelshift_r(W[k], W[k + 1], sh) : W[k];
+// st[i] = the 32-bit value that starts sh/8 bytes into word k0 + i of W, for
+// i < cnt.  Each word is read once: lane l holds word k0 + b + l and takes
+// the next word from lane l + 1 (lane 31 reads it itself).  Word k0 + cnt is
+// read only when sh != 0, and then it holds the last bytes of value cnt - 1,
+// so every word read lies on a page that the values occupy.
+__device__ __forceinline__ void stage_words(const uint32_t* W, uint64_t k0, uint32_t cnt, unsigned sh, int lane,
+                                            uint32_t* st) {
+    const uint32_t lim = cnt + (sh ? 1u : 0u);  // words [0, lim) may be read
+    for (uint32_t b = 0; b < cnt; b += 32) {
+        const uint32_t i = b + lane;
+        const uint32_t w = i < lim ? W[k0 + i] : 0u;
+        uint32_t nx = __shfl_down_sync(0xffffffffu, w, 1);
+        if (lane == 31) nx = (sh && i + 1 < lim) ? W[k0 + i + 1] : 0u;
+        if (i < cnt) st[i] = sh ? __funnelshift_r(w, nx, sh) : w;
+    }
 }
 
 __global__ void __launch_bounds__(kWarps * 32) k_parse_tables(const uint8_t* __restrict__ raw,
                                                               const AttachRec* __restrict__ recs, long n_obj,
                                                               AttachOut o) {
-    __shared__ uint32_t stage[kWarps][kChunkVox * kVoxWords];
+    __shared__ uint32_t stage[kWarps][kStage];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t* st = stage[w];
     const long nw = ((long)gridDim.x * blockDim.x) >> 5;
@@ -53,23 +66,28 @@ __global__ void __launch_bounds__(kWarps * 32) k_parse_tables(const uint8_t* __r
         const uintptr_t base = reinterpret_cast<uintptr_t>(raw) + r.meta;
         const uint32_t* W = reinterpret_cast<const uint32_t*>(base & ~uintptr_t(3));
         const unsigned sh = (unsigned)(base & 3) * 8;
+        const uint64_t xw = kHdWords + (uint64_t)r.vnum * kVoxWords;  // first transform word
         bool bad = false;
-        // object Hausdorff values: 5 x (hausdorff, proxy)
-        if (lane < 2 * kNumLods) {
-            const float v = __uint_as_float(word_at(W, lane, sh));
-            if (lane & 1) o.obj_phd[ob * kNumLods + (lane >> 1)] = v;
-            else o.obj_hd[ob * kNumLods + (lane >> 1)] = v;
-        }
         float lo0 = INFINITY, lo1 = INFINITY, lo2 = INFINITY, hi0 = -INFINITY, hi1 = -INFINITY, hi2 = -INFINITY;
         unsigned long long tris[kNumLods] = {0, 0, 0, 0, 0};
+        float xf = 0.f;
+        // windows of the metadata block: [Hausdorff values] 32 voxels [transform]
         for (uint32_t c0 = 0; c0 < r.vnum; c0 += kChunkVox) {
             const uint32_t m = min((uint32_t)kChunkVox, r.vnum - c0);
-            const uint64_t w0 = 2 * kNumLods + (uint64_t)c0 * kVoxWords;  // first word of this chunk
+            const bool last = c0 + m == r.vnum;
+            const uint64_t ws = c0 == 0 ? 0 : kHdWords + (uint64_t)c0 * kVoxWords;
+            const uint64_t we = kHdWords + (uint64_t)(c0 + m) * kVoxWords + (last ? 3 : 0);
             __syncwarp();
-            for (uint32_t k = lane; k < m * kVoxWords; k += 32) st[k] = word_at(W, w0 + k, sh);
+            stage_words(W, ws, (uint32_t)(we - ws), sh, lane, st);
             __syncwarp();
+            if (c0 == 0 && lane < kHdWords) {  // object Hausdorff values: 5 x (hausdorff, proxy)
+                const float v = __uint_as_float(st[lane]);
+                if (lane & 1) o.obj_phd[ob * kNumLods + (lane >> 1)] = v;
+                else o.obj_hd[ob * kNumLods + (lane >> 1)] = v;
+            }
+            if (last && lane < 3) xf = __uint_as_float(st[xw - ws + lane]);
             if (lane < m) {
-                const uint32_t* q = st + lane * kVoxWords;
+                const uint32_t* q = st + (kHdWords + (uint64_t)(c0 + lane) * kVoxWords - ws);
                 const uint32_t v = r.vox0 + c0 + lane;
                 float b[9];
 #pragma unroll
@@ -110,8 +128,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_parse_tables(const uint8_t* __r
 #pragma unroll
             for (int l = 0; l < kNumLods; ++l) tris[l] += __shfl_xor_sync(0xffffffffu, tris[l], s);
         }
-        const uint64_t xw = 2 * kNumLods + (uint64_t)r.vnum * kVoxWords;
-        if (lane < 3) o.boxes[6 * n_obj + 3 * ob + lane] = __uint_as_float(word_at(W, xw + lane, sh));
+        if (lane < 3) o.boxes[6 * n_obj + 3 * ob + lane] = xf;
         if (lane == 0) {
             float* bx = o.boxes + 6 * ob;
             bx[0] = lo0; bx[1] = lo1; bx[2] = lo2; bx[3] = hi0; bx[4] = hi1; bx[5] = hi2;
