@@ -550,9 +550,11 @@ struct LazyLayout {
     static constexpr int kOffClS = 8 * CA;
     static constexpr int kOffClA = kOffClS + 4 * kNCl;
     static constexpr int kOffAuxB = kOffClA + 4 * kNCl;
-    static constexpr int kOffQueue = kOffAuxB + 4 * kCB;
+    static constexpr int kOffSphB = kOffAuxB + 4 * kCB;    // B spheres (spread cull)
+    static constexpr int kOffSeedB = kOffSphB + 4 * kCB;   // each lane's queued seed, -1 for none
+    static constexpr int kOffQueue = kOffSeedB + kCB;
     static constexpr int kWarpFloats = kOffQueue + kQueue / 2;
-    static_assert(kWarpFloats % 4 == 0, "float4 arrays must stay 16-byte aligned");
+    static_assert(kWarpFloats % 4 == 0 && kOffSphB % 4 == 0, "float4 arrays must stay 16-byte aligned");
     // bulk-copy staging (TMA configurations): the raw 48-byte records of the
     // A chunk and of the B chunk, and the warp's mbarrier
     static constexpr int kOffRawA = kWarpFloats;
@@ -641,7 +643,12 @@ __device__ __forceinline__ void lazy_pre(const float4* __restrict__ t, float4 o,
 // one 1-D bulk copy (cp.async.bulk, completion on the warp's mbarrier); the
 // bounds pass and the evaluations then read the records from shared memory.
 // A wait that gives up sets work_counter[1] and leaves the item's results NaN.
-template <int WARPS, int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false>
+// SPREAD: the cull spreads a cluster's member tests over the warp -- one
+// test per lane for each (lane that needs the cluster, member) pair, 32 per
+// round, reading the B lane's sphere and bounds from shared memory -- instead
+// of every lane stepping through the 8 members while most of them need none.
+// The same pairs are queued (in another order), so the minima are the same.
+template <int WARPS, int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false, bool SPREAD = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const float4* __restrict__ triA,
                                                                     const float4* __restrict__ triB,
                                                                     const RefineItem* __restrict__ items,
@@ -671,6 +678,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
     float4* clS = reinterpret_cast<float4*>(ws + L::kOffClS);
     float4* clA = reinterpret_cast<float4*>(ws + L::kOffClA);
     float4* auxB = reinterpret_cast<float4*>(ws + L::kOffAuxB);
+    float4* sphB = reinterpret_cast<float4*>(ws + L::kOffSphB);
+    int* seedB = reinterpret_cast<int*>(ws + L::kOffSeedB);
     unsigned short* queue = reinterpret_cast<unsigned short*>(ws + L::kOffQueue);
     const unsigned lt_mask = (1u << lane) - 1u;
     unsigned long long full_evals = 0;
@@ -779,6 +788,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                 if (bval) {
                     lazy_bounds(tB, lane, o4, u, true, rmax, sb, ab);
                     auxB[lane] = ab;
+                    if (SPREAD) sphB[lane] = sb;
                 }
                 __syncwarp();
                 int seed = -1;
@@ -828,7 +838,60 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                 bool flush = true;
                 int i = 0;
                 bool kc = false;
+                // spread cull: the cluster being expanded (cm: the lanes that
+                // need it; t0: tests done) -- i then is its first member
+                unsigned cm = 0;
+                int t0 = 0;
+                if (SPREAD) {
+                    seedB[lane] = seed;
+                    __syncwarp();
+                }
                 for (;;) {
+                    if (SPREAD) {
+                        while (!flush && qn < (ONE ? 32 : 16) && (cm || i < ca)) {
+                            if (!cm) {
+                                bool need = false;
+                                if (bval) {
+                                    const float4 s = clS[i / kCl], a = clA[i / kCl];
+                                    const float thr = fmaxf(bd, fmaxf(bl + a.x + ab.x, bh - a.y - ab.y));
+                                    const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
+                                    const float reach = s.w + sb.w + thr;
+                                    need = ab.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach;
+                                }
+                                cm = __ballot_sync(0xffffffffu, need);
+                                t0 = 0;
+                                if (!cm) {
+                                    i += kCl;
+                                    continue;
+                                }
+                            }
+                            // one round: test t = t0 + lane is member t % 8 for the
+                            // (t / 8)-th lane of cm
+                            const int nt = __popc(cm) * kCl;
+                            const int t = t0 + lane;
+                            bool keep = false;
+                            int mi = 0, src = 0;
+                            if (t < nt) {
+                                src = (int)__fns(cm, 0, t / kCl + 1);
+                                mi = i + (t & (kCl - 1));
+                                if (mi < ca && mi != seedB[src]) {
+                                    const float4 s = sphA[mi], a = auxA[mi], sbq = sphB[src], abq = auxB[src];
+                                    const float thr = fmaxf(bd, fmaxf(bl + a.x + abq.x, bh - a.y - abq.y));
+                                    const float dx = s.x - sbq.x, dy = s.y - sbq.y, dz = s.z - sbq.z;
+                                    const float reach = s.w + sbq.w + thr;
+                                    keep = abq.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach;
+                                }
+                            }
+                            const unsigned m = __ballot_sync(0xffffffffu, keep);
+                            if (keep) queue[qn + __popc(m & lt_mask)] = (unsigned short)((mi << 8) | src);
+                            qn += __popc(m);
+                            t0 += 32;
+                            if (t0 >= nt) {
+                                cm = 0;
+                                i += kCl;
+                            }
+                        }
+                    } else
                     while (!flush && qn < (ONE ? 32 : 16) && i < ca) {
                         if ((i & (kCl - 1)) == 0) {
                             kc = false;
@@ -858,7 +921,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                         ++i;
                     }
                     if (qn == 0) {
-                        if (i >= ca) break;
+                        if (i >= ca && !cm) break;
                         flush = false;
                         continue;
                     }
@@ -900,8 +963,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                     if (lane < qn) queue[lane] = moved;
                     __syncwarp();
                     flush = false;
-                    if (i >= ca && qn == 0) break;
-                    if (i >= ca) flush = true;
+                    if (i >= ca && !cm && qn == 0) break;
+                    if (i >= ca && !cm) flush = true;
                 }
             }
             if (TMA && stalled) break;
@@ -950,10 +1013,11 @@ struct TunedCfgDef {
 // staged, PreTri built per evaluated pair (refine_lazy_kernel); 8-9: the lazy
 // kernel with one lane per queued pair (both halves in the lane); 10-11: the
 // lazy kernel, two lanes and one lane per pair, queuing 8 seeds first;
-// 12-13: the lazy kernel staging its raw records by 1-D bulk copies (TMA)
+// 12-13: the lazy kernel staging its raw records by 1-D bulk copies (TMA);
+// 14-15: the lazy kernel with 8 seeds first and the spread cull
 constexpr TunedCfgDef kTunedCfgs[kTunedConfigs] = {{64, 3}, {48, 3}, {32, 4}, {128, 3}, {128, 4}, {64, 4},
                                                     {128, 5}, {128, 6}, {128, 4}, {128, 5}, {128, 5}, {128, 5},
-                                                    {128, 4}, {64, 5}};
+                                                    {128, 4}, {64, 5}, {128, 5}, {128, 4}};
 
 TunedConfig tuned_config(int cfg) {
     if (cfg < 0 || cfg >= kTunedConfigs) cfg = 0;
@@ -985,13 +1049,13 @@ static cudaError_t launch_tuned_cfg(const float4* triA, const float4* triB, cons
     return cudaGetLastError();
 }
 
-template <int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false>
+template <int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false, bool SPREAD = false>
 static cudaError_t launch_lazy_cfg(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                    float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
                                    cudaStream_t s, const unsigned* n_items_dev, const float* init_bd) {
     const size_t smem = (size_t)kTunedWarps *
                         (TMA ? LazyLayout<CA>::kWarpFloatsTma : LazyLayout<CA>::kWarpFloats) * sizeof(float);
-    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB, ONE, SEEDS, TMA>;
+    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB, ONE, SEEDS, TMA, SPREAD>;
     if (smem > 48 * 1024) {
         static bool attr_set[64] = {};  // per device
         int dev = 0;
@@ -1031,6 +1095,8 @@ cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const Re
         case 11: return launch_lazy_cfg<128, 5, true, 8>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 12: return launch_lazy_cfg<128, 4, false, 32, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 13: return launch_lazy_cfg<64, 5, false, 32, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 14: return launch_lazy_cfg<128, 5, false, 8, false, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 15: return launch_lazy_cfg<128, 4, false, 8, false, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         default: return launch_tuned_cfg<64, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
     }
 }
