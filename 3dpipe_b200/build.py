@@ -28,9 +28,10 @@ CXX = shutil.which("g++") or "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                      "--expt-relaxed-constexpr", "-I", str(ROOT / "include"), "-I", str(PKG / "src")]
-# bounds_kernels.cu: no contraction of a*b+c into an FMA, so its FP64 values are
-# those of the same expressions rounded one operation at a time (as on the host)
-PER_FILE_FLAGS = {"bounds_kernels.cu": ["-fmad=false"]}
+# bounds_kernels.cu, prep_kernels.cu: no contraction of a*b+c into an FMA, so
+# their values are those of the same expressions rounded one operation at a
+# time (as on the host)
+PER_FILE_FLAGS = {"bounds_kernels.cu": ["-fmad=false"], "prep_kernels.cu": ["-fmad=false"]}
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-Wall", "-Wno-unused-function",
              "-I", str(ROOT / "include"), "-I", str(PKG / "src"),
              "-I", "/usr/local/cuda/include"]

@@ -795,21 +795,24 @@ void parallel_for(long n, int threads, Fn fn) {
 
 }  // namespace
 
-int gen_tiles(const GenParams& p, uint8_t* nuc_buf, size_t nuc_cap, size_t* nuc_len, uint8_t* ves_buf,
-              size_t ves_cap, size_t* ves_len, std::string& err) {
+namespace {
+
+struct Protos {
+    Proto nuc, ves;
+    TubeParam tp;
+    int key[5];
+};
+
+// prototypes (cached per parameter set) and the placed instances of a tile pair
+int make_instances(const GenParams& p, Protos*& PR, std::vector<VesselInst>& ves, std::vector<NucleusInst>& nuc,
+                   std::string& err) {
     if (p.n_vessels <= 0 || p.nuclei_per_vessel < 0 || p.voxel_size <= 0 || p.nucleus_subdiv < 0 ||
         p.nucleus_subdiv > 5 || p.tube_sides < 3 || p.tube_rings < 2) {
         err = "bad generator parameters";
         return TDP_ERR_ARG;
     }
     static std::mutex cache_mu;
-    struct Protos {
-        Proto nuc, ves;
-        TubeParam tp;
-        int key[5];
-    };
     static std::unique_ptr<Protos> cache;
-    Protos* PR;
     {
         std::lock_guard<std::mutex> g(cache_mu);
         int key[5] = {p.voxel_size, p.nucleus_subdiv, p.tube_sides, p.tube_rings, (int)(p.seed & 0x7fffffff)};
@@ -825,25 +828,11 @@ int gen_tiles(const GenParams& p, uint8_t* nuc_buf, size_t nuc_cap, size_t* nuc_
         PR = cache.get();
     }
     const Proto& PN = PR->nuc;
-    const Proto& PV = PR->ves;
-    const size_t nuc_obj = object_bytes(PN), ves_obj = object_bytes(PV);
     const long n_nuc = (long)p.n_vessels * p.nuclei_per_vessel;
-    const long nb0 = std::max(0L, std::min(p.nuclei_begin, n_nuc));
-    const long nb1 = p.nuclei_end <= 0 ? n_nuc : std::max(nb0, std::min(p.nuclei_end, n_nuc));
-    const size_t need_n = 1 + nuc_obj * (size_t)(nb1 - nb0), need_v = 1 + ves_obj * (size_t)p.n_vessels;
-    if (nuc_len) *nuc_len = need_n;
-    if (ves_len) *ves_len = need_v;
-    if (!nuc_buf && !ves_buf) return TDP_OK;
-    if ((nuc_buf && nuc_cap < need_n) || (ves_buf && ves_cap < need_v)) {
-        err = "generator output buffer too small";
-        return TDP_ERR_ARG;
-    }
-    const int threads = p.threads > 0 ? p.threads : std::max(1u, std::thread::hardware_concurrency());
-
     // vessels on a grid of cells p.grid apart
     int gx = (int)std::ceil(std::cbrt((double)p.n_vessels) - 1e-9);
     if (gx < 1) gx = 1;
-    std::vector<VesselInst> ves(p.n_vessels);
+    ves.assign(p.n_vessels, VesselInst{});
     for (int i = 0; i < p.n_vessels; ++i) {
         Rng g(p.seed, 1000000 + i);
         D3 c = {p.grid * (i % gx + 0.5), p.grid * ((i / gx) % gx + 0.5), p.grid * (i / (gx * gx) + 0.5)};
@@ -851,7 +840,7 @@ int gen_tiles(const GenParams& p, uint8_t* nuc_buf, size_t nuc_cap, size_t* nuc_
     }
     // nuclei placement: sequential rejection sampling with a hash grid
     const double nuc_reach = 12.0 * 1.1 + 0.01;  // max semi-axis times max radial noise
-    std::vector<NucleusInst> nuc(n_nuc);
+    nuc.assign(n_nuc, NucleusInst{});
     {
         const double cell = 2 * nuc_reach + 2.0;
         std::unordered_map<uint64_t, std::vector<int>> hash;
@@ -910,6 +899,38 @@ int gen_tiles(const GenParams& p, uint8_t* nuc_buf, size_t nuc_cap, size_t* nuc_
             }
         }
     }
+    return TDP_OK;
+}
+
+void nuclei_range(const GenParams& p, long& b, long& e) {
+    const long n_nuc = (long)p.n_vessels * p.nuclei_per_vessel;
+    b = std::max(0L, std::min(p.nuclei_begin, n_nuc));
+    e = p.nuclei_end <= 0 ? n_nuc : std::max(b, std::min(p.nuclei_end, n_nuc));
+}
+
+}  // namespace
+
+int gen_tiles(const GenParams& p, uint8_t* nuc_buf, size_t nuc_cap, size_t* nuc_len, uint8_t* ves_buf,
+              size_t ves_cap, size_t* ves_len, std::string& err) {
+    Protos* PR = nullptr;
+    std::vector<VesselInst> ves;
+    std::vector<NucleusInst> nuc;
+    int rc = make_instances(p, PR, ves, nuc, err);
+    if (rc != TDP_OK) return rc;
+    const Proto& PN = PR->nuc;
+    const Proto& PV = PR->ves;
+    const size_t nuc_obj = object_bytes(PN), ves_obj = object_bytes(PV);
+    long nb0, nb1;
+    nuclei_range(p, nb0, nb1);
+    const size_t need_n = 1 + nuc_obj * (size_t)(nb1 - nb0), need_v = 1 + ves_obj * (size_t)p.n_vessels;
+    if (nuc_len) *nuc_len = need_n;
+    if (ves_len) *ves_len = need_v;
+    if (!nuc_buf && !ves_buf) return TDP_OK;
+    if ((nuc_buf && nuc_cap < need_n) || (ves_buf && ves_cap < need_v)) {
+        err = "generator output buffer too small";
+        return TDP_ERR_ARG;
+    }
+    const int threads = p.threads > 0 ? p.threads : std::max(1u, std::thread::hardware_concurrency());
     if (nuc_buf) {
         nuc_buf[0] = kRawType;
         parallel_for(nb1 - nb0, threads, [&](long j) {
@@ -932,6 +953,49 @@ int gen_tiles(const GenParams& p, uint8_t* nuc_buf, size_t nuc_cap, size_t* nuc_
             }
             write_object(PV, Vf, ves_buf + 1 + ves_obj * (size_t)i);
         });
+    }
+    return TDP_OK;
+}
+
+int gen_meshes(const GenParams& p, int which, float* V, size_t vcap, int64_t* voff, uint32_t* F, size_t fcap,
+               int64_t* foff, size_t* n_vert, size_t* n_face, long* n_obj, std::string& err) {
+    if (which != 0 && which != 1) {
+        err = "which must be 0 (nuclei) or 1 (vessels)";
+        return TDP_ERR_ARG;
+    }
+    Protos* PR = nullptr;
+    std::vector<VesselInst> ves;
+    std::vector<NucleusInst> nuc;
+    int rc = make_instances(p, PR, ves, nuc, err);
+    if (rc != TDP_OK) return rc;
+    const Proto& P = which == 0 ? PR->nuc : PR->ves;
+    long b = 0, e = p.n_vessels;
+    if (which == 0) nuclei_range(p, b, e);
+    const long n = e - b;
+    const size_t nv = P.m.V.size(), nf = P.m.F.size();
+    if (n_vert) *n_vert = nv * (size_t)n;
+    if (n_face) *n_face = nf * (size_t)n;
+    if (n_obj) *n_obj = n;
+    if (!V && !F) return TDP_OK;
+    if (!V || !F || !voff || !foff || vcap < 3 * nv * (size_t)n || fcap < 3 * nf * (size_t)n) {
+        err = "mesh output buffers too small";
+        return TDP_ERR_ARG;
+    }
+    const int threads = p.threads > 0 ? p.threads : std::max(1u, std::thread::hardware_concurrency());
+    parallel_for(n, threads, [&](long j) {
+        const long i = b + j;
+        float* dst = V + 3 * nv * (size_t)j;
+        for (size_t k = 0; k < nv; ++k) {
+            const D3 q = which == 0 ? nucleus_vertex(nuc[i], P.m.V[k]) : vessel_vertex(ves[i], PR->tp, (int)k);
+            dst[3 * k] = (float)q.x; dst[3 * k + 1] = (float)q.y; dst[3 * k + 2] = (float)q.z;
+        }
+        uint32_t* fd = F + 3 * nf * (size_t)j;
+        for (size_t f = 0; f < nf; ++f)
+            for (int k = 0; k < 3; ++k) fd[3 * f + k] = (uint32_t)P.m.F[f][k];
+    });
+    for (long j = 0; j <= n; ++j) {
+        voff[j] = (int64_t)(nv * (size_t)j);
+        foff[j] = (int64_t)(nf * (size_t)j);
     }
     return TDP_OK;
 }

@@ -46,4 +46,10 @@ struct GenParams {
 int gen_tiles(const GenParams& p, uint8_t* nuclei, size_t nuclei_cap, size_t* nuclei_len, uint8_t* vessels,
               size_t vessels_cap, size_t* vessels_len, std::string& err);
 
+// The LOD-100 meshes of the same objects (which: 0 nuclei [nuclei_begin,
+// nuclei_end), 1 vessels): float vertices exactly as the tile stores them and
+// the prototype's facets, per object.  Null V and F: sizes only.
+int gen_meshes(const GenParams& p, int which, float* V, size_t vcap, int64_t* voff, uint32_t* F, size_t fcap,
+               int64_t* foff, size_t* n_vert, size_t* n_face, long* n_obj, std::string& err);
+
 }  // namespace tdp

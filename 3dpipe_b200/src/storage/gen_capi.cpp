@@ -25,9 +25,9 @@ void tdp_gen_default_params(tdp_gen_params* p) {
     p->nuclei_end = 0;
 }
 
-int tdp_gen_tiles(const tdp_gen_params* p, uint8_t* nuclei, size_t nuclei_cap, size_t* nuclei_len,
-                  uint8_t* vessels, size_t vessels_cap, size_t* vessels_len, char* err, size_t err_cap) {
-    if (!p) return TDP_ERR_ARG;
+namespace {
+
+tdp::GenParams to_gen(const tdp_gen_params* p) {
     tdp::GenParams g;
     g.n_vessels = p->n_vessels;
     g.nuclei_per_vessel = p->nuclei_per_vessel;
@@ -42,13 +42,35 @@ int tdp_gen_tiles(const tdp_gen_params* p, uint8_t* nuclei, size_t nuclei_cap, s
     g.shell_max = p->shell_max;
     g.nuclei_begin = p->nuclei_begin;
     g.nuclei_end = p->nuclei_end;
-    std::string msg;
-    int rc = tdp::gen_tiles(g, nuclei, nuclei_cap, nuclei_len, vessels, vessels_cap, vessels_len, msg);
+    return g;
+}
+
+int report(int rc, const std::string& msg, char* err, size_t err_cap) {
     if (rc != TDP_OK && err && err_cap) {
         std::strncpy(err, msg.c_str(), err_cap - 1);
         err[err_cap - 1] = 0;
     }
     return rc;
+}
+
+}  // namespace
+
+int tdp_gen_tiles(const tdp_gen_params* p, uint8_t* nuclei, size_t nuclei_cap, size_t* nuclei_len,
+                  uint8_t* vessels, size_t vessels_cap, size_t* vessels_len, char* err, size_t err_cap) {
+    if (!p) return TDP_ERR_ARG;
+    std::string msg;
+    const int rc = tdp::gen_tiles(to_gen(p), nuclei, nuclei_cap, nuclei_len, vessels, vessels_cap, vessels_len, msg);
+    return report(rc, msg, err, err_cap);
+}
+
+int tdp_gen_meshes(const tdp_gen_params* p, int which, float* vertices, size_t vert_cap, int64_t* vert_off,
+                   uint32_t* faces, size_t face_cap, int64_t* face_off, size_t* n_vert, size_t* n_face,
+                   long* n_obj, char* err, size_t err_cap) {
+    if (!p) return TDP_ERR_ARG;
+    std::string msg;
+    const int rc = tdp::gen_meshes(to_gen(p), which, vertices, vert_cap, vert_off, faces, face_cap, face_off, n_vert,
+                                   n_face, n_obj, msg);
+    return report(rc, msg, err, err_cap);
 }
 
 }  // extern "C"

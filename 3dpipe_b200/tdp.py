@@ -727,3 +727,133 @@ def _fp32_peak(self) -> float:
 
 
 Context.fp32_peak = _fp32_peak
+
+
+# ---- LOD preparation (GPU) ------------------------------------------------
+EXPORTED += ["tdp_raw_prep_bound", "tdp_raw_from_meshes", "tdp_gen_meshes"]
+
+
+class PrepInfo(C.Structure):
+    _fields_ = [("total_ms", C.c_double), ("decimate_ms", C.c_double), ("voxel_ms", C.c_double),
+                ("write_ms", C.c_double), ("bounds_ms", C.c_double), ("n_objects", C.c_long),
+                ("n_triangles", C.c_long * 5), ("n_voxels", C.c_long), ("batches", C.c_long)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["n_triangles"] = list(self.n_triangles)
+        return d
+
+
+def _mesh_arrays(vertices, vert_off, faces, face_off):
+    V = np.ascontiguousarray(vertices, np.float32).reshape(-1)
+    F = np.ascontiguousarray(faces, np.uint32).reshape(-1)
+    vo = np.ascontiguousarray(vert_off, np.int64)
+    fo = np.ascontiguousarray(face_off, np.int64)
+    if vo.size != fo.size or vo.size < 1:
+        raise ValueError("vert_off and face_off need n_objects + 1 entries each")
+    if vo[-1] * 3 > V.size or fo[-1] * 3 > F.size:
+        raise ValueError("offsets run past the vertex or facet arrays")
+    return V, vo, F, fo
+
+
+def raw_prep_bound(face_off, voxel_size=100):
+    """Bytes that always hold tdp_raw_from_meshes' tile of these objects."""
+    L = lib()
+    L.tdp_raw_prep_bound.argtypes = [C.c_void_p, C.c_long, C.c_int, C.POINTER(C.c_size_t)]
+    fo = np.ascontiguousarray(face_off, np.int64)
+    n = C.c_size_t()
+    rc = L.tdp_raw_prep_bound(_ptr(fo), fo.size - 1, voxel_size, C.byref(n))
+    if rc != TDP_OK:
+        raise TdpError(rc, "tdp_raw_prep_bound: bad arguments")
+    return n.value
+
+
+def _raw_from_meshes(self, vertices, vert_off, faces, face_off, voxel_size=100, out=None):
+    """LOD-100 meshes -> (RAW tile bytes, prep stats), every step on the GPU.
+    Object o: vertices[vert_off[o]:vert_off[o+1]] (x, y, z) and facets
+    faces[face_off[o]:face_off[o+1]] (indices local to the object).  `out`
+    (a writable uint8 buffer of at least raw_prep_bound bytes) receives it."""
+    L = lib()
+    L.tdp_raw_from_meshes.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_int,
+                                      C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(PrepInfo)]
+    V, vo, F, fo = _mesh_arrays(vertices, vert_off, faces, face_off)
+    cap = raw_prep_bound(fo, voxel_size)
+    buf = np.empty(cap, np.uint8) if out is None else out
+    if buf.nbytes < cap or not buf.flags.c_contiguous:
+        raise ValueError("out must be a contiguous buffer of at least raw_prep_bound bytes")
+    n = C.c_size_t()
+    info = PrepInfo()
+    self.check(L.tdp_raw_from_meshes(self._h, _ptr(V), _ptr(vo), _ptr(F), _ptr(fo), fo.size - 1, voxel_size,
+                                     _ptr(buf), buf.nbytes, C.byref(n), C.byref(info)))
+    return buf[:n.value], info.as_dict()
+
+
+Context.raw_from_meshes = _raw_from_meshes
+
+
+def gen_meshes(n_vessels=10, nuclei_per_vessel=20, seed=20260001, which="nuclei", **kw):
+    """The LOD-100 meshes of the generator's objects (the same vertices its
+    tiles hold): (vertices[nv, 3] float32, vert_off, faces[nf, 3] uint32, face_off)."""
+    L = lib()
+    L.tdp_gen_meshes.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t,
+                                 C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_long),
+                                 C.c_char_p, C.c_size_t]
+    p = GenParams()
+    L.tdp_gen_default_params(C.byref(p))
+    p.n_vessels, p.nuclei_per_vessel, p.seed = n_vessels, nuclei_per_vessel, seed
+    for k, v in kw.items():
+        setattr(p, k, v)
+    w = {"nuclei": 0, "vessels": 1}[which]
+    nv, nf, no = C.c_size_t(), C.c_size_t(), C.c_long()
+    err = C.create_string_buffer(512)
+    rc = L.tdp_gen_meshes(C.byref(p), w, None, 0, None, None, 0, None, C.byref(nv), C.byref(nf), C.byref(no), err, 512)
+    if rc != TDP_OK:
+        raise TdpError(rc, err.value.decode())
+    V = np.empty((nv.value, 3), np.float32)
+    F = np.empty((nf.value, 3), np.uint32)
+    vo = np.empty(no.value + 1, np.int64)
+    fo = np.empty(no.value + 1, np.int64)
+    rc = L.tdp_gen_meshes(C.byref(p), w, _ptr(V), V.size, _ptr(vo), _ptr(F), F.size, _ptr(fo), C.byref(nv),
+                          C.byref(nf), C.byref(no), err, 512)
+    if rc != TDP_OK:
+        raise TdpError(rc, err.value.decode())
+    return V, vo, F, fo
+
+
+def read_off(path_or_text):
+    """One OFF polyhedron (the reference's mesh text format, as in its data/*.pt
+    prototypes) -> (vertices[n, 3] float32, triangles[m, 3] uint32).  Polygons
+    with more than three corners are fanned from their first corner."""
+    text = path_or_text
+    if isinstance(path_or_text, (str, os.PathLike)) and Path(path_or_text).exists():
+        text = Path(path_or_text).read_text()
+    tok = []
+    for line in str(text).splitlines():
+        line = line.split("#", 1)[0].strip()
+        if line:
+            tok.extend(line.split())
+    if not tok or tok[0] != "OFF":
+        raise ValueError("not an OFF mesh")
+    nv, nf = int(tok[1]), int(tok[2])
+    at = 4
+    V = np.array(tok[at:at + 3 * nv], np.float32).reshape(nv, 3)
+    at += 3 * nv
+    tris = []
+    for _ in range(nf):
+        k = int(tok[at])
+        idx = [int(x) for x in tok[at + 1:at + 1 + k]]
+        at += 1 + k
+        for j in range(1, k - 1):
+            tris.append((idx[0], idx[j], idx[j + 1]))
+    return V, np.array(tris, np.uint32).reshape(-1, 3)
+
+
+def stack_meshes(meshes):
+    """[(vertices, triangles), ...] -> (vertices, vert_off, faces, face_off) for raw_from_meshes."""
+    vs = [np.asarray(v, np.float32).reshape(-1, 3) for v, _ in meshes]
+    fs = [np.asarray(f, np.uint32).reshape(-1, 3) for _, f in meshes]
+    vo = np.concatenate([[0], np.cumsum([len(v) for v in vs])]).astype(np.int64)
+    fo = np.concatenate([[0], np.cumsum([len(f) for f in fs])]).astype(np.int64)
+    V = np.concatenate(vs) if vs else np.zeros((0, 3), np.float32)
+    F = np.concatenate(fs) if fs else np.zeros((0, 3), np.uint32)
+    return V, vo, F, fo

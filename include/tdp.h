@@ -230,6 +230,40 @@ typedef struct {
 int tdp_tile_compute_bounds(tdp_ctx *ctx, tdp_tile *tile, tdp_bounds_info *info);
 int tdp_raw_compute_bounds(tdp_ctx *ctx, const void *raw, size_t len, void *out, tdp_bounds_info *info);
 
+/* ---- LOD preparation (GPU) --------------------------------------------------
+ * Replaces the reference's CGAL preparation of a tile from LOD-100 meshes (the
+ * OFF polyhedra of its data/ prototypes): progressive decimation into LODs
+ * (src/spatial/himesh_comp.cpp:28-190), skeleton voxels
+ * (src/spatial/himesh_skeleton.cpp:17-168), LOD triangles to voxels
+ * (src/spatial/himesh_retrieve.cpp:183-200), the Hausdorff bounds and the RAW
+ * writer of tdbase convert (src/storage/tile_IO.cpp:79-172).  Every step runs
+ * on the GPU (csrc/prep_kernels.cu states the rule): LODs 80/60/40/20 by
+ * shortest-edge half-edge collapse, voxels of about voxel_size LOD-100 facets
+ * by farthest-point seeds and two Lloyd steps, triangles to the voxel with the
+ * nearest core, then the bounds of tdp_raw_compute_bounds.
+ * Object o: vertices[3 vert_off[o] .. 3 vert_off[o+1]) (x, y, z floats) and
+ * facets faces[3 face_off[o] .. 3 face_off[o+1]) (vertex indices local to the
+ * object); vert_off and face_off hold n_objects + 1 non-decreasing entries.
+ * out receives the RAW tile (*len bytes); cap >= the size tdp_raw_prep_bound
+ * gives always suffices; out = NULL only computes *len.  TDP_ERR_ARG names
+ * the first object without vertices or facets, with an index out of range, a
+ * facet repeating a vertex or a non-finite coordinate. */
+typedef struct {
+    double total_ms;      /* host wall time of the call */
+    double decimate_ms;   /* device time of the decimation kernels */
+    double voxel_ms;      /* device time of the voxel kernel */
+    double write_ms;      /* device time of the RAW writer */
+    double bounds_ms;     /* host wall time of the bound preparation */
+    long n_objects;
+    long n_triangles[5];  /* per LOD 20..100 */
+    long n_voxels;
+    long batches;         /* object batches the call was split into */
+} tdp_prep_info;
+int tdp_raw_prep_bound(const int64_t *face_off, long n_objects, int voxel_size, size_t *max_len);
+int tdp_raw_from_meshes(tdp_ctx *ctx, const float *vertices, const int64_t *vert_off, const uint32_t *faces,
+                        const int64_t *face_off, long n_objects, int voxel_size, void *out, size_t cap,
+                        size_t *len, tdp_prep_info *info);
+
 /* ---- object candidates (host only) ------------------------------------------
  * The object-level filter: replaces OctreeNode::query_knn_fast / query_within
  * over Tile::build_octree (reference src/index/octree.cpp:215-330,
@@ -501,6 +535,13 @@ typedef struct {
 void tdp_gen_default_params(tdp_gen_params *p);
 int tdp_gen_tiles(const tdp_gen_params *p, uint8_t *nuclei, size_t nuclei_cap, size_t *nuclei_len,
                   uint8_t *vessels, size_t vessels_cap, size_t *vessels_len, char *err, size_t err_cap);
+/* The LOD-100 meshes of the same objects, as tdp_raw_from_meshes takes them:
+ * which = 0 the nuclei [nuclei_begin, nuclei_end), 1 the vessels; float
+ * vertices as the tiles store them, the prototype's facets per object.  Null
+ * vertices and faces: only n_vert, n_face and n_obj are set. */
+int tdp_gen_meshes(const tdp_gen_params *p, int which, float *vertices, size_t vert_cap, int64_t *vert_off,
+                   uint32_t *faces, size_t face_cap, int64_t *face_off, size_t *n_vert, size_t *n_face,
+                   long *n_obj, char *err, size_t err_cap);
 
 #ifdef __cplusplus
 }

@@ -25,6 +25,12 @@ int tdo_tile_bounds(const uint8_t *raw, size_t len, uint8_t *out, int prune, int
 /* largest violation of a tile's bounds over sampled points, see bounds_oracle.cpp */
 int tdo_bounds_violation(const uint8_t *raw, size_t len, int samples, uint64_t seed, double out[2]);
 
+/* LOD preparation of meshes into a RAW tile with zero bounds (lodprep_oracle.cpp);
+ * 0, -1 for bad arguments or a short buffer, -1 - o for bad object o */
+long tdo_raw_from_meshes(const float *vertices, const int64_t *vert_off, const uint32_t *faces,
+                         const int64_t *face_off, long n_objects, int voxel_size, uint8_t *out, size_t cap,
+                         size_t *len, int threads);
+
 #ifdef __cplusplus
 }
 #endif

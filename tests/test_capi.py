@@ -73,6 +73,9 @@ calls = {
     "tdp_partition_queries": (None, None, None, C.c_long(0), None, None, None, C.c_long(0), i0, i0, i1, f0,
                               C.c_int(2), None, None),
     "tdp_raw_partition": (None, z, None, z, i0, i1, f0, C.c_int(2), None, None, None, z),
+    "tdp_raw_prep_bound": (None, C.c_long(1), C.c_int(100), None),
+    "tdp_raw_from_meshes": (None, None, None, None, None, C.c_long(0), C.c_int(100), None, z, None, None),
+    "tdp_gen_meshes": (None, i0, None, z, None, None, z, None, None, None, None, None, z),
 }
 for name, args in calls.items():
     print(name, getattr(L, name)(*args))
