@@ -9,8 +9,8 @@
 //      LOD-100 surface), and, at Hausdorff level 2, also the pair's upper
 //      bound pmx when it was decided (d + h1 + h2 at a lower LOD bounds D);
 //      each widened by its FP32 error, max(perr, 1e-4 (value + 1));
-//      U is then tightened by refining kExK = 8 voxel pairs per object pair in
-//      FP32 (the ones with the closest cores): each minimum d32 + err_bound(R)
+//      U is then tightened by refining, in FP32, the voxel pair with the
+//      closest cores (kExK per object pair): its minimum d32 + err_bound(R)
 //      is a distance between two surface points, hence also >= D;
 //   2. every LOD-100 voxel pair whose box gap is <= U is a candidate (the
 //      voxel pair holding the closest points has gap <= D <= U);
@@ -21,8 +21,10 @@
 //      min d32 and E = max e;
 //   4. a candidate can hold the minimum only if d32 - E <= best32 + E (its
 //      true minimum is >= d32 - e, and D <= best32 + E): those are evaluated
-//      in FP64, skipping triangle pairs whose (inflated) bounding-sphere gap
-//      exceeds best32 + 2E;
+//      again triangle pair by triangle pair, skipping pairs whose (inflated)
+//      bounding-sphere gap exceeds best32 + 2E; a pair's FP32 distance d32'
+//      with its error e' comes first, and only a pair with d32' - e' <=
+//      best32 + E (one that can be the minimum) is evaluated in FP64;
 //   5. D = the smallest FP64 distance over the evaluated candidates.
 // Every filter is conservative, so D is the exact minimum over the stored
 // float coordinates up to the FP64 rounding of one triangle distance.
@@ -43,8 +45,10 @@ namespace {
 constexpr int kBlk = 256;
 
 // Voxel pairs per object pair refined in FP32 to tighten U (the ones with
-// the closest cores).
-constexpr int kExK = 8;
+// the closest cores).  Eight cost 8x the FP32 work of one and left the
+// candidate set 1.4 % smaller on the within-400 join (28.0 M voxel pairs
+// against 28.4 M), so one is refined.
+constexpr int kExK = 1;
 
 // U of every reported pair: min core-to-core distance over its voxel pairs,
 // and pmx when it is a proven bound (pmx_valid); item1[kExK p + k] = the voxel
@@ -218,7 +222,7 @@ __global__ void k_exact_best(const float4* __restrict__ res, const int* __restri
 __global__ void k_exact_select(const float4* __restrict__ res, const RefineItem* __restrict__ items,
                                const int* __restrict__ item_pair, int64_t E, const unsigned* __restrict__ best32,
                                const unsigned* __restrict__ emax, RefineItem* __restrict__ sel,
-                               int* __restrict__ sel_pair, float* __restrict__ sel_thr, unsigned* __restrict__ n_sel) {
+                               int* __restrict__ sel_pair, float2* __restrict__ sel_thr, unsigned* __restrict__ n_sel) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
         const float x = res[e].x;
         if (!(x < FLT_MAX)) continue;
@@ -228,7 +232,7 @@ __global__ void k_exact_select(const float4* __restrict__ res, const RefineItem*
             const unsigned w = atomicAdd(n_sel, 1u);
             sel[w] = items[e];
             sel_pair[w] = p;
-            sel_thr[w] = b + 2.f * m;
+            sel_thr[w] = make_float2(b + 2.f * m, b + m);  // sphere reach, FP64 limit
         }
     }
 }
@@ -254,16 +258,30 @@ __device__ __forceinline__ void pre64(const float4* t, double ox, double oy, dou
            v3<double>(c.x - ox, c.y - oy, c.z - oz));
 }
 
+// the FP32 operands as the refine forms them (translated to o), and the
+// largest |coordinate| after translation (the R of the error model)
+__device__ __forceinline__ float pre32(const float4* t, float4 o, PreTri<float>& P) {
+    const float4 a = t[0], b = t[1], c = t[2];
+    const V3<float> x = v3<float>(a.x - o.x, a.y - o.y, a.z - o.z), y = v3<float>(b.x - o.x, b.y - o.y, b.z - o.z),
+                    z = v3<float>(c.x - o.x, c.y - o.y, c.z - o.z);
+    pretri(P, x, y, z);
+    float r = 0.f;
+    r = fmaxf(r, fmaxf(fabsf(x.x), fmaxf(fabsf(x.y), fabsf(x.z))));
+    r = fmaxf(r, fmaxf(fabsf(y.x), fmaxf(fabsf(y.y), fabsf(y.z))));
+    return fmaxf(r, fmaxf(fabsf(z.x), fmaxf(fabsf(z.y), fabsf(z.z))));
+}
+
 constexpr int kExWarps = 4;
 
 // FP64 minimum over the triangle pairs of a selected voxel pair whose FP32
-// bounding-sphere gap is <= the item's threshold; one warp per item, lane j
-// owns B triangle j of the current chunk of 32, A spheres staged per chunk.
+// bounding-sphere gap is <= the item's reach and whose FP32 distance, less its
+// error bound, is <= the item's limit; one warp per item, lane j owns B
+// triangle j of the current chunk of 32, A spheres staged per chunk.
 __global__ void __launch_bounds__(kExWarps * 32) k_exact_f64(const float4* __restrict__ triA,
                                                              const float4* __restrict__ triB,
                                                              const RefineItem* __restrict__ sel,
                                                              const int* __restrict__ sel_pair,
-                                                             const float* __restrict__ sel_thr,
+                                                             const float2* __restrict__ sel_thr,
                                                              const unsigned* __restrict__ n_sel,
                                                              unsigned long long* __restrict__ pexact_bits) {
     __shared__ float4 sphA[kExWarps][32];
@@ -271,15 +289,20 @@ __global__ void __launch_bounds__(kExWarps * 32) k_exact_f64(const float4* __res
     const unsigned n = *n_sel;
     for (unsigned it = blockIdx.x * kExWarps + w; it < n; it += gridDim.x * kExWarps) {
         const RefineItem r = sel[it];
-        const float thr = sel_thr[it];
+        const float2 tl = sel_thr[it];
+        const float thr = tl.x, lim = tl.y;
         const float4 o4 = triA[(size_t)r.a_off * kTriF4];
         const double ox = o4.x, oy = o4.y, oz = o4.z;
         double best = 1e300;
         for (uint32_t b0 = 0; b0 < r.b_cnt; b0 += 32) {
             const bool bv = b0 + lane < r.b_cnt;
             const float4* tb = triB + ((size_t)r.b_off + b0 + lane) * kTriF4;
-            float bx = 0.f, by = 0.f, bz = 0.f, br = 0.f;
-            if (bv) sphere_rel(tb, o4, bx, by, bz, br);
+            float bx = 0.f, by = 0.f, bz = 0.f, br = 0.f, rB = 0.f;
+            PreTri<float> B32;
+            if (bv) {
+                sphere_rel(tb, o4, bx, by, bz, br);
+                rB = pre32(tb, o4, B32);
+            }
             for (uint32_t a0 = 0; a0 < r.a_cnt; a0 += 32) {
                 const int ca = (int)min(32u, r.a_cnt - a0);
                 __syncwarp();
@@ -294,11 +317,17 @@ __global__ void __launch_bounds__(kExWarps * 32) k_exact_f64(const float4* __res
                     const float dx = s.x - bx, dy = s.y - by, dz = s.z - bz;
                     const float reach = s.w + br + thr;
                     if (bv && dx * dx + dy * dy + dz * dz <= reach * reach) {
-                        PreTri<double> A, B;
-                        pre64(triA + ((size_t)r.a_off + a0 + i) * kTriF4, ox, oy, oz, A);
-                        pre64(tb, ox, oy, oz, B);
-                        const double d2 = tri_dist2(A, B);
-                        best = d2 < best ? d2 : best;
+                        const float4* ta = triA + ((size_t)r.a_off + a0 + i) * kTriF4;
+                        PreTri<float> A32;
+                        const float rA = pre32(ta, o4, A32);
+                        const float d32 = sqrtf(tri_dist2(A32, B32));
+                        if (!(d32 - err_bound(fmaxf(rA, rB)) > lim)) {  // it can be the minimum
+                            PreTri<double> A, B;
+                            pre64(ta, ox, oy, oz, A);
+                            pre64(tb, ox, oy, oz, B);
+                            const double d2 = tri_dist2(A, B);
+                            best = d2 < best ? d2 : best;
+                        }
                     }
                 }
             }
@@ -396,7 +425,7 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     ENS(71, Pz * 4);                   // emax
     ENS(72, Ez * sizeof(RefineItem));  // selected items
     ENS(73, Ez * 4);                   // selected -> pair
-    ENS(74, Ez * 4);                   // selected thresholds
+    ENS(74, Ez * 8);                   // selected (reach, limit)
     ENS(81, Ez * 4);                   // presets
     RefineItem* items = (RefineItem*)ctx->scratch[67].p;
     int* item_pair = (int*)ctx->scratch[68].p;
@@ -405,7 +434,7 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     unsigned* emax = (unsigned*)ctx->scratch[71].p;
     RefineItem* sel = (RefineItem*)ctx->scratch[72].p;
     int* sel_pair = (int*)ctx->scratch[73].p;
-    float* sel_thr = (float*)ctx->scratch[74].p;
+    float2* sel_thr = (float2*)ctx->scratch[74].p;
     float* preset = (float*)ctx->scratch[81].p;
     ctr = (unsigned*)ctx->scratch[75].p;
     k_exact_vp<true><<<pg, kBlk, 0, s>>>(d, Ub, vt1, vt2, nullptr, off, items, item_pair, preset);

@@ -425,6 +425,69 @@ def run_bounds_prep(pkg, ctx, nb, vb, n_nuclei=20000):
     return out
 
 
+def run_lod_prep(pkg, ctx, n_nuclei=20000, n_vessels=100):
+    """GPU LOD preparation (tdp_raw_from_meshes: decimation, voxels, RAW writer
+    and bounds on the device) of the LOD-100 meshes of the first n_nuclei
+    nuclei and n_vessels vessels of the join's generator, beside the CPU
+    restatement of the same rule (oracle/lodprep_oracle.cpp on all host cores,
+    then the FP64 bound oracle) on a few objects of each; the GPU tile of a
+    small sample must equal the CPU one byte for byte."""
+    import ctypes
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_bind import oracle
+    L = oracle().L
+    P = ctypes.c_void_p
+    L.tdo_raw_from_meshes.argtypes = [P, P, P, P, ctypes.c_long, ctypes.c_int, P, ctypes.c_size_t,
+                                      ctypes.POINTER(ctypes.c_size_t), ctypes.c_int]
+    L.tdo_raw_from_meshes.restype = ctypes.c_long
+    L.tdo_tile_bounds.argtypes = [P, ctypes.c_size_t, P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    cores = os.cpu_count() or 1
+
+    def cpu_prep(V, vo, F, fo):
+        V, vo, F, fo = (np.ascontiguousarray(x) for x in (V, vo, F, fo))
+        n = ctypes.c_size_t()
+        args = (V.ctypes.data, vo.ctypes.data, F.ctypes.data, fo.ctypes.data, len(vo) - 1, 100)
+        assert L.tdo_raw_from_meshes(*args, None, 0, ctypes.byref(n), cores) == 0
+        raw = np.empty(n.value, np.uint8)
+        assert L.tdo_raw_from_meshes(*args, raw.ctypes.data, raw.size, ctypes.byref(n), cores) == 0
+        out = np.empty_like(raw)
+        ev = ctypes.c_double()
+        assert L.tdo_tile_bounds(raw.ctypes.data, raw.size, out.ctypes.data, 1, cores, ctypes.byref(ev)) == 0
+        return out
+
+    def sub(V, vo, F, fo, k):
+        return V[:vo[k]], vo[:k + 1], F[:fo[k]], fo[:k + 1]
+
+    out = {"workload": f"LOD preparation of the LOD-100 meshes of the first {n_nuclei} nuclei and {n_vessels} "
+                       "vessels of the join's generator: LODs 80/60/40/20 by half-edge collapse, voxels of ~100 "
+                       "facets, RAW bytes, per-triangle bounds"}
+    kinds = {"nuclei": pkg.tdp.gen_meshes(N_VESSELS, NUCLEI_PER_VESSEL, seed=SEED, which="nuclei", nuclei_end=n_nuclei),
+             "vessels": pkg.tdp.gen_meshes(N_VESSELS, NUCLEI_PER_VESSEL, seed=SEED, which="vessels")}
+    kinds["vessels"] = sub(*kinds["vessels"], n_vessels)
+    for name, (V, vo, F, fo) in kinds.items():
+        k_cpu = 4 * cores if name == "nuclei" else cores
+        k_cpu = min(k_cpu, len(vo) - 1)
+        small = sub(V, vo, F, fo, min(k_cpu, 8))
+        got, _ = ctx.raw_from_meshes(*small)            # untimed first run, checked below
+        equal = bool(np.array_equal(np.array(got), cpu_prep(*small)))
+        raw, info = ctx.raw_from_meshes(V, vo, F, fo)
+        t0 = time.perf_counter()
+        cpu_prep(*sub(V, vo, F, fo, k_cpu))
+        cpu_s = time.perf_counter() - t0
+        n_obj = len(vo) - 1
+        gpu_rate = n_obj / (info["total_ms"] / 1e3)
+        out[name] = {"objects": n_obj, "facets": int(fo[-1]), "raw_bytes": int(raw.size), "gpu": info,
+                     "objects_per_s": gpu_rate, "sample_equal_to_cpu": equal,
+                     "cpu_objects_per_s": k_cpu / cpu_s, "cpu_cores": cores,
+                     "cpu_sample": f"first {k_cpu} {name}: CPU restatement + FP64 bound oracle, one run of {cpu_s:.2f} s",
+                     "gpu_over_cpu": gpu_rate / (k_cpu / cpu_s)}
+        log(f"lod prep {name}: {n_obj} objects in {info['total_ms']:.0f} ms (decimate {info['decimate_ms']:.0f}, "
+            f"voxels {info['voxel_ms']:.0f}, write {info['write_ms']:.0f}, bounds {info['bounds_ms']:.0f} ms), "
+            f"CPU {k_cpu / cpu_s:.1f}/s on {cores} cores, sample equal: {equal}")
+        del raw
+    return out
+
+
 def run_out_of_core(a):
     """Config 4 scaled to the host: a 10-NN join of nuclei against 10,000
     vessels under a 16 GB device budget, both tiles in host memory (the vessel
@@ -495,6 +558,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream measurement")
     ap.add_argument("--no-self", action="store_true", help="skip the 10-NN self-join measurement")
     ap.add_argument("--no-bounds", action="store_true", help="skip the GPU bound-preparation measurement")
+    ap.add_argument("--no-prep", action="store_true", help="skip the GPU LOD-preparation measurement")
     ap.add_argument("--refine-config", type=int, default=-1,
                     help="tuned refine configuration (default: autotuned in the warm-up)")
     ap.add_argument("--out-of-core", action="store_true",
@@ -734,6 +798,9 @@ def main():
             T1.free()
             T2.free()
             bounds_prep = run_bounds_prep(pkg, ctx, nb, vb)
+        lod_prep = None
+        if not a.no_prep and ws == 1:
+            lod_prep = run_lod_prep(pkg, ctx)
         del flush_buf
 
     pinned.release()
@@ -784,6 +851,7 @@ def main():
             "exact_distances": exact,
             "serving": serving,
             "bounds_prep": bounds_prep,
+            "lod_prep": lod_prep,
             "knn_self_join": knn_self,
             "gpu_launches": int(launches_t),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
