@@ -9,10 +9,10 @@
 // record, one warp per object reads that object's metadata block -- about 1.5
 // KB for a nucleus, every 170 KB of the file -- straight from the mapped host
 // bytes, instead of a host pass over them followed by copies of its results.
-// The blocks follow a one-byte header, so they are read as aligned 32-bit
-// words, each once, and realigned with a funnel shift against the next word
-// (from the neighbouring lane); every word read holds bytes of the record,
-// which the walk checked lies inside the buffer.
+// The blocks follow a one-byte header, so they are read as the 16-byte
+// aligned chunks that hold them, all of a window's loads in flight at once,
+// and realigned with a funnel shift in shared memory; every chunk read holds
+// bytes of the record, which the walk checked lies inside the buffer.
 //
 // Validation: every check the host parser makes on these fields (voxel boxes
 // not inverted, each LOD range inside the object's data block, 4-byte
@@ -37,35 +37,61 @@ constexpr int kChunkVox = 32;  // voxels per warp and round (one per lane)
 constexpr int kHdWords = 2 * kNumLods;
 constexpr int kStage = kHdWords + kChunkVox * kVoxWords + 3;  // words staged per window
 
-// st[i] = the 32-bit value that starts sh/8 bytes into word k0 + i of W, for
-// i < cnt.  Each word is read once: lane l holds word k0 + b + l and takes
-// the next word from lane l + 1 (lane 31 reads it itself).  Word k0 + cnt is
-// read only when sh != 0, and then it holds the last bytes of value cnt - 1,
-// so every word read lies on a page that the values occupy.
-__device__ __forceinline__ void stage_words(const uint32_t* W, uint64_t k0, uint32_t cnt, unsigned sh, int lane,
-                                            uint32_t* st) {
-    const uint32_t lim = cnt + (sh ? 1u : 0u);  // words [0, lim) may be read
-    for (uint32_t b = 0; b < cnt; b += 32) {
-        const uint32_t i = b + lane;
-        const uint32_t w = i < lim ? W[k0 + i] : 0u;
-        uint32_t nx = __shfl_down_sync(0xffffffffu, w, 1);
-        if (lane == 31) nx = (sh && i + 1 < lim) ? W[k0 + i + 1] : 0u;
-        if (i < cnt) st[i] = sh ? __funnelshift_r(w, nx, sh) : w;
+constexpr int kChunks = (4 * kStage + 30) / 16 + 1;  // 16-byte chunks a window spans, at most
+constexpr int kChunkLoads = (kChunks + 31) / 32;      // per lane
+constexpr int kWordLoads = (kStage + 31) / 32;        // per lane
+constexpr int kStageAlloc = 4 * kChunks + 8;          // words of a warp's stage (16-byte rows)
+
+// st[i] = the 32-bit value at byte address p + 4 i, for i < cnt (p of any
+// alignment).  The bytes are read as the 16-byte aligned chunks that hold
+// them -- every chunk holds a byte of the values, so it lies on a page they
+// occupy -- with every load of the window issued before any is used (a
+// zero-copy read of host memory takes microseconds, and more loads in flight
+// per warp lift the rate from ~33 to ~49 GB/s); the chunks land in the stage
+// as they are and are realigned in place through registers.
+__device__ __forceinline__ void stage_chunks(uintptr_t p, uint32_t cnt, int lane, uint32_t* st) {
+    const uintptr_t a0 = p & ~uintptr_t(15);
+    const uint32_t nq = (uint32_t)((((p + 4 * (uintptr_t)cnt + 15) & ~uintptr_t(15)) - a0) >> 4);
+    const uint4* Q = reinterpret_cast<const uint4*>(a0);
+    uint4 q[kChunkLoads];
+#pragma unroll
+    for (int k = 0; k < kChunkLoads; ++k) {
+        const uint32_t i = 32 * k + lane;
+        q[k] = i < nq ? Q[i] : make_uint4(0u, 0u, 0u, 0u);
+    }
+    uint4* S4 = reinterpret_cast<uint4*>(st);
+#pragma unroll
+    for (int k = 0; k < kChunkLoads; ++k) {
+        const uint32_t i = 32 * k + lane;
+        if (i < nq) S4[i] = q[k];
+    }
+    __syncwarp();
+    const uint32_t off = (uint32_t)(p - a0), w0 = off >> 2;
+    const unsigned sh = (off & 3) * 8;
+    uint32_t v[kWordLoads];
+#pragma unroll
+    for (int k = 0; k < kWordLoads; ++k) {
+        const uint32_t i = 32 * k + lane;  // w0 + i + 1 <= 4 kChunks + 3 < kStageAlloc
+        v[k] = i < cnt ? (sh ? __funnelshift_r(st[w0 + i], st[w0 + i + 1], sh) : st[w0 + i]) : 0u;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < kWordLoads; ++k) {
+        const uint32_t i = 32 * k + lane;
+        if (i < cnt) st[i] = v[k];
     }
 }
 
 __global__ void __launch_bounds__(kWarps * 32) k_parse_tables(const uint8_t* __restrict__ raw,
                                                               const AttachRec* __restrict__ recs, long n_obj,
                                                               AttachOut o) {
-    __shared__ uint32_t stage[kWarps][kStage];
+    __shared__ __align__(16) uint32_t stage[kWarps][kStageAlloc];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t* st = stage[w];
     const long nw = ((long)gridDim.x * blockDim.x) >> 5;
     for (long ob = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ob < n_obj; ob += nw) {
         const AttachRec r = recs[ob];
         const uintptr_t base = reinterpret_cast<uintptr_t>(raw) + r.meta;
-        const uint32_t* W = reinterpret_cast<const uint32_t*>(base & ~uintptr_t(3));
-        const unsigned sh = (unsigned)(base & 3) * 8;
         const uint64_t xw = kHdWords + (uint64_t)r.vnum * kVoxWords;  // first transform word
         bool bad = false;
         float lo0 = INFINITY, lo1 = INFINITY, lo2 = INFINITY, hi0 = -INFINITY, hi1 = -INFINITY, hi2 = -INFINITY;
@@ -78,7 +104,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_parse_tables(const uint8_t* __r
             const uint64_t ws = c0 == 0 ? 0 : kHdWords + (uint64_t)c0 * kVoxWords;
             const uint64_t we = kHdWords + (uint64_t)(c0 + m) * kVoxWords + (last ? 3 : 0);
             __syncwarp();
-            stage_words(W, ws, (uint32_t)(we - ws), sh, lane, st);
+            stage_chunks(base + 4 * ws, (uint32_t)(we - ws), lane, st);
             __syncwarp();
             if (c0 == 0 && lane < kHdWords) {  // object Hausdorff values: 5 x (hausdorff, proxy)
                 const float v = __uint_as_float(st[lane]);

@@ -755,7 +755,10 @@ extern "C" int tdp_raw_from_meshes(tdp_ctx* ctx, const float* vertices, const in
     // batches of consecutive objects within a device-memory budget
     size_t free_b = 0, total_b = 0;
     CU(cudaMemGetInfo(&free_b, &total_b));
-    const size_t budget = std::max<size_t>((size_t)256 << 20, std::min<size_t>((size_t)6 << 30, free_b / 4));
+    // a batch holds at most min(6 GiB, a quarter of the free memory, an eighth of the context's cap)
+    size_t budget = std::min<size_t>((size_t)6 << 30, free_b / 4);
+    if (ctx->budget) budget = std::min(budget, ctx->budget / 8);
+    budget = std::max<size_t>(budget, (size_t)16 << 20);
     std::vector<long> cuts{0};
     {
         size_t acc = 0;
