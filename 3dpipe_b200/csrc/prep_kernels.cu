@@ -59,7 +59,7 @@ namespace {
 constexpr int kDecLods = kNumLods - 1;  // LODs made by decimation (20..80)
 constexpr int kPrepThreads = 256;       // voxel and writer kernels
 constexpr size_t kSmemSmall = 40 << 10;  // decimation in shared memory, 128 threads
-constexpr size_t kSmemLarge = 200 << 10; // decimation in shared memory, 512 threads
+constexpr size_t kSmemLarge = 200 << 10; // decimation in shared memory, 1024 threads
 
 struct Meshes {  // one batch on the device; object o: vertices V[3 voff[o]..), facets F[3 foff[o]..)
     const float* V;
@@ -121,6 +121,21 @@ __device__ __forceinline__ void mark(uint32_t* M, uint32_t x, uint32_t y, uint32
     if (z != c) atomicOr(M + (z >> 5), 1u << (z & 31));
 }
 
+// smallest key (|P_a - P_b|^2, a, b) over the candidate slots of facet f with
+// flags fla, folded into (bl, ba, bb, bf)
+template <typename VI>
+__device__ __forceinline__ void fold_facet(const float* P, const VI* fv, uint32_t f, uint32_t fla, double& bl,
+                                           uint32_t& ba, uint32_t& bb, uint32_t& bf) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        if (fla & (2u << j)) continue;
+        const uint32_t x = fv[3 * f + j], y = fv[3 * f + (j == 2 ? 0 : j + 1)];
+        const uint32_t a = min(x, y), b = max(x, y);
+        const double L = dist2(vtx(P, a), vtx(P, b));
+        if (key_less(L, a, b, bl, ba, bb)) { bl = L; ba = a; bb = b; bf = f; }
+    }
+}
+
 // bytes of decimation storage for an object (facets, flags, 4 masks)
 __host__ __device__ inline size_t dec_bytes(int64_t n, int64_t m, size_t vi) {
     return round16(3 * (size_t)m * vi) + round16((size_t)m) + 16 * (size_t)((n + 31) / 32);
@@ -172,9 +187,12 @@ __global__ void __launch_bounds__(T) k_decimate(Meshes M, const int* __restrict_
         for (uint32_t w = tid; w < 4 * W; w += T) Mu[w] = 0;
         if (tid == 0) s_alive = (int)m;
         __syncthreads();
+        // this thread's smallest candidate key and the facet holding it; a full
+        // rescan (dirty) is needed only when that facet changes, any other
+        // changed facet is folded in
         bool dirty = true;
         double bl = INFINITY;
-        uint32_t ba = UINT_MAX, bb = UINT_MAX;
+        uint32_t ba = UINT_MAX, bb = UINT_MAX, bf = UINT_MAX;
         int li = kDecLods - 1;
         while (li >= 0) {
             const uint32_t target = (uint32_t)((uint64_t)m * (uint64_t)(20 * (li + 1)) / 100);  // LOD 20 (li + 1)
@@ -183,18 +201,10 @@ __global__ void __launch_bounds__(T) k_decimate(Meshes M, const int* __restrict_
             if (!snap) {
                 if (dirty) {  // smallest key among this thread's candidate edges
                     bl = INFINITY;
-                    ba = bb = UINT_MAX;
+                    ba = bb = bf = UINT_MAX;
                     for (uint32_t f = tid; f < m; f += T) {
                         const uint32_t fla = fl[f];
-                        if (!(fla & 1)) continue;
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) {
-                            if (fla & (2u << j)) continue;
-                            const uint32_t x = fv[3 * f + j], y = fv[3 * f + (j == 2 ? 0 : j + 1)];
-                            const uint32_t a = min(x, y), b = max(x, y);
-                            const double L = dist2(vtx(P, a), vtx(P, b));
-                            if (key_less(L, a, b, bl, ba, bb)) { bl = L; ba = a; bb = b; }
-                        }
+                        if (fla & 1) fold_facet(P, fv, f, fla, bl, ba, bb, bf);
                     }
                     dirty = false;
                 }
@@ -313,7 +323,7 @@ __global__ void __launch_bounds__(T) k_decimate(Meshes M, const int* __restrict_
                 const uint32_t x = t[0], y = t[1], z = t[2];
                 if (mode) {
                     const bool hr = x == r || y == r || z == r, hk = x == k || y == k || z == k;
-                    if (hr && hk) { fl[f] = 0; ++kills; dirty = true; continue; }
+                    if (hr && hk) { fl[f] = 0; ++kills; dirty |= f == bf; continue; }
                     if (!hr && !hk) continue;
                     if (hr) {
                         if (x == r) t[0] = (VI)k;
@@ -325,7 +335,8 @@ __global__ void __launch_bounds__(T) k_decimate(Meshes M, const int* __restrict_
                     for (int j = 0; j < 3; ++j)
                         if ((uint32_t)t[j] == k || (uint32_t)t[j == 2 ? 0 : j + 1] == k) nf &= ~(2u << j);
                     fl[f] = (uint8_t)nf;
-                    dirty = true;
+                    if (f == bf) dirty = true;  // its old keys may have been the minimum
+                    else fold_facet(P, fv, f, nf, bl, ba, bb, bf);
                 } else {
                     const bool hu = x == u || y == u || z == u, hv = x == v || y == v || z == v;
                     if (!(hu && hv)) continue;
@@ -336,7 +347,7 @@ __global__ void __launch_bounds__(T) k_decimate(Meshes M, const int* __restrict_
                         if ((a == u && b == v) || (a == v && b == u)) nf |= 2u << j;
                     }
                     fl[f] = (uint8_t)nf;
-                    dirty = true;
+                    dirty |= f == bf;  // slots only left the candidates
                 }
             }
             if (kills) atomicSub(&s_alive, kills);
@@ -852,9 +863,9 @@ extern "C" int tdp_raw_from_meshes(tdp_ctx* ctx, const float* vertices, const in
             CU(cudaGetLastError());
         }
         if (!large.empty()) {
-            auto kern = k_decimate<uint16_t, 512>;
+            auto kern = k_decimate<uint16_t, 1024>;
             CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s_large));
-            kern<<<(int)large.size(), 512, s_large, s>>>(Mh, dl + small.size(), (int)large.size(), nullptr, nullptr,
+            kern<<<(int)large.size(), 1024, s_large, s>>>(Mh, dl + small.size(), (int)large.size(), nullptr, nullptr,
                                                          lodF, Ftot, lodCnt);
             CU(cudaGetLastError());
         }
@@ -864,7 +875,7 @@ extern "C" int tdp_raw_from_meshes(tdp_ctx* ctx, const float* vertices, const in
             CU(dm.get(&gst, (size_t)hoff.back()));
             CU(dm.get(&dho, hoff.size()));
             CU(cudaMemcpyAsync(dho, hoff.data(), 8 * hoff.size(), cudaMemcpyHostToDevice, s));
-            k_decimate<uint32_t, 512><<<(int)huge.size(), 512, 0, s>>>(Mh, dl + small.size() + large.size(),
+            k_decimate<uint32_t, 1024><<<(int)huge.size(), 1024, 0, s>>>(Mh, dl + small.size() + large.size(),
                                                                       (int)huge.size(), gst, dho, lodF, Ftot, lodCnt);
             CU(cudaGetLastError());
         }

@@ -342,17 +342,26 @@ def run_serving(pkg, ctx, T2, nb, rates, per_rate_cap=600, seconds=3.0, pool_siz
             th = threading.Thread(target=submitter)
             th.start()
             th.join()
-            lat, batch_sizes = [], []
+            lat, batch_sizes, infos = [], [], []
             for rid in ids:
                 _, _, _, info = srv.wait(rid)
                 lat.append(info["latency_ms"])
                 batch_sizes.append(info["batch_requests"])
+                infos.append(info)
             wall = time.perf_counter() - t0
             st = srv.stats()
         batched = {"p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "requests_per_s": len(reqs) / wall,
                    "nuclei_per_s": nuclei / wall, "batches": st["batches"],
                    "mean_requests_per_batch": len(reqs) / max(1, st["batches"]),
                    "join_busy_frac": st["busy_ms"] / 1e3 / wall, "h2d_gb_per_s": st["upload_bytes"] / wall / 1e9}
+        # the requests behind the tail: the slowest 1 %
+        slow = sorted(range(len(reqs)), key=lambda k: -lat[k])[:max(1, len(reqs) // 100)]
+        batched["slowest"] = [{"latency_ms": round(lat[k], 2), "nuclei": sizes[reqs[k][1]], "query": reqs[k][2],
+                               "knn": reqs[k][3] if reqs[k][2] == "nn" else None,
+                               "tau": round(reqs[k][4], 1) if reqs[k][2] == "within" else None,
+                               "batch_requests": batch_sizes[k],
+                               **{f: round(infos[k][f], 2) for f in ("queue_ms", "join_ms") if f in infos[k]}}
+                              for k in slow]
         # plain per-request launches, same schedule
         lat2 = []
         t0 = time.perf_counter()
