@@ -9,9 +9,9 @@
 //      LOD-100 surface), and, at Hausdorff level 2, also the pair's upper
 //      bound pmx when it was decided (d + h1 + h2 at a lower LOD bounds D);
 //      each widened by its FP32 error, max(perr, 1e-4 (value + 1));
-//      U is then tightened by refining, in FP32, the kExK voxel pairs with
-//      the smallest box gaps: each minimum d32 + err_bound(R) is a distance
-//      between two surface points, hence also >= D;
+//      U is then tightened by refining, in FP32, the voxel pair with the
+//      closest cores (kExK per object pair): its minimum d32 + err_bound(R)
+//      is a distance between two surface points, hence also >= D;
 //   2. every LOD-100 voxel pair whose box gap is <= U is a candidate (the
 //      voxel pair holding the closest points has gap <= D <= U);
 //   3. the tuned FP32 refine, its minimum preset to U plus the candidate's
@@ -44,27 +44,18 @@ namespace {
 
 constexpr int kBlk = 256;
 
-// Voxel pairs per object pair refined in FP32 to tighten U: the ones with
-// the smallest box gaps, which hold the closest points far more often than
-// the ones with the closest cores (eight closest-core pairs left the
-// candidate set of the within-400 join only 1.4 % smaller than one).
-constexpr int kExK = 2;
-
-// squared box gap of two voxels, as vox_dist2 computes it
-__device__ __forceinline__ float box_gap2(const float4* a, const float4* b) {
-    const float4 alo = a[0], ahi = a[1], blo = b[0], bhi = b[1];
-    const float gx = fmaxf(fmaxf(alo.x - bhi.x, blo.x - ahi.x), 0.f);
-    const float gy = fmaxf(fmaxf(alo.y - bhi.y, blo.y - ahi.y), 0.f);
-    const float gz = fmaxf(fmaxf(alo.z - bhi.z, blo.z - ahi.z), 0.f);
-    return gx * gx + gy * gy + gz * gz;
-}
+// Voxel pairs per object pair refined in FP32 to tighten U (the ones with
+// the closest cores).  On the within-400 join eight cost 8x the FP32 work of
+// one and left the candidate set 1.4 % smaller (28.0 M voxel pairs against
+// 28.4 M); the two with the smallest box gaps instead gave a looser U (29.6 M
+// candidates, 15 % more FP32 work); so one is refined.
+constexpr int kExK = 1;
 
 // U of every reported pair: min core-to-core distance over its voxel pairs,
 // and pmx when it is a proven bound (pmx_valid); item1[kExK p + k] = the voxel
-// pairs with the kExK smallest box gaps (ties: closer cores; empty items for
-// the rest and for pairs that are not reported).  Each lane keeps a sorted top
-// kExK of its own (strided) voxel pairs; the warp then takes the kExK
-// smallest heads.
+// pairs with the kExK closest cores (empty items for the rest and for pairs
+// that are not reported).  Each lane keeps a sorted top kExK of its own
+// (strided) voxel pairs; the warp then takes the kExK smallest heads.
 __global__ void __launch_bounds__(kBlk) k_exact_upper(JoinDev d, int pmx_valid, const uint32_t* __restrict__ vt1,
                                                       const uint32_t* __restrict__ vt2, float* __restrict__ U,
                                                       RefineItem* __restrict__ item1) {
@@ -79,32 +70,25 @@ __global__ void __launch_bounds__(kBlk) k_exact_upper(JoinDev d, int pmx_valid, 
         }
         const int q = d.pq[p], t = d.pt[p];
         const uint32_t a0 = d.ovox1[q], a1 = d.ovox1[q + 1], b0 = d.ovox2[t], b1 = d.ovox2[t + 1];
-        // keys: (box gap^2, core distance^2) lexicographic, as one 64-bit
-        // value (non-negative floats order like their bit patterns)
-        unsigned long long kv[kExK];
+        float kv[kExK];
         uint32_t ka[kExK], kb[kExK];
-        float best = FLT_MAX;  // smallest core distance^2
 #pragma unroll
-        for (int k = 0; k < kExK; ++k) { kv[k] = ~0ull; ka[k] = a0; kb[k] = b0; }
+        for (int k = 0; k < kExK; ++k) { kv[k] = FLT_MAX; ka[k] = a0; kb[k] = b0; }
         for (uint32_t b = b0 + lane; b < b1; b += 32) {
             if (vt2[b + 1] == vt2[b]) continue;
-            const float4* vb = d.vox2 + 3 * (size_t)b;
-            const float4 cb = vb[2];
+            const float4 cb = d.vox2[3 * (size_t)b + 2];
             for (uint32_t a = a0; a < a1; ++a) {
                 if (vt1[a + 1] == vt1[a]) continue;
-                const float4* va = d.vox1 + 3 * (size_t)a;
-                const float4 ca = va[2];
+                const float4 ca = d.vox1[3 * (size_t)a + 2];
                 const float dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;
-                const float c2 = dx * dx + dy * dy + dz * dz;
-                best = fminf(best, c2);
-                unsigned long long v = ((unsigned long long)__float_as_uint(box_gap2(va, vb)) << 32) | __float_as_uint(c2);
+                float v = dx * dx + dy * dy + dz * dz;
                 if (!(v < kv[kExK - 1])) continue;
                 // insert into the lane's sorted list (unrolled, registers only)
                 uint32_t ia = a, ib = b;
 #pragma unroll
                 for (int k = 0; k < kExK; ++k) {
                     if (v < kv[k]) {
-                        const unsigned long long tv = kv[k];
+                        const float tv = kv[k];
                         const uint32_t ta = ka[k], tb = kb[k];
                         kv[k] = v; ka[k] = ia; kb[k] = ib;
                         v = tv; ia = ta; ib = tb;
@@ -112,26 +96,23 @@ __global__ void __launch_bounds__(kBlk) k_exact_upper(JoinDev d, int pmx_valid, 
                 }
             }
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(0xffffffffu, best, o));
         // the warp's kExK smallest: each round takes the smallest lane head
+        float best = FLT_MAX;
         for (int k = 0; k < kExK; ++k) {
-            unsigned long long h = kv[0];
+            float h = kv[0];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const unsigned long long x = __shfl_xor_sync(0xffffffffu, h, o);
-                h = x < h ? x : h;
-            }
+            for (int o = 16; o > 0; o >>= 1) h = fminf(h, __shfl_xor_sync(0xffffffffu, h, o));
             const unsigned who = __ballot_sync(0xffffffffu, kv[0] == h);
             const int src = __ffs(who) - 1;
             const uint32_t wa = __shfl_sync(0xffffffffu, ka[0], src), wb = __shfl_sync(0xffffffffu, kb[0], src);
+            if (k == 0) best = h;
             if (lane == 0)
-                it1[k] = h != ~0ull ? RefineItem{vt1[wa], vt1[wa + 1] - vt1[wa], vt2[wb], vt2[wb + 1] - vt2[wb]}
-                                    : RefineItem{0, 0, 0, 0};
+                it1[k] = h < FLT_MAX ? RefineItem{vt1[wa], vt1[wa + 1] - vt1[wa], vt2[wb], vt2[wb + 1] - vt2[wb]}
+                                     : RefineItem{0, 0, 0, 0};
             if (lane == src) {  // pop the head
 #pragma unroll
                 for (int j = 0; j + 1 < kExK; ++j) { kv[j] = kv[j + 1]; ka[j] = ka[j + 1]; kb[j] = kb[j + 1]; }
-                kv[kExK - 1] = ~0ull;
+                kv[kExK - 1] = FLT_MAX;
             }
         }
         if (lane == 0) {
@@ -159,6 +140,15 @@ __global__ void k_exact_tighten(const float4* __restrict__ res1, int64_t P, floa
         }
         U[p] = u;
     }
+}
+
+// squared box gap of two voxels, as vox_dist2 computes it
+__device__ __forceinline__ float box_gap2(const float4* a, const float4* b) {
+    const float4 alo = a[0], ahi = a[1], blo = b[0], bhi = b[1];
+    const float gx = fmaxf(fmaxf(alo.x - bhi.x, blo.x - ahi.x), 0.f);
+    const float gy = fmaxf(fmaxf(alo.y - bhi.y, blo.y - ahi.y), 0.f);
+    const float gz = fmaxf(fmaxf(alo.z - bhi.z, blo.z - ahi.z), 0.f);
+    return gx * gx + gy * gy + gz * gz;
 }
 
 // count (WRITE = false) or write the candidate voxel pairs of every reported pair

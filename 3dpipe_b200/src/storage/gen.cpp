@@ -634,6 +634,16 @@ D3 vessel_vertex(const VesselInst& v, const TubeParam& tp, int i) {
     return p + (v.e1[k] * std::cos(tp.theta[i]) + v.e2[k] * std::sin(tp.theta[i])) * v.r;
 }
 
+// the noise amplitude's normaliser of a nucleus: 1 / max |noise| over the
+// prototype's vertices (a function of its coefficients alone, computed only
+// for the nuclei a call writes, by the writing thread)
+void noise_scale(NucleusInst& n, const Mesh& proto) {
+    if (n.nscale >= 0.0) return;
+    double mx = 0;
+    for (auto& u : proto.V) mx = std::max(mx, std::fabs(noise_basis(n.coef, u)));
+    n.nscale = mx > 0 ? 1.0 / mx : 0.0;
+}
+
 double seg_axis_dist(const VesselInst& v, D3 p) {
     double d = 1e300;
     for (int k = 0; k < kSegs; ++k) d = std::min(d, pt_seg(p, v.start[k], v.start[k] + v.dir[k] * v.len[k]));
@@ -838,6 +848,25 @@ int make_instances(const GenParams& p, Protos*& PR, std::vector<VesselInst>& ves
         D3 c = {p.grid * (i % gx + 0.5), p.grid * ((i / gx) % gx + 0.5), p.grid * (i / (gx * gx) + 0.5)};
         ves[i] = make_vessel(g, c);
     }
+    // each vessel's axis box: seg_axis_dist(v, c) is at least the distance from
+    // c to it, so a vessel whose box is farther than the clearance (plus a
+    // margin far above rounding) is skipped without changing any outcome
+    std::vector<std::array<double, 6>> vbox(p.n_vessels);
+    for (int i = 0; i < p.n_vessels; ++i) {
+        std::array<double, 6>& b = vbox[i];
+        b = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+        for (int k = 0; k < kSegs; ++k)
+            for (const D3 q : {ves[i].start[k], ves[i].start[k] + ves[i].dir[k] * ves[i].len[k]}) {
+                b[0] = std::min(b[0], q.x); b[1] = std::min(b[1], q.y); b[2] = std::min(b[2], q.z);
+                b[3] = std::max(b[3], q.x); b[4] = std::max(b[4], q.y); b[5] = std::max(b[5], q.z);
+            }
+    }
+    auto box_gap2 = [&](int i, D3 c) {
+        const std::array<double, 6>& b = vbox[i];
+        const double gx = std::max({b[0] - c.x, c.x - b[3], 0.0}), gy = std::max({b[1] - c.y, c.y - b[4], 0.0});
+        const double gz = std::max({b[2] - c.z, c.z - b[5], 0.0});
+        return gx * gx + gy * gy + gz * gz;
+    };
     // nuclei placement: sequential rejection sampling with a hash grid
     const double nuc_reach = 12.0 * 1.1 + 0.01;  // max semi-axis times max radial noise
     nuc.assign(n_nuc, NucleusInst{});
@@ -866,8 +895,11 @@ int make_instances(const GenParams& p, Protos*& PR, std::vector<VesselInst>& ves
                     D3 c = axis + radial * rho;
                     // keep clear of every vessel and every other nucleus
                     bool bad = false;
-                    for (int wv = std::max(0, vi - gx * gx - gx - 1); wv < std::min(p.n_vessels, vi + gx * gx + gx + 2) && !bad; ++wv)
-                        if (seg_axis_dist(ves[wv], c) < ves[wv].r + nuc_reach + (wv == vi ? p.shell_min : 5.0)) bad = true;
+                    for (int wv = std::max(0, vi - gx * gx - gx - 1); wv < std::min(p.n_vessels, vi + gx * gx + gx + 2) && !bad; ++wv) {
+                        const double clear = ves[wv].r + nuc_reach + (wv == vi ? p.shell_min : 5.0);
+                        if (box_gap2(wv, c) > (clear + 1e-6) * (clear + 1e-6)) continue;
+                        if (seg_axis_dist(ves[wv], c) < clear) bad = true;
+                    }
                     if (bad) continue;
                     long cx = (long)std::floor(c.x / cell), cy = (long)std::floor(c.y / cell), cz = (long)std::floor(c.z / cell);
                     for (long a = -1; a <= 1 && !bad; ++a)
@@ -889,9 +921,7 @@ int make_instances(const GenParams& p, Protos*& PR, std::vector<VesselInst>& ves
                 n.ax = g.uni(8, 12); n.ay = g.uni(8, 12); n.az = g.uni(8, 12);
                 random_rotation(g, n.rot);
                 for (double& cf : n.coef) cf = g.normal();
-                double mx = 0;
-                for (auto& u : PN.m.V) mx = std::max(mx, std::fabs(noise_basis(n.coef, u)));
-                n.nscale = mx > 0 ? 1.0 / mx : 0.0;
+                n.nscale = -1.0;  // set by noise_scale() when the nucleus is written
                 long id = (long)vi * p.nuclei_per_vessel + j;
                 nuc[id] = n;
                 long cx = (long)std::floor(n.c.x / cell), cy = (long)std::floor(n.c.y / cell), cz = (long)std::floor(n.c.z / cell);
@@ -937,6 +967,7 @@ int gen_tiles(const GenParams& p, uint8_t* nuc_buf, size_t nuc_cap, size_t* nuc_
             const long i = nb0 + j;
             std::vector<float> Vf(3 * PN.m.V.size());
             for (size_t k = 0; k < PN.m.V.size(); ++k) {
+                if (k == 0) noise_scale(nuc[i], PN.m);
                 D3 q = nucleus_vertex(nuc[i], PN.m.V[k]);
                 Vf[3 * k] = (float)q.x; Vf[3 * k + 1] = (float)q.y; Vf[3 * k + 2] = (float)q.z;
             }
@@ -986,6 +1017,7 @@ int gen_meshes(const GenParams& p, int which, float* V, size_t vcap, int64_t* vo
         const long i = b + j;
         float* dst = V + 3 * nv * (size_t)j;
         for (size_t k = 0; k < nv; ++k) {
+            if (which == 0 && k == 0) noise_scale(nuc[i], P.m);
             const D3 q = which == 0 ? nucleus_vertex(nuc[i], P.m.V[k]) : vessel_vertex(ves[i], PR->tp, (int)k);
             dst[3 * k] = (float)q.x; dst[3 * k + 1] = (float)q.y; dst[3 * k + 2] = (float)q.z;
         }

@@ -95,11 +95,12 @@ class GenParams(C.Structure):
                 ("nuclei_end", C.c_long)]
 
 
-def gen_tiles(n_vessels: int = 10, nuclei_per_vessel: int = 20, seed: int = 20260001, out=None, **kw):
+def gen_tiles(n_vessels: int = 10, nuclei_per_vessel: int = 20, seed: int = 20260001, out=None, only=None, **kw):
     """Generate (nuclei_tile_bytes, vessel_tile_bytes) as uint8 arrays in RAW .dt format.
 
     `out`, if given, is a callable (nbytes) -> writable uint8 array (for example a
-    pinned buffer); otherwise numpy arrays are allocated."""
+    pinned buffer); otherwise numpy arrays are allocated.  only="nuclei" or
+    "vessels" writes just that tile (the other is returned as None)."""
     L = lib()
     p = GenParams()
     L.tdp_gen_default_params(C.byref(p))
@@ -111,12 +112,16 @@ def gen_tiles(n_vessels: int = 10, nuclei_per_vessel: int = 20, seed: int = 2026
     rc = L.tdp_gen_tiles(C.byref(p), None, 0, C.byref(nl), None, 0, C.byref(vl), err, 512)
     if rc != TDP_OK:
         raise TdpError(rc, err.value.decode())
+    if only not in (None, "nuclei", "vessels"):
+        raise ValueError("only must be None, 'nuclei' or 'vessels'")
     alloc = out or (lambda n: np.empty(n, np.uint8))
-    nb, vb = alloc(nl.value), alloc(vl.value)
-    rc = L.tdp_gen_tiles(C.byref(p), _ptr(nb), nb.size, C.byref(nl), _ptr(vb), vb.size, C.byref(vl), err, 512)
+    nb = alloc(nl.value) if only != "vessels" else None
+    vb = alloc(vl.value) if only != "nuclei" else None
+    rc = L.tdp_gen_tiles(C.byref(p), _ptr(nb), 0 if nb is None else nb.size, C.byref(nl), _ptr(vb),
+                         0 if vb is None else vb.size, C.byref(vl), err, 512)
     if rc != TDP_OK:
         raise TdpError(rc, err.value.decode())
-    return nb[:nl.value], vb[:vl.value]
+    return (None if nb is None else nb[:nl.value]), (None if vb is None else vb[:vl.value])
 
 
 class Context:
