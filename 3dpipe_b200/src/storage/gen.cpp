@@ -561,7 +561,6 @@ struct NucleusInst {
     double ax, ay, az;
     double rot[9];
     double coef[9];
-    double nscale;
 };
 
 struct VesselInst {
@@ -587,8 +586,8 @@ double noise_basis(const double* cf, D3 u) {
     return s;
 }
 
-D3 nucleus_vertex(const NucleusInst& n, D3 u) {
-    double r = 1.0 + 0.1 * noise_basis(n.coef, u) * n.nscale;
+D3 nucleus_vertex(const NucleusInst& n, D3 u, double nscale) {
+    double r = 1.0 + 0.1 * noise_basis(n.coef, u) * nscale;
     D3 q = {u.x * n.ax * r, u.y * n.ay * r, u.z * n.az * r};
     return {n.c.x + n.rot[0] * q.x + n.rot[1] * q.y + n.rot[2] * q.z,
             n.c.y + n.rot[3] * q.x + n.rot[4] * q.y + n.rot[5] * q.z,
@@ -637,11 +636,10 @@ D3 vessel_vertex(const VesselInst& v, const TubeParam& tp, int i) {
 // the noise amplitude's normaliser of a nucleus: 1 / max |noise| over the
 // prototype's vertices (a function of its coefficients alone, computed only
 // for the nuclei a call writes, by the writing thread)
-void noise_scale(NucleusInst& n, const Mesh& proto) {
-    if (n.nscale >= 0.0) return;
+double noise_scale(const NucleusInst& n, const Mesh& proto) {
     double mx = 0;
     for (auto& u : proto.V) mx = std::max(mx, std::fabs(noise_basis(n.coef, u)));
-    n.nscale = mx > 0 ? 1.0 / mx : 0.0;
+    return mx > 0 ? 1.0 / mx : 0.0;
 }
 
 double seg_axis_dist(const VesselInst& v, D3 p) {
@@ -814,20 +812,56 @@ struct Protos {
 };
 
 // prototypes (cached per parameter set) and the placed instances of a tile pair
-int make_instances(const GenParams& p, Protos*& PR, std::vector<VesselInst>& ves, std::vector<NucleusInst>& nuc,
-                   std::string& err) {
+struct Instances {
+    std::shared_ptr<const Protos> protos;
+    std::vector<VesselInst> ves;
+    std::vector<NucleusInst> nuc;
+};
+
+int place_instances(const GenParams& p, std::shared_ptr<const Protos>& PR, std::vector<VesselInst>& ves,
+                    std::vector<NucleusInst>& nuc, std::string& err);
+
+// The placed instances of a parameter set, computed once and kept (the last
+// set) so that the size query, the write and every later range of the same
+// tiles reuse them; they are never modified after placement.
+int make_instances(const GenParams& p, std::shared_ptr<const Instances>& out, std::string& err) {
+    static std::mutex mu;
+    static std::shared_ptr<const Instances> last;
+    static GenParams last_p;
+    std::lock_guard<std::mutex> g(mu);
+    auto same = [&](const GenParams& a, const GenParams& b) {
+        return a.n_vessels == b.n_vessels && a.nuclei_per_vessel == b.nuclei_per_vessel && a.seed == b.seed &&
+               a.voxel_size == b.voxel_size && a.nucleus_subdiv == b.nucleus_subdiv && a.tube_sides == b.tube_sides &&
+               a.tube_rings == b.tube_rings && a.grid == b.grid && a.shell_min == b.shell_min &&
+               a.shell_max == b.shell_max;
+    };
+    if (last && same(p, last_p)) {
+        out = last;
+        return TDP_OK;
+    }
+    auto inst = std::make_shared<Instances>();
+    const int rc = place_instances(p, inst->protos, inst->ves, inst->nuc, err);
+    if (rc != TDP_OK) return rc;
+    last = inst;
+    last_p = p;
+    out = inst;
+    return TDP_OK;
+}
+
+int place_instances(const GenParams& p, std::shared_ptr<const Protos>& PR, std::vector<VesselInst>& ves,
+                    std::vector<NucleusInst>& nuc, std::string& err) {
     if (p.n_vessels <= 0 || p.nuclei_per_vessel < 0 || p.voxel_size <= 0 || p.nucleus_subdiv < 0 ||
         p.nucleus_subdiv > 5 || p.tube_sides < 3 || p.tube_rings < 2) {
         err = "bad generator parameters";
         return TDP_ERR_ARG;
     }
     static std::mutex cache_mu;
-    static std::unique_ptr<Protos> cache;
+    static std::shared_ptr<const Protos> cache;
     {
         std::lock_guard<std::mutex> g(cache_mu);
         int key[5] = {p.voxel_size, p.nucleus_subdiv, p.tube_sides, p.tube_rings, (int)(p.seed & 0x7fffffff)};
         if (!cache || std::memcmp(cache->key, key, sizeof key) != 0) {
-            auto c = std::make_unique<Protos>();
+            auto c = std::make_shared<Protos>();
             std::memcpy(c->key, key, sizeof key);
             c->nuc.m = icosphere(p.nucleus_subdiv);
             build_proto(c->nuc, p.voxel_size, p.seed);
@@ -835,7 +869,7 @@ int make_instances(const GenParams& p, Protos*& PR, std::vector<VesselInst>& ves
             build_proto(c->ves, p.voxel_size, p.seed + 1);
             cache = std::move(c);
         }
-        PR = cache.get();
+        PR = cache;
     }
     const Proto& PN = PR->nuc;
     const long n_nuc = (long)p.n_vessels * p.nuclei_per_vessel;
@@ -869,6 +903,44 @@ int make_instances(const GenParams& p, Protos*& PR, std::vector<VesselInst>& ves
     };
     // nuclei placement: sequential rejection sampling with a hash grid
     const double nuc_reach = 12.0 * 1.1 + 0.01;  // max semi-axis times max radial noise
+    // vessel cells: every vessel is listed (in index order) in each cell of
+    // edge p.grid that its axis box, widened by its largest clearance, meets;
+    // a point outside that widened box never fails the clearance test, so the
+    // test visits only the vessels of the point's cell
+    const double vcell = std::max(1.0, (double)p.grid);
+    double vlo[3] = {1e300, 1e300, 1e300}, vhi[3] = {-1e300, -1e300, -1e300};
+    std::vector<double> widen(p.n_vessels);
+    for (int i = 0; i < p.n_vessels; ++i) {
+        widen[i] = ves[i].r + nuc_reach + std::max((double)p.shell_min, 5.0) + 1e-3;
+        for (int d = 0; d < 3; ++d) {
+            vlo[d] = std::min(vlo[d], vbox[i][d] - widen[i]);
+            vhi[d] = std::max(vhi[d], vbox[i][3 + d] + widen[i]);
+        }
+    }
+    long vdim[3];
+    for (int d = 0; d < 3; ++d) vdim[d] = (long)std::floor((vhi[d] - vlo[d]) / vcell) + 1;
+    std::vector<std::vector<int>> vcells((size_t)vdim[0] * vdim[1] * vdim[2]);
+    for (int i = 0; i < p.n_vessels; ++i) {
+        long c0[3], c1[3];
+        for (int d = 0; d < 3; ++d) {
+            c0[d] = (long)std::floor((vbox[i][d] - widen[i] - vlo[d]) / vcell);
+            c1[d] = (long)std::floor((vbox[i][3 + d] + widen[i] - vlo[d]) / vcell);
+        }
+        for (long x = c0[0]; x <= c1[0]; ++x)
+            for (long y = c0[1]; y <= c1[1]; ++y)
+                for (long z = c0[2]; z <= c1[2]; ++z) vcells[((size_t)x * vdim[1] + y) * vdim[2] + z].push_back(i);
+    }
+    const std::vector<int> no_vessels;
+    auto vessels_near = [&](D3 c) -> const std::vector<int>& {
+        const double q[3] = {c.x, c.y, c.z};
+        long k[3];
+        for (int d = 0; d < 3; ++d) {
+            const double f = std::floor((q[d] - vlo[d]) / vcell);
+            if (!(f >= 0.0) || f >= (double)vdim[d]) return no_vessels;
+            k[d] = (long)f;
+        }
+        return vcells[((size_t)k[0] * vdim[1] + k[1]) * vdim[2] + k[2]];
+    };
     nuc.assign(n_nuc, NucleusInst{});
     {
         const double cell = 2 * nuc_reach + 2.0;
@@ -895,10 +967,12 @@ int make_instances(const GenParams& p, Protos*& PR, std::vector<VesselInst>& ves
                     D3 c = axis + radial * rho;
                     // keep clear of every vessel and every other nucleus
                     bool bad = false;
-                    for (int wv = std::max(0, vi - gx * gx - gx - 1); wv < std::min(p.n_vessels, vi + gx * gx + gx + 2) && !bad; ++wv) {
+                    const int wlo = std::max(0, vi - gx * gx - gx - 1), whi = std::min(p.n_vessels, vi + gx * gx + gx + 2);
+                    for (int wv : vessels_near(c)) {
+                        if (wv < wlo || wv >= whi) continue;
                         const double clear = ves[wv].r + nuc_reach + (wv == vi ? p.shell_min : 5.0);
                         if (box_gap2(wv, c) > (clear + 1e-6) * (clear + 1e-6)) continue;
-                        if (seg_axis_dist(ves[wv], c) < clear) bad = true;
+                        if (seg_axis_dist(ves[wv], c) < clear) { bad = true; break; }
                     }
                     if (bad) continue;
                     long cx = (long)std::floor(c.x / cell), cy = (long)std::floor(c.y / cell), cz = (long)std::floor(c.z / cell);
@@ -921,7 +995,6 @@ int make_instances(const GenParams& p, Protos*& PR, std::vector<VesselInst>& ves
                 n.ax = g.uni(8, 12); n.ay = g.uni(8, 12); n.az = g.uni(8, 12);
                 random_rotation(g, n.rot);
                 for (double& cf : n.coef) cf = g.normal();
-                n.nscale = -1.0;  // set by noise_scale() when the nucleus is written
                 long id = (long)vi * p.nuclei_per_vessel + j;
                 nuc[id] = n;
                 long cx = (long)std::floor(n.c.x / cell), cy = (long)std::floor(n.c.y / cell), cz = (long)std::floor(n.c.z / cell);
@@ -942,11 +1015,12 @@ void nuclei_range(const GenParams& p, long& b, long& e) {
 
 int gen_tiles(const GenParams& p, uint8_t* nuc_buf, size_t nuc_cap, size_t* nuc_len, uint8_t* ves_buf,
               size_t ves_cap, size_t* ves_len, std::string& err) {
-    Protos* PR = nullptr;
-    std::vector<VesselInst> ves;
-    std::vector<NucleusInst> nuc;
-    int rc = make_instances(p, PR, ves, nuc, err);
+    std::shared_ptr<const Instances> inst;
+    int rc = make_instances(p, inst, err);
     if (rc != TDP_OK) return rc;
+    const Protos* PR = inst->protos.get();
+    const std::vector<VesselInst>& ves = inst->ves;
+    const std::vector<NucleusInst>& nuc = inst->nuc;
     const Proto& PN = PR->nuc;
     const Proto& PV = PR->ves;
     const size_t nuc_obj = object_bytes(PN), ves_obj = object_bytes(PV);
@@ -965,10 +1039,10 @@ int gen_tiles(const GenParams& p, uint8_t* nuc_buf, size_t nuc_cap, size_t* nuc_
         nuc_buf[0] = kRawType;
         parallel_for(nb1 - nb0, threads, [&](long j) {
             const long i = nb0 + j;
+            const double ns = noise_scale(nuc[i], PN.m);
             std::vector<float> Vf(3 * PN.m.V.size());
             for (size_t k = 0; k < PN.m.V.size(); ++k) {
-                if (k == 0) noise_scale(nuc[i], PN.m);
-                D3 q = nucleus_vertex(nuc[i], PN.m.V[k]);
+                D3 q = nucleus_vertex(nuc[i], PN.m.V[k], ns);
                 Vf[3 * k] = (float)q.x; Vf[3 * k + 1] = (float)q.y; Vf[3 * k + 2] = (float)q.z;
             }
             write_object(PN, Vf, nuc_buf + 1 + nuc_obj * (size_t)j);
@@ -994,11 +1068,12 @@ int gen_meshes(const GenParams& p, int which, float* V, size_t vcap, int64_t* vo
         err = "which must be 0 (nuclei) or 1 (vessels)";
         return TDP_ERR_ARG;
     }
-    Protos* PR = nullptr;
-    std::vector<VesselInst> ves;
-    std::vector<NucleusInst> nuc;
-    int rc = make_instances(p, PR, ves, nuc, err);
+    std::shared_ptr<const Instances> inst;
+    int rc = make_instances(p, inst, err);
     if (rc != TDP_OK) return rc;
+    const Protos* PR = inst->protos.get();
+    const std::vector<VesselInst>& ves = inst->ves;
+    const std::vector<NucleusInst>& nuc = inst->nuc;
     const Proto& P = which == 0 ? PR->nuc : PR->ves;
     long b = 0, e = p.n_vessels;
     if (which == 0) nuclei_range(p, b, e);
@@ -1015,10 +1090,10 @@ int gen_meshes(const GenParams& p, int which, float* V, size_t vcap, int64_t* vo
     const int threads = p.threads > 0 ? p.threads : std::max(1u, std::thread::hardware_concurrency());
     parallel_for(n, threads, [&](long j) {
         const long i = b + j;
+        const double ns = which == 0 ? noise_scale(nuc[i], P.m) : 0.0;
         float* dst = V + 3 * nv * (size_t)j;
         for (size_t k = 0; k < nv; ++k) {
-            if (which == 0 && k == 0) noise_scale(nuc[i], P.m);
-            const D3 q = which == 0 ? nucleus_vertex(nuc[i], P.m.V[k]) : vessel_vertex(ves[i], PR->tp, (int)k);
+            const D3 q = which == 0 ? nucleus_vertex(nuc[i], P.m.V[k], ns) : vessel_vertex(ves[i], PR->tp, (int)k);
             dst[3 * k] = (float)q.x; dst[3 * k + 1] = (float)q.y; dst[3 * k + 2] = (float)q.z;
         }
         uint32_t* fd = F + 3 * nf * (size_t)j;
