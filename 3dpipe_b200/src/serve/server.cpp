@@ -136,7 +136,7 @@ struct tdp_server {
     std::deque<Request*> pending;
     std::unordered_map<uint64_t, std::unique_ptr<Request>> table;
     uint64_t next_id = 1;
-    long batches = 0, completed = 0, failed = 0;
+    long batches = 0, completed = 0, failed = 0, split_batches = 0;
     double busy_ms = 0, upload_ms = 0, upload_bytes = 0, fetch_bytes = 0;
     bool stop = false;
     std::thread admitter, executor;
@@ -275,6 +275,15 @@ bool fetchable(const uint8_t* raw, size_t len, const TileHost& h, const uint8_t*
     return true;
 }
 
+// Estimated join time of a request on its own, from the serving workload's
+// per-nucleus costs on a B200 (5,000-nucleus requests against 1,000 vessels:
+// kNN 0.25 + 0.107 K us per nucleus for K = 1..50, within about 0.5 us).
+// Only the split of a batch into a small and a big pass reads it.
+double estimated_ms(const Request& r) {
+    const double per = r.knn > 0 ? 0.25 + 0.107 * r.knn : 0.5;
+    return 1e-3 * per * (double)r.host.n_obj;
+}
+
 void finish(tdp_server* S, Request* r, int status) {
     r->status = status;
     r->t_done = Clock::now();
@@ -397,47 +406,78 @@ void executor_loop(tdp_server* S) {
         }
         std::vector<Request*> reqs = a->reqs;
         lk.unlock();
-        // per-object queries of the batch
+        // Small requests first: when a batch mixes requests whose estimated
+        // join time exceeds big_request_ms with smaller ones, it runs as two joins over
+        // the arena -- the small requests' objects with their queries and the
+        // big ones' as within-0 (nearly free), then the reverse -- and each
+        // request completes with its own pass.  A query object's result does
+        // not depend on the other objects' queries, so the rows are the ones
+        // a single join gives.
+        std::vector<Request*> small, big;
+        const double big_ms = S->p.big_request_ms;
+        for (Request* r : reqs) (big_ms > 0.0 && estimated_ms(*r) > big_ms ? big : small).push_back(r);
+        std::vector<std::vector<Request*>> passes;
+        if (!small.empty() && !big.empty()) passes = {small, big};
+        else passes = {reqs};
+        if (passes.size() > 1) {
+            lk.lock();
+            ++S->split_batches;
+            lk.unlock();
+        }
         const long n = a->tile.n_obj;
-        obj_knn.assign(n, 0);
-        obj_within.assign(n, 0.f);
-        for (Request* r : reqs)
-            for (long i = 0; i < r->host.n_obj; ++i) {
-                obj_knn[r->o0 + i] = r->knn;
-                obj_within[r->o0 + i] = r->within;
-            }
-        tdp_join_params jp;
-        tdp_join_default_params(&jp);
-        std::memcpy(jp.lods, S->p.lods, sizeof(jp.lods));
-        jp.n_lods = S->p.n_lods;
-        jp.hausdorff_level = S->p.hausdorff_level;
-        jp.form = S->p.form;
-        jp.obj_knn = obj_knn.data();
-        jp.obj_within = obj_within.data();
-        tdp_result* res = nullptr;
         int rc = cudaStreamWaitEvent(ctx->stream, a->ready, 0) == cudaSuccess ? TDP_OK : TDP_ERR_CUDA;
-        if (rc == TDP_OK) rc = tdp_join(ctx, &a->tile, S->t2, &jp, &res);
-        const double fetched = rc == TDP_OK ? ctx->stats.fetch_bytes : 0.0;
-        // split the rows (sorted by query object) by request
-        if (rc == TDP_OK) {
-            for (Request* r : reqs) {
-                r->res.reset(new tdp_result());
-                const long lo = r->o0, hi = r->o0 + r->host.n_obj;
-                auto b = std::lower_bound(res->q.begin(), res->q.end(), (int)lo);
-                auto e = std::lower_bound(res->q.begin(), res->q.end(), (int)hi);
-                const size_t i0 = b - res->q.begin(), i1 = e - res->q.begin();
-                r->res->q.reserve(i1 - i0);
-                for (size_t i = i0; i < i1; ++i) r->res->q.push_back(res->q[i] - (int)lo);
-                r->res->t.assign(res->t.begin() + i0, res->t.begin() + i1);
-                r->res->d.assign(res->d.begin() + i0, res->d.begin() + i1);
+        double fetched = 0.0;
+        size_t done_passes = 0;  // passes whose requests are finished (a finished request may be freed at once)
+        for (const std::vector<Request*>& pass : passes) {
+            if (rc != TDP_OK) break;
+            // per-object queries of this pass
+            obj_knn.assign(n, 0);
+            obj_within.assign(n, 0.f);
+            for (Request* r : pass)
+                for (long i = 0; i < r->host.n_obj; ++i) {
+                    obj_knn[r->o0 + i] = r->knn;
+                    obj_within[r->o0 + i] = r->within;
+                }
+            tdp_join_params jp;
+            tdp_join_default_params(&jp);
+            std::memcpy(jp.lods, S->p.lods, sizeof(jp.lods));
+            jp.n_lods = S->p.n_lods;
+            jp.hausdorff_level = S->p.hausdorff_level;
+            jp.form = S->p.form;
+            jp.obj_knn = obj_knn.data();
+            jp.obj_within = obj_within.data();
+            tdp_result* res = nullptr;
+            if (rc == TDP_OK) rc = tdp_join(ctx, &a->tile, S->t2, &jp, &res);
+            if (rc == TDP_OK) fetched += ctx->stats.fetch_bytes;
+            // split the rows (sorted by query object) by request
+            if (rc == TDP_OK) {
+                for (Request* r : pass) {
+                    r->res.reset(new tdp_result());
+                    const long lo = r->o0, hi = r->o0 + r->host.n_obj;
+                    auto b = std::lower_bound(res->q.begin(), res->q.end(), (int)lo);
+                    auto e = std::lower_bound(res->q.begin(), res->q.end(), (int)hi);
+                    const size_t i0 = b - res->q.begin(), i1 = e - res->q.begin();
+                    r->res->q.reserve(i1 - i0);
+                    for (size_t i = i0; i < i1; ++i) r->res->q.push_back(res->q[i] - (int)lo);
+                    r->res->t.assign(res->t.begin() + i0, res->t.begin() + i1);
+                    r->res->d.assign(res->d.begin() + i0, res->d.begin() + i1);
+                }
+            }
+            delete res;
+            if (&pass != &passes.back() && rc == TDP_OK) {  // this pass's requests are done
+                lk.lock();
+                for (Request* r : pass) finish(S, r, rc);
+                S->cv.notify_all();
+                lk.unlock();
+                ++done_passes;
             }
         }
-        delete res;
         const double busy = ms_between(t_start, Clock::now());
         lk.lock();
         S->busy_ms += busy;
         S->fetch_bytes += fetched;
-        for (Request* r : reqs) finish(S, r, rc);
+        for (size_t k = done_passes; k < passes.size(); ++k)
+            for (Request* r : passes[k]) finish(S, r, rc);
         reset_arena(*a);
         a->state = ArenaState::kFree;
         S->cv.notify_all();
@@ -457,6 +497,7 @@ void tdp_server_default_params(tdp_server_params* p) {
     p->max_request_bytes = (size_t)1 << 30;
     p->hausdorff_level = 2;
     p->form = TDP_FORM_TUNED;
+    p->big_request_ms = 4.0;
 }
 
 int tdp_server_create(tdp_ctx* ctx, const tdp_tile* t2, const tdp_server_params* p, tdp_server** out) {
@@ -590,6 +631,7 @@ int tdp_server_get_stats(const tdp_server* S, tdp_server_stats* o) {
     if (!S || !o) return TDP_ERR_ARG;
     std::lock_guard<std::mutex> lk(const_cast<tdp_server*>(S)->mu);
     o->batches = S->batches;
+    o->split_batches = S->split_batches;
     o->requests = S->completed;
     o->failed = S->failed;
     o->busy_ms = S->busy_ms;

@@ -546,7 +546,7 @@ def raw_slice(raw: np.ndarray, offsets: np.ndarray, b: int, e: int) -> np.ndarra
 class ServerParams(C.Structure):
     _fields_ = [("arena_objects", C.c_long), ("arena_voxels", C.c_long), ("arena_tris", C.c_long),
                 ("max_request_bytes", C.c_size_t), ("lods", C.c_int * 8), ("n_lods", C.c_int),
-                ("hausdorff_level", C.c_int), ("form", C.c_int)]
+                ("hausdorff_level", C.c_int), ("form", C.c_int), ("big_request_ms", C.c_double)]
 
 
 class RequestInfo(C.Structure):
@@ -556,7 +556,8 @@ class RequestInfo(C.Structure):
 
 class ServerStats(C.Structure):
     _fields_ = [("batches", C.c_long), ("requests", C.c_long), ("failed", C.c_long), ("busy_ms", C.c_double),
-                ("upload_ms", C.c_double), ("upload_bytes", C.c_double), ("fetch_bytes", C.c_double)]
+                ("upload_ms", C.c_double), ("upload_bytes", C.c_double), ("fetch_bytes", C.c_double),
+                ("split_batches", C.c_long)]
 
 
 class Server:

@@ -435,6 +435,10 @@ typedef struct {
     int n_lods;
     int hausdorff_level;       /* default 2 */
     int form;                  /* default TDP_FORM_TUNED */
+    double big_request_ms;     /* a batch that mixes requests estimated above this join
+                                  time with smaller ones runs as two joins, the small
+                                  requests first, each request done with its own pass
+                                  (default 4; <= 0: one join per batch)                  */
 } tdp_server_params;
 typedef struct {
     double queue_ms;           /* submit -> its batch started                              */
@@ -454,6 +458,7 @@ typedef struct {
                                   of requests not in page-locked memory                    */
     double fetch_bytes;        /* RAW bytes the batch joins fetched from page-locked
                                   requests (only the voxels they refined)                  */
+    long split_batches;        /* batches run as a small pass and a big pass               */
 } tdp_server_stats;
 void tdp_server_default_params(tdp_server_params *p);
 /* allocates both arenas in the context (counted against its budget) */

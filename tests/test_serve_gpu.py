@@ -36,13 +36,16 @@ def setup(pkg, ctx):
 
 @pytest.mark.parametrize("arena_objects", [40, 100000])
 @pytest.mark.parametrize("pinned", [False, True])
-def test_each_request_equals_its_join_alone(pkg, ctx, setup, arena_objects, pinned):
+@pytest.mark.parametrize("big_ms", [4.0, 0.005])
+def test_each_request_equals_its_join_alone(pkg, ctx, setup, arena_objects, pinned, big_ms):
     """pinned: requests in page-locked memory, whose triangles the batch joins
-    fetch from the caller's bytes instead of staging them whole."""
+    fetch from the caller's bytes instead of staging them whole.  big_ms =
+    0.005: these requests' estimated join times (3 of them below, 5 above)
+    make every mixed batch run as a small pass then a big pass."""
     T2, reqs, alone = setup
     bufs = [pkg.tdp.pinned_copy(r[0]) if pinned else r[0] for r in reqs]
     with pkg.tdp.Server(ctx, T2, arena_objects=arena_objects, arena_voxels=1 << 16, arena_tris=1 << 20,
-                        max_request_bytes=64 << 20) as srv:
+                        max_request_bytes=64 << 20, big_request_ms=big_ms) as srv:
         ids = [None] * len(reqs)
 
         def client(k):
@@ -73,6 +76,10 @@ def test_each_request_equals_its_join_alone(pkg, ctx, setup, arena_objects, pinn
         if arena_objects == 40:
             assert st["batches"] >= 4  # 128 objects of requests, at most 40 per batch
         assert max(i["batch_requests"] for i in infos) >= 2  # requests were mixed in a batch
+        if big_ms == 4.0:
+            assert st["split_batches"] == 0  # every request here is far below 4 ms
+        elif arena_objects == 100000 and max(i["batch_requests"] for i in infos) == len(reqs):
+            assert st["split_batches"] >= 1  # one batch held small and big requests
     # the context is usable again after the server is closed
     raw, query, K, tau = reqs[0]
     T1 = pkg.tdp.Tile(ctx, raw)
