@@ -435,7 +435,10 @@ __global__ void k_recheck_knn(JoinDev d, int K_all, const double* __restrict__ p
     }
 }
 
-__global__ void __launch_bounds__(kBlock) k_pair_update(JoinDev d, int stamp, int tuned) {
+// decide != 0: the within decision of k_within_decide is taken here too, for
+// the within query objects, as soon as the pair's bounds are known (the tuned
+// LOD loop; it saves a launch and a pass over the pairs per LOD)
+__global__ void __launch_bounds__(kBlock) k_pair_update(JoinDev d, int stamp, int tuned, int decide, float tau_all) {
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < d.P; p += nw) {
@@ -461,6 +464,20 @@ __global__ void __launch_bounds__(kBlock) k_pair_update(JoinDev d, int stamp, in
             d.pmn[p] = mindist;
             d.pmx[p] = minmax;
             d.perr[p] = err;
+            if (decide) {  // as k_within_decide
+                float tau = tau_all;
+                bool within = true;
+                if (d.qk) {
+                    const int q = d.pq[p];
+                    within = d.qk[q] <= 0;
+                    tau = d.qtau[q];
+                }
+                if (within) {
+                    const float e = tuned ? err : 0.f;
+                    if (minmax + e <= tau) d.pstat[p] = kReported;
+                    else if (mindist - e > tau) d.pstat[p] = kDropped;
+                }
+            }
         }
     }
 }
@@ -560,9 +577,9 @@ cudaError_t launch_apply_results(const JoinDev& d, const float4* res, const int*
     k_apply_results<<<grid_for(W, 256), 256, 0, s>>>(d, res, item_vp, W, W_dev, highest, level, li, stamp);
     return cudaGetLastError();
 }
-cudaError_t launch_pair_update(const JoinDev& d, int stamp, int tuned, cudaStream_t s) {
+cudaError_t launch_pair_update(const JoinDev& d, int stamp, int tuned, cudaStream_t s, int decide, float tau) {
     if (d.P <= 0) return cudaSuccess;
-    k_pair_update<<<grid_for(d.P, kBlock / 32), kBlock, 0, s>>>(d, stamp, tuned);
+    k_pair_update<<<grid_for(d.P, kBlock / 32), kBlock, 0, s>>>(d, stamp, tuned, decide, tau);
     return cudaGetLastError();
 }
 cudaError_t launch_recheck_items(const JoinDev& d, const uint32_t* vt1, const uint32_t* vt2, RefineItem* items,

@@ -77,7 +77,8 @@ cudaError_t launch_build_items(const JoinDev& d, const uint32_t* vtri1, const ui
 // W: item count, or an upper bound when W_dev (the exact count in device memory) is given
 cudaError_t launch_apply_results(const JoinDev& d, const float4* res, const int* item_vp, int W, int highest,
                                  int level, int lod_idx, int stamp, cudaStream_t s, const unsigned* W_dev = nullptr);
-cudaError_t launch_pair_update(const JoinDev& d, int stamp, int tuned, cudaStream_t s);
+// decide != 0 also takes the within decision (k_within_decide) of each pair
+cudaError_t launch_pair_update(const JoinDev& d, int stamp, int tuned, cudaStream_t s, int decide = 0, float tau = 0.f);
 // tuned form: FP64 recheck of the pairs left undecided after LOD 100
 cudaError_t launch_recheck_items(const JoinDev& d, const uint32_t* vtri1, const uint32_t* vtri2, RefineItem* items,
                                  int* item_vp, double* vexact, unsigned* counter, cudaStream_t s);

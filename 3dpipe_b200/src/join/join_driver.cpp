@@ -118,9 +118,10 @@ int enqueue_lod_loop(tdp_ctx* ctx, const LodLoop& L, cudaStream_t s, bool captur
                                 cnt_items));
         CUL(rec(L.ev[2 * k + 1]));
         CUL(launch_apply_results(L.d, L.res, L.item_vp, V, highest, L.hlevel, L.li[k], k, s, cnt_items));
-        CUL(launch_pair_update(L.d, k, 1, s));
+        // the within decision is taken inside the pair update; the kNN rank
+        // reads every candidate of a query and stays its own launch
+        CUL(launch_pair_update(L.d, k, 1, s, L.any_within ? 1 : 0, L.tau));
         if (L.any_knn) CUL(launch_knn_rank(L.d, L.K, 1, L.rankst, s));
-        if (L.any_within) CUL(launch_within_decide(L.d, L.tau, 1, s));
     }
     if (L.recheck) {
         CUL(launch_count_status(L.d, cnt_recheck, s));
@@ -463,7 +464,12 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         L.side = ctx->side;
         for (int k = 0; k < 16; ++k) L.pf[k] = ctx->pf_ev[k];
         if ((rc = run_lod_loop(ctx, L, s, &st.lod_graph))) return rc;
-        launches += 5 * L.nl + (L.recheck ? (knn ? 6 : 5) : 0);
+        {   // per LOD: items, refine, apply, pair update (with the within decision),
+            // the kNN rank; on attached tiles the fetch and the next LOD's prefetch
+            const bool attached = L.lz1.on || L.lz2.on;
+            launches += (4 + (L.any_knn ? 1 : 0) + (attached ? 1 : 0)) * L.nl +
+                        (attached && L.side ? L.nl - 1 : 0) + (L.recheck ? (knn ? 6 : 5) : 0);
+        }
         st.refine_launches += L.nl;
     }
 
