@@ -184,7 +184,37 @@ __global__ void k_check_layout(AttachOut o, long n_vox) {
     }
 }
 
+// the u64 at byte address p (any alignment) from the aligned words around it;
+// the 4 bytes after it belong to the same record (data or the voxel table
+// follow both fields read here)
+__device__ __forceinline__ uint64_t u64_at(uintptr_t p) {
+    const uint32_t* W = reinterpret_cast<const uint32_t*>(p & ~uintptr_t(3));
+    const unsigned sh = (unsigned)(p & 3) * 8;
+    const uint32_t w0 = W[0], w1 = W[1];
+    const uint32_t lo = sh ? __funnelshift_r(w0, w1, sh) : w0;
+    const uint32_t hi = sh ? __funnelshift_r(w1, W[2], sh) : w1;
+    return (uint64_t)lo | ((uint64_t)hi << 32);
+}
+
+__global__ void k_check_strided(const uint8_t* __restrict__ raw, const AttachRec* __restrict__ recs, long n_obj,
+                                uint64_t data_size, uint64_t vnum, unsigned long long* first_bad) {
+    for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n_obj; o += (long)gridDim.x * blockDim.x) {
+        const AttachRec r = recs[o];
+        const uintptr_t base = reinterpret_cast<uintptr_t>(raw);
+        if (u64_at(base + r.data_off - 8) != data_size || u64_at(base + r.meta - 8) != vnum)
+            atomicMin(first_bad, (unsigned long long)o);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_check_strided(const uint8_t* raw_dev, const AttachRec* recs, long n_obj, uint64_t data_size,
+                                 uint64_t vnum, unsigned long long* first_bad, int num_sms, cudaStream_t s) {
+    if (n_obj <= 0) return cudaSuccess;
+    const int blocks = (int)std::max<long>(1, std::min<long>((n_obj + 255) / 256, (long)num_sms * 8));
+    k_check_strided<<<blocks, 256, 0, s>>>(raw_dev, recs, n_obj, data_size, vnum, first_bad);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_attach_tables(const uint8_t* raw_dev, const AttachRec* recs, long n_obj, long n_vox,
                                  const AttachOut& out, void* scan_tmp, size_t& scan_bytes, int num_sms,

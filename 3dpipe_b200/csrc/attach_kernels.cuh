@@ -40,4 +40,11 @@ cudaError_t launch_attach_tables(const uint8_t* raw_dev, const AttachRec* recs, 
                                  const AttachOut& out, void* scan_tmp, size_t& scan_bytes, int num_sms,
                                  cudaStream_t s);
 
+// Records placed by the first record's stride instead of a walk: each
+// object's data size and voxel count (the 8 bytes before data_off and before
+// meta) must equal the first object's, else *first_bad takes the lowest
+// object that differs (the caller then walks the tile on the host).
+cudaError_t launch_check_strided(const uint8_t* raw_dev, const AttachRec* recs, long n_obj, uint64_t data_size,
+                                 uint64_t vnum, unsigned long long* first_bad, int num_sms, cudaStream_t s);
+
 }  // namespace tdp

@@ -103,8 +103,24 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
     auto ms_since = [](std::chrono::steady_clock::time_point a) {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
     };
+    // A tile of equal-size records (instances of one mesh) needs no walk:
+    // the records are placed at the first record's stride when the length is
+    // a whole number of strides, and the GPU checks every object's size
+    // fields against the first one's (any difference: the host walks it).
     HostVec<RawRec> recs;
-    if (!walk_raw_dt(buf, len, max_objects, recs) || recs.empty()) {
+    RawRec r0{};
+    uint64_t stride = 0;
+    const bool strided = max_objects <= 0 && raw_first_record(buf, len, r0, stride) && (len - 1) % stride == 0 &&
+                         (len - 1) / stride >= 1024;
+    if (strided) {
+        const long ns = (long)((len - 1) / stride);
+        recs.resize((size_t)ns);
+        RawRec* rp = recs.data();
+        host_parallel(ns, [&](long b, long e) {
+            for (long o = b; o < e; ++o)
+                rp[o] = RawRec{r0.data_off + o * stride, r0.data_size, r0.meta + o * stride, r0.vnum};
+        });
+    } else if (!walk_raw_dt(buf, len, max_objects, recs) || recs.empty()) {
         tile_release(ctx, T);
         return kUseHostParse;
     }
@@ -200,6 +216,9 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
     GCTRY(cudaMemcpyAsync(T->obj_vox + n, nvox_src, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
     GCTRY(cudaMemsetAsync(ctr.p, 0, 8 * sizeof(unsigned long long), s));
     GCTRY(cudaMemsetAsync((unsigned long long*)ctr.p + 8, 0xff, sizeof(unsigned long long), s));
+    if (strided)
+        GCTRY(launch_check_strided(dev_view, (const AttachRec*)recs_d.p, n, r0.data_size, r0.vnum, o.first_bad,
+                                   ctx->num_sms, s));
     GCTRY(launch_attach_tables(dev_view, (const AttachRec*)recs_d.p, n, (long)nvox, o, tmp.p, scan_bytes,
                                ctx->num_sms, s));
     unsigned long long res[9] = {0};

@@ -286,6 +286,14 @@ bool walk_chain(const uint8_t* buf, size_t len, size_t& pos, long limit, Rec* ou
 // parallel into arrays sized from the walk.  Content errors are reported for
 // the lowest object that has one, the error the sequential parser would meet
 // first, with the same message.
+bool raw_first_record(const uint8_t* buf, size_t len, RawRec& r, uint64_t& stride) {
+    if (!buf || len < 2 || buf[0] != kRawType) return false;
+    size_t p = 1;
+    if (!walk_one(buf, len, p, r)) return false;
+    stride = p - 1;
+    return true;
+}
+
 bool walk_raw_dt(const uint8_t* buf, size_t len, long max_objects, HostVec<RawRec>& recs) {
     recs.clear();
     if (!buf || len < 1 || buf[0] != kRawType) return false;

@@ -138,6 +138,10 @@ struct RawRec {
 // type byte; the voxel tables are not read.
 bool walk_raw_dt(const uint8_t* buf, size_t len, long max_objects, HostVec<RawRec>& recs);
 
+// The record of the first object and its length in bytes (the stride), or
+// false when the first record is not well formed.
+bool raw_first_record(const uint8_t* buf, size_t len, RawRec& r, uint64_t& stride);
+
 // Parse `len` bytes; at most max_objects objects (<= 0: all).  Returns 0 or a
 // TDP_ERR_* code with a message in `err`.
 int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& out, std::string& err,

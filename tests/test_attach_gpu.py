@@ -168,3 +168,31 @@ def test_attached_metadata_equal_uploaded(pkg, pctx):
             np.testing.assert_array_equal(i1, i2)
         U.free()
         A.free()
+
+
+def test_strided_attach_equals_walked(pkg, pctx):
+    """A tile of equal-size records is attached without a host walk (records
+    placed at the first record's stride, every object's size fields checked
+    on the GPU).  Records of equal size but different kinds (1 voxel with
+    triangles, or 12 voxels without) fail that check at the first record of
+    the other kind and the tile is walked on the host: both give the host
+    parser's counts and, for the generated tile, the uploaded tile's
+    candidates."""
+    from test_raw_parse import _uniform_tile, _record
+    nb, _ = pkg.tdp.gen_tiles(10, 200, seed=9)           # 2,000 equal nucleus records: strided
+    U = pkg.tdp.Tile(pctx, nb)
+    A = pkg.tdp.Tile(pctx, pkg.tdp.pinned_copy(nb), attach=True)
+    for k in ("n_objects", "n_voxels", "n_tris"):
+        assert U.info()[k] == A.info()[k], k
+    o1, i1 = pkg.tdp.tile_candidates(pctx, U, None, knn=4)
+    o2, i2 = pkg.tdp.tile_candidates(pctx, A, None, knn=4)
+    np.testing.assert_array_equal(o1, o2)
+    np.testing.assert_array_equal(i1, i2)
+    U.free()
+    A.free()
+    raw, nvox, _ = _uniform_tile(3000, 12)               # two record kinds of one size: walked after the check
+    assert len(_record("A")) == len(_record("B"))
+    A = pkg.tdp.Tile(pctx, pkg.tdp.pinned_copy(raw), attach=True)
+    info = A.info()
+    assert info["n_objects"] == 3000 and info["n_voxels"] == int(nvox.sum())
+    A.free()
