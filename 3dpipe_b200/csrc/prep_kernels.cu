@@ -715,16 +715,17 @@ using namespace tdp;
 
 namespace {
 
-struct DevMem {  // allocations of one call, freed on every return
+struct DevMem {  // allocations of one batch, back to the context's block cache on every return
     tdp_ctx* ctx;
     std::vector<void*> ps;
     ~DevMem() {
-        for (void* p : ps) dfree(ctx, p);
+        cudaStreamSynchronize(ctx->stream);  // nothing queued may still use a block
+        for (void* p : ps) block_release(ctx, p);
     }
     template <typename X>
     cudaError_t get(X** p, size_t count) {
         void* q = nullptr;
-        const cudaError_t e = dmalloc(ctx, &q, std::max<size_t>(count, 1) * sizeof(X));
+        const cudaError_t e = block_alloc(ctx, &q, std::max<size_t>(count, 1) * sizeof(X));
         if (e == cudaSuccess) ps.push_back(q);
         *p = (X*)q;
         return e;
@@ -903,11 +904,16 @@ extern "C" int tdp_raw_from_meshes(tdp_ctx* ctx, const float* vertices, const in
         CU(cudaGetLastError());
         CU(cudaEventRecord(ev[2], s));
         bytes.assign(nb, 0);
+        float ms_vox[2] = {0, 0};
         std::vector<uint32_t> hcnt((size_t)kDecLods * nb), hnvox(nb);
         CU(cudaMemcpyAsync(bytes.data(), dbytes, 8 * nb, cudaMemcpyDeviceToHost, s));
         CU(cudaMemcpyAsync(hcnt.data(), lodCnt, 4 * hcnt.size(), cudaMemcpyDeviceToHost, s));
         CU(cudaMemcpyAsync(hnvox.data(), S.nvox, 4 * nb, cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
+        cudaEventElapsedTime(&ms_vox[0], ev[0], ev[1]);
+        cudaEventElapsedTime(&ms_vox[1], ev[1], ev[2]);
+        inf.decimate_ms += ms_vox[0];
+        inf.voxel_ms += ms_vox[1];
         std::vector<unsigned long long> hpos(nb);
         unsigned long long run = 0;
         for (long i = 0; i < nb; ++i) {
@@ -922,21 +928,15 @@ extern "C" int tdp_raw_from_meshes(tdp_ctx* ctx, const float* vertices, const in
             uint32_t* dout;
             CU(dm.get(&dout, (size_t)(run / 4)));
             CU(cudaMemcpyAsync(dpos, hpos.data(), 8 * nb, cudaMemcpyHostToDevice, s));
+            CU(cudaEventRecord(ev[2], s));  // the writer alone (the host's allocation above is not timed)
             k_write<kPrepThreads><<<(int)nb, kPrepThreads, 0, s>>>(Mh, lodF, lodCnt, S, dpos, dout);
             CU(cudaGetLastError());
             CU(cudaEventRecord(ev[3], s));
             CU(cudaMemcpyAsync((uint8_t*)out + pos_out, dout, (size_t)run, cudaMemcpyDeviceToHost, s));
             CU(cudaStreamSynchronize(s));
-            float ms[3] = {0, 0, 0};
-            for (int k = 0; k < 3; ++k) cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]);
-            inf.decimate_ms += ms[0];
-            inf.voxel_ms += ms[1];
-            inf.write_ms += ms[2];
-        } else {
-            float ms[2] = {0, 0};
-            for (int k = 0; k < 2; ++k) cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]);
-            inf.decimate_ms += ms[0];
-            inf.voxel_ms += ms[1];
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev[2], ev[3]);
+            inf.write_ms += ms;
         }
         pos_out += (size_t)run;
         inf.batches += 1;
