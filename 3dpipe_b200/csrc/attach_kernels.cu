@@ -35,7 +35,10 @@ constexpr int kWarps = 8;
 constexpr int kVoxWords = 29;  // 9 floats + 5 x (offset, count) as u64
 constexpr int kChunkVox = 32;  // voxels per warp and round (one per lane)
 constexpr int kHdWords = 2 * kNumLods;
-constexpr int kStage = kHdWords + kChunkVox * kVoxWords + 3;  // words staged per window
+// words staged per window: 2 lead words (the voxel count before the
+// Hausdorff values, first window), the tables, the transform and 2 tail
+// words (the next object's data size, last window)
+constexpr int kStage = 2 + kHdWords + kChunkVox * kVoxWords + 3 + 2;
 
 constexpr int kChunks = (4 * kStage + 30) / 16 + 1;  // 16-byte chunks a window spans, at most
 constexpr int kChunkLoads = (kChunks + 31) / 32;      // per lane
@@ -82,9 +85,13 @@ __device__ __forceinline__ void stage_chunks(uintptr_t p, uint32_t cnt, int lane
     }
 }
 
+// strided: the records were placed at the first record's stride instead of
+// walked, so every object's voxel count (the 8 bytes before its Hausdorff
+// values) and the next object's data size (the 8 bytes after its transform)
+// are checked against the first object's, read with the windows they border
 __global__ void __launch_bounds__(kWarps * 32) k_parse_tables(const uint8_t* __restrict__ raw,
                                                               const AttachRec* __restrict__ recs, long n_obj,
-                                                              AttachOut o) {
+                                                              AttachOut o, int strided, uint64_t data_size0) {
     __shared__ __align__(16) uint32_t stage[kWarps][kStageAlloc];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t* st = stage[w];
@@ -103,17 +110,22 @@ __global__ void __launch_bounds__(kWarps * 32) k_parse_tables(const uint8_t* __r
             const bool last = c0 + m == r.vnum;
             const uint64_t ws = c0 == 0 ? 0 : kHdWords + (uint64_t)c0 * kVoxWords;
             const uint64_t we = kHdWords + (uint64_t)(c0 + m) * kVoxWords + (last ? 3 : 0);
+            const uint32_t lead = strided && c0 == 0 ? 2u : 0u;
+            const uint32_t tail = strided && last && ob + 1 < n_obj ? 2u : 0u;
             __syncwarp();
-            stage_chunks(base + 4 * ws, (uint32_t)(we - ws), lane, st);
+            stage_chunks(base + 4 * ws - 4 * lead, (uint32_t)(we - ws) + lead + tail, lane, st);
             __syncwarp();
+            const uint32_t* S = st + lead;  // S[i]: word ws + i of the block
+            if (lead && ((uint64_t)st[0] | ((uint64_t)st[1] << 32)) != r.vnum) bad = true;
+            if (tail && ((uint64_t)S[we - ws] | ((uint64_t)S[we - ws + 1] << 32)) != data_size0) bad = true;
             if (c0 == 0 && lane < kHdWords) {  // object Hausdorff values: 5 x (hausdorff, proxy)
-                const float v = __uint_as_float(st[lane]);
+                const float v = __uint_as_float(S[lane]);
                 if (lane & 1) o.obj_phd[ob * kNumLods + (lane >> 1)] = v;
                 else o.obj_hd[ob * kNumLods + (lane >> 1)] = v;
             }
-            if (last && lane < 3) xf = __uint_as_float(st[xw - ws + lane]);
+            if (last && lane < 3) xf = __uint_as_float(S[xw - ws + lane]);
             if (lane < m) {
-                const uint32_t* q = st + (kHdWords + (uint64_t)(c0 + lane) * kVoxWords - ws);
+                const uint32_t* q = S + (kHdWords + (uint64_t)(c0 + lane) * kVoxWords - ws);
                 const uint32_t v = r.vox0 + c0 + lane;
                 float b[9];
 #pragma unroll
@@ -184,41 +196,11 @@ __global__ void k_check_layout(AttachOut o, long n_vox) {
     }
 }
 
-// the u64 at byte address p (any alignment) from the aligned words around it;
-// the 4 bytes after it belong to the same record (data or the voxel table
-// follow both fields read here)
-__device__ __forceinline__ uint64_t u64_at(uintptr_t p) {
-    const uint32_t* W = reinterpret_cast<const uint32_t*>(p & ~uintptr_t(3));
-    const unsigned sh = (unsigned)(p & 3) * 8;
-    const uint32_t w0 = W[0], w1 = W[1];
-    const uint32_t lo = sh ? __funnelshift_r(w0, w1, sh) : w0;
-    const uint32_t hi = sh ? __funnelshift_r(w1, W[2], sh) : w1;
-    return (uint64_t)lo | ((uint64_t)hi << 32);
-}
-
-__global__ void k_check_strided(const uint8_t* __restrict__ raw, const AttachRec* __restrict__ recs, long n_obj,
-                                uint64_t data_size, uint64_t vnum, unsigned long long* first_bad) {
-    for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n_obj; o += (long)gridDim.x * blockDim.x) {
-        const AttachRec r = recs[o];
-        const uintptr_t base = reinterpret_cast<uintptr_t>(raw);
-        if (u64_at(base + r.data_off - 8) != data_size || u64_at(base + r.meta - 8) != vnum)
-            atomicMin(first_bad, (unsigned long long)o);
-    }
-}
-
 }  // namespace
-
-cudaError_t launch_check_strided(const uint8_t* raw_dev, const AttachRec* recs, long n_obj, uint64_t data_size,
-                                 uint64_t vnum, unsigned long long* first_bad, int num_sms, cudaStream_t s) {
-    if (n_obj <= 0) return cudaSuccess;
-    const int blocks = (int)std::max<long>(1, std::min<long>((n_obj + 255) / 256, (long)num_sms * 8));
-    k_check_strided<<<blocks, 256, 0, s>>>(raw_dev, recs, n_obj, data_size, vnum, first_bad);
-    return cudaGetLastError();
-}
 
 cudaError_t launch_attach_tables(const uint8_t* raw_dev, const AttachRec* recs, long n_obj, long n_vox,
                                  const AttachOut& out, void* scan_tmp, size_t& scan_bytes, int num_sms,
-                                 cudaStream_t s) {
+                                 cudaStream_t s, bool strided, uint64_t data_size0) {
     if (!scan_tmp) {  // size query for the scans
         size_t b = 0;
         const cudaError_t e =
@@ -232,7 +214,7 @@ cudaError_t launch_attach_tables(const uint8_t* raw_dev, const AttachRec* recs, 
         if (e != cudaSuccess) return e;
     }
     const int blocks = (int)std::max<long>(1, std::min<long>((n_obj + kWarps - 1) / kWarps, (long)num_sms * 16));
-    k_parse_tables<<<blocks, kWarps * 32, 0, s>>>(raw_dev, recs, n_obj, out);
+    k_parse_tables<<<blocks, kWarps * 32, 0, s>>>(raw_dev, recs, n_obj, out, strided ? 1 : 0, data_size0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     for (int l = 0; l < kNumLods; ++l) {  // in place: counts at [1, n_vox] become the prefix

@@ -36,15 +36,12 @@ struct AttachOut {
 // Parse the voxel tables of n_obj objects from raw_dev (the device view of the
 // page-locked tile bytes), scan the counts into vtri, check the layout.  Call
 // first with scan_tmp == nullptr to learn scan_bytes.
+// strided: the records were placed at the first record's stride (no walk);
+// each object's voxel count and the next object's data size are then
+// checked against the first object's (data_size0), and a difference flags
+// the object in first_bad (the caller walks the tile on the host).
 cudaError_t launch_attach_tables(const uint8_t* raw_dev, const AttachRec* recs, long n_obj, long n_vox,
                                  const AttachOut& out, void* scan_tmp, size_t& scan_bytes, int num_sms,
-                                 cudaStream_t s);
-
-// Records placed by the first record's stride instead of a walk: each
-// object's data size and voxel count (the 8 bytes before data_off and before
-// meta) must equal the first object's, else *first_bad takes the lowest
-// object that differs (the caller then walks the tile on the host).
-cudaError_t launch_check_strided(const uint8_t* raw_dev, const AttachRec* recs, long n_obj, uint64_t data_size,
-                                 uint64_t vnum, unsigned long long* first_bad, int num_sms, cudaStream_t s);
+                                 cudaStream_t s, bool strided = false, uint64_t data_size0 = 0);
 
 }  // namespace tdp

@@ -125,11 +125,22 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
         return kUseHostParse;
     }
     const long n = (long)recs.size();
-    uint64_t nvox = 0, meta_bytes = 0;
-    for (const RawRec& r : recs) {
-        nvox += r.vnum;
-        meta_bytes += 2 * kNumLods * 4 + r.vnum * 116 + 12;
+    // voxel counts per chunk of objects, in parallel, then their prefix
+    const long nch = std::max(1L, std::min<long>((long)std::thread::hardware_concurrency(), n / 4096));
+    std::vector<uint64_t> ch_vox(nch + 1, 0);
+    {
+        std::vector<std::thread> pool;
+        for (long k = 0; k < nch; ++k)
+            pool.emplace_back([&, k] {
+                uint64_t sv = 0;
+                for (long o = n * k / nch; o < n * (k + 1) / nch; ++o) sv += recs[o].vnum;
+                ch_vox[k + 1] = sv;
+            });
+        for (auto& th : pool) th.join();
+        for (long k = 0; k < nch; ++k) ch_vox[k + 1] += ch_vox[k];
     }
+    const uint64_t nvox = ch_vox[nch];
+    const uint64_t meta_bytes = (uint64_t)n * (2 * kNumLods * 4 + 12) + nvox * 116;
     if (nvox >= 0xffffffffull) {
         tile_release(ctx, T);
         return kUseHostParse;
@@ -148,15 +159,23 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
         ar_pageable.resize(n + 1);
         ar = ar_pageable.data();
     }
-    uint32_t v0 = 0;
-    for (long o = 0; o < n; ++o) {
-        const RawRec& r = recs[o];
-        ar[o] = AttachRec{r.data_off, r.data_size, r.meta, (uint32_t)r.vnum, v0};
-        H.obj_vox_off[o] = v0;
-        H.obj_data_off[o] = r.data_off;
-        H.obj_data_size[o] = r.data_size;
-        v0 += (uint32_t)r.vnum;
+    {
+        std::vector<std::thread> pool;
+        for (long k = 0; k < nch; ++k)
+            pool.emplace_back([&, k] {
+                uint32_t v0 = (uint32_t)ch_vox[k];
+                for (long o = n * k / nch; o < n * (k + 1) / nch; ++o) {
+                    const RawRec& r = recs[o];
+                    ar[o] = AttachRec{r.data_off, r.data_size, r.meta, (uint32_t)r.vnum, v0};
+                    H.obj_vox_off[o] = v0;
+                    H.obj_data_off[o] = r.data_off;
+                    H.obj_data_size[o] = r.data_size;
+                    v0 += (uint32_t)r.vnum;
+                }
+            });
+        for (auto& th : pool) th.join();
     }
+    const uint32_t v0 = (uint32_t)nvox;
     H.obj_vox_off[n] = v0;
     uint32_t* nvox_src = reinterpret_cast<uint32_t*>(ar + n);
     *nvox_src = v0;
@@ -216,11 +235,8 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
     GCTRY(cudaMemcpyAsync(T->obj_vox + n, nvox_src, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
     GCTRY(cudaMemsetAsync(ctr.p, 0, 8 * sizeof(unsigned long long), s));
     GCTRY(cudaMemsetAsync((unsigned long long*)ctr.p + 8, 0xff, sizeof(unsigned long long), s));
-    if (strided)
-        GCTRY(launch_check_strided(dev_view, (const AttachRec*)recs_d.p, n, r0.data_size, r0.vnum, o.first_bad,
-                                   ctx->num_sms, s));
     GCTRY(launch_attach_tables(dev_view, (const AttachRec*)recs_d.p, n, (long)nvox, o, tmp.p, scan_bytes,
-                               ctx->num_sms, s));
+                               ctx->num_sms, s, strided, r0.data_size));
     unsigned long long res[9] = {0};
     GCTRY(cudaMemcpyAsync(res, ctr.p, 9 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     H.obj_box.resize((size_t)6 * n);
