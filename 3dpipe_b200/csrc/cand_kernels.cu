@@ -322,8 +322,10 @@ int upload_grid(tdp_ctx* ctx, DevGrid& g, const CellGrid& h) {
     }
     g.cell = h.cell;
     g.slack = h.slack;
-    if (dmalloc(ctx, (void**)&g.start, h.start.size() * 8) != cudaSuccess ||
-        dmalloc(ctx, (void**)&g.items, std::max<size_t>(h.items.size(), 1) * 4) != cudaSuccess)
+    // from the block cache (at least a cached block's size): a tile attached
+    // and freed every request then neither allocates nor frees device memory
+    if (block_alloc(ctx, (void**)&g.start, std::max<size_t>(h.start.size() * 8, kCachedBlockMin)) != cudaSuccess ||
+        block_alloc(ctx, (void**)&g.items, std::max<size_t>(h.items.size() * 4, kCachedBlockMin)) != cudaSuccess)
         return fail(ctx, TDP_ERR_NOMEM, "cannot allocate the candidate grid");
     cudaMemcpyAsync(g.start, h.start.data(), h.start.size() * 8, cudaMemcpyHostToDevice, ctx->stream);
     if (!h.items.empty())

@@ -85,10 +85,10 @@ void tile_release(tdp_ctx* ctx, tdp_tile* t) {
     block_release(ctx, t->lazy_state);
     block_release(ctx, t->lazy_bytes);
     block_release(ctx, t->d_boxes);
-    dfree(ctx, t->box_grid.start);
-    dfree(ctx, t->box_grid.items);
-    dfree(ctx, t->point_grid.start);
-    dfree(ctx, t->point_grid.items);
+    block_release(ctx, t->box_grid.start);
+    block_release(ctx, t->box_grid.items);
+    block_release(ctx, t->point_grid.start);
+    block_release(ctx, t->point_grid.items);
     delete t;
 }
 
