@@ -159,14 +159,6 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
         ar_pageable.resize(n + 1);
         ar = ar_pageable.data();
     }
-    // Strided records: every object's voxel table (with the voxel count before
-    // it and the next object's data size after it) is one row of a 2-D copy
-    // engine transfer into device memory, pitch dpitch, and the pass reads
-    // the rows there (ar[o].meta is then an offset into that buffer); the
-    // copy engine moves these 1.6 KB rows 170 KB apart faster than the SMs'
-    // zero-copy reads (52 against 45-49 GB/s).
-    const uint64_t meta_rec = 2 * kNumLods * 4 + r0.vnum * 116 + 12;  // Hausdorff values to record end
-    const uint64_t dpitch = strided ? ((8 + meta_rec + 8 + 15) & ~uint64_t(15)) : 0;
     {
         std::vector<std::thread> pool;
         for (long k = 0; k < nch; ++k)
@@ -174,8 +166,7 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
                 uint32_t v0 = (uint32_t)ch_vox[k];
                 for (long o = n * k / nch; o < n * (k + 1) / nch; ++o) {
                     const RawRec& r = recs[o];
-                    const uint64_t meta = strided ? (uint64_t)o * dpitch + 8 : r.meta;
-                    ar[o] = AttachRec{r.data_off, r.data_size, meta, (uint32_t)r.vnum, v0};
+                    ar[o] = AttachRec{r.data_off, r.data_size, r.meta, (uint32_t)r.vnum, v0};
                     H.obj_vox_off[o] = v0;
                     H.obj_data_off[o] = r.data_off;
                     H.obj_data_size[o] = r.data_size;
@@ -217,8 +208,6 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
     Buf& vobj = ctx->scratch[98];
     Buf& tmp = ctx->scratch[99];
     Buf& ctr = ctx->scratch[100];
-    Buf& rows = ctx->scratch[101];
-    if (strided) GTRY(ensure(ctx, rows, (size_t)n * dpitch + 16));
     GTRY(ensure(ctx, recs_d, (size_t)(n + 1) * sizeof(AttachRec)));
     GTRY(ensure(ctx, off4, (size_t)kNumLods * std::max<uint64_t>(nvox, 1) * sizeof(uint32_t)));
     GTRY(ensure(ctx, vobj, (size_t)std::max<uint64_t>(nvox, 1) * sizeof(uint32_t)));
@@ -246,17 +235,7 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
     GCTRY(cudaMemcpyAsync(T->obj_vox + n, nvox_src, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
     GCTRY(cudaMemsetAsync(ctr.p, 0, 8 * sizeof(unsigned long long), s));
     GCTRY(cudaMemsetAsync((unsigned long long*)ctr.p + 8, 0xff, sizeof(unsigned long long), s));
-    const uint8_t* meta_src = dev_view;
-    if (strided) {
-        const uint8_t* src0 = buf + r0.meta - 8;
-        uint8_t* dst = (uint8_t*)rows.p;
-        if (n > 1)
-            GCTRY(cudaMemcpy2DAsync(dst, dpitch, src0, stride, 8 + meta_rec + 8, n - 1, cudaMemcpyHostToDevice, s));
-        GCTRY(cudaMemcpyAsync(dst + (n - 1) * dpitch, src0 + (n - 1) * stride, 8 + meta_rec,
-                              cudaMemcpyHostToDevice, s));
-        meta_src = dst;
-    }
-    GCTRY(launch_attach_tables(meta_src, (const AttachRec*)recs_d.p, n, (long)nvox, o, tmp.p, scan_bytes,
+    GCTRY(launch_attach_tables(dev_view, (const AttachRec*)recs_d.p, n, (long)nvox, o, tmp.p, scan_bytes,
                                ctx->num_sms, s, strided, r0.data_size));
     unsigned long long res[9] = {0};
     GCTRY(cudaMemcpyAsync(res, ctr.p, 9 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
