@@ -849,7 +849,8 @@ def main():
             h1 = time.perf_counter()
             q, r, d = ctx.join(U1, U2, query="within", within=TAU, form=pkg.FORM_TUNED)
             h2 = time.perf_counter()
-            fetched = ctx.stats()["fetch_bytes"]
+            sj = ctx.stats()
+            fetched = sj["fetch_bytes"]
             i1, i2 = U1.info(), U2.info()
             h2d_b = i1["h2d_bytes"] + i2["h2d_bytes"] + int(fetched)
             U1.free(); U2.free()
@@ -860,7 +861,9 @@ def main():
                     {"tiles_ms": 1e3 * (h1 - h0), "parse_ms": i1["parse_ms"] + i2["parse_ms"],
                      "alloc_ms": i1["alloc_ms"] + i2["alloc_ms"], "meta_ms": i1["meta_ms"] + i2["meta_ms"],
                      "load_ms": i1["load_ms"] + i2["load_ms"], "join_ms": 1e3 * (h2 - h1),
-                     "fetch_bytes": fetched, "release_ms": 1e3 * (h3 - h2)})
+                     "fetch_bytes": fetched, "release_ms": 1e3 * (h3 - h2),
+                     "join_device": {k: sj[k] for k in ("total_ms", "candidates_ms", "filter_ms", "lod_ms", "refine_ms",
+                                                        "host_syncs", "lod_graph")}})
 
         e2e_ms, h2d, d2h, e2e_parts = [], 0, 0, None
         for i in range(a.e2e_steps + 1 if a.e2e_steps > 0 else 0):
