@@ -85,19 +85,24 @@ __device__ __forceinline__ void stage_chunks(uintptr_t p, uint32_t cnt, int lane
     }
 }
 
-// strided: the records were placed at the first record's stride instead of
+// sr.on: the records are placed at the first record's stride instead of
 // walked, so every object's voxel count (the 8 bytes before its Hausdorff
 // values) and the next object's data size (the 8 bytes after its transform)
 // are checked against the first object's, read with the windows they border
 __global__ void __launch_bounds__(kWarps * 32) k_parse_tables(const uint8_t* __restrict__ raw,
                                                               const AttachRec* __restrict__ recs, long n_obj,
-                                                              AttachOut o, int strided, uint64_t data_size0) {
+                                                              AttachOut o, AttachStride sr) {
+    const bool strided = sr.on != 0;
+    const uint64_t data_size0 = sr.first.data_size;
     __shared__ __align__(16) uint32_t stage[kWarps][kStageAlloc];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t* st = stage[w];
     const long nw = ((long)gridDim.x * blockDim.x) >> 5;
     for (long ob = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ob < n_obj; ob += nw) {
-        const AttachRec r = recs[ob];
+        const AttachRec r = strided ? AttachRec{sr.first.data_off + (uint64_t)ob * sr.stride, sr.first.data_size,
+                                                sr.first.meta + (uint64_t)ob * sr.stride, sr.first.vnum,
+                                                (uint32_t)ob * sr.first.vnum}
+                                    : recs[ob];
         const uintptr_t base = reinterpret_cast<uintptr_t>(raw) + r.meta;
         const uint64_t xw = kHdWords + (uint64_t)r.vnum * kVoxWords;  // first transform word
         bool bad = false;
@@ -200,7 +205,7 @@ __global__ void k_check_layout(AttachOut o, long n_vox) {
 
 cudaError_t launch_attach_tables(const uint8_t* raw_dev, const AttachRec* recs, long n_obj, long n_vox,
                                  const AttachOut& out, void* scan_tmp, size_t& scan_bytes, int num_sms,
-                                 cudaStream_t s, bool strided, uint64_t data_size0) {
+                                 cudaStream_t s, const AttachStride& st) {
     if (!scan_tmp) {  // size query for the scans
         size_t b = 0;
         const cudaError_t e =
@@ -214,7 +219,7 @@ cudaError_t launch_attach_tables(const uint8_t* raw_dev, const AttachRec* recs, 
         if (e != cudaSuccess) return e;
     }
     const int blocks = (int)std::max<long>(1, std::min<long>((n_obj + kWarps - 1) / kWarps, (long)num_sms * 16));
-    k_parse_tables<<<blocks, kWarps * 32, 0, s>>>(raw_dev, recs, n_obj, out, strided ? 1 : 0, data_size0);
+    k_parse_tables<<<blocks, kWarps * 32, 0, s>>>(raw_dev, recs, n_obj, out, st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     for (int l = 0; l < kNumLods; ++l) {  // in place: counts at [1, n_vox] become the prefix

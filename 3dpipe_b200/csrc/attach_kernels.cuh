@@ -18,6 +18,15 @@ struct AttachRec {
     uint32_t vox0;       // first voxel of the object in the tile
 };
 
+// Records placed at a fixed stride instead of walked (a tile of equal-size
+// records): object o is `first` moved o * stride bytes on, its first voxel
+// o * first.vnum.  on == 0: the records come from the uploaded array.
+struct AttachStride {
+    int on;
+    uint64_t stride;
+    AttachRec first;
+};
+
 // Where the pass writes (all device memory).
 struct AttachOut {
     float4* vox;                      // [3 n_vox] (low, 0) (high, 0) (core, 0)
@@ -36,12 +45,12 @@ struct AttachOut {
 // Parse the voxel tables of n_obj objects from raw_dev (the device view of the
 // page-locked tile bytes), scan the counts into vtri, check the layout.  Call
 // first with scan_tmp == nullptr to learn scan_bytes.
-// strided: the records were placed at the first record's stride (no walk);
-// each object's voxel count and the next object's data size are then
-// checked against the first object's (data_size0), and a difference flags
-// the object in first_bad (the caller walks the tile on the host).
+// st.on: the records are placed at the first record's stride (no walk, recs
+// unused); each object's voxel count and the next object's data size are
+// then checked against the first object's, and a difference flags the
+// object in first_bad (the caller walks the tile on the host).
 cudaError_t launch_attach_tables(const uint8_t* raw_dev, const AttachRec* recs, long n_obj, long n_vox,
                                  const AttachOut& out, void* scan_tmp, size_t& scan_bytes, int num_sms,
-                                 cudaStream_t s, bool strided = false, uint64_t data_size0 = 0);
+                                 cudaStream_t s, const AttachStride& st = AttachStride{});
 
 }  // namespace tdp

@@ -17,6 +17,7 @@ void cache_trim(tdp_ctx* ctx) {
     for (auto& kv : ctx->block_cache) cudaFree(kv.second);
     ctx->block_cache.clear();
     ctx->cached_bytes = 0;
+    ctx->small_cached = 0;
 }
 
 cudaError_t dmalloc(tdp_ctx* ctx, void** p, size_t bytes) {
@@ -37,9 +38,16 @@ cudaError_t dmalloc(tdp_ctx* ctx, void** p, size_t bytes) {
     return cudaSuccess;
 }
 
+static size_t block_class(size_t bytes) {
+    if (bytes >= kCachedBlockMin) return bytes;
+    size_t c = 256;
+    while (c < bytes) c <<= 1;
+    return c;
+}
+
 cudaError_t block_alloc(tdp_ctx* ctx, void** p, size_t bytes) {
     *p = nullptr;
-    if (bytes == 0) bytes = 16;
+    bytes = block_class(bytes == 0 ? 16 : bytes);
     auto it = ctx->block_cache.lower_bound(bytes);
     if (it != ctx->block_cache.end() && it->first <= bytes + bytes / 4) {
         if (ctx->budget && ctx->in_use + it->first > ctx->budget) return cudaErrorMemoryAllocation;
@@ -47,6 +55,7 @@ cudaError_t block_alloc(tdp_ctx* ctx, void** p, size_t bytes) {
         ctx->allocs[*p] = it->first;
         ctx->in_use += it->first;
         ctx->cached_bytes -= it->first;
+        if (it->first < kCachedBlockMin) --ctx->small_cached;
         ctx->block_cache.erase(it);
         return cudaSuccess;
     }
@@ -56,7 +65,11 @@ cudaError_t block_alloc(tdp_ctx* ctx, void** p, size_t bytes) {
 void block_release(tdp_ctx* ctx, void* p) {
     if (!p) return;
     auto it = ctx->allocs.find(p);
-    if (it == ctx->allocs.end() || it->second < kCachedBlockMin) { dfree(ctx, p); return; }
+    if (it == ctx->allocs.end() || (it->second < kCachedBlockMin && ctx->small_cached >= kSmallCached)) {
+        dfree(ctx, p);
+        return;
+    }
+    if (it->second < kCachedBlockMin) ++ctx->small_cached;
     ctx->in_use -= it->second;
     ctx->cached_bytes += it->second;
     ctx->block_cache.emplace(it->second, p);

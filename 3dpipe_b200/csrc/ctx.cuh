@@ -84,6 +84,7 @@ struct tdp_ctx {
     // budget, and on destroy.
     std::multimap<size_t, void*> block_cache;
     size_t cached_bytes = 0;
+    size_t small_cached = 0;  // cached blocks below kCachedBlockMin
     // page-locked staging of tile metadata (grow-only): two buffers taken in
     // turn, each with an event recorded after its last copy, so an attach
     // returns while its copies run and the next attach stages into the other
@@ -100,11 +101,16 @@ cudaError_t dmalloc(tdp_ctx* ctx, void** p, size_t bytes);
 void dfree(tdp_ctx* ctx, void* p);
 // grow-only scratch buffer; returns TDP_OK or an error status (recorded in ctx)
 int ensure(tdp_ctx* ctx, Buf& b, size_t bytes);
-// large blocks for tile arrays: block_alloc reuses an idle cached
-// block of the size (or up to 25 % larger); block_release caches blocks of
-// at least kCachedBlockMin bytes (the caller has synchronised the context's
-// stream, so the block is idle) and frees smaller ones
+// blocks for tile arrays: block_alloc reuses an idle cached block of the
+// size (or up to 25 % larger); block_release caches the block (the caller
+// has synchronised the context's stream, so the block is idle).  Requests
+// below kCachedBlockMin are rounded up to a power of two of at least 256
+// bytes, so a small block fits the next request of its class exactly; at
+// most kSmallCached small blocks stay cached, further ones are freed.  A
+// tile's small arrays (object and voxel offsets of a tile of a thousand
+// objects) then cost no cudaMalloc / cudaFree per attach either.
 constexpr size_t kCachedBlockMin = (size_t)1 << 20;
+constexpr size_t kSmallCached = 512;
 cudaError_t block_alloc(tdp_ctx* ctx, void** p, size_t bytes);
 void block_release(tdp_ctx* ctx, void* p);
 void cache_trim(tdp_ctx* ctx);

@@ -273,11 +273,30 @@ __device__ __forceinline__ float pre32(const float4* t, float4 o, PreTri<float>&
 }
 
 constexpr int kExWarps = 4;
+constexpr int kExQueue = 64;  // queued triangle pairs per warp (>= 32 + 31)
+
+// FP32 distance with its error bound, and the FP64 distance when the pair can
+// still be the minimum (d32 - e <= lim), of triangle pair (a, b) of an item
+__device__ __forceinline__ double exact_pair(const float4* ta, const float4* tb, float4 o4, float lim) {
+    PreTri<float> A32, B32;
+    const float rA = pre32(ta, o4, A32);
+    const float rB = pre32(tb, o4, B32);
+    const float d32 = sqrtf(tri_dist2(A32, B32));
+    if (d32 - err_bound(fmaxf(rA, rB)) > lim) return 1e300;
+    PreTri<double> A, B;
+    const double ox = o4.x, oy = o4.y, oz = o4.z;
+    pre64(ta, ox, oy, oz, A);
+    pre64(tb, ox, oy, oz, B);
+    return tri_dist2(A, B);
+}
 
 // FP64 minimum over the triangle pairs of a selected voxel pair whose FP32
 // bounding-sphere gap is <= the item's reach and whose FP32 distance, less its
-// error bound, is <= the item's limit; one warp per item, lane j owns B
-// triangle j of the current chunk of 32, A spheres staged per chunk.
+// error bound, is <= the item's limit; one warp per item.  Lane j owns B
+// triangle j of the current chunk of 32 and tests it against the A chunk's
+// spheres (staged in shared memory); the pairs that pass are queued, and
+// every 32 queued pairs are evaluated one per lane, so the evaluations run
+// with the whole warp instead of with the few lanes whose test passed.
 __global__ void __launch_bounds__(kExWarps * 32) k_exact_f64(const float4* __restrict__ triA,
                                                              const float4* __restrict__ triB,
                                                              const RefineItem* __restrict__ sel,
@@ -286,53 +305,61 @@ __global__ void __launch_bounds__(kExWarps * 32) k_exact_f64(const float4* __res
                                                              const unsigned* __restrict__ n_sel,
                                                              unsigned long long* __restrict__ pexact_bits) {
     __shared__ float4 sphA[kExWarps][32];
+    __shared__ uint2 queue[kExWarps][kExQueue];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
     const unsigned n = *n_sel;
+    uint2* q = queue[w];
     for (unsigned it = blockIdx.x * kExWarps + w; it < n; it += gridDim.x * kExWarps) {
         const RefineItem r = sel[it];
         const float2 tl = sel_thr[it];
         const float thr = tl.x, lim = tl.y;
         const float4 o4 = triA[(size_t)r.a_off * kTriF4];
-        const double ox = o4.x, oy = o4.y, oz = o4.z;
+        const float4* tA = triA + (size_t)r.a_off * kTriF4;
+        const float4* tB = triB + (size_t)r.b_off * kTriF4;
         double best = 1e300;
+        int qn = 0;
+        // evaluate the first `take` queued pairs, one per lane, and move the
+        // rest to the front
+        auto drain = [&](int take) {
+            __syncwarp();
+            if (lane < take) {
+                const uint2 e = q[lane];
+                const double d2 = exact_pair(tA + (size_t)e.x * kTriF4, tB + (size_t)e.y * kTriF4, o4, lim);
+                best = d2 < best ? d2 : best;
+            }
+            const uint2 moved = lane + take < qn ? q[lane + take] : make_uint2(0u, 0u);
+            __syncwarp();
+            if (lane + take < qn) q[lane] = moved;
+            qn -= take;
+            __syncwarp();
+        };
         for (uint32_t b0 = 0; b0 < r.b_cnt; b0 += 32) {
             const bool bv = b0 + lane < r.b_cnt;
-            const float4* tb = triB + ((size_t)r.b_off + b0 + lane) * kTriF4;
-            float bx = 0.f, by = 0.f, bz = 0.f, br = 0.f, rB = 0.f;
-            PreTri<float> B32;
-            if (bv) {
-                sphere_rel(tb, o4, bx, by, bz, br);
-                rB = pre32(tb, o4, B32);
-            }
+            float bx = 0.f, by = 0.f, bz = 0.f, br = 0.f;
+            if (bv) sphere_rel(tB + (size_t)(b0 + lane) * kTriF4, o4, bx, by, bz, br);
             for (uint32_t a0 = 0; a0 < r.a_cnt; a0 += 32) {
                 const int ca = (int)min(32u, r.a_cnt - a0);
                 __syncwarp();
                 if (lane < ca) {
                     float cx, cy, cz, rr;
-                    sphere_rel(triA + ((size_t)r.a_off + a0 + lane) * kTriF4, o4, cx, cy, cz, rr);
+                    sphere_rel(tA + (size_t)(a0 + lane) * kTriF4, o4, cx, cy, cz, rr);
                     sphA[w][lane] = make_float4(cx, cy, cz, rr);
                 }
                 __syncwarp();
                 for (int i = 0; i < ca; ++i) {
-                    const float4 s = sphA[w][i];
-                    const float dx = s.x - bx, dy = s.y - by, dz = s.z - bz;
-                    const float reach = s.w + br + thr;
-                    if (bv && dx * dx + dy * dy + dz * dz <= reach * reach) {
-                        const float4* ta = triA + ((size_t)r.a_off + a0 + i) * kTriF4;
-                        PreTri<float> A32;
-                        const float rA = pre32(ta, o4, A32);
-                        const float d32 = sqrtf(tri_dist2(A32, B32));
-                        if (!(d32 - err_bound(fmaxf(rA, rB)) > lim)) {  // it can be the minimum
-                            PreTri<double> A, B;
-                            pre64(ta, ox, oy, oz, A);
-                            pre64(tb, ox, oy, oz, B);
-                            const double d2 = tri_dist2(A, B);
-                            best = d2 < best ? d2 : best;
-                        }
-                    }
+                    const float4 sa = sphA[w][i];
+                    const float dx = sa.x - bx, dy = sa.y - by, dz = sa.z - bz;
+                    const float reach = sa.w + br + thr;
+                    const bool keep = bv && dx * dx + dy * dy + dz * dz <= reach * reach;
+                    const unsigned m = __ballot_sync(0xffffffffu, keep);
+                    if (keep) q[qn + __popc(m & lt)] = make_uint2(a0 + (uint32_t)i, b0 + (uint32_t)lane);
+                    qn += __popc(m);
+                    if (qn >= 32) drain(32);
                 }
             }
         }
+        if (qn > 0) drain(qn);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const double v = __shfl_xor_sync(0xffffffffu, best, o);
@@ -415,7 +442,7 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     int64_t E = 0;
     CU(cudaMemcpyAsync(&E, off + d.P, 8, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
-    info.launches += 6;
+    info.launches += 6 + (lz1.on || lz2.on ? 1 : 0);
     info.items = (long)E;
     if (E >= (1LL << 31)) return fail(ctx, TDP_ERR_ARG, "too many voxel pairs for the exact-distance stage");
     const size_t Ez = (size_t)std::max<int64_t>(E, 1);
@@ -463,7 +490,7 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
         k_exact_err<<<grid(d.P, 256, ctx->num_sms * 8), 256, 0, s>>>(d, best32, pexact, ctr + 8);
         CU(cudaGetLastError());
         CU(cudaEventRecord(ctx->xev[4], s));
-        info.launches += 6;
+        info.launches += 6 + (lz1.on || lz2.on ? 1 : 0);
         unsigned ns[12] = {0};
         CU(cudaMemcpyAsync(ns, ctr + 4, 48, cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));

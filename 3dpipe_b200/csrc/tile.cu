@@ -22,6 +22,7 @@
 #include "attach_kernels.cuh"
 #include "ctx.cuh"
 #include "storage/dev_tile.h"
+#include "storage/host_pool.h"
 #include "tile_kernels.cuh"
 
 namespace tdp {
@@ -59,14 +60,10 @@ cudaError_t launch_unpack(const uint8_t* raw, const UnpackSeg* segs, int nseg, f
     return cudaGetLastError();
 }
 
-// fn(b, e) over [0, n) in a few host threads (one for small n)
+// fn(b, e) over [0, n) on the host pool's threads (one range for small n)
 template <typename Fn>
 static void host_parallel(long n, Fn fn) {
-    const long nt = std::max(1L, std::min<long>((long)std::thread::hardware_concurrency(), n / 4096));
-    if (nt == 1) { fn(0L, n); return; }
-    std::vector<std::thread> pool;
-    for (long k = 0; k < nt; ++k) pool.emplace_back([&, k] { fn(n * k / nt, n * (k + 1) / nt); });
-    for (auto& th : pool) th.join();
+    host_ranges(n, 4096, fn);
 }
 
 // Device arrays go back to the context's block cache: every caller has
@@ -112,31 +109,22 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
     uint64_t stride = 0;
     const bool strided = max_objects <= 0 && raw_first_record(buf, len, r0, stride) && (len - 1) % stride == 0 &&
                          (len - 1) / stride >= 1024;
-    if (strided) {
-        const long ns = (long)((len - 1) / stride);
-        recs.resize((size_t)ns);
-        RawRec* rp = recs.data();
-        host_parallel(ns, [&](long b, long e) {
-            for (long o = b; o < e; ++o)
-                rp[o] = RawRec{r0.data_off + o * stride, r0.data_size, r0.meta + o * stride, r0.vnum};
-        });
-    } else if (!walk_raw_dt(buf, len, max_objects, recs) || recs.empty()) {
+    if (!strided && (!walk_raw_dt(buf, len, max_objects, recs) || recs.empty())) {
         tile_release(ctx, T);
         return kUseHostParse;
     }
-    const long n = (long)recs.size();
+    const long n = strided ? (long)((len - 1) / stride) : (long)recs.size();
     // voxel counts per chunk of objects, in parallel, then their prefix
-    const long nch = std::max(1L, std::min<long>((long)std::thread::hardware_concurrency(), n / 4096));
+    const long nch = std::max(1L, std::min<long>((long)host_threads(), n / 4096));
     std::vector<uint64_t> ch_vox(nch + 1, 0);
-    {
-        std::vector<std::thread> pool;
-        for (long k = 0; k < nch; ++k)
-            pool.emplace_back([&, k] {
-                uint64_t sv = 0;
-                for (long o = n * k / nch; o < n * (k + 1) / nch; ++o) sv += recs[o].vnum;
-                ch_vox[k + 1] = sv;
-            });
-        for (auto& th : pool) th.join();
+    if (strided) {
+        for (long k = 0; k < nch; ++k) ch_vox[k + 1] = (uint64_t)(n * (k + 1) / nch) * r0.vnum;
+    } else {
+        host_for(nch, [&](long k) {
+            uint64_t sv = 0;
+            for (long o = n * k / nch; o < n * (k + 1) / nch; ++o) sv += recs[o].vnum;
+            ch_vox[k + 1] = sv;
+        });
         for (long k = 0; k < nch; ++k) ch_vox[k + 1] += ch_vox[k];
     }
     const uint64_t nvox = ch_vox[nch];
@@ -152,29 +140,27 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
     H.obj_data_off.resize(n);
     H.obj_data_size.resize(n);
     // the object records go up through the staging slot, obj_vox[n] after them
-    grow_stage((size_t)(n + 1) * sizeof(AttachRec) + 64);
+    grow_stage(std::max((size_t)(n + 1) * sizeof(AttachRec), (size_t)9 * n * sizeof(float)) + 64);
     AttachRec* ar = (AttachRec*)ctx->hstage[slot];
     std::vector<AttachRec> ar_pageable;
     if (!ar) {
         ar_pageable.resize(n + 1);
         ar = ar_pageable.data();
     }
-    {
-        std::vector<std::thread> pool;
-        for (long k = 0; k < nch; ++k)
-            pool.emplace_back([&, k] {
-                uint32_t v0 = (uint32_t)ch_vox[k];
-                for (long o = n * k / nch; o < n * (k + 1) / nch; ++o) {
-                    const RawRec& r = recs[o];
-                    ar[o] = AttachRec{r.data_off, r.data_size, r.meta, (uint32_t)r.vnum, v0};
-                    H.obj_vox_off[o] = v0;
-                    H.obj_data_off[o] = r.data_off;
-                    H.obj_data_size[o] = r.data_size;
-                    v0 += (uint32_t)r.vnum;
-                }
-            });
-        for (auto& th : pool) th.join();
-    }
+    // strided: the GPU places the records itself (k_parse_tables), so only
+    // the host's copies of the object arrays are written here
+    host_for(nch, [&](long k) {
+        uint32_t v0 = (uint32_t)ch_vox[k];
+        for (long o = n * k / nch; o < n * (k + 1) / nch; ++o) {
+            const RawRec r = strided ? RawRec{r0.data_off + o * stride, r0.data_size, r0.meta + o * stride, r0.vnum}
+                                     : recs[o];
+            if (!strided) ar[o] = AttachRec{r.data_off, r.data_size, r.meta, (uint32_t)r.vnum, v0};
+            H.obj_vox_off[o] = v0;
+            H.obj_data_off[o] = r.data_off;
+            H.obj_data_size[o] = r.data_size;
+            v0 += (uint32_t)r.vnum;
+        }
+    });
     const uint32_t v0 = (uint32_t)nvox;
     H.obj_vox_off[n] = v0;
     uint32_t* nvox_src = reinterpret_cast<uint32_t*>(ar + n);
@@ -231,22 +217,39 @@ static int attach_on_gpu(tdp_ctx* ctx, tdp_tile* T, const uint8_t* buf, const ui
     GTRY(ensure(ctx, tmp, scan_bytes + 16));
     T->alloc_ms = ms_since(ta);
     const auto tm = std::chrono::steady_clock::now();
-    GCTRY(cudaMemcpyAsync(recs_d.p, ar, (size_t)n * sizeof(AttachRec), cudaMemcpyHostToDevice, s));
+    if (!strided) GCTRY(cudaMemcpyAsync(recs_d.p, ar, (size_t)n * sizeof(AttachRec), cudaMemcpyHostToDevice, s));
     GCTRY(cudaMemcpyAsync(T->obj_vox + n, nvox_src, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
     GCTRY(cudaMemsetAsync(ctr.p, 0, 8 * sizeof(unsigned long long), s));
     GCTRY(cudaMemsetAsync((unsigned long long*)ctr.p + 8, 0xff, sizeof(unsigned long long), s));
+    AttachStride ast{};
+    if (strided) ast = AttachStride{1, stride, AttachRec{r0.data_off, r0.data_size, r0.meta, (uint32_t)r0.vnum, 0u}};
     GCTRY(launch_attach_tables(dev_view, (const AttachRec*)recs_d.p, n, (long)nvox, o, tmp.p, scan_bytes,
-                               ctx->num_sms, s, strided, r0.data_size));
+                               ctx->num_sms, s, ast));
     unsigned long long res[9] = {0};
     GCTRY(cudaMemcpyAsync(res, ctr.p, 9 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    // the object boxes and transforms come back through the staging slot (its
+    // records have gone up by then, in stream order) and are spread into the
+    // host arrays after the synchronisation
     H.obj_box.resize((size_t)6 * n);
     H.obj_xf.resize((size_t)3 * n);
-    GCTRY(cudaMemcpyAsync(H.obj_box.data(), T->d_boxes, (size_t)6 * n * sizeof(float), cudaMemcpyDeviceToHost, s));
-    GCTRY(cudaMemcpyAsync(H.obj_xf.data(), T->d_boxes + 6 * n, (size_t)3 * n * sizeof(float),
-                          cudaMemcpyDeviceToHost, s));
+    float* box_stage = ar_pageable.empty() ? reinterpret_cast<float*>(ctx->hstage[slot]) : nullptr;
+    GCTRY(cudaMemcpyAsync(box_stage ? box_stage : H.obj_box.data(), T->d_boxes,
+                          (size_t)(box_stage ? 9 : 6) * n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    if (!box_stage)
+        GCTRY(cudaMemcpyAsync(H.obj_xf.data(), T->d_boxes + 6 * n, (size_t)3 * n * sizeof(float),
+                              cudaMemcpyDeviceToHost, s));
     if (!ctx->hstage_ev[slot]) GCTRY(cudaEventCreateWithFlags(&ctx->hstage_ev[slot], cudaEventDisableTiming));
     GCTRY(cudaEventRecord(ctx->hstage_ev[slot], s));
     GCTRY(cudaStreamSynchronize(s));
+    if (box_stage)
+        host_ranges(9 * n, 1 << 16, [&](long b, long e) {
+            const long m = std::min(e, 6 * n);
+            if (b < m) std::memcpy(H.obj_box.data() + b, box_stage + b, (size_t)(m - b) * sizeof(float));
+            if (e > 6 * n) {
+                const long xb = std::max(b, 6 * n);
+                std::memcpy(H.obj_xf.data() + (xb - 6 * n), box_stage + xb, (size_t)(e - xb) * sizeof(float));
+            }
+        });
     if (res[8] != ~0ull) {  // a check failed: the host parser reports it
         tile_release(ctx, T);
         return kUseHostParse;

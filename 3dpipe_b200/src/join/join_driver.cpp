@@ -404,6 +404,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
             refine_items += W;
             if (W > 0) {
                 CU(launch_fetch_items(items, nullptr, W, li, lz1, lz2, ctx->num_sms, s));
+                if (lz1.on || lz2.on) launches += 2;
                 CU(cudaEventRecord(ctx->ev[2], s));
                 CU(launch_refine_plain(t1->tri[li], t2->tri[li], items, W, res, s));
                 CU(cudaEventRecord(ctx->ev[3], s));
@@ -467,8 +468,10 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         {   // per LOD: items, refine, apply, pair update (with the within decision),
             // the kNN rank; on attached tiles the fetch and the next LOD's prefetch
             const bool attached = L.lz1.on || L.lz2.on;
-            launches += (4 + (L.any_knn ? 1 : 0) + (attached ? 1 : 0)) * L.nl +
-                        (attached && L.side ? L.nl - 1 : 0) + (L.recheck ? (knn ? 6 : 5) : 0);
+            // (a fetch or a prefetch is a mark launch and a copy launch)
+            launches += (4 + (L.any_knn ? 1 : 0) + (attached ? 2 : 0)) * L.nl +
+                        (attached && L.side ? 2 * (L.nl - 1) : 0) +
+                        (L.recheck ? (knn ? 5 : 4) + (attached ? 2 : 0) : 0);
         }
         st.refine_launches += L.nl;
     }

@@ -1,5 +1,6 @@
 // dt_format.cpp -- bounds-checked parser of the RAW tile format (see dt_format.h).
 #include "storage/dt_format.h"
+#include "storage/host_pool.h"
 
 #include <algorithm>
 #include <array>
@@ -307,7 +308,7 @@ bool walk_raw_dt(const uint8_t* buf, size_t len, long max_objects, HostVec<RawRe
     if (max_objects <= 0) {
         size_t p1 = 1;
         Rec r0;
-        const long hw = (long)std::thread::hardware_concurrency();
+        const long hw = (long)host_threads();
         if (walk_one(buf, len, p1, r0)) {
             const uint64_t stride = p1 - 1;
             const long n_est = (long)((len - 1) / stride);
@@ -318,17 +319,14 @@ bool walk_raw_dt(const uint8_t* buf, size_t len, long max_objects, HostVec<RawRe
                 std::vector<long> got(nt, 0);
                 std::vector<size_t> end(nt, 0);
                 std::vector<char> clean(nt, 0);
-                std::vector<std::thread> pool;
-                for (long k = 0; k < nt; ++k)
-                    pool.emplace_back([&, k] {
-                        size_t q = 1 + (size_t)(k * per) * stride;
-                        if (q >= len) return;
-                        long c = 0;
-                        clean[k] = walk_chain(buf, len, q, per, &recs[(size_t)(k * per)], c);
-                        got[k] = c;
-                        end[k] = q;
-                    });
-                for (auto& th : pool) th.join();
+                host_for(nt, [&](long k) {
+                    size_t q = 1 + (size_t)(k * per) * stride;
+                    if (q >= len) return;
+                    long c = 0;
+                    clean[k] = walk_chain(buf, len, q, per, &recs[(size_t)(k * per)], c);
+                    got[k] = c;
+                    end[k] = q;
+                });
                 long kept = 0;
                 for (long k = 0; k < nt; ++k) {
                     if (!clean[k] || 1 + (size_t)(k * per) * stride != pos) break;
@@ -390,8 +388,7 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
     }
     // chunks of whole objects with about equal voxel counts (a vessel tile
     // has few objects of many voxels each)
-    const int nt = (int)std::max<long>(
-        1, std::min<long>({(long)std::thread::hardware_concurrency(), (long)(nvox / 2048), n}));
+    const int nt = (int)std::max<long>(1, std::min<long>({(long)host_threads(), (long)(nvox / 2048), n}));
     std::vector<long> first(nt + 1, n);
     for (int k = 0; k < nt; ++k)
         first[k] = std::lower_bound(T.obj_vox_off.begin(), T.obj_vox_off.begin() + n, (uint32_t)(nvox * k / nt)) -
@@ -471,13 +468,7 @@ int parse_raw_dt(const uint8_t* buf, size_t len, long max_objects, TileHost& T, 
         }
         store_fence();
     };
-    if (nt == 1) {
-        work(0);
-    } else {
-        std::vector<std::thread> pool;
-        for (int k = 0; k < nt; ++k) pool.emplace_back(work, k);
-        for (auto& th : pool) th.join();
-    }
+    host_for(nt, [&](long k) { work((int)k); });
     for (int k = 0; k < nt; ++k)
         if (bad[k] >= 0) {  // chunks are in object order: the first failing chunk holds the lowest object
             err = msg[k];
@@ -523,18 +514,7 @@ void vtri_prefix(const TileHost& T, uint32_t* const out[kNumLods], uint32_t* con
             }
         }
     };
-    const long nt = std::min<long>(tasks, std::max<long>(1, (long)std::thread::hardware_concurrency()));
-    if (nt <= 1) {
-        for (long t = 0; t < tasks; ++t) run(t);
-        return;
-    }
-    std::atomic<long> next{0};
-    std::vector<std::thread> pool;
-    for (long i = 0; i < nt; ++i)
-        pool.emplace_back([&] {
-            for (long t = next++; t < tasks; t = next++) run(t);
-        });
-    for (auto& th : pool) th.join();
+    host_for(tasks, [&](long t) { run(t); });
 }
 
 }  // namespace tdp
