@@ -17,12 +17,14 @@
 //   3. the tuned FP32 refine, its minimum preset to U plus the candidate's
 //      largest possible FP32 error, gives each candidate that has a triangle
 //      pair below that preset its minimum d32 (error e = err_bound(R)) and
-//      skips the rest after a few cluster tests; per object pair best32 =
+//      skips the rest after a few cluster tests (sphere and cylinder bounds);
+//      per object pair best32 =
 //      min d32 and E = max e;
 //   4. a candidate can hold the minimum only if d32 - E <= best32 + E (its
 //      true minimum is >= d32 - e, and D <= best32 + E): those are evaluated
 //      again triangle pair by triangle pair, skipping pairs whose (inflated)
-//      bounding-sphere gap exceeds best32 + 2E; a pair's FP32 distance d32'
+//      bounding-sphere gap or cylinder bound exceeds best32 + 2E; a pair's
+//      FP32 distance d32'
 //      with its error e' comes first, and only a pair with d32' - e' <=
 //      best32 + E (one that can be the minimum) is evaluated in FP64;
 //   5. D = the smallest FP64 distance over the evaluated candidates.
@@ -50,6 +52,12 @@ constexpr int kBlk = 256;
 // 28.4 M); the two with the smallest box gaps instead gave a looser U (29.6 M
 // candidates, 15 % more FP32 work); so one is refined.
 constexpr int kExK = 1;
+
+// The FP32 passes run the lazy refine with the cylinder bound in its culls
+// (configuration 16): a reported pair's closest points face each other across
+// a gap of up to tau, where the sphere gap keeps every triangle pair whose
+// centres are offset sideways by less than about sqrt(2 gap (r1 + r2)).
+constexpr int kExactRefineCfg = 16;
 
 // U of every reported pair: min core-to-core distance over its voxel pairs,
 // and pmx when it is a proven bound (pmx_valid); item1[kExK p + k] = the voxel
@@ -253,6 +261,17 @@ __device__ __forceinline__ void sphere_rel(const float4* t, float4 o, float& cx,
     r = sqrtf(r2) * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f;
 }
 
+// extent of a triangle's projection on the unit axis u, relative to o,
+// widened like the refine's staged bounds
+__device__ __forceinline__ float2 proj_rel(const float4* t, float4 o, float3 u) {
+    const float4 a = t[0], b = t[1], c = t[2];
+    const float p0 = (a.x - o.x) * u.x + (a.y - o.y) * u.y + (a.z - o.z) * u.z;
+    const float p1 = (b.x - o.x) * u.x + (b.y - o.y) * u.y + (b.z - o.z) * u.z;
+    const float p2 = (c.x - o.x) * u.x + (c.y - o.y) * u.y + (c.z - o.z) * u.z;
+    const float mg = 1e-5f * (fabsf(p0) + fabsf(p1) + fabsf(p2)) + 1e-6f;
+    return make_float2(fminf(p0, fminf(p1, p2)) - mg, fmaxf(p0, fmaxf(p1, p2)) + mg);
+}
+
 __device__ __forceinline__ void pre64(const float4* t, double ox, double oy, double oz, PreTri<double>& P) {
     const float4 a = t[0], b = t[1], c = t[2];
     pretri(P, v3<double>(a.x - ox, a.y - oy, a.z - oz), v3<double>(b.x - ox, b.y - oy, b.z - oz),
@@ -291,7 +310,9 @@ __device__ __forceinline__ double exact_pair(const float4* ta, const float4* tb,
 }
 
 // FP64 minimum over the triangle pairs of a selected voxel pair whose FP32
-// bounding-sphere gap is <= the item's reach and whose FP32 distance, less its
+// bounding-sphere gap and cylinder bound (cyl_keep, along the axis from the
+// item's first A vertex to its first B vertex) are <= the item's reach and
+// whose FP32 distance, less its
 // error bound, is <= the item's limit; one warp per item.  Lane j owns B
 // triangle j of the current chunk of 32 and tests it against the A chunk's
 // spheres (staged in shared memory); the pairs that pass are queued, and
@@ -305,6 +326,7 @@ __global__ void __launch_bounds__(kExWarps * 32) k_exact_f64(const float4* __res
                                                              const unsigned* __restrict__ n_sel,
                                                              unsigned long long* __restrict__ pexact_bits) {
     __shared__ float4 sphA[kExWarps][32];
+    __shared__ float2 prjA[kExWarps][32];
     __shared__ uint2 queue[kExWarps][kExQueue];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -317,6 +339,15 @@ __global__ void __launch_bounds__(kExWarps * 32) k_exact_f64(const float4* __res
         const float4 o4 = triA[(size_t)r.a_off * kTriF4];
         const float4* tA = triA + (size_t)r.a_off * kTriF4;
         const float4* tB = triB + (size_t)r.b_off * kTriF4;
+        // the item's axis: from the first A vertex to the first B vertex
+        float3 u;
+        {
+            const float4 q = tB[0];
+            const float ux = q.x - o4.x, uy = q.y - o4.y, uz = q.z - o4.z;
+            const float n2 = ux * ux + uy * uy + uz * uz;
+            const float inv = n2 > 0.f ? rsqrtf(n2) : 0.f;
+            u = make_float3(ux * inv, uy * inv, uz * inv);
+        }
         double best = 1e300;
         int qn = 0;
         // evaluate the first `take` queued pairs, one per lane, and move the
@@ -337,7 +368,11 @@ __global__ void __launch_bounds__(kExWarps * 32) k_exact_f64(const float4* __res
         for (uint32_t b0 = 0; b0 < r.b_cnt; b0 += 32) {
             const bool bv = b0 + lane < r.b_cnt;
             float bx = 0.f, by = 0.f, bz = 0.f, br = 0.f;
-            if (bv) sphere_rel(tB + (size_t)(b0 + lane) * kTriF4, o4, bx, by, bz, br);
+            float2 pb = make_float2(0.f, 0.f);
+            if (bv) {
+                sphere_rel(tB + (size_t)(b0 + lane) * kTriF4, o4, bx, by, bz, br);
+                pb = proj_rel(tB + (size_t)(b0 + lane) * kTriF4, o4, u);
+            }
             for (uint32_t a0 = 0; a0 < r.a_cnt; a0 += 32) {
                 const int ca = (int)min(32u, r.a_cnt - a0);
                 __syncwarp();
@@ -345,13 +380,16 @@ __global__ void __launch_bounds__(kExWarps * 32) k_exact_f64(const float4* __res
                     float cx, cy, cz, rr;
                     sphere_rel(tA + (size_t)(a0 + lane) * kTriF4, o4, cx, cy, cz, rr);
                     sphA[w][lane] = make_float4(cx, cy, cz, rr);
+                    prjA[w][lane] = proj_rel(tA + (size_t)(a0 + lane) * kTriF4, o4, u);
                 }
                 __syncwarp();
                 for (int i = 0; i < ca; ++i) {
                     const float4 sa = sphA[w][i];
+                    const float2 pa = prjA[w][i];
                     const float dx = sa.x - bx, dy = sa.y - by, dz = sa.z - bz;
                     const float reach = sa.w + br + thr;
-                    const bool keep = bv && dx * dx + dy * dy + dz * dz <= reach * reach;
+                    const bool keep = bv && dx * dx + dy * dy + dz * dz <= reach * reach &&
+                                      cyl_keep(dx, dy, dz, sa.w + br, fmaxf(pb.x - pa.y, pa.x - pb.y), u, thr);
                     const unsigned m = __ballot_sync(0xffffffffu, keep);
                     if (keep) q[qn + __popc(m & lt)] = make_uint2(a0 + (uint32_t)i, b0 + (uint32_t)lane);
                     qn += __popc(m);
@@ -429,7 +467,7 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     if (n1 >= (1LL << 31)) return fail(ctx, TDP_ERR_ARG, "too many object pairs for the exact-distance stage");
     CU(launch_fetch_items(item1, nullptr, n1, kNumLods - 1, lz1, lz2, ctx->num_sms, s));
     CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], item1, (int)n1, res1, ctr, nullptr,
-                           ctx->num_sms, ctx->lod_cfg[kNumLods - 1] >= 0 ? ctx->lod_cfg[kNumLods - 1] : ctx->tuned_cfg, s));
+                           ctx->num_sms, kExactRefineCfg, s));
     k_exact_tighten<<<grid(d.P, 256, ctx->num_sms * 8), 256, 0, s>>>(res1, d.P, Ub);
     CU(cudaGetLastError());
     CU(cudaEventRecord(ctx->xev[1], s));
@@ -476,7 +514,7 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     if (E > 0) {
         CU(launch_fetch_items(items, nullptr, E, kNumLods - 1, lz1, lz2, ctx->num_sms, s));
         CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], items, (int)E, res, ctr, n_full,
-                               ctx->num_sms, ctx->lod_cfg[kNumLods - 1] >= 0 ? ctx->lod_cfg[kNumLods - 1] : ctx->tuned_cfg, s, nullptr, preset));
+                               ctx->num_sms, kExactRefineCfg, s, nullptr, preset));
         const int eg = grid(E, 256, ctx->num_sms * 16);
         k_exact_best<<<eg, 256, 0, s>>>(res, item_pair, E, best32, emax);
         CU(cudaGetLastError());

@@ -289,7 +289,6 @@ __device__ __forceinline__ float warp_min_nonneg(float v) {
     return __uint_as_float(__reduce_min_sync(0xffffffffu, __float_as_uint(v)));
 }
 
-__device__ __forceinline__ float approx_len(float d2) { return d2 * rsqrtf(fmaxf(d2, 1e-30f)); }
 
 template <int WARPS, int CA, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const float4* __restrict__ triA,
@@ -648,7 +647,12 @@ __device__ __forceinline__ void lazy_pre(const float4* __restrict__ t, float4 o,
 // round, reading the B lane's sphere and bounds from shared memory -- instead
 // of every lane stepping through the 8 members while most of them need none.
 // The same pairs are queued (in another order), so the minima are the same.
-template <int WARPS, int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false, bool SPREAD = false>
+// CYL: every cluster and member test also takes the cylinder bound
+// (cyl_keep) along the item's axis u, which drops the pairs of two surfaces
+// facing each other whose centres are offset sideways; the bound holds for
+// every pair of points, so the minima are again the same.
+template <int WARPS, int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false, bool SPREAD = false,
+          bool CYL = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const float4* __restrict__ triA,
                                                                     const float4* __restrict__ triB,
                                                                     const RefineItem* __restrict__ items,
@@ -856,7 +860,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                                     const float thr = fmaxf(bd, fmaxf(bl + a.x + ab.x, bh - a.y - ab.y));
                                     const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
                                     const float reach = s.w + sb.w + thr;
-                                    need = ab.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach;
+                                    need = ab.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach &&
+                                           (!CYL || cyl_keep(dx, dy, dz, s.w + sb.w, ab.z - a.z, u, thr));
                                 }
                                 cm = __ballot_sync(0xffffffffu, need);
                                 t0 = 0;
@@ -879,7 +884,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                                     const float thr = fmaxf(bd, fmaxf(bl + a.x + abq.x, bh - a.y - abq.y));
                                     const float dx = s.x - sbq.x, dy = s.y - sbq.y, dz = s.z - sbq.z;
                                     const float reach = s.w + sbq.w + thr;
-                                    keep = abq.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach;
+                                    keep = abq.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach &&
+                                           (!CYL || cyl_keep(dx, dy, dz, s.w + sbq.w, abq.z - a.z, u, thr));
                                 }
                             }
                             const unsigned m = __ballot_sync(0xffffffffu, keep);
@@ -900,7 +906,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                                 const float thr = fmaxf(bd, fmaxf(bl + a.x + ab.x, bh - a.y - ab.y));
                                 const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
                                 const float reach = s.w + sb.w + thr;
-                                kc = ab.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach;
+                                kc = ab.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach &&
+                                     (!CYL || cyl_keep(dx, dy, dz, s.w + sb.w, ab.z - a.z, u, thr));
                             }
                             if (!__any_sync(0xffffffffu, kc)) {
                                 i += kCl;
@@ -913,7 +920,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                             const float thr = fmaxf(bd, fmaxf(bl + a.x + ab.x, bh - a.y - ab.y));
                             const float dx = s.x - sb.x, dy = s.y - sb.y, dz = s.z - sb.z;
                             const float reach = s.w + sb.w + thr;
-                            keep = ab.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach;
+                            keep = ab.z - a.z < thr && dx * dx + dy * dy + dz * dz < reach * reach &&
+                                   (!CYL || cyl_keep(dx, dy, dz, s.w + sb.w, ab.z - a.z, u, thr));
                         }
                         const unsigned m = __ballot_sync(0xffffffffu, keep);
                         if (keep) queue[qn + __popc(m & lt_mask)] = (unsigned short)((i << 8) | lane);
@@ -1014,10 +1022,11 @@ struct TunedCfgDef {
 // kernel with one lane per queued pair (both halves in the lane); 10-11: the
 // lazy kernel, two lanes and one lane per pair, queuing 8 seeds first;
 // 12-13: the lazy kernel staging its raw records by 1-D bulk copies (TMA);
-// 14-15: the lazy kernel with 8 seeds first and the spread cull
+// 14-15: the lazy kernel with 8 seeds first and the spread cull; 16-17: 14-15
+// with the cylinder bound in every cull test
 constexpr TunedCfgDef kTunedCfgs[kTunedConfigs] = {{64, 3}, {48, 3}, {32, 4}, {128, 3}, {128, 4}, {64, 4},
                                                     {128, 5}, {128, 6}, {128, 4}, {128, 5}, {128, 5}, {128, 5},
-                                                    {128, 4}, {64, 5}, {128, 5}, {128, 4}};
+                                                    {128, 4}, {64, 5}, {128, 5}, {128, 4}, {128, 5}, {128, 4}};
 
 TunedConfig tuned_config(int cfg) {
     if (cfg < 0 || cfg >= kTunedConfigs) cfg = 0;
@@ -1049,13 +1058,14 @@ static cudaError_t launch_tuned_cfg(const float4* triA, const float4* triB, cons
     return cudaGetLastError();
 }
 
-template <int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false, bool SPREAD = false>
+template <int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false, bool SPREAD = false,
+          bool CYL = false>
 static cudaError_t launch_lazy_cfg(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                    float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
                                    cudaStream_t s, const unsigned* n_items_dev, const float* init_bd) {
     const size_t smem = (size_t)kTunedWarps *
                         (TMA ? LazyLayout<CA>::kWarpFloatsTma : LazyLayout<CA>::kWarpFloats) * sizeof(float);
-    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB, ONE, SEEDS, TMA, SPREAD>;
+    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB, ONE, SEEDS, TMA, SPREAD, CYL>;
     if (smem > 48 * 1024) {
         static bool attr_set[64] = {};  // per device
         int dev = 0;
@@ -1097,6 +1107,8 @@ cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const Re
         case 13: return launch_lazy_cfg<64, 5, false, 32, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 14: return launch_lazy_cfg<128, 5, false, 8, false, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 15: return launch_lazy_cfg<128, 4, false, 8, false, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 16: return launch_lazy_cfg<128, 5, false, 8, false, true, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
+        case 17: return launch_lazy_cfg<128, 4, false, 8, false, true, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         default: return launch_tuned_cfg<64, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
     }
 }

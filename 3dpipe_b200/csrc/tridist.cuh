@@ -220,4 +220,26 @@ __host__ __device__ __forceinline__ R tri_dist2_half(const PreTri<R>& X, const P
     return best;
 }
 
+#ifdef __CUDACC__
+__device__ __forceinline__ float approx_len(float d2) { return d2 * rsqrtf(fmaxf(d2, 1e-30f)); }
+
+// Cylinder bound of two triangles (or clusters) with centres d = cA - cB
+// apart, radii summing to rsum, and projections on the item's unit axis u
+// at least slab apart (<= 0 when they overlap): every pair of their points
+// is at least max(slab, 0) apart along u and |d across u| - rsum across it,
+// so the pair is kept only when the two together are below thr.  Where the
+// surfaces face each other along u this is far tighter than the sphere gap
+// |d| - rsum, which spends both radii in the direction of d.  The radii and
+// projections carry the staging's inflation, so FP32 rounding never drops a
+// pair that could be the minimum.
+__device__ __forceinline__ bool cyl_keep(float dx, float dy, float dz, float rsum, float slab, float3 u,
+                                         float thr) {
+    const float du = dx * u.x + dy * u.y + dz * u.z;
+    const float px = dx - du * u.x, py = dy - du * u.y, pz = dz - du * u.z;
+    const float lat = fmaxf(approx_len(px * px + py * py + pz * pz) - rsum, 0.f);
+    const float sl = fmaxf(slab, 0.f);
+    return sl * sl + lat * lat < thr * thr;
+}
+#endif
+
 }  // namespace tdp

@@ -110,7 +110,9 @@ int tdp_fp32_peak(tdp_ctx *ctx, double *tflops);
  * 8-9 do the same with one lane per evaluated pair; 10-11 are 6 and 9 queuing
  * only the 8 most promising first pairs before the cull; 12-13 stage each
  * chunk's triangle records in shared memory by a 1-D bulk copy (TMA); 14-15
- * spread each needed cluster's member tests over the warp).  All return identical results;
+ * spread each needed cluster's member tests over the warp; 16-17 are 14-15
+ * with a cylinder bound -- gap along the item's axis, centre distance across
+ * it less both radii -- in every cull test).  All return identical results;
  * they differ only in speed, which depends on the voxel sizes of the join.
  * A context starts with configuration 0.  The reference has one fixed launch
  * shape (one CTA of 512 threads per voxel pair,
