@@ -284,6 +284,17 @@ __device__ __forceinline__ float4 quick_sphere(const float4* __restrict__ t, flo
     return make_float4(cx, cy, cz, sqrtf(r2) * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f);
 }
 
+// the triangle's extreme projection on u relative to o (the smallest for far,
+// else the largest), widened as lazy_bounds widens it
+__device__ __forceinline__ float quick_proj(const float4* __restrict__ t, float4 o, float3 u, bool far) {
+    const float4 t0 = t[0], t1 = t[1], t2 = t[2];
+    const float p0 = (t0.x - o.x) * u.x + (t0.y - o.y) * u.y + (t0.z - o.z) * u.z;
+    const float p1 = (t1.x - o.x) * u.x + (t1.y - o.y) * u.y + (t1.z - o.z) * u.z;
+    const float p2 = (t2.x - o.x) * u.x + (t2.y - o.y) * u.y + (t2.z - o.z) * u.z;
+    const float mg = 1e-5f * (fabsf(p0) + fabsf(p1) + fabsf(p2)) + 1e-6f;
+    return far ? fminf(p0, fminf(p1, p2)) - mg : fmaxf(p0, fmaxf(p1, p2)) + mg;
+}
+
 // the three minima are >= 0, so their bit patterns order like unsigned ints
 __device__ __forceinline__ float warp_min_nonneg(float v) {
     return __uint_as_float(__reduce_min_sync(0xffffffffu, __float_as_uint(v)));
@@ -725,20 +736,27 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                 const int ncl = (ca + kCl - 1) / kCl;
                 __syncwarp();
                 for (int k = lane; k < ca; k += 32) {
-                    sphA[k] = quick_sphere(triA + ((size_t)w.a_off + a0 + k) * kTriF4, o4);
-                    auxA[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    const float4* t = triA + ((size_t)w.a_off + a0 + k) * kTriF4;
+                    sphA[k] = quick_sphere(t, o4);
+                    auxA[k] = make_float4(0.f, 0.f, CYL ? quick_proj(t, o4, u, false) : 0.f, 0.f);
                 }
                 __syncwarp();
                 build_clusters<CA>(sphA, auxA, ca, clS, clA, lane);
                 __syncwarp();
                 for (uint32_t b0 = 0; b0 < w.b_cnt && !need; b0 += kCB) {
                     if (b0 + lane >= w.b_cnt) break;
-                    const float4 sb = quick_sphere(triB + ((size_t)w.b_off + b0 + lane) * kTriF4, o4);
+                    const float4* t = triB + ((size_t)w.b_off + b0 + lane) * kTriF4;
+                    const float4 sb = quick_sphere(t, o4);
+                    const float pb = CYL ? quick_proj(t, o4, u, true) : 0.f;
                     for (int c = 0; c < ncl; ++c) {
                         const float4 cs = clS[c];
                         const float dx = cs.x - sb.x, dy = cs.y - sb.y, dz = cs.z - sb.z;
                         const float reach = cs.w + sb.w + bd;
-                        if (dx * dx + dy * dy + dz * dz < reach * reach) { need = true; break; }
+                        if (dx * dx + dy * dy + dz * dz < reach * reach &&
+                            (!CYL || cyl_keep(dx, dy, dz, cs.w + sb.w, pb - clA[c].z, u, bd))) {
+                            need = true;
+                            break;
+                        }
                     }
                 }
             }
