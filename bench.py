@@ -964,8 +964,8 @@ def main():
             "gpu_launches": int(launches_t),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
-                         "traffic_source": "DRAM read+write bytes per launch, ncu 1-pass capture of this workload "
-                                           "(profiles/refine_within400.md)",
+                         "traffic_source": "DRAM read+write bytes per launch: ncu capture of the 20k-nuclei case, "
+                                           "scaled by the refined voxel pairs (profiles/refine_within400.md)",
                          "kernel": "refine_lazy_kernel" if cfg_by_lod[100] >= 3 else "refine_tuned_kernel",
                          "peak_source": "measured FP32 FMA probe (tdp_fp32_peak); MEASURED_PEAKS.json has no CUDA-core FP32 figure",
                          "work": f"full evals x {F_TRI:.0f} + culled pairs x {F_CULL:.0f} FLOPs",
