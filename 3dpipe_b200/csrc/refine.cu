@@ -743,21 +743,62 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                 __syncwarp();
                 build_clusters<CA>(sphA, auxA, ca, clS, clA, lane);
                 __syncwarp();
-                for (uint32_t b0 = 0; b0 < w.b_cnt && !need; b0 += kCB) {
-                    if (b0 + lane >= w.b_cnt) break;
-                    const float4* t = triB + ((size_t)w.b_off + b0 + lane) * kTriF4;
-                    const float4 sb = quick_sphere(t, o4);
-                    const float pb = CYL ? quick_proj(t, o4, u, true) : 0.f;
-                    for (int c = 0; c < ncl; ++c) {
-                        const float4 cs = clS[c];
-                        const float dx = cs.x - sb.x, dy = cs.y - sb.y, dz = cs.z - sb.z;
-                        const float reach = cs.w + sb.w + bd;
-                        if (dx * dx + dy * dy + dz * dz < reach * reach &&
-                            (!CYL || cyl_keep(dx, dy, dz, cs.w + sb.w, pb - clA[c].z, u, bd))) {
-                            need = true;
-                            break;
+                // the chunk's own bound first: a sphere around its cluster
+                // spheres and their largest projection on u (inflated like
+                // the cluster spheres), so that a B triangle far from the
+                // whole chunk costs one test instead of one per cluster
+                float4 vs;
+                float vz;
+                {
+                    const bool v = lane < ncl;
+                    const float4 cs = v ? clS[lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    float lx = v ? cs.x : FLT_MAX, hx = v ? cs.x : -FLT_MAX;
+                    float ly = v ? cs.y : FLT_MAX, hy = v ? cs.y : -FLT_MAX;
+                    float lz = v ? cs.z : FLT_MAX, hz = v ? cs.z : -FLT_MAX;
+                    vz = v ? clA[lane].z : -FLT_MAX;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
+                        hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, o));
+                        ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, o));
+                        hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, o));
+                        lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, o));
+                        hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, o));
+                        vz = fmaxf(vz, __shfl_xor_sync(0xffffffffu, vz, o));
+                    }
+                    const float cx = 0.5f * (lx + hx), cy = 0.5f * (ly + hy), cz = 0.5f * (lz + hz);
+                    float r = 0.f;
+                    if (v) {
+                        const float dx = cs.x - cx, dy = cs.y - cy, dz = cs.z - cz;
+                        r = sqrtf(dx * dx + dy * dy + dz * dz) + cs.w;
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) r = fmaxf(r, __shfl_xor_sync(0xffffffffu, r, o));
+                    vs = make_float4(cx, cy, cz, r * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f);
+                }
+                // every lane tests its B triangle; the warp stops at the
+                // first chunk of B where any lane needs a cluster
+                for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += kCB) {
+                    if (b0 + lane < w.b_cnt) {
+                        const float4* t = triB + ((size_t)w.b_off + b0 + lane) * kTriF4;
+                        const float4 sb = quick_sphere(t, o4);
+                        const float pb = CYL ? quick_proj(t, o4, u, true) : 0.f;
+                        const float vx = vs.x - sb.x, vy = vs.y - sb.y, vw = vs.z - sb.z;
+                        const float vr = vs.w + sb.w + bd;
+                        const bool near = vx * vx + vy * vy + vw * vw < vr * vr &&
+                                          (!CYL || cyl_keep(vx, vy, vw, vs.w + sb.w, pb - vz, u, bd));
+                        for (int c = 0; near && c < ncl; ++c) {
+                            const float4 cs = clS[c];
+                            const float dx = cs.x - sb.x, dy = cs.y - sb.y, dz = cs.z - sb.z;
+                            const float reach = cs.w + sb.w + bd;
+                            if (dx * dx + dy * dy + dz * dz < reach * reach &&
+                                (!CYL || cyl_keep(dx, dy, dz, cs.w + sb.w, pb - clA[c].z, u, bd))) {
+                                need = true;
+                                break;
+                            }
                         }
                     }
+                    if (__any_sync(0xffffffffu, need)) break;
                 }
             }
             if (!__any_sync(0xffffffffu, need)) {
