@@ -217,6 +217,8 @@ int tdp_last_stats(const tdp_ctx* ctx, tdp_stats* o) {
     o->exact_full_evals = s.exact_full_evals;
     o->candidates_on_device = s.candidates_on_device;
     o->candidate_redone = s.candidate_redone;
+    o->exact_dropped_items = s.exact_dropped_items;
+    o->exact_below_items = s.exact_below_items;
     return TDP_OK;
 }
 

@@ -44,6 +44,8 @@ struct LastStats {
     unsigned long long exact_full_evals = 0;   // exact stage: triangle pairs fully evaluated in FP32
     long candidates_on_device = 0;   // 1: object candidates came from the GPU (the tuned form)
     long candidate_redone = 0;       // kNN queries redone with the global ring-search buffer
+    long exact_dropped_items = 0;    // exact stage: FP32-pass items dropped by the item-level test
+    long exact_below_items = 0;      // exact stage: FP32-pass items below their preset
 };
 
 }  // namespace tdp

@@ -216,14 +216,31 @@ __global__ void __launch_bounds__(kBlk) k_exact_vp(JoinDev d, const float* __res
 
 // per object pair: best32 = min d32, emax = max error bound (non-negative
 // floats order like their bit patterns)
+// counts[0]: items the refine's item-level test dropped (rmax 0, nothing
+// staged); counts[1]: items with a triangle pair below their preset
 __global__ void k_exact_best(const float4* __restrict__ res, const int* __restrict__ item_pair, int64_t E,
-                             unsigned* __restrict__ best32, unsigned* __restrict__ emax) {
+                             unsigned* __restrict__ best32, unsigned* __restrict__ emax,
+                             unsigned* __restrict__ counts) {
+    unsigned dropped = 0, below = 0;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
         const float4 r = res[e];
-        if (!(r.x < FLT_MAX)) continue;  // no triangle pair below the preset
+        if (!(r.x < FLT_MAX)) {  // no triangle pair below the preset
+            dropped += r.w == 0.f;
+            continue;
+        }
+        ++below;
         const int p = item_pair[e];
         atomicMin(best32 + p, __float_as_uint(fmaxf(r.x, 0.f)));
         atomicMax(emax + p, __float_as_uint(err_bound(r.w)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        dropped += __shfl_xor_sync(0xffffffffu, dropped, o);
+        below += __shfl_xor_sync(0xffffffffu, below, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (dropped) atomicAdd(counts, dropped);
+        if (below) atomicAdd(counts + 1, below);
     }
 }
 
@@ -509,14 +526,15 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     CU(cudaMemsetAsync(emax, 0, Pz * 4, s));
     CU(cudaMemsetAsync(ctr, 0, 64, s));
     CU(cudaEventRecord(ctx->xev[2], s));
-    // ctr: [0] work counter, [4] selected items, [8] FP32 error bits, [12..13] full evaluations (u64)
+    // ctr: [0] work counter, [4] selected items, [8] FP32 error bits, [12..13] full evaluations (u64),
+    // [14] items the item-level test dropped, [15] items below their preset
     unsigned long long* n_full = reinterpret_cast<unsigned long long*>(ctr + 12);
     if (E > 0) {
         CU(launch_fetch_items(items, nullptr, E, kNumLods - 1, lz1, lz2, ctx->num_sms, s));
         CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], items, (int)E, res, ctr, n_full,
                                ctx->num_sms, kExactRefineCfg, s, nullptr, preset));
         const int eg = grid(E, 256, ctx->num_sms * 16);
-        k_exact_best<<<eg, 256, 0, s>>>(res, item_pair, E, best32, emax);
+        k_exact_best<<<eg, 256, 0, s>>>(res, item_pair, E, best32, emax, ctr + 14);
         CU(cudaGetLastError());
         k_exact_select<<<eg, 256, 0, s>>>(res, items, item_pair, E, best32, emax, sel, sel_pair, sel_thr, ctr + 4);
         CU(cudaGetLastError());
@@ -537,6 +555,8 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
         std::memcpy(&e32, &ns[4], 4);
         info.max_rel_err32 = e32;
         std::memcpy(&info.full_evals, &ns[8], 8);
+        info.dropped_items = ns[10];
+        info.below_items = ns[11];
         float ms[4] = {0, 0, 0, 0};
         for (int k = 0; k < 4; ++k) cudaEventElapsedTime(&ms[k], ctx->xev[k], ctx->xev[k + 1]);
         for (int k = 0; k < 4; ++k) info.phase_ms[k] = ms[k];

@@ -16,6 +16,8 @@ struct ExactInfo {
     double max_rel_err32 = 0;  // max |FP32 object minimum - FP64 distance| / max(distance, 1)
     double phase_ms[4] = {0, 0, 0, 0};  // upper bounds, candidates, FP32 pass, FP64 pass (device time)
     unsigned long long full_evals = 0;  // triangle pairs the FP32 pass evaluated fully
+    long dropped_items = 0;  // FP32 pass items dropped by the refine's item-level test
+    long below_items = 0;    // FP32 pass items with a triangle pair below their preset
 };
 
 // For every object pair with pstat == kReported: the exact minimum triangle

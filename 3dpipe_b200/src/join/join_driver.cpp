@@ -603,6 +603,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         st.fp32_max_rel_err = xi.max_rel_err32;
         for (int k = 0; k < 4; ++k) st.exact_phase_ms[k] = xi.phase_ms[k];
         st.exact_full_evals = xi.full_evals;
+        st.exact_dropped_items = xi.dropped_items;
+        st.exact_below_items = xi.below_items;
     }
     ctx->stats = st;
     *out = R;

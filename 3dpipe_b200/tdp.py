@@ -46,7 +46,8 @@ class Stats(C.Structure):
                 ("fp32_max_rel_err", C.c_double), ("fetch_bytes", C.c_double), ("lod_graph", C.c_long),
                 ("refine_ms_lod", C.c_double * 5), ("exact_phase_ms", C.c_double * 4),
                 ("exact_full_evals", C.c_ulonglong), ("candidates_on_device", C.c_long),
-                ("candidate_redone", C.c_long)]
+                ("candidate_redone", C.c_long), ("exact_dropped_items", C.c_long),
+                ("exact_below_items", C.c_long)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}

@@ -832,6 +832,8 @@ def main():
                                           st_x["exact_phase_ms"])),
                      "voxel_pairs_fp32": st_x["exact_items"], "voxel_pairs_fp64": st_x["exact_f64_items"],
                      "fp32_full_evals": st_x["exact_full_evals"], "fp32_max_rel_err": st_x["fp32_max_rel_err"],
+                     "fp32_items_dropped": st_x["exact_dropped_items"],
+                     "fp32_items_below_preset": st_x["exact_below_items"],
                      "steps": a.exact_steps, "note": "median of the timed joins; resident tiles"}
 
         # end to end through the C ABI from the page-locked host tile bytes:

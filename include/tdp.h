@@ -97,6 +97,11 @@ typedef struct {
     long candidate_redone;           /* kNN queries whose ring search outgrew a
                                         warp's shared-memory buffer and were
                                         redone on the GPU with a global one    */
+    long exact_dropped_items;        /* exact stage: FP32-pass voxel pairs
+                                        dropped by the refine's item-level
+                                        bound test (no triangle staged)        */
+    long exact_below_items;          /* exact stage: FP32-pass voxel pairs with
+                                        a triangle pair below their preset     */
 } tdp_stats;
 int tdp_last_stats(const tdp_ctx *ctx, tdp_stats *out);
 /* measured FP32 FMA throughput of the context's device in TFLOP/s (CUDA cores,
