@@ -310,11 +310,6 @@ __device__ __forceinline__ float pre32(const float4* t, float4 o, PreTri<float>&
 
 constexpr int kExWarps = 4;
 constexpr int kExQueue = 64;  // queued triangle pairs per warp (>= 32 + 31)
-// At least 3 blocks (12 warps) per SM, which holds the kernel to 168
-// registers per thread: left alone it took 255 for its FP64 path and ran 7
-// warps per SM.  At 3 it spills 116 bytes (at 4, 128 registers, 488 bytes),
-// in the FP64 path, which only a pair inside the error band takes.
-constexpr int kExBlocksPerSm = 3;
 
 // FP32 distance with its error bound, and the FP64 distance when the pair can
 // still be the minimum (d32 - e <= lim), of triangle pair (a, b) of an item
@@ -340,7 +335,7 @@ __device__ __forceinline__ double exact_pair(const float4* ta, const float4* tb,
 // spheres (staged in shared memory); the pairs that pass are queued, and
 // every 32 queued pairs are evaluated one per lane, so the evaluations run
 // with the whole warp instead of with the few lanes whose test passed.
-__global__ void __launch_bounds__(kExWarps * 32, kExBlocksPerSm) k_exact_f64(const float4* __restrict__ triA,
+__global__ void __launch_bounds__(kExWarps * 32) k_exact_f64(const float4* __restrict__ triA,
                                                              const float4* __restrict__ triB,
                                                              const RefineItem* __restrict__ sel,
                                                              const int* __restrict__ sel_pair,

@@ -776,65 +776,26 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                     for (int o = 16; o > 0; o >>= 1) r = fmaxf(r, __shfl_xor_sync(0xffffffffu, r, o));
                     vs = make_float4(cx, cy, cz, r * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f);
                 }
-                // every lane stages its B triangle; each 8 lanes form a B
-                // cluster (built like the A clusters), the warp tests every
-                // (A cluster, B cluster) pair -- lane 8 g + j takes A
-                // clusters j, j + 8 against its own group g -- and a lane
-                // then tests its triangle only against the A clusters that
-                // passed with its group.  The warp stops at the first chunk
-                // of B where any lane needs a cluster.
+                // every lane tests its B triangle; the warp stops at the
+                // first chunk of B where any lane needs a cluster
                 for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += kCB) {
-                    const bool bval = b0 + lane < w.b_cnt;
-                    float4 sb = make_float4(0.f, 0.f, 0.f, 0.f);
-                    float pb = FLT_MAX;
-                    if (bval) {
+                    if (b0 + lane < w.b_cnt) {
                         const float4* t = triB + ((size_t)w.b_off + b0 + lane) * kTriF4;
-                        sb = quick_sphere(t, o4);
-                        if (CYL) pb = quick_proj(t, o4, u, true);
-                    }
-                    const float lx = grp8_min(bval ? sb.x : FLT_MAX), hx = grp8_max(bval ? sb.x : -FLT_MAX);
-                    const float ly = grp8_min(bval ? sb.y : FLT_MAX), hy = grp8_max(bval ? sb.y : -FLT_MAX);
-                    const float lz = grp8_min(bval ? sb.z : FLT_MAX), hz = grp8_max(bval ? sb.z : -FLT_MAX);
-                    const bool gval = lx <= hx;  // the group holds a triangle
-                    const float gx = 0.5f * (lx + hx), gy = 0.5f * (ly + hy), gz = 0.5f * (lz + hz);
-                    float gr = 0.f;
-                    if (bval) {
-                        const float dx = sb.x - gx, dy = sb.y - gy, dz = sb.z - gz;
-                        gr = sqrtf(dx * dx + dy * dy + dz * dz) + sb.w;
-                    }
-                    gr = grp8_max(gr) * 1.0001f + 1e-5f * (fabsf(gx) + fabsf(gy) + fabsf(gz)) + 1e-6f;
-                    const float gp = CYL ? grp8_min(pb) : 0.f;
-                    unsigned mask = 0;
-                    for (int r = 0; r * kCl < ncl; ++r) {
-                        const int c = r * kCl + (lane & (kCl - 1));
-                        bool hit = false;
-                        if (gval && c < ncl) {
-                            const float4 cs = clS[c];
-                            const float dx = cs.x - gx, dy = cs.y - gy, dz = cs.z - gz;
-                            const float reach = cs.w + gr + bd;
-                            hit = dx * dx + dy * dy + dz * dz < reach * reach &&
-                                  (!CYL || cyl_keep(dx, dy, dz, cs.w + gr, gp - clA[c].z, u, bd));
-                        }
-                        const unsigned bal = __ballot_sync(0xffffffffu, hit);
-                        mask |= ((bal >> (lane & ~(kCl - 1))) & 0xffu) << (kCl * r);
-                    }
-                    if (bval) {
+                        const float4 sb = quick_sphere(t, o4);
+                        const float pb = CYL ? quick_proj(t, o4, u, true) : 0.f;
                         const float vx = vs.x - sb.x, vy = vs.y - sb.y, vw = vs.z - sb.z;
                         const float vr = vs.w + sb.w + bd;
-                        if (!(vx * vx + vy * vy + vw * vw < vr * vr &&
-                              (!CYL || cyl_keep(vx, vy, vw, vs.w + sb.w, pb - vz, u, bd))))
-                            mask = 0;
-                    }
-                    while (bval && mask) {
-                        const int c = __ffs(mask) - 1;
-                        mask &= mask - 1;
-                        const float4 cs = clS[c];
-                        const float dx = cs.x - sb.x, dy = cs.y - sb.y, dz = cs.z - sb.z;
-                        const float reach = cs.w + sb.w + bd;
-                        if (dx * dx + dy * dy + dz * dz < reach * reach &&
-                            (!CYL || cyl_keep(dx, dy, dz, cs.w + sb.w, pb - clA[c].z, u, bd))) {
-                            need = true;
-                            break;
+                        const bool near = vx * vx + vy * vy + vw * vw < vr * vr &&
+                                          (!CYL || cyl_keep(vx, vy, vw, vs.w + sb.w, pb - vz, u, bd));
+                        for (int c = 0; near && c < ncl; ++c) {
+                            const float4 cs = clS[c];
+                            const float dx = cs.x - sb.x, dy = cs.y - sb.y, dz = cs.z - sb.z;
+                            const float reach = cs.w + sb.w + bd;
+                            if (dx * dx + dy * dy + dz * dz < reach * reach &&
+                                (!CYL || cyl_keep(dx, dy, dz, cs.w + sb.w, pb - clA[c].z, u, bd))) {
+                                need = true;
+                                break;
+                            }
                         }
                     }
                     if (__any_sync(0xffffffffu, need)) break;
