@@ -42,6 +42,25 @@ template <typename R> __host__ __device__ __forceinline__ V3<R> cross(V3<R> a, V
 template <typename R> __host__ __device__ __forceinline__ R clamp01(R v) { return v < R(0) ? R(0) : (v > R(1) ? R(1) : v); }
 template <typename R> __host__ __device__ __forceinline__ R fminf_t(R a, R b) { return b < a ? b : a; }
 
+// 1/x.  In FP32 on the device: the hardware's approximate reciprocal
+// (rcp.approx.ftz, within an ulp or so) instead of the correctly rounded
+// division sequence, which is several dependent instructions on the
+// critical path of every evaluation.  Where it scales a parameter (t, s, u
+// of a closest point) the point stays on its segment, and the distance at an
+// interior minimum moves only to second order; where it scales a squared
+// plane distance it adds about an ulp, inside the error bound the join's
+// decisions carry.  FP64 and host code divide.
+template <typename R> __host__ __device__ __forceinline__ R recip(R x) {
+#ifdef __CUDA_ARCH__
+    if constexpr (sizeof(R) == 4) {
+        float r;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+        return r;
+    }
+#endif
+    return R(1) / x;
+}
+
 // A triangle with everything the pair test needs that depends on it alone.
 template <typename R> struct PreTri {
     V3<R> v[3];    // vertices (already translated to the pair's local origin)
@@ -59,12 +78,12 @@ __host__ __device__ __forceinline__ void pretri(PreTri<R>& t, V3<R> a, V3<R> b, 
     t.e[0] = b - a; t.e[1] = c - b; t.e[2] = a - c;
     t.n = cross(t.e[0], t.e[1]);
     R nn = dot(t.n, t.n);
-    t.inn = nn > R(0) ? R(1) / nn : R(0);
+    t.inn = nn > R(0) ? recip(nn) : R(0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         R ee = dot(t.e[k], t.e[k]);
         t.ee[k] = ee;
-        t.iee[k] = ee > R(0) ? R(1) / ee : R(0);
+        t.iee[k] = ee > R(0) ? recip(ee) : R(0);
         t.m[k] = cross(t.n, t.e[k]);
     }
 }
@@ -126,7 +145,7 @@ __host__ __device__ __forceinline__ R edge_pair_interior2(V3<R> a, V3<R> e, R ee
                                            v3<double>(b.x, b.y, b.z), v3<double>(f.x, f.y, f.z));
         return r2 < 3.0e38 ? R(r2) : R(3.0e38);
     }
-    R id = R(1) / den;
+    R id = recip(den);
     R s = (ef * fg - ff * eg) * id;
     R u = (ee * fg - ef * eg) * id;
     if (!(s > R(0) && s < R(1) && u > R(0) && u < R(1))) return R(3.0e38);
