@@ -275,7 +275,7 @@ __device__ __forceinline__ void sphere_rel(const float4* t, float4 o, float& cx,
     r2 = fmaxf(r2, (x1 - cx) * (x1 - cx) + (y1 - cy) * (y1 - cy) + (z1 - cz) * (z1 - cz));
     r2 = fmaxf(r2, (x2 - cx) * (x2 - cx) + (y2 - cy) * (y2 - cy) + (z2 - cz) * (z2 - cz));
     // inflated so FP32 rounding never drops a pair that could be the minimum
-    r = sqrtf(r2) * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f;
+    r = radius_sqrt(r2) * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f;
 }
 
 // extent of a triangle's projection on the unit axis u, relative to o,

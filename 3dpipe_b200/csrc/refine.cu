@@ -197,7 +197,7 @@ __device__ __forceinline__ void tri_sphere(const PreTri<float>& t, float3& c, fl
         r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
     }
     // inflate so FP32 rounding of the centre/radius can never cull a needed pair
-    r = sqrtf(r2) * 1.0001f + 1e-6f;
+    r = radius_sqrt(r2) * 1.0001f + 1e-6f;
 }
 
 // Stage triangle record `idx`: its PreTri fields into column k of a structure
@@ -256,7 +256,7 @@ __device__ __forceinline__ void build_clusters(const float4* sph, const float4* 
         float reach = 0.f;
         if (v) {
             const float dx = c.x - cx, dy = c.y - cy, dz = c.z - cz;
-            reach = sqrtf(dx * dx + dy * dy + dz * dz) + c.w;
+            reach = radius_sqrt(dx * dx + dy * dy + dz * dz) + c.w;
         }
         reach = grp8_max(reach);
         const float phx = grp8_max(v ? a.x : 0.f);
@@ -281,7 +281,7 @@ __device__ __forceinline__ float4 quick_sphere(const float4* __restrict__ t, flo
     float r2 = (x0 - cx) * (x0 - cx) + (y0 - cy) * (y0 - cy) + (z0 - cz) * (z0 - cz);
     r2 = fmaxf(r2, (x1 - cx) * (x1 - cx) + (y1 - cy) * (y1 - cy) + (z1 - cz) * (z1 - cz));
     r2 = fmaxf(r2, (x2 - cx) * (x2 - cx) + (y2 - cy) * (y2 - cy) + (z2 - cz) * (z2 - cz));
-    return make_float4(cx, cy, cz, sqrtf(r2) * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f);
+    return make_float4(cx, cy, cz, radius_sqrt(r2) * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f);
 }
 
 // the triangle's extreme projection on u relative to o (the smallest for far,
@@ -630,7 +630,7 @@ __device__ __forceinline__ void lazy_bounds(const float4* __restrict__ tri, size
     const float p1 = v[1].x * u.x + v[1].y * u.y + v[1].z * u.z;
     const float p2 = v[2].x * u.x + v[2].y * u.y + v[2].z * u.z;
     const float mg = 1e-5f * (fabsf(p0) + fabsf(p1) + fabsf(p2)) + 1e-6f;
-    sph = make_float4(c.x, c.y, c.z, sqrtf(r2) * 1.0001f + 1e-6f);
+    sph = make_float4(c.x, c.y, c.z, radius_sqrt(r2) * 1.0001f + 1e-6f);
     aux = make_float4(t0.w, t1.w, far ? fminf(p0, fminf(p1, p2)) - mg : fmaxf(p0, fmaxf(p1, p2)) + mg, 0.f);
 }
 
@@ -770,7 +770,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                     float r = 0.f;
                     if (v) {
                         const float dx = cs.x - cx, dy = cs.y - cy, dz = cs.z - cz;
-                        r = sqrtf(dx * dx + dy * dy + dz * dz) + cs.w;
+                        r = radius_sqrt(dx * dx + dy * dy + dz * dz) + cs.w;
                     }
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) r = fmaxf(r, __shfl_xor_sync(0xffffffffu, r, o));

@@ -242,6 +242,14 @@ __host__ __device__ __forceinline__ R tri_dist2_half(const PreTri<R>& X, const P
 #ifdef __CUDACC__
 __device__ __forceinline__ float approx_len(float d2) { return d2 * rsqrtf(fmaxf(d2, 1e-30f)); }
 
+// Square root of a bounding radius: the hardware's approximation (within an
+// ulp or so); every radius it feeds is then inflated by 1e-4 of itself.
+__device__ __forceinline__ float radius_sqrt(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Cylinder bound of two triangles (or clusters) with centres d = cA - cB
 // apart, radii summing to rsum, and projections on the item's unit axis u
 // at least slab apart (<= 0 when they overlap): every pair of their points
