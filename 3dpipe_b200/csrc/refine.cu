@@ -19,7 +19,6 @@
 //                        cluster- then triangle-level lower bounds against the
 //                        warp's running minima skip pairs that cannot lower any
 //                        of the three minima (details above the kernel).
-#include <type_traits>
 #include <float.h>
 #include "common.cuh"
 #include "tridist.cuh"
@@ -564,7 +563,7 @@ struct LazyLayout {
     static constexpr int kOffSphB = kOffAuxB + 4 * kCB;    // B spheres (spread cull)
     static constexpr int kOffSeedB = kOffSphB + 4 * kCB;   // each lane's queued seed, -1 for none
     static constexpr int kOffQueue = kOffSeedB + kCB;
-    static constexpr int kWarpFloats = kOffQueue + kQueue;  // 32-bit entries (CARRY)
+    static constexpr int kWarpFloats = kOffQueue + kQueue / 2;
     static_assert(kWarpFloats % 4 == 0 && kOffSphB % 4 == 0, "float4 arrays must stay 16-byte aligned");
     // bulk-copy staging (TMA configurations): the raw 48-byte records of the
     // A chunk and of the B chunk, and the warp's mbarrier
@@ -659,19 +658,12 @@ __device__ __forceinline__ void lazy_pre(const float4* __restrict__ t, float4 o,
 // round, reading the B lane's sphere and bounds from shared memory -- instead
 // of every lane stepping through the 8 members while most of them need none.
 // The same pairs are queued (in another order), so the minima are the same.
-// CARRY (two-lane drain, no TMA): a chunk of B that ends with fewer than a
-// full round of queued pairs leaves them queued for the next chunk's pairs
-// instead of draining them with most lanes idle; the queue then holds each
-// pair's B triangle as its index in the item and the drain reads that
-// triangle's (proxy, Hausdorff) from its record.  The same pairs are
-// evaluated (in another order, against thresholds tightened later), so the
-// minima are the same.
 // CYL: every cluster and member test also takes the cylinder bound
 // (cyl_keep) along the item's axis u, which drops the pairs of two surfaces
 // facing each other whose centres are offset sideways; the bound holds for
 // every pair of points, so the minima are again the same.
 template <int WARPS, int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false, bool SPREAD = false,
-          bool CYL = false, bool CARRY = false>
+          bool CYL = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const float4* __restrict__ triA,
                                                                     const float4* __restrict__ triB,
                                                                     const RefineItem* __restrict__ items,
@@ -703,9 +695,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
     float4* auxB = reinterpret_cast<float4*>(ws + L::kOffAuxB);
     float4* sphB = reinterpret_cast<float4*>(ws + L::kOffSphB);
     int* seedB = reinterpret_cast<int*>(ws + L::kOffSeedB);
-    static_assert(!(CARRY && (ONE || TMA)), "CARRY is for the two-lane drain reading global records");
-    using QE = typename std::conditional<CARRY, unsigned, unsigned short>::type;
-    QE* queue = reinterpret_cast<QE*>(ws + L::kOffQueue);
+    unsigned short* queue = reinterpret_cast<unsigned short*>(ws + L::kOffQueue);
     const unsigned lt_mask = (1u << lane) - 1u;
     unsigned long long full_evals = 0;
 
@@ -839,20 +829,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
             for (int k = lane; k < ca; k += 32) lazy_bounds(tA, k, o4, u, false, rmax, sphA[k], auxA[k]);
             __syncwarp();
             build_clusters<CA>(sphA, auxA, ca, clS, clA, lane);
-            // CARRY: queued pairs may wait for the next B chunk; entries then
-            // hold the B triangle's index in the item (16 bits), so an item
-            // of more B triangles drains per chunk as without it
-            const bool carry = CARRY && w.b_cnt <= 65536u;
-            const float4* tBi = triB + (size_t)w.b_off * kTriF4;
-            int qcarry = 0;
             for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += kCB) {
                 const int cb = min((uint32_t)kCB, w.b_cnt - b0);
                 const float4* tB = triB + ((size_t)w.b_off + b0) * kTriF4;
-                const int qn0 = qcarry;
-                auto qenc = [&](int ia, int ib) -> QE {
-                    return CARRY ? (QE)(((unsigned)ia << 16) | (unsigned)(carry ? (int)b0 + ib : ib))
-                                 : (QE)((ia << 8) | ib);
-                };
                 __syncwarp();
                 if (TMA) {
                     if (lane == 0) {
@@ -867,7 +846,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                     }
                     tB = rawB;
                 }
-                const float4* tQ = carry ? tBi : tB;  // what the queue's B indices count from
                 const bool bval = lane < cb;
                 float4 sb = make_float4(0.f, 0.f, 0.f, 0.f), ab = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (bval) {
@@ -918,8 +896,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                 }
                 if (!sq) seed = -1;
                 const unsigned sqm = __ballot_sync(0xffffffffu, sq);
-                int qn = qn0 + __popc(sqm);
-                if (sq) queue[qn0 + __popc(sqm & lt_mask)] = qenc(seed, lane);
+                int qn = __popc(sqm);
+                if (sq) queue[__popc(sqm & lt_mask)] = (unsigned short)((seed << 8) | lane);
                 bool flush = true;
                 int i = 0;
                 bool kc = false;
@@ -970,7 +948,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                                 }
                             }
                             const unsigned m = __ballot_sync(0xffffffffu, keep);
-                            if (keep) queue[qn + __popc(m & lt_mask)] = qenc(mi, src);
+                            if (keep) queue[qn + __popc(m & lt_mask)] = (unsigned short)((mi << 8) | src);
                             qn += __popc(m);
                             t0 += 32;
                             if (t0 >= nt) {
@@ -1005,7 +983,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                                    (!CYL || cyl_keep(dx, dy, dz, s.w + sb.w, ab.z - a.z, u, thr));
                         }
                         const unsigned m = __ballot_sync(0xffffffffu, keep);
-                        if (keep) queue[qn + __popc(m & lt_mask)] = qenc(i, lane);
+                        if (keep) queue[qn + __popc(m & lt_mask)] = (unsigned short)((i << 8) | lane);
                         qn += __popc(m);
                         ++i;
                     }
@@ -1021,28 +999,23 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                     int qi = 0, qj = 0;
                     if (pl < take) {
                         const unsigned e = queue[pl];
-                        qi = CARRY ? e >> 16 : e >> 8;
-                        qj = CARRY ? e & 0xffffu : e & 0xffu;
+                        qi = e >> 8;
+                        qj = e & 0xff;
                         PreTri<float> X, Y;
                         if (ONE) {
                             lazy_pre(tA + (size_t)qi * kTriF4, o4, X);
                             lazy_pre(tB + (size_t)qj * kTriF4, o4, Y);
                             d2 = fminf(tri_dist2_half(X, Y, 0), tri_dist2_half(Y, X, 1));
                         } else {
-                            lazy_pre(part ? tQ + (size_t)qj * kTriF4 : tA + (size_t)qi * kTriF4, o4, X);
-                            lazy_pre(part ? tA + (size_t)qi * kTriF4 : tQ + (size_t)qj * kTriF4, o4, Y);
+                            lazy_pre(part ? tB + (size_t)qj * kTriF4 : tA + (size_t)qi * kTriF4, o4, X);
+                            lazy_pre(part ? tA + (size_t)qi * kTriF4 : tB + (size_t)qj * kTriF4, o4, Y);
                             d2 = tri_dist2_half(X, Y, part);
                         }
                     }
                     if (!ONE) d2 = fminf(d2, __shfl_xor_sync(0xffffffffu, d2, 16));
                     if (pl < take && part == 0) {
                         const float d = sqrtf(d2);
-                        const float4 xa = auxA[qi];
-                        // a carried pair's B record may be from an earlier chunk:
-                        // its (proxy, Hausdorff) come from the record itself
-                        const float4 xb = carry ? make_float4(tQ[(size_t)qj * kTriF4].w, tQ[(size_t)qj * kTriF4 + 1].w,
-                                                              0.f, 0.f)
-                                                : auxB[qj];
+                        const float4 xa = auxA[qi], xb = auxB[qj];
                         bd = fminf(bd, d);
                         bl = fminf(bl, fmaxf(d - xa.x - xb.x, 0.f));
                         bh = fminf(bh, d + xa.y + xb.y);
@@ -1052,20 +1025,14 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
                     bl = warp_min_nonneg(bl);
                     bh = warp_min_nonneg(bh);
                     qn -= take;
-                    const QE moved = lane < qn ? queue[take + lane] : QE(0);
+                    const unsigned short moved = lane < qn ? queue[take + lane] : 0;
                     __syncwarp();
                     if (lane < qn) queue[lane] = moved;
                     __syncwarp();
                     flush = false;
                     if (i >= ca && !cm && qn == 0) break;
-                    if (i >= ca && !cm) {
-                        // CARRY: fewer than a full round left -- they wait for
-                        // the next B chunk's pairs instead of a partial drain
-                        if (carry && b0 + kCB < w.b_cnt && qn < 16) break;
-                        flush = true;
-                    }
+                    if (i >= ca && !cm) flush = true;
                 }
-                qcarry = carry ? qn : 0;
             }
             if (TMA && stalled) break;
         }
@@ -1115,12 +1082,10 @@ struct TunedCfgDef {
 // lazy kernel, two lanes and one lane per pair, queuing 8 seeds first;
 // 12-13: the lazy kernel staging its raw records by 1-D bulk copies (TMA);
 // 14-15: the lazy kernel with 8 seeds first and the spread cull; 16-17: 14-15
-// with the cylinder bound in every cull test; 18-19: 16-17 carrying partial
-// rounds of queued pairs over to the next chunk of B
+// with the cylinder bound in every cull test
 constexpr TunedCfgDef kTunedCfgs[kTunedConfigs] = {{64, 3}, {48, 3}, {32, 4}, {128, 3}, {128, 4}, {64, 4},
                                                     {128, 5}, {128, 6}, {128, 4}, {128, 5}, {128, 5}, {128, 5},
-                                                    {128, 4}, {64, 5}, {128, 5}, {128, 4}, {128, 5}, {128, 4},
-                                                    {128, 5}, {128, 4}};
+                                                    {128, 4}, {64, 5}, {128, 5}, {128, 4}, {128, 5}, {128, 4}};
 
 TunedConfig tuned_config(int cfg) {
     if (cfg < 0 || cfg >= kTunedConfigs) cfg = 0;
@@ -1153,13 +1118,13 @@ static cudaError_t launch_tuned_cfg(const float4* triA, const float4* triB, cons
 }
 
 template <int CA, int MINB, bool ONE = false, int SEEDS = 32, bool TMA = false, bool SPREAD = false,
-          bool CYL = false, bool CARRY = false>
+          bool CYL = false>
 static cudaError_t launch_lazy_cfg(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                    float4* out, unsigned* work_counter, unsigned long long* n_full, int num_sms,
                                    cudaStream_t s, const unsigned* n_items_dev, const float* init_bd) {
     const size_t smem = (size_t)kTunedWarps *
                         (TMA ? LazyLayout<CA>::kWarpFloatsTma : LazyLayout<CA>::kWarpFloats) * sizeof(float);
-    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB, ONE, SEEDS, TMA, SPREAD, CYL, CARRY>;
+    auto kern = refine_lazy_kernel<kTunedWarps, CA, MINB, ONE, SEEDS, TMA, SPREAD, CYL>;
     if (smem > 48 * 1024) {
         static bool attr_set[64] = {};  // per device
         int dev = 0;
@@ -1203,8 +1168,6 @@ cudaError_t launch_refine_tuned(const float4* triA, const float4* triB, const Re
         case 15: return launch_lazy_cfg<128, 4, false, 8, false, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 16: return launch_lazy_cfg<128, 5, false, 8, false, true, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         case 17: return launch_lazy_cfg<128, 4, false, 8, false, true, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
-        case 18: return launch_lazy_cfg<128, 5, false, 8, false, true, true, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
-        case 19: return launch_lazy_cfg<128, 4, false, 8, false, true, true, true>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
         default: return launch_tuned_cfg<64, 3>(triA, triB, items, n_items, out, work_counter, n_full, num_sms, s, n_items_dev, init_bd);
     }
 }

@@ -10,7 +10,7 @@ namespace tdp {
 cudaError_t launch_refine_plain(const float4* triA, const float4* triB, const RefineItem* items, int n_items,
                                 float4* out, cudaStream_t s);
 // tuned-kernel configurations (index 0 is the default); see refine.cu
-constexpr int kTunedConfigs = 20;
+constexpr int kTunedConfigs = 18;
 struct TunedConfig {
     int chunk_a;      // A-side triangles staged per warp and chunk
     int ctas_per_sm;  // resident CTAs per SM the launch is sized for

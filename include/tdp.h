@@ -117,9 +117,7 @@ int tdp_fp32_peak(tdp_ctx *ctx, double *tflops);
  * chunk's triangle records in shared memory by a 1-D bulk copy (TMA); 14-15
  * spread each needed cluster's member tests over the warp; 16-17 are 14-15
  * with a cylinder bound -- gap along the item's axis, centre distance across
- * it less both radii -- in every cull test; 18-19 are 16-17 carrying a
- * partial round of queued pairs over to the next chunk).  All return
- * identical results;
+ * it less both radii -- in every cull test).  All return identical results;
  * they differ only in speed, which depends on the voxel sizes of the join.
  * A context starts with configuration 0.  The reference has one fixed launch
  * shape (one CTA of 512 threads per voxel pair,

@@ -134,7 +134,7 @@ def test_null_arguments_are_errors_not_crashes(pkg, tmp_path):
         elif name == "tdp_host_cache_bytes":
             assert int(value) == 0                             # trimmed just before
         elif name == "tdp_refine_config_count":
-            assert int(value) == 20
+            assert int(value) == 18
         else:
             assert int(value) == 1, (name, value)              # TDP_ERR_ARG
     assert set(got) == set(declared_symbols()), sorted(set(declared_symbols()) ^ set(got))
