@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <atomic>
 #include <condition_variable>
+#include <exception>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -20,7 +21,8 @@ struct Job {
     const std::function<void(long)>* fn = nullptr;
     long n = 0;
     std::atomic<long> next{0};
-    int refs = 0;  // guarded by Pool::m
+    int refs = 0;                // guarded by Pool::m
+    std::exception_ptr error;    // the first task that threw (guarded by Pool::m)
 };
 
 struct Pool {
@@ -34,11 +36,19 @@ struct Pool {
 
 thread_local bool t_in_task = false;
 
-void run_tasks(Job& J) {
+// Runs tasks until none is left; a task that throws ends this thread's share
+// (the exception is returned; threads still in the loop take the rest).
+std::exception_ptr run_tasks(Job& J) {
     const bool outer = t_in_task;
     t_in_task = true;
-    for (long k = J.next++; k < J.n; k = J.next++) (*J.fn)(k);
+    std::exception_ptr err;
+    try {
+        for (long k = J.next++; k < J.n; k = J.next++) (*J.fn)(k);
+    } catch (...) {
+        err = std::current_exception();
+    }
     t_in_task = outer;
+    return err;
 }
 
 void worker_main(Pool* P) {
@@ -51,8 +61,9 @@ void worker_main(Pool* P) {
         if (!J) continue;
         ++J->refs;
         lk.unlock();
-        run_tasks(*J);
+        std::exception_ptr err = run_tasks(*J);
         lk.lock();
+        if (err && !J->error) J->error = err;
         if (--J->refs == 0) P->idle.notify_all();
     }
 }
@@ -114,12 +125,17 @@ void host_for(long n, const std::function<void(long)>& fn) {
         ++P->gen;
     }
     P->work.notify_all();
-    run_tasks(J);
-    // every task is claimed once the caller's own loop ends; wait for the
-    // workers still running one, after which none can enter this job
-    std::unique_lock<std::mutex> lk(P->m);
-    P->cur = nullptr;
-    P->idle.wait(lk, [&] { return J.refs == 0; });
+    std::exception_ptr err = run_tasks(J);
+    // every task is claimed once the caller's own loop ends (or has thrown);
+    // wait for the workers still running one, after which none can enter
+    // this job, then pass on the first exception a task threw
+    {
+        std::unique_lock<std::mutex> lk(P->m);
+        P->cur = nullptr;
+        P->idle.wait(lk, [&] { return J.refs == 0; });
+        if (!err) err = J.error;
+    }
+    if (err) std::rethrow_exception(err);
 }
 
 }  // namespace tdp

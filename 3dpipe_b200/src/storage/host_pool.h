@@ -19,7 +19,9 @@ int host_threads();
 // fn(k) for every k in [0, n), on the pool's workers and the calling thread;
 // returns when every call has returned.  A call made from inside fn runs its
 // tasks serially on the calling thread.  One loop runs at a time; concurrent
-// callers queue.
+// callers queue.  If a call throws, the loop still waits for the calls in
+// flight and then rethrows the first exception (tasks not yet started when
+// the throwing thread stopped may be skipped).
 void host_for(long n, const std::function<void(long)>& fn);
 
 // fn(b, e) over [0, n) in at most host_threads() contiguous ranges of at
