@@ -258,3 +258,35 @@ def test_concurrent_parses_share_the_block_cache(pkg):
     assert not errors, errors[:3]
     pkg.tdp.host_cache_trim()
     assert pkg.tdp.host_cache_bytes() == 0
+
+
+@pytest.mark.filterwarnings("ignore:This process .* is multi-threaded")
+def test_parallel_parse_on_the_host_pool_survives_fork(pkg):
+    """The parser's parallel loops (the chunked walk, the voxel tables, the
+    prefix sums) run on one process-wide pool of host threads; a child
+    forked from a process that has started the pool starts its own."""
+    import os
+    import signal
+    import time
+    nb, _ = pkg.tdp.gen_tiles(50, 200, seed=31, only="nuclei")  # 10,000 equal records
+    first = pkg.tdp.raw_check(nb)
+    assert first == (10000, 130000)
+    assert pkg.tdp.raw_check(nb) == first
+    pid = os.fork()
+    if pid == 0:
+        code = 3
+        try:
+            code = 0 if pkg.tdp.raw_check(nb) == first else 2
+        finally:
+            os._exit(code)
+    deadline = time.time() + 120
+    while True:
+        done, status = os.waitpid(pid, os.WNOHANG)
+        if done:
+            break
+        if time.time() > deadline:
+            os.kill(pid, signal.SIGKILL)
+            os.waitpid(pid, 0)
+            pytest.fail("the forked child did not finish parsing")
+        time.sleep(0.05)
+    assert os.WIFEXITED(status) and os.WEXITSTATUS(status) == 0
