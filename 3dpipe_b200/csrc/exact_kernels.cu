@@ -38,6 +38,7 @@
 #include <string>
 
 #include "exact_kernels.cuh"
+#include "cull.cuh"
 #include "refine.cuh"
 #include "tridist.cuh"
 
@@ -211,6 +212,53 @@ __global__ void __launch_bounds__(kBlk) k_exact_vp(JoinDev d, const float* __res
             count += __popc(bal);
         }
         if (!WRITE && lane == 0) cnt[p] = count;
+    }
+}
+
+constexpr int kRjWarps = 8;
+constexpr int kRjCA = 128;  // A triangles staged per round, as the refine stages them
+
+// The FP32 pass's item-level test on its own, ahead of the refine: a small
+// kernel (no queue, no triangle distances) that keeps the candidates which
+// may have a triangle pair below their preset and compacts them -- item,
+// object pair, preset -- for the refine.  About 92 % of the candidates of
+// the within-400 join fall here; in the refine the same test shared a large
+// kernel's instruction cache and registers with the evaluations.
+__global__ void __launch_bounds__(kRjWarps * 32) k_exact_reject(const float4* __restrict__ triA,
+                                                                const float4* __restrict__ triB,
+                                                                const RefineItem* __restrict__ items,
+                                                                const int* __restrict__ item_pair,
+                                                                const float* __restrict__ preset, int64_t E,
+                                                                RefineItem* __restrict__ out_items,
+                                                                int* __restrict__ out_pair,
+                                                                float* __restrict__ out_preset,
+                                                                unsigned* __restrict__ n_out) {
+    __shared__ __align__(16) float4 stage[kRjWarps][2 * kRjCA + 2 * (kRjCA / kCl)];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float4* sphA = stage[wid];
+    float4* auxA = sphA + kRjCA;
+    float4* clS = auxA + kRjCA;
+    float4* clA = clS + kRjCA / kCl;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < E; e += nw) {
+        const RefineItem it = items[e];
+        if (it.a_cnt == 0 || it.b_cnt == 0) continue;  // nothing to refine
+        const float4 o4 = triA[(size_t)it.a_off * kTriF4];
+        float3 u;  // the refine's axis: first A vertex to first B vertex
+        {
+            const float4 q = triB[(size_t)it.b_off * kTriF4];
+            const float ux = q.x - o4.x, uy = q.y - o4.y, uz = q.z - o4.z;
+            const float n2 = ux * ux + uy * uy + uz * uz;
+            const float inv = n2 > 0.f ? rsqrtf(n2) : 0.f;
+            u = make_float3(ux * inv, uy * inv, uz * inv);
+        }
+        const float bd = preset[e];
+        if (item_may_go_below<kRjCA, true>(triA, triB, it, o4, u, bd, sphA, auxA, clS, clA, lane) && lane == 0) {
+            const unsigned w = atomicAdd(n_out, 1u);
+            out_items[w] = it;
+            out_pair[w] = item_pair[e];
+            out_preset[w] = bd;
+        }
     }
 }
 
@@ -510,6 +558,9 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     ENS(73, Ez * 4);                   // selected -> pair
     ENS(74, Ez * 8);                   // selected (reach, limit)
     ENS(81, Ez * 4);                   // presets
+    ENS(84, Ez * sizeof(RefineItem));  // items that pass the item-level test
+    ENS(85, Ez * 4);                   // their pairs
+    ENS(86, Ez * 4);                   // their presets
     RefineItem* items = (RefineItem*)ctx->scratch[67].p;
     int* item_pair = (int*)ctx->scratch[68].p;
     float4* res = (float4*)ctx->scratch[69].p;
@@ -531,12 +582,25 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
     unsigned long long* n_full = reinterpret_cast<unsigned long long*>(ctr + 12);
     if (E > 0) {
         CU(launch_fetch_items(items, nullptr, E, kNumLods - 1, lz1, lz2, ctx->num_sms, s));
-        CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], items, (int)E, res, ctr, n_full,
-                               ctx->num_sms, kExactRefineCfg, s, nullptr, preset));
-        const int eg = grid(E, 256, ctx->num_sms * 16);
-        k_exact_best<<<eg, 256, 0, s>>>(res, item_pair, E, best32, emax, ctr + 14);
+        // the item-level test first, in its own kernel; ctr[2] counts the survivors
+        RefineItem* items2 = (RefineItem*)ctx->scratch[84].p;
+        int* pair2 = (int*)ctx->scratch[85].p;
+        float* preset2 = (float*)ctx->scratch[86].p;
+        k_exact_reject<<<grid(E, kRjWarps, ctx->num_sms * 16), kRjWarps * 32, 0, s>>>(
+            t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], items, item_pair, preset, E, items2, pair2, preset2, ctr + 2);
         CU(cudaGetLastError());
-        k_exact_select<<<eg, 256, 0, s>>>(res, items, item_pair, E, best32, emax, sel, sel_pair, sel_thr, ctr + 4);
+        unsigned e2 = 0;
+        CU(cudaMemcpyAsync(&e2, ctr + 2, 4, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        const int64_t E2 = e2;
+        info.launches += 1;
+        if (E2 > 0)
+            CU(launch_refine_tuned(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], items2, (int)E2, res, ctr, n_full,
+                                   ctx->num_sms, kExactRefineCfg, s, nullptr, preset2));
+        const int eg = grid(std::max<int64_t>(E2, 1), 256, ctx->num_sms * 16);
+        k_exact_best<<<eg, 256, 0, s>>>(res, pair2, E2, best32, emax, ctr + 14);
+        CU(cudaGetLastError());
+        k_exact_select<<<eg, 256, 0, s>>>(res, items2, pair2, E2, best32, emax, sel, sel_pair, sel_thr, ctr + 4);
         CU(cudaGetLastError());
         CU(cudaEventRecord(ctx->xev[3], s));
         k_exact_f64<<<ctx->num_sms * 8, kExWarps * 32, 0, s>>>(t1->tri[kNumLods - 1], t2->tri[kNumLods - 1], sel,
@@ -555,7 +619,7 @@ int exact_distances(tdp_ctx* ctx, const JoinDev& d, const tdp_tile* t1, const td
         std::memcpy(&e32, &ns[4], 4);
         info.max_rel_err32 = e32;
         std::memcpy(&info.full_evals, &ns[8], 8);
-        info.dropped_items = ns[10];
+        info.dropped_items = (long)(E - E2) + ns[10];
         info.below_items = ns[11];
         float ms[4] = {0, 0, 0, 0};
         for (int k = 0; k < 4; ++k) cudaEventElapsedTime(&ms[k], ctx->xev[k], ctx->xev[k + 1]);
