@@ -85,83 +85,103 @@ __device__ __forceinline__ float quick_proj(const float4* __restrict__ t, float4
 // cylinder bound along u -- comes below bd, so that no triangle pair of the
 // item does.  The A triangles' spheres go through sphA / auxA and the
 // clusters through clS / clA (a warp's staging, CA triangles at a time).
+
+// The bound of a staged chunk of A as a whole: a sphere around its cluster
+// spheres and their largest projection on u (inflated like the cluster
+// spheres), so that a B triangle far from the whole chunk costs one test
+// instead of one per cluster.
+struct ChunkBound {
+    float4 s;
+    float pz;
+};
+
+// Stage A triangles [a0, a0 + ca) of item w: spheres and projections on u
+// relative to o4, their clusters, and the chunk's bound.
+template <int CA, bool CYL>
+__device__ __forceinline__ ChunkBound stage_a_chunk(const float4* __restrict__ triA, const RefineItem& w, uint32_t a0,
+                                                    int ca, float4 o4, float3 u, float4* sphA, float4* auxA,
+                                                    float4* clS, float4* clA, int lane) {
+    const int ncl = (ca + kCl - 1) / kCl;
+    __syncwarp();
+    for (int k = lane; k < ca; k += 32) {
+        const float4* t = triA + ((size_t)w.a_off + a0 + k) * kTriF4;
+        sphA[k] = quick_sphere(t, o4);
+        auxA[k] = make_float4(0.f, 0.f, CYL ? quick_proj(t, o4, u, false) : 0.f, 0.f);
+    }
+    __syncwarp();
+    build_clusters<CA>(sphA, auxA, ca, clS, clA, lane);
+    __syncwarp();
+    const bool v = lane < ncl;
+    const float4 cs = v ? clS[lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float lx = v ? cs.x : FLT_MAX, hx = v ? cs.x : -FLT_MAX;
+    float ly = v ? cs.y : FLT_MAX, hy = v ? cs.y : -FLT_MAX;
+    float lz = v ? cs.z : FLT_MAX, hz = v ? cs.z : -FLT_MAX;
+    float vz = v ? clA[lane].z : -FLT_MAX;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
+        hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, o));
+        ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, o));
+        hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, o));
+        lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, o));
+        hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, o));
+        vz = fmaxf(vz, __shfl_xor_sync(0xffffffffu, vz, o));
+    }
+    const float cx = 0.5f * (lx + hx), cy = 0.5f * (ly + hy), cz = 0.5f * (lz + hz);
+    float r = 0.f;
+    if (v) {
+        const float dx = cs.x - cx, dy = cs.y - cy, dz = cs.z - cz;
+        r = radius_sqrt(dx * dx + dy * dy + dz * dz) + cs.w;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r = fmaxf(r, __shfl_xor_sync(0xffffffffu, r, o));
+    return ChunkBound{make_float4(cx, cy, cz, r * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f), vz};
+}
+
+// True (on every lane) when some B triangle of item w and some cluster of
+// the staged A chunk (ncl clusters, bound vb) come below bd: every lane
+// tests its B triangle; the warp stops at the first chunk of B where any
+// lane needs a cluster.
+template <bool CYL>
+__device__ __forceinline__ bool b_needs_chunk(const float4* __restrict__ triB, const RefineItem& w, int ncl,
+                                              const ChunkBound& vb, float4 o4, float3 u, float bd,
+                                              const float4* clS, const float4* clA, int lane) {
+    bool need = false;
+    for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += kCB) {
+        if (b0 + lane < w.b_cnt) {
+            const float4* t = triB + ((size_t)w.b_off + b0 + lane) * kTriF4;
+            const float4 sb = quick_sphere(t, o4);
+            const float pb = CYL ? quick_proj(t, o4, u, true) : 0.f;
+            const float vx = vb.s.x - sb.x, vy = vb.s.y - sb.y, vw = vb.s.z - sb.z;
+            const float vr = vb.s.w + sb.w + bd;
+            const bool near = vx * vx + vy * vy + vw * vw < vr * vr &&
+                              (!CYL || cyl_keep(vx, vy, vw, vb.s.w + sb.w, pb - vb.pz, u, bd));
+            for (int c = 0; near && c < ncl; ++c) {
+                const float4 cs = clS[c];
+                const float dx = cs.x - sb.x, dy = cs.y - sb.y, dz = cs.z - sb.z;
+                const float reach = cs.w + sb.w + bd;
+                if (dx * dx + dy * dy + dz * dz < reach * reach &&
+                    (!CYL || cyl_keep(dx, dy, dz, cs.w + sb.w, pb - clA[c].z, u, bd))) {
+                    need = true;
+                    break;
+                }
+            }
+        }
+        if (__any_sync(0xffffffffu, need)) return true;
+    }
+    return false;
+}
+
 template <int CA, bool CYL>
 __device__ __forceinline__ bool item_may_go_below(const float4* __restrict__ triA, const float4* __restrict__ triB,
                                                   const RefineItem& w, float4 o4, float3 u, float bd, float4* sphA,
                                                   float4* auxA, float4* clS, float4* clA, int lane) {
-    constexpr int kCA = CA;
-    bool need = false;
-    for (uint32_t a0 = 0; a0 < w.a_cnt && !__any_sync(0xffffffffu, need); a0 += kCA) {
-        const int ca = min((uint32_t)kCA, w.a_cnt - a0);
-        const int ncl = (ca + kCl - 1) / kCl;
-        __syncwarp();
-        for (int k = lane; k < ca; k += 32) {
-            const float4* t = triA + ((size_t)w.a_off + a0 + k) * kTriF4;
-            sphA[k] = quick_sphere(t, o4);
-            auxA[k] = make_float4(0.f, 0.f, CYL ? quick_proj(t, o4, u, false) : 0.f, 0.f);
-        }
-        __syncwarp();
-        build_clusters<CA>(sphA, auxA, ca, clS, clA, lane);
-        __syncwarp();
-        // the chunk's own bound first: a sphere around its cluster
-        // spheres and their largest projection on u (inflated like
-        // the cluster spheres), so that a B triangle far from the
-        // whole chunk costs one test instead of one per cluster
-        float4 vs;
-        float vz;
-        {
-            const bool v = lane < ncl;
-            const float4 cs = v ? clS[lane] : make_float4(0.f, 0.f, 0.f, 0.f);
-            float lx = v ? cs.x : FLT_MAX, hx = v ? cs.x : -FLT_MAX;
-            float ly = v ? cs.y : FLT_MAX, hy = v ? cs.y : -FLT_MAX;
-            float lz = v ? cs.z : FLT_MAX, hz = v ? cs.z : -FLT_MAX;
-            vz = v ? clA[lane].z : -FLT_MAX;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
-                hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, o));
-                ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, o));
-                hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, o));
-                lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, o));
-                hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, o));
-                vz = fmaxf(vz, __shfl_xor_sync(0xffffffffu, vz, o));
-            }
-            const float cx = 0.5f * (lx + hx), cy = 0.5f * (ly + hy), cz = 0.5f * (lz + hz);
-            float r = 0.f;
-            if (v) {
-                const float dx = cs.x - cx, dy = cs.y - cy, dz = cs.z - cz;
-                r = radius_sqrt(dx * dx + dy * dy + dz * dz) + cs.w;
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) r = fmaxf(r, __shfl_xor_sync(0xffffffffu, r, o));
-            vs = make_float4(cx, cy, cz, r * 1.0001f + 1e-5f * (fabsf(cx) + fabsf(cy) + fabsf(cz)) + 1e-6f);
-        }
-        // every lane tests its B triangle; the warp stops at the
-        // first chunk of B where any lane needs a cluster
-        for (uint32_t b0 = 0; b0 < w.b_cnt; b0 += kCB) {
-            if (b0 + lane < w.b_cnt) {
-                const float4* t = triB + ((size_t)w.b_off + b0 + lane) * kTriF4;
-                const float4 sb = quick_sphere(t, o4);
-                const float pb = CYL ? quick_proj(t, o4, u, true) : 0.f;
-                const float vx = vs.x - sb.x, vy = vs.y - sb.y, vw = vs.z - sb.z;
-                const float vr = vs.w + sb.w + bd;
-                const bool near = vx * vx + vy * vy + vw * vw < vr * vr &&
-                                  (!CYL || cyl_keep(vx, vy, vw, vs.w + sb.w, pb - vz, u, bd));
-                for (int c = 0; near && c < ncl; ++c) {
-                    const float4 cs = clS[c];
-                    const float dx = cs.x - sb.x, dy = cs.y - sb.y, dz = cs.z - sb.z;
-                    const float reach = cs.w + sb.w + bd;
-                    if (dx * dx + dy * dy + dz * dz < reach * reach &&
-                        (!CYL || cyl_keep(dx, dy, dz, cs.w + sb.w, pb - clA[c].z, u, bd))) {
-                        need = true;
-                        break;
-                    }
-                }
-            }
-            if (__any_sync(0xffffffffu, need)) break;
-        }
+    for (uint32_t a0 = 0; a0 < w.a_cnt; a0 += CA) {
+        const int ca = min((uint32_t)CA, w.a_cnt - a0);
+        const ChunkBound vb = stage_a_chunk<CA, CYL>(triA, w, a0, ca, o4, u, sphA, auxA, clS, clA, lane);
+        if (b_needs_chunk<CYL>(triB, w, (ca + kCl - 1) / kCl, vb, o4, u, bd, clS, clA, lane)) return true;
     }
-    return __any_sync(0xffffffffu, need);
+    return false;
 }
 
 }  // namespace tdp

@@ -239,21 +239,47 @@ __global__ void __launch_bounds__(kRjWarps * 32) k_exact_reject(const float4* __
     float4* auxA = sphA + kRjCA;
     float4* clS = auxA + kRjCA;
     float4* clA = clS + kRjCA / kCl;
+    // each warp takes a contiguous run of candidates: those of one object
+    // pair come A voxel by A voxel, so consecutive candidates mostly share
+    // their A voxel, whose staging (and the axis it was staged along) is
+    // then reused -- any axis gives a valid bound
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < E; e += nw) {
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t per = (E + nw - 1) / nw;
+    const int64_t e_end = min(E, (gw + 1) * per);
+    uint32_t held_off = 0, held_cnt = 0;  // the A voxel staged (held_cnt 0: none)
+    float4 o4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float3 u = make_float3(0.f, 0.f, 0.f);
+    ChunkBound vb{};
+    for (int64_t e = gw * per; e < e_end; ++e) {
         const RefineItem it = items[e];
         if (it.a_cnt == 0 || it.b_cnt == 0) continue;  // nothing to refine
-        const float4 o4 = triA[(size_t)it.a_off * kTriF4];
-        float3 u;  // the refine's axis: first A vertex to first B vertex
-        {
+        const float bd = preset[e];
+        bool keep;
+        if (it.a_cnt <= (uint32_t)kRjCA) {
+            if (it.a_off != held_off || it.a_cnt != held_cnt) {
+                o4 = triA[(size_t)it.a_off * kTriF4];
+                const float4 q = triB[(size_t)it.b_off * kTriF4];  // first A vertex to first B vertex
+                const float ux = q.x - o4.x, uy = q.y - o4.y, uz = q.z - o4.z;
+                const float n2 = ux * ux + uy * uy + uz * uz;
+                const float inv = n2 > 0.f ? rsqrtf(n2) : 0.f;
+                u = make_float3(ux * inv, uy * inv, uz * inv);
+                vb = stage_a_chunk<kRjCA, true>(triA, it, 0, (int)it.a_cnt, o4, u, sphA, auxA, clS, clA, lane);
+                held_off = it.a_off;
+                held_cnt = it.a_cnt;
+            }
+            keep = b_needs_chunk<true>(triB, it, ((int)it.a_cnt + kCl - 1) / kCl, vb, o4, u, bd, clS, clA, lane);
+        } else {  // a voxel larger than one staging round
+            const float4 oa = triA[(size_t)it.a_off * kTriF4];
             const float4 q = triB[(size_t)it.b_off * kTriF4];
-            const float ux = q.x - o4.x, uy = q.y - o4.y, uz = q.z - o4.z;
+            const float ux = q.x - oa.x, uy = q.y - oa.y, uz = q.z - oa.z;
             const float n2 = ux * ux + uy * uy + uz * uz;
             const float inv = n2 > 0.f ? rsqrtf(n2) : 0.f;
-            u = make_float3(ux * inv, uy * inv, uz * inv);
+            const float3 ua = make_float3(ux * inv, uy * inv, uz * inv);
+            keep = item_may_go_below<kRjCA, true>(triA, triB, it, oa, ua, bd, sphA, auxA, clS, clA, lane);
+            held_cnt = 0;  // the staging was overwritten
         }
-        const float bd = preset[e];
-        if (item_may_go_below<kRjCA, true>(triA, triB, it, o4, u, bd, sphA, auxA, clS, clA, lane) && lane == 0) {
+        if (keep && lane == 0) {
             const unsigned w = atomicAdd(n_out, 1u);
             out_items[w] = it;
             out_pair[w] = item_pair[e];
