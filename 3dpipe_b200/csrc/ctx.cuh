@@ -63,7 +63,7 @@ struct tdp_ctx {
     cudaEvent_t pf_ev[16] = {};   // fork / join of the prefetches (no timing)
     std::string last_error;
     std::unordered_map<void*, size_t> allocs;
-    tdp::Buf scratch[104];  // slots: refine-batch 0-4, tile upload 12-13, join 20-48, candidates 50-59 and 88-90, result sort 60-63, exact distances 64-81, per-object queries 82-83, GPU attach pass 96-100
+    tdp::Buf scratch[104];  // slots: refine-batch 0-4, tile upload 12-13, join 20-48, candidates 50-59 and 88-90, result sort 60-63, exact distances 64-81 and 84-86, per-object queries 82-83, last-LOD presets 91, GPU attach pass 96-100
     unsigned* d_counter = nullptr;            // work counters (device)
     unsigned long long* d_stats = nullptr;    // device-side statistics
     tdp::LastStats stats;

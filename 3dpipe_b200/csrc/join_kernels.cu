@@ -302,8 +302,33 @@ __global__ void __launch_bounds__(kBlock) k_vps(JoinDev d, int within_all, float
 // item count and n1*n2 sum to the counters, the lanes write at the claimed
 // base plus their rank among the warp's items.  (The items form a set: their
 // order never changes a result.)
+// The preset of a within item at the last LOD (LOD 100): its query's
+// distance plus twice the largest FP32 error of a triangle pair that could
+// be within it.  Such a pair's coordinates, taken from a vertex of the A
+// voxel, stay below tau + both voxel extents (R), so its FP32 distance is
+// below tau + err_bound(R): an item with nothing below the preset has no
+// pair within tau.  kNN items get FLT_MAX (no preset).
+__device__ __forceinline__ float within_preset(const JoinDev& d, int p, int a, int b, float tau_all) {
+    float tau = tau_all;
+    if (d.qk) {
+        const int q = d.pq[p];
+        if (d.qk[q] > 0) return FLT_MAX;
+        tau = d.qtau[q];
+    }
+    const float4* va = d.vox1 + 3 * (size_t)a;
+    const float4* vb = d.vox2 + 3 * (size_t)b;
+    const float4 alo = va[0], ahi = va[1], blo = vb[0], bhi = vb[1];
+    const float da = (ahi.x - alo.x) + (ahi.y - alo.y) + (ahi.z - alo.z);
+    const float db = (bhi.x - blo.x) + (bhi.y - blo.y) + (bhi.z - blo.z);
+    const float R = (tau + da + db) * 1.001f + 1.f;
+    return tau + 2.f * err_bound(R) + 1e-6f;
+}
+
+// preset != NULL (the tuned form's last LOD of a join with within queries):
+// also write each item's preset (within_preset)
 __global__ void k_build_items(JoinDev d, const uint32_t* __restrict__ vt1, const uint32_t* __restrict__ vt2,
-                              RefineItem* __restrict__ items, int* __restrict__ item_vp, unsigned* __restrict__ counter) {
+                              RefineItem* __restrict__ items, int* __restrict__ item_vp, unsigned* __restrict__ counter,
+                              float* __restrict__ preset, float tau_all) {
     // counter[0] = items, counter[2..3] = sum n1*n2 (u64)
     const int lane = threadIdx.x & 31;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -312,8 +337,10 @@ __global__ void k_build_items(JoinDev d, const uint32_t* __restrict__ vt1, const
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < vend; v += stride) {
         bool ok = v < d.V && d.valive[v] && d.pstat[d.vpair[v]] == kUndecided;
         uint32_t o1 = 0, n1 = 0, o2 = 0, n2 = 0;
+        int a = 0, b = 0;
         if (ok) {
-            const int a = d.vpa[v], b = d.vpb[v];
+            a = d.vpa[v];
+            b = d.vpb[v];
             o1 = vt1[a]; n1 = vt1[a + 1] - o1;
             o2 = vt2[b]; n2 = vt2[b + 1] - o2;
             ok = n1 > 0 && n2 > 0;
@@ -333,18 +360,35 @@ __global__ void k_build_items(JoinDev d, const uint32_t* __restrict__ vt1, const
             const unsigned w = base + __popc(m & ((1u << lane) - 1u));
             items[w] = RefineItem{o1, n1, o2, n2};
             item_vp[w] = (int)v;
+            if (preset) preset[w] = within_preset(d, d.vpair[v], a, b, tau_all);
         }
     }
 }
 
+// A voxel pair whose refine found nothing below its preset is out of its
+// query's reach: both its bounds go to kFar, so it never lowers the pair's
+// minimum, never reports it, and adds no error term.
+constexpr float kFar = 3.0e38f;
+
 __global__ void k_apply_results(JoinDev d, const float4* __restrict__ res, const int* __restrict__ item_vp, int W_host,
-                                const unsigned* W_dev, int highest, int level, int li, int stamp) {
+                                const unsigned* W_dev, int highest, int level, int li, int stamp,
+                                const float* __restrict__ preset) {
     const int W = W_dev ? (int)*W_dev : W_host;
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) {
         const int v = item_vp[w];
         const float4 r = res[w];
         float mn = d.vmn[v], mx = d.vmx[v];
         const float e = err_bound(r.w);
+        if (highest && preset) {
+            const float pb = preset[w];
+            if (pb < FLT_MAX && !(r.x < pb)) {
+                d.vmn[v] = kFar;
+                d.vmx[v] = kFar;
+                d.verr[v] = fmaxf(d.verr[v], e);
+                d.vupd[v] = stamp;
+                continue;
+            }
+        }
         if (highest) {
             mn = r.x;
             mx = r.x;
@@ -566,15 +610,16 @@ cudaError_t launch_write_vps(const JoinDev& d, int within, float tau, int tuned,
     return cudaGetLastError();
 }
 cudaError_t launch_build_items(const JoinDev& d, const uint32_t* vt1, const uint32_t* vt2, RefineItem* items,
-                               int* item_vp, unsigned* counter, cudaStream_t s) {
+                               int* item_vp, unsigned* counter, cudaStream_t s, float* preset, float tau) {
     if (d.V <= 0) return cudaSuccess;
-    k_build_items<<<grid_for(d.V, 256), 256, 0, s>>>(d, vt1, vt2, items, item_vp, counter);
+    k_build_items<<<grid_for(d.V, 256), 256, 0, s>>>(d, vt1, vt2, items, item_vp, counter, preset, tau);
     return cudaGetLastError();
 }
 cudaError_t launch_apply_results(const JoinDev& d, const float4* res, const int* item_vp, int W, int highest,
-                                 int level, int li, int stamp, cudaStream_t s, const unsigned* W_dev) {
+                                 int level, int li, int stamp, cudaStream_t s, const unsigned* W_dev,
+                                 const float* preset) {
     if (W <= 0) return cudaSuccess;
-    k_apply_results<<<grid_for(W, 256), 256, 0, s>>>(d, res, item_vp, W, W_dev, highest, level, li, stamp);
+    k_apply_results<<<grid_for(W, 256), 256, 0, s>>>(d, res, item_vp, W, W_dev, highest, level, li, stamp, preset);
     return cudaGetLastError();
 }
 cudaError_t launch_pair_update(const JoinDev& d, int stamp, int tuned, cudaStream_t s, int decide, float tau) {

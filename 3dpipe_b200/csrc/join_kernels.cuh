@@ -72,11 +72,17 @@ cudaError_t launch_knn_rank(const JoinDev& d, int K, int tuned, int* scratch_sta
 cudaError_t launch_count_vps(const JoinDev& d, int within, float tau, int tuned, int64_t* cnt, cudaStream_t s);
 cudaError_t launch_write_vps(const JoinDev& d, int within, float tau, int tuned, cudaStream_t s);
 // LOD step
+// preset != NULL: also each item's preset for the refine's init_bd (the
+// tuned form's last LOD, LOD 100, of a join with within queries): the
+// query's distance plus the FP32 error band, FLT_MAX for kNN items
 cudaError_t launch_build_items(const JoinDev& d, const uint32_t* vtri1, const uint32_t* vtri2, RefineItem* items,
-                               int* item_vp, unsigned* counter, cudaStream_t s);
-// W: item count, or an upper bound when W_dev (the exact count in device memory) is given
+                               int* item_vp, unsigned* counter, cudaStream_t s, float* preset = nullptr,
+                               float tau = 0.f);
+// W: item count, or an upper bound when W_dev (the exact count in device memory) is given;
+// preset: the presets the last LOD's refine ran with (NULL: none)
 cudaError_t launch_apply_results(const JoinDev& d, const float4* res, const int* item_vp, int W, int highest,
-                                 int level, int lod_idx, int stamp, cudaStream_t s, const unsigned* W_dev = nullptr);
+                                 int level, int lod_idx, int stamp, cudaStream_t s, const unsigned* W_dev = nullptr,
+                                 const float* preset = nullptr);
 // decide != 0 also takes the within decision (k_within_decide) of each pair
 cudaError_t launch_pair_update(const JoinDev& d, int stamp, int tuned, cudaStream_t s, int decide = 0, float tau = 0.f);
 // tuned form: FP64 recheck of the pairs left undecided after LOD 100

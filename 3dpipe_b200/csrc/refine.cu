@@ -283,9 +283,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
             u = make_float3(ux * inv, uy * inv, uz * inv);
         }
         float bd = FLT_MAX, bl = FLT_MAX, bh = FLT_MAX, rmax = 0.f;
-        // with init_bd (the exact-distance stage) only the minimum distance
-        // matters: it starts at the item's bound, and the two Hausdorff minima
-        // are parked at -FLT_MAX so they never widen a threshold
+        // with init_bd (the exact-distance stage, and a join's last LOD) only
+        // the minimum distance matters: it starts at the item's bound, and the
+        // two Hausdorff minima are parked at -FLT_MAX so they never widen a
+        // threshold.  An item preset to FLT_MAX has no bound and skips the
+        // item-level test.
         float b_init = FLT_MAX;
         if (init_bd) {
             b_init = init_bd[it];
@@ -296,7 +298,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_tuned_kernel(const fl
             // A triangles (clustered as below) against each lane's B triangle;
             // if no pair of spheres is closer than the preset, no triangle pair
             // is, and the item has nothing below it
-            bool need = false;
+            bool need = !(b_init < FLT_MAX);
             for (uint32_t a0 = 0; a0 < w.a_cnt && !__any_sync(0xffffffffu, need); a0 += kCA) {
                 const int ca = min((uint32_t)kCA, w.a_cnt - a0);
                 const int ncl = (ca + kCl - 1) / kCl;
@@ -660,8 +662,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) refine_lazy_kernel(const flo
             bh = -FLT_MAX;
             // item-level reject, as in refine_tuned_kernel: if no pair of
             // (cluster, triangle) bounds is closer than the preset, no
-            // triangle pair is, and the item has nothing below it
-            const bool need = item_may_go_below<CA, CYL>(triA, triB, w, o4, u, bd, sphA, auxA, clS, clA, lane);
+            // triangle pair is, and the item has nothing below it (b_init is
+            // the same on every lane, so the branch is uniform)
+            const bool need =
+                !(b_init < FLT_MAX) || item_may_go_below<CA, CYL>(triA, triB, w, o4, u, bd, sphA, auxA, clS, clA, lane);
             if (!__any_sync(0xffffffffu, need)) {
                 if (lane == 0) out[it] = make_float4(FLT_MAX, -FLT_MAX, -FLT_MAX, 0.f);
                 it = __shfl_sync(0xffffffffu, next, 0);

@@ -47,6 +47,7 @@ enum Slot {
     kKeyA = 60, kKeyB, kValA, kValB,  // result sort (50-59 hold the candidate buffers)
     kPexOut = 76, kOutD64,            // exact distances (64-75 and 78-81 are the exact stage's own)
     kQk = 82, kQtau,                  // per query object queries
+    kPreset = 91,                     // the last LOD's item presets (within queries)
 };
 
 template <typename T>
@@ -74,6 +75,10 @@ struct LodLoop {
     float tau;
     int* rankst;
     double *vexact, *res64, *pexact;
+    // within queries with LOD 100 last: each last-LOD item's preset (its
+    // query's distance plus the FP32 error band), so that the refine drops the
+    // items and triangle pairs that cannot come within it; NULL otherwise
+    float* preset;
     cudaEvent_t ev[16];
     LazyTile lz1, lz2;  // attached tiles: fetch each LOD's voxels before its refine
     cudaStream_t side;  // attached tiles: the next LOD's prefetch runs here
@@ -101,8 +106,9 @@ int enqueue_lod_loop(tdp_ctx* ctx, const LodLoop& L, cudaStream_t s, bool captur
     const bool prefetch = (L.lz1.on || L.lz2.on) && L.side;
     for (int k = 0; k < L.nl; ++k) {
         const int highest = k == L.highest_k;
+        float* preset = highest ? L.preset : nullptr;
         CUL(cudaMemsetAsync(cnt_items, 0, 4, s));
-        CUL(launch_build_items(L.d, L.vt1[k], L.vt2[k], L.items, L.item_vp, cnt_items, s));
+        CUL(launch_build_items(L.d, L.vt1[k], L.vt2[k], L.items, L.item_vp, cnt_items, s, preset, L.tau));
         if (prefetch && k > 0) CUL(cudaStreamWaitEvent(s, L.pf[2 * (k - 1) + 1], 0));
         CUL(launch_fetch_items(L.items, cnt_items, 0, L.li[k], L.lz1, L.lz2, L.num_sms, s));
         if (prefetch && k + 1 < L.nl) {
@@ -115,9 +121,9 @@ int enqueue_lod_loop(tdp_ctx* ctx, const LodLoop& L, cudaStream_t s, bool captur
         CUL(cudaMemcpyAsync(lod_counts + k, cnt_items, 4, cudaMemcpyDeviceToDevice, s));
         CUL(rec(L.ev[2 * k]));
         CUL(launch_refine_tuned(L.tri1[k], L.tri2[k], L.items, V, L.res, L.counter, L.dstats, L.num_sms, L.cfg[k], s,
-                                cnt_items));
+                                cnt_items, preset));
         CUL(rec(L.ev[2 * k + 1]));
-        CUL(launch_apply_results(L.d, L.res, L.item_vp, V, highest, L.hlevel, L.li[k], k, s, cnt_items));
+        CUL(launch_apply_results(L.d, L.res, L.item_vp, V, highest, L.hlevel, L.li[k], k, s, cnt_items, preset));
         // the within decision is taken inside the pair update; the kNN rank
         // reads every candidate of a query and stays its own launch
         CUL(launch_pair_update(L.d, k, 1, s, L.any_within ? 1 : 0, L.tau));
@@ -435,6 +441,8 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         // the FP64 recheck) is enqueued without a host round trip; kernels with
         // nothing left to do exit at once
         ENS(kVexact, Vz * 8); ENS(kPexact, Pz * 8); ENS(kRes64, Vz * 8);
+        const bool presets = any_within && !isect && lods.back() == 100;
+        if (presets) ENS(kPreset, Vz * 4);
         // 3b. after LOD 100, the FP64 recheck of pairs whose FP32 ranges
         // stayed inside their error band
         LodLoop L;
@@ -462,6 +470,7 @@ int tdp_join(tdp_ctx* ctx, const tdp_tile* t1, const tdp_tile* t2, const tdp_joi
         L.rankst = buf<int>(ctx, kRankSt);
         L.vexact = buf<double>(ctx, kVexact); L.res64 = buf<double>(ctx, kRes64); L.pexact = buf<double>(ctx, kPexact);
         L.lz1 = lz1; L.lz2 = lz2;
+        L.preset = presets ? buf<float>(ctx, kPreset) : nullptr;
         L.side = ctx->side;
         for (int k = 0; k < 16; ++k) L.pf[k] = ctx->pf_ev[k];
         if ((rc = run_lod_loop(ctx, L, s, &st.lod_graph))) return rc;
