@@ -104,9 +104,17 @@ void knn_rank(std::vector<Pair>& P, long b, long e, int K, int& conf) {
 // The join for the query objects qsel (ids into tile 1); when qsel is empty,
 // for the first max_queries objects of tile 1, or all of them when
 // max_queries <= 0.  Results are (tile-1 id, tile-2 id) pairs.
+//
+// cap_rel >= 0 (within joins at Hausdorff level 2 only) replays a cap on the
+// LODs before the last: at each such LOD a pair's cap is C = max(tau, the
+// smallest upper bound vmx of the voxel pairs this LOD refines) * (1 +
+// cap_rel) + cap_rel, above the pair's minmax after the LOD (vmx is a running
+// minimum); a voxel pair whose Hausdorff lower bound comes out above C keeps
+// its previous vmn and vmx.  cap_stats (2 doubles): such voxel-pair refines
+// and their triangle pairs.
 long join_impl(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t l2, int self_join, int is_knn, int knn,
                float tau, const int* lods, int nlods, int level, int threads, long max_queries, std::vector<int> qsel,
-               int* oq, int* ot, long cap, double* stats) {
+               int* oq, int* ot, long cap, double* stats, float cap_rel = -1.f, double* cap_stats = nullptr) {
     auto t0 = std::chrono::steady_clock::now();
     std::vector<RObject> T1 = oracle::read_tile(b1, l1);
     std::vector<RObject> T2 = self_join ? std::vector<RObject>() : oracle::read_tile(b2, l2);
@@ -178,16 +186,24 @@ long join_impl(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t l2, int s
     if (L.empty()) L = {20, 40, 60, 80, 100};
     std::sort(L.begin(), L.end());
     L.erase(std::unique(L.begin(), L.end()), L.end());
-    std::atomic<long long> tri_pairs{0}, vp_refined{0};
+    std::atomic<long long> tri_pairs{0}, vp_refined{0}, capped_vp{0}, capped_tp{0};
     for (size_t k = 0; k < L.size(); ++k) {
         const int li = L[k] / 20 - 1;
         const bool highest = k + 1 == L.size();
+        const bool capping = cap_rel >= 0.f && !is_knn && level == 2 && !highest;
         par((long)P.size(), threads, [&](long i) {
             Pair& p = P[i];
             if (p.stat) return;
             std::vector<float> ta, ha, tb, hb;
             double minmax = DBL_MAX;
-            long long tp = 0, nv = 0;
+            long long tp = 0, nv = 0, cvp = 0, ctp = 0;
+            float C = FLT_MAX;
+            if (capping) {
+                float base = FLT_MAX;
+                for (auto& v : p.vps)
+                    if (v.alive && T1[p.q].vox[v.a].cnt[li] && S[p.t].vox[v.b].cnt[li]) base = std::min(base, v.mx);
+                if (base < FLT_MAX) C = std::max(tau, base) * (1.f + cap_rel) + cap_rel;
+            }
             for (auto& v : p.vps) {
                 v.upd = false;
                 if (!v.alive) continue;
@@ -201,6 +217,7 @@ long join_impl(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t l2, int s
                 tp += (long long)(A.cnt[li] * B.cnt[li]);
                 ++nv;
                 if (highest) { v.mn = r.distance; v.mx = r.distance; }
+                else if (capping && r.min_dist > C) { ++cvp; ctp += (long long)(A.cnt[li] * B.cnt[li]); }
                 else if (level == 2) { v.mn = std::min(v.mn, r.min_dist); v.mx = std::min(v.mx, r.max_dist); }
                 else if (level == 1) {
                     v.mn = std::min(v.mn, r.distance - T1[p.q].hd[li] - S[p.t].hd[li]);
@@ -223,6 +240,8 @@ long join_impl(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t l2, int s
             }
             tri_pairs += tp;
             vp_refined += nv;
+            capped_vp += cvp;
+            capped_tp += ctp;
         });
         if (is_knn) par(n1, threads, [&](long q) { knn_rank(P, qoff[q], qoff[q + 1], knn, conf[q]); });
         long und = 0;
@@ -240,6 +259,10 @@ long join_impl(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t l2, int s
         stats[1] = (double)tri_pairs.load();
         stats[2] = (double)vp_refined.load();
         stats[3] = (double)P.size();
+    }
+    if (cap_stats) {
+        cap_stats[0] = (double)capped_vp.load();
+        cap_stats[1] = (double)capped_tp.load();
     }
     return n <= cap ? n : -n;
 }
@@ -264,4 +287,12 @@ extern "C" long tdr_join_sel(const uint8_t* b1, size_t l1, const uint8_t* b2, si
     if (nq <= 0) return 0;
     return join_impl(b1, l1, b2, l2, self_join, is_knn, knn, tau, lods, nlods, level, threads, 0,
                      std::vector<int>(qids, qids + nq), oq, ot, cap, stats);
+}
+
+// tdr_join with the cap of join_impl replayed (cap_rel >= 0); cap_stats as there.
+extern "C" long tdr_join_capped(const uint8_t* b1, size_t l1, const uint8_t* b2, size_t l2, int self_join,
+                                int is_knn, int knn, float tau, const int* lods, int nlods, int level, int threads,
+                                float cap_rel, int* oq, int* ot, long cap, double* stats, double* cap_stats) {
+    return join_impl(b1, l1, b2, l2, self_join, is_knn, knn, tau, lods, nlods, level, threads, 0, {}, oq, ot, cap,
+                     stats, cap_rel, cap_stats);
 }

@@ -157,3 +157,30 @@ def ref_join(tile1, tile2, self_join, is_knn, knn=1, tau=0.0, lods=None, level=2
             o = np.lexsort((t[:n], q[:n]))
             return q[:n][o], t[:n][o], st
         cap = -n
+
+
+def ref_join_capped(tile1, tile2, self_join, tau, cap_rel, lods=None, threads=0):
+    """The within join of the reference rules (level 2) with a cap replayed on
+    the LODs before the last (ref_join.cpp, join_impl): a voxel pair whose
+    Hausdorff lower bound comes out above the pair's cap keeps its previous
+    bounds.  Returns (q, t, (capped voxel-pair refines, their triangle pairs))."""
+    R = reference()
+    if R is None:
+        return None
+    L = R.L
+    L.tdr_join_capped.argtypes = [P, C.c_size_t, P, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_float, P, C.c_int,
+                                  C.c_int, C.c_int, C.c_float, P, P, C.c_long, P, P]
+    L.tdr_join_capped.restype = C.c_long
+    t1 = np.ascontiguousarray(tile1, np.uint8)
+    t2 = t1 if tile2 is None else np.ascontiguousarray(tile2, np.uint8)
+    lods = np.array(lods or [20, 40, 60, 80, 100], np.int32)
+    cap = 1 << 16
+    while True:
+        q = np.empty(cap, np.int32); t = np.empty(cap, np.int32); st = np.zeros(4); cs = np.zeros(2)
+        n = L.tdr_join_capped(_p(t1), t1.size, _p(t2), t2.size, int(self_join), 0, 0, float(tau), _p(lods),
+                              len(lods), 2, int(threads), float(cap_rel), _p(q), _p(t), cap, _p(st), _p(cs))
+        if n >= 0:
+            o = np.lexsort((t[:n], q[:n]))
+            return q[:n][o], t[:n][o], cs
+        cap = -n
+
