@@ -29,7 +29,7 @@ def test_capped_lods_keep_the_result_set(name):
     q0, t0, _ = ref_join(nb, t2, self_join, False, tau=tau, lods=lods, level=2)
     q1, t1, capped = ref_join_capped(nb, t2, self_join, tau, 1e-4, lods=lods)
     assert np.array_equal(q0, q1) and np.array_equal(t0, t1)
-    assert capped[1] <= capped[0] * 1e9
+    assert (capped >= 0).all()
 
 
 def test_caps_spare_part_of_the_refine():
